@@ -1,0 +1,335 @@
+"""Benchmark: plain wavefront path tracing on one B200 (or N independent replicas).
+
+Workload (cfg2): 1920x1080 image, ~4.7M-triangle scene (1024x1024-vertex fBm
+terrain + 512 icosphere/torus meshes), 2048x1024 HDRI dome + directional
+light, max depth 8, Russian roulette from depth 3.  One step = one progressive
+iteration (1 sample per pixel over the whole image, 2,073,600 camera paths);
+64 steps make the configuration's 64-spp frame.  The reference's estimator
+(compat flags) with the B200 alias-table dome sampler.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun with N ranks, every rank renders its own replica (the path
+tracer does not shard: replicas only); value = all ranks' paths / max time.
+`--impl reference` times the reference's algorithm on the host cores (the
+CPU oracle port, all threads), rank 0 only.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpaths/s and equal-time relMSE vs FP64 oracle, neural-guided vs plain, 1 B200"
+UNIT = "Mpaths/s"
+L2_BYTES = 126 * 1024 * 1024
+RAY_IN, HIT_OUT, NODE_BYTES, TRI_BYTES = 32, 16, 80, 48
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_desc(s):
+    return {"workload": f"{s.name}: wavefront path tracing {s.width}x{s.height}, max depth {s.max_depth}, RR from "
+                        f"{s.rr_start}, {s.num_triangles} triangles, {s.dome().texels.shape[1]}x"
+                        f"{s.dome().texels.shape[0]} HDRI dome + directional light; 1 step = 1 spp over the image "
+                        f"({s.spp} steps = the {s.spp}-spp frame)",
+            "image": [s.width, s.height], "triangles": s.num_triangles, "max_depth": s.max_depth,
+            "rr_start": s.rr_start, "spp_per_step": 1, "estimator": "reference (compat Q1-Q9) + alias dome sampler",
+            "l2": "inputs larger than L2 (BVH + scene + film > 126 MB), no flush", "seed": 0}
+
+
+class Dist:
+    def __init__(self, gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([float(x)], device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.proc, self.lines = index, None, []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=lambda: self.lines.extend(self.proc.stdout), daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the closest-hit kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "trace_closest_cfg2.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("dram_bytes_per_ray")
+    return None
+
+
+def cpu_baseline(scene, seconds, threads):
+    """The oracle (the reference's algorithm restated in C++) on the host cores,
+    1 spp over a strided pixel sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle
+    pyoracle.build()
+    o = pyoracle.OracleScene(scene.flatten())
+    npx = scene.width * scene.height
+    probe = np.arange(0, npx, max(1, npx // 2000), dtype=np.uint32)
+    t0 = time.perf_counter()
+    o.render(1, max_depth=scene.max_depth, rr_start=scene.rr_start, flags=pyoracle.COMPAT_ALL, pixels=probe,
+             threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    want = int(min(npx, max(1000, len(probe) * seconds / dt)))
+    pix = np.linspace(0, npx - 1, want).astype(np.uint32)
+    t0 = time.perf_counter()
+    _, _, cnt = o.render(1, max_depth=scene.max_depth, rr_start=scene.rr_start, flags=pyoracle.COMPAT_ALL,
+                         pixels=pix, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": round(len(pix) / dt / 1e6, 6), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(pix)} of {npx} pixels (evenly strided), 1 spp, {dt:.1f} s; "
+                      f"{int(cnt[0])} closest + {int(cnt[1])} shadow rays ({(cnt[0] + cnt[1]) / dt / 1e6:.3f} Mrays/s)"}
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from colvillea_b200 import scenes
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import pyoracle
+    pyoracle.build()
+    s = scenes.CONFIGS[args.config](0)
+    threads = os.cpu_count() or 1
+    o = pyoracle.OracleScene(s.flatten())
+    npx = s.width * s.height
+    # size one step to about one second of host work
+    probe = np.arange(0, npx, max(1, npx // 2000), dtype=np.uint32)
+    t0 = time.perf_counter()
+    o.render(1, max_depth=s.max_depth, rr_start=s.rr_start, flags=pyoracle.COMPAT_ALL, pixels=probe, threads=threads)
+    per = max(time.perf_counter() - t0, 1e-4) / len(probe)
+    nstep = int(min(npx, max(256, 1.0 / per)))
+    total, elapsed = 0, 0.0
+    for k in range(args.warmup + args.steps):
+        pix = ((np.arange(nstep, dtype=np.int64) * (npx // nstep) + k) % npx).astype(np.uint32)
+        t0 = time.perf_counter()
+        o.render(1, max_depth=s.max_depth, rr_start=s.rr_start, flags=pyoracle.COMPAT_ALL, pixels=pix,
+                 threads=threads, frame0=k)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            total += nstep
+            elapsed += dt
+    v = total / elapsed / 1e6
+    line = {"metric": METRIC, "value": round(v, 6), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * elapsed / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_desc(s),
+            "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"each step: 1 spp over {nstep} of {npx} pixels (strided), all host threads"},
+            "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+    dist = Dist(args.gpus)
+    torch.cuda.set_device(dist.local)
+    import colvillea_b200 as cb
+    from colvillea_b200 import build as cbuild, scenes
+    if not os.path.exists(os.path.join(ROOT, "colvillea_b200", "libcolvillea_b200.so")):
+        cbuild.build()
+    s = scenes.CONFIGS[args.config](0)
+    W, H = s.width, s.height
+    flags = cb.COMPAT_ALL | cb.DOME_ALIAS
+    it = cb.load_scene(s, flags=flags | cb.PROFILE_STAGES)
+    st0 = it.stats()
+
+    # Traversal counters on the identical ray set of the first timed step.
+    sit = cb.load_scene(s, flags=flags | cb.TRACE_STATS)
+    if args.warmup:
+        sit.render(args.warmup)
+    sit.render(1)
+    sst = sit.stats()
+    sit.close()
+
+    for _ in range(args.warmup):
+        it.render(1)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(dist.local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    ms_trace = ms_shade = ms_shadow = ms_dev = 0.0
+    rays_c = rays_s = 0
+    launches = trace_launches = 0
+    for _ in range(args.steps):
+        it.render(1)
+        st = it.stats()
+        ms_trace += st["ms_trace"]; ms_shade += st["ms_shade"]; ms_shadow += st["ms_shadow"]
+        ms_dev += st["ms_last_render"]
+        rays_c += st["last_rays_closest"]; rays_s += st["last_rays_shadow"]
+        launches += 1 + 4 * st["waves"]
+        trace_launches += st["waves"]
+    ev1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dist.barrier()
+    ms = dist.max(ev0.elapsed_time(ev1))
+    paths = W * H * args.steps * dist.world
+    value = paths / (ms * 1e-3) / 1e6
+
+    # End to end through the public API: camera in (host), render, film out to pinned host memory.
+    e2e = None
+    if not args.no_e2e:
+        film = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True)
+        arr = film.numpy()
+        cam = np.ascontiguousarray(s.camera, np.float32)
+        for _ in range(args.warmup):
+            it.updateCamera(cam); it.render(1); it.readbackFramebuffer(arr)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            it.updateCamera(cam)
+            it.render(1)
+            it.readbackFramebuffer(arr)
+        e1.record()
+        torch.cuda.synchronize()
+        ems = dist.max(e0.elapsed_time(e1))
+        e2e = {"value": round(W * H * args.steps * dist.world / (ems * 1e-3) / 1e6, 4), "unit": UNIT,
+               "h2d_bytes_per_step": int(cam.nbytes), "d2h_bytes_per_step": int(arr.nbytes),
+               "ms_per_step": round(ems / args.steps, 3)}
+    it.close()
+
+    if dist.rank != 0:
+        dist.close()
+        return 0
+    # Roofline of the dominant kernel: closest-hit traversal.
+    n_rays = max(1, sst["last_rays_closest"])
+    nodes_per_ray = sst["trace_nodes"] / n_rays
+    tris_per_ray = sst["trace_tris"] / n_rays
+    bytes_per_ray = RAY_IN + HIT_OUT + NODE_BYTES * nodes_per_ray + TRI_BYTES * tris_per_ray
+    achieved = bytes_per_ray * rays_c / (ms_trace * 1e-3) / 1e9 if ms_trace > 0 else None
+    peak, peak_kind = peaks()
+    traffic = ncu_traffic()
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {**workload_desc(s), "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"},
+        "mrays_per_s": round((rays_c + rays_s) * dist.world / (ms * 1e-3) / 1e6, 2),
+        "stage_ms_per_step": {"trace": round(ms_trace / args.steps, 3), "shade": round(ms_shade / args.steps, 3),
+                              "shadow": round(ms_shadow / args.steps, 3),
+                              "device_total": round(ms_dev / args.steps, 3)},
+        "roofline": {"kernel": "kTraceClosest (8-wide BVH closest hit)", "bound": "hbm",
+                     "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if achieved else None,
+                     "peak_kind": f"{peak_kind} HBM copy",
+                     "traffic": round(traffic * rays_c / max(1, trace_launches)) if traffic else None,
+                     "bytes_per_ray": round(bytes_per_ray, 1), "nodes_per_ray": round(nodes_per_ray, 2),
+                     "tris_per_ray": round(tris_per_ray, 2),
+                     "formula": "per closest-hit ray: 32 B ray + 16 B hit + 80 B x nodes + 48 B x triangles"},
+        "clocks": clk, "gpu_launches": launches,
+        "build": {"bvh_ms": round(st0["ms_bvh_build"], 2), "bvh_nodes": st0["bvh_nodes"],
+                  "bvh_depth": st0["bvh_depth"], "dome_ms": round(st0["ms_dome_build"], 2)},
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if dist.world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(s, args.cpu_seconds, os.cpu_count() or 1)
+    print(json.dumps(line))
+    dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,199 @@
+"""colvillea_b200: a B200 (sm_100a) wavefront path tracer behind Colvillea's
+integrator interface.
+
+The Python layer mirrors `colvillea::core::Integrator`
+(include/colvillea/librender/integrator.h:34-103): same method names and
+meaning, errors raised as ClError instead of the reference's exit(-1).
+All work runs in libcolvillea_b200.so (CUDA kernels for sm_100a, C ABI in
+include/colvillea_b200.h); there is no CPU fallback.
+"""
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _native as N
+from ._native import ClError
+
+__all__ = ["IntegratorType", "Integrator", "RenderConfig", "ClError", "COMPAT_ALL", "DOME_ALIAS", "FILM_FP64",
+           "PROFILE_STAGES", "TRACE_STATS", "load_scene"]
+
+COMPAT_PDF, COMPAT_FRAME, COMPAT_ESCAPE, COMPAT_ALL = N.CL_COMPAT_PDF, N.CL_COMPAT_FRAME, N.CL_COMPAT_ESCAPE, N.CL_COMPAT_ALL
+DOME_ALIAS, FILM_FP64, PROFILE_STAGES, TRACE_STATS = N.CL_DOME_ALIAS, N.CL_FILM_FP64, N.CL_PROFILE_STAGES, N.CL_TRACE_STATS
+
+
+class IntegratorType(enum.IntEnum):
+    """IntegratorType (integrator.h:22-32)."""
+    WavefrontDirectLighting = N.CL_INTEGRATOR_DIRECT_LIGHTING
+    WavefrontPathTracing = N.CL_INTEGRATOR_PATH_TRACING
+
+
+def RenderConfig(max_depth=5, rr_start_depth=0, flags=COMPAT_ALL, path_slots=0):
+    return N.RenderConfig(max_depth, rr_start_depth, flags, path_slots)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+class Integrator:
+    """A wavefront integrator on the current CUDA device (one stream)."""
+
+    def __init__(self, handle, itype, width, height):
+        self._h = handle
+        self.type = itype
+        self._size = (width, height)
+
+    @staticmethod
+    def createIntegrator(itype, width, height, config=None):
+        """Integrator::createIntegrator (src/core/librender/integrator.cpp:10-22)."""
+        h = ctypes.c_void_p()
+        cfg = config if config is not None else RenderConfig()
+        N.call("cl_integrator_create", int(itype), width, height, ctypes.byref(cfg), ctypes.byref(h))
+        return Integrator(h, IntegratorType(itype), width, height)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().cl_integrator_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- scene building (Integrator::build*) ---------------------------------
+    def buildBLAS(self, meshes):
+        """meshes: list of scenes.Mesh (positions, normals, tangents, uvs, indices)."""
+        keep, descs = [], (N.MeshDesc * len(meshes))()
+        for i, m in enumerate(meshes):
+            arrs = [_f32(m.positions), None if m.normals is None else _f32(m.normals), _f32(m.tangents),
+                    None if m.uvs is None else _f32(m.uvs), np.ascontiguousarray(m.indices, np.uint32)]
+            keep.append(arrs)
+            p, n, t, uv, idx = arrs
+            descs[i] = N.MeshDesc(_ptr(p), _ptr(n), _ptr(t), _ptr(uv), len(p), _ptr(idx), len(idx))
+        N.call("cl_build_meshes", self._h, descs, len(meshes))
+
+    def buildTLAS(self, instances):
+        """instances: list of (mesh_id, material_index, 3x4 row-major transform);
+        covers buildTLAS and buildGeometryEntities (integrator.h:49-54)."""
+        descs = (N.InstanceDesc * len(instances))()
+        for i, (mid, mat, xf) in enumerate(instances):
+            descs[i] = N.InstanceDesc(mid, mat, (ctypes.c_float * 12)(*xf))
+        N.call("cl_build_instances", self._h, descs, len(instances))
+
+    def buildMaterials(self, materials):
+        descs = (N.MaterialDesc * len(materials))()
+        for i, m in enumerate(materials):
+            descs[i] = N.MaterialDesc(m.type, (ctypes.c_float * 3)(*m.reflectance), m.roughness, m.interior_ior,
+                                      (ctypes.c_float * 3)(*m.eta), (ctypes.c_float * 3)(*m.k))
+        N.call("cl_build_materials", self._h, descs, len(materials))
+
+    def buildEmitters(self, emitters):
+        keep, descs = [], (N.EmitterDesc * len(emitters))()
+        for i, e in enumerate(emitters):
+            tex = None if e.texels is None else _f32(e.texels)
+            keep.append(tex)
+            h, w = (tex.shape[:2] if tex is not None else (0, 0))
+            descs[i] = N.EmitterDesc(e.type, (ctypes.c_float * 3)(*e.intensity), (ctypes.c_float * 3)(*e.direction),
+                                     e.angular_radius, _ptr(tex), w, h)
+        N.call("cl_build_emitters", self._h, descs, len(emitters))
+
+    def updateCamera(self, cam12):
+        c = _f32(cam12)
+        N.call("cl_update_camera", self._h, ctypes.byref(N.Camera(*(
+            (ctypes.c_float * 3)(*c[3 * i:3 * i + 3]) for i in range(4)))))
+
+    # --- rendering ------------------------------------------------------------
+    def render(self, spp=1):
+        """`spp` progressive iterations (Integrator::render, one per call in the reference)."""
+        N.call("cl_render", self._h, spp)
+
+    def resize(self, width, height):
+        N.call("cl_resize", self._h, width, height)
+        self._size = (width, height)
+
+    def getFilmSize(self):
+        w, h = ctypes.c_uint32(), ctypes.c_uint32()
+        N.call("cl_get_film_size", self._h, ctypes.byref(w), ctypes.byref(h))
+        return w.value, h.value
+
+    def resetIterationIndex(self):
+        N.call("cl_reset_iteration", self._h)
+
+    def readbackFramebuffer(self, out=None):
+        """Linear HDR mean radiance, (H, W, 4) float32."""
+        w, h = self._size
+        if out is None:
+            out = np.empty((h, w, 4), np.float32)
+        N.call("cl_readback_film", self._h, _ptr(out), out.nbytes)
+        return out
+
+    def readbackFilmStats(self):
+        """FP64 per-pixel (sum, sumsq) of per-sample radiance, each (H*W, 3)."""
+        w, h = self._size
+        s1 = np.zeros((w * h, 3)); s2 = np.zeros((w * h, 3))
+        N.call("cl_readback_film_stats", self._h, _ptr(s1), _ptr(s2), s1.size)
+        return s1, s2
+
+    def stats(self):
+        s = N.Stats()
+        N.call("cl_get_stats", self._h, ctypes.byref(s))
+        return s.as_dict()
+
+    # --- ray queries ------------------------------------------------------------
+    def traceRays(self, rays):
+        rays = _f32(rays)
+        n = len(rays)
+        t = np.zeros(n, np.float32); prim = np.zeros(n, np.uint32)
+        b1 = np.zeros(n, np.float32); b2 = np.zeros(n, np.float32)
+        N.call("cl_trace_rays", self._h, _ptr(rays), n, _ptr(t), _ptr(prim), _ptr(b1), _ptr(b2))
+        return t, prim, b1, b2
+
+    def occludedRays(self, rays):
+        rays = _f32(rays)
+        occ = np.zeros(len(rays), np.uint8)
+        N.call("cl_occluded_rays", self._h, _ptr(rays), len(rays), _ptr(occ))
+        return occ
+
+    def traceStats(self, rays):
+        rays = _f32(rays)
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        N.call("cl_trace_stats", self._h, _ptr(rays), len(rays), ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def domeTables(self, w, h):
+        pU = np.zeros((w + 1) * h, np.float32); cU = np.zeros_like(pU)
+        pV = np.zeros(h + 1, np.float32); cV = np.zeros_like(pV)
+        N.call("cl_get_dome_tables", self._h, _ptr(pU), _ptr(cU), _ptr(pV), _ptr(cV))
+        return pU, cU, pV, cV
+
+    def domeAliasSample(self, u2):
+        u2 = _f32(u2)
+        n = len(u2)
+        d = np.zeros((n, 3), np.float32); p = np.zeros(n, np.float32); v = np.zeros((n, 3), np.float32)
+        N.call("cl_dome_alias_sample", self._h, _ptr(u2), _ptr(d), _ptr(p), _ptr(v), n)
+        return d, p, v
+
+
+def load_scene(scene, itype=IntegratorType.WavefrontPathTracing, flags=COMPAT_ALL, max_depth=None, rr_start=None,
+               path_slots=0):
+    """Integrator for a colvillea_b200.scenes.Scene, scene built, camera set
+    (the RenderEngine::startRendering compile sequence, renderengine.cpp:27-114)."""
+    cfg = RenderConfig(scene.max_depth if max_depth is None else max_depth,
+                       scene.rr_start if rr_start is None else rr_start, flags, path_slots)
+    it = Integrator.createIntegrator(itype, scene.width, scene.height, cfg)
+    it.buildMaterials(scene.materials)
+    it.buildBLAS(scene.meshes)
+    it.buildTLAS(scene.instances)
+    it.buildEmitters(scene.emitters)
+    it.updateCamera(scene.camera)
+    return it

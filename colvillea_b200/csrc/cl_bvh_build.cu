@@ -1,0 +1,600 @@
+// Device build of the 8-wide compressed BVH (layout in cl_bvh.cuh).
+//
+// Replaces OptiX's BLAS/TLAS builds (owlGroupBuildAccel,
+// src/core/devices/optixdevice.cpp:136-233) with a hand-written builder:
+//   1. per-triangle boxes and centroid bounds;
+//   2. 63-bit Morton codes of the centroids, sorted (CUB radix sort);
+//   3. binary radix tree (Karras, HPG 2012), one thread per inner node;
+//   4. bottom-up boxes and triangle counts (atomic arrival counters);
+//   5. top-down collapse to 8-wide nodes, one level per launch: each wide
+//      node greedily opens its largest-area child with more than 3 triangles
+//      until it has 8 children; children with at most 3 triangles become
+//      leaf slots; slots are assigned by octant; child boxes are quantised to
+//      8 bits per plane, rounded outwards around a widened parent box.
+#include "cl_bvh.cuh"
+#include "cl_internal.h"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <vector>
+
+namespace clb
+{
+namespace
+{
+constexpr uint32_t kLeafFlag = 0x80000000u;
+
+__device__ __forceinline__ uint32_t fordered(float f)
+{
+    uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float funordered(uint32_t b)
+{
+    return __uint_as_float((b & 0x80000000u) ? (b & 0x7fffffffu) : ~b);
+}
+
+struct Bounds
+{
+    uint32_t clo[3], chi[3]; // centroid bounds (ordered ints)
+    uint32_t slo[3], shi[3]; // scene bounds
+};
+
+__global__ void kTriBounds(const float* __restrict__ tri9, uint32_t n, float* __restrict__ lo, float* __restrict__ hi,
+                           Bounds* b)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float    c[3], l[3], h[3];
+    bool     valid = i < n;
+    if (valid)
+    {
+        const float* t = tri9 + 9 * size_t(i);
+        for (int a = 0; a < 3; ++a)
+        {
+            l[a] = fminf(fminf(t[a], t[3 + a]), t[6 + a]);
+            h[a] = fmaxf(fmaxf(t[a], t[3 + a]), t[6 + a]);
+            c[a] = 0.5f * l[a] + 0.5f * h[a];
+            lo[3 * size_t(i) + a] = l[a];
+            hi[3 * size_t(i) + a] = h[a];
+        }
+    }
+    for (int a = 0; a < 3; ++a)
+    {
+        uint32_t cl = valid ? fordered(c[a]) : 0xffffffffu, ch = valid ? fordered(c[a]) : 0u;
+        uint32_t sl = valid ? fordered(l[a]) : 0xffffffffu, sh = valid ? fordered(h[a]) : 0u;
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            cl = min(cl, __shfl_xor_sync(0xffffffffu, cl, o));
+            ch = max(ch, __shfl_xor_sync(0xffffffffu, ch, o));
+            sl = min(sl, __shfl_xor_sync(0xffffffffu, sl, o));
+            sh = max(sh, __shfl_xor_sync(0xffffffffu, sh, o));
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            atomicMin(&b->clo[a], cl);
+            atomicMax(&b->chi[a], ch);
+            atomicMin(&b->slo[a], sl);
+            atomicMax(&b->shi[a], sh);
+        }
+    }
+}
+
+__device__ __forceinline__ uint64_t expand21(uint32_t v)
+{
+    uint64_t x = v & 0x1fffffu;
+    x          = (x | x << 32) & 0x1f00000000ffffull;
+    x          = (x | x << 16) & 0x1f0000ff0000ffull;
+    x          = (x | x << 8) & 0x100f00f00f00f00full;
+    x          = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x          = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+
+__global__ void kMorton(const float* __restrict__ lo, const float* __restrict__ hi, uint32_t n, const Bounds* b,
+                        uint64_t* __restrict__ keys, uint32_t* __restrict__ ids)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t q[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        float cmin = funordered(b->clo[a]), cmax = funordered(b->chi[a]);
+        float c    = 0.5f * lo[3 * size_t(i) + a] + 0.5f * hi[3 * size_t(i) + a];
+        float ext  = cmax - cmin;
+        float u    = ext > 0.0f ? (c - cmin) / ext : 0.5f;
+        u          = fminf(fmaxf(u, 0.0f), 1.0f);
+        q[a]       = min(uint32_t(u * 2097152.0f), 2097151u);
+    }
+    keys[i] = expand21(q[0]) | (expand21(q[1]) << 1) | (expand21(q[2]) << 2);
+    ids[i]  = i;
+}
+
+__device__ __forceinline__ int delta(const uint64_t* keys, int n, int i, int j)
+{
+    if (j < 0 || j > n - 1) return -1;
+    uint64_t a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz(uint32_t(i) ^ uint32_t(j));
+    return __clzll(a ^ b);
+}
+
+__global__ void kRadixTree(const uint64_t* __restrict__ keys, int n, uint32_t* __restrict__ left,
+                           uint32_t* __restrict__ right, uint32_t* __restrict__ parent)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d    = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j     = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s     = 0;
+    int t     = l;
+    do
+    {
+        t = (t + 1) / 2;
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+    } while (t > 1);
+    int      g  = i + s * d + min(d, 0);
+    uint32_t lc = (min(i, j) == g) ? (uint32_t(g) | kLeafFlag) : uint32_t(g);
+    uint32_t rc = (max(i, j) == g + 1) ? (uint32_t(g + 1) | kLeafFlag) : uint32_t(g + 1);
+    left[i]     = lc;
+    right[i]    = rc;
+    parent[(lc & kLeafFlag) ? (n - 1 + (lc & ~kLeafFlag)) : lc] = uint32_t(i);
+    parent[(rc & kLeafFlag) ? (n - 1 + (rc & ~kLeafFlag)) : rc] = uint32_t(i);
+}
+
+__device__ __forceinline__ void refBox(uint32_t ref, const float* lo, const float* hi, const uint32_t* ids,
+                                       const float* nlo, const float* nhi, float* l, float* h)
+{
+    if (ref & kLeafFlag)
+    {
+        uint32_t t = ids[ref & ~kLeafFlag];
+        for (int a = 0; a < 3; ++a)
+        {
+            l[a] = lo[3 * size_t(t) + a];
+            h[a] = hi[3 * size_t(t) + a];
+        }
+    }
+    else
+        for (int a = 0; a < 3; ++a)
+        {
+            l[a] = __ldcg(nlo + 3 * size_t(ref) + a);
+            h[a] = __ldcg(nhi + 3 * size_t(ref) + a);
+        }
+}
+
+__global__ void kBottomUp(int n, const float* __restrict__ lo, const float* __restrict__ hi, const uint32_t* __restrict__ ids,
+                          const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                          const uint32_t* __restrict__ parent, float* nlo, float* nhi, uint32_t* count,
+                          uint32_t* arrive)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint32_t node = parent[n - 1 + j];
+    while (node != 0xffffffffu)
+    {
+        __threadfence();
+        if (atomicAdd(&arrive[node], 1u) == 0u) return;
+        __threadfence();
+        float    l0[3], h0[3], l1[3], h1[3];
+        uint32_t a = left[node], b = right[node];
+        refBox(a, lo, hi, ids, nlo, nhi, l0, h0);
+        refBox(b, lo, hi, ids, nlo, nhi, l1, h1);
+        for (int k = 0; k < 3; ++k)
+        {
+            nlo[3 * size_t(node) + k] = fminf(l0[k], l1[k]);
+            nhi[3 * size_t(node) + k] = fmaxf(h0[k], h1[k]);
+        }
+        uint32_t ca = (a & kLeafFlag) ? 1u : __ldcg(count + a);
+        uint32_t cb = (b & kLeafFlag) ? 1u : __ldcg(count + b);
+        count[node] = ca + cb;
+        node        = parent[node];
+    }
+}
+
+struct CollapseArgs
+{
+    const float*    triPos; // 9 floats per triangle, original order
+    const float*    lo;     // triangle boxes
+    const float*    hi;
+    const uint32_t* ids;    // sorted position -> triangle id
+    const uint32_t* left;
+    const uint32_t* right;
+    const float*    nlo;
+    const float*    nhi;
+    const uint32_t* count;
+    uint4*          nodes;
+    float4*         tris;
+    uint32_t*       nodeCounter;
+    uint32_t*       triCounter;
+    uint32_t*       nextCount;
+    uint2*          nextTasks;
+    float           margin;
+    uint32_t        maxNodes;
+    uint32_t*       err;
+};
+
+__device__ __forceinline__ uint32_t refCount(const CollapseArgs& A, uint32_t r)
+{
+    return (r & kLeafFlag) ? 1u : A.count[r];
+}
+
+__device__ __forceinline__ uint32_t quantExp(float ext)
+{
+    // Smallest power of two e with 255 * e >= ext; returns its biased exponent.
+    float    x  = ext / 255.0f;
+    uint32_t b  = __float_as_uint(x);
+    uint32_t ex = (b >> 23) & 0xffu;
+    if (b & 0x7fffffu) ex += 1;
+    if (ex < 1) ex = 1;
+    if (ex > 254) ex = 254;
+    float e = __uint_as_float(ex << 23);
+    while (e * 255.0f < ext && ex < 254)
+    {
+        ++ex;
+        e = __uint_as_float(ex << 23);
+    }
+    return ex;
+}
+
+__global__ void kCollapse(CollapseArgs A, const uint2* __restrict__ tasks, uint32_t ntasks)
+{
+    uint32_t ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= ntasks) return;
+    uint32_t ref  = tasks[ti].x;
+    uint32_t wide = tasks[ti].y;
+
+    uint32_t ch[8];
+    int      cnt = 0;
+    if ((ref & kLeafFlag) || A.count[ref] <= 3u)
+        ch[cnt++] = ref;
+    else
+    {
+        ch[cnt++] = A.left[ref];
+        ch[cnt++] = A.right[ref];
+        while (cnt < 8)
+        {
+            int   best = -1;
+            float bestArea = -1.0f;
+            for (int k = 0; k < cnt; ++k)
+            {
+                uint32_t r = ch[k];
+                if ((r & kLeafFlag) || A.count[r] <= 3u) continue;
+                float dx = A.nhi[3 * size_t(r)] - A.nlo[3 * size_t(r)];
+                float dy = A.nhi[3 * size_t(r) + 1] - A.nlo[3 * size_t(r) + 1];
+                float dz = A.nhi[3 * size_t(r) + 2] - A.nlo[3 * size_t(r) + 2];
+                float area = dx * dy + dy * dz + dz * dx;
+                if (area > bestArea)
+                {
+                    bestArea = area;
+                    best     = k;
+                }
+            }
+            if (best < 0) break;
+            uint32_t r = ch[best];
+            ch[best]   = A.left[r];
+            ch[cnt++]  = A.right[r];
+        }
+    }
+
+    // Child boxes, parent box (widened by the margin).
+    float clo[8][3], chi[8][3], plo[3], phi[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        plo[a] = FLT_MAX;
+        phi[a] = -FLT_MAX;
+    }
+    for (int k = 0; k < cnt; ++k)
+    {
+        refBox(ch[k], A.lo, A.hi, A.ids, A.nlo, A.nhi, clo[k], chi[k]);
+        for (int a = 0; a < 3; ++a)
+        {
+            clo[k][a] -= A.margin;
+            chi[k][a] += A.margin;
+            plo[a] = fminf(plo[a], clo[k][a]);
+            phi[a] = fmaxf(phi[a], chi[k][a]);
+        }
+    }
+
+    // Octant slot assignment (greedy on the alignment of child offset and
+    // slot direction).
+    int   slotOf[8];
+    bool  used[8] = {false, false, false, false, false, false, false, false};
+    bool  done[8] = {false, false, false, false, false, false, false, false};
+    float pc[3];
+    for (int a = 0; a < 3; ++a) pc[a] = 0.5f * (plo[a] + phi[a]);
+    for (int it = 0; it < cnt; ++it)
+    {
+        float bestC = -FLT_MAX;
+        int   bk = 0, bs = 0;
+        for (int k = 0; k < cnt; ++k)
+        {
+            if (done[k]) continue;
+            float dx = 0.5f * (clo[k][0] + chi[k][0]) - pc[0];
+            float dy = 0.5f * (clo[k][1] + chi[k][1]) - pc[1];
+            float dz = 0.5f * (clo[k][2] + chi[k][2]) - pc[2];
+            for (int s = 0; s < 8; ++s)
+            {
+                if (used[s]) continue;
+                float c = ((s & 1) ? dx : -dx) + ((s & 2) ? dy : -dy) + ((s & 4) ? dz : -dz);
+                if (c > bestC)
+                {
+                    bestC = c;
+                    bk    = k;
+                    bs    = s;
+                }
+            }
+        }
+        done[bk]   = true;
+        used[bs]   = true;
+        slotOf[bk] = bs;
+    }
+    int childAt[8];
+    for (int s = 0; s < 8; ++s) childAt[s] = -1;
+    for (int k = 0; k < cnt; ++k) childAt[slotOf[k]] = k;
+
+    uint32_t nInner = 0, nTris = 0;
+    for (int k = 0; k < cnt; ++k)
+    {
+        uint32_t c = refCount(A, ch[k]);
+        if (c <= 3u)
+            nTris += c;
+        else
+            ++nInner;
+    }
+    uint32_t base  = nInner ? atomicAdd(A.nodeCounter, nInner) : 0u;
+    uint32_t tbase = atomicAdd(A.triCounter, nTris);
+    if (base + nInner > A.maxNodes)
+    {
+        atomicOr(A.err, 2u);
+        return;
+    }
+
+    // Quantisation frame.
+    uint32_t ex[3];
+    float    e[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        ex[a] = quantExp(phi[a] - plo[a]);
+        e[a]  = __uint_as_float(ex[a] << 23);
+    }
+    uint32_t imask = 0, meta[2] = {0, 0}, qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    uint32_t innerRank = 0, triOff = 0;
+    for (int s = 0; s < 8; ++s)
+    {
+        int      word = s >> 2, sh = 8 * (s & 3);
+        int      k    = childAt[s];
+        uint32_t ql[3], qh[3];
+        if (k < 0)
+        {
+            ql[0] = ql[1] = ql[2] = 255u;
+            qh[0] = qh[1] = qh[2] = 0u;
+        }
+        else
+        {
+            for (int a = 0; a < 3; ++a)
+            {
+                int lo_ = int(floorf((clo[k][a] - plo[a]) / e[a]));
+                int hi_ = int(ceilf((chi[k][a] - plo[a]) / e[a]));
+                lo_     = max(0, min(255, lo_));
+                hi_     = max(0, min(255, hi_));
+                while (lo_ > 0 && plo[a] + e[a] * float(lo_) > clo[k][a]) --lo_;
+                while (hi_ < 255 && plo[a] + e[a] * float(hi_) < chi[k][a]) ++hi_;
+                ql[a] = uint32_t(lo_);
+                qh[a] = uint32_t(hi_);
+            }
+            uint32_t r = ch[k];
+            uint32_t c = refCount(A, r);
+            if (c > 3u)
+            {
+                imask |= 1u << s;
+                uint32_t slotIdx        = base + innerRank++;
+                uint32_t ti2            = atomicAdd(A.nextCount, 1u);
+                A.nextTasks[ti2]        = make_uint2(r, slotIdx);
+            }
+            else
+            {
+                // Gather the subtree's triangles (at most 3).
+                uint32_t st[4];
+                int      sp = 0;
+                st[sp++]    = r;
+                uint32_t got = 0;
+                while (sp > 0)
+                {
+                    uint32_t x = st[--sp];
+                    if (x & kLeafFlag)
+                    {
+                        uint32_t tid = A.ids[x & ~kLeafFlag];
+                        const float* tp = A.triPos + 9 * size_t(tid);
+                        float4* dst = A.tris + size_t(tbase + triOff + got) * 3;
+                        dst[0]      = make_float4(tp[0], tp[1], tp[2], __uint_as_float(tid));
+                        dst[1]      = make_float4(tp[3], tp[4], tp[5], 0.0f);
+                        dst[2]      = make_float4(tp[6], tp[7], tp[8], 0.0f);
+                        ++got;
+                    }
+                    else
+                    {
+                        st[sp++] = A.right[x];
+                        st[sp++] = A.left[x];
+                    }
+                }
+                uint32_t unary = (1u << got) - 1u;
+                meta[word] |= ((unary << 5) | triOff) << sh;
+                triOff += got;
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+        {
+            qlo[a][word] |= ql[a] << sh;
+            qhi[a][word] |= qh[a] << sh;
+        }
+    }
+    uint4* np = A.nodes + size_t(wide) * 5;
+    np[0]     = make_uint4(__float_as_uint(plo[0]), __float_as_uint(plo[1]), __float_as_uint(plo[2]),
+                           ex[0] | (ex[1] << 8) | (ex[2] << 16) | (imask << 24));
+    np[1]     = make_uint4(base, tbase, meta[0], meta[1]);
+    np[2]     = make_uint4(qlo[0][0], qlo[0][1], qlo[1][0], qlo[1][1]);
+    np[3]     = make_uint4(qlo[2][0], qlo[2][1], qhi[0][0], qhi[0][1]);
+    np[4]     = make_uint4(qhi[1][0], qhi[1][1], qhi[2][0], qhi[2][1]);
+}
+
+} // namespace
+
+cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err)
+{
+    out->release();
+    if (n == 0)
+    {
+        *err = "cannot build a BVH over zero triangles";
+        return CL_ERR_INVALID_ARG;
+    }
+    DevBuf lo, hi, keys, keys2, ids, ids2, left, right, parent, nlo, nhi, count, arrive, bounds, tmp, tasksA, tasksB,
+        ctr;
+    size_t nn = n;
+    CL_TRY(lo.alloc(nn * 3 * 4, err));
+    CL_TRY(hi.alloc(nn * 3 * 4, err));
+    CL_TRY(keys.alloc(nn * 8, err));
+    CL_TRY(keys2.alloc(nn * 8, err));
+    CL_TRY(ids.alloc(nn * 4, err));
+    CL_TRY(ids2.alloc(nn * 4, err));
+    size_t ni = nn > 1 ? nn - 1 : 1;
+    CL_TRY(left.alloc(ni * 4, err));
+    CL_TRY(right.alloc(ni * 4, err));
+    CL_TRY(parent.alloc((2 * nn) * 4, err));
+    CL_TRY(nlo.alloc(ni * 3 * 4, err));
+    CL_TRY(nhi.alloc(ni * 3 * 4, err));
+    CL_TRY(count.alloc(ni * 4, err));
+    CL_TRY(arrive.alloc(ni * 4, err));
+    CL_TRY(bounds.alloc(sizeof(Bounds), err));
+    CL_TRY(ctr.alloc(16, err));
+
+    Bounds b0;
+    for (int a = 0; a < 3; ++a)
+    {
+        b0.clo[a] = b0.slo[a] = 0xffffffffu;
+        b0.chi[a] = b0.shi[a] = 0u;
+    }
+    CL_CUDA(cudaMemcpyAsync(bounds.p, &b0, sizeof(b0), cudaMemcpyHostToDevice, st), err);
+    uint32_t blocks = (n + 255) / 256;
+    kTriBounds<<<blocks, 256, 0, st>>>(dTri9, n, lo.f(), hi.f(), (Bounds*)bounds.p);
+    kMorton<<<blocks, 256, 0, st>>>(lo.f(), hi.f(), n, (Bounds*)bounds.p, (uint64_t*)keys.p, ids.u());
+    CL_CUDA(cudaGetLastError(), err);
+
+    size_t tmpBytes = 0;
+    CL_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpBytes, (uint64_t*)keys.p, (uint64_t*)keys2.p, ids.u(), ids2.u(),
+                                            int(n), 0, 63, st),
+            err);
+    CL_TRY(tmp.alloc(tmpBytes, err));
+    CL_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmpBytes, (uint64_t*)keys.p, (uint64_t*)keys2.p, ids.u(), ids2.u(),
+                                            int(n), 0, 63, st),
+            err);
+    tmp.release();
+    keys.release();
+    ids.release();
+
+    CL_CUDA(cudaMemsetAsync(parent.p, 0xff, 2 * nn * 4, st), err);
+    CL_CUDA(cudaMemsetAsync(arrive.p, 0, ni * 4, st), err);
+    if (n > 1)
+    {
+        kRadixTree<<<(n - 1 + 255) / 256, 256, 0, st>>>((uint64_t*)keys2.p, int(n), left.u(), right.u(), parent.u());
+        kBottomUp<<<blocks, 256, 0, st>>>(int(n), lo.f(), hi.f(), ids2.u(), left.u(), right.u(), parent.u(), nlo.f(),
+                                          nhi.f(), count.u(), arrive.u());
+        CL_CUDA(cudaGetLastError(), err);
+    }
+
+    Bounds bh;
+    CL_CUDA(cudaMemcpyAsync(&bh, bounds.p, sizeof(bh), cudaMemcpyDeviceToHost, st), err);
+    CL_CUDA(cudaStreamSynchronize(st), err);
+    float scale = 0.0f;
+    for (int a = 0; a < 3; ++a)
+    {
+        auto unord = [](uint32_t v) {
+            uint32_t bits = (v & 0x80000000u) ? (v & 0x7fffffffu) : ~v;
+            float    f;
+            memcpy(&f, &bits, 4);
+            return f;
+        };
+        float l = unord(bh.slo[a]), h = unord(bh.shi[a]);
+        scale   = std::max(scale, std::max(std::fabs(l), std::fabs(h)));
+        scale   = std::max(scale, h - l);
+    }
+    float margin = scale * 9.5367431640625e-07f + 1e-30f; // 2^-20 of the scene scale
+
+    uint32_t maxNodes = n + 1;
+    CL_TRY(out->nodes.alloc(size_t(maxNodes) * 80, err));
+    CL_TRY(out->tris.alloc(nn * 48, err));
+    size_t taskCap = nn / 2 + 8;
+    CL_TRY(tasksA.alloc(taskCap * 8, err));
+    CL_TRY(tasksB.alloc(taskCap * 8, err));
+    // ctr: [0] node counter, [1] tri counter, [2] next task count, [3] error
+    uint32_t c0[4] = {1u, 0u, 0u, 0u};
+    CL_CUDA(cudaMemcpyAsync(ctr.p, c0, 16, cudaMemcpyHostToDevice, st), err);
+    uint2 root = make_uint2(n > 1 ? 0u : kLeafFlag, 0u);
+    CL_CUDA(cudaMemcpyAsync(tasksA.p, &root, 8, cudaMemcpyHostToDevice, st), err);
+
+    CollapseArgs A;
+    A.triPos      = dTri9;
+    A.lo          = lo.f();
+    A.hi          = hi.f();
+    A.ids         = ids2.u();
+    A.left        = left.u();
+    A.right       = right.u();
+    A.nlo         = nlo.f();
+    A.nhi         = nhi.f();
+    A.count       = count.u();
+    A.nodes       = (uint4*)out->nodes.p;
+    A.tris        = (float4*)out->tris.p;
+    A.nodeCounter = ctr.u() + 0;
+    A.triCounter  = ctr.u() + 1;
+    A.nextCount   = ctr.u() + 2;
+    A.margin      = margin;
+    A.maxNodes    = maxNodes;
+    A.err         = ctr.u() + 3;
+
+    uint32_t ntasks = 1, depth = 0;
+    DevBuf*  cur = &tasksA;
+    DevBuf*  nxt = &tasksB;
+    while (ntasks > 0)
+    {
+        ++depth;
+        A.nextTasks = (uint2*)nxt->p;
+        CL_CUDA(cudaMemsetAsync(ctr.u() + 2, 0, 4, st), err);
+        kCollapse<<<(ntasks + 63) / 64, 64, 0, st>>>(A, (const uint2*)cur->p, ntasks);
+        CL_CUDA(cudaGetLastError(), err);
+        uint32_t hc[4];
+        CL_CUDA(cudaMemcpyAsync(hc, ctr.p, 16, cudaMemcpyDeviceToHost, st), err);
+        CL_CUDA(cudaStreamSynchronize(st), err);
+        if (hc[3])
+        {
+            *err = "BVH collapse exceeded its node bound";
+            return CL_ERR_STATE;
+        }
+        ntasks = hc[2];
+        if (ntasks > taskCap)
+        {
+            *err = "BVH collapse task list overflow";
+            return CL_ERR_STATE;
+        }
+        std::swap(cur, nxt);
+        out->numNodes = hc[0];
+        if (hc[1] > n)
+        {
+            *err = "BVH collapse emitted too many triangles";
+            return CL_ERR_STATE;
+        }
+    }
+    out->depth   = depth;
+    out->numTris = n;
+    if (depth + 1 > uint32_t(kStackDepth))
+    {
+        *err = "BVH depth " + std::to_string(depth) + " exceeds the traversal stack";
+        return CL_ERR_STATE;
+    }
+    return CL_OK;
+}
+
+} // namespace clb

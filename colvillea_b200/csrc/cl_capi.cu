@@ -1,0 +1,321 @@
+// C ABI (include/colvillea_b200.h) over the C++ integrator.  Every entry
+// point returns a status and records a message for cl_last_error; no entry
+// point throws or exits (the reference exits on CUDA errors,
+// src/core/devices/cudacommon.h:13-26).
+#include "cl_integrator.h"
+
+#include <new>
+
+struct cl_integrator
+{
+    clb::Integrator impl;
+    cl_integrator(cl_integrator_type t, uint32_t w, uint32_t h, const cl_render_config& c) : impl(t, w, h, c) {}
+};
+
+namespace clb
+{
+static thread_local std::string gLastError;
+void setLastError(const std::string& msg) { gLastError = msg; }
+
+cl_status unitBsdfEval(uint32_t, const float*, const float*, const float*, float*, uint32_t, std::string*);
+cl_status unitBsdfPdf(uint32_t, const float*, const float*, const float*, float*, uint32_t, uint32_t, std::string*);
+cl_status unitBsdfSample(uint32_t, const float*, const float*, const float*, float*, float*, float*, uint32_t,
+                         std::string*);
+cl_status unitGgxEval(const float*, const float*, const float*, const float*, float*, float*, float*, float*, uint32_t,
+                      std::string*);
+cl_status unitGgxSample(const float*, const float*, float*, float*, uint32_t, std::string*);
+cl_status unitFresnelConductor(const float*, const float*, const float*, float*, uint32_t, std::string*);
+cl_status unitFresnelDielectric(const float*, const float*, float*, float*, uint32_t, std::string*);
+cl_status unitWarp(const float*, float*, float*, uint32_t, std::string*);
+cl_status unitMakeFrame(const float*, float*, float*, uint32_t, std::string*);
+cl_status unitFrame(const float*, const float*, const float*, const float*, float*, float*, uint32_t, std::string*);
+cl_status unitPcg(const uint32_t*, uint32_t*, uint32_t, std::string*);
+cl_status unitSeq(const uint32_t*, uint32_t, uint32_t, float*, std::string*);
+cl_status unitDomeSample(const float*, uint32_t, uint32_t, const float*, const float*, const float*, const float*,
+                         const float*, float*, float*, float*, uint32_t, std::string*);
+cl_status unitDomePdfEval(const float*, uint32_t, uint32_t, const float*, const float*, const float*, float*, float*,
+                          uint32_t, std::string*);
+cl_status unitDirectional(const float*, const float*, float*, float*, float*, uint32_t, std::string*);
+} // namespace clb
+
+namespace
+{
+template <class F> cl_status guarded(F&& f)
+{
+    std::string err;
+    cl_status   s;
+    try
+    {
+        s = f(&err);
+    }
+    catch (const std::bad_alloc&)
+    {
+        err = "host allocation failed";
+        s   = CL_ERR_OOM;
+    }
+    catch (const std::exception& e)
+    {
+        err = e.what();
+        s   = CL_ERR_STATE;
+    }
+    if (s != CL_OK)
+        clb::setLastError(err.empty() ? std::string("error ") + std::to_string(s) : err);
+    return s;
+}
+
+#define CL_NEED(ptr)                                                                                                   \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        if (!(ptr))                                                                                                    \
+        {                                                                                                              \
+            clb::setLastError(#ptr " is null");                                                                        \
+            return CL_ERR_INVALID_ARG;                                                                                 \
+        }                                                                                                              \
+    } while (0)
+} // namespace
+
+extern "C" {
+
+cl_status cl_integrator_create(cl_integrator_type type, uint32_t width, uint32_t height, const cl_render_config* config,
+                               cl_integrator** out)
+{
+    CL_NEED(out);
+    *out = nullptr;
+    if (type != CL_INTEGRATOR_PATH_TRACING && type != CL_INTEGRATOR_DIRECT_LIGHTING)
+    {
+        clb::setLastError("unknown integrator type");
+        return CL_ERR_INVALID_ARG;
+    }
+    cl_render_config cfg{5u, 0u, CL_COMPAT_ALL, 0u};
+    if (config) cfg = *config;
+    return guarded([&](std::string* err) -> cl_status {
+        auto* it = new cl_integrator(type, width, height, cfg);
+        cl_status s = it->impl.init(err);
+        if (s != CL_OK)
+        {
+            delete it;
+            return s;
+        }
+        *out = it;
+        return CL_OK;
+    });
+}
+
+cl_status cl_integrator_destroy(cl_integrator* it)
+{
+    delete it;
+    return CL_OK;
+}
+
+cl_status cl_build_meshes(cl_integrator* it, const cl_mesh_desc* meshes, uint32_t count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.buildMeshes(meshes, count, e); });
+}
+
+cl_status cl_build_instances(cl_integrator* it, const cl_instance_desc* instances, uint32_t count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.buildInstances(instances, count, e); });
+}
+
+cl_status cl_build_materials(cl_integrator* it, const cl_material_desc* materials, uint32_t count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.buildMaterials(materials, count, e); });
+}
+
+cl_status cl_build_emitters(cl_integrator* it, const cl_emitter_desc* emitters, uint32_t count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.buildEmitters(emitters, count, e); });
+}
+
+cl_status cl_update_camera(cl_integrator* it, const cl_camera* camera)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.updateCamera(camera, e); });
+}
+
+cl_status cl_render(cl_integrator* it, uint32_t spp)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.render(spp, e); });
+}
+
+cl_status cl_readback_film(cl_integrator* it, float* rgba, size_t bytes)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.readbackFilm(rgba, bytes, e); });
+}
+
+cl_status cl_readback_film_stats(cl_integrator* it, double* sum, double* sumsq, size_t count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.readbackFilmStats(sum, sumsq, count, e); });
+}
+
+cl_status cl_resize(cl_integrator* it, uint32_t width, uint32_t height)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.resize(width, height, e); });
+}
+
+cl_status cl_get_film_size(cl_integrator* it, uint32_t* width, uint32_t* height)
+{
+    CL_NEED(it);
+    CL_NEED(width);
+    CL_NEED(height);
+    *width  = it->impl.width();
+    *height = it->impl.height();
+    return CL_OK;
+}
+
+cl_status cl_reset_iteration(cl_integrator* it)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.resetIteration(e); });
+}
+
+cl_status cl_get_stats(cl_integrator* it, cl_stats* stats)
+{
+    CL_NEED(it);
+    CL_NEED(stats);
+    it->impl.stats(stats);
+    return CL_OK;
+}
+
+cl_status cl_last_error(char* buffer, size_t size)
+{
+    CL_NEED(buffer);
+    if (size == 0) return CL_ERR_INVALID_ARG;
+    const std::string& s = clb::gLastError;
+    size_t             n = std::min(size - 1, s.size());
+    memcpy(buffer, s.data(), n);
+    buffer[n] = '\0';
+    return CL_OK;
+}
+
+cl_status cl_trace_rays(cl_integrator* it, const float* rays, uint32_t count, float* t, uint32_t* prim, float* b1,
+                        float* b2)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.traceRays(rays, count, t, prim, b1, b2, e); });
+}
+
+cl_status cl_occluded_rays(cl_integrator* it, const float* rays, uint32_t count, uint8_t* occluded)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.occludedRays(rays, count, occluded, e); });
+}
+
+cl_status cl_trace_stats(cl_integrator* it, const float* rays, uint32_t count, uint64_t* nodes, uint64_t* triangles)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.traceStats(rays, count, nodes, triangles, e); });
+}
+
+cl_status cl_get_dome_tables(cl_integrator* it, float* pU, float* cU, float* pV, float* cV)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.domeTables(pU, cU, pV, cV, e); });
+}
+
+cl_status cl_dome_alias_sample(cl_integrator* it, const float* u2, float* dir, float* pdf, float* value, uint32_t count)
+{
+    CL_NEED(it);
+    CL_NEED(u2);
+    CL_NEED(dir);
+    CL_NEED(pdf);
+    CL_NEED(value);
+    return guarded([&](std::string* e) { return it->impl.domeAliasSample(u2, dir, pdf, value, count, e); });
+}
+
+cl_status cl_unit_bsdf_eval(uint32_t type, const float* params, const float* wo, const float* wi, float* value,
+                            uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitBsdfEval(type, params, wo, wi, value, count, e); });
+}
+
+cl_status cl_unit_bsdf_pdf(uint32_t type, const float* params, const float* wo, const float* wi, float* pdf,
+                           uint32_t count, uint32_t compat)
+{
+    return guarded([&](std::string* e) { return clb::unitBsdfPdf(type, params, wo, wi, pdf, count, compat, e); });
+}
+
+cl_status cl_unit_bsdf_sample(uint32_t type, const float* params, const float* wo, const float* u2, float* wi,
+                              float* pdf, float* value, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitBsdfSample(type, params, wo, u2, wi, pdf, value, count, e); });
+}
+
+cl_status cl_unit_ggx_eval(const float* alpha, const float* m, const float* wi, const float* wo, float* D, float* G1wi,
+                           float* G, float* pdfAll, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitGgxEval(alpha, m, wi, wo, D, G1wi, G, pdfAll, count, e); });
+}
+
+cl_status cl_unit_ggx_sample(const float* alpha, const float* u2, float* m, float* pdf, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitGgxSample(alpha, u2, m, pdf, count, e); });
+}
+
+cl_status cl_unit_fresnel_conductor(const float* cos_i, const float* eta, const float* k, float* out, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitFresnelConductor(cos_i, eta, k, out, count, e); });
+}
+
+cl_status cl_unit_fresnel_dielectric(const float* cos_i, const float* eta, float* F, float* cos_t, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitFresnelDielectric(cos_i, eta, F, cos_t, count, e); });
+}
+
+cl_status cl_unit_warp(const float* u2, float* disk, float* hemisphere, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitWarp(u2, disk, hemisphere, count, e); });
+}
+
+cl_status cl_unit_make_frame(const float* a, float* b, float* c, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitMakeFrame(a, b, c, count, e); });
+}
+
+cl_status cl_unit_frame(const float* s, const float* t, const float* n, const float* v, float* local, float* world,
+                        uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitFrame(s, t, n, v, local, world, count, e); });
+}
+
+cl_status cl_unit_pcg4d(const uint32_t* in, uint32_t* out, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitPcg(in, out, count, e); });
+}
+
+cl_status cl_unit_sampler_sequence(const uint32_t* px_py_frame, uint32_t count, uint32_t draws, float* out)
+{
+    return guarded([&](std::string* e) { return clb::unitSeq(px_py_frame, count, draws, out, e); });
+}
+
+cl_status cl_unit_dome_sample(const float* texels, uint32_t w, uint32_t h, const float* pUcondV_c, const float* cdfU,
+                              const float* pV_c, const float* cdfV, const float* u2, float* dir, float* pdf,
+                              float* value, uint32_t count)
+{
+    return guarded([&](std::string* e) {
+        return clb::unitDomeSample(texels, w, h, pUcondV_c, cdfU, pV_c, cdfV, u2, dir, pdf, value, count, e);
+    });
+}
+
+cl_status cl_unit_dome_pdf_eval(const float* texels, uint32_t w, uint32_t h, const float* pUcondV_c, const float* pV_c,
+                                const float* dirs, float* pdf, float* value, uint32_t count)
+{
+    return guarded(
+        [&](std::string* e) { return clb::unitDomePdfEval(texels, w, h, pUcondV_c, pV_c, dirs, pdf, value, count, e); });
+}
+
+cl_status cl_unit_directional_sample(const float* params7, const float* u2, float* dir, float* pdf, float* value,
+                                     uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitDirectional(params7, u2, dir, pdf, value, count, e); });
+}
+
+} // extern "C"

@@ -1,0 +1,189 @@
+// HDRI dome preprocessing on the device, in FP64.
+//
+// Replaces the reference's FP32 preprocessing kernels (prefiltering,
+// preprocessPCondV, preprocessPV: libkernel/emitters/hdridome.h:311-432,
+// src/kernel/emitters/hdridome.cu:15-51, launched by
+// src/core/devices/cudadevice.h:155-177).  Outputs:
+//   * the reference's tables (same layout and meaning, hdridome.h:494-510),
+//     rounded to FP32 from FP64 sums: pUcondV_c and CDFpUcondV ((w+1)*h),
+//     pV_c and CDFpV (h+1).  They serve the CDF sampler and every pdf lookup;
+//   * alias tables for O(1) sampling of the same density: per row over
+//     columns (w*h entries) and over rows (h entries), Vose's method in FP64.
+// Texel weights are sin(theta_v) * luminance(texel) at texel centres
+// (hdridome.h:319-323, luminance weights math.h:155-158).
+#include "cl_dome.h"
+
+namespace clb
+{
+namespace
+{
+__global__ void kDomeWeights(const float4* __restrict__ tex, int w, int h, double* __restrict__ wgt)
+{
+    int u = blockIdx.x * blockDim.x + threadIdx.x;
+    int v = blockIdx.y;
+    if (u >= w || v >= h) return;
+    float4 t     = tex[size_t(v) * w + u];
+    double lum   = double(t.x) * 0.212671 + double(t.y) * 0.71516 + double(t.z) * 0.072169;
+    double sinth = sin(3.14159265358979323846 * (double(v) + 0.5) / double(h));
+    wgt[size_t(v) * w + u] = sinth * lum;
+}
+
+// Vose alias construction over n weights (FP64); prob/alias as uint2 {float
+// bits, index}.  `small` and `large` are scratch index lists of n entries.
+__device__ void voseBuild(const double* wgt, int n, double total, uint2* out, uint32_t* small, uint32_t* large,
+                          double* q)
+{
+    if (!(total > 0.0))
+    {
+        for (int i = 0; i < n; ++i) out[i] = make_uint2(__float_as_uint(1.0f), uint32_t(i));
+        return;
+    }
+    int ns = 0, nl = 0;
+    for (int i = 0; i < n; ++i)
+    {
+        q[i] = wgt[i] * double(n) / total;
+        if (q[i] < 1.0)
+            small[ns++] = uint32_t(i);
+        else
+            large[nl++] = uint32_t(i);
+    }
+    while (ns > 0 && nl > 0)
+    {
+        uint32_t l = small[--ns];
+        uint32_t g = large[--nl];
+        out[l]     = make_uint2(__float_as_uint(float(q[l])), g);
+        q[g]       = (q[g] + q[l]) - 1.0;
+        if (q[g] < 1.0)
+            small[ns++] = g;
+        else
+            large[nl++] = g;
+    }
+    while (nl > 0)
+    {
+        uint32_t g = large[--nl];
+        out[g]     = make_uint2(__float_as_uint(1.0f), g);
+    }
+    while (ns > 0)
+    {
+        uint32_t l = small[--ns];
+        out[l]     = make_uint2(__float_as_uint(1.0f), l);
+    }
+}
+
+// One thread per row: FP64 row sums, CDF row, alias row.
+__global__ void kDomeRows(const double* __restrict__ wgt, int w, int h, float* __restrict__ pU, float* __restrict__ cU,
+                          double* __restrict__ rowC, uint2* __restrict__ aliasCol, uint32_t* scratchIdx,
+                          double* scratchQ)
+{
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= h) return;
+    const double* f   = wgt + size_t(v) * w;
+    float*        p   = pU + size_t(v) * (w + 1);
+    float*        c   = cU + size_t(v) * (w + 1);
+    double        sum = 0.0;
+    for (int i = 0; i < w; ++i) sum += f[i];
+    double cv = sum / double(w);
+    rowC[v]   = cv;
+    if (cv > 0.0)
+    {
+        double acc = 0.0;
+        c[0]       = 0.0f;
+        for (int i = 0; i < w; ++i)
+        {
+            p[i] = float(f[i]);
+            acc += f[i];
+            c[i + 1] = float(acc / sum);
+        }
+        c[w] = 1.0f;
+        p[w] = float(cv);
+    }
+    else
+    {
+        for (int i = 0; i < w; ++i)
+        {
+            p[i] = 0.0f;
+            c[i] = float(i) / float(w);
+        }
+        c[w] = 1.0f;
+        p[w] = 0.0f;
+    }
+    voseBuild(f, w, sum, aliasCol + size_t(v) * w, scratchIdx + size_t(v) * 2 * w, scratchIdx + size_t(v) * 2 * w + w,
+              scratchQ + size_t(v) * w);
+}
+
+// Single thread: marginal over rows.
+__global__ void kDomeMarginal(const double* __restrict__ rowC, int h, float* __restrict__ pV, float* __restrict__ cV,
+                              uint2* __restrict__ aliasRow, uint32_t* scratchIdx, double* scratchQ)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    double sum = 0.0;
+    for (int v = 0; v < h; ++v) sum += rowC[v];
+    double c = sum / double(h);
+    if (c > 0.0)
+    {
+        double acc = 0.0;
+        cV[0]      = 0.0f;
+        for (int v = 0; v < h; ++v)
+        {
+            pV[v] = float(rowC[v]);
+            acc += rowC[v];
+            cV[v + 1] = float(acc / sum);
+        }
+        cV[h] = 1.0f;
+        pV[h] = float(c);
+    }
+    else
+    {
+        for (int v = 0; v <= h; ++v)
+        {
+            pV[v] = 0.0f;
+            cV[v] = float(v) / float(h);
+        }
+    }
+    voseBuild(rowC, h, sum, aliasRow, scratchIdx, scratchIdx + h, scratchQ);
+}
+
+} // namespace
+
+cl_status launchDomeBuild(const float4* dTex, int w, int h, cudaStream_t st, const DomeScratch& s, float* pU, float* cU,
+                          float* pV, float* cV, uint2* aliasRow, uint2* aliasCol, std::string* err)
+{
+    dim3 g((w + 127) / 128, h);
+    kDomeWeights<<<g, 128, 0, st>>>(dTex, w, h, s.weights);
+    kDomeRows<<<(h + 63) / 64, 64, 0, st>>>(s.weights, w, h, pU, cU, s.rowC, aliasCol, s.idx, s.q);
+    kDomeMarginal<<<1, 32, 0, st>>>(s.rowC, h, pV, cV, aliasRow, s.idx, s.q);
+    CL_CUDA(cudaGetLastError(), err);
+    return CL_OK;
+}
+
+cl_status buildDome(const float* hostTexels, int w, int h, cudaStream_t st, DomeTables* out, std::string* err)
+{
+    if (w <= 0 || h <= 0 || !hostTexels)
+    {
+        *err = "dome: invalid texture";
+        return CL_ERR_INVALID_ARG;
+    }
+    out->w = w;
+    out->h = h;
+    size_t n = size_t(w) * h;
+    CL_TRY(out->tex.alloc(n * 16, err));
+    CL_TRY(out->pU.alloc(size_t(w + 1) * h * 4, err));
+    CL_TRY(out->cU.alloc(size_t(w + 1) * h * 4, err));
+    CL_TRY(out->pV.alloc(size_t(h + 1) * 4, err));
+    CL_TRY(out->cV.alloc(size_t(h + 1) * 4, err));
+    CL_TRY(out->aliasRow.alloc(size_t(h) * 8, err));
+    CL_TRY(out->aliasCol.alloc(n * 8, err));
+    DevBuf weights, rowC, idx, q;
+    CL_TRY(weights.alloc(n * 8, err));
+    CL_TRY(rowC.alloc(size_t(h) * 8, err));
+    CL_TRY(idx.alloc(n * 2 * 4 + size_t(h) * 2 * 4, err));
+    CL_TRY(q.alloc(n * 8 + size_t(h) * 8, err));
+    CL_CUDA(cudaMemcpyAsync(out->tex.p, hostTexels, n * 16, cudaMemcpyHostToDevice, st), err);
+    DomeScratch s{weights.as<double>(), rowC.as<double>(), idx.u(), q.as<double>()};
+    CL_TRY(launchDomeBuild(out->tex.as<float4>(), w, h, st, s, out->pU.f(), out->cU.f(), out->pV.f(), out->cV.f(),
+                           out->aliasRow.as<uint2>(), out->aliasCol.as<uint2>(), err));
+    CL_CUDA(cudaStreamSynchronize(st), err);
+    return CL_OK;
+}
+
+} // namespace clb

@@ -1,0 +1,1429 @@
+// Wavefront path tracing and direct lighting on B200.
+//
+// Reference loop (src/core/integrators/path.cpp:84-231): per iteration, raygen
+// over all pixels, then per bounce: reset queues, trace, escaped rays, shade,
+// trace shadow rays, with a full host synchronisation after every launch
+// (30 launches per spp).  Here the same stages run as persistent kernels over
+// device-resident queues, with no host round trip per launch:
+//
+//   wave(cur):  kTraceClosest(rq[cur])  -> hit[]
+//               kShade(rq[cur], hit[])  -> shadow queue, rq[cur^1]; finished
+//                                          paths are written to the film and
+//                                          their slot restarts the next camera
+//                                          path (path regeneration)
+//               kShadow(shadow queue)   -> radiance; finishes paths whose last
+//                                          vertex had a shadow ray
+//               kAdvance                -> queue counters for the next wave
+//
+// A path's state lives in a slot (psInfo/psT/psE/psL); the ray queues hold
+// slot indices and are compacted with warp-aggregated atomics (one atomicAdd
+// per warp, __ballot_sync/__popc ranks), replacing the reference's one
+// atomicAdd per item (libkernel/base/soa.h:39-63).  Waves are replayed from a
+// CUDA graph until no path is left in flight.
+//
+// The per-sample arithmetic follows the reference kernels
+// (src/kernel/integrators/raygeneration.cu:59-456, src/core/devices/optix.cu:112-284);
+// Russian roulette is added (absent from the reference, path.cpp:135).
+#include "cl_integrator.h"
+
+#include <cstdio>
+
+namespace clb
+{
+namespace
+{
+constexpr uint32_t kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t laneId() { return threadIdx.x & 31u; }
+
+// Warp-aggregated append: every lane of the warp calls it; lanes with pred
+// receive consecutive indices from one atomicAdd.
+__device__ __forceinline__ uint32_t warpAppend(uint32_t* counter, bool pred)
+{
+    uint32_t mask = __ballot_sync(kFull, pred);
+    if (mask == 0u) return 0u;
+    uint32_t leader = __ffs(mask) - 1u;
+    uint32_t base   = 0u;
+    if (laneId() == leader) base = atomicAdd(counter, uint32_t(__popc(mask)));
+    base = __shfl_sync(kFull, base, leader);
+    return base + __popc(mask & ((1u << laneId()) - 1u));
+}
+
+__device__ __forceinline__ uint32_t warpFetch(uint32_t* counter)
+{
+    uint32_t base = 0u;
+    if (laneId() == 0u) base = atomicAdd(counter, 32u);
+    return __shfl_sync(kFull, base, 0);
+}
+
+__device__ __forceinline__ uint32_t loadCount(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+
+__device__ __forceinline__ Bsdf loadMaterial(const float4* mats, uint32_t m)
+{
+    float4 a = __ldg(mats + 3 * m), b = __ldg(mats + 3 * m + 1), c = __ldg(mats + 3 * m + 2);
+    Bsdf   s;
+    s.type   = __float_as_uint(a.x);
+    s.r      = {a.y, a.z, a.w};
+    s.alpha  = b.x;
+    s.etaInt = b.y;
+    s.eta    = {b.z, b.w, c.x};
+    s.k      = {c.y, c.z, c.w};
+    return s;
+}
+
+struct HitAttr
+{
+    f3       p, ng, ns, dpdu, dpdv;
+    f2       uv;
+    uint32_t material;
+};
+
+// Closest-hit attributes (optix.cu:137-227).
+__device__ __forceinline__ HitAttr hitAttributes(const SceneDev& sc, uint32_t prim, float b1, float b2)
+{
+    uint4   ti = __ldg(sc.triIdx + prim);
+    float4  a0 = __ldg(sc.vtx + 3 * size_t(ti.x)), a1 = __ldg(sc.vtx + 3 * size_t(ti.x) + 1), a2 = __ldg(sc.vtx + 3 * size_t(ti.x) + 2);
+    float4  c0 = __ldg(sc.vtx + 3 * size_t(ti.y)), c1 = __ldg(sc.vtx + 3 * size_t(ti.y) + 1), c2 = __ldg(sc.vtx + 3 * size_t(ti.y) + 2);
+    float4  e0 = __ldg(sc.vtx + 3 * size_t(ti.z)), e1 = __ldg(sc.vtx + 3 * size_t(ti.z) + 1), e2 = __ldg(sc.vtx + 3 * size_t(ti.z) + 2);
+    f3      p0{a0.x, a0.y, a0.z}, p1{c0.x, c0.y, c0.z}, p2{e0.x, e0.y, e0.z};
+    uint32_t flags = __float_as_uint(a2.w);
+    float   b0    = 1.0f - b1 - b2;
+    HitAttr h;
+    h.material = ti.w;
+    h.p        = b0 * p0 + b1 * p1;
+    h.p        = h.p + b2 * p2;
+    if (flags & 2u)
+        h.uv = {b0 * a2.y + b1 * c2.y + b2 * e2.y, b0 * a2.z + b1 * c2.z + b2 * e2.z};
+    else
+        h.uv = {b0, b1};
+    f3 Ng = normalize(cross(p1 - p0, p2 - p0));
+    f3 Ns;
+    if (flags & 1u)
+    {
+        f3 n = b0 * f3{a0.w, a1.x, a1.y} + b1 * f3{c0.w, c1.x, c1.y};
+        n    = n + b2 * f3{e0.w, e1.x, e1.y};
+        Ns   = normalize(n);
+    }
+    else
+        Ns = normalize(Ng);
+    if (dot(Ns, Ns) == 0.0f) Ns = Ng;
+    if (dot(Ng, Ns) < 0.0f) Ng = -Ng;
+    f3 t    = b0 * f3{a1.z, a1.w, a2.x} + b1 * f3{c1.z, c1.w, c2.x};
+    t       = t + b2 * f3{e1.z, e1.w, e2.x};
+    f3 dpdu = normalize(t);
+    f3 dpdv{0.0f, 0.0f, 0.0f};
+    if (dot(dpdu, dpdu) > 0.0f)
+    {
+        dpdv = cross(Ns, dpdu);
+        if (dot(dpdv, dpdv) > 0.0f)
+        {
+            dpdv = normalize(dpdv);
+            dpdu = cross(dpdv, Ns);
+        }
+        else
+            makeFrame(Ns, &dpdu, &dpdv);
+    }
+    else
+        makeFrame(Ns, &dpdu, &dpdv);
+    h.ng   = Ng;
+    h.ns   = Ns;
+    h.dpdu = dpdu;
+    h.dpdv = dpdv;
+    return h;
+}
+
+// Camera path start (generateCameraRays, raygeneration.cu:83-102): path index
+// p -> pixel p mod W*H, frame frame0 + p / (W*H).
+__device__ __forceinline__ void startPath(const Params& P, const WaveParams& wp, uint32_t slot, unsigned long long p,
+                                          int q, uint32_t idx)
+{
+    unsigned long long wh = (unsigned long long)wp.W * wp.H;
+    uint32_t pix   = uint32_t(p % wh);
+    uint32_t frame = wp.frame0 + uint32_t(p / wh);
+    uint32_t px = pix % wp.W, py = pix / wp.W;
+    Rng      rng{px, py, frame, 0u};
+    f2       j = rng.next2D();
+    f2       screen{(float(px) + j.x) / float(wp.W), (float(py) + j.y) / float(wp.H)};
+    f3       pos{wp.cam[0], wp.cam[1], wp.cam[2]}, d00{wp.cam[3], wp.cam[4], wp.cam[5]};
+    f3       ddu{wp.cam[6], wp.cam[7], wp.cam[8]}, ddv{wp.cam[9], wp.cam[10], wp.cam[11]};
+    f3       d = d00 + screen.x * ddu;
+    d          = d + screen.y * ddv;
+    d          = normalize(d);
+    P.q.psInfo[slot]   = make_uint4(pix, frame, 1u | (rng.ctr << 8), 0u);
+    P.q.psT[slot]      = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    P.q.psE[slot]      = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    P.q.psL[slot]      = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    P.q.rqO[q][idx]    = make_float4(pos.x, pos.y, pos.z, 0.0f);
+    P.q.rqD[q][idx]    = make_float4(d.x, d.y, d.z, FLT_MAX);
+    P.q.rqSlot[q][idx] = slot;
+}
+
+// Film write of finished paths, then regeneration of their slots.  Called by
+// every lane of the warp.
+__device__ __forceinline__ void finishPaths(const Params& P, const WaveParams& wp, int nxt, bool finish, uint32_t slot,
+                                            f3 L)
+{
+    if (finish)
+    {
+        uint32_t pix = P.q.psInfo[slot].x;
+        float*   f   = reinterpret_cast<float*>(P.q.film + pix);
+        atomicAdd(f + 0, L.x);
+        atomicAdd(f + 1, L.y);
+        atomicAdd(f + 2, L.z);
+        if (P.q.film64)
+        {
+            double* g = P.q.film64 + 6 * size_t(pix);
+            atomicAdd(g + 0, double(L.x));
+            atomicAdd(g + 1, double(L.y));
+            atomicAdd(g + 2, double(L.z));
+            atomicAdd(g + 3, double(L.x) * double(L.x));
+            atomicAdd(g + 4, double(L.y) * double(L.y));
+            atomicAdd(g + 5, double(L.z) * double(L.z));
+        }
+    }
+    uint32_t mask = __ballot_sync(kFull, finish);
+    if (mask == 0u) return;
+    uint32_t           leader = __ffs(mask) - 1u;
+    unsigned long long base   = 0ull;
+    if (laneId() == leader) base = atomicAdd(&P.q.ctr->pathNext, (unsigned long long)__popc(mask));
+    base                  = __shfl_sync(kFull, base, leader);
+    unsigned long long p  = base + __popc(mask & ((1u << laneId()) - 1u));
+    bool               gen = finish && p < wp.totalPaths;
+    uint32_t           idx = warpAppend(&P.q.ctr->rayCount[nxt], gen);
+    if (gen) startPath(P, wp, slot, p, nxt, idx);
+}
+
+__device__ __forceinline__ f3 ld3(float4 v) { return {v.x, v.y, v.z}; }
+__device__ __forceinline__ float maxComp(f3 v)
+{
+    float m = v.x;
+    if (v.y > m) m = v.y;
+    if (v.z > m) m = v.z;
+    return m;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+template <bool STATS>
+__global__ void __launch_bounds__(kTraceBlock) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
+                                                             const float4* __restrict__ D, const uint32_t* count,
+                                                             uint32_t* fetch, float4* __restrict__ hitOut,
+                                                             Counters* ctr)
+{
+    __shared__ uint2 stack[kStackDepth * kTraceBlock];
+    const uint32_t   n = loadCount(count);
+    TraceCounters    tc{0u, 0u};
+    for (;;)
+    {
+        uint32_t base = warpFetch(fetch);
+        if (base >= n) break;
+        uint32_t i = base + laneId();
+        if (i < n)
+        {
+            float4 o = O[i], d = D[i];
+            float  t, b1, b2;
+            uint32_t prim = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
+                                                   stack + threadIdx.x, &tc, &ctr->error);
+            hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
+        }
+    }
+    if (STATS)
+    {
+        unsigned long long a = tc.nodes, b = tc.tris;
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            a += __shfl_xor_sync(kFull, a, o);
+            b += __shfl_xor_sync(kFull, b, o);
+        }
+        if (laneId() == 0)
+        {
+            atomicAdd(&ctr->statNodes, a);
+            atomicAdd(&ctr->statTris, b);
+        }
+    }
+}
+
+template <bool DL>
+__global__ void __launch_bounds__(128) kShade(Params P, int cur)
+{
+    const WaveParams wp = *P.wp;
+    const SceneDev&  sc = P.sc;
+    const uint32_t   n  = loadCount(&P.q.ctr->rayCount[cur]);
+    const int        nxt = cur ^ 1;
+    const bool compatPdf   = wp.flags & CL_COMPAT_PDF;
+    const bool compatFrame = wp.flags & CL_COMPAT_FRAME;
+    const bool compatEsc   = wp.flags & CL_COMPAT_ESCAPE;
+    const bool alias       = wp.flags & CL_DOME_ALIAS;
+    const uint32_t N       = sc.numEmitters;
+    for (;;)
+    {
+        uint32_t base = warpFetch(&P.q.ctr->fetchShade);
+        if (base >= n) break;
+        uint32_t i = base + laneId();
+        bool     valid = i < n;
+        bool     pushShadow = false, shadow1 = false, shadow2 = false, pushRay = false, finish = false;
+        uint32_t slot = 0u, info2 = 0u;
+        f3       L{0, 0, 0}, T{1, 1, 1}, E{0, 0, 0}, pHit{0, 0, 0}, sdir{0, 0, 0}, Li{0, 0, 0}, sdir2{0, 0, 0},
+            Ld{0, 0, 0}, ndir{0, 0, 0};
+        if (valid)
+        {
+            slot          = P.q.rqSlot[cur][i];
+            float4 hh     = P.q.hit[i];
+            float4 rd     = P.q.rqD[cur][i];
+            uint4  info   = P.q.psInfo[slot];
+            uint32_t depth = info.z & 0xffu;
+            Rng    rng{info.x % wp.W, info.x / wp.W, info.y, info.z >> 8};
+            T             = ld3(P.q.psT[slot]);
+            E             = ld3(P.q.psE[slot]);
+            L             = ld3(P.q.psL[slot]);
+            f3       d    = ld3(rd);
+            uint32_t prim = __float_as_uint(hh.y);
+            if (prim == kMissPrim)
+            {
+                // evaluateEscapedRays (raygeneration.cu:105-136)
+                if (sc.hasDome)
+                {
+                    f3 Le = domeEval(sc.dome, d);
+                    if (depth == 1u)
+                        L = L + Le;
+                    else if (compatEsc)
+                        L = L + T * (Le * E);
+                    else
+                    {
+                        float pd = domePdf(sc.dome, d) / float(N);
+                        float w  = E.x / (E.x + pd);
+                        L        = L + T * (Le * w);
+                    }
+                }
+                finish = true;
+            }
+            else if (!DL && depth == wp.maxDepth)
+                finish = true;
+            else
+            {
+                HitAttr a    = hitAttributes(sc, prim, hh.z, hh.w);
+                Bsdf    bsdf = loadMaterial(sc.mats, a.material);
+                pHit         = a.p;
+                f3    wo     = -d;
+                f2    u      = rng.next2D();
+                Frame fr{a.dpdv, a.dpdu, (!DL && compatFrame) ? a.ng : a.ns};
+                // Emitter sampling with MIS (raygeneration.cu:332-384 / 174-227).
+                if (N > 0u)
+                {
+                    uint32_t pick = min(uint32_t(floorf(u.x * float(N))), N - 1u);
+                    f2       us{u.x * float(N) - float(pick), u.y};
+                    f3       ldir{0, 0, 0};
+                    float    lpdf = 0.0f;
+                    const EmitterDev& em = sc.emitters[pick];
+                    f3 value = em.type == 0u ? directionalSample(em.dl, us, &ldir, &lpdf)
+                                             : domeSample(sc.dome, us, alias, &ldir, &lpdf);
+                    if (compatEsc) value = value * float(N);
+                    if (lpdf == 0.0f) value = {0.0f, 0.0f, 0.0f};
+                    if (nonzero(value) && lpdf > 0.0f)
+                    {
+                        f3 wiL = fr.toLocal(ldir), woL = fr.toLocal(wo);
+                        f3 f   = bsdfEval(bsdf, woL, wiL);
+                        if (nonzero(f))
+                        {
+                            float bp = bsdfPdf(bsdf, woL, wiL, compatPdf);
+                            float c  = (DL && compatEsc) ? wiL.z : fabsf(wiL.z);
+                            f3    baseV = DL ? value : T * value;
+                            float w, pl;
+                            if (compatEsc)
+                            {
+                                w  = misBalanced(lpdf, bp);
+                                pl = lpdf;
+                            }
+                            else
+                            {
+                                pl = lpdf / float(N);
+                                w  = em.type == 1u ? misBalanced(pl, bp) : 1.0f;
+                            }
+                            Li      = baseV * f;
+                            Li      = Li * c;
+                            Li      = Li * w;
+                            Li      = Li / pl;
+                            sdir    = ldir;
+                            shadow1 = true;
+                        }
+                    }
+                }
+                // BSDF sampling with MIS (raygeneration.cu:391-455 / 234-281).
+                f2    u2  = rng.next2D();
+                f3    woL = fr.toLocal(wo);
+                f3    wiL{0, 0, 0};
+                float bp = 0.0f;
+                f3    f  = bsdfSample(bsdf, woL, u2, &wiL, &bp);
+                if (!nonzero(f))
+                    finish = true;
+                else
+                {
+                    f3    dir      = fr.toWorld(wiL);
+                    float lightPdf = sc.hasDome ? domePdf(sc.dome, dir) : 0.0f;
+                    if (DL)
+                    {
+                        if (sc.hasDome && !(compatEsc && !(lightPdf > 0.0f)))
+                        {
+                            float c  = compatEsc ? wiL.z : fabsf(wiL.z);
+                            float pl = compatEsc ? lightPdf : lightPdf / float(N);
+                            Ld       = domeEval(sc.dome, dir);
+                            float w  = misBalanced(bp, pl);
+                            f3    kk{f.x * c * w / bp, f.y * c * w / bp, f.z * c * w / bp};
+                            Ld      = Ld * kk;
+                            sdir2   = dir;
+                            shadow2 = true;
+                        }
+                        finish = true;
+                    }
+                    else
+                    {
+                        float c = fabsf(wiL.z);
+                        f3    tk{f.x * c / bp, f.y * c / bp, f.z * c / bp};
+                        T          = T * tk;
+                        bool alive = true;
+                        if (wp.rrStart > 0u && depth >= wp.rrStart)
+                        {
+                            float q = maxComp(T);
+                            q       = q < 1.0f ? q : 1.0f;
+                            float r = rng.next1D();
+                            if (r >= q)
+                                alive = false;
+                            else
+                                T = T / q;
+                        }
+                        if (alive)
+                        {
+                            if (compatEsc)
+                            {
+                                if (!(lightPdf > 0.0f))
+                                    alive = false;
+                                else
+                                {
+                                    float w = misBalanced(bp, lightPdf);
+                                    E       = {f.x * c * w / bp, f.y * c * w / bp, f.z * c * w / bp};
+                                }
+                            }
+                            else
+                                E = {bp, 0.0f, 0.0f};
+                        }
+                        if (alive)
+                        {
+                            pushRay = true;
+                            ndir    = dir;
+                            info2   = (depth + 1u) | (rng.ctr << 8);
+                        }
+                        else
+                            finish = true;
+                    }
+                }
+            }
+            pushShadow = shadow1 || shadow2;
+        }
+        // Shadow queue (one entry per path vertex).
+        uint32_t sIdx = warpAppend(&P.q.ctr->shadowCount, pushShadow);
+        if (pushShadow)
+        {
+            if (sIdx < P.q.shadowCap)
+            {
+                uint32_t tag     = slot | (finish ? kLastFlag : 0u);
+                P.q.sqO[sIdx]    = make_float4(pHit.x, pHit.y, pHit.z, __uint_as_float(tag));
+                P.q.sqD[sIdx]    = make_float4(sdir.x, sdir.y, sdir.z, shadow1 ? 1.0f : 0.0f);
+                P.q.sqL[sIdx]    = make_float4(Li.x, Li.y, Li.z, 0.0f);
+                if (DL)
+                {
+                    P.q.sqD2[sIdx] = make_float4(sdir2.x, sdir2.y, sdir2.z, shadow2 ? 1.0f : 0.0f);
+                    P.q.sqL2[sIdx] = make_float4(Ld.x, Ld.y, Ld.z, 0.0f);
+                }
+            }
+            else
+                atomicOr(&P.q.ctr->error, 4u);
+        }
+        // Next-bounce ray queue.
+        uint32_t rIdx = warpAppend(&P.q.ctr->rayCount[nxt], pushRay);
+        if (pushRay)
+        {
+            P.q.rqO[nxt][rIdx]    = make_float4(pHit.x, pHit.y, pHit.z, kRayEps);
+            P.q.rqD[nxt][rIdx]    = make_float4(ndir.x, ndir.y, ndir.z, FLT_MAX);
+            P.q.rqSlot[nxt][rIdx] = slot;
+            P.q.psInfo[slot].z    = info2;
+            P.q.psT[slot]         = make_float4(T.x, T.y, T.z, 0.0f);
+            P.q.psE[slot]         = make_float4(E.x, E.y, E.z, 0.0f);
+        }
+        if (pushRay || (pushShadow && finish)) P.q.psL[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+        finishPaths(P, wp, nxt, finish && !pushShadow, slot, L);
+    }
+}
+
+template <bool DL, bool STATS>
+__global__ void __launch_bounds__(kTraceBlock) kShadow(Params P, int cur)
+{
+    __shared__ uint2 stack[kStackDepth * kTraceBlock];
+    const WaveParams wp  = *P.wp;
+    const uint32_t   n   = loadCount(&P.q.ctr->shadowCount);
+    const int        nxt = cur ^ 1;
+    TraceCounters    tc{0u, 0u};
+    for (;;)
+    {
+        uint32_t base = warpFetch(&P.q.ctr->fetchShadow);
+        if (base >= n) break;
+        uint32_t i      = base + laneId();
+        bool     finish = false;
+        uint32_t slot   = 0u;
+        f3       L{0, 0, 0};
+        if (i < n)
+        {
+            float4   o4  = P.q.sqO[i];
+            uint32_t tag = __float_as_uint(o4.w);
+            slot         = tag & ~kLastFlag;
+            f3       o{o4.x, o4.y, o4.z};
+            L            = ld3(P.q.psL[slot]);
+            float4 d4    = P.q.sqD[i];
+            if (d4.w != 0.0f)
+            {
+                float t, b1, b2;
+                uint32_t h = traverse<true, STATS>(P.sc.bvh, o, ld3(d4), kRayEps, FLT_MAX, &t, &b1, &b2,
+                                                   stack + threadIdx.x, &tc, &P.q.ctr->error);
+                if (h == kMissPrim) L = L + ld3(P.q.sqL[i]);
+            }
+            if (DL)
+            {
+                float4 e4 = P.q.sqD2[i];
+                if (e4.w != 0.0f)
+                {
+                    float t, b1, b2;
+                    uint32_t h = traverse<true, STATS>(P.sc.bvh, o, ld3(e4), kRayEps, FLT_MAX, &t, &b1, &b2,
+                                                       stack + threadIdx.x, &tc, &P.q.ctr->error);
+                    if (h == kMissPrim) L = L + ld3(P.q.sqL2[i]);
+                }
+            }
+            if (tag & kLastFlag)
+                finish = true;
+            else
+                P.q.psL[slot] = make_float4(L.x, L.y, L.z, 0.0f);
+        }
+        finishPaths(P, wp, nxt, finish, slot, L);
+    }
+    if (STATS)
+    {
+        unsigned long long a = tc.nodes, b = tc.tris;
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            a += __shfl_xor_sync(kFull, a, o);
+            b += __shfl_xor_sync(kFull, b, o);
+        }
+        if (laneId() == 0)
+        {
+            atomicAdd(&P.q.ctr->statNodesS, a);
+            atomicAdd(&P.q.ctr->statTrisS, b);
+        }
+    }
+}
+
+// Initial fill: slot s starts path s.
+__global__ void kRaygen(Params P, uint32_t count)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const WaveParams wp = *P.wp;
+    startPath(P, wp, s, s, 0, s);
+}
+
+__global__ void kAdvance(Counters* c, int cur)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    c->raysClosest += c->rayCount[cur];
+    c->raysShadow += c->shadowCount;
+    c->rayCount[cur] = 0u;
+    c->shadowCount   = 0u;
+    c->fetchTrace    = 0u;
+    c->fetchShade    = 0u;
+    c->fetchShadow   = 0u;
+}
+
+__global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const float4* __restrict__ O,
+                                                         const float4* __restrict__ D, uint32_t n,
+                                                         uint8_t* __restrict__ occ, uint32_t* err)
+{
+    __shared__ uint2 stack[kStackDepth * kTraceBlock];
+    uint32_t         i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4        o = O[i], d = D[i];
+    float         t, b1, b2;
+    TraceCounters tc{0u, 0u};
+    uint32_t      h = traverse<true, false>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
+                                       stack + threadIdx.x, &tc, err);
+    occ[i]          = h == kMissPrim ? 0 : 1;
+}
+
+__global__ void kAliasSample(DomeView dome, const float2* __restrict__ u, float* dir, float* pdf, float* val, uint32_t n)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3    d{0, 0, 0};
+    float p = 0.0f;
+    float2 uu = u[i];
+    f3    v = domeSample(dome, f2{uu.x, uu.y}, true, &d, &p);
+    dir[3 * i] = d.x;
+    dir[3 * i + 1] = d.y;
+    dir[3 * i + 2] = d.z;
+    pdf[i] = p;
+    val[3 * i] = v.x;
+    val[3 * i + 1] = v.y;
+    val[3 * i + 2] = v.z;
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+Integrator::Integrator(cl_integrator_type type, uint32_t w, uint32_t h, const cl_render_config& cfg)
+    : type_(type), W_(w), H_(h), cfg_(cfg)
+{
+}
+
+Integrator::~Integrator()
+{
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (evA_) cudaEventDestroy(evA_);
+    if (evB_) cudaEventDestroy(evB_);
+    for (auto& e : evS_)
+        if (e) cudaEventDestroy(e);
+    if (hostWp_) cudaFreeHost(hostWp_);
+    if (hostCount_) cudaFreeHost(hostCount_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+cl_status Integrator::init(std::string* err)
+{
+    if (W_ == 0 || H_ == 0)
+    {
+        *err = "film size must be non-zero";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (cfg_.max_depth == 0) cfg_.max_depth = 5;
+    if (cfg_.max_depth > 255)
+    {
+        *err = "max_depth must be at most 255";
+        return CL_ERR_INVALID_ARG;
+    }
+    int dev = 0;
+    CL_CUDA(cudaGetDevice(&dev), err);
+    CL_CUDA(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, dev), err);
+    CL_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), err);
+    CL_CUDA(cudaEventCreate(&evA_), err);
+    CL_CUDA(cudaEventCreate(&evB_), err);
+    for (auto& e : evS_) CL_CUDA(cudaEventCreate(&e), err);
+    CL_CUDA(cudaMallocHost((void**)&hostWp_, sizeof(WaveParams)), err);
+    CL_CUDA(cudaMallocHost((void**)&hostCount_, 64), err);
+    int b = 0;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTraceClosest<false>, kTraceBlock, 0), err);
+    traceBlocks_ = std::max(1, b) * numSMs_;
+    bool dl = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dl ? (const void*)kShade<true> : (const void*)kShade<false>,
+                                                          128, 0),
+            err);
+    shadeBlocks_ = std::max(1, b) * numSMs_;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &b, dl ? (const void*)kShadow<true, false> : (const void*)kShadow<false, false>, kTraceBlock, 0),
+            err);
+    shadowBlocks_ = std::max(1, b) * numSMs_;
+    CL_TRY(ctr_.alloc(sizeof(Counters), err));
+    CL_TRY(wp_.alloc(sizeof(WaveParams), err));
+    CL_CUDA(cudaMemsetAsync(ctr_.p, 0, sizeof(Counters), stream_), err);
+    return CL_OK;
+}
+
+cl_status Integrator::buildMeshes(const cl_mesh_desc* meshes, uint32_t n, std::string* err)
+{
+    if (!meshes && n)
+    {
+        *err = "meshes is null";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::vector<HostMesh> out(n);
+    for (uint32_t m = 0; m < n; ++m)
+    {
+        const cl_mesh_desc& d = meshes[m];
+        if (!d.positions || !d.indices || !d.tangents || d.num_vertices == 0 || d.num_triangles == 0)
+        {
+            *err = "mesh " + std::to_string(m) + ": positions, tangents and indices are required";
+            return CL_ERR_INVALID_ARG;
+        }
+        HostMesh& h = out[m];
+        size_t    nv = d.num_vertices, nt = d.num_triangles;
+        h.pos.assign(d.positions, d.positions + 3 * nv);
+        h.tan.assign(d.tangents, d.tangents + 3 * nv);
+        h.hasN = d.normals != nullptr;
+        if (h.hasN) h.nrm.assign(d.normals, d.normals + 3 * nv);
+        h.hasUV = d.uvs != nullptr;
+        if (h.hasUV) h.uv.assign(d.uvs, d.uvs + 2 * nv);
+        h.idx.assign(d.indices, d.indices + 3 * nt);
+        for (uint32_t v : h.idx)
+            if (v >= d.num_vertices)
+            {
+                *err = "mesh " + std::to_string(m) + ": vertex index out of range";
+                return CL_ERR_INVALID_ARG;
+            }
+    }
+    meshes_.swap(out);
+    sceneBuilt_ = false;
+    return CL_OK;
+}
+
+cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, std::string* err)
+{
+    if ((!inst && n) || n == 0)
+    {
+        *err = "at least one instance is required";
+        return CL_ERR_INVALID_ARG;
+    }
+    size_t nv = 0, nt = 0;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        if (inst[i].mesh_id >= meshes_.size())
+        {
+            *err = "instance " + std::to_string(i) + ": mesh_id out of range";
+            return CL_ERR_INVALID_ARG;
+        }
+        nv += meshes_[inst[i].mesh_id].pos.size() / 3;
+        nt += meshes_[inst[i].mesh_id].idx.size() / 3;
+    }
+    if (nt >= 0x7fffffffu || nv >= 0xffffffffu)
+    {
+        *err = "scene too large";
+        return CL_ERR_INVALID_ARG;
+    }
+    // Flatten instances into world space (the reference's TLAS has no
+    // transforms, optix.cu:115; identity transforms are copied exactly).
+    std::vector<float>    vtx(nv * 12);
+    std::vector<uint32_t> tidx(nt * 4);
+    std::vector<float>    tri9(nt * 9);
+    size_t vo = 0, to = 0;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const HostMesh& m = meshes_[inst[i].mesh_id];
+        const float*    M = inst[i].transform;
+        bool ident = M[0] == 1 && M[1] == 0 && M[2] == 0 && M[3] == 0 && M[4] == 0 && M[5] == 1 && M[6] == 0 &&
+                     M[7] == 0 && M[8] == 0 && M[9] == 0 && M[10] == 1 && M[11] == 0;
+        // Normal matrix: inverse transpose of the linear part.
+        double a = M[0], b = M[1], c = M[2], d = M[4], e = M[5], f = M[6], g = M[8], h = M[9], k = M[10];
+        double det = a * (e * k - f * h) - b * (d * k - f * g) + c * (d * h - e * g);
+        if (!ident && std::fabs(det) < 1e-30)
+        {
+            *err = "instance " + std::to_string(i) + ": singular transform";
+            return CL_ERR_INVALID_ARG;
+        }
+        double N9[9] = {(e * k - f * h) / det, -(d * k - f * g) / det, (d * h - e * g) / det,
+                        -(b * k - c * h) / det, (a * k - c * g) / det,  -(a * h - b * g) / det,
+                        (b * f - c * e) / det,  -(a * f - c * d) / det, (a * e - b * d) / det};
+        size_t mv = m.pos.size() / 3;
+        uint32_t flags = (m.hasN ? 1u : 0u) | (m.hasUV ? 2u : 0u);
+        for (size_t v = 0; v < mv; ++v)
+        {
+            float p[3], nn[3] = {0, 0, 0}, t[3], uv[2] = {0, 0};
+            for (int q = 0; q < 3; ++q)
+            {
+                p[q] = m.pos[3 * v + q];
+                t[q] = m.tan[3 * v + q];
+                if (m.hasN) nn[q] = m.nrm[3 * v + q];
+            }
+            if (m.hasUV)
+            {
+                uv[0] = m.uv[2 * v];
+                uv[1] = m.uv[2 * v + 1];
+            }
+            if (!ident)
+            {
+                float P2[3], T2[3], N2[3];
+                for (int r = 0; r < 3; ++r)
+                {
+                    P2[r] = float(double(M[4 * r]) * p[0] + double(M[4 * r + 1]) * p[1] + double(M[4 * r + 2]) * p[2] +
+                                  double(M[4 * r + 3]));
+                    T2[r] = float(double(M[4 * r]) * t[0] + double(M[4 * r + 1]) * t[1] + double(M[4 * r + 2]) * t[2]);
+                    // n' = N^T n with N = inverse of the linear part: n'_r = sum_c Ninv[c][r] n_c
+                    N2[r] = float(N9[3 * 0 + r] * nn[0] + N9[3 * 1 + r] * nn[1] + N9[3 * 2 + r] * nn[2]);
+                }
+                for (int q = 0; q < 3; ++q)
+                {
+                    p[q]  = P2[q];
+                    t[q]  = T2[q];
+                    nn[q] = N2[q];
+                }
+            }
+            float* o = &vtx[(vo + v) * 12];
+            o[0] = p[0]; o[1] = p[1]; o[2] = p[2]; o[3] = nn[0];
+            o[4] = nn[1]; o[5] = nn[2]; o[6] = t[0]; o[7] = t[1];
+            uint32_t fb = flags;
+            float    ff;
+            memcpy(&ff, &fb, 4);
+            o[8] = t[2]; o[9] = uv[0]; o[10] = uv[1]; o[11] = ff;
+        }
+        size_t mt = m.idx.size() / 3;
+        for (size_t t = 0; t < mt; ++t)
+        {
+            uint32_t* o = &tidx[(to + t) * 4];
+            for (int q = 0; q < 3; ++q)
+            {
+                uint32_t gv = uint32_t(vo + m.idx[3 * t + q]);
+                o[q]        = gv;
+                for (int c2 = 0; c2 < 3; ++c2) tri9[(to + t) * 9 + 3 * q + c2] = vtx[size_t(gv) * 12 + c2];
+            }
+            o[3] = inst[i].material_index;
+        }
+        vo += mv;
+        to += mt;
+    }
+    CL_TRY(vtx_.alloc(vtx.size() * 4, err));
+    CL_TRY(triIdx_.alloc(tidx.size() * 4, err));
+    CL_TRY(triPos_.alloc(tri9.size() * 4, err));
+    CL_CUDA(cudaMemcpyAsync(vtx_.p, vtx.data(), vtx.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(triIdx_.p, tidx.data(), tidx.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(triPos_.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaEventRecord(evA_, stream_), err);
+    CL_TRY(buildWideBvh(triPos_.f(), uint32_t(nt), stream_, &bvh_, err));
+    CL_CUDA(cudaEventRecord(evB_, stream_), err);
+    CL_CUDA(cudaEventSynchronize(evB_), err);
+    CL_CUDA(cudaEventElapsedTime(&msBvh_, evA_, evB_), err);
+    triPos_.release();
+    numTris_    = uint32_t(nt);
+    sceneBuilt_ = true;
+    graphValid_ = false;
+    // Material indices are checked at render time against the material count.
+    maxMaterialIndex_ = 0;
+    for (uint32_t i = 0; i < n; ++i) maxMaterialIndex_ = std::max(maxMaterialIndex_, inst[i].material_index);
+    return CL_OK;
+}
+
+cl_status Integrator::buildMaterials(const cl_material_desc* m, uint32_t n, std::string* err)
+{
+    if (!m || n == 0)
+    {
+        *err = "at least one material is required";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::vector<float> h(size_t(n) * 12);
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const cl_material_desc& d = m[i];
+        if (d.type > CL_MATERIAL_GLASS)
+        {
+            *err = "material " + std::to_string(i) + ": unknown type";
+            return CL_ERR_INVALID_ARG;
+        }
+        if (d.type == CL_MATERIAL_GLASS && d.interior_ior == 1.0f)
+        {
+            *err = "material " + std::to_string(i) + ": glass IOR must differ from 1 (roughdielectric.h:28)";
+            return CL_ERR_INVALID_ARG;
+        }
+        float*   o = &h[size_t(i) * 12];
+        uint32_t t = d.type;
+        memcpy(&o[0], &t, 4);
+        o[1]  = d.reflectance[0];
+        o[2]  = d.reflectance[1];
+        o[3]  = d.reflectance[2];
+        o[4]  = d.roughness * d.roughness; // metal.h:52, glass.h:26
+        o[5]  = d.interior_ior;
+        o[6]  = d.eta[0];
+        o[7]  = d.eta[1];
+        o[8]  = d.eta[2];
+        o[9]  = d.k[0];
+        o[10] = d.k[1];
+        o[11] = d.k[2];
+    }
+    CL_TRY(mats_.alloc(h.size() * 4, err));
+    CL_CUDA(cudaMemcpyAsync(mats_.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    numMaterials_ = n;
+    graphValid_   = false;
+    return CL_OK;
+}
+
+cl_status Integrator::buildEmitters(const cl_emitter_desc* e, uint32_t n, std::string* err)
+{
+    if ((!e && n) || n > uint32_t(kMaxEmitters))
+    {
+        *err = "between 0 and 8 emitters are supported";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::vector<EmitterDev> out;
+    int                     domeIdx = -1;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        EmitterDev d{};
+        d.type = e[i].type;
+        if (e[i].type == CL_EMITTER_DIRECTIONAL)
+            d.dl = DirectionalLight{{e[i].intensity[0], e[i].intensity[1], e[i].intensity[2]},
+                                    {e[i].direction[0], e[i].direction[1], e[i].direction[2]},
+                                    e[i].angular_radius};
+        else if (e[i].type == CL_EMITTER_HDRI_DOME)
+        {
+            if (!e[i].texels || e[i].width == 0 || e[i].height == 0)
+            {
+                *err = "dome emitter needs texels and a size";
+                return CL_ERR_INVALID_ARG;
+            }
+            domeIdx = int(i);
+        }
+        else
+        {
+            *err = "emitter " + std::to_string(i) + ": unknown type";
+            return CL_ERR_INVALID_ARG;
+        }
+        out.push_back(d);
+    }
+    hasDome_ = false;
+    if (domeIdx >= 0)
+    {
+        CL_CUDA(cudaEventRecord(evA_, stream_), err);
+        CL_TRY(buildDome(e[domeIdx].texels, int(e[domeIdx].width), int(e[domeIdx].height), stream_, &dome_, err));
+        CL_CUDA(cudaEventRecord(evB_, stream_), err);
+        CL_CUDA(cudaEventSynchronize(evB_), err);
+        CL_CUDA(cudaEventElapsedTime(&msDome_, evA_, evB_), err);
+        hasDome_ = true;
+    }
+    emitters_.swap(out);
+    graphValid_ = false;
+    return CL_OK;
+}
+
+cl_status Integrator::updateCamera(const cl_camera* c, std::string* err)
+{
+    if (!c)
+    {
+        *err = "camera is null";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (!hasCamera_ || memcmp(&camera_, c, sizeof(cl_camera)) != 0)
+    {
+        camera_    = *c;
+        hasCamera_ = true;
+        return resetIteration(err); // path.h:73-80
+    }
+    return CL_OK;
+}
+
+cl_status Integrator::ensureFilm(std::string* err)
+{
+    size_t np = size_t(W_) * H_;
+    if (!film_.p || film_.bytes != np * 16)
+    {
+        graphValid_ = false;
+        CL_TRY(film_.alloc(np * 16, err));
+        CL_CUDA(cudaMemsetAsync(film_.p, 0, np * 16, stream_), err);
+    }
+    if ((cfg_.flags & CL_FILM_FP64) && (!film64_.p || film64_.bytes != np * 48))
+    {
+        graphValid_ = false;
+        CL_TRY(film64_.alloc(np * 48, err));
+        CL_CUDA(cudaMemsetAsync(film64_.p, 0, np * 48, stream_), err);
+    }
+    return CL_OK;
+}
+
+cl_status Integrator::clearFilm(std::string* err)
+{
+    if (film_.p) CL_CUDA(cudaMemsetAsync(film_.p, 0, film_.bytes, stream_), err);
+    if (film64_.p) CL_CUDA(cudaMemsetAsync(film64_.p, 0, film64_.bytes, stream_), err);
+    filmSpp_ = 0;
+    return CL_OK;
+}
+
+cl_status Integrator::ensureQueues(std::string* err)
+{
+    uint32_t slots = cfg_.path_slots ? cfg_.path_slots : (1u << 21);
+    if (slots == slots_ && rqO_[0].p) return CL_OK;
+    size_t s = slots;
+    for (int q = 0; q < 2; ++q)
+    {
+        CL_TRY(rqO_[q].alloc(s * 16, err));
+        CL_TRY(rqD_[q].alloc(s * 16, err));
+        CL_TRY(rqSlot_[q].alloc(s * 4, err));
+    }
+    CL_TRY(hit_.alloc(s * 16, err));
+    CL_TRY(sqO_.alloc(s * 16, err));
+    CL_TRY(sqD_.alloc(s * 16, err));
+    CL_TRY(sqL_.alloc(s * 16, err));
+    if (type_ == CL_INTEGRATOR_DIRECT_LIGHTING)
+    {
+        CL_TRY(sqD2_.alloc(s * 16, err));
+        CL_TRY(sqL2_.alloc(s * 16, err));
+    }
+    CL_TRY(psInfo_.alloc(s * 16, err));
+    CL_TRY(psT_.alloc(s * 16, err));
+    CL_TRY(psE_.alloc(s * 16, err));
+    CL_TRY(psL_.alloc(s * 16, err));
+    slots_      = slots;
+    shadowCap_  = slots;
+    graphValid_ = false;
+    return CL_OK;
+}
+
+Params Integrator::params() const
+{
+    Params P{};
+    P.sc.bvh.nodes = bvh_.nodes.as<const uint4>();
+    P.sc.bvh.tris  = bvh_.tris.as<const float4>();
+    P.sc.triIdx    = triIdx_.as<const uint4>();
+    P.sc.vtx       = vtx_.as<const float4>();
+    P.sc.mats      = mats_.as<const float4>();
+    P.sc.hasDome   = hasDome_ ? 1 : 0;
+    if (hasDome_) P.sc.dome = dome_.view();
+    P.sc.numEmitters = uint32_t(emitters_.size());
+    for (size_t i = 0; i < emitters_.size(); ++i) P.sc.emitters[i] = emitters_[i];
+    for (int q = 0; q < 2; ++q)
+    {
+        P.q.rqO[q]    = rqO_[q].as<float4>();
+        P.q.rqD[q]    = rqD_[q].as<float4>();
+        P.q.rqSlot[q] = rqSlot_[q].u();
+    }
+    P.q.hit       = hit_.as<float4>();
+    P.q.sqO       = sqO_.as<float4>();
+    P.q.sqD       = sqD_.as<float4>();
+    P.q.sqL       = sqL_.as<float4>();
+    P.q.sqD2      = sqD2_.as<float4>();
+    P.q.sqL2      = sqL2_.as<float4>();
+    P.q.psInfo    = psInfo_.as<uint4>();
+    P.q.psT       = psT_.as<float4>();
+    P.q.psE       = psE_.as<float4>();
+    P.q.psL       = psL_.as<float4>();
+    P.q.film      = film_.as<float4>();
+    P.q.film64    = (cfg_.flags & CL_FILM_FP64) ? film64_.as<double>() : nullptr;
+    P.q.ctr       = ctr_.as<Counters>();
+    P.q.slots     = slots_;
+    P.q.shadowCap = shadowCap_;
+    P.wp          = wp_.as<const WaveParams>();
+    return P;
+}
+
+cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
+{
+    Params P  = params();
+    bool   dl = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
+    Counters* c = ctr_.as<Counters>();
+    const bool st = cfg_.flags & CL_TRACE_STATS;
+    if (profile) CL_CUDA(cudaEventRecord(evS_[0], stream_), err);
+    if (st)
+        kTraceClosest<true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur],
+                                                                        &c->rayCount[cur], &c->fetchTrace, P.q.hit, c);
+    else
+        kTraceClosest<false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur],
+                                                                         &c->rayCount[cur], &c->fetchTrace, P.q.hit, c);
+    if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
+    if (dl)
+        kShade<true><<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
+    else
+        kShade<false><<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
+    if (profile) CL_CUDA(cudaEventRecord(evS_[2], stream_), err);
+    if (dl && st)
+        kShadow<true, true><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+    else if (dl)
+        kShadow<true, false><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+    else if (st)
+        kShadow<false, true><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+    else
+        kShadow<false, false><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+    if (profile) CL_CUDA(cudaEventRecord(evS_[3], stream_), err);
+    kAdvance<<<1, 32, 0, stream_>>>(c, cur);
+    CL_CUDA(cudaGetLastError(), err);
+    return CL_OK;
+}
+
+cl_status Integrator::captureGraph(std::string* err)
+{
+    if (graph_)
+    {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CL_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), err);
+    cl_status s = CL_OK;
+    for (int w = 0; w < 4 && s == CL_OK; ++w) s = launchWave(w & 1, false, err);
+    cudaError_t e = cudaStreamEndCapture(stream_, &g);
+    if (s != CL_OK) return s;
+    CL_CUDA(e, err);
+    CL_CUDA(cudaGraphInstantiate(&graph_, g, 0), err);
+    cudaGraphDestroy(g);
+    graphValid_ = true;
+    return CL_OK;
+}
+
+cl_status Integrator::render(uint32_t spp, std::string* err)
+{
+    if (!sceneBuilt_ || !mats_.p || !hasCamera_)
+    {
+        *err = "render needs meshes, instances, materials and a camera";
+        return CL_ERR_STATE;
+    }
+    if (maxMaterialIndex_ >= numMaterials_)
+    {
+        *err = "an instance references material " + std::to_string(maxMaterialIndex_) + " of " +
+               std::to_string(numMaterials_);
+        return CL_ERR_INVALID_ARG;
+    }
+    if (spp == 0) return CL_OK;
+    CL_TRY(ensureFilm(err));
+    CL_TRY(ensureQueues(err));
+    const bool dl      = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
+    const bool profile = cfg_.flags & CL_PROFILE_STAGES;
+
+    WaveParams& wp = *hostWp_;
+    wp.W           = W_;
+    wp.H           = H_;
+    wp.frame0      = iteration_;
+    wp.maxDepth    = dl ? 1u : cfg_.max_depth;
+    wp.rrStart     = cfg_.rr_start_depth;
+    wp.flags       = cfg_.flags;
+    wp.dl          = dl ? 1u : 0u;
+    wp.totalPaths  = (unsigned long long)W_ * H_ * spp;
+    memcpy(wp.cam, &camera_, sizeof(camera_));
+    CL_CUDA(cudaMemcpyAsync(wp_.p, hostWp_, sizeof(WaveParams), cudaMemcpyHostToDevice, stream_), err);
+    uint32_t init = uint32_t(std::min<unsigned long long>(slots_, wp.totalPaths));
+    Counters c0{};
+    c0.rayCount[0] = init;
+    c0.pathNext    = init;
+    CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(Counters), cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err); // hostWp_/c0 reused next call
+
+    CL_CUDA(cudaEventRecord(evA_, stream_), err);
+    kRaygen<<<(init + 255) / 256, 256, 0, stream_>>>(params(), init);
+    CL_CUDA(cudaGetLastError(), err);
+    if (!profile && !graphValid_) CL_TRY(captureGraph(err));
+
+    msTrace_ = msShade_ = msShadow_ = 0.0f;
+    waves_   = 0;
+    Counters* dc = ctr_.as<Counters>();
+    for (int iter = 0; iter < 1 << 20; ++iter)
+    {
+        if (profile)
+        {
+            for (int w = 0; w < 4; ++w)
+            {
+                CL_TRY(launchWave(w & 1, true, err));
+                CL_CUDA(cudaStreamSynchronize(stream_), err);
+                float a = 0, b = 0, c = 0;
+                CL_CUDA(cudaEventElapsedTime(&a, evS_[0], evS_[1]), err);
+                CL_CUDA(cudaEventElapsedTime(&b, evS_[1], evS_[2]), err);
+                CL_CUDA(cudaEventElapsedTime(&c, evS_[2], evS_[3]), err);
+                msTrace_ += a;
+                msShade_ += b;
+                msShadow_ += c;
+            }
+        }
+        else
+            CL_CUDA(cudaGraphLaunch(graph_, stream_), err);
+        waves_ += 4;
+        CL_CUDA(cudaMemcpyAsync(hostCount_, &dc->rayCount[0], 4, cudaMemcpyDeviceToHost, stream_), err);
+        CL_CUDA(cudaStreamSynchronize(stream_), err);
+        if (hostCount_[0] == 0u) break;
+        if (iter + 1 == 1 << 20)
+        {
+            *err = "render did not drain its queues";
+            return CL_ERR_TIMEOUT;
+        }
+    }
+    CL_CUDA(cudaEventRecord(evB_, stream_), err);
+    Counters ch;
+    CL_CUDA(cudaMemcpyAsync(&ch, ctr_.p, sizeof(Counters), cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaEventSynchronize(evB_), err);
+    CL_CUDA(cudaEventElapsedTime(&msRender_, evA_, evB_), err);
+    if (ch.error)
+    {
+        *err = std::string("device error flags ") + std::to_string(ch.error) +
+               (ch.error & 1u ? " (traversal stack overflow)" : "") + (ch.error & 4u ? " (shadow queue overflow)" : "");
+        return (ch.error & 4u) ? CL_ERR_QUEUE_OVERFLOW : CL_ERR_STATE;
+    }
+    pathsDone_ += wp.totalPaths;
+    raysClosest_ += ch.raysClosest;
+    raysShadow_ += ch.raysShadow;
+    lastRaysC_  = ch.raysClosest;
+    lastRaysS_  = ch.raysShadow;
+    lastNodes_  = ch.statNodes;
+    lastTris_   = ch.statTris;
+    lastNodesS_ = ch.statNodesS;
+    lastTrisS_  = ch.statTrisS;
+    launches_   = waves_;
+    iteration_ += spp;
+    filmSpp_ += spp;
+    return CL_OK;
+}
+
+cl_status Integrator::readbackFilm(float* rgba, size_t bytes, std::string* err)
+{
+    size_t np = size_t(W_) * H_;
+    if (!rgba || bytes < np * 16)
+    {
+        *err = "film buffer too small";
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_TRY(ensureFilm(err));
+    CL_CUDA(cudaMemcpyAsync(rgba, film_.p, np * 16, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    float inv = filmSpp_ ? 1.0f / float(filmSpp_) : 0.0f;
+    for (size_t i = 0; i < np; ++i)
+    {
+        rgba[4 * i]     = rgba[4 * i] * inv;
+        rgba[4 * i + 1] = rgba[4 * i + 1] * inv;
+        rgba[4 * i + 2] = rgba[4 * i + 2] * inv;
+        rgba[4 * i + 3] = 1.0f;
+    }
+    return CL_OK;
+}
+
+cl_status Integrator::readbackFilmStats(double* sum, double* sumsq, size_t count, std::string* err)
+{
+    size_t np = size_t(W_) * H_;
+    if (!(cfg_.flags & CL_FILM_FP64))
+    {
+        *err = "FP64 film not enabled (CL_FILM_FP64)";
+        return CL_ERR_STATE;
+    }
+    if (!sum || !sumsq || count < np * 3)
+    {
+        *err = "film stats buffers too small";
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_TRY(ensureFilm(err));
+    std::vector<double> h(np * 6);
+    CL_CUDA(cudaMemcpyAsync(h.data(), film64_.p, np * 48, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    for (size_t i = 0; i < np; ++i)
+        for (int c = 0; c < 3; ++c)
+        {
+            sum[3 * i + c]   = h[6 * i + c];
+            sumsq[3 * i + c] = h[6 * i + 3 + c];
+        }
+    return CL_OK;
+}
+
+cl_status Integrator::resize(uint32_t w, uint32_t h, std::string* err)
+{
+    if (w == 0 || h == 0)
+    {
+        *err = "film size must be non-zero";
+        return CL_ERR_INVALID_ARG;
+    }
+    W_ = w;
+    H_ = h;
+    film_.release();
+    film64_.release();
+    CL_TRY(ensureFilm(err));
+    iteration_ = 0;
+    filmSpp_   = 0;
+    return CL_OK;
+}
+
+cl_status Integrator::resetIteration(std::string* err)
+{
+    iteration_ = 0;
+    return clearFilm(err);
+}
+
+void Integrator::stats(cl_stats* s) const
+{
+    memset(s, 0, sizeof(*s));
+    s->paths          = pathsDone_;
+    s->rays_closest   = raysClosest_;
+    s->rays_shadow    = raysShadow_;
+    s->iteration      = iteration_;
+    s->spp            = filmSpp_;
+    s->bvh_nodes      = bvh_.numNodes;
+    s->bvh_depth      = bvh_.depth;
+    s->triangles      = numTris_;
+    s->waves          = waves_;
+    s->ms_bvh_build   = msBvh_;
+    s->ms_dome_build  = msDome_;
+    s->ms_last_render = msRender_;
+    s->ms_trace       = msTrace_;
+    s->ms_shade       = msShade_;
+    s->ms_shadow      = msShadow_;
+    s->launches       = launches_;
+    s->trace_nodes    = lastNodes_;
+    s->trace_tris     = lastTris_;
+    s->shadow_nodes   = lastNodesS_;
+    s->shadow_tris    = lastTrisS_;
+    s->last_rays_closest = lastRaysC_;
+    s->last_rays_shadow  = lastRaysS_;
+}
+
+cl_status Integrator::traceRays(const float* rays, uint32_t n, float* t, uint32_t* prim, float* b1, float* b2,
+                                std::string* err)
+{
+    if (!sceneBuilt_)
+    {
+        *err = "scene not built";
+        return CL_ERR_STATE;
+    }
+    if (n == 0) return CL_OK;
+    if (!rays || !t || !prim || !b1 || !b2)
+    {
+        *err = "null argument";
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_TRY(ensureQueues(err));
+    std::vector<float4> o(slots_), d(slots_), h(slots_);
+    Counters* dc = ctr_.as<Counters>();
+    for (uint32_t base = 0; base < n; base += slots_)
+    {
+        uint32_t m = std::min(slots_, n - base);
+        for (uint32_t i = 0; i < m; ++i)
+        {
+            const float* r = rays + 8 * size_t(base + i);
+            o[i]           = make_float4(r[0], r[1], r[2], r[3]);
+            d[i]           = make_float4(r[4], r[5], r[6], r[7]);
+        }
+        CL_CUDA(cudaMemcpyAsync(rqO_[0].p, o.data(), m * 16, cudaMemcpyHostToDevice, stream_), err);
+        CL_CUDA(cudaMemcpyAsync(rqD_[0].p, d.data(), m * 16, cudaMemcpyHostToDevice, stream_), err);
+        Counters c0{};
+        c0.rayCount[0] = m;
+        CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
+        kTraceClosest<false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+            BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, rqO_[0].as<float4>(),
+            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc);
+        CL_CUDA(cudaGetLastError(), err);
+        CL_CUDA(cudaMemcpyAsync(h.data(), hit_.p, m * 16, cudaMemcpyDeviceToHost, stream_), err);
+        Counters ch;
+        CL_CUDA(cudaMemcpyAsync(&ch, ctr_.p, sizeof(ch), cudaMemcpyDeviceToHost, stream_), err);
+        CL_CUDA(cudaStreamSynchronize(stream_), err);
+        if (ch.error)
+        {
+            *err = "traversal error flags " + std::to_string(ch.error);
+            return CL_ERR_STATE;
+        }
+        for (uint32_t i = 0; i < m; ++i)
+        {
+            t[base + i]    = h[i].x;
+            uint32_t pb;
+            memcpy(&pb, &h[i].y, 4);
+            prim[base + i] = pb;
+            b1[base + i]   = h[i].z;
+            b2[base + i]   = h[i].w;
+        }
+    }
+    return CL_OK;
+}
+
+cl_status Integrator::occludedRays(const float* rays, uint32_t n, uint8_t* occ, std::string* err)
+{
+    if (!sceneBuilt_)
+    {
+        *err = "scene not built";
+        return CL_ERR_STATE;
+    }
+    if (n == 0) return CL_OK;
+    if (!rays || !occ)
+    {
+        *err = "null argument";
+        return CL_ERR_INVALID_ARG;
+    }
+    DevBuf o, d, r;
+    CL_TRY(o.alloc(size_t(n) * 16, err));
+    CL_TRY(d.alloc(size_t(n) * 16, err));
+    CL_TRY(r.alloc(n, err));
+    std::vector<float4> ho(n), hd(n);
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const float* q = rays + 8 * size_t(i);
+        ho[i]          = make_float4(q[0], q[1], q[2], q[3]);
+        hd[i]          = make_float4(q[4], q[5], q[6], q[7]);
+    }
+    CL_CUDA(cudaMemcpyAsync(o.p, ho.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(d.p, hd.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaMemsetAsync(ctr_.p, 0, sizeof(Counters), stream_), err);
+    kOccluded<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream_>>>(
+        BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, o.as<float4>(), d.as<float4>(), n,
+        r.as<uint8_t>(), &ctr_.as<Counters>()->error);
+    CL_CUDA(cudaGetLastError(), err);
+    CL_CUDA(cudaMemcpyAsync(occ, r.p, n, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    return CL_OK;
+}
+
+cl_status Integrator::traceStats(const float* rays, uint32_t n, uint64_t* nodes, uint64_t* tris, std::string* err)
+{
+    if (!sceneBuilt_)
+    {
+        *err = "scene not built";
+        return CL_ERR_STATE;
+    }
+    if (!rays || !nodes || !tris)
+    {
+        *err = "null argument";
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_TRY(ensureQueues(err));
+    Counters* dc = ctr_.as<Counters>();
+    uint64_t  an = 0, at = 0;
+    std::vector<float4> o(slots_), d(slots_);
+    for (uint32_t base = 0; base < n; base += slots_)
+    {
+        uint32_t m = std::min(slots_, n - base);
+        for (uint32_t i = 0; i < m; ++i)
+        {
+            const float* r = rays + 8 * size_t(base + i);
+            o[i]           = make_float4(r[0], r[1], r[2], r[3]);
+            d[i]           = make_float4(r[4], r[5], r[6], r[7]);
+        }
+        CL_CUDA(cudaMemcpyAsync(rqO_[0].p, o.data(), m * 16, cudaMemcpyHostToDevice, stream_), err);
+        CL_CUDA(cudaMemcpyAsync(rqD_[0].p, d.data(), m * 16, cudaMemcpyHostToDevice, stream_), err);
+        Counters c0{};
+        c0.rayCount[0] = m;
+        CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
+        kTraceClosest<true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+            BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, rqO_[0].as<float4>(),
+            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc);
+        CL_CUDA(cudaGetLastError(), err);
+        Counters ch;
+        CL_CUDA(cudaMemcpyAsync(&ch, ctr_.p, sizeof(ch), cudaMemcpyDeviceToHost, stream_), err);
+        CL_CUDA(cudaStreamSynchronize(stream_), err);
+        an += ch.statNodes;
+        at += ch.statTris;
+    }
+    *nodes = an;
+    *tris  = at;
+    return CL_OK;
+}
+
+cl_status Integrator::domeTables(float* pU, float* cU, float* pV, float* cV, std::string* err)
+{
+    if (!hasDome_)
+    {
+        *err = "no dome emitter";
+        return CL_ERR_STATE;
+    }
+    size_t a = size_t(dome_.w + 1) * dome_.h * 4, b = size_t(dome_.h + 1) * 4;
+    if (pU) CL_CUDA(cudaMemcpyAsync(pU, dome_.pU.p, a, cudaMemcpyDeviceToHost, stream_), err);
+    if (cU) CL_CUDA(cudaMemcpyAsync(cU, dome_.cU.p, a, cudaMemcpyDeviceToHost, stream_), err);
+    if (pV) CL_CUDA(cudaMemcpyAsync(pV, dome_.pV.p, b, cudaMemcpyDeviceToHost, stream_), err);
+    if (cV) CL_CUDA(cudaMemcpyAsync(cV, dome_.cV.p, b, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    return CL_OK;
+}
+
+cl_status Integrator::domeAliasSample(const float* u2, float* dir, float* pdf, float* val, uint32_t n, std::string* err)
+{
+    if (!hasDome_)
+    {
+        *err = "no dome emitter";
+        return CL_ERR_STATE;
+    }
+    if (n == 0) return CL_OK;
+    DevBuf du, dd, dp, dv;
+    CL_TRY(du.alloc(size_t(n) * 8, err));
+    CL_TRY(dd.alloc(size_t(n) * 12, err));
+    CL_TRY(dp.alloc(size_t(n) * 4, err));
+    CL_TRY(dv.alloc(size_t(n) * 12, err));
+    CL_CUDA(cudaMemcpyAsync(du.p, u2, size_t(n) * 8, cudaMemcpyHostToDevice, stream_), err);
+    kAliasSample<<<(n + 255) / 256, 256, 0, stream_>>>(dome_.view(), du.as<float2>(), dd.f(), dp.f(), dv.f(), n);
+    CL_CUDA(cudaGetLastError(), err);
+    CL_CUDA(cudaMemcpyAsync(dir, dd.p, size_t(n) * 12, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(pdf, dp.p, size_t(n) * 4, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(val, dv.p, size_t(n) * 12, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    return CL_OK;
+}
+
+} // namespace clb

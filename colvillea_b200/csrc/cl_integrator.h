@@ -1,0 +1,167 @@
+// The wavefront integrator (host side) and its device-visible layouts.
+#pragma once
+
+#include "cl_bvh.cuh"
+#include "cl_dome.h"
+#include "cl_internal.h"
+
+#include <vector>
+
+namespace clb
+{
+constexpr int      kMaxEmitters = 8;
+constexpr uint32_t kLastFlag    = 0x80000000u; // shadow entry: path ends after this shadow query
+
+struct EmitterDev
+{
+    uint32_t         type; // 0 directional, 1 dome
+    DirectionalLight dl;
+};
+
+struct SceneDev
+{
+    BvhView bvh;
+    const uint4* __restrict__ triIdx;  // per primitive: i0, i1, i2, material
+    const float4* __restrict__ vtx;    // 3 per vertex: {p.xyz, n.x} {n.y, n.z, t.x, t.y} {t.z, u, v, flags}
+    const float4* __restrict__ mats;   // 3 per material: {type, r.xyz} {alpha, etaInt, eta.xy} {eta.z, k.xyz}
+    DomeView   dome;
+    int        hasDome;
+    uint32_t   numEmitters;
+    EmitterDev emitters[kMaxEmitters];
+};
+
+// Per-render values, in device memory so that captured graphs stay valid.
+struct WaveParams
+{
+    uint32_t           W, H, frame0, maxDepth, rrStart, flags, dl, pad;
+    unsigned long long totalPaths;
+    float              cam[12];
+};
+
+struct Counters
+{
+    uint32_t           rayCount[2];
+    uint32_t           shadowCount;
+    uint32_t           fetchTrace, fetchShade, fetchShadow;
+    uint32_t           error;
+    uint32_t           pad;
+    unsigned long long pathNext;
+    unsigned long long raysClosest, raysShadow;
+    unsigned long long statNodes, statTris;
+    unsigned long long statNodesS, statTrisS;
+};
+
+struct QueueDev
+{
+    float4*   rqO[2];
+    float4*   rqD[2];
+    uint32_t* rqSlot[2];
+    float4*   hit;
+    float4*   sqO;  // {o.xyz, slot | kLastFlag bits}
+    float4*   sqD;  // {d.xyz, -}
+    float4*   sqL;  // {Li.xyz, -}
+    float4*   sqD2; // direct lighting: second (BSDF-sampled) shadow ray {d.xyz, valid}
+    float4*   sqL2;
+    uint4*    psInfo; // {pixel, frame, depth | rngCounter << 8, -}
+    float4*   psT;    // throughput
+    float4*   psE;    // escape weight (compat) / BSDF pdf in .x
+    float4*   psL;    // radiance so far
+    float4*   film;
+    double*   film64; // 6 per pixel: sum.rgb, sumsq.rgb
+    Counters* ctr;
+    uint32_t  slots;
+    uint32_t  shadowCap;
+};
+
+struct Params
+{
+    SceneDev          sc;
+    QueueDev          q;
+    const WaveParams* wp;
+};
+
+class Integrator
+{
+public:
+    Integrator(cl_integrator_type type, uint32_t w, uint32_t h, const cl_render_config& cfg);
+    ~Integrator();
+    cl_status init(std::string* err);
+
+    cl_status buildMeshes(const cl_mesh_desc* meshes, uint32_t n, std::string* err);
+    cl_status buildInstances(const cl_instance_desc* inst, uint32_t n, std::string* err);
+    cl_status buildMaterials(const cl_material_desc* m, uint32_t n, std::string* err);
+    cl_status buildEmitters(const cl_emitter_desc* e, uint32_t n, std::string* err);
+    cl_status updateCamera(const cl_camera* c, std::string* err);
+    cl_status render(uint32_t spp, std::string* err);
+    cl_status readbackFilm(float* rgba, size_t bytes, std::string* err);
+    cl_status readbackFilmStats(double* sum, double* sumsq, size_t count, std::string* err);
+    cl_status resize(uint32_t w, uint32_t h, std::string* err);
+    cl_status resetIteration(std::string* err);
+    void      stats(cl_stats* s) const;
+    cl_status traceRays(const float* rays, uint32_t n, float* t, uint32_t* prim, float* b1, float* b2,
+                        std::string* err);
+    cl_status occludedRays(const float* rays, uint32_t n, uint8_t* occ, std::string* err);
+    cl_status traceStats(const float* rays, uint32_t n, uint64_t* nodes, uint64_t* tris, std::string* err);
+    cl_status domeTables(float* pU, float* cU, float* pV, float* cV, std::string* err);
+    cl_status domeAliasSample(const float* u2, float* dir, float* pdf, float* val, uint32_t n, std::string* err);
+
+    uint32_t width() const { return W_; }
+    uint32_t height() const { return H_; }
+
+private:
+    cl_status ensureFilm(std::string* err);
+    cl_status ensureQueues(std::string* err);
+    cl_status clearFilm(std::string* err);
+    cl_status captureGraph(std::string* err);
+    cl_status launchWave(int cur, bool profile, std::string* err);
+    Params    params() const;
+
+    cl_integrator_type type_;
+    uint32_t           W_, H_;
+    cl_render_config   cfg_;
+    cudaStream_t       stream_ = nullptr;
+    int                numSMs_ = 148;
+    int                traceBlocks_ = 0, shadeBlocks_ = 0, shadowBlocks_ = 0;
+
+    // Meshes as given (host copies), flattened on instance build.
+    struct HostMesh
+    {
+        std::vector<float>    pos, nrm, tan, uv;
+        std::vector<uint32_t> idx;
+        bool                  hasN = false, hasUV = false;
+    };
+    std::vector<HostMesh> meshes_;
+
+    // Device scene.
+    DevBuf   triIdx_, vtx_, mats_, triPos_;
+    WideBvh  bvh_;
+    DomeTables dome_;
+    bool     hasDome_ = false;
+    std::vector<EmitterDev> emitters_;
+    uint32_t numMaterials_ = 0;
+    uint32_t numTris_      = 0;
+    uint32_t maxMaterialIndex_ = 0;
+    bool     sceneBuilt_   = false;
+
+    // Film and wavefront state.
+    DevBuf film_, film64_;
+    DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
+    DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_;
+    uint32_t slots_ = 0, shadowCap_ = 0;
+    WaveParams* hostWp_ = nullptr;   // pinned
+    uint32_t*   hostCount_ = nullptr; // pinned
+    cudaGraphExec_t graph_ = nullptr;
+    bool            graphValid_ = false;
+
+    cl_camera camera_{};
+    bool      hasCamera_ = false;
+    uint32_t  iteration_ = 0;
+    uint32_t  filmSpp_   = 0;
+    uint64_t  pathsDone_ = 0, raysClosest_ = 0, raysShadow_ = 0;
+    uint32_t  waves_ = 0, launches_ = 0;
+    uint64_t  lastNodes_ = 0, lastTris_ = 0, lastNodesS_ = 0, lastTrisS_ = 0, lastRaysC_ = 0, lastRaysS_ = 0;
+    float     msBvh_ = 0, msDome_ = 0, msRender_ = 0, msTrace_ = 0, msShade_ = 0, msShadow_ = 0;
+    cudaEvent_t evA_ = nullptr, evB_ = nullptr, evS_[6] = {};
+};
+
+} // namespace clb

@@ -1,0 +1,89 @@
+// Host-side internals shared by the library's translation units: device
+// buffers, error propagation and the built acceleration structure.
+#pragma once
+
+#include "../../include/colvillea_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+namespace clb
+{
+// Device allocation owned by one object (the reference's DeviceBuffer,
+// src/core/devices/cudabuffer.h:39-96, with errors returned, not exit()).
+struct DevBuf
+{
+    void*  p     = nullptr;
+    size_t bytes = 0;
+    DevBuf()     = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p     = nullptr;
+        bytes = 0;
+    }
+    cl_status alloc(size_t n, std::string* err)
+    {
+        release();
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess)
+        {
+            p    = nullptr;
+            *err = std::string("cudaMalloc(") + std::to_string(n) + ") failed: " + cudaGetErrorString(e);
+            cudaGetLastError();
+            return e == cudaErrorMemoryAllocation ? CL_ERR_OOM : CL_ERR_CUDA;
+        }
+        bytes = n;
+        return CL_OK;
+    }
+    float*    f() const { return static_cast<float*>(p); }
+    uint32_t* u() const { return static_cast<uint32_t*>(p); }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+#define CL_TRY(expr)                                                                                                   \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cl_status _s = (expr);                                                                                         \
+        if (_s != CL_OK) return _s;                                                                                    \
+    } while (0)
+
+#define CL_CUDA(expr, errp)                                                                                            \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t _e = (expr);                                                                                       \
+        if (_e != cudaSuccess)                                                                                         \
+        {                                                                                                              \
+            *(errp) = std::string(#expr) + ": " + cudaGetErrorString(_e);                                              \
+            return CL_ERR_CUDA;                                                                                        \
+        }                                                                                                              \
+    } while (0)
+
+struct WideBvh
+{
+    DevBuf   nodes; // 5 uint4 per node
+    DevBuf   tris;  // 3 float4 per triangle, leaf order
+    uint32_t numNodes = 0, depth = 0, numTris = 0;
+    void     release()
+    {
+        nodes.release();
+        tris.release();
+        numNodes = depth = numTris = 0;
+    }
+};
+
+// dTri9: 9 floats per triangle (world-space vertices), device memory.
+cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err);
+
+// Thread-local last error message (cl_last_error).
+void setLastError(const std::string& msg);
+
+} // namespace clb

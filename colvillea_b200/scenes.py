@@ -1,0 +1,435 @@
+"""Seeded synthetic scenes for the benchmark configurations.
+
+The reference's sample assets (sphere.obj, venice_sunset_2k.hdr,
+src/colvillea/colvillea.cpp:62,68) are not in its repository, so the
+workloads are generated here, deterministically from a seed:
+
+  cfg1  256x256, 16 spp, depth 5, RR from 3: 20x20 ground quad (2 tris) +
+        32 icospheres (subdivision 2, 320 tris), 256x128 HDRI + directional.
+  cfg2  1920x1080, 64 spp, depth 8, RR from 3: 1024x1024-vertex fBm terrain
+        (2,093,058 tris) + 512 icosphere/torus meshes (~5k tris each),
+        2048x1024 HDRI (8 lobes, peak 200) + directional.
+  cfg3  cfg1 scene at 1920x1080, 128 spp.
+  cfg4  cfg1 geometry with 60% rough dielectric (alpha U[0.01,0.1]),
+        2048x1024 HDRI with one lobe (peak 5000, sigma 0.5 deg).
+  cfg5  3840x2160, 256 spp, depth 16: 2048x2048-vertex terrain + 128 unique
+        meshes x 12 instances with random rotations and scales U[0.5, 2].
+
+Every mesh carries per-vertex normals, tangents and uvs (the reference
+requires tangents, src/core/devices/optix.cu:187-188).  A `Scene` holds the
+meshes, instances (entities), materials, emitters and camera in the
+reference's units and can be flattened to world-space arrays (`flatten`).
+"""
+import functools
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+MAT_DIFFUSE, MAT_METAL, MAT_GLASS = 0, 1, 2
+EMIT_DIRECTIONAL, EMIT_DOME = 0, 1
+GOLD_ETA = (0.143119, 0.374957, 1.442479)
+GOLD_K = (3.983160, 2.385721, 1.603215)
+IDENTITY = (1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0, 0.0)
+
+
+@dataclass
+class Mesh:
+    positions: np.ndarray  # (nv, 3) float32
+    normals: np.ndarray    # (nv, 3) float32 or None
+    tangents: np.ndarray   # (nv, 3) float32
+    uvs: np.ndarray        # (nv, 2) float32 or None
+    indices: np.ndarray    # (nt, 3) uint32
+
+
+@dataclass
+class Material:
+    type: int
+    reflectance: tuple = (0.0, 0.0, 0.0)
+    roughness: float = 0.0
+    interior_ior: float = 1.5
+    eta: tuple = (0.0, 0.0, 0.0)
+    k: tuple = (0.0, 0.0, 0.0)
+
+    def as_array(self):
+        return np.array([self.type, *self.reflectance, self.roughness, self.interior_ior, *self.eta, *self.k],
+                        np.float32)
+
+
+@dataclass
+class Emitter:
+    type: int
+    intensity: tuple = (0.0, 0.0, 0.0)
+    direction: tuple = (0.0, -1.0, 0.0)
+    angular_radius: float = 0.0
+    texels: np.ndarray = None  # (h, w, 4) float32
+
+    def as_array(self):
+        w = h = 0
+        if self.texels is not None:
+            h, w = self.texels.shape[:2]
+        return np.array([self.type, *self.intensity, *self.direction, self.angular_radius, w, h, 0, 0], np.float32)
+
+
+@dataclass
+class Scene:
+    width: int
+    height: int
+    meshes: list
+    instances: list          # (mesh_id, material_index, transform 12 floats)
+    materials: list
+    emitters: list
+    camera: np.ndarray       # (12,) pos, d00, ddu, ddv
+    spp: int = 16
+    max_depth: int = 5
+    rr_start: int = 3
+    name: str = ""
+    info: dict = field(default_factory=dict)
+
+    @property
+    def num_triangles(self):
+        return sum(len(self.meshes[m].indices) for m, _, _ in self.instances)
+
+    def dome(self):
+        for e in reversed(self.emitters):
+            if e.type == EMIT_DOME:
+                return e
+        return None
+
+    def flatten(self):
+        """World-space arrays in instance order (the order of global triangle ids)."""
+        pos, nrm, tan, uv, idx, tm = [], [], [], [], [], []
+        base = 0
+        for mesh_id, mat, xf in self.instances:
+            m = self.meshes[mesh_id]
+            M = np.asarray(xf, np.float64).reshape(3, 4)
+            if np.array_equal(M, np.asarray(IDENTITY).reshape(3, 4)):
+                p, n, t = m.positions, m.normals, m.tangents
+            else:
+                L = M[:, :3]
+                p = (m.positions.astype(np.float64) @ L.T + M[:, 3]).astype(np.float32)
+                t = (m.tangents.astype(np.float64) @ L.T).astype(np.float32)
+                n = (m.normals.astype(np.float64) @ np.linalg.inv(L)).astype(np.float32)
+            pos.append(p); nrm.append(n); tan.append(t); uv.append(m.uvs)
+            idx.append(m.indices.astype(np.uint32) + np.uint32(base))
+            tm.append(np.full(len(m.indices), mat, np.uint32))
+            base += len(m.positions)
+        dome = self.dome()
+        return FlatScene(
+            pos=np.concatenate(pos), nrm=np.concatenate(nrm), tan=np.concatenate(tan), uv=np.concatenate(uv),
+            idx=np.concatenate(idx), tri_material=np.concatenate(tm),
+            materials=np.stack([m.as_array() for m in self.materials]),
+            emitters=np.stack([e.as_array() for e in self.emitters]) if self.emitters else np.zeros((0, 12), np.float32),
+            dome_texels=dome.texels if dome is not None else np.zeros((1, 1, 4), np.float32),
+            camera=np.asarray(self.camera, np.float32), width=self.width, height=self.height)
+
+
+@dataclass
+class FlatScene:
+    pos: np.ndarray
+    nrm: np.ndarray
+    tan: np.ndarray
+    uv: np.ndarray
+    idx: np.ndarray
+    tri_material: np.ndarray
+    materials: np.ndarray
+    emitters: np.ndarray
+    dome_texels: np.ndarray
+    camera: np.ndarray
+    width: int
+    height: int
+
+
+# ---------------------------------------------------------------------------
+# Geometry
+# ---------------------------------------------------------------------------
+def _frame_from_normal(n):
+    """Unit tangent perpendicular to n, along the longitude direction."""
+    up = np.zeros_like(n); up[:, 1] = 1.0
+    t = np.cross(up, n)
+    bad = np.linalg.norm(t, axis=1) < 1e-6
+    t[bad] = np.array([1.0, 0.0, 0.0])
+    return t / np.linalg.norm(t, axis=1, keepdims=True)
+
+
+@functools.lru_cache(maxsize=8)
+def icosphere(subdiv):
+    """Unit icosphere: (positions, indices) float64/uint32 (cached; do not modify)."""
+    p = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, p, 0), (1, p, 0), (-1, -p, 0), (1, -p, 0), (0, -1, p), (0, 1, p), (0, -1, -p), (0, 1, -p),
+         (p, 0, -1), (p, 0, 1), (-p, 0, -1), (-p, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(x, np.float64) / np.linalg.norm(x) for x in v]
+    faces = f
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    v_out, f_out = np.array(verts), np.array(faces, np.uint32)
+    v_out.flags.writeable = False
+    f_out.flags.writeable = False
+    return v_out, f_out
+
+
+def sphere_mesh(subdiv, center, radius):
+    v, f = icosphere(subdiv)
+    n = v.copy()
+    pos = v * radius + np.asarray(center)
+    t = _frame_from_normal(n)
+    uv = np.stack([np.arctan2(n[:, 0], n[:, 2]) / (2 * np.pi) + 0.5, np.arccos(np.clip(n[:, 1], -1, 1)) / np.pi], 1)
+    return Mesh(pos.astype(np.float32), n.astype(np.float32), t.astype(np.float32), uv.astype(np.float32), f)
+
+
+def torus_mesh(nu, nv, center, R, r):
+    u = np.arange(nu) * 2 * np.pi / nu
+    w = np.arange(nv) * 2 * np.pi / nv
+    U, V = np.meshgrid(u, w, indexing="ij")
+    cu, su, cv, sv = np.cos(U), np.sin(U), np.cos(V), np.sin(V)
+    pos = np.stack([(R + r * cv) * cu, r * sv, (R + r * cv) * su], -1).reshape(-1, 3)
+    nrm = np.stack([cv * cu, sv, cv * su], -1).reshape(-1, 3)
+    tan = np.stack([-su, np.zeros_like(su), cu], -1).reshape(-1, 3)
+    uv = np.stack([U / (2 * np.pi), V / (2 * np.pi)], -1).reshape(-1, 2)
+    i = np.arange(nu)[:, None]; j = np.arange(nv)[None, :]
+    a = (i * nv + j); b = ((i + 1) % nu) * nv + j; c = ((i + 1) % nu) * nv + (j + 1) % nv; d = i * nv + (j + 1) % nv
+    idx = np.concatenate([np.stack([a, b, c], -1).reshape(-1, 3), np.stack([a, c, d], -1).reshape(-1, 3)])
+    return Mesh((pos + np.asarray(center)).astype(np.float32), nrm.astype(np.float32), tan.astype(np.float32),
+                uv.astype(np.float32), idx.astype(np.uint32))
+
+
+def quad_mesh(size, y=0.0):
+    h = size / 2.0
+    pos = np.array([[-h, y, -h], [h, y, -h], [h, y, h], [-h, y, h]], np.float32)
+    nrm = np.tile(np.array([0, 1, 0], np.float32), (4, 1))
+    tan = np.tile(np.array([1, 0, 0], np.float32), (4, 1))
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    idx = np.array([[0, 2, 1], [0, 3, 2]], np.uint32)
+    return Mesh(pos, nrm, tan, uv, idx)
+
+
+def _value_noise(x, z, rng_seed):
+    """2-D value noise on the integer lattice, smoothstep-interpolated."""
+    xi, zi = np.floor(x).astype(np.int64), np.floor(z).astype(np.int64)
+    fx, fz = x - xi, z - zi
+
+    def h(a, b):
+        k = (a * 73856093) ^ (b * 19349663) ^ (rng_seed * 83492791)
+        k = (k ^ (k >> 13)) * 1274126177
+        k = k ^ (k >> 16)
+        return (k & 0xFFFF).astype(np.float64) / 65535.0 * 2.0 - 1.0
+
+    sx, sz = fx * fx * (3 - 2 * fx), fz * fz * (3 - 2 * fz)
+    a = h(xi, zi) * (1 - sx) + h(xi + 1, zi) * sx
+    b = h(xi, zi + 1) * (1 - sx) + h(xi + 1, zi + 1) * sx
+    return a * (1 - sz) + b * sz
+
+
+def terrain_mesh(n, extent, amplitude, octaves, seed, y0=0.0):
+    """n x n vertex fBm heightfield over [-extent, extent]^2."""
+    s = np.linspace(-extent, extent, n)
+    X, Z = np.meshgrid(s, s, indexing="xy")
+    Hh = np.zeros_like(X)
+    freq, amp, norm = 4.0 / (2 * extent), 1.0, 0.0
+    for o in range(octaves):
+        Hh += amp * _value_noise(X * freq + 17.3 * o, Z * freq - 9.1 * o, seed + o)
+        norm += amp
+        freq *= 2.0
+        amp *= 0.5
+    Hh = Hh / norm * amplitude + y0
+    pos = np.stack([X, Hh, Z], -1).reshape(-1, 3)
+    dx = np.gradient(Hh, s, axis=1)
+    dz = np.gradient(Hh, s, axis=0)
+    nrm = np.stack([-dx, np.ones_like(dx), -dz], -1).reshape(-1, 3)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    tan = np.stack([np.ones_like(dx), dx, np.zeros_like(dx)], -1).reshape(-1, 3)
+    tan /= np.linalg.norm(tan, axis=1, keepdims=True)
+    uv = np.stack([(X + extent) / (2 * extent), (Z + extent) / (2 * extent)], -1).reshape(-1, 2)
+    i = np.arange(n - 1)[:, None]; j = np.arange(n - 1)[None, :]
+    a = i * n + j; b = a + 1; c = a + n + 1; d = a + n
+    idx = np.concatenate([np.stack([a, c, b], -1).reshape(-1, 3), np.stack([a, d, c], -1).reshape(-1, 3)])
+    return Mesh(pos.astype(np.float32), nrm.astype(np.float32), tan.astype(np.float32), uv.astype(np.float32),
+                idx.astype(np.uint32))
+
+
+# ---------------------------------------------------------------------------
+# Lights and camera
+# ---------------------------------------------------------------------------
+def texel_directions(w, h):
+    """Direction of each texel centre (hdridome.h:207-222 mapping)."""
+    u = (np.arange(w) + 0.5) / w
+    v = (np.arange(h) + 0.5) / h
+    U, V = np.meshgrid(u, v, indexing="xy")
+    th, ph = np.pi * V, -2 * np.pi * (U - 0.5)
+    return np.stack([np.sin(th) * np.sin(ph), np.cos(th), np.sin(th) * np.cos(ph)], -1)
+
+
+def hdri(w, h, lobes, rng, zenith=(0.3, 0.5, 1.0), horizon=(1.0, 1.0, 1.0)):
+    """Vertical sky gradient (zenith to horizon; lower hemisphere = horizon)
+    plus Gaussian lobes [(direction, sigma_deg, peak)], RGBA32F (h, w, 4)."""
+    d = texel_directions(w, h)
+    t = np.clip(d[..., 1], 0.0, 1.0)[..., None]
+    sky = np.asarray(horizon) * (1 - t) + np.asarray(zenith) * t
+    for dirv, sigma_deg, peak in lobes:
+        dirv = np.asarray(dirv, np.float64) / np.linalg.norm(dirv)
+        ang = np.arccos(np.clip(d @ dirv, -1.0, 1.0))
+        sig = math.radians(sigma_deg)
+        sky = sky + peak * np.exp(-ang * ang / (2 * sig * sig))[..., None]
+    out = np.ones((h, w, 4), np.float32)
+    out[..., :3] = sky
+    return out
+
+
+def random_upper_dirs(rng, n, min_y=0.15):
+    out = []
+    while len(out) < n:
+        v = rng.normal(size=3)
+        v /= np.linalg.norm(v)
+        if v[1] > min_y:
+            out.append(v)
+    return out
+
+
+def directional(irradiance=3.0, radius_deg=0.5, direction=(-0.35, -1.0, 0.45)):
+    """Sun disk: the reference's directional value is radiance over a cone of
+    the angular radius (directional.h:36-54), so intensity = E / (pi tan^2 r)."""
+    r = math.radians(radius_deg)
+    L = irradiance / (math.pi * math.tan(r) ** 2)
+    d = np.asarray(direction, np.float64)
+    d /= np.linalg.norm(d)
+    return Emitter(EMIT_DIRECTIONAL, (L, L, L), tuple(float(x) for x in d), r)
+
+
+def look_at_camera(pos, at, up, fov_deg, width, height):
+    """(pos, d00, ddu, ddv) of a pinhole camera (camera.h:8-27): pixel (x, y)
+    looks along d00 + (x/W) ddu + (y/H) ddv; y grows downwards."""
+    pos, at, up = (np.asarray(a, np.float64) for a in (pos, at, up))
+    f = at - pos
+    f /= np.linalg.norm(f)
+    r = np.cross(f, up); r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    hh = 2.0 * math.tan(math.radians(fov_deg) / 2.0)
+    ww = hh * width / height
+    ddu = r * ww
+    ddv = -u * hh
+    d00 = f - 0.5 * ddu - 0.5 * ddv
+    return np.concatenate([pos, d00, ddu, ddv]).astype(np.float32)
+
+
+def _random_material(rng, glass_frac=None, glass_alpha=(0.05, 0.3)):
+    if glass_frac is not None:
+        kind = MAT_GLASS if rng.random() < glass_frac else int(rng.integers(0, 2))
+    else:
+        kind = int(rng.integers(0, 3))
+    if kind == MAT_DIFFUSE:
+        return Material(MAT_DIFFUSE, reflectance=tuple(float(x) for x in rng.uniform(0.2, 0.8, 3)))
+    if kind == MAT_METAL:
+        a = rng.uniform(0.05, 0.5)
+        return Material(MAT_METAL, reflectance=(1.0, 1.0, 1.0), roughness=float(math.sqrt(a)), eta=GOLD_ETA, k=GOLD_K)
+    a = rng.uniform(*glass_alpha)
+    return Material(MAT_GLASS, roughness=float(math.sqrt(a)), interior_ior=1.5)
+
+
+# ---------------------------------------------------------------------------
+# Configurations
+# ---------------------------------------------------------------------------
+def config1(seed=0, width=256, height=256, glass_frac=None, glass_alpha=(0.05, 0.3), dome=None):
+    rng = np.random.default_rng(seed)
+    meshes, inst, mats = [quad_mesh(20.0)], [(0, 0, IDENTITY)], [Material(MAT_DIFFUSE, reflectance=(0.5, 0.5, 0.5))]
+    for i in range(32):
+        r = rng.uniform(0.2, 0.6)
+        c = (rng.uniform(-4, 4), rng.uniform(0.2, 2.0), rng.uniform(-4, 4))
+        meshes.append(sphere_mesh(2, c, r))
+        mats.append(_random_material(rng, glass_frac, glass_alpha))
+        inst.append((len(meshes) - 1, len(mats) - 1, IDENTITY))
+    if dome is None:
+        lobes = [(d, 2.0, 50.0) for d in random_upper_dirs(rng, 3)]
+        dome = Emitter(EMIT_DOME, texels=hdri(256, 128, lobes, rng))
+    ems = [directional(), dome]
+    cam = look_at_camera((0, 3, -10), (0, 0, 0), (0, 1, 0), 45.0, width, height)
+    return Scene(width, height, meshes, inst, mats, ems, cam, spp=16, max_depth=5, rr_start=3, name="cfg1")
+
+
+def config2(seed=0, width=1920, height=1080, terrain_n=1024, objects=512, hdri_size=(2048, 1024)):
+    rng = np.random.default_rng(seed)
+    meshes = [terrain_mesh(terrain_n, 40.0, 2.0, 5, seed + 101, y0=-1.0)]
+    mats = [Material(MAT_DIFFUSE, reflectance=(0.45, 0.42, 0.38))]
+    inst = [(0, 0, IDENTITY)]
+    for i in range(objects):
+        c = (rng.uniform(-30, 30), rng.uniform(0.5, 3.0), rng.uniform(-20, 40))
+        if rng.random() < 0.5:
+            meshes.append(sphere_mesh(4, c, rng.uniform(0.3, 1.2)))
+        else:
+            R = rng.uniform(0.4, 1.0)
+            meshes.append(torus_mesh(50, 50, c, R, R * rng.uniform(0.2, 0.4)))
+        mats.append(_random_material(rng))
+        inst.append((len(meshes) - 1, len(mats) - 1, IDENTITY))
+    w, h = hdri_size
+    lobes = [(d, 2.0, 200.0) for d in random_upper_dirs(rng, 8)]
+    dome = Emitter(EMIT_DOME, texels=hdri(w, h, lobes, rng))
+    cam = look_at_camera((0, 3, -10), (0, 0, 0), (0, 1, 0), 45.0, width, height)
+    return Scene(width, height, meshes, inst, mats, [directional(), dome], cam, spp=64, max_depth=8, rr_start=3,
+                 name="cfg2")
+
+
+def config3(seed=0):
+    s = config1(seed, 1920, 1080)
+    s.spp, s.name = 128, "cfg3"
+    return s
+
+
+def config4(seed=0):
+    rng = np.random.default_rng(seed + 7)
+    lobe = [(random_upper_dirs(rng, 1)[0], 0.5, 5000.0)]
+    dome = Emitter(EMIT_DOME, texels=hdri(2048, 1024, lobe, rng))
+    s = config1(seed, 1920, 1080, glass_frac=0.6, glass_alpha=(0.01, 0.1), dome=dome)
+    s.spp, s.max_depth, s.name = 128, 16, "cfg4"
+    return s
+
+
+def _rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    a, b, c, d = q
+    return np.array([[a*a+b*b-c*c-d*d, 2*(b*c-a*d), 2*(b*d+a*c)],
+                     [2*(b*c+a*d), a*a-b*b+c*c-d*d, 2*(c*d-a*b)],
+                     [2*(b*d-a*c), 2*(c*d+a*b), a*a-b*b-c*c+d*d]])
+
+
+def config5(seed=0, width=3840, height=2160, terrain_n=2048, unique=128, copies=12):
+    rng = np.random.default_rng(seed)
+    meshes = [terrain_mesh(terrain_n, 60.0, 2.5, 5, seed + 202, y0=-1.0)]
+    mats = [Material(MAT_DIFFUSE, reflectance=(0.45, 0.42, 0.38))]
+    inst = [(0, 0, IDENTITY)]
+    for u in range(unique):
+        if u % 2 == 0:
+            meshes.append(sphere_mesh(4, (0, 0, 0), 0.6))       # 5,120 tris
+        else:
+            meshes.append(torus_mesh(44, 44, (0, 0, 0), 0.6, 0.2))  # 3,872 tris
+        mats.append(_random_material(rng))
+        for c in range(copies):
+            s = rng.uniform(0.5, 2.0)
+            L = _rotation(rng) * s
+            t = (rng.uniform(-50, 50), rng.uniform(0.5, 4.0), rng.uniform(-30, 60))
+            M = np.concatenate([L, np.asarray(t)[:, None]], 1).reshape(-1)
+            inst.append((len(meshes) - 1, len(mats) - 1, tuple(float(x) for x in M)))
+    lobes = [(d, 2.0, 200.0) for d in random_upper_dirs(rng, 8)]
+    dome = Emitter(EMIT_DOME, texels=hdri(4096, 2048, lobes, rng))
+    cam = look_at_camera((0, 3, -10), (0, 0, 0), (0, 1, 0), 45.0, width, height)
+    return Scene(width, height, meshes, inst, mats, [directional(), dome], cam, spp=256, max_depth=16, rr_start=3,
+                 name="cfg5")
+
+
+CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4, 5: config5}

@@ -1,0 +1,272 @@
+/*
+ * colvillea_b200 — C ABI of the B200 (sm_100a) wavefront path tracer.
+ *
+ * This is the drop-in boundary for Colvillea's integrator layer.  It replaces
+ * the C++ interface `colvillea::core::Integrator`
+ * (include/colvillea/librender/integrator.h:34-103) and its factory
+ * `Integrator::createIntegrator` (src/core/librender/integrator.cpp:10-22),
+ * implemented in the reference by WavefrontPathTracingIntegrator
+ * (src/core/integrators/path.{h,cpp}) and WavefrontDirectLightingIntegrator
+ * (src/core/integrators/direct.{h,cpp}) on top of OptiX/OWL.
+ *
+ * Conventions
+ *   - Every call returns cl_status (CL_OK == 0).  Nothing calls exit(); the
+ *     reference's CHECK_CUDA_CALL -> exit(-1) (src/core/devices/cudacommon.h:13-26)
+ *     becomes an error code plus a message from cl_last_error().
+ *   - Inputs are caller-owned host arrays, copied during the call
+ *     (as the reference copies build* inputs, src/core/integrators/path.cpp:53-82).
+ *   - One host thread per integrator; calls are blocking, like the
+ *     reference's synchronous launches (src/core/devices/cudadevice.h:185-219).
+ *     Each integrator owns one CUDA stream on the current device.
+ *   - No torch or CUDA types appear in this header: plain pointers and sizes.
+ */
+#ifndef COLVILLEA_B200_H
+#define COLVILLEA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t cl_status;
+enum
+{
+    CL_OK                 = 0,
+    CL_ERR_CUDA           = 1, /* a CUDA runtime call failed */
+    CL_ERR_OOM            = 2, /* device allocation failed */
+    CL_ERR_QUEUE_OVERFLOW = 3, /* a work queue would have overflowed; items were dropped */
+    CL_ERR_TIMEOUT        = 4, /* a bounded device-side wait ran out */
+    CL_ERR_INVALID_ARG    = 5, /* bad argument (null, size, index out of range) */
+    CL_ERR_STATE          = 6  /* call out of order (e.g. render before the scene is built) */
+};
+
+/* IntegratorType (include/colvillea/librender/integrator.h:22-32). */
+typedef enum
+{
+    CL_INTEGRATOR_DIRECT_LIGHTING = 1, /* WavefrontDirectLighting */
+    CL_INTEGRATOR_PATH_TRACING    = 2  /* WavefrontPathTracing */
+} cl_integrator_type;
+
+/* Render configuration flags. */
+enum
+{
+    /* Reproduce the reference's pdf functions (SmoothDiffuse/RoughConductor/
+     * RoughDielectric::pdf, quirks Q1-Q3 of the survey). */
+    CL_COMPAT_PDF = 1u << 0,
+    /* Path tracing: shading frame normal = geometric normal, as the reference's
+     * swapped getShadingFrame arguments (raygeneration.cu:324-330). */
+    CL_COMPAT_FRAME = 1u << 1,
+    /* The reference's MIS / escaped-ray bookkeeping: emitter value scaled by
+     * the emitter count with the unscaled pdf in the weight, indirect rays only
+     * where the dome pdf is non-zero, and the BSDF weight applied twice to
+     * escaped indirect rays (raygeneration.cu:357,417,429-452,131). */
+    CL_COMPAT_ESCAPE = 1u << 2,
+    CL_COMPAT_ALL    = (1u << 0) | (1u << 1) | (1u << 2),
+    /* Sample the HDRI dome with the FP64-built alias tables instead of the
+     * reference's CDF binary search (same pdf values). */
+    CL_DOME_ALIAS = 1u << 4,
+    /* Keep an FP64 per-pixel film (sum and sum of squares of per-sample path
+     * radiance) next to the FP32 film. */
+    CL_FILM_FP64 = 1u << 5,
+    /* Time each wavefront stage with CUDA events (cl_get_stats). */
+    CL_PROFILE_STAGES = 1u << 6,
+    /* Count BVH nodes visited and triangles tested by the traversal kernels
+     * of each render (cl_get_stats); slower, for roofline accounting. */
+    CL_TRACE_STATS = 1u << 7
+};
+
+typedef struct
+{
+    uint32_t max_depth;      /* ray segments per path (reference: 5, path.cpp:135) */
+    uint32_t rr_start_depth; /* Russian roulette from this path depth on; 0 = off */
+    uint32_t flags;          /* CL_COMPAT_*, CL_DOME_ALIAS, CL_FILM_FP64, CL_PROFILE_STAGES */
+    uint32_t path_slots;     /* paths in flight; 0 = automatic */
+} cl_render_config;
+
+/* A triangle mesh (TriMesh, include/colvillea/libkernel/shapes/trimesh.h:16-32).
+ * positions/normals/tangents: 3 floats per vertex; uvs: 2 floats per vertex;
+ * indices: 3 uint32 per triangle.  Tangents are required (optix.cu:187-188);
+ * normals and uvs may be null (Ns = Ng, uv = barycentrics, optix.cu:146-172). */
+typedef struct
+{
+    const float*    positions;
+    const float*    normals;
+    const float*    tangents;
+    const float*    uvs;
+    uint32_t        num_vertices;
+    const uint32_t* indices;
+    uint32_t        num_triangles;
+} cl_mesh_desc;
+
+/* An entity: mesh instance + material (kernel::Entity, libkernel/base/entity.h:24-31,
+ * with a row-major 3x4 object-to-world transform; the reference has none). */
+typedef struct
+{
+    uint32_t mesh_id;
+    uint32_t material_index;
+    float    transform[12];
+} cl_instance_desc;
+
+/* Material (MaterialType, libkernel/base/material.h:24-37) in the reference's
+ * units: Diffuse{reflectance}; Metal{specular reflectance, roughness, eta, k};
+ * Glass{roughness, interior IOR}.  GGX alpha = roughness^2 (metal.h:52, glass.h:26). */
+enum
+{
+    CL_MATERIAL_DIFFUSE = 0,
+    CL_MATERIAL_METAL   = 1,
+    CL_MATERIAL_GLASS   = 2
+};
+typedef struct
+{
+    uint32_t type;
+    float    reflectance[3];
+    float    roughness;
+    float    interior_ior;
+    float    eta[3];
+    float    k[3];
+} cl_material_desc;
+
+/* Emitter (EmitterType, libkernel/base/emitter.h:16-26).  Directional:
+ * intensity, direction (from the light), angular radius (directional.h:19-22).
+ * Dome: RGBA32F texels (width*height*4 floats, row-major, v down from +Y). */
+enum
+{
+    CL_EMITTER_DIRECTIONAL = 0,
+    CL_EMITTER_HDRI_DOME   = 1
+};
+typedef struct
+{
+    uint32_t     type;
+    float        intensity[3];
+    float        direction[3];
+    float        angular_radius;
+    const float* texels;
+    uint32_t     width;
+    uint32_t     height;
+} cl_emitter_desc;
+
+/* Camera (include/colvillea/librender/nodebase/camera.h:8-27). */
+typedef struct
+{
+    float pos[3];
+    float d00[3];
+    float ddu[3];
+    float ddv[3];
+} cl_camera;
+
+typedef struct
+{
+    uint64_t paths;          /* camera paths completed, all renders */
+    uint64_t rays_closest;   /* closest-hit segments traced */
+    uint64_t rays_shadow;    /* shadow rays traced */
+    uint32_t iteration;      /* progressive frame index (path.cpp:220) */
+    uint32_t spp;            /* samples accumulated in the film */
+    uint32_t bvh_nodes;      /* 8-wide BVH nodes */
+    uint32_t bvh_depth;      /* 8-wide BVH depth */
+    uint32_t triangles;
+    uint32_t waves;          /* wavefront iterations in the last render */
+    float    ms_bvh_build;
+    float    ms_dome_build;
+    float    ms_last_render; /* device time of the last cl_render */
+    float    ms_trace;       /* last render, CL_PROFILE_STAGES: closest-hit kernels */
+    float    ms_shade;       /* ... shading kernels */
+    float    ms_shadow;      /* ... shadow kernels */
+    uint32_t launches;       /* last render: closest-hit kernel launches */
+    uint32_t pad;
+    uint64_t trace_nodes;    /* last render, CL_TRACE_STATS: closest-hit nodes visited */
+    uint64_t trace_tris;     /* ... closest-hit triangles tested */
+    uint64_t shadow_nodes;   /* ... shadow-ray nodes visited */
+    uint64_t shadow_tris;    /* ... shadow-ray triangles tested */
+    uint64_t last_rays_closest; /* last render: closest-hit segments */
+    uint64_t last_rays_shadow;  /* last render: shadow rays */
+} cl_stats;
+
+typedef struct cl_integrator cl_integrator;
+
+/* Integrator::createIntegrator (src/core/librender/integrator.cpp:10-22). */
+cl_status cl_integrator_create(cl_integrator_type type, uint32_t width, uint32_t height,
+                               const cl_render_config* config, cl_integrator** out);
+cl_status cl_integrator_destroy(cl_integrator* integrator);
+
+/* Integrator::buildBLAS (integrator.h:47). */
+cl_status cl_build_meshes(cl_integrator* integrator, const cl_mesh_desc* meshes, uint32_t count);
+/* Integrator::buildTLAS + buildGeometryEntities (integrator.h:49-54): builds the
+ * 8-wide BVH on the device over all instances. */
+cl_status cl_build_instances(cl_integrator* integrator, const cl_instance_desc* instances, uint32_t count);
+/* Integrator::buildMaterials (integrator.h:52). */
+cl_status cl_build_materials(cl_integrator* integrator, const cl_material_desc* materials, uint32_t count);
+/* Integrator::buildEmitters (integrator.h:56-58): the last dome in the list is
+ * the environment; its sampling tables are built on the device in FP64. */
+cl_status cl_build_emitters(cl_integrator* integrator, const cl_emitter_desc* emitters, uint32_t count);
+/* Integrator::updateCamera (integrator.h:80): resets accumulation on change
+ * (src/core/integrators/path.h:73-80). */
+cl_status cl_update_camera(cl_integrator* integrator, const cl_camera* camera);
+/* Integrator::render (integrator.h:61): `spp` progressive iterations. */
+cl_status cl_render(cl_integrator* integrator, uint32_t spp);
+/* Integrator::readbackFramebuffer (integrator.h:72): linear HDR mean radiance,
+ * RGBA32F, width*height*4 floats (alpha = 1). */
+cl_status cl_readback_film(cl_integrator* integrator, float* rgba, size_t bytes);
+/* FP64 film (CL_FILM_FP64): per-pixel sum and sum of squares, 3 doubles each. */
+cl_status cl_readback_film_stats(cl_integrator* integrator, double* sum, double* sumsq, size_t count);
+/* Integrator::resize / getFilmSize / resetIterationIndex (integrator.h:64,74,76). */
+cl_status cl_resize(cl_integrator* integrator, uint32_t width, uint32_t height);
+cl_status cl_get_film_size(cl_integrator* integrator, uint32_t* width, uint32_t* height);
+cl_status cl_reset_iteration(cl_integrator* integrator);
+cl_status cl_get_stats(cl_integrator* integrator, cl_stats* stats);
+/* Last error message of the calling thread. */
+cl_status cl_last_error(char* buffer, size_t size);
+
+/* ---- Ray queries on a built scene (OptiX trace replacement, optix.cu:38-110).
+ * rays: 8 floats each {o.xyz, tmin, d.xyz, tmax}.  Closest hit in (tmin, tmax);
+ * miss: prim = 0xffffffff.  prim is the triangle's global id in instance order. */
+cl_status cl_trace_rays(cl_integrator* integrator, const float* rays, uint32_t count, float* t, uint32_t* prim,
+                        float* b1, float* b2);
+cl_status cl_occluded_rays(cl_integrator* integrator, const float* rays, uint32_t count, uint8_t* occluded);
+/* Traversal statistics over the given rays: wide nodes visited and triangles
+ * tested, summed (closest-hit kernel). */
+cl_status cl_trace_stats(cl_integrator* integrator, const float* rays, uint32_t count, uint64_t* nodes,
+                         uint64_t* triangles);
+/* The dome's sampling tables as used by the device (reference layout,
+ * hdridome.h:494-510): pUcondV_c and CDFpUcondV (w+1)*h, pV_c and CDFpV h+1. */
+cl_status cl_get_dome_tables(cl_integrator* integrator, float* pUcondV_c, float* cdfU, float* pV_c, float* cdfV);
+
+/* ---- Device functions on batches (the exact device code the integrator runs).
+ * BSDF params: 11 floats per item {r.xyz, alpha, interior IOR, eta.xyz, k.xyz};
+ * type: CL_MATERIAL_* (BSDFType, libkernel/base/bsdf.h:17-30). */
+cl_status cl_unit_bsdf_eval(uint32_t type, const float* params, const float* wo, const float* wi, float* value,
+                            uint32_t count);
+cl_status cl_unit_bsdf_pdf(uint32_t type, const float* params, const float* wo, const float* wi, float* pdf,
+                           uint32_t count, uint32_t compat);
+cl_status cl_unit_bsdf_sample(uint32_t type, const float* params, const float* wo, const float* u2, float* wi,
+                              float* pdf, float* value, uint32_t count);
+cl_status cl_unit_ggx_eval(const float* alpha, const float* m, const float* wi, const float* wo, float* D, float* G1wi,
+                           float* G, float* pdfAll, uint32_t count);
+cl_status cl_unit_ggx_sample(const float* alpha, const float* u2, float* m, float* pdf, uint32_t count);
+cl_status cl_unit_fresnel_conductor(const float* cos_i, const float* eta, const float* k, float* out, uint32_t count);
+cl_status cl_unit_fresnel_dielectric(const float* cos_i, const float* eta, float* F, float* cos_t, uint32_t count);
+cl_status cl_unit_warp(const float* u2, float* disk, float* hemisphere, uint32_t count);
+cl_status cl_unit_make_frame(const float* a, float* b, float* c, uint32_t count);
+cl_status cl_unit_frame(const float* s, const float* t, const float* n, const float* v, float* local, float* world,
+                        uint32_t count);
+cl_status cl_unit_pcg4d(const uint32_t* in, uint32_t* out, uint32_t count);
+cl_status cl_unit_sampler_sequence(const uint32_t* px_py_frame, uint32_t count, uint32_t draws, float* out);
+/* HDRI dome against caller tables (reference layout): CDF sampling, pdf, eval. */
+cl_status cl_unit_dome_sample(const float* texels, uint32_t w, uint32_t h, const float* pUcondV_c, const float* cdfU,
+                              const float* pV_c, const float* cdfV, const float* u2, float* dir, float* pdf,
+                              float* value, uint32_t count);
+cl_status cl_unit_dome_pdf_eval(const float* texels, uint32_t w, uint32_t h, const float* pUcondV_c,
+                                const float* pV_c, const float* dirs, float* pdf, float* value, uint32_t count);
+/* Directional emitter: params {intensity.xyz, direction.xyz, angular radius}. */
+cl_status cl_unit_directional_sample(const float* params7, const float* u2, float* dir, float* pdf, float* value,
+                                     uint32_t count);
+/* Alias-table dome sampling on the integrator's dome (CL_DOME_ALIAS path). */
+cl_status cl_dome_alias_sample(cl_integrator* integrator, const float* u2, float* dir, float* pdf, float* value,
+                               uint32_t count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* COLVILLEA_B200_H */

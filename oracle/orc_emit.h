@@ -1,0 +1,383 @@
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of the reference's emitters (directional cone light, HDRI
+// dome with its 2-D piecewise-constant CDF sampler), the RGBA32F bilinear
+// texture lookup, the triangle hit-attribute computation and the ray-triangle
+// test.  See orc_core.h for the rules this restatement follows.
+#pragma once
+
+#include "orc_core.h"
+
+#include <vector>
+
+namespace orc
+{
+// ---------------------------------------------------------------------------
+// Texture lookup: tex2D<float4> on an RGBA32F array with wrap addressing,
+// linear filtering and normalised coordinates (imagetex2d.h:34-37, texture
+// description imagetex2d.cpp:51-65).  The hardware filter is replaced by
+// this FP32 definition, used identically on the GPU.
+// ---------------------------------------------------------------------------
+inline int wrapIndex(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+inline V3<float> texBilinear(const float* rgba, int w, int h, float u, float v)
+{
+    u       = u - std::floor(u);
+    v       = v - std::floor(v);
+    float x = u * float(w) - 0.5f;
+    float y = v * float(h) - 0.5f;
+    float fx = std::floor(x), fy = std::floor(y);
+    float ax = x - fx, ay = y - fy;
+    int   ix = int(fx), iy = int(fy);
+    int   x0 = wrapIndex(ix, w), x1 = wrapIndex(ix + 1, w);
+    int   y0 = wrapIndex(iy, h), y1 = wrapIndex(iy + 1, h);
+    const float* t00 = rgba + 4 * (size_t(y0) * w + x0);
+    const float* t10 = rgba + 4 * (size_t(y0) * w + x1);
+    const float* t01 = rgba + 4 * (size_t(y1) * w + x0);
+    const float* t11 = rgba + 4 * (size_t(y1) * w + x1);
+    float bx = 1.0f - ax, by = 1.0f - ay;
+    V3<float> out;
+    for (int c = 0; c < 3; ++c)
+    {
+        float top = t00[c] * bx + t10[c] * ax;
+        float bot = t01[c] * bx + t11[c] * ax;
+        out[c]    = top * by + bot * ay;
+    }
+    return out;
+}
+
+// linearToLuminance (math.h:155-158): evaluated in double, returned as float.
+inline float luminance(V3<float> c) { return float(double(c.x) * 0.212671 + double(c.y) * 0.71516 + double(c.z) * 0.072169); }
+
+// ---------------------------------------------------------------------------
+// HDRI dome (emitters/hdridome.h).  Tables laid out as the reference:
+// pUcondV_c and CDFpUcondV (w+1)*h, pV_c and CDFpV h+1.
+// ---------------------------------------------------------------------------
+struct Dome
+{
+    int          w = 0, h = 0;
+    const float* texels = nullptr; // RGBA32F, w*h
+    const float* pUcondV_c = nullptr;
+    const float* cdfU      = nullptr;
+    const float* pV_c      = nullptr;
+    const float* cdfV      = nullptr;
+};
+
+// Preprocessing, FP32, in the reference's order: prefiltering
+// (hdridome.h:311-324), preprocessPCondV (:333-385), preprocessPV (:387-432).
+inline void buildDomeTables(const float* texels, int w, int h, std::vector<float>& pU, std::vector<float>& cU,
+                            std::vector<float>& pV, std::vector<float>& cV)
+{
+    const int W1 = w + 1;
+    pU.assign(size_t(W1) * h, 0.0f);
+    cU.assign(size_t(W1) * h, 0.0f);
+    pV.assign(h + 1, 0.0f);
+    cV.assign(h + 1, 0.0f);
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x)
+        {
+            float u        = (float(x) + 0.5f) / float(w);
+            float v        = (float(y) + 0.5f) / float(h);
+            float sinTheta = std::sin(kPiF * (float(y) + 0.5f) / float(h));
+            pU[size_t(y) * W1 + x] = sinTheta * luminance(texBilinear(texels, w, h, u, v));
+        }
+    for (int y = 0; y < h; ++y)
+    {
+        float* p = &pU[size_t(y) * W1];
+        float* c = &cU[size_t(y) * W1];
+        c[0]     = 0.0f;
+        for (int i = 1; i < w + 1; ++i) c[i] = c[i - 1] + p[i - 1] / float(w);
+        float csum = c[w];
+        p[w]       = csum;
+        if (csum <= 0.0f)
+        {
+            for (int i = 0; i < w; ++i)
+            {
+                p[i] = 0.0f;
+                c[i] = float(i) / float(w);
+            }
+            c[w] = 1.0f;
+            p[w] = 0.0f;
+        }
+        else
+            for (int i = 0; i < w + 1; ++i) c[i] = c[i] / csum;
+        pV[y] = csum;
+    }
+    // preprocessPV: every job j in [0, h] reads pV[0..h-1] only.
+    std::vector<float> cdfOut(h + 1), pvOut(pV);
+    for (int j = 0; j <= h; ++j)
+    {
+        float sum = 0.0f, c = 0.0f;
+        for (int i = 1; i <= h; ++i)
+        {
+            if (i <= j) sum += pV[i - 1];
+            c += pV[i - 1];
+        }
+        cdfOut[j] = sum / float(h);
+        c         = c / float(h);
+        if (j == h) pvOut[h] = c;
+        if (c <= 0.0f)
+        {
+            pvOut[j]  = 0.0f;
+            cdfOut[j] = float(j) / float(h);
+        }
+        else
+            cdfOut[j] = cdfOut[j] / c;
+    }
+    pV = pvOut;
+    cV = cdfOut;
+}
+
+// upper_bound (math.h:84-96) over [begin, end).
+inline uint32_t upperBound(const float* a, uint32_t begin, uint32_t end, float value)
+{
+    while (begin < end)
+    {
+        uint32_t middle = begin + (end - begin) / 2;
+        if (a[middle] <= value)
+            begin = middle + 1;
+        else
+            end = middle;
+    }
+    return begin;
+}
+
+// Distribution1D::sample1D (hdridome.h:30-60).
+inline float sample1D(const float* f, const float* cdf, uint32_t N, float c, float u, uint32_t cdfOffset, float* pdf,
+                      uint32_t* sampledOffset)
+{
+    if (c == 0.0f) return 0.0f;
+    uint32_t off = upperBound(cdf, cdfOffset, cdfOffset + N + 1, u);
+    off          = off - 1;
+    off          = off < cdfOffset ? cdfOffset : (off > cdfOffset + N - 1 ? cdfOffset + N - 1 : off);
+    *pdf         = f[off] / c;
+    float du     = u - cdf[off];
+    if (cdf[off + 1] - cdf[off] != 0.0f) du = du / (cdf[off + 1] - cdf[off]);
+    off            = off - cdfOffset;
+    *sampledOffset = off;
+    return (float(off) + du) / float(N);
+}
+
+// Distribution2D::sample2D (hdridome.h:95-123).
+inline V2<float> sample2D(const Dome& d, V2<float> r, float* pdf)
+{
+    float    px = 0.0f, py = 0.0f;
+    uint32_t off = 0;
+    V2<float> pt{0.0f, 0.0f};
+    pt.y = sample1D(d.pV_c, d.cdfV, uint32_t(d.h), d.pV_c[d.h], r.y, 0, &py, &off);
+    uint32_t W1 = uint32_t(d.w) + 1;
+    pt.x        = sample1D(d.pUcondV_c, d.cdfU, uint32_t(d.w), d.pUcondV_c[size_t(off) * W1 + d.w], r.x, off * W1, &px, &off);
+    *pdf        = px * py;
+    return pt;
+}
+
+// Distribution2D::pdf2D (hdridome.h:125-135).
+inline float pdf2D(const Dome& d, V2<float> s)
+{
+    if (s.x < 0.f || s.y < 0.f) return 0.0f;
+    uint32_t tu = uint32_t(float(d.w) * s.x);
+    uint32_t tv = uint32_t(float(d.h) * s.y);
+    tu          = tu > uint32_t(d.w) - 1 ? uint32_t(d.w) - 1 : tu;
+    tv          = tv > uint32_t(d.h) - 1 ? uint32_t(d.h) - 1 : tv;
+    return d.pUcondV_c[size_t(tv) * (d.w + 1) + tu] / d.pV_c[d.h];
+}
+
+// directionToUVCoords (hdridome.h:472-476).
+inline V2<float> dirToUV(V3<float> dir)
+{
+    return {std::atan2(dir.x, dir.z) * -kInvPi * 0.5f + 0.5f, std::acos(dir.y) * kInvPi};
+}
+
+// evalEnvironment (hdridome.h:291-297).
+inline V3<float> domeEval(const Dome& d, V3<float> dir)
+{
+    V2<float> uv = dirToUV(dir);
+    return texBilinear(d.texels, d.w, d.h, uv.x, uv.y);
+}
+
+// HDRIDome::pdfDirect (hdridome.h:248-279), IMPORTANCE_SAMPLING on (Q11).
+inline float domePdf(const Dome& d, V3<float> dir)
+{
+    float phi      = std::atan2(dir.x, dir.z);
+    float theta    = std::acos(dir.y);
+    float sinTheta = std::sin(theta);
+    if (sinTheta == 0.0f) return 0.0f;
+    V2<float> uv{phi * -kInvPi * 0.5f + 0.5f, theta * kInvPi};
+    return pdf2D(d, uv) / (2.0f * kPiF * kPiF * sinTheta);
+}
+
+// HDRIDome::sampleDirect (hdridome.h:186-228).
+inline V3<float> domeSample(const Dome& d, V2<float> u, V3<float>* dir, float* pdf)
+{
+    V2<float> uv       = sample2D(d, u, pdf);
+    float     theta    = kPiF * uv.y;
+    float     phi      = -2 * kPiF * (uv.x - 0.5f);
+    float     sinTheta = std::sin(theta), cosTheta = std::cos(theta);
+    float     sinPhi = std::sin(phi), cosPhi = std::cos(phi);
+    if (sinTheta == 0.0f)
+    {
+        *pdf = 0.0f;
+        return {0.0f, 0.0f, 0.0f};
+    }
+    *dir = {sinTheta * sinPhi, cosTheta, sinTheta * cosPhi}; // warp.h:16-22
+    *pdf = *pdf / (2.0f * kPiF * kPiF * sinTheta);
+    return texBilinear(d.texels, d.w, d.h, uv.x, uv.y);
+}
+
+// ---------------------------------------------------------------------------
+// Directional emitter (emitters/directional.h:30-66).
+// ---------------------------------------------------------------------------
+struct Directional
+{
+    V3<float> intensity, direction;
+    float     angularRadius;
+};
+
+inline V3<float> directionalSample(const Directional& e, V2<float> u, V3<float>* dir, float* pdf)
+{
+    V3<float> rev  = -e.direction;
+    V2<float> disk = concentricDisk(u);
+    float     tr   = std::tan(e.angularRadius);
+    disk           = {disk.x * tr, disk.y * tr};
+    V3<float> ax, ay;
+    makeFrame(rev, &ax, &ay);
+    V3<float> d       = rev + ax * disk.x;
+    d                 = d + ay * disk.y;
+    *dir              = normalize(d);
+    float tanTheta    = std::sqrt(disk.x * disk.x + disk.y * disk.y);
+    float cosTheta    = 1.0f / std::sqrt(1.0f + tanTheta * tanTheta);
+    float tanR        = std::tan(e.angularRadius);
+    *pdf              = kInvPi / (tanR * tanR * cosTheta * cosTheta * cosTheta);
+    return e.intensity;
+}
+
+// ---------------------------------------------------------------------------
+// Ray-triangle test.  Watertight algorithm of Woop, Benthin and Wald (JCGT
+// 2013): shear into a ray-aligned frame, signed edge functions with a
+// double-precision re-evaluation when an edge function is exactly 0.
+// Replaces OptiX's built-in triangle test (optix.cu:64-74); the product's
+// traversal kernels evaluate the identical FP32 sequence.
+// ---------------------------------------------------------------------------
+struct RayPre
+{
+    V3<float> o;
+    int       kx, ky, kz;
+    float     Sx, Sy, Sz;
+};
+
+inline RayPre rayPrepare(V3<float> o, V3<float> d)
+{
+    RayPre r;
+    r.o      = o;
+    float ax = std::abs(d.x), ay = std::abs(d.y), az = std::abs(d.z);
+    r.kz     = (ax > ay) ? ((ax > az) ? 0 : 2) : ((ay > az) ? 1 : 2);
+    r.kx     = r.kz + 1 == 3 ? 0 : r.kz + 1;
+    r.ky     = r.kx + 1 == 3 ? 0 : r.kx + 1;
+    if (d[r.kz] < 0.0f) std::swap(r.kx, r.ky);
+    r.Sx = d[r.kx] / d[r.kz];
+    r.Sy = d[r.ky] / d[r.kz];
+    r.Sz = 1.0f / d[r.kz];
+    return r;
+}
+
+// Returns true with t, b1, b2 when the ray plane-crosses inside the
+// triangle (edges inclusive) with det != 0; the t-range test is the caller's.
+inline bool intersectTri(const RayPre& r, V3<float> v0, V3<float> v1, V3<float> v2, float* t, float* b1, float* b2)
+{
+    V3<float> A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+    float     Ax = A[r.kx] - r.Sx * A[r.kz], Ay = A[r.ky] - r.Sy * A[r.kz];
+    float     Bx = B[r.kx] - r.Sx * B[r.kz], By = B[r.ky] - r.Sy * B[r.kz];
+    float     Cx = C[r.kx] - r.Sx * C[r.kz], Cy = C[r.ky] - r.Sy * C[r.kz];
+    float     U = Cx * By - Cy * Bx;
+    float     V = Ax * Cy - Ay * Cx;
+    float     W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f)
+    {
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = U + V + W;
+    if (det == 0.0f) return false;
+    float Az = r.Sz * A[r.kz], Bz = r.Sz * B[r.kz], Cz = r.Sz * C[r.kz];
+    float T  = U * Az + V * Bz + W * Cz;
+    float rcp = 1.0f / det;
+    *t        = T * rcp;
+    *b1       = V * rcp;
+    *b2       = W * rcp;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Hit attributes (closest-hit program, optix.cu:137-227).
+// ---------------------------------------------------------------------------
+struct MeshView
+{
+    const float*    pos;  // 3 per vertex
+    const float*    nrm;  // 3 per vertex or null
+    const float*    tan;  // 3 per vertex (required, optix.cu:187-188)
+    const float*    uv;   // 2 per vertex or null
+    const uint32_t* idx;  // 3 per triangle (global vertex ids)
+};
+
+struct HitAttr
+{
+    V3<float> p, ng, ns, dpdu, dpdv;
+    V2<float> uv;
+};
+
+inline V3<float> ld3(const float* p, uint32_t i) { return {p[3 * size_t(i)], p[3 * size_t(i) + 1], p[3 * size_t(i) + 2]}; }
+
+inline HitAttr hitAttributes(const MeshView& m, uint32_t prim, float b1, float b2)
+{
+    uint32_t  i0 = m.idx[3 * size_t(prim)], i1 = m.idx[3 * size_t(prim) + 1], i2 = m.idx[3 * size_t(prim) + 2];
+    V3<float> p0 = ld3(m.pos, i0), p1 = ld3(m.pos, i1), p2 = ld3(m.pos, i2);
+    float     b0 = 1.0f - b1 - b2;
+    HitAttr   a;
+    a.p = b0 * p0 + b1 * p1;
+    a.p = a.p + b2 * p2;
+    if (m.uv)
+    {
+        const float* u = m.uv;
+        a.uv = {b0 * u[2 * i0] + b1 * u[2 * i1] + b2 * u[2 * i2], b0 * u[2 * i0 + 1] + b1 * u[2 * i1 + 1] + b2 * u[2 * i2 + 1]};
+    }
+    else
+        a.uv = {b0, b1};
+    V3<float> Ng = normalize(cross(p1 - p0, p2 - p0));
+    V3<float> Ns;
+    if (m.nrm)
+    {
+        V3<float> n = b0 * ld3(m.nrm, i0) + b1 * ld3(m.nrm, i1);
+        n           = n + b2 * ld3(m.nrm, i2);
+        Ns          = normalize(n);
+    }
+    else
+        Ns = normalize(Ng);
+    if (dot(Ns, Ns) == 0.0f) Ns = Ng;
+    if (dot(Ng, Ns) < 0.0f) Ng = -Ng;
+    V3<float> t    = b0 * ld3(m.tan, i0) + b1 * ld3(m.tan, i1);
+    t              = t + b2 * ld3(m.tan, i2);
+    V3<float> dpdu = normalize(t);
+    V3<float> dpdv{0.0f, 0.0f, 0.0f};
+    if (dot(dpdu, dpdu) > 0.0f)
+    {
+        dpdv = cross(Ns, dpdu);
+        if (dot(dpdv, dpdv) > 0.0f)
+        {
+            dpdv = normalize(dpdv);
+            dpdu = cross(dpdv, Ns);
+        }
+        else
+            makeFrame(Ns, &dpdu, &dpdv);
+    }
+    else
+        makeFrame(Ns, &dpdu, &dpdv);
+    a.ng   = Ng;
+    a.ns   = Ns;
+    a.dpdu = dpdu;
+    a.dpdv = dpdv;
+    return a;
+}
+
+} // namespace orc

@@ -1,0 +1,136 @@
+"""GPU unit kernels (cl_unit_*: the integrator's device functions) against the
+reference's own outputs (tests/golden, compiled from its sources) and the
+oracle, within 4 ulp in FP32; rarer differences must be explained by the FP64
+evaluation of the same formula (ill-conditioned spots, branch flips)."""
+import numpy as np
+import pytest
+
+from colvillea_b200 import _native as N
+from conftest import ulp_diff
+from gpu_util import P, check_ulp, f32, gpu_bsdf_eval, gpu_bsdf_pdf, gpu_bsdf_sample
+
+pytestmark = pytest.mark.gpu
+BSDFS = [(0, "diffuse"), (1, "conductor"), (2, "dielectric")]
+
+
+def test_pcg4d_and_sampler_exact(native, golden, oracle):
+    v = golden["pcg4d_in"]
+    out = np.zeros_like(v)
+    N.call("cl_unit_pcg4d", P(v), P(out), len(v))
+    assert np.array_equal(out, golden["pcg4d_out"])
+    s = golden["sampler_seeds"]
+    m = golden["sampler_seq"].shape[1]
+    seq = np.zeros((len(s), m), np.float32)
+    N.call("cl_unit_sampler_sequence", P(s), len(s), m, P(seq))
+    assert ulp_diff(seq, golden["sampler_seq"]).max() == 0
+
+
+@pytest.mark.parametrize("btype,name", BSDFS)
+def test_bsdf_vs_reference_golden(native, golden, oracle, btype, name):
+    g = lambda k: golden[f"{name}_{k}"]
+    ev = gpu_bsdf_eval(btype, g("params"), g("wo"), g("wi"))
+    ev64 = oracle.bsdf_eval(btype, g("params"), g("wo"), g("wi"), fp64=True)
+    check_ulp(f"{name}.eval", ev, g("eval"), ref64=ev64)
+    pdf = gpu_bsdf_pdf(btype, g("params"), g("wo"), g("wi"))
+    pdf64 = oracle.bsdf_pdf(btype, g("params"), g("wo"), g("wi"), compat=True, fp64=True)
+    check_ulp(f"{name}.pdf", pdf, g("pdf"), ref64=pdf64)
+    wi, spdf, sval = gpu_bsdf_sample(btype, g("params"), g("wo"), g("u2"))
+    wi64, spdf64, sval64 = oracle.bsdf_sample(btype, g("params"), g("wo"), g("u2"), fp64=True)
+    check_ulp(f"{name}.sample.wi", wi, g("swi"), ref64=wi64, min_frac=0.995)
+    check_ulp(f"{name}.sample.pdf", spdf, g("spdf"), ref64=spdf64, min_frac=0.995)
+    check_ulp(f"{name}.sample.value", sval, g("sval"), ref64=sval64, min_frac=0.995)
+
+
+@pytest.mark.parametrize("btype,name", BSDFS)
+def test_bsdf_vs_oracle_large(native, oracle, btype, name):
+    """2^16 seeded cases per BSDF, reference (compat) and corrected pdfs."""
+    rng = np.random.default_rng(100 + btype)
+    n = 1 << 16
+    p = np.zeros((n, 11), np.float32)
+    p[:, 0:3] = rng.uniform(0, 1, (n, 3)); p[:, 3] = rng.uniform(0.002, 0.8, n); p[:, 4] = rng.uniform(1.05, 2.4, n)
+    p[:, 5:8] = rng.uniform(0.05, 2.0, (n, 3)); p[:, 8:11] = rng.uniform(0.5, 5.0, (n, 3))
+    wo = rng.normal(size=(n, 3)); wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    wi = rng.normal(size=(n, 3)); wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+    wo[: n // 2, 2] = np.abs(wo[: n // 2, 2]); wi[: n // 2, 2] = np.abs(wi[: n // 2, 2])
+    u2 = rng.uniform(0, 1, (n, 2)).astype(np.float32)
+    wo, wi = f32(wo), f32(wi)
+    check_ulp(f"{name}.eval[64k]", gpu_bsdf_eval(btype, p, wo, wi), oracle.bsdf_eval(btype, p, wo, wi),
+              ref64=oracle.bsdf_eval(btype, p, wo, wi, fp64=True))
+    for compat in (True, False):
+        check_ulp(f"{name}.pdf[64k,compat={compat}]", gpu_bsdf_pdf(btype, p, wo, wi, compat),
+                  oracle.bsdf_pdf(btype, p, wo, wi, compat), ref64=oracle.bsdf_pdf(btype, p, wo, wi, compat, fp64=True))
+    g = gpu_bsdf_sample(btype, p, wo, u2)
+    c = oracle.bsdf_sample(btype, p, wo, u2)
+    c64 = oracle.bsdf_sample(btype, p, wo, u2, fp64=True)
+    for k, nm in enumerate(("wi", "pdf", "value")):
+        check_ulp(f"{name}.sample.{nm}[64k]", g[k], c[k], ref64=c64[k], other=c[k], min_frac=0.995)
+
+
+def test_ggx_fresnel_warps_frames(native, golden):
+    n = len(golden["ggx_alpha"])
+    D, G1, G, pa = (np.zeros(n, np.float32) for _ in range(4))
+    N.call("cl_unit_ggx_eval", P(golden["ggx_alpha"]), P(golden["ggx_m"]), P(golden["ggx_wi"]), P(golden["ggx_wo"]),
+           P(D), P(G1), P(G), P(pa), n)
+    for a, k in ((D, "ggx_D"), (G1, "ggx_G1"), (G, "ggx_G"), (pa, "ggx_pdfAll")):
+        check_ulp(k, a, golden[k])
+    m = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
+    N.call("cl_unit_ggx_sample", P(golden["ggx_alpha"]), P(golden["ggx_u2"]), P(m), P(pdf), n)
+    check_ulp("ggx.sample.m", m, golden["ggx_sm"], min_frac=0.995)
+    check_ulp("ggx.sample.pdf", pdf, golden["ggx_spdf"], min_frac=0.995)
+    fc = np.zeros((n, 3), np.float32)
+    N.call("cl_unit_fresnel_conductor", P(golden["fres_cos"]), P(golden["fres_eta3"]), P(golden["fres_k3"]), P(fc), n)
+    check_ulp("fresnel.conductor", fc, golden["fres_cond"])
+    F = np.zeros(n, np.float32); ct = np.zeros(n, np.float32)
+    N.call("cl_unit_fresnel_dielectric", P(golden["fres_cos"]), P(golden["fres_eta"]), P(F), P(ct), n)
+    check_ulp("fresnel.dielectric.F", F, golden["fres_diel"])
+    check_ulp("fresnel.dielectric.cosT", ct, golden["fres_cost"])
+    d = np.zeros((n, 2), np.float32); h = np.zeros((n, 3), np.float32)
+    N.call("cl_unit_warp", P(golden["warp_u2"]), P(d), P(h), n)
+    check_ulp("warp.disk", d, golden["warp_disk"], min_frac=0.995)
+    check_ulp("warp.hemisphere", h, golden["warp_hemi"], min_frac=0.995)
+    b = np.zeros((n, 3), np.float32); c = np.zeros((n, 3), np.float32)
+    N.call("cl_unit_make_frame", P(golden["mf_a"]), P(b), P(c), n)
+    assert ulp_diff(b, golden["mf_b"]).max() == 0 and ulp_diff(c, golden["mf_c"]).max() == 0
+    loc = np.zeros((n, 3), np.float32); wld = np.zeros((n, 3), np.float32)
+    N.call("cl_unit_frame", P(golden["fr_s"]), P(golden["fr_t"]), P(golden["fr_n"]), P(golden["fr_v"]), P(loc), P(wld), n)
+    assert ulp_diff(loc, golden["fr_local"]).max() == 0 and ulp_diff(wld, golden["fr_world"]).max() == 0
+
+
+def test_directional_and_dome_vs_oracle(native, oracle):
+    rng = np.random.default_rng(9)
+    n = 1 << 14
+    u2 = rng.uniform(0, 1, (n, 2)).astype(np.float32)
+    from colvillea_b200 import scenes
+    e = scenes.directional()
+    p7 = np.array([*e.intensity, *e.direction, e.angular_radius], np.float32)
+    dg = np.zeros((n, 3), np.float32); pg = np.zeros(n, np.float32); vg = np.zeros((n, 3), np.float32)
+    N.call("cl_unit_directional_sample", P(p7), P(u2), P(dg), P(pg), P(vg), n)
+    dc, pc, vc = oracle.directional_sample(p7, u2)
+    check_ulp("directional.dir", dg, dc)
+    check_ulp("directional.pdf", pg, pc)
+    assert np.array_equal(vg, vc)
+    # HDRI dome: CDF sampling, pdf and lookup against identical (oracle-built) tables
+    w, h = 256, 128
+    tex = scenes.hdri(w, h, [(d, 2.0, 50.0) for d in scenes.random_upper_dirs(rng, 3)], rng)
+    tabs = oracle.dome_build_tables(tex, w, h)
+    dg = np.zeros((n, 3), np.float32); pg = np.zeros(n, np.float32); vg = np.zeros((n, 3), np.float32)
+    N.call("cl_unit_dome_sample", P(f32(tex)), w, h, *(P(t) for t in tabs), P(u2), P(dg), P(pg), P(vg), n)
+    dc, pc, vc = oracle.dome_sample(tex, w, h, tabs, u2)
+    check_ulp("dome.sample.dir", dg, dc, min_frac=0.995)
+    check_ulp("dome.sample.pdf", pg, pc, min_frac=0.995)
+    check_ulp("dome.sample.value", vg, vc, min_frac=0.995)
+    dirs = rng.normal(size=(n, 3)); dirs = f32(dirs / np.linalg.norm(dirs, axis=1, keepdims=True))
+    pg = np.zeros(n, np.float32); vg = np.zeros((n, 3), np.float32)
+    N.call("cl_unit_dome_pdf_eval", P(f32(tex)), w, h, P(tabs[0]), P(tabs[2]), P(dirs), P(pg), P(vg), n)
+    pc, vc = oracle.dome_pdf_eval(tex, w, h, tabs, dirs)
+    check_ulp("dome.pdf", pg, pc, min_frac=0.99)
+    check_ulp("dome.eval", vg, vc, min_frac=0.99)
+
+
+def test_unit_entry_points_reject_bad_input(native):
+    L = N.lib()
+    assert L.cl_unit_bsdf_eval(3, None, None, None, None, 4) == N.CL_ERR_INVALID_ARG
+    assert L.cl_unit_sampler_sequence(None, 1, 1, None) == N.CL_ERR_INVALID_ARG
+    # zero-size batches are valid no-ops
+    z = np.zeros(1, np.float32)
+    assert L.cl_unit_warp(P(z), P(z), P(z), 0) == N.CL_OK
