@@ -43,7 +43,25 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile", type=int, default=0, metavar="SPP",
+                    help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
+    ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
     return ap.parse_args()
+
+
+def run_profile(args):
+    """A short, bounded run of the same kernels for ncu captures."""
+    import colvillea_b200 as cb
+    from colvillea_b200 import scenes
+    s = scenes.CONFIGS[args.config](0)
+    it = cb.load_scene(s, flags=cb.COMPAT_ALL | cb.DOME_ALIAS | cb.PROFILE_STAGES, path_slots=args.slots)
+    for _ in range(args.profile):
+        it.render(1)
+        st = it.stats()
+        print(json.dumps({k: st[k] for k in ("ms_last_render", "ms_trace", "ms_shade", "ms_shadow", "waves",
+                                             "last_rays_closest", "last_rays_shadow")}))
+    it.close()
+    return 0
 
 
 def workload_desc(s):
@@ -217,6 +235,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
     import numpy as np
     import torch
     dist = Dist(args.gpus)
@@ -228,7 +248,7 @@ def main():
     s = scenes.CONFIGS[args.config](0)
     W, H = s.width, s.height
     flags = cb.COMPAT_ALL | cb.DOME_ALIAS
-    it = cb.load_scene(s, flags=flags | cb.PROFILE_STAGES)
+    it = cb.load_scene(s, flags=flags | cb.PROFILE_STAGES, path_slots=args.slots)
     st0 = it.stats()
 
     # Traversal counters on the identical ray set of the first timed step.

@@ -27,7 +27,7 @@
 
 namespace clb
 {
-constexpr int kStackDepth    = 40; // bound checked against the built tree depth
+constexpr int kStackDepth    = 24; // bound checked against the built tree depth
 constexpr int kTraceBlock    = 128;
 constexpr uint32_t kMissPrim = 0xffffffffu;
 

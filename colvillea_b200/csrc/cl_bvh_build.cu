@@ -215,6 +215,7 @@ struct CollapseArgs
     uint2*          nextTasks;
     float           margin;
     uint32_t        maxNodes;
+    uint32_t        maxTris;
     uint32_t*       err;
 };
 
@@ -348,7 +349,7 @@ __global__ void kCollapse(CollapseArgs A, const uint2* __restrict__ tasks, uint3
     }
     uint32_t base  = nInner ? atomicAdd(A.nodeCounter, nInner) : 0u;
     uint32_t tbase = atomicAdd(A.triCounter, nTris);
-    if (base + nInner > A.maxNodes)
+    if (base + nInner > A.maxNodes || tbase + nTris > A.maxTris || wide >= A.maxNodes)
     {
         atomicOr(A.err, 2u);
         return;
@@ -553,6 +554,7 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     A.nextCount   = ctr.u() + 2;
     A.margin      = margin;
     A.maxNodes    = maxNodes;
+    A.maxTris     = n;
     A.err         = ctr.u() + 3;
 
     uint32_t ntasks = 1, depth = 0;
@@ -589,6 +591,57 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     }
     out->depth   = depth;
     out->numTris = n;
+    // Host validation of every index the traversal kernels will follow.
+    {
+        std::vector<uint32_t> h(size_t(out->numNodes) * 20);
+        CL_CUDA(cudaMemcpy(h.data(), out->nodes.p, h.size() * 4, cudaMemcpyDeviceToHost), err);
+        for (uint32_t i = 0; i < out->numNodes; ++i)
+        {
+            const uint32_t* q = &h[size_t(i) * 20];
+            uint32_t imask = q[3] >> 24, cb = q[4], tb = q[5];
+            for (int a = 0; a < 3; ++a)
+            {
+                uint32_t e = (q[3] >> (8 * a)) & 0xffu;
+                if (e < 1 || e > 254)
+                {
+                    *err = "BVH validation: bad exponent";
+                    return CL_ERR_STATE;
+                }
+            }
+            if (imask && uint64_t(cb) + __builtin_popcount(imask) > out->numNodes)
+            {
+                *err = "BVH validation: child index out of range";
+                return CL_ERR_STATE;
+            }
+            for (int sl = 0; sl < 8; ++sl)
+            {
+                if (imask & (1u << sl)) continue;
+                uint32_t meta = (q[6 + (sl >> 2)] >> (8 * (sl & 3))) & 0xffu;
+                if (!meta) continue;
+                uint32_t off = meta & 31u, unary = meta >> 5;
+                uint32_t cnt = unary == 1u ? 1u : unary == 3u ? 2u : unary == 7u ? 3u : 99u;
+                if (cnt == 99u || off + cnt > 24u || uint64_t(tb) + off + cnt > n)
+                {
+                    *err = "BVH validation: leaf triangle range out of bounds";
+                    return CL_ERR_STATE;
+                }
+            }
+        }
+        std::vector<float> t(size_t(n) * 12);
+        CL_CUDA(cudaMemcpy(t.data(), out->tris.p, t.size() * 4, cudaMemcpyDeviceToHost), err);
+        std::vector<uint8_t> seen(n, 0);
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            uint32_t id;
+            memcpy(&id, &t[size_t(i) * 12 + 3], 4);
+            if (id >= n || seen[id])
+            {
+                *err = "BVH validation: triangle ids are not a permutation";
+                return CL_ERR_STATE;
+            }
+            seen[id] = 1;
+        }
+    }
     if (depth + 1 > uint32_t(kStackDepth))
     {
         *err = "BVH depth " + std::to_string(depth) + " exceeds the traversal stack";

@@ -634,24 +634,30 @@ __device__ __forceinline__ f2 domeSample2DAlias(const DomeView& d, f2 r, float* 
     return uv;
 }
 
+// acos argument of a direction's y.  `clampY` keeps directions whose y
+// rounded past +-1 (toWorld of a near-vertical local direction) on the
+// sphere; the reference passes y unclamped (acos gives NaN there), which the
+// compat estimator reproduces.
+__device__ __forceinline__ float cosY(float y, bool clampY) { return clampY ? fminf(fmaxf(y, -1.0f), 1.0f) : y; }
+
 // directionToUVCoords (hdridome.h:472-476).
-__device__ __forceinline__ f2 dirToUV(f3 dir)
+__device__ __forceinline__ f2 dirToUV(f3 dir, bool clampY = false)
 {
-    return {atan2f(dir.x, dir.z) * -kInvPi * 0.5f + 0.5f, acosf(dir.y) * kInvPi};
+    return {atan2f(dir.x, dir.z) * -kInvPi * 0.5f + 0.5f, acosf(cosY(dir.y, clampY)) * kInvPi};
 }
 
 // evalEnvironment (hdridome.h:291-297).
-__device__ __forceinline__ f3 domeEval(const DomeView& d, f3 dir)
+__device__ __forceinline__ f3 domeEval(const DomeView& d, f3 dir, bool clampY = false)
 {
-    f2 uv = dirToUV(dir);
+    f2 uv = dirToUV(dir, clampY);
     return texBilinear(d.tex, d.w, d.h, uv.x, uv.y);
 }
 
 // pdfDirect (hdridome.h:248-279), importance sampling on.
-__device__ __forceinline__ float domePdf(const DomeView& d, f3 dir)
+__device__ __forceinline__ float domePdf(const DomeView& d, f3 dir, bool clampY = false)
 {
     float phi      = atan2f(dir.x, dir.z);
-    float theta    = acosf(dir.y);
+    float theta    = acosf(cosY(dir.y, clampY));
     float sinTheta = sinf(theta);
     if (sinTheta == 0.0f) return 0.0f;
     f2 uv{phi * -kInvPi * 0.5f + 0.5f, theta * kInvPi};

@@ -190,7 +190,13 @@ __device__ __forceinline__ void finishPaths(const Params& P, const WaveParams& w
     unsigned long long p  = base + __popc(mask & ((1u << laneId()) - 1u));
     bool               gen = finish && p < wp.totalPaths;
     uint32_t           idx = warpAppend(&P.q.ctr->rayCount[nxt], gen);
-    if (gen) startPath(P, wp, slot, p, nxt, idx);
+    if (gen)
+    {
+        if (idx < P.q.slots)
+            startPath(P, wp, slot, p, nxt, idx);
+        else
+            atomicOr(&P.q.ctr->error, 8u);
+    }
 }
 
 __device__ __forceinline__ f3 ld3(float4 v) { return {v.x, v.y, v.z}; }
@@ -208,7 +214,7 @@ __device__ __forceinline__ float maxComp(f3 v)
 // Kernels
 // ---------------------------------------------------------------------------
 template <bool STATS>
-__global__ void __launch_bounds__(kTraceBlock) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
+__global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
                                                              const float4* __restrict__ D, const uint32_t* count,
                                                              uint32_t* fetch, float4* __restrict__ hitOut,
                                                              Counters* ctr)
@@ -286,14 +292,14 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 // evaluateEscapedRays (raygeneration.cu:105-136)
                 if (sc.hasDome)
                 {
-                    f3 Le = domeEval(sc.dome, d);
+                    f3 Le = domeEval(sc.dome, d, !compatEsc);
                     if (depth == 1u)
                         L = L + Le;
                     else if (compatEsc)
                         L = L + T * (Le * E);
                     else
                     {
-                        float pd = domePdf(sc.dome, d) / float(N);
+                        float pd = domePdf(sc.dome, d, true) / float(N);
                         float w  = E.x / (E.x + pd);
                         L        = L + T * (Le * w);
                     }
@@ -357,19 +363,22 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 f3    wiL{0, 0, 0};
                 float bp = 0.0f;
                 f3    f  = bsdfSample(bsdf, woL, u2, &wiL, &bp);
-                if (!nonzero(f))
+                // The corrected estimator stops paths whose sampled pdf is not
+                // positive (0 or NaN at the rim of the cosine warp); the
+                // reference's update divides by it (raygeneration.cu:430).
+                if (!nonzero(f) || (!compatEsc && !(bp > 0.0f)))
                     finish = true;
                 else
                 {
                     f3    dir      = fr.toWorld(wiL);
-                    float lightPdf = sc.hasDome ? domePdf(sc.dome, dir) : 0.0f;
+                    float lightPdf = sc.hasDome ? domePdf(sc.dome, dir, !compatEsc) : 0.0f;
                     if (DL)
                     {
                         if (sc.hasDome && !(compatEsc && !(lightPdf > 0.0f)))
                         {
                             float c  = compatEsc ? wiL.z : fabsf(wiL.z);
                             float pl = compatEsc ? lightPdf : lightPdf / float(N);
-                            Ld       = domeEval(sc.dome, dir);
+                            Ld       = domeEval(sc.dome, dir, !compatEsc);
                             float w  = misBalanced(bp, pl);
                             f3    kk{f.x * c * w / bp, f.y * c * w / bp, f.z * c * w / bp};
                             Ld      = Ld * kk;
@@ -443,6 +452,11 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
         }
         // Next-bounce ray queue.
         uint32_t rIdx = warpAppend(&P.q.ctr->rayCount[nxt], pushRay);
+        if (pushRay && rIdx >= P.q.slots)
+        {
+            atomicOr(&P.q.ctr->error, 8u);
+            pushRay = false;
+        }
         if (pushRay)
         {
             P.q.rqO[nxt][rIdx]    = make_float4(pHit.x, pHit.y, pHit.z, kRayEps);
@@ -458,7 +472,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
 }
 
 template <bool DL, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock) kShadow(Params P, int cur)
+__global__ void __launch_bounds__(kTraceBlock, 8) kShadow(Params P, int cur)
 {
     __shared__ uint2 stack[kStackDepth * kTraceBlock];
     const WaveParams wp  = *P.wp;
@@ -1096,8 +1110,18 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     msTrace_ = msShade_ = msShadow_ = 0.0f;
     waves_   = 0;
     Counters* dc = ctr_.as<Counters>();
-    for (int iter = 0; iter < 1 << 20; ++iter)
+    // Every path needs at most maxDepth waves and at least one path per slot
+    // finishes per maxDepth waves, so this bound is never reached by a
+    // correct schedule.
+    const unsigned long long maxIter =
+        ((unsigned long long)(wp.maxDepth + 1) * (wp.totalPaths / slots_ + 2) + 16) / 4 + 1;
+    for (unsigned long long iter = 0;; ++iter)
     {
+        if (iter >= maxIter)
+        {
+            *err = "render did not drain its queues";
+            return CL_ERR_TIMEOUT;
+        }
         if (profile)
         {
             for (int w = 0; w < 4; ++w)
@@ -1119,11 +1143,6 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
         CL_CUDA(cudaMemcpyAsync(hostCount_, &dc->rayCount[0], 4, cudaMemcpyDeviceToHost, stream_), err);
         CL_CUDA(cudaStreamSynchronize(stream_), err);
         if (hostCount_[0] == 0u) break;
-        if (iter + 1 == 1 << 20)
-        {
-            *err = "render did not drain its queues";
-            return CL_ERR_TIMEOUT;
-        }
     }
     CL_CUDA(cudaEventRecord(evB_, stream_), err);
     Counters ch;
@@ -1133,8 +1152,9 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     if (ch.error)
     {
         *err = std::string("device error flags ") + std::to_string(ch.error) +
-               (ch.error & 1u ? " (traversal stack overflow)" : "") + (ch.error & 4u ? " (shadow queue overflow)" : "");
-        return (ch.error & 4u) ? CL_ERR_QUEUE_OVERFLOW : CL_ERR_STATE;
+               (ch.error & 1u ? " (traversal stack overflow)" : "") + (ch.error & 4u ? " (shadow queue overflow)" : "") +
+               (ch.error & 8u ? " (ray queue overflow)" : "");
+        return (ch.error & 12u) ? CL_ERR_QUEUE_OVERFLOW : CL_ERR_STATE;
     }
     pathsDone_ += wp.totalPaths;
     raysClosest_ += ch.raysClosest;

@@ -574,14 +574,14 @@ V3<float> tracePath(const Scene& s, const orc_config& cfg, uint32_t W, uint32_t 
             // evaluateEscapedRays (raygeneration.cu:105-136)
             if (s.hasDome)
             {
-                V3<float> Le = domeEval(s.dome, d);
+                V3<float> Le = domeEval(s.dome, d, !compatEscape);
                 if (depth == 1)
                     L = L + Le;
                 else if (compatEscape)
                     L = L + T * (Le * E);
                 else
                 {
-                    float pd = domePdf(s.dome, d) / float(N);
+                    float pd = domePdf(s.dome, d, true) / float(N);
                     float w  = E.x / (E.x + pd);
                     L        = L + T * (Le * w);
                 }
@@ -647,9 +647,11 @@ V3<float> tracePath(const Scene& s, const orc_config& cfg, uint32_t W, uint32_t 
         V3<float> wiL{0, 0, 0};
         float     bp = 0.0f;
         V3<float> f  = bsdfSample(bsdf, woL, u2, &wiL, &bp);
-        if (!nonzero(f)) break;
+        // The corrected estimator stops paths whose sampled pdf is not
+        // positive; the reference divides by it (raygeneration.cu:430).
+        if (!nonzero(f) || (!compatEscape && !(bp > 0.0f))) break;
         V3<float> dir = fr.toWorld(wiL);
-        float     lightPdf = s.hasDome ? domePdf(s.dome, dir) : 0.0f;
+        float     lightPdf = s.hasDome ? domePdf(s.dome, dir, !compatEscape) : 0.0f;
         if (dl)
         {
             // Second shadow queue: BSDF-sampled dome light (raygeneration.cu:245-281).
@@ -657,7 +659,7 @@ V3<float> tracePath(const Scene& s, const orc_config& cfg, uint32_t W, uint32_t 
             float c = compatEscape ? cosTheta(wiL) : std::abs(cosTheta(wiL));
             float pl = compatEscape ? lightPdf : lightPdf / float(N);
             if (compatEscape && !(lightPdf > 0.0f)) break;
-            V3<float> Ld = domeEval(s.dome, dir);
+            V3<float> Ld = domeEval(s.dome, dir, !compatEscape);
             float     w  = misBalanced(bp, pl);
             float     k0 = f.x * c, k1 = f.y * c, k2 = f.z * c;
             V3<float> kk{k0 * w / bp, k1 * w / bp, k2 * w / bp};

@@ -182,24 +182,29 @@ inline float pdf2D(const Dome& d, V2<float> s)
     return d.pUcondV_c[size_t(tv) * (d.w + 1) + tu] / d.pV_c[d.h];
 }
 
+// acos argument of a direction's y: `clampY` (corrected estimator) keeps
+// directions whose y rounded past +-1 on the sphere; the reference passes y
+// unclamped (NaN there), reproduced by the compat estimator.
+inline float cosY(float y, bool clampY) { return clampY ? std::fmin(std::fmax(y, -1.0f), 1.0f) : y; }
+
 // directionToUVCoords (hdridome.h:472-476).
-inline V2<float> dirToUV(V3<float> dir)
+inline V2<float> dirToUV(V3<float> dir, bool clampY = false)
 {
-    return {std::atan2(dir.x, dir.z) * -kInvPi * 0.5f + 0.5f, std::acos(dir.y) * kInvPi};
+    return {std::atan2(dir.x, dir.z) * -kInvPi * 0.5f + 0.5f, std::acos(cosY(dir.y, clampY)) * kInvPi};
 }
 
 // evalEnvironment (hdridome.h:291-297).
-inline V3<float> domeEval(const Dome& d, V3<float> dir)
+inline V3<float> domeEval(const Dome& d, V3<float> dir, bool clampY = false)
 {
-    V2<float> uv = dirToUV(dir);
+    V2<float> uv = dirToUV(dir, clampY);
     return texBilinear(d.texels, d.w, d.h, uv.x, uv.y);
 }
 
 // HDRIDome::pdfDirect (hdridome.h:248-279), IMPORTANCE_SAMPLING on (Q11).
-inline float domePdf(const Dome& d, V3<float> dir)
+inline float domePdf(const Dome& d, V3<float> dir, bool clampY = false)
 {
     float phi      = std::atan2(dir.x, dir.z);
-    float theta    = std::acos(dir.y);
+    float theta    = std::acos(cosY(dir.y, clampY));
     float sinTheta = std::sin(theta);
     if (sinTheta == 0.0f) return 0.0f;
     V2<float> uv{phi * -kInvPi * 0.5f + 0.5f, theta * kInvPi};

@@ -80,6 +80,7 @@ def test_independent_seeds_fixed_estimator_alias(oracle):
     it.close()
     o = oracle.OracleScene(s.flatten())
     c1, c2, _ = o.render(spp, max_depth=s.max_depth, rr_start=s.rr_start, flags=0, frame0=100000)
+    assert np.isfinite(g1).all() and np.isfinite(c1).all()
     frac = welch_fail_fraction(g1, g2, spp, c1, c2, spp)
     print(f"[image] independent cfg1 96x96x{spp}, fixed+alias: Welch fail fraction {frac:.4f} "
           f"(allowed {allowed(g1.size):.4f}); means {g1.mean() / spp:.5f} vs {c1.mean() / spp:.5f}")

@@ -7,7 +7,7 @@ import pytest
 
 from colvillea_b200 import _native as N
 from conftest import ulp_diff
-from gpu_util import P, check_ulp, f32, gpu_bsdf_eval, gpu_bsdf_pdf, gpu_bsdf_sample
+from gpu_util import P, bilinear64, check_ulp, check_vec, f32, gpu_bsdf_eval, gpu_bsdf_pdf, gpu_bsdf_sample
 
 pytestmark = pytest.mark.gpu
 BSDFS = [(0, "diffuse"), (1, "conductor"), (2, "dielectric")]
@@ -28,17 +28,17 @@ def test_pcg4d_and_sampler_exact(native, golden, oracle):
 @pytest.mark.parametrize("btype,name", BSDFS)
 def test_bsdf_vs_reference_golden(native, golden, oracle, btype, name):
     g = lambda k: golden[f"{name}_{k}"]
+    # eval and pdf: every value within 4 ulp of the reference's own code
     ev = gpu_bsdf_eval(btype, g("params"), g("wo"), g("wi"))
-    ev64 = oracle.bsdf_eval(btype, g("params"), g("wo"), g("wi"), fp64=True)
-    check_ulp(f"{name}.eval", ev, g("eval"), ref64=ev64)
+    check_ulp(f"{name}.eval", ev, g("eval"), min_frac=1.0)
     pdf = gpu_bsdf_pdf(btype, g("params"), g("wo"), g("wi"))
-    pdf64 = oracle.bsdf_pdf(btype, g("params"), g("wo"), g("wi"), compat=True, fp64=True)
-    check_ulp(f"{name}.pdf", pdf, g("pdf"), ref64=pdf64)
+    check_ulp(f"{name}.pdf", pdf, g("pdf"), min_frac=1.0)
+    # sampling goes through sinf/cosf (CUDA vs glibc): outliers explained by FP64
     wi, spdf, sval = gpu_bsdf_sample(btype, g("params"), g("wo"), g("u2"))
     wi64, spdf64, sval64 = oracle.bsdf_sample(btype, g("params"), g("wo"), g("u2"), fp64=True)
-    check_ulp(f"{name}.sample.wi", wi, g("swi"), ref64=wi64, min_frac=0.995)
-    check_ulp(f"{name}.sample.pdf", spdf, g("spdf"), ref64=spdf64, min_frac=0.995)
-    check_ulp(f"{name}.sample.value", sval, g("sval"), ref64=sval64, min_frac=0.995)
+    check_vec(f"{name}.sample.wi", wi, g("swi"), ref64=wi64, min_frac=0.98, max_unexplained_frac=1e-3)
+    check_ulp(f"{name}.sample.pdf", spdf, g("spdf"), ref64=spdf64, min_frac=0.98, max_unexplained_frac=1e-3)
+    check_vec(f"{name}.sample.value", sval, g("sval"), ref64=sval64, min_frac=0.98, max_unexplained_frac=1e-3)
 
 
 @pytest.mark.parametrize("btype,name", BSDFS)
@@ -54,16 +54,16 @@ def test_bsdf_vs_oracle_large(native, oracle, btype, name):
     wo[: n // 2, 2] = np.abs(wo[: n // 2, 2]); wi[: n // 2, 2] = np.abs(wi[: n // 2, 2])
     u2 = rng.uniform(0, 1, (n, 2)).astype(np.float32)
     wo, wi = f32(wo), f32(wi)
-    check_ulp(f"{name}.eval[64k]", gpu_bsdf_eval(btype, p, wo, wi), oracle.bsdf_eval(btype, p, wo, wi),
-              ref64=oracle.bsdf_eval(btype, p, wo, wi, fp64=True))
+    check_ulp(f"{name}.eval[64k]", gpu_bsdf_eval(btype, p, wo, wi), oracle.bsdf_eval(btype, p, wo, wi), min_frac=1.0)
     for compat in (True, False):
         check_ulp(f"{name}.pdf[64k,compat={compat}]", gpu_bsdf_pdf(btype, p, wo, wi, compat),
-                  oracle.bsdf_pdf(btype, p, wo, wi, compat), ref64=oracle.bsdf_pdf(btype, p, wo, wi, compat, fp64=True))
+                  oracle.bsdf_pdf(btype, p, wo, wi, compat), min_frac=1.0)
     g = gpu_bsdf_sample(btype, p, wo, u2)
     c = oracle.bsdf_sample(btype, p, wo, u2)
     c64 = oracle.bsdf_sample(btype, p, wo, u2, fp64=True)
-    for k, nm in enumerate(("wi", "pdf", "value")):
-        check_ulp(f"{name}.sample.{nm}[64k]", g[k], c[k], ref64=c64[k], other=c[k], min_frac=0.995)
+    check_vec(f"{name}.sample.wi[64k]", g[0], c[0], ref64=c64[0], min_frac=0.98, max_unexplained_frac=1e-3)
+    check_ulp(f"{name}.sample.pdf[64k]", g[1], c[1], ref64=c64[1], min_frac=0.98, max_unexplained_frac=1e-3)
+    check_vec(f"{name}.sample.value[64k]", g[2], c[2], ref64=c64[2], min_frac=0.98, max_unexplained_frac=1e-3)
 
 
 def test_ggx_fresnel_warps_frames(native, golden):
@@ -72,22 +72,26 @@ def test_ggx_fresnel_warps_frames(native, golden):
     N.call("cl_unit_ggx_eval", P(golden["ggx_alpha"]), P(golden["ggx_m"]), P(golden["ggx_wi"]), P(golden["ggx_wo"]),
            P(D), P(G1), P(G), P(pa), n)
     for a, k in ((D, "ggx_D"), (G1, "ggx_G1"), (G, "ggx_G"), (pa, "ggx_pdfAll")):
-        check_ulp(k, a, golden[k])
+        check_ulp(k, a, golden[k], min_frac=1.0)
     m = np.zeros((n, 3), np.float32); pdf = np.zeros(n, np.float32)
     N.call("cl_unit_ggx_sample", P(golden["ggx_alpha"]), P(golden["ggx_u2"]), P(m), P(pdf), n)
-    check_ulp("ggx.sample.m", m, golden["ggx_sm"], min_frac=0.995)
-    check_ulp("ggx.sample.pdf", pdf, golden["ggx_spdf"], min_frac=0.995)
+    check_vec("ggx.sample.m", m, golden["ggx_sm"], min_frac=0.999)
+    check_ulp("ggx.sample.pdf", pdf, golden["ggx_spdf"], min_frac=1.0)
     fc = np.zeros((n, 3), np.float32)
     N.call("cl_unit_fresnel_conductor", P(golden["fres_cos"]), P(golden["fres_eta3"]), P(golden["fres_k3"]), P(fc), n)
-    check_ulp("fresnel.conductor", fc, golden["fres_cond"])
+    check_ulp("fresnel.conductor", fc, golden["fres_cond"], min_frac=1.0)
     F = np.zeros(n, np.float32); ct = np.zeros(n, np.float32)
     N.call("cl_unit_fresnel_dielectric", P(golden["fres_cos"]), P(golden["fres_eta"]), P(F), P(ct), n)
-    check_ulp("fresnel.dielectric.F", F, golden["fres_diel"])
-    check_ulp("fresnel.dielectric.cosT", ct, golden["fres_cost"])
+    check_ulp("fresnel.dielectric.F", F, golden["fres_diel"], min_frac=1.0)
+    check_ulp("fresnel.dielectric.cosT", ct, golden["fres_cost"], min_frac=1.0)
     d = np.zeros((n, 2), np.float32); h = np.zeros((n, 3), np.float32)
     N.call("cl_unit_warp", P(golden["warp_u2"]), P(d), P(h), n)
-    check_ulp("warp.disk", d, golden["warp_disk"], min_frac=0.995)
-    check_ulp("warp.hemisphere", h, golden["warp_hemi"], min_frac=0.995)
+    check_vec("warp.disk", d, golden["warp_disk"], min_frac=0.999)
+    # z = sqrt(1 - x^2 - y^2) amplifies the error of x, y by r / z near the rim
+    r2 = np.sum(golden["warp_disk"].astype(np.float64) ** 2, axis=1)
+    z = np.sqrt(np.maximum(1.0 - r2, 1e-12))
+    check_vec("warp.hemisphere", h, golden["warp_hemi"], min_frac=0.98, cond_ulp=4 + 4 * np.sqrt(r2) / z,
+              ill=r2 > 1 - 1e-6)
     b = np.zeros((n, 3), np.float32); c = np.zeros((n, 3), np.float32)
     N.call("cl_unit_make_frame", P(golden["mf_a"]), P(b), P(c), n)
     assert ulp_diff(b, golden["mf_b"]).max() == 0 and ulp_diff(c, golden["mf_c"]).max() == 0
@@ -106,8 +110,8 @@ def test_directional_and_dome_vs_oracle(native, oracle):
     dg = np.zeros((n, 3), np.float32); pg = np.zeros(n, np.float32); vg = np.zeros((n, 3), np.float32)
     N.call("cl_unit_directional_sample", P(p7), P(u2), P(dg), P(pg), P(vg), n)
     dc, pc, vc = oracle.directional_sample(p7, u2)
-    check_ulp("directional.dir", dg, dc)
-    check_ulp("directional.pdf", pg, pc)
+    check_vec("directional.dir", dg, dc)
+    check_ulp("directional.pdf", pg, pc, min_frac=1.0)
     assert np.array_equal(vg, vc)
     # HDRI dome: CDF sampling, pdf and lookup against identical (oracle-built) tables
     w, h = 256, 128
@@ -116,15 +120,30 @@ def test_directional_and_dome_vs_oracle(native, oracle):
     dg = np.zeros((n, 3), np.float32); pg = np.zeros(n, np.float32); vg = np.zeros((n, 3), np.float32)
     N.call("cl_unit_dome_sample", P(f32(tex)), w, h, *(P(t) for t in tabs), P(u2), P(dg), P(pg), P(vg), n)
     dc, pc, vc = oracle.dome_sample(tex, w, h, tabs, u2)
-    check_ulp("dome.sample.dir", dg, dc, min_frac=0.995)
-    check_ulp("dome.sample.pdf", pg, pc, min_frac=0.995)
-    check_ulp("dome.sample.value", vg, vc, min_frac=0.995)
+    check_vec("dome.sample.dir", dg, dc, min_frac=0.999)
+    check_ulp("dome.sample.pdf", pg, pc, min_frac=0.999)
+    check_vec("dome.sample.value", vg, vc, min_frac=0.999)
     dirs = rng.normal(size=(n, 3)); dirs = f32(dirs / np.linalg.norm(dirs, axis=1, keepdims=True))
     pg = np.zeros(n, np.float32); vg = np.zeros((n, 3), np.float32)
     N.call("cl_unit_dome_pdf_eval", P(f32(tex)), w, h, P(tabs[0]), P(tabs[2]), P(dirs), P(pg), P(vg), n)
     pc, vc = oracle.dome_pdf_eval(tex, w, h, tabs, dirs)
-    check_ulp("dome.pdf", pg, pc, min_frac=0.99)
-    check_ulp("dome.eval", vg, vc, min_frac=0.99)
+    # sin(acos(y)) is ill-conditioned at the poles; the texel lookup jumps at
+    # cell boundaries of u = atan2(x, z) / 2pi, v = acos(y) / pi
+    d64 = dirs.astype(np.float64)
+    u = np.arctan2(d64[:, 0], d64[:, 2]) * (-0.5 / np.pi) + 0.5
+    v = np.arccos(np.clip(d64[:, 1], -1, 1)) / np.pi
+    fu, fv = (u * w) % 1.0, (v * h) % 1.0
+    edge = (np.minimum(fu, 1 - fu) < 1e-4) | (np.minimum(fv, 1 - fv) < 1e-4) | (1 - np.abs(d64[:, 1]) < 1e-4)
+    check_ulp("dome.pdf", pg, pc, min_frac=0.99, ill=edge, rel_ok=1e-4)
+    # the bilinear lookup amplifies an atan2/acos ulp difference by the texel
+    # gradient: bound it by the FP64 response to a 4e-7 change of u and v
+    base = bilinear64(tex, u, v)
+    resp = np.zeros(len(u))
+    for du, dv in ((4e-7, 0), (-4e-7, 0), (0, 4e-7), (0, -4e-7)):
+        resp = np.maximum(resp, np.max(np.abs(bilinear64(tex, u + du, v + dv) - base), axis=1))
+    scale = np.max(np.abs(vc.astype(np.float64)), axis=1)
+    unit = np.spacing(np.maximum(scale, 1e-30).astype(np.float32)).astype(np.float64)
+    check_vec("dome.eval", vg, vc, min_frac=0.99, ill=edge, cond_ulp=4 + resp / unit)
 
 
 def test_unit_entry_points_reject_bad_input(native):
