@@ -107,6 +107,7 @@ _SIGS = {
     "cl_unit_dome_sample": [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp, u32],
     "cl_unit_dome_pdf_eval": [vp, u32, u32, vp, vp, vp, vp, vp, u32],
     "cl_unit_directional_sample": [vp, vp, vp, vp, vp, u32],
+    "cl_dome_build_tables_noalloc": [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp],
 }
 
 _lib = None

@@ -187,3 +187,111 @@ cl_status buildDome(const float* hostTexels, int w, int h, cudaStream_t st, Dome
 }
 
 } // namespace clb
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the dome build (cl_dome_build_tables_noalloc).
+//
+// For callers that cannot allocate device memory: code recording a CUDA
+// graph by stream capture, or hosts whose allocator owns all device memory.
+// The scratch of launchDomeBuild comes from one static device array instead
+// of cudaMalloc.  In host code `gDomeScratch` names a host-side stand-in, not
+// the device array, so its device address is resolved once per device with
+// cudaGetSymbolAddress (with that device current) and passed to the kernels.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace clb
+{
+namespace
+{
+constexpr size_t kNoAllocTexels = size_t(CL_DOME_NOALLOC_MAX_TEXELS);
+constexpr size_t kNoAllocRows   = size_t(CL_DOME_NOALLOC_MAX_ROWS);
+// Layout: weights (double, texels) | q (double, texels + rows) |
+//         rowC (double, rows) | idx (uint32, 2 texels + 2 rows).
+constexpr size_t kOffQ     = 8 * kNoAllocTexels;
+constexpr size_t kOffRowC  = kOffQ + 8 * (kNoAllocTexels + kNoAllocRows);
+constexpr size_t kOffIdx   = kOffRowC + 8 * kNoAllocRows;
+constexpr size_t kScratchB = kOffIdx + 4 * (2 * kNoAllocTexels + 2 * kNoAllocRows);
+static_assert(kScratchB == size_t(CL_DOME_NOALLOC_SCRATCH_BYTES), "scratch size mismatch");
+
+static __device__ __align__(256) unsigned char gDomeScratch[kScratchB];
+
+constexpr int kMaxDevices = 64;
+std::mutex    gScratchMutex;
+unsigned char* gScratchAddr[kMaxDevices] = {};
+
+// Device address of gDomeScratch on the current device (resolved on the
+// first call per device).
+cl_status scratchAddress(unsigned char** out, std::string* err)
+{
+    int dev = 0;
+    CL_CUDA(cudaGetDevice(&dev), err);
+    if (dev < 0 || dev >= kMaxDevices)
+    {
+        *err = "device index out of range";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lock(gScratchMutex);
+    if (!gScratchAddr[dev])
+    {
+        void*       p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, gDomeScratch);
+        if (e != cudaSuccess || !p)
+        {
+            *err = std::string("cudaGetSymbolAddress(dome scratch): ") + cudaGetErrorString(e);
+            cudaGetLastError();
+            return CL_ERR_CUDA;
+        }
+        gScratchAddr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = gScratchAddr[dev];
+    return CL_OK;
+}
+
+cl_status domeNoAlloc(const float* texels, uint32_t w, uint32_t h, float* pU, float* cU, float* pV, float* cV,
+                      uint32_t* aliasRow, uint32_t* aliasCol, void* stream, std::string* err)
+{
+    if (!texels || !pU || !cU || !pV || !cV || !aliasRow || !aliasCol)
+    {
+        *err = "cl_dome_build_tables_noalloc: null buffer";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (w == 0 || h == 0)
+    {
+        *err = "cl_dome_build_tables_noalloc: empty texture";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (size_t(w) * h > kNoAllocTexels || h > kNoAllocRows)
+    {
+        *err = "cl_dome_build_tables_noalloc: " + std::to_string(w) + "x" + std::to_string(h) +
+               " exceeds the static scratch (at most " + std::to_string(kNoAllocTexels) + " texels and " +
+               std::to_string(kNoAllocRows) + " rows); use cl_build_emitters";
+        return CL_ERR_INVALID_ARG;
+    }
+    if ((reinterpret_cast<uintptr_t>(texels) & 15u) || (reinterpret_cast<uintptr_t>(aliasRow) & 7u) ||
+        (reinterpret_cast<uintptr_t>(aliasCol) & 7u))
+    {
+        *err = "cl_dome_build_tables_noalloc: texels must be 16-byte and alias tables 8-byte aligned";
+        return CL_ERR_INVALID_ARG;
+    }
+    unsigned char* base = nullptr;
+    CL_TRY(scratchAddress(&base, err));
+    DomeScratch s{reinterpret_cast<double*>(base), reinterpret_cast<double*>(base + kOffRowC),
+                  reinterpret_cast<uint32_t*>(base + kOffIdx), reinterpret_cast<double*>(base + kOffQ)};
+    return launchDomeBuild(reinterpret_cast<const float4*>(texels), int(w), int(h), static_cast<cudaStream_t>(stream),
+                           s, pU, cU, pV, cV, reinterpret_cast<uint2*>(aliasRow), reinterpret_cast<uint2*>(aliasCol),
+                           err);
+}
+} // namespace
+} // namespace clb
+
+extern "C" cl_status cl_dome_build_tables_noalloc(const float* texels, uint32_t width, uint32_t height,
+                                                  float* pUcondV_c, float* cdfU, float* pV_c, float* cdfV,
+                                                  uint32_t* alias_row, uint32_t* alias_col, void* stream)
+{
+    std::string err;
+    cl_status   s = clb::domeNoAlloc(texels, width, height, pUcondV_c, cdfU, pV_c, cdfV, alias_row, alias_col, stream,
+                                     &err);
+    if (s != CL_OK) clb::setLastError(err);
+    return s;
+}

@@ -265,6 +265,43 @@ cl_status cl_unit_directional_sample(const float* params7, const float* u2, floa
 cl_status cl_dome_alias_sample(cl_integrator* integrator, const float* u2, float* dir, float* pdf, float* value,
                                uint32_t count);
 
+/* ---- Allocation-free dome preprocessing.
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory: code running while a CUDA stream is being captured into a graph,
+ * or hosts whose allocator owns all device memory (a memory pool handed out
+ * to the renderer), where cudaMalloc is either illegal or would bypass the
+ * pool.  The caller passes device buffers for the input and every output;
+ * the function allocates nothing.  Its FP64 scratch (texel weights, row
+ * integrals, alias work lists) lives in one static device array of
+ * CL_DOME_NOALLOC_SCRATCH_BYTES (about 12 MiB) that every GPU loading the
+ * library holds until the process exits; it limits the dome to
+ * CL_DOME_NOALLOC_MAX_TEXELS texels (e.g. 1024x512) and
+ * CL_DOME_NOALLOC_MAX_ROWS rows, larger sizes return CL_ERR_INVALID_ARG.
+ *   texels     device, RGBA32F, width*height*4 floats, 16-byte aligned
+ *   pUcondV_c, cdfU  device, (width+1)*height floats each
+ *   pV_c, cdfV       device, height+1 floats each
+ *   alias_row  device, 2*height uint32 {prob bits, row}, 8-byte aligned
+ *   alias_col  device, 2*width*height uint32 {prob bits, column}, 8-byte aligned
+ *   stream     cudaStream_t to run on (null: the legacy default stream)
+ * Results equal the tables cl_build_emitters builds for the same texels.
+ * The call is asynchronous on `stream`.  Its first call on a device resolves
+ * the scratch array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture begins.  All calls
+ * on a device share the one scratch array (each call overwrites every scratch
+ * value it reads, so nothing needs clearing), so calls whose work overlaps on
+ * the GPU (different streams, or threads) race: serialise them. */
+enum
+{
+    CL_DOME_NOALLOC_MAX_TEXELS = 1 << 19,
+    CL_DOME_NOALLOC_MAX_ROWS   = 4096
+};
+#define CL_DOME_NOALLOC_SCRATCH_BYTES                                                                              \
+    (8u * CL_DOME_NOALLOC_MAX_TEXELS + 8u * (CL_DOME_NOALLOC_MAX_TEXELS + CL_DOME_NOALLOC_MAX_ROWS) +              \
+     8u * CL_DOME_NOALLOC_MAX_ROWS + 4u * (2u * CL_DOME_NOALLOC_MAX_TEXELS + 2u * CL_DOME_NOALLOC_MAX_ROWS))
+cl_status cl_dome_build_tables_noalloc(const float* texels, uint32_t width, uint32_t height, float* pUcondV_c,
+                                       float* cdfU, float* pV_c, float* cdfV, uint32_t* alias_row,
+                                       uint32_t* alias_col, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
