@@ -42,7 +42,13 @@ struct TraceCounters
     uint32_t nodes, tris;
 };
 
-__device__ __forceinline__ float byteAt(uint32_t word, int b) { return float((word >> (8 * b)) & 0xffu); }
+// Exact float of byte b of `word`: PRMT builds 0x4B0000bb (= 2^23 + byte as
+// a float) and one FADD removes 2^23; both run on full-rate pipes (an I2F
+// conversion would go through the quarter-rate XU pipe).
+__device__ __forceinline__ float byteAt(uint32_t word, int b)
+{
+    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | uint32_t(b))) - 8388608.0f;
+}
 
 // Intersects the ray with the 8 children of one node; returns the hit mask:
 // bits 24..31 inner-child keys (slot ^ octant), bits 0..23 triangle offsets.
@@ -97,94 +103,126 @@ __device__ __forceinline__ uint32_t intersectNode(const BvhView& bvh, uint32_t i
     return hits;
 }
 
-// Traversal.  ANY: stop at the first hit in (tmin, tmax) (shadow rays; the
-// reference searches for the closest hit there, optix.cu:99-109, which gives
-// the same visibility).  Closest: smallest t in (tmin, tmax), ties to the
-// lower primitive id.  `stack` points at this thread's column of a shared
-// [kStackDepth][kTraceBlock] array.  Returns the primitive id or kMissPrim.
+// Per-ray traversal state, advanced one node (plus that node's triangles) per
+// step so that a warp can refill lanes whose ray finished.
+struct Trav
+{
+    RayPre   pre;
+    f3       inv;
+    uint32_t oct;
+    float    tmin, tmax;
+    uint2    ng, tg;
+    int      sp;
+    uint32_t best;
+    float    bt, b1, b2;
+};
+
+__device__ __forceinline__ void travInit(Trav& s, f3 o, f3 d, float tmin, float tmax)
+{
+    s.pre   = rayPrepare(o, d);
+    s.inv.x = 1.0f / (fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x);
+    s.inv.y = 1.0f / (fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y);
+    s.inv.z = 1.0f / (fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
+    s.oct   = (s.inv.x < 0.0f ? 1u : 0u) | (s.inv.y < 0.0f ? 2u : 0u) | (s.inv.z < 0.0f ? 4u : 0u);
+    s.tmin  = tmin;
+    s.tmax  = tmax;
+    // The root is slot 0 of a virtual parent: key = oct, imask = 1.
+    s.ng   = make_uint2(0u, (1u << (24 + s.oct)) | 1u);
+    s.tg   = make_uint2(0u, 0u);
+    s.sp   = 0;
+    s.best = kMissPrim;
+    s.bt   = tmax;
+    s.b1 = s.b2 = 0.0f;
+}
+
+// One traversal step.  ANY: stop at the first hit in (tmin, tmax) (shadow
+// rays; the reference searches for the closest hit there, optix.cu:99-109,
+// which gives the same visibility).  Closest: smallest t in (tmin, tmax),
+// ties to the lower primitive id.  `stack` points at this thread's column of
+// a shared [kStackDepth][kTraceBlock] array.  Returns true when the ray is
+// finished (s.best: primitive id or kMissPrim; s.bt, s.b1, s.b2).
+template <bool ANY, bool STATS>
+__device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* stack, TraceCounters* cnt, uint32_t* err)
+{
+    if (s.ng.y > 0x00ffffffu)
+    {
+        uint32_t key = __ffs(s.ng.y >> 24) - 1;
+        s.ng.y &= ~(1u << (24 + key));
+        uint32_t slot  = key ^ s.oct;
+        uint32_t imask = s.ng.y & 0xffu;
+        uint32_t child = s.ng.x + __popc(imask & ((1u << slot) - 1u));
+        if (s.ng.y > 0x00ffffffu)
+        {
+            if (s.sp >= kStackDepth)
+            {
+                atomicOr(err, 1u);
+                s.best = kMissPrim;
+                return true;
+            }
+            stack[s.sp * kTraceBlock] = s.ng;
+            ++s.sp;
+        }
+        uint32_t cb, tb, im;
+        uint32_t hits = intersectNode(bvh, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im);
+        if (STATS) cnt->nodes++;
+        s.ng = make_uint2(cb, (hits & 0xff000000u) | im);
+        s.tg = make_uint2(tb, hits & 0x00ffffffu);
+    }
+    while (s.tg.y)
+    {
+        uint32_t k = __ffs(s.tg.y) - 1;
+        s.tg.y &= ~(1u << k);
+        const float4* tp = bvh.tris + size_t(s.tg.x + k) * 3;
+        float4        a  = __ldg(tp + 0);
+        float4        b  = __ldg(tp + 1);
+        float4        c  = __ldg(tp + 2);
+        if (STATS) cnt->tris++;
+        float t, u, v;
+        if (intersectTri(s.pre, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z}, &t, &u, &v) && t > s.tmin)
+        {
+            uint32_t id = __float_as_uint(a.w);
+            if (ANY)
+            {
+                if (t < s.tmax)
+                {
+                    s.bt   = t;
+                    s.best = id;
+                    return true;
+                }
+            }
+            else if (t < s.bt || (t == s.bt && id < s.best))
+            {
+                s.bt   = t;
+                s.best = id;
+                s.b1   = u;
+                s.b2   = v;
+            }
+        }
+    }
+    if (s.ng.y <= 0x00ffffffu)
+    {
+        if (s.sp == 0) return true;
+        --s.sp;
+        s.ng = stack[s.sp * kTraceBlock];
+    }
+    return false;
+}
+
+// Whole traversal of one ray (used where lanes are not refilled).
 template <bool ANY, bool STATS>
 __device__ __forceinline__ uint32_t traverse(const BvhView& bvh, f3 o, f3 d, float tmin, float tmax, float* tHit,
                                              float* b1Hit, float* b2Hit, uint2* stack, TraceCounters* cnt,
                                              uint32_t* err)
 {
-    RayPre pre = rayPrepare(o, d);
-    f3     inv;
-    inv.x = 1.0f / (fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x);
-    inv.y = 1.0f / (fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y);
-    inv.z = 1.0f / (fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
-    uint32_t oct  = (inv.x < 0.0f ? 1u : 0u) | (inv.y < 0.0f ? 2u : 0u) | (inv.z < 0.0f ? 4u : 0u);
-    uint32_t best = kMissPrim;
-    float    bt = tmax, bb1 = 0.0f, bb2 = 0.0f;
-    int      sp = 0;
-    // The root is slot 0 of a virtual parent: key = oct, imask = 1.
-    uint2 ng = make_uint2(0u, (1u << (24 + oct)) | 1u);
-    for (;;)
+    Trav s;
+    travInit(s, o, d, tmin, tmax);
+    while (!travStep<ANY, STATS>(bvh, s, stack, cnt, err))
     {
-        uint2 tg = make_uint2(0u, 0u);
-        if (ng.y > 0x00ffffffu)
-        {
-            uint32_t key  = __ffs(ng.y >> 24) - 1;
-            ng.y &= ~(1u << (24 + key));
-            uint32_t slot  = key ^ oct;
-            uint32_t imask = ng.y & 0xffu;
-            uint32_t child = ng.x + __popc(imask & ((1u << slot) - 1u));
-            if (ng.y > 0x00ffffffu)
-            {
-                if (sp >= kStackDepth)
-                {
-                    atomicOr(err, 1u);
-                    break;
-                }
-                stack[sp * kTraceBlock] = ng;
-                ++sp;
-            }
-            uint32_t cb, tb, im;
-            uint32_t hits = intersectNode(bvh, child, o, inv, oct, tmin, bt, &cb, &tb, &im);
-            if (STATS) cnt->nodes++;
-            ng = make_uint2(cb, (hits & 0xff000000u) | im);
-            tg = make_uint2(tb, hits & 0x00ffffffu);
-        }
-        while (tg.y)
-        {
-            uint32_t k = __ffs(tg.y) - 1;
-            tg.y &= ~(1u << k);
-            const float4* tp = bvh.tris + size_t(tg.x + k) * 3;
-            float4        a  = __ldg(tp + 0);
-            float4        b  = __ldg(tp + 1);
-            float4        c  = __ldg(tp + 2);
-            if (STATS) cnt->tris++;
-            float t, u, v;
-            if (intersectTri(pre, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z}, &t, &u, &v) && t > tmin)
-            {
-                uint32_t id = __float_as_uint(a.w);
-                if (ANY)
-                {
-                    if (t < tmax)
-                    {
-                        *tHit = t;
-                        return id;
-                    }
-                }
-                else if (t < bt || (t == bt && id < best))
-                {
-                    bt   = t;
-                    best = id;
-                    bb1  = u;
-                    bb2  = v;
-                }
-            }
-        }
-        if (ng.y <= 0x00ffffffu)
-        {
-            if (sp == 0) break;
-            --sp;
-            ng = stack[sp * kTraceBlock];
-        }
     }
-    *tHit  = bt;
-    *b1Hit = bb1;
-    *b2Hit = bb2;
-    return best;
+    *tHit  = s.bt;
+    *b1Hit = s.b1;
+    *b2Hit = s.b2;
+    return s.best;
 }
 
 } // namespace clb

@@ -4,9 +4,10 @@
 // src/core/devices/optixdevice.cpp:136-233) with a hand-written builder:
 //   1. per-triangle boxes and centroid bounds;
 //   2. 63-bit Morton codes of the centroids, sorted (CUB radix sort);
-//   3. binary radix tree (Karras, HPG 2012), one thread per inner node;
-//   4. bottom-up boxes and triangle counts (atomic arrival counters);
-//   5. top-down collapse to 8-wide nodes, one level per launch: each wide
+//   3. binary tree by PLOC clustering over the Morton order (Meister and
+//      Bittner 2018), SAH-quality at LBVH speed; the binary radix tree of
+//      Karras (HPG 2012) with bottom-up boxes is kept as a fallback;
+//   4. top-down collapse to 8-wide nodes, one level per launch: each wide
 //      node greedily opens its largest-area child with more than 3 triangles
 //      until it has 8 children; children with at most 3 triangles become
 //      leaf slots; slots are assigned by octant; child boxes are quantised to
@@ -15,6 +16,7 @@
 #include "cl_internal.h"
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <vector>
 
@@ -194,6 +196,145 @@ __global__ void kBottomUp(int n, const float* __restrict__ lo, const float* __re
         count[node] = ca + cb;
         node        = parent[node];
     }
+}
+
+// ---------------------------------------------------------------------------
+// PLOC (Meister and Bittner, "Parallel Locally-Ordered Clustering for
+// Bounding Volume Hierarchy Construction", IEEE TVCG 2018).  Clusters start as
+// the Morton-sorted triangles; each iteration finds every cluster's nearest
+// neighbour (smallest merged surface area) within a window of +-kPlocRadius
+// positions, merges mutual nearest neighbours into a new inner node and
+// compacts the cluster list in order, until one cluster is left.
+// ---------------------------------------------------------------------------
+constexpr int kPlocRadius = 16;
+constexpr int kPlocBlock  = 256;
+
+__device__ __forceinline__ float mergedArea(float4 alo, float4 ahi, float4 blo, float4 bhi)
+{
+    float dx = fmaxf(ahi.x, bhi.x) - fminf(alo.x, blo.x);
+    float dy = fmaxf(ahi.y, bhi.y) - fminf(alo.y, blo.y);
+    float dz = fmaxf(ahi.z, bhi.z) - fminf(alo.z, blo.z);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void kPlocInit(uint32_t n, const uint32_t* __restrict__ ids, const float* __restrict__ lo,
+                          const float* __restrict__ hi, uint32_t* __restrict__ C, float4* __restrict__ blo,
+                          float4* __restrict__ bhi)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t t = ids[i];
+    C[i]       = i | kLeafFlag;
+    blo[i]     = make_float4(lo[3 * size_t(t)], lo[3 * size_t(t) + 1], lo[3 * size_t(t) + 2], 0.0f);
+    bhi[i]     = make_float4(hi[3 * size_t(t)], hi[3 * size_t(t) + 1], hi[3 * size_t(t) + 2], 0.0f);
+}
+
+__global__ void __launch_bounds__(kPlocBlock) kPlocNearest(uint32_t m, const float4* __restrict__ blo,
+                                                           const float4* __restrict__ bhi, uint32_t* __restrict__ nn)
+{
+    __shared__ float4 slo[kPlocBlock + 2 * kPlocRadius], shi[kPlocBlock + 2 * kPlocRadius];
+    const int b0 = int(blockIdx.x) * kPlocBlock - kPlocRadius;
+    for (int k = threadIdx.x; k < kPlocBlock + 2 * kPlocRadius; k += kPlocBlock)
+    {
+        int g = b0 + k;
+        if (g >= 0 && g < int(m))
+        {
+            slo[k] = blo[g];
+            shi[k] = bhi[g];
+        }
+    }
+    __syncthreads();
+    int i = int(blockIdx.x) * kPlocBlock + int(threadIdx.x);
+    if (i >= int(m)) return;
+    int    li = i - b0;
+    float4 alo = slo[li], ahi = shi[li];
+    float  best  = FLT_MAX;
+    int    bestj = i == 0 ? 1 : i - 1;
+    int    j0 = max(0, i - kPlocRadius), j1 = min(int(m) - 1, i + kPlocRadius);
+    for (int j = j0; j <= j1; ++j)
+    {
+        if (j == i) continue;
+        float c = mergedArea(alo, ahi, slo[j - b0], shi[j - b0]);
+        if (c < best)
+        {
+            best  = c;
+            bestj = j;
+        }
+    }
+    nn[i] = uint32_t(bestj);
+}
+
+struct PlocTree
+{
+    uint32_t* left;
+    uint32_t* right;
+    float*    nlo;
+    float*    nhi;
+    uint32_t* count;
+    uint32_t* nodeCounter;
+};
+
+__global__ void kPlocMerge(uint32_t m, const uint32_t* __restrict__ C, const float4* __restrict__ blo,
+                           const float4* __restrict__ bhi, const uint32_t* __restrict__ nn, uint32_t* __restrict__ valid,
+                           uint32_t* __restrict__ C2, float4* __restrict__ blo2, float4* __restrict__ bhi2, PlocTree T,
+                           uint32_t maxInner)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    uint32_t j      = nn[i];
+    bool     mutual = nn[j] == i;
+    if (mutual && j < i)
+    {
+        valid[i] = 0u; // merged into cluster j
+        return;
+    }
+    valid[i] = 1u;
+    if (!mutual)
+    {
+        C2[i]   = C[i];
+        blo2[i] = blo[i];
+        bhi2[i] = bhi[i];
+        return;
+    }
+    uint32_t k = atomicAdd(T.nodeCounter, 1u);
+    if (k >= maxInner)
+    {
+        valid[i] = 1u;
+        C2[i]    = C[i];
+        blo2[i]  = blo[i];
+        bhi2[i]  = bhi[i];
+        return;
+    }
+    uint32_t a = C[i], b = C[j];
+    float4   lo = make_float4(fminf(blo[i].x, blo[j].x), fminf(blo[i].y, blo[j].y), fminf(blo[i].z, blo[j].z), 0.0f);
+    float4   hi = make_float4(fmaxf(bhi[i].x, bhi[j].x), fmaxf(bhi[i].y, bhi[j].y), fmaxf(bhi[i].z, bhi[j].z), 0.0f);
+    T.left[k]  = a;
+    T.right[k] = b;
+    T.nlo[3 * size_t(k)] = lo.x;
+    T.nlo[3 * size_t(k) + 1] = lo.y;
+    T.nlo[3 * size_t(k) + 2] = lo.z;
+    T.nhi[3 * size_t(k)] = hi.x;
+    T.nhi[3 * size_t(k) + 1] = hi.y;
+    T.nhi[3 * size_t(k) + 2] = hi.z;
+    uint32_t ca = (a & kLeafFlag) ? 1u : T.count[a];
+    uint32_t cb = (b & kLeafFlag) ? 1u : T.count[b];
+    T.count[k]  = ca + cb;
+    C2[i]       = k;
+    blo2[i]     = lo;
+    bhi2[i]     = hi;
+}
+
+__global__ void kPlocScatter(uint32_t m, const uint32_t* __restrict__ valid, const uint32_t* __restrict__ pos,
+                             const uint32_t* __restrict__ C2, const float4* __restrict__ blo2,
+                             const float4* __restrict__ bhi2, uint32_t* __restrict__ C, float4* __restrict__ blo,
+                             float4* __restrict__ bhi)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m || !valid[i]) return;
+    uint32_t d = pos[i];
+    C[d]       = C2[i];
+    blo[d]     = blo2[i];
+    bhi[d]     = bhi2[i];
 }
 
 struct CollapseArgs
@@ -497,14 +638,62 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     keys.release();
     ids.release();
 
-    CL_CUDA(cudaMemsetAsync(parent.p, 0xff, 2 * nn * 4, st), err);
-    CL_CUDA(cudaMemsetAsync(arrive.p, 0, ni * 4, st), err);
+    // Binary tree: PLOC over the Morton order (LBVH radix tree as fallback).
+    uint32_t rootRef = kLeafFlag; // a single triangle: the root is a leaf
     if (n > 1)
     {
-        kRadixTree<<<(n - 1 + 255) / 256, 256, 0, st>>>((uint64_t*)keys2.p, int(n), left.u(), right.u(), parent.u());
-        kBottomUp<<<blocks, 256, 0, st>>>(int(n), lo.f(), hi.f(), ids2.u(), left.u(), right.u(), parent.u(), nlo.f(),
-                                          nhi.f(), count.u(), arrive.u());
-        CL_CUDA(cudaGetLastError(), err);
+        DevBuf C, C2, blo, bhi, blo2, bhi2, nnb, valid, pos, scanTmp;
+        CL_TRY(C.alloc(nn * 4, err));
+        CL_TRY(C2.alloc(nn * 4, err));
+        CL_TRY(blo.alloc(nn * 16, err));
+        CL_TRY(bhi.alloc(nn * 16, err));
+        CL_TRY(blo2.alloc(nn * 16, err));
+        CL_TRY(bhi2.alloc(nn * 16, err));
+        CL_TRY(nnb.alloc(nn * 4, err));
+        CL_TRY(valid.alloc(nn * 4, err));
+        CL_TRY(pos.alloc(nn * 4, err));
+        size_t scanBytes = 0;
+        CL_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scanBytes, valid.u(), pos.u(), int(n), st), err);
+        CL_TRY(scanTmp.alloc(scanBytes, err));
+        CL_CUDA(cudaMemsetAsync(ctr.p, 0, 16, st), err);
+        PlocTree T{left.u(), right.u(), nlo.f(), nhi.f(), count.u(), ctr.u()};
+        kPlocInit<<<blocks, 256, 0, st>>>(n, ids2.u(), lo.f(), hi.f(), C.u(), blo.as<float4>(), bhi.as<float4>());
+        uint32_t m = n, iters = 0;
+        while (m > 1 && iters < 4096)
+        {
+            uint32_t g = (m + kPlocBlock - 1) / kPlocBlock;
+            kPlocNearest<<<g, kPlocBlock, 0, st>>>(m, blo.as<float4>(), bhi.as<float4>(), nnb.u());
+            kPlocMerge<<<g, kPlocBlock, 0, st>>>(m, C.u(), blo.as<float4>(), bhi.as<float4>(), nnb.u(), valid.u(),
+                                                 C2.u(), blo2.as<float4>(), bhi2.as<float4>(), T, n - 1);
+            CL_CUDA(cub::DeviceScan::ExclusiveSum(scanTmp.p, scanBytes, valid.u(), pos.u(), int(m), st), err);
+            kPlocScatter<<<g, kPlocBlock, 0, st>>>(m, valid.u(), pos.u(), C2.u(), blo2.as<float4>(), bhi2.as<float4>(),
+                                                   C.u(), blo.as<float4>(), bhi.as<float4>());
+            CL_CUDA(cudaGetLastError(), err);
+            uint32_t tail[2];
+            CL_CUDA(cudaMemcpyAsync(&tail[0], pos.u() + (m - 1), 4, cudaMemcpyDeviceToHost, st), err);
+            CL_CUDA(cudaMemcpyAsync(&tail[1], valid.u() + (m - 1), 4, cudaMemcpyDeviceToHost, st), err);
+            CL_CUDA(cudaStreamSynchronize(st), err);
+            m = tail[0] + tail[1];
+            ++iters;
+        }
+        if (m == 1)
+        {
+            CL_CUDA(cudaMemcpy(&rootRef, C.p, 4, cudaMemcpyDeviceToHost), err);
+            out->buildIterations = iters;
+        }
+        else
+        {
+            // Fall back to the LBVH radix tree (Karras 2012) with bottom-up boxes.
+            CL_CUDA(cudaMemsetAsync(parent.p, 0xff, 2 * nn * 4, st), err);
+            CL_CUDA(cudaMemsetAsync(arrive.p, 0, ni * 4, st), err);
+            kRadixTree<<<(n - 1 + 255) / 256, 256, 0, st>>>((uint64_t*)keys2.p, int(n), left.u(), right.u(),
+                                                            parent.u());
+            kBottomUp<<<blocks, 256, 0, st>>>(int(n), lo.f(), hi.f(), ids2.u(), left.u(), right.u(), parent.u(),
+                                              nlo.f(), nhi.f(), count.u(), arrive.u());
+            CL_CUDA(cudaGetLastError(), err);
+            rootRef = 0u;
+            out->buildIterations = 0;
+        }
     }
 
     Bounds bh;
@@ -534,7 +723,7 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     // ctr: [0] node counter, [1] tri counter, [2] next task count, [3] error
     uint32_t c0[4] = {1u, 0u, 0u, 0u};
     CL_CUDA(cudaMemcpyAsync(ctr.p, c0, 16, cudaMemcpyHostToDevice, st), err);
-    uint2 root = make_uint2(n > 1 ? 0u : kLeafFlag, 0u);
+    uint2 root = make_uint2(rootRef, 0u);
     CL_CUDA(cudaMemcpyAsync(tasksA.p, &root, 8, cudaMemcpyHostToDevice, st), err);
 
     CollapseArgs A;

@@ -11,7 +11,8 @@
 //                                          paths are written to the film and
 //                                          their slot restarts the next camera
 //                                          path (path regeneration)
-//               kShadow(shadow queue)   -> radiance; finishes paths whose last
+//               kTraceShadow(shadows)   -> visibility per shadow ray
+//               kShadowResolve          -> radiance; finishes paths whose last
 //                                          vertex had a shadow ray
 //               kAdvance                -> queue counters for the next wave
 //
@@ -213,11 +214,31 @@ __device__ __forceinline__ float maxComp(f3 v)
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void warpStats(const TraceCounters& tc, unsigned long long* nodes, unsigned long long* tris)
+{
+    unsigned long long a = tc.nodes, b = tc.tris;
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        a += __shfl_xor_sync(kFull, a, o);
+        b += __shfl_xor_sync(kFull, b, o);
+    }
+    if (laneId() == 0)
+    {
+        atomicAdd(nodes, a);
+        atomicAdd(tris, b);
+    }
+}
+
+// Closest-hit traversal of a ray queue.  Persistent warps fetch 32
+// consecutive rays at a time (one atomicAdd per warp) and each lane runs its
+// ray to completion.  (Refilling finished lanes mid-warp was measured slower
+// on B200: the per-step warp vote forces reconvergence and raised the
+// instruction count by half.)
 template <bool STATS>
 __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
-                                                             const float4* __restrict__ D, const uint32_t* count,
-                                                             uint32_t* fetch, float4* __restrict__ hitOut,
-                                                             Counters* ctr)
+                                                                const float4* __restrict__ D, const uint32_t* count,
+                                                                uint32_t* fetch, float4* __restrict__ hitOut,
+                                                                Counters* ctr)
 {
     __shared__ uint2 stack[kStackDepth * kTraceBlock];
     const uint32_t   n = loadCount(count);
@@ -229,27 +250,47 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
         uint32_t i = base + laneId();
         if (i < n)
         {
-            float4 o = O[i], d = D[i];
-            float  t, b1, b2;
+            float4   o = O[i], d = D[i];
+            float    t, b1, b2;
             uint32_t prim = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
                                                    stack + threadIdx.x, &tc, &ctr->error);
-            hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
+            hitOut[i]     = make_float4(t, __uint_as_float(prim), b1, b2);
         }
     }
-    if (STATS)
+    if (STATS) warpStats(tc, &ctr->statNodes, &ctr->statTris);
+}
+
+// Shadow rays (any hit) of the shadow queue.  Item k is entry k (path
+// tracing) or ray k&1 of entry k>>1 (direct lighting, two rays per entry).
+// vis[k] = 1 when the ray reaches its light, 0 otherwise.
+template <bool DL, bool STATS>
+__global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
+{
+    __shared__ uint2 stack[kStackDepth * kTraceBlock];
+    const uint32_t   n = loadCount(&P.q.ctr->shadowCount) * (DL ? 2u : 1u);
+    TraceCounters    tc{0u, 0u};
+    for (;;)
     {
-        unsigned long long a = tc.nodes, b = tc.tris;
-        for (int o = 16; o > 0; o >>= 1)
+        uint32_t base = warpFetch(&P.q.ctr->fetchShadow);
+        if (base >= n) break;
+        uint32_t item = base + laneId();
+        if (item < n)
         {
-            a += __shfl_xor_sync(kFull, a, o);
-            b += __shfl_xor_sync(kFull, b, o);
-        }
-        if (laneId() == 0)
-        {
-            atomicAdd(&ctr->statNodes, a);
-            atomicAdd(&ctr->statTris, b);
+            uint32_t e  = DL ? item >> 1 : item;
+            float4   o4 = P.q.sqO[e];
+            float4   d4 = (DL && (item & 1u)) ? P.q.sqD2[e] : P.q.sqD[e];
+            uint8_t  v  = 0;
+            if (d4.w != 0.0f)
+            {
+                float    t, b1, b2;
+                uint32_t h = traverse<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
+                                                   &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error);
+                v = h == kMissPrim ? 1 : 0;
+            }
+            P.q.vis[item] = v;
         }
     }
+    if (STATS) warpStats(tc, &P.q.ctr->statNodesS, &P.q.ctr->statTrisS);
 }
 
 template <bool DL>
@@ -471,17 +512,17 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
     }
 }
 
-template <bool DL, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock, 8) kShadow(Params P, int cur)
+// Radiance of visible shadow rays, then completion of paths whose last
+// vertex had a shadow ray (shadow miss, optix.cu:265-284).
+template <bool DL>
+__global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
 {
-    __shared__ uint2 stack[kStackDepth * kTraceBlock];
     const WaveParams wp  = *P.wp;
     const uint32_t   n   = loadCount(&P.q.ctr->shadowCount);
     const int        nxt = cur ^ 1;
-    TraceCounters    tc{0u, 0u};
     for (;;)
     {
-        uint32_t base = warpFetch(&P.q.ctr->fetchShadow);
+        uint32_t base = warpFetch(&P.q.ctr->fetchResolve);
         if (base >= n) break;
         uint32_t i      = base + laneId();
         bool     finish = false;
@@ -489,50 +530,17 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kShadow(Params P, int cur)
         f3       L{0, 0, 0};
         if (i < n)
         {
-            float4   o4  = P.q.sqO[i];
-            uint32_t tag = __float_as_uint(o4.w);
+            uint32_t tag = __float_as_uint(P.q.sqO[i].w);
             slot         = tag & ~kLastFlag;
-            f3       o{o4.x, o4.y, o4.z};
             L            = ld3(P.q.psL[slot]);
-            float4 d4    = P.q.sqD[i];
-            if (d4.w != 0.0f)
-            {
-                float t, b1, b2;
-                uint32_t h = traverse<true, STATS>(P.sc.bvh, o, ld3(d4), kRayEps, FLT_MAX, &t, &b1, &b2,
-                                                   stack + threadIdx.x, &tc, &P.q.ctr->error);
-                if (h == kMissPrim) L = L + ld3(P.q.sqL[i]);
-            }
-            if (DL)
-            {
-                float4 e4 = P.q.sqD2[i];
-                if (e4.w != 0.0f)
-                {
-                    float t, b1, b2;
-                    uint32_t h = traverse<true, STATS>(P.sc.bvh, o, ld3(e4), kRayEps, FLT_MAX, &t, &b1, &b2,
-                                                       stack + threadIdx.x, &tc, &P.q.ctr->error);
-                    if (h == kMissPrim) L = L + ld3(P.q.sqL2[i]);
-                }
-            }
+            if (P.q.vis[DL ? 2 * i : i]) L = L + ld3(P.q.sqL[i]);
+            if (DL && P.q.vis[2 * i + 1]) L = L + ld3(P.q.sqL2[i]);
             if (tag & kLastFlag)
                 finish = true;
             else
                 P.q.psL[slot] = make_float4(L.x, L.y, L.z, 0.0f);
         }
         finishPaths(P, wp, nxt, finish, slot, L);
-    }
-    if (STATS)
-    {
-        unsigned long long a = tc.nodes, b = tc.tris;
-        for (int o = 16; o > 0; o >>= 1)
-        {
-            a += __shfl_xor_sync(kFull, a, o);
-            b += __shfl_xor_sync(kFull, b, o);
-        }
-        if (laneId() == 0)
-        {
-            atomicAdd(&P.q.ctr->statNodesS, a);
-            atomicAdd(&P.q.ctr->statTrisS, b);
-        }
     }
 }
 
@@ -555,6 +563,7 @@ __global__ void kAdvance(Counters* c, int cur)
     c->fetchTrace    = 0u;
     c->fetchShade    = 0u;
     c->fetchShadow   = 0u;
+    c->fetchResolve  = 0u;
 }
 
 __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const float4* __restrict__ O,
@@ -641,7 +650,7 @@ cl_status Integrator::init(std::string* err)
             err);
     shadeBlocks_ = std::max(1, b) * numSMs_;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &b, dl ? (const void*)kShadow<true, false> : (const void*)kShadow<false, false>, kTraceBlock, 0),
+                &b, dl ? (const void*)kShadowResolve<true> : (const void*)kShadowResolve<false>, 128, 0),
             err);
     shadowBlocks_ = std::max(1, b) * numSMs_;
     CL_TRY(ctr_.alloc(sizeof(Counters), err));
@@ -965,6 +974,7 @@ cl_status Integrator::ensureQueues(std::string* err)
         CL_TRY(sqD2_.alloc(s * 16, err));
         CL_TRY(sqL2_.alloc(s * 16, err));
     }
+    CL_TRY(vis_.alloc(s * 2, err));
     CL_TRY(psInfo_.alloc(s * 16, err));
     CL_TRY(psT_.alloc(s * 16, err));
     CL_TRY(psE_.alloc(s * 16, err));
@@ -999,6 +1009,7 @@ Params Integrator::params() const
     P.q.sqL       = sqL_.as<float4>();
     P.q.sqD2      = sqD2_.as<float4>();
     P.q.sqL2      = sqL2_.as<float4>();
+    P.q.vis       = vis_.as<uint8_t>();
     P.q.psInfo    = psInfo_.as<uint4>();
     P.q.psT       = psT_.as<float4>();
     P.q.psE       = psE_.as<float4>();
@@ -1032,13 +1043,17 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
         kShade<false><<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
     if (profile) CL_CUDA(cudaEventRecord(evS_[2], stream_), err);
     if (dl && st)
-        kShadow<true, true><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+        kTraceShadow<true, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
     else if (dl)
-        kShadow<true, false><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+        kTraceShadow<true, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
     else if (st)
-        kShadow<false, true><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+        kTraceShadow<false, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
     else
-        kShadow<false, false><<<shadowBlocks_, kTraceBlock, 0, stream_>>>(P, cur);
+        kTraceShadow<false, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
+    if (dl)
+        kShadowResolve<true><<<shadowBlocks_, 128, 0, stream_>>>(P, cur);
+    else
+        kShadowResolve<false><<<shadowBlocks_, 128, 0, stream_>>>(P, cur);
     if (profile) CL_CUDA(cudaEventRecord(evS_[3], stream_), err);
     kAdvance<<<1, 32, 0, stream_>>>(c, cur);
     CL_CUDA(cudaGetLastError(), err);

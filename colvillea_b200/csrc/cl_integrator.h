@@ -42,9 +42,8 @@ struct Counters
 {
     uint32_t           rayCount[2];
     uint32_t           shadowCount;
-    uint32_t           fetchTrace, fetchShade, fetchShadow;
+    uint32_t           fetchTrace, fetchShade, fetchShadow, fetchResolve;
     uint32_t           error;
-    uint32_t           pad;
     unsigned long long pathNext;
     unsigned long long raysClosest, raysShadow;
     unsigned long long statNodes, statTris;
@@ -62,6 +61,7 @@ struct QueueDev
     float4*   sqL;  // {Li.xyz, -}
     float4*   sqD2; // direct lighting: second (BSDF-sampled) shadow ray {d.xyz, valid}
     float4*   sqL2;
+    uint8_t*  vis;    // shadow ray visibility (1 = reaches the light), 2 per entry
     uint4*    psInfo; // {pixel, frame, depth | rngCounter << 8, -}
     float4*   psT;    // throughput
     float4*   psE;    // escape weight (compat) / BSDF pdf in .x
@@ -146,7 +146,7 @@ private:
     // Film and wavefront state.
     DevBuf film_, film64_;
     DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
-    DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_;
+    DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_, vis_;
     uint32_t slots_ = 0, shadowCap_ = 0;
     WaveParams* hostWp_ = nullptr;   // pinned
     uint32_t*   hostCount_ = nullptr; // pinned

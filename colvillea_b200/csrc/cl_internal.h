@@ -71,7 +71,7 @@ struct WideBvh
 {
     DevBuf   nodes; // 5 uint4 per node
     DevBuf   tris;  // 3 float4 per triangle, leaf order
-    uint32_t numNodes = 0, depth = 0, numTris = 0;
+    uint32_t numNodes = 0, depth = 0, numTris = 0, buildIterations = 0;
     void     release()
     {
         nodes.release();

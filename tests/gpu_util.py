@@ -68,12 +68,15 @@ def _finish(name, err, bad_ok, max_ulp, min_frac, max_unexplained_frac):
 
 
 def check_ulp(name, got, ref, max_ulp=4, min_frac=0.999, ref64=None, other=None, ill=None, slack=8.0,
-              rel_ok=None, max_unexplained_frac=5e-4):
-    """Scalars.  rel_ok: outliers within this relative error of `ref` count as explained."""
+              rel_ok=None, max_unexplained_frac=5e-4, cond_ulp=None):
+    """Scalars.  rel_ok: outliers within this relative error of `ref` count as
+    explained; cond_ulp: per-value error bound (ulps) from the conditioning."""
     got = np.asarray(got, np.float32).ravel()
     ref = np.asarray(ref, np.float32).ravel()
     err = ulp_diff(got, ref).astype(np.float64)
     ok = np.zeros(len(err), bool)
+    if cond_ulp is not None:
+        ok |= err <= np.asarray(cond_ulp, np.float64).ravel()
     if ref64 is not None:
         r64 = np.asarray(ref64, np.float64).ravel()
         o = (np.asarray(other, np.float32).ravel() if other is not None else ref).astype(np.float64)
