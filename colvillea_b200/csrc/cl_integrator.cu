@@ -233,12 +233,24 @@ __device__ __forceinline__ void warpStats(const TraceCounters& tc, unsigned long
 // consecutive rays at a time (one atomicAdd per warp) and each lane runs its
 // ray to completion.  (Refilling finished lanes mid-warp was measured slower
 // on B200: the per-step warp vote forces reconvergence and raised the
-// instruction count by half.)
-template <bool STATS>
+// instruction count by half.)  CLASSIFY: the finished batch is appended to
+// the four shading-class queues (the hit material's BSDF type, or escaped),
+// so that each shading kernel runs one BSDF per warp.
+struct ClassifyView
+{
+    const uint4* __restrict__ triIdx;
+    const float4* __restrict__ mats;
+    uint32_t* classIdx;
+    uint32_t  cap;
+};
+
+constexpr int kClassEscaped = 3;
+
+template <bool STATS, bool CLASSIFY>
 __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
                                                                 const float4* __restrict__ D, const uint32_t* count,
                                                                 uint32_t* fetch, float4* __restrict__ hitOut,
-                                                                Counters* ctr)
+                                                                Counters* ctr, ClassifyView cv)
 {
     __shared__ uint2 stack[kStackDepth * kTraceBlock];
     const uint32_t   n = loadCount(count);
@@ -247,14 +259,34 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
     {
         uint32_t base = warpFetch(fetch);
         if (base >= n) break;
-        uint32_t i = base + laneId();
+        uint32_t i    = base + laneId();
+        uint32_t prim = kMissPrim;
         if (i < n)
         {
-            float4   o = O[i], d = D[i];
-            float    t, b1, b2;
-            uint32_t prim = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                                   stack + threadIdx.x, &tc, &ctr->error);
-            hitOut[i]     = make_float4(t, __uint_as_float(prim), b1, b2);
+            float4 o = O[i], d = D[i];
+            float  t, b1, b2;
+            prim      = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
+                                               stack + threadIdx.x, &tc, &ctr->error);
+            hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
+        }
+        if (CLASSIFY)
+        {
+            int cls = -1;
+            if (i < n)
+                cls = prim == kMissPrim ? kClassEscaped
+                                        : int(__float_as_uint(__ldg(&cv.mats[3 * __ldg(&cv.triIdx[prim]).w].x)));
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                uint32_t k = warpAppend(&ctr->classCount[c], cls == c);
+                if (cls == c)
+                {
+                    if (k < cv.cap)
+                        cv.classIdx[size_t(c) * cv.cap + k] = i;
+                    else
+                        atomicOr(&ctr->error, 8u);
+                }
+            }
         }
     }
     if (STATS) warpStats(tc, &ctr->statNodes, &ctr->statTris);
@@ -293,24 +325,31 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
     if (STATS) warpStats(tc, &P.q.ctr->statNodesS, &P.q.ctr->statTrisS);
 }
 
-template <bool DL>
+// CMP: 1 = the reference's estimator (all CL_COMPAT_* flags), 0 = the
+// corrected one, 2 = a mix read at run time; ALIAS: alias-table dome sampling.
+// MAT: the shading class this launch serves (BSDF type 0-2, or 3 = escaped
+// rays), from the class queues written by kTraceClosest; -1 = every ray of
+// the ray queue.  Specialising keeps each instantiation free of the other
+// modes' and materials' code.
+template <bool DL, int CMP, bool ALIAS, int MAT>
 __global__ void __launch_bounds__(128) kShade(Params P, int cur)
 {
     const WaveParams wp = *P.wp;
     const SceneDev&  sc = P.sc;
-    const uint32_t   n  = loadCount(&P.q.ctr->rayCount[cur]);
+    const uint32_t   n  = MAT < 0 ? loadCount(&P.q.ctr->rayCount[cur]) : loadCount(&P.q.ctr->classCount[MAT < 0 ? 0 : MAT]);
     const int        nxt = cur ^ 1;
-    const bool compatPdf   = wp.flags & CL_COMPAT_PDF;
-    const bool compatFrame = wp.flags & CL_COMPAT_FRAME;
-    const bool compatEsc   = wp.flags & CL_COMPAT_ESCAPE;
-    const bool alias       = wp.flags & CL_DOME_ALIAS;
+    const bool compatPdf   = CMP == 2 ? (wp.flags & CL_COMPAT_PDF) != 0 : CMP == 1;
+    const bool compatFrame = CMP == 2 ? (wp.flags & CL_COMPAT_FRAME) != 0 : CMP == 1;
+    const bool compatEsc   = CMP == 2 ? (wp.flags & CL_COMPAT_ESCAPE) != 0 : CMP == 1;
+    const bool alias       = ALIAS;
     const uint32_t N       = sc.numEmitters;
     for (;;)
     {
-        uint32_t base = warpFetch(&P.q.ctr->fetchShade);
+        uint32_t base = warpFetch(MAT < 0 ? &P.q.ctr->fetchShade : &P.q.ctr->fetchClass[MAT < 0 ? 0 : MAT]);
         if (base >= n) break;
-        uint32_t i = base + laneId();
+        uint32_t i     = base + laneId();
         bool     valid = i < n;
+        if (MAT >= 0 && valid) i = P.q.classIdx[size_t(MAT) * P.q.slots + i];
         bool     pushShadow = false, shadow1 = false, shadow2 = false, pushRay = false, finish = false;
         uint32_t slot = 0u, info2 = 0u;
         f3       L{0, 0, 0}, T{1, 1, 1}, E{0, 0, 0}, pHit{0, 0, 0}, sdir{0, 0, 0}, Li{0, 0, 0}, sdir2{0, 0, 0},
@@ -328,7 +367,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             L             = ld3(P.q.psL[slot]);
             f3       d    = ld3(rd);
             uint32_t prim = __float_as_uint(hh.y);
-            if (prim == kMissPrim)
+            if (MAT == kClassEscaped || (MAT < 0 && prim == kMissPrim))
             {
                 // evaluateEscapedRays (raygeneration.cu:105-136)
                 if (sc.hasDome)
@@ -353,6 +392,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             {
                 HitAttr a    = hitAttributes(sc, prim, hh.z, hh.w);
                 Bsdf    bsdf = loadMaterial(sc.mats, a.material);
+                if (MAT >= 0) bsdf.type = uint32_t(MAT);
                 pHit         = a.p;
                 f3    wo     = -d;
                 f2    u      = rng.next2D();
@@ -564,6 +604,11 @@ __global__ void kAdvance(Counters* c, int cur)
     c->fetchShade    = 0u;
     c->fetchShadow   = 0u;
     c->fetchResolve  = 0u;
+    for (int k = 0; k < 4; ++k)
+    {
+        c->classCount[k] = 0u;
+        c->fetchClass[k] = 0u;
+    }
 }
 
 __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const float4* __restrict__ O,
@@ -601,6 +646,38 @@ __global__ void kAliasSample(DomeView dome, const float2* __restrict__ u, float*
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
+namespace
+{
+using ShadeFn = void (*)(Params, int);
+
+template <bool DL, int MAT> ShadeFn shadeKernelM(uint32_t flags)
+{
+    uint32_t c   = flags & CL_COMPAT_ALL;
+    int      cmp = c == CL_COMPAT_ALL ? 1 : (c == 0u ? 0 : 2);
+    bool     al  = (flags & CL_DOME_ALIAS) != 0u;
+    if (cmp == 1) return al ? kShade<DL, 1, true, MAT> : kShade<DL, 1, false, MAT>;
+    if (cmp == 0) return al ? kShade<DL, 0, true, MAT> : kShade<DL, 0, false, MAT>;
+    return al ? kShade<DL, 2, true, MAT> : kShade<DL, 2, false, MAT>;
+}
+
+// Shading kernel of class `mat` (0-2 BSDF type, 3 escaped rays).
+template <bool DL> ShadeFn shadeKernelT(int mat, uint32_t flags)
+{
+    switch (mat)
+    {
+        case 0: return shadeKernelM<DL, 0>(flags);
+        case 1: return shadeKernelM<DL, 1>(flags);
+        case 2: return shadeKernelM<DL, 2>(flags);
+        default: return shadeKernelM<DL, 3>(flags);
+    }
+}
+
+ShadeFn shadeKernel(bool dl, int mat, uint32_t flags)
+{
+    return dl ? shadeKernelT<true>(mat, flags) : shadeKernelT<false>(mat, flags);
+}
+} // namespace
+
 Integrator::Integrator(cl_integrator_type type, uint32_t w, uint32_t h, const cl_render_config& cfg)
     : type_(type), W_(w), H_(h), cfg_(cfg)
 {
@@ -642,11 +719,10 @@ cl_status Integrator::init(std::string* err)
     CL_CUDA(cudaMallocHost((void**)&hostWp_, sizeof(WaveParams)), err);
     CL_CUDA(cudaMallocHost((void**)&hostCount_, 64), err);
     int b = 0;
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTraceClosest<false>, kTraceBlock, 0), err);
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTraceClosest<false, true>, kTraceBlock, 0), err);
     traceBlocks_ = std::max(1, b) * numSMs_;
     bool dl = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, dl ? (const void*)kShade<true> : (const void*)kShade<false>,
-                                                          128, 0),
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)shadeKernel(dl, 2, cfg_.flags), 128, 0),
             err);
     shadeBlocks_ = std::max(1, b) * numSMs_;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
@@ -975,6 +1051,7 @@ cl_status Integrator::ensureQueues(std::string* err)
         CL_TRY(sqL2_.alloc(s * 16, err));
     }
     CL_TRY(vis_.alloc(s * 2, err));
+    CL_TRY(classIdx_.alloc(s * 4 * 4, err));
     CL_TRY(psInfo_.alloc(s * 16, err));
     CL_TRY(psT_.alloc(s * 16, err));
     CL_TRY(psE_.alloc(s * 16, err));
@@ -983,6 +1060,11 @@ cl_status Integrator::ensureQueues(std::string* err)
     shadowCap_  = slots;
     graphValid_ = false;
     return CL_OK;
+}
+
+ClassifyView Integrator::classifyView() const
+{
+    return ClassifyView{triIdx_.as<const uint4>(), mats_.as<const float4>(), classIdx_.u(), slots_};
 }
 
 Params Integrator::params() const
@@ -1010,6 +1092,7 @@ Params Integrator::params() const
     P.q.sqD2      = sqD2_.as<float4>();
     P.q.sqL2      = sqL2_.as<float4>();
     P.q.vis       = vis_.as<uint8_t>();
+    P.q.classIdx  = classIdx_.u();
     P.q.psInfo    = psInfo_.as<uint4>();
     P.q.psT       = psT_.as<float4>();
     P.q.psE       = psE_.as<float4>();
@@ -1031,16 +1114,13 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     const bool st = cfg_.flags & CL_TRACE_STATS;
     if (profile) CL_CUDA(cudaEventRecord(evS_[0], stream_), err);
     if (st)
-        kTraceClosest<true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur],
-                                                                        &c->rayCount[cur], &c->fetchTrace, P.q.hit, c);
+        kTraceClosest<true, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+            P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur], &c->fetchTrace, P.q.hit, c, classifyView());
     else
-        kTraceClosest<false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur],
-                                                                         &c->rayCount[cur], &c->fetchTrace, P.q.hit, c);
+        kTraceClosest<false, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+            P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur], &c->fetchTrace, P.q.hit, c, classifyView());
     if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
-    if (dl)
-        kShade<true><<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
-    else
-        kShade<false><<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
+    for (int m = 0; m < 4; ++m) shadeKernel(dl, m, cfg_.flags)<<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
     if (profile) CL_CUDA(cudaEventRecord(evS_[2], stream_), err);
     if (dl && st)
         kTraceShadow<true, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
@@ -1315,9 +1395,9 @@ cl_status Integrator::traceRays(const float* rays, uint32_t n, float* t, uint32_
         Counters c0{};
         c0.rayCount[0] = m;
         CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
-        kTraceClosest<false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+        kTraceClosest<false, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
             BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, rqO_[0].as<float4>(),
-            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc);
+            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc, ClassifyView{});
         CL_CUDA(cudaGetLastError(), err);
         CL_CUDA(cudaMemcpyAsync(h.data(), hit_.p, m * 16, cudaMemcpyDeviceToHost, stream_), err);
         Counters ch;
@@ -1407,9 +1487,9 @@ cl_status Integrator::traceStats(const float* rays, uint32_t n, uint64_t* nodes,
         Counters c0{};
         c0.rayCount[0] = m;
         CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
-        kTraceClosest<true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+        kTraceClosest<true, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
             BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, rqO_[0].as<float4>(),
-            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc);
+            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc, ClassifyView{});
         CL_CUDA(cudaGetLastError(), err);
         Counters ch;
         CL_CUDA(cudaMemcpyAsync(&ch, ctr_.p, sizeof(ch), cudaMemcpyDeviceToHost, stream_), err);

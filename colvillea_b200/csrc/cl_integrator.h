@@ -9,6 +9,7 @@
 
 namespace clb
 {
+struct ClassifyView;
 constexpr int      kMaxEmitters = 8;
 constexpr uint32_t kLastFlag    = 0x80000000u; // shadow entry: path ends after this shadow query
 
@@ -44,6 +45,8 @@ struct Counters
     uint32_t           shadowCount;
     uint32_t           fetchTrace, fetchShade, fetchShadow, fetchResolve;
     uint32_t           error;
+    uint32_t           classCount[4]; // per shading class: diffuse, conductor, dielectric, escaped
+    uint32_t           fetchClass[4];
     unsigned long long pathNext;
     unsigned long long raysClosest, raysShadow;
     unsigned long long statNodes, statTris;
@@ -61,6 +64,7 @@ struct QueueDev
     float4*   sqL;  // {Li.xyz, -}
     float4*   sqD2; // direct lighting: second (BSDF-sampled) shadow ray {d.xyz, valid}
     float4*   sqL2;
+    uint32_t* classIdx; // 4 x slots ray-queue indices, sorted by shading class
     uint8_t*  vis;    // shadow ray visibility (1 = reaches the light), 2 per entry
     uint4*    psInfo; // {pixel, frame, depth | rngCounter << 8, -}
     float4*   psT;    // throughput
@@ -115,6 +119,7 @@ private:
     cl_status captureGraph(std::string* err);
     cl_status launchWave(int cur, bool profile, std::string* err);
     Params    params() const;
+    ClassifyView classifyView() const;
 
     cl_integrator_type type_;
     uint32_t           W_, H_;
@@ -146,7 +151,7 @@ private:
     // Film and wavefront state.
     DevBuf film_, film64_;
     DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
-    DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_, vis_;
+    DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_, vis_, classIdx_;
     uint32_t slots_ = 0, shadowCap_ = 0;
     WaveParams* hostWp_ = nullptr;   // pinned
     uint32_t*   hostCount_ = nullptr; // pinned
