@@ -16,7 +16,7 @@ from . import _native as N
 from ._native import ClError
 
 __all__ = ["IntegratorType", "Integrator", "RenderConfig", "ClError", "COMPAT_ALL", "DOME_ALIAS", "FILM_FP64",
-           "PROFILE_STAGES", "TRACE_STATS", "load_scene"]
+           "PROFILE_STAGES", "TRACE_STATS", "load_scene", "GuideConfig", "Guide"]
 
 COMPAT_PDF, COMPAT_FRAME, COMPAT_ESCAPE, COMPAT_ALL = N.CL_COMPAT_PDF, N.CL_COMPAT_FRAME, N.CL_COMPAT_ESCAPE, N.CL_COMPAT_ALL
 DOME_ALIAS, FILM_FP64, PROFILE_STAGES, TRACE_STATS = N.CL_DOME_ALIAS, N.CL_FILM_FP64, N.CL_PROFILE_STAGES, N.CL_TRACE_STATS
@@ -182,6 +182,123 @@ class Integrator:
         d = np.zeros((n, 3), np.float32); p = np.zeros(n, np.float32); v = np.zeros((n, 3), np.float32)
         N.call("cl_dome_alias_sample", self._h, _ptr(u2), _ptr(d), _ptr(p), _ptr(v), n)
         return d, p, v
+
+
+def GuideConfig(**kw):
+    """cl_guide_config with the library's defaults, fields overridden by kw
+    (resolutions: a sequence of 16 level resolutions)."""
+    c = N.GuideConfig()
+    N.lib().cl_guide_default_config(ctypes.byref(c))
+    for k, v in kw.items():
+        if k == "resolutions":
+            for i, r in enumerate(v):
+                c.resolutions[i] = int(r)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def default_resolutions(n_min, n_max):
+    r = np.zeros(16, np.uint32)
+    N.call("cl_guide_default_resolutions", float(n_min), float(n_max), _ptr(r))
+    return r
+
+
+class Guide:
+    """The neural path-guiding network (no counterpart in the reference):
+    hash grid + one-blob encoding, 96-64-64-64-64-48 MLP on the tensor cores,
+    8-lobe vMF mixture head, Adam training."""
+
+    def __init__(self, handle, owned=True):
+        self._h = handle
+        self._owned = owned
+
+    @staticmethod
+    def create(config=None):
+        h = ctypes.c_void_p()
+        cfg = config if config is not None else GuideConfig()
+        N.call("cl_guide_create", ctypes.byref(cfg), ctypes.byref(h))
+        return Guide(h)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._owned:
+            N.lib().cl_guide_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def param_count(self):
+        n = ctypes.c_uint64()
+        N.call("cl_guide_param_count", self._h, ctypes.byref(n))
+        return n.value
+
+    def resolutions(self):
+        r = np.zeros(16, np.uint32)
+        N.call("cl_guide_get_resolutions", self._h, _ptr(r))
+        return r
+
+    def get_params(self):
+        p = np.zeros(self.param_count(), np.float32)
+        N.call("cl_guide_get_params", self._h, _ptr(p), p.size)
+        return p
+
+    def set_params(self, p):
+        p = _f32(p)
+        N.call("cl_guide_set_params", self._h, _ptr(p), p.size)
+
+    def forward(self, in9):
+        in9 = _f32(in9)
+        out = np.zeros((len(in9), 48), np.float32)
+        N.call("cl_guide_forward", self._h, _ptr(in9), len(in9), _ptr(out))
+        return out
+
+    def gradient(self, rec13):
+        rec13 = _f32(rec13)
+        g = np.zeros(self.param_count(), np.float32)
+        loss = ctypes.c_double()
+        N.call("cl_guide_gradient", self._h, _ptr(rec13), len(rec13), ctypes.byref(loss), _ptr(g))
+        return loss.value, g
+
+    def train_step(self, rec13):
+        rec13 = _f32(rec13)
+        loss = ctypes.c_double()
+        N.call("cl_guide_train_step", self._h, _ptr(rec13), len(rec13), ctypes.byref(loss))
+        return loss.value
+
+    def sample(self, in9, u3):
+        in9, u3 = _f32(in9), _f32(u3)
+        d = np.zeros((len(in9), 3), np.float32); p = np.zeros(len(in9), np.float32)
+        N.call("cl_guide_sample", self._h, _ptr(in9), _ptr(u3), len(in9), _ptr(d), _ptr(p))
+        return d, p
+
+    def pdf(self, in9, dirs):
+        in9, dirs = _f32(in9), _f32(dirs)
+        p = np.zeros(len(in9), np.float32)
+        N.call("cl_guide_pdf", self._h, _ptr(in9), _ptr(dirs), len(in9), _ptr(p))
+        return p
+
+
+def _set_guiding(self, config):
+    """Guided path tracing with a fresh network (None: off)."""
+    N.call("cl_integrator_set_guiding", self._h, ctypes.byref(config) if config is not None else None)
+
+
+def _guide(self):
+    h = ctypes.c_void_p()
+    N.call("cl_integrator_get_guide", self._h, ctypes.byref(h))
+    return Guide(h, owned=False) if h.value else None
+
+
+def _guide_stats(self):
+    s = N.GuideStats()
+    N.call("cl_integrator_guide_stats", self._h, ctypes.byref(s))
+    return s.as_dict()
+
+
+Integrator.setGuiding = _set_guiding
+Integrator.guide = _guide
+Integrator.guideStats = _guide_stats
 
 
 def load_scene(scene, itype=IntegratorType.WavefrontPathTracing, flags=COMPAT_ALL, max_depth=None, rr_start=None,

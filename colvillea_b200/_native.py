@@ -70,7 +70,23 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-# name -> (restype, argtypes)
+class GuideConfig(ctypes.Structure):
+    _fields_ = [("log2_table", u32), ("resolutions", u32 * 16), ("n_min", ctypes.c_float), ("n_max", ctypes.c_float),
+                ("learning_rate", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
+                ("epsilon", ctypes.c_float), ("bsdf_fraction", ctypes.c_float), ("batch", u32),
+                ("train_spp", u32), ("class_mask", u32), ("seed", u32)]
+
+
+class GuideStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_uint64), ("samples_trained", ctypes.c_uint64), ("records_last", ctypes.c_uint64),
+                ("inferred", ctypes.c_uint64), ("last_loss", ctypes.c_double), ("ms_train", ctypes.c_float),
+                ("ms_infer", ctypes.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# name -> argtypes (every entry point returns cl_status unless listed in _VOID)
 _SIGS = {
     "cl_integrator_create": [u32, u32, u32, ctypes.POINTER(RenderConfig), ctypes.POINTER(vp)],
     "cl_integrator_destroy": [vp],
@@ -108,7 +124,24 @@ _SIGS = {
     "cl_unit_dome_pdf_eval": [vp, u32, u32, vp, vp, vp, vp, vp, u32],
     "cl_unit_directional_sample": [vp, vp, vp, vp, vp, u32],
     "cl_dome_build_tables_noalloc": [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp],
+    "cl_guide_default_config": [ctypes.POINTER(GuideConfig)],
+    "cl_guide_default_resolutions": [ctypes.c_float, ctypes.c_float, vp],
+    "cl_guide_create": [ctypes.POINTER(GuideConfig), ctypes.POINTER(vp)],
+    "cl_guide_destroy": [vp],
+    "cl_guide_param_count": [vp, ctypes.POINTER(ctypes.c_uint64)],
+    "cl_guide_get_resolutions": [vp, vp],
+    "cl_guide_set_params": [vp, vp, ctypes.c_uint64],
+    "cl_guide_get_params": [vp, vp, ctypes.c_uint64],
+    "cl_guide_forward": [vp, vp, u32, vp],
+    "cl_guide_gradient": [vp, vp, u32, ctypes.POINTER(ctypes.c_double), vp],
+    "cl_guide_train_step": [vp, vp, u32, ctypes.POINTER(ctypes.c_double)],
+    "cl_guide_sample": [vp, vp, vp, u32, vp, vp],
+    "cl_guide_pdf": [vp, vp, vp, u32, vp],
+    "cl_integrator_set_guiding": [vp, ctypes.POINTER(GuideConfig)],
+    "cl_integrator_get_guide": [vp, ctypes.POINTER(vp)],
+    "cl_integrator_guide_stats": [vp, ctypes.POINTER(GuideStats)],
 }
+_VOID = {"cl_guide_default_config"}
 
 _lib = None
 
@@ -129,7 +162,7 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         for name, args in _SIGS.items():
             f = getattr(L, name)
-            f.restype = ctypes.c_int32
+            f.restype = None if name in _VOID else ctypes.c_int32
             f.argtypes = args
         _lib = L
     return _lib

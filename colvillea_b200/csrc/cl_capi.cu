@@ -4,11 +4,27 @@
 // src/core/devices/cudacommon.h:13-26).
 #include "cl_integrator.h"
 
+#include <memory>
 #include <new>
+
+// A guiding network: standalone (own network and stream) or the network of
+// an integrator (borrowed, on the integrator's stream).
+struct cl_guide
+{
+    clb::GuideNet*                 net = nullptr;
+    std::unique_ptr<clb::GuideNet> own;
+    cudaStream_t                   stream = nullptr;
+    ~cl_guide()
+    {
+        own.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
 
 struct cl_integrator
 {
     clb::Integrator impl;
+    cl_guide        guideView; // borrowed view of impl's network
     cl_integrator(cl_integrator_type t, uint32_t w, uint32_t h, const cl_render_config& c) : impl(t, w, h, c) {}
 };
 
@@ -316,6 +332,140 @@ cl_status cl_unit_directional_sample(const float* params7, const float* u2, floa
                                      uint32_t count)
 {
     return guarded([&](std::string* e) { return clb::unitDirectional(params7, u2, dir, pdf, value, count, e); });
+}
+
+// ---- Neural path guiding ----
+void cl_guide_default_config(cl_guide_config* config)
+{
+    if (config) clb::guideDefaultConfig(config);
+}
+
+cl_status cl_guide_default_resolutions(float n_min, float n_max, uint32_t* resolutions16)
+{
+    CL_NEED(resolutions16);
+    cl_status s = clb::guideResolutions(n_min, n_max, resolutions16);
+    if (s != CL_OK) clb::setLastError("n_min/n_max out of range");
+    return s;
+}
+
+cl_status cl_guide_create(const cl_guide_config* config, cl_guide** out)
+{
+    CL_NEED(config);
+    CL_NEED(out);
+    *out = nullptr;
+    return guarded([&](std::string* e) -> cl_status {
+        std::unique_ptr<cl_guide> g(new cl_guide());
+        if (cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            g->stream = nullptr;
+            cudaGetLastError();
+            *e = "cudaStreamCreate failed";
+            return CL_ERR_CUDA;
+        }
+        g->own.reset(new clb::GuideNet(*config));
+        g->net = g->own.get();
+        CL_TRY(g->net->init(g->stream, e));
+        *out = g.release();
+        return CL_OK;
+    });
+}
+
+cl_status cl_guide_destroy(cl_guide* guide)
+{
+    if (guide && !guide->own)
+    {
+        clb::setLastError("an integrator's network is destroyed with the integrator");
+        return CL_ERR_INVALID_ARG;
+    }
+    delete guide;
+    return CL_OK;
+}
+
+cl_status cl_guide_param_count(const cl_guide* guide, uint64_t* count)
+{
+    CL_NEED(guide);
+    CL_NEED(count);
+    *count = guide->net->paramCount();
+    return CL_OK;
+}
+
+cl_status cl_guide_get_resolutions(const cl_guide* guide, uint32_t* resolutions16)
+{
+    CL_NEED(guide);
+    CL_NEED(resolutions16);
+    for (int l = 0; l < CL_GUIDE_LEVELS; ++l) resolutions16[l] = guide->net->resolutions()[l];
+    return CL_OK;
+}
+
+cl_status cl_guide_set_params(cl_guide* guide, const float* params, uint64_t count)
+{
+    CL_NEED(guide);
+    return guarded([&](std::string* e) { return guide->net->setParams(params, count, e); });
+}
+
+cl_status cl_guide_get_params(const cl_guide* guide, float* params, uint64_t count)
+{
+    CL_NEED(guide);
+    return guarded([&](std::string* e) { return guide->net->getParams(params, count, e); });
+}
+
+cl_status cl_guide_forward(cl_guide* guide, const float* in9, uint32_t count, float* out48)
+{
+    CL_NEED(guide);
+    return guarded([&](std::string* e) { return guide->net->forward(in9, count, out48, e); });
+}
+
+cl_status cl_guide_gradient(cl_guide* guide, const float* rec13, uint32_t count, double* loss, float* grad)
+{
+    CL_NEED(guide);
+    return guarded([&](std::string* e) { return guide->net->gradient(rec13, count, loss, grad, e); });
+}
+
+cl_status cl_guide_train_step(cl_guide* guide, const float* rec13, uint32_t count, double* loss)
+{
+    CL_NEED(guide);
+    return guarded([&](std::string* e) { return guide->net->trainStepHost(rec13, count, loss, e); });
+}
+
+cl_status cl_guide_sample(cl_guide* guide, const float* in9, const float* u3, uint32_t count, float* dir3, float* pdf)
+{
+    CL_NEED(guide);
+    return guarded([&](std::string* e) { return guide->net->sample(in9, u3, count, dir3, pdf, e); });
+}
+
+cl_status cl_guide_pdf(cl_guide* guide, const float* in9, const float* dir3, uint32_t count, float* pdf)
+{
+    CL_NEED(guide);
+    return guarded([&](std::string* e) { return guide->net->pdf(in9, dir3, count, pdf, e); });
+}
+
+cl_status cl_integrator_set_guiding(cl_integrator* it, const cl_guide_config* config)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.setGuiding(config, e); });
+}
+
+cl_status cl_integrator_get_guide(cl_integrator* it, cl_guide** guide)
+{
+    CL_NEED(it);
+    CL_NEED(guide);
+    clb::GuideNet* net = it->impl.guideNet();
+    if (!net)
+    {
+        *guide = nullptr;
+        return CL_OK;
+    }
+    it->guideView.net    = net;
+    it->guideView.stream = nullptr;
+    *guide               = &it->guideView;
+    return CL_OK;
+}
+
+cl_status cl_integrator_guide_stats(cl_integrator* it, cl_guide_stats* stats)
+{
+    CL_NEED(it);
+    CL_NEED(stats);
+    return guarded([&](std::string* e) { return it->impl.guideStats(stats, e); });
 }
 
 } // extern "C"

@@ -1,0 +1,901 @@
+// Guiding network kernels: parameter initialisation, fragment-ordered weight
+// copies, inference, the fused training forward/backward pass, the
+// weight-gradient reduction over the batch, and Adam.  No counterpart in the
+// reference renderer.
+#include "cl_guide.h"
+
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <vector>
+
+namespace clb
+{
+using namespace guide;
+
+namespace
+{
+constexpr int kInferWarps = 8;  // inference: 8 warps x 32 samples per CTA pass
+constexpr int kTrainWarps = 4;  // training forward/backward: 4 warps x 16 samples
+constexpr int kGradChunk  = 4096; // samples per weight-gradient block
+constexpr int kGradStep   = 64;   // samples staged in shared memory per step
+constexpr int kXTile      = 32 * kXS * 2; // bytes of a 32-row encoded tile (6656)
+
+__device__ __forceinline__ uint32_t laneIdx() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    // splitmix64 finaliser
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ float uniformPM1(uint64_t seed, uint64_t i)
+{
+    uint64_t h = mix64(seed * 0x9e3779b97f4a7c15ull + i + 1);
+    return float(int64_t(h >> 40) - (int64_t(1) << 23)) * (1.0f / float(1 << 23)); // [-1, 1)
+}
+
+// Hash entries U[-1e-4, 1e-4]; W_l Glorot-uniform sqrt(6 / (in + out)).
+__global__ void kInitParams(float* p, uint64_t hashN, uint32_t seed)
+{
+    uint64_t n = hashN + kMlpParams;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    {
+        float u = uniformPM1(seed, i);
+        if (i < hashN)
+            p[i] = 1e-4f * u;
+        else
+        {
+            int o = int(i - hashN), l = 0;
+            while (l < kLayers - 1 && o >= weightOffset(l + 1)) ++l;
+            p[i] = u * sqrtf(6.0f / float(layerIn(l) + layerOut(l)));
+        }
+    }
+}
+
+__global__ void kTableCopy(const float* __restrict__ p, __nv_bfloat16* __restrict__ t, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        t[i] = __float2bfloat16_rn(p[i]);
+}
+
+// Fragment-ordered bf16 weights.  Forward fragment (kt, nt) of layer l, lane
+// (g, t): b0 = W[8nt+g][16kt+2t .. +1], b1 = W[8nt+g][16kt+2t+8 .. +9].
+// Backward fragment (kt over outputs, nt over inputs): b0 = W[16kt+2t][8nt+g],
+// W[16kt+2t+1][8nt+g]; b1 the same 8 rows further down.
+__global__ void kFrags(const float* __restrict__ mlp, uint2* __restrict__ wf, uint2* __restrict__ wb)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < kFwdFrags * 32)
+    {
+        int f = e >> 5, lane = e & 31, l = 0;
+        while (l < kLayers - 1 && f >= fwdFragOffset(l + 1)) ++l;
+        int          loc = f - fwdFragOffset(l), kt = loc / fwdNT(l), nt = loc % fwdNT(l);
+        int          g = lane >> 2, t = lane & 3, K = layerIn(l);
+        const float* W   = mlp + weightOffset(l) + (nt * 8 + g) * K + kt * 16 + 2 * t;
+        wf[e]            = make_uint2(packBf16(W[0], W[1]), packBf16(W[8], W[9]));
+        return;
+    }
+    e -= kFwdFrags * 32;
+    if (e < kBwdFrags * 32)
+    {
+        int f = e >> 5, lane = e & 31, l = 0;
+        while (l < kLayers - 1 && f >= bwdFragOffset(l + 1)) ++l;
+        int          loc = f - bwdFragOffset(l), kt = loc / bwdNT(l), nt = loc % bwdNT(l);
+        int          g = lane >> 2, t = lane & 3, K = layerIn(l);
+        const float* W   = mlp + weightOffset(l) + (kt * 16 + 2 * t) * K + nt * 8 + g;
+        wb[e]            = make_uint2(packBf16(W[0], W[K]), packBf16(W[8 * K], W[9 * K]));
+    }
+}
+
+__device__ __forceinline__ void loadFrags(uint2* dst, const uint2* __restrict__ src, int count)
+{
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+    uint4*       d = reinterpret_cast<uint4*>(dst);
+    for (int i = threadIdx.x; i < count / 2; i += blockDim.x) d[i] = __ldg(s + i);
+}
+
+__device__ __forceinline__ f3 ldf3(const float* p) { return {p[0], p[1], p[2]}; }
+
+// Forward pass of `n` host-given samples (in9 rows) -> raw head outputs.
+__global__ void __launch_bounds__(kInferWarps * 32) kInferUnit(GridView g, const uint2* __restrict__ wfG,
+                                                                const float* __restrict__ in9, uint32_t n,
+                                                                float* __restrict__ out48)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2*         wf   = reinterpret_cast<uint2*>(smem);
+    const uint32_t lane = laneIdx(), warp = threadIdx.x >> 5;
+    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + kFwdFragBytes + warp * kXTile);
+    loadFrags(wf, wfG, kFwdFrags * 32);
+    __syncthreads();
+    for (uint32_t base = (blockIdx.x * kInferWarps + warp) * 32u; base < n; base += gridDim.x * kInferWarps * 32u)
+    {
+        uint32_t i = base + lane;
+        if (i < n)
+        {
+            const float* r = in9 + 9 * size_t(i);
+            encodeRow(g, ldf3(r), ldf3(r + 3), ldf3(r + 6), x + lane * kXS);
+        }
+        else
+            zeroRow(x + lane * kXS);
+        __syncwarp();
+        float out[2][6][4];
+        mlpInfer<2>(wf, x, lane, out);
+        __syncwarp();
+        float* o = reinterpret_cast<float*>(x);
+        storeOut<2>(out, o, lane);
+        __syncwarp();
+        if (i < n)
+            for (int c = 0; c < kOut; ++c) out48[size_t(i) * kOut + c] = o[lane * kOS + c];
+        __syncwarp();
+    }
+}
+
+// Mixture sample / pdf of given head outputs.
+__global__ void kSampleUnit(const float* __restrict__ out48, const float* __restrict__ u3, uint32_t n,
+                            float* __restrict__ dir, float* __restrict__ pdf)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Lobes L;
+    headLobes(out48 + size_t(i) * kOut, &L);
+    f3 d         = mixtureSample(L, u3[3 * i], u3[3 * i + 1], u3[3 * i + 2]);
+    dir[3 * i]     = d.x;
+    dir[3 * i + 1] = d.y;
+    dir[3 * i + 2] = d.z;
+    pdf[i]         = mixturePdf(L, d);
+}
+__global__ void kPdfUnit(const float* __restrict__ out48, const float* __restrict__ dir, uint32_t n,
+                         float* __restrict__ pdf)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Lobes L;
+    headLobes(out48 + size_t(i) * kOut, &L);
+    pdf[i] = mixturePdf(L, f3{dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]});
+}
+
+// ---------------------------------------------------------------------------
+// Training
+// ---------------------------------------------------------------------------
+struct TrainArgs
+{
+    const float4* __restrict__ rec;
+    const uint32_t* count;
+    uint32_t        batch;
+    GridView        g;
+    const uint2* __restrict__ wf;
+    const uint2* __restrict__ wb;
+    float2*        gradTable;
+    __nv_bfloat16* acts;
+    __nv_bfloat16* deltas;
+    double*        scal; // [0] sum of weights, [1] loss
+};
+
+// A step trains on B = min(count, batch) samples; when more records were
+// collected, sample j takes record floor(j * count / B) (an even subsample).
+__device__ __forceinline__ uint32_t recordOf(uint32_t j, uint32_t count, uint32_t nB)
+{
+    return count > nB ? uint32_t(uint64_t(j) * count / nB) : j;
+}
+
+__global__ void kTrainPrep(TrainArgs a)
+{
+    __shared__ double part[32];
+    const uint32_t count = *a.count, nB = min(count, a.batch);
+    double         s     = 0.0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nB; j += gridDim.x * blockDim.x)
+        s += double(a.rec[kRecordF4 * size_t(recordOf(j, count, nB))].w);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (laneIdx() == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double t = 0.0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) t += part[w];
+        if (t != 0.0) atomicAdd(&a.scal[0], t);
+    }
+}
+
+// log p(omega) of the mixture given by the head outputs o[0..47], and its
+// gradient with respect to o (grad[40..47] = 0: unused outputs).
+__device__ __forceinline__ float headLossGrad(const float* o, f3 om, float* grad)
+{
+    float mx = -FLT_MAX;
+#pragma unroll
+    for (int k = 0; k < kLobes; ++k) mx = fmaxf(mx, o[5 * k + 4]);
+    float e[kLobes], S = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kLobes; ++k)
+    {
+        e[k] = expf(o[5 * k + 4] - mx);
+        S += e[k];
+    }
+    const float logS = logf(S);
+    float       lp[kLobes], kap[kLobes], c[kLobes], nrm[kLobes];
+    f3          mu[kLobes];
+    float       m = -FLT_MAX;
+#pragma unroll
+    for (int k = 0; k < kLobes; ++k)
+    {
+        f3 raw{o[5 * k], o[5 * k + 1], o[5 * k + 2]};
+        nrm[k]   = fmaxf(sqrtf(dot(raw, raw)), 1e-6f);
+        mu[k]    = raw * (1.0f / nrm[k]);
+        float lk = fminf(fmaxf(o[5 * k + 3], kKappaMin), kKappaMax);
+        kap[k]   = expf(lk);
+        c[k]     = dot(mu[k], om);
+        lp[k]    = (o[5 * k + 4] - mx - logS) + lk - logf(2.0f * kPiF) - logf(-expm1f(-2.0f * kap[k])) +
+                kap[k] * (c[k] - 1.0f);
+        m = fmaxf(m, lp[k]);
+    }
+    float R = 0.0f, r[kLobes];
+#pragma unroll
+    for (int k = 0; k < kLobes; ++k)
+    {
+        r[k] = expf(lp[k] - m);
+        R += r[k];
+    }
+    const float invR = 1.0f / R;
+#pragma unroll
+    for (int k = 0; k < kLobes; ++k)
+    {
+        float rk       = r[k] * invR;
+        grad[5 * k + 4] = rk - e[k] / S;
+        float lkr      = o[5 * k + 3];
+        float dlk      = 1.0f / kap[k] - 2.0f * expf(-2.0f * kap[k]) / -expm1f(-2.0f * kap[k]) + (c[k] - 1.0f);
+        grad[5 * k + 3] = (lkr > kKappaMin && lkr < kKappaMax) ? rk * dlk * kap[k] : 0.0f;
+        f3    dm       = om * kap[k];
+        float pr       = dot(dm, mu[k]);
+        f3    proj     = dm - mu[k] * pr;
+        float sc       = rk / nrm[k];
+        grad[5 * k]     = proj.x * sc;
+        grad[5 * k + 1] = proj.y * sc;
+        grad[5 * k + 2] = proj.z * sc;
+    }
+#pragma unroll
+    for (int k = 5 * kLobes; k < kOut; ++k) grad[k] = 0.0f;
+    return m + logf(R);
+}
+
+// A fragments (k-tiles kt < KT) of a 16-row tile -> bf16 rows of a staging
+// matrix (row stride ld, starting at column 0 of `base`), rows < valid.
+template <int KT>
+__device__ __forceinline__ void storeA(const uint32_t (&a)[4][4], __nv_bfloat16* base, int ld, uint32_t rows,
+                                       uint32_t lane)
+{
+    const uint32_t g = lane >> 2, t = lane & 3u;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt)
+    {
+        if (g < rows)
+        {
+            __nv_bfloat16* p = base + size_t(g) * ld + kt * 16 + 2 * t;
+            *reinterpret_cast<uint32_t*>(p)     = a[kt][0];
+            *reinterpret_cast<uint32_t*>(p + 8) = a[kt][2];
+        }
+        if (g + 8 < rows)
+        {
+            __nv_bfloat16* p = base + size_t(g + 8) * ld + kt * 16 + 2 * t;
+            *reinterpret_cast<uint32_t*>(p)     = a[kt][1];
+            *reinterpret_cast<uint32_t*>(p + 8) = a[kt][3];
+        }
+    }
+}
+
+// Backward through a layer with 64 inputs: d (KT k-tiles over the layer's
+// outputs) times W, masked by the ReLU of the layer's input (its A fragments
+// hPrev: a zero bf16 means the unit was off), rounded to bf16 -> the output
+// gradient of the layer below, as A fragments.
+template <int KT>
+__device__ __forceinline__ void backHidden(const uint2* __restrict__ wbL, const uint32_t (&d)[4][4],
+                                           const uint32_t (&hPrev)[4][4], uint32_t (&dOut)[4][4], uint32_t lane)
+{
+    float acc[8][4];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt)
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+        {
+            uint2 b = wbL[(kt * 8 + nt) * 32 + lane];
+            mma16816(acc[nt], d[kt], b.x, b.y);
+        }
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+    {
+        const uint32_t lo = hPrev[nt >> 1][(nt & 1) ? 2 : 0], hi = hPrev[nt >> 1][(nt & 1) ? 3 : 1];
+        if (!(lo & 0xffffu)) acc[nt][0] = 0.0f;
+        if (!(lo >> 16)) acc[nt][1] = 0.0f;
+        if (!(hi & 0xffffu)) acc[nt][2] = 0.0f;
+        if (!(hi >> 16)) acc[nt][3] = 0.0f;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        dOut[j][0] = packBf16(acc[2 * j][0], acc[2 * j][1]);
+        dOut[j][1] = packBf16(acc[2 * j][2], acc[2 * j][3]);
+        dOut[j][2] = packBf16(acc[2 * j + 1][0], acc[2 * j + 1][1]);
+        dOut[j][3] = packBf16(acc[2 * j + 1][2], acc[2 * j + 1][3]);
+    }
+}
+
+constexpr int kTrainXBytes    = 16 * kXS * 2;                // 3328: encoded inputs, then head outputs
+constexpr int kTrainDBytes    = 16 * kDS * 2;                // 1792: head-output gradients
+constexpr int kTrainWarpBytes = kTrainXBytes + kTrainDBytes + 16 * 3 * 4;
+constexpr int kTrainSmem      = kFwdFragBytes + kBwdFragBytes + kTrainWarps * kTrainWarpBytes;
+static_assert(16 * kOS * 4 <= kTrainXBytes, "output tile must fit in the input tile");
+static_assert(kTrainWarpBytes % 16 == 0, "warp staging must stay 16-byte aligned");
+
+// Forward and backward pass of the training batch, 16 samples per warp tile:
+// encodes, runs the MLP keeping every layer's input in registers, writes the
+// inputs and the back-propagated output gradients of every layer (bf16) for
+// the weight-gradient reduction, accumulates the loss, and scatters the
+// input gradient of the hash features to the table gradient (float2 atomics).
+__global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2*         wf   = reinterpret_cast<uint2*>(smem);
+    uint2*         wb   = reinterpret_cast<uint2*>(smem + kFwdFragBytes);
+    const uint32_t lane = laneIdx(), warp = threadIdx.x >> 5;
+    unsigned char* ws   = smem + kFwdFragBytes + kBwdFragBytes + warp * kTrainWarpBytes;
+    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(ws);
+    __nv_bfloat16* dT   = reinterpret_cast<__nv_bfloat16*>(ws + kTrainXBytes);
+    float*         posS = reinterpret_cast<float*>(ws + kTrainXBytes + kTrainDBytes);
+    loadFrags(wf, a.wf, kFwdFrags * 32);
+    loadFrags(wb, a.wb, kBwdFrags * 32);
+    __syncthreads();
+    const uint32_t count = *a.count, nB = min(count, a.batch);
+    const double   wsum  = a.scal[0];
+    const float    invW  = wsum > 0.0 ? float(1.0 / wsum) : 0.0f;
+    const uint32_t g = lane >> 2, t = lane & 3u, r = lane & 15u, half = lane >> 4;
+    for (uint32_t tile = blockIdx.x * kTrainWarps + warp; tile * 16u < nB; tile += gridDim.x * kTrainWarps)
+    {
+        const uint32_t j0 = tile * 16u, rows = min(16u, nB - j0), j = j0 + r;
+        const bool     valid = r < rows;
+        __nv_bfloat16* row   = x + r * kXS;
+        const float4*  R     = a.rec + kRecordF4 * size_t(recordOf(valid ? j : j0, count, nB));
+        if (valid)
+        {
+            float4 r0 = R[0], rd = R[1 + half];
+            f3     p  = clampUnit(f3{r0.x, r0.y, r0.z});
+            if (half == 0)
+            {
+                posS[3 * r]     = p.x;
+                posS[3 * r + 1] = p.y;
+                posS[3 * r + 2] = p.z;
+            }
+#pragma unroll 2
+            for (int l = int(half) * 8; l < int(half) * 8 + 8; ++l)
+            {
+                float2 f = encodeLevel(a.g, l, p);
+                *reinterpret_cast<__nv_bfloat162*>(row + 2 * l) = __floats2bfloat162_rn(f.x, f.y);
+            }
+            oneBlob(f3{rd.x, rd.y, rd.z}, row + kHashF + half * 2 * kBlob);
+        }
+        else
+        {
+            uint32_t* z = reinterpret_cast<uint32_t*>(row);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) z[half * 8 + i] = 0u;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) z[(kHashF + half * 2 * kBlob) / 2 + i] = 0u;
+        }
+        __syncwarp();
+        for (uint32_t e = lane; e < 16u * 12u; e += 32u)
+        {
+            uint32_t rr = e / 12u, c = e % 12u;
+            if (rr < rows)
+                reinterpret_cast<uint4*>(a.acts + size_t(j0 + rr) * kActRow)[c] =
+                    reinterpret_cast<const uint4*>(x + rr * kXS)[c];
+        }
+        uint32_t h[4][1][4][4];
+        float    out[1][6][4];
+        mlpForward<1>(wf, x, lane, h, out);
+#pragma unroll
+        for (int l = 0; l < 4; ++l)
+            storeA<4>(h[l][0], a.acts + size_t(j0) * kActRow + actOffset(l + 1), kActRow, rows, lane);
+        __syncwarp();
+        float* o = reinterpret_cast<float*>(x);
+        storeOut<1>(out, o, lane);
+        __syncwarp();
+        float lossPart = 0.0f;
+        if (lane < 16u)
+        {
+            uint32_t* drow = reinterpret_cast<uint32_t*>(dT + lane * kDS);
+            if (valid)
+            {
+                float4 r0 = R[0], r3 = R[3];
+                float  gr[kOut];
+                float  lp = headLossGrad(o + lane * kOS, f3{r3.x, r3.y, r3.z}, gr);
+                float  s  = -r0.w * invW;
+                lossPart  = s * lp;
+#pragma unroll
+                for (int c = 0; c < kOut / 2; ++c) drow[c] = packBf16(gr[2 * c] * s, gr[2 * c + 1] * s);
+            }
+            else
+#pragma unroll
+                for (int c = 0; c < kOut / 2; ++c) drow[c] = 0u;
+        }
+        for (int off = 16; off > 0; off >>= 1) lossPart += __shfl_xor_sync(0xffffffffu, lossPart, off);
+        if (lane == 0 && lossPart != 0.0f) atomicAdd(&a.scal[1], double(lossPart));
+        __syncwarp();
+        for (uint32_t e = lane; e < 16u * 6u; e += 32u)
+        {
+            uint32_t rr = e / 6u, c = e % 6u;
+            if (rr < rows)
+                reinterpret_cast<uint4*>(a.deltas + size_t(j0 + rr) * kDeltaRow + deltaOffset(4))[c] =
+                    reinterpret_cast<const uint4*>(dT + rr * kDS)[c];
+        }
+        // Backward: layer 4 (3 k-tiles over its 48 outputs), then 3, 2, 1.
+        uint32_t d4[4][4], d3[4][4];
+#pragma unroll
+        for (int kt = 0; kt < 3; ++kt) loadA(d4[kt], dT, kDS, kt, lane);
+        d4[3][0] = d4[3][1] = d4[3][2] = d4[3][3] = 0u;
+        backHidden<3>(wb + bwdFragOffset(4) * 32, d4, h[3][0], d3, lane);
+        storeA<4>(d3, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(3), kDeltaRow, rows, lane);
+        backHidden<4>(wb + bwdFragOffset(3) * 32, d3, h[2][0], d4, lane);
+        storeA<4>(d4, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(2), kDeltaRow, rows, lane);
+        backHidden<4>(wb + bwdFragOffset(2) * 32, d4, h[1][0], d3, lane);
+        storeA<4>(d3, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(1), kDeltaRow, rows, lane);
+        backHidden<4>(wb + bwdFragOffset(1) * 32, d3, h[0][0], d4, lane);
+        storeA<4>(d4, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(0), kDeltaRow, rows, lane);
+        // Layer 0: gradient of the 32 hash features (FP32).
+        float gx[4][4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) gx[n][0] = gx[n][1] = gx[n][2] = gx[n][3] = 0.0f;
+        const uint2* w0 = wb + bwdFragOffset(0) * 32;
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt)
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt)
+            {
+                uint2 b = w0[(kt * 4 + nt) * 32 + lane];
+                mma16816(gx[nt], d4[kt], b.x, b.y);
+            }
+        // Column 8nt + 2t + f is feature f of level 4nt + t.
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+        {
+            const int level = 4 * nt + int(t);
+#pragma unroll
+            for (int hr = 0; hr < 2; ++hr)
+            {
+                const uint32_t rr = g + 8u * hr;
+                const float    d0 = gx[nt][2 * hr], d1 = gx[nt][2 * hr + 1];
+                if (rr >= rows || (d0 == 0.0f && d1 == 0.0f)) continue;
+                f3     p    = {posS[3 * rr], posS[3 * rr + 1], posS[3 * rr + 2]};
+                Cell   c    = gridCell(a.g.res[level], p);
+                float2* gb  = a.gradTable + (size_t(level) << a.g.log2T);
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                {
+                    float w = cornerWeight(c, k);
+                    atomicAdd(gb + cornerIndex(a.g, level, c, k), make_float2(w * d0, w * d1));
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// dW_l = sum_s delta_l[s]^T a_l[s] over a chunk of kGradChunk samples of the
+// batch (block (chunk, layer)): both operands are staged in shared memory
+// 64 samples at a time and read transposed with ldmatrix.trans; warp w owns
+// output rows 16w..16w+15 of the layer; FP32 partials go to the gradient with
+// one atomicAdd per element per block.
+__global__ void __launch_bounds__(128) kWeightGrad(const __nv_bfloat16* __restrict__ acts,
+                                                   const __nv_bfloat16* __restrict__ deltas, const uint32_t* count,
+                                                   uint32_t batch, float* __restrict__ gradMlp)
+{
+    __shared__ __align__(16) __nv_bfloat16 dS[kGradStep][kWidth + 8];
+    __shared__ __align__(16) __nv_bfloat16 aS[kGradStep][kIn + 8];
+    const int      l = blockIdx.y, O = layerOut(l), I = layerIn(l);
+    const uint32_t nB = min(*count, batch);
+    const uint32_t s0 = blockIdx.x * kGradChunk, s1 = min(s0 + uint32_t(kGradChunk), nB);
+    if (s0 >= s1) return;
+    const uint32_t lane = laneIdx(), w = threadIdx.x >> 5, jm = lane >> 3;
+    const bool     active = int(w) < O / 16;
+    float          acc[12][4];
+#pragma unroll
+    for (int n = 0; n < 12; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
+    const int dq = O / 8, aq = I / 8; // uint4 per staged row
+    for (uint32_t s = s0; s < s1; s += kGradStep)
+    {
+        __syncthreads();
+        for (int e = threadIdx.x; e < kGradStep * dq; e += blockDim.x)
+        {
+            int  rr = e / dq, c = e % dq;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (s + rr < s1) v = __ldg(reinterpret_cast<const uint4*>(deltas + size_t(s + rr) * kDeltaRow + deltaOffset(l)) + c);
+            reinterpret_cast<uint4*>(&dS[rr][0])[c] = v;
+        }
+        for (int e = threadIdx.x; e < kGradStep * aq; e += blockDim.x)
+        {
+            int  rr = e / aq, c = e % aq;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (s + rr < s1) v = __ldg(reinterpret_cast<const uint4*>(acts + size_t(s + rr) * kActRow + actOffset(l)) + c);
+            reinterpret_cast<uint4*>(&aS[rr][0])[c] = v;
+        }
+        __syncthreads();
+        if (!active) continue;
+#pragma unroll
+        for (int ks = 0; ks < kGradStep / 16; ++ks)
+        {
+            uint32_t A[4];
+            ldsm4t(A, &dS[ks * 16 + (lane & 7) + 8 * (jm >> 1)][w * 16 + 8 * (jm & 1)]);
+#pragma unroll
+            for (int np = 0; np < 6; ++np)
+            {
+                if (np < I / 16)
+                {
+                    uint32_t B[4];
+                    ldsm4t(B, &aS[ks * 16 + (lane & 7) + 8 * (jm & 1)][np * 16 + 8 * (jm >> 1)]);
+                    mma16816(acc[2 * np], A, B[0], B[1]);
+                    mma16816(acc[2 * np + 1], A, B[2], B[3]);
+                }
+            }
+        }
+    }
+    if (!active) return;
+    const uint32_t g = lane >> 2, t = lane & 3u;
+    float*         G = gradMlp + weightOffset(l);
+#pragma unroll
+    for (int nt = 0; nt < 12; ++nt)
+    {
+        if (nt < I / 8)
+        {
+            int o = int(w) * 16 + int(g), i = nt * 8 + 2 * int(t);
+            atomicAdd(G + o * I + i, acc[nt][0]);
+            atomicAdd(G + o * I + i + 1, acc[nt][1]);
+            atomicAdd(G + (o + 8) * I + i, acc[nt][2]);
+            atomicAdd(G + (o + 8) * I + i + 1, acc[nt][3]);
+        }
+    }
+}
+
+// Adam (FP32 master parameters); clears the gradient it consumed and
+// refreshes the bf16 copy of the hash table.
+__global__ void kAdam(float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m, float* __restrict__ v,
+                      uint64_t n, uint64_t hashN, float lr, float b1, float b2, float eps, float c1, float c2,
+                      __nv_bfloat16* __restrict__ table)
+{
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    {
+        float gi = grad[i];
+        grad[i]  = 0.0f;
+        float mi = b1 * m[i] + (1.0f - b1) * gi;
+        float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i]     = mi;
+        v[i]     = vi;
+        float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        p[i]     = pi;
+        if (i < hashN) table[i] = __float2bfloat16_rn(pi);
+    }
+}
+
+int gridFor(uint64_t n, int block, int cap)
+{
+    uint64_t b = (n + block - 1) / block;
+    return int(b < uint64_t(cap) ? (b ? b : 1) : cap);
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+void guideDefaultConfig(cl_guide_config* c)
+{
+    std::memset(c, 0, sizeof(*c));
+    c->log2_table    = 19;
+    c->n_min         = 16.0f;
+    c->n_max         = 1024.0f;
+    c->learning_rate = 1e-2f;
+    c->beta1         = 0.9f;
+    c->beta2         = 0.99f;
+    c->epsilon       = 1e-10f;
+    c->bsdf_fraction = 0.5f;
+    c->batch         = 1u << 18;
+    c->train_spp     = 32;
+    c->class_mask    = 3u;
+    c->seed          = 1;
+}
+
+cl_status guideResolutions(float nmin, float nmax, uint32_t* res)
+{
+    if (!(nmin >= 1.0f) || !(nmax >= nmin) || nmax > 16777216.0f) return CL_ERR_INVALID_ARG;
+    double b = std::exp((std::log(double(nmax)) - std::log(double(nmin))) / double(kLevels - 1));
+    for (int l = 0; l < kLevels; ++l) res[l] = uint32_t(std::floor(double(nmin) * std::pow(b, double(l))));
+    return CL_OK;
+}
+
+GuideNet::GuideNet(const cl_guide_config& c) : cfg_(c) {}
+GuideNet::~GuideNet() = default;
+
+cl_status GuideNet::init(cudaStream_t st, std::string* err)
+{
+    st_ = st;
+    if (cfg_.log2_table < 8 || cfg_.log2_table > 24)
+    {
+        *err = "guide: log2_table must be in [8, 24]";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (cfg_.batch == 0 || cfg_.batch > (1u << 24) || !(cfg_.learning_rate > 0.0f) || !(cfg_.bsdf_fraction >= 0.0f) ||
+        !(cfg_.bsdf_fraction <= 1.0f) || !(cfg_.beta1 >= 0.0f && cfg_.beta1 < 1.0f) ||
+        !(cfg_.beta2 >= 0.0f && cfg_.beta2 < 1.0f) || !(cfg_.epsilon >= 0.0f))
+    {
+        *err = "guide: batch, learning rate, Adam or bsdf_fraction out of range";
+        return CL_ERR_INVALID_ARG;
+    }
+    bool given = false;
+    for (int l = 0; l < kLevels; ++l) given |= cfg_.resolutions[l] != 0u;
+    if (given)
+    {
+        for (int l = 0; l < kLevels; ++l)
+        {
+            if (cfg_.resolutions[l] < 1u || cfg_.resolutions[l] > (1u << 24))
+            {
+                *err = "guide: resolutions must be in [1, 2^24]";
+                return CL_ERR_INVALID_ARG;
+            }
+            res_[l] = cfg_.resolutions[l];
+        }
+    }
+    else if (guideResolutions(cfg_.n_min, cfg_.n_max, res_) != CL_OK)
+    {
+        *err = "guide: n_min/n_max out of range";
+        return CL_ERR_INVALID_ARG;
+    }
+    const uint64_t T = 1ull << cfg_.log2_table;
+    denseMask_       = 0;
+    for (int l = 0; l < kLevels; ++l)
+    {
+        uint64_t r1 = uint64_t(res_[l]) + 1;
+        if (r1 * r1 * r1 <= T) denseMask_ |= 1u << l;
+    }
+    hashParams_ = uint64_t(kLevels) * T * kFeat;
+    const uint64_t n = paramCount();
+    int dev = 0;
+    CL_CUDA(cudaGetDevice(&dev), err);
+    CL_CUDA(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, dev), err);
+    CL_CUDA(cudaFuncSetAttribute(kInferUnit, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kFwdFragBytes + kInferWarps * kXTile),
+            err);
+    CL_CUDA(cudaFuncSetAttribute(kTrainFwdBwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem), err);
+    int occ = 0;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kTrainFwdBwd, kTrainWarps * 32, kTrainSmem), err);
+    trainBlocks_ = numSMs_ * (occ > 0 ? occ : 1);
+    CL_TRY(params_.alloc(n * 4, err));
+    CL_TRY(grad_.alloc(n * 4, err));
+    CL_TRY(m_.alloc(n * 4, err));
+    CL_TRY(v_.alloc(n * 4, err));
+    CL_TRY(table_.alloc(hashParams_ * 2, err));
+    CL_TRY(wf_.alloc(kFwdFragBytes, err));
+    CL_TRY(wb_.alloc(kBwdFragBytes, err));
+    CL_TRY(acts_.alloc(size_t(cfg_.batch) * kActRow * 2, err));
+    CL_TRY(deltas_.alloc(size_t(cfg_.batch) * kDeltaRow * 2, err));
+    CL_TRY(scal_.alloc(64, err));
+    kInitParams<<<gridFor(n, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), hashParams_, cfg_.seed);
+    CL_CUDA(cudaGetLastError(), err);
+    CL_CUDA(cudaMemsetAsync(grad_.p, 0, n * 4, st_), err);
+    CL_CUDA(cudaMemsetAsync(m_.p, 0, n * 4, st_), err);
+    CL_CUDA(cudaMemsetAsync(v_.p, 0, n * 4, st_), err);
+    CL_CUDA(cudaMemsetAsync(scal_.p, 0, 64, st_), err);
+    step_ = 0;
+    CL_TRY(refreshCopies(err));
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+GridView GuideNet::grid() const
+{
+    GridView g;
+    g.table     = table_.as<const __nv_bfloat162>();
+    g.log2T     = cfg_.log2_table;
+    g.mask      = (1u << cfg_.log2_table) - 1u;
+    g.denseMask = denseMask_;
+    for (int l = 0; l < kLevels; ++l) g.res[l] = res_[l];
+    return g;
+}
+
+cl_status GuideNet::refreshCopies(std::string* err)
+{
+    kTableCopy<<<gridFor(hashParams_, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), table_.as<__nv_bfloat16>(),
+                                                                        hashParams_);
+    CL_CUDA(cudaGetLastError(), err);
+    kFrags<<<((kFwdFrags + kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
+                                                                         wb_.as<uint2>());
+    CL_CUDA(cudaGetLastError(), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::setParams(const float* p, uint64_t n, std::string* err)
+{
+    if (!p || n != paramCount())
+    {
+        *err = "guide: parameter count mismatch";
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_CUDA(cudaMemcpyAsync(params_.p, p, n * 4, cudaMemcpyHostToDevice, st_), err);
+    CL_CUDA(cudaMemsetAsync(grad_.p, 0, n * 4, st_), err);
+    CL_CUDA(cudaMemsetAsync(m_.p, 0, n * 4, st_), err);
+    CL_CUDA(cudaMemsetAsync(v_.p, 0, n * 4, st_), err);
+    step_ = 0;
+    CL_TRY(refreshCopies(err));
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::getParams(float* p, uint64_t n, std::string* err)
+{
+    if (!p || n != paramCount())
+    {
+        *err = "guide: parameter count mismatch";
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_CUDA(cudaMemcpyAsync(p, params_.p, n * 4, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::forward(const float* in9, uint32_t n, float* out48, std::string* err)
+{
+    if ((!in9 || !out48) && n)
+    {
+        *err = "guide: null buffer";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (n == 0) return CL_OK;
+    CL_TRY(io_.alloc(size_t(n) * 9 * 4, err));
+    CL_TRY(io2_.alloc(size_t(n) * kOut * 4, err));
+    CL_CUDA(cudaMemcpyAsync(io_.p, in9, size_t(n) * 9 * 4, cudaMemcpyHostToDevice, st_), err);
+    const int smem = kFwdFragBytes + kInferWarps * kXTile;
+    kInferUnit<<<gridFor(n, kInferWarps * 32, numSMs_ * 2), kInferWarps * 32, smem, st_>>>(grid(), fwdFrags(), io_.f(),
+                                                                                           n, io2_.f());
+    CL_CUDA(cudaGetLastError(), err);
+    CL_CUDA(cudaMemcpyAsync(out48, io2_.p, size_t(n) * kOut * 4, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::sample(const float* in9, const float* u3, uint32_t n, float* dir, float* pdf, std::string* err)
+{
+    if (n == 0) return CL_OK;
+    if (!in9 || !u3 || !dir || !pdf)
+    {
+        *err = "guide: null buffer";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::vector<float> out(size_t(n) * kOut);
+    CL_TRY(forward(in9, n, out.data(), err));
+    DevBuf u, d, p;
+    CL_TRY(u.alloc(size_t(n) * 12, err));
+    CL_TRY(d.alloc(size_t(n) * 12, err));
+    CL_TRY(p.alloc(size_t(n) * 4, err));
+    CL_CUDA(cudaMemcpyAsync(u.p, u3, size_t(n) * 12, cudaMemcpyHostToDevice, st_), err);
+    kSampleUnit<<<(n + 127) / 128, 128, 0, st_>>>(io2_.f(), u.f(), n, d.f(), p.f());
+    CL_CUDA(cudaGetLastError(), err);
+    CL_CUDA(cudaMemcpyAsync(dir, d.p, size_t(n) * 12, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaMemcpyAsync(pdf, p.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::pdf(const float* in9, const float* dir, uint32_t n, float* pdf, std::string* err)
+{
+    if (n == 0) return CL_OK;
+    if (!in9 || !dir || !pdf)
+    {
+        *err = "guide: null buffer";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::vector<float> out(size_t(n) * kOut);
+    CL_TRY(forward(in9, n, out.data(), err));
+    DevBuf d, p;
+    CL_TRY(d.alloc(size_t(n) * 12, err));
+    CL_TRY(p.alloc(size_t(n) * 4, err));
+    CL_CUDA(cudaMemcpyAsync(d.p, dir, size_t(n) * 12, cudaMemcpyHostToDevice, st_), err);
+    kPdfUnit<<<(n + 127) / 128, 128, 0, st_>>>(io2_.f(), d.f(), n, p.f());
+    CL_CUDA(cudaGetLastError(), err);
+    CL_CUDA(cudaMemcpyAsync(pdf, p.p, size_t(n) * 4, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+// rec13 rows -> device records; the record count goes to scal[2] (u32).
+cl_status GuideNet::upload(const float* rec13, uint32_t n, std::string* err)
+{
+    if (!rec13 || n == 0)
+    {
+        *err = "guide: empty or null batch";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::vector<float> h(size_t(n) * 16, 0.0f);
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const float* s = rec13 + 13 * size_t(i);
+        float*       d = h.data() + 16 * size_t(i);
+        d[0] = s[0], d[1] = s[1], d[2] = s[2], d[3] = s[12];
+        d[4] = s[3], d[5] = s[4], d[6] = s[5];
+        d[8] = s[6], d[9] = s[7], d[10] = s[8];
+        d[12] = s[9], d[13] = s[10], d[14] = s[11];
+    }
+    CL_TRY(rec_.alloc(h.size() * 4, err));
+    CL_CUDA(cudaMemcpyAsync(rec_.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st_), err);
+    CL_CUDA(cudaMemcpyAsync(scal_.as<unsigned char>() + 16, &n, 4, cudaMemcpyHostToDevice, st_), err);
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::computeGradient(const float4* rec, const uint32_t* count, std::string* err)
+{
+    CL_CUDA(cudaMemsetAsync(scal_.p, 0, 16, st_), err);
+    TrainArgs a;
+    a.rec       = rec;
+    a.count     = count;
+    a.batch     = cfg_.batch;
+    a.g         = grid();
+    a.wf        = wf_.as<const uint2>();
+    a.wb        = wb_.as<const uint2>();
+    a.gradTable = reinterpret_cast<float2*>(grad_.f());
+    a.acts      = acts_.as<__nv_bfloat16>();
+    a.deltas    = deltas_.as<__nv_bfloat16>();
+    a.scal      = scal_.as<double>();
+    kTrainPrep<<<numSMs_ * 2, 256, 0, st_>>>(a);
+    CL_CUDA(cudaGetLastError(), err);
+    kTrainFwdBwd<<<trainBlocks_, kTrainWarps * 32, kTrainSmem, st_>>>(a);
+    CL_CUDA(cudaGetLastError(), err);
+    dim3 gg((cfg_.batch + kGradChunk - 1) / kGradChunk, kLayers);
+    kWeightGrad<<<gg, 128, 0, st_>>>(acts_.as<const __nv_bfloat16>(), deltas_.as<const __nv_bfloat16>(), count,
+                                     cfg_.batch, grad_.f() + hashParams_);
+    CL_CUDA(cudaGetLastError(), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::trainDevice(const float4* rec, const uint32_t* count, std::string* err)
+{
+    CL_TRY(computeGradient(rec, count, err));
+    ++step_;
+    const float c1 = float(1.0 - std::pow(double(cfg_.beta1), double(step_)));
+    const float c2 = float(1.0 - std::pow(double(cfg_.beta2), double(step_)));
+    const uint64_t n = paramCount();
+    kAdam<<<gridFor(n, 256, numSMs_ * 16), 256, 0, st_>>>(params_.f(), grad_.f(), m_.f(), v_.f(), n, hashParams_,
+                                                         cfg_.learning_rate, cfg_.beta1, cfg_.beta2, cfg_.epsilon, c1,
+                                                         c2, table_.as<__nv_bfloat16>());
+    CL_CUDA(cudaGetLastError(), err);
+    kFrags<<<((kFwdFrags + kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
+                                                                         wb_.as<uint2>());
+    CL_CUDA(cudaGetLastError(), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::gradient(const float* rec13, uint32_t n, double* loss, float* grad, std::string* err)
+{
+    if (!grad || !loss)
+    {
+        *err = "guide: null output";
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_TRY(upload(rec13, n, err));
+    const uint32_t* cnt = reinterpret_cast<const uint32_t*>(scal_.as<unsigned char>() + 16);
+    CL_TRY(computeGradient(rec_.as<const float4>(), cnt, err));
+    CL_CUDA(cudaMemcpyAsync(grad, grad_.p, paramCount() * 4, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaMemcpyAsync(loss, scal_.as<double>() + 1, 8, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaMemsetAsync(grad_.p, 0, paramCount() * 4, st_), err);
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+cl_status GuideNet::trainStepHost(const float* rec13, uint32_t n, double* loss, std::string* err)
+{
+    CL_TRY(upload(rec13, n, err));
+    const uint32_t* cnt = reinterpret_cast<const uint32_t*>(scal_.as<unsigned char>() + 16);
+    CL_TRY(trainDevice(rec_.as<const float4>(), cnt, err));
+    if (loss) CL_CUDA(cudaMemcpyAsync(loss, scal_.as<double>() + 1, 8, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaStreamSynchronize(st_), err);
+    return CL_OK;
+}
+
+} // namespace clb

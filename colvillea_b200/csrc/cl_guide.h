@@ -1,0 +1,69 @@
+// Guiding network, host side: parameters, Adam state, training staging and
+// the kernels' launch sequence (no counterpart in the reference renderer).
+#pragma once
+
+#include "cl_guide.cuh"
+#include "cl_internal.h"
+
+namespace clb
+{
+// One training record in device memory (4 float4):
+// {p.xyz in [0,1]^3, w} {n.xyz, -} {wo.xyz, -} {omega.xyz, -}.
+constexpr int kRecordF4 = 4;
+
+class GuideNet
+{
+public:
+    explicit GuideNet(const cl_guide_config& c);
+    ~GuideNet();
+    cl_status init(cudaStream_t st, std::string* err);
+
+    uint64_t paramCount() const { return hashParams_ + uint64_t(guide::kMlpParams); }
+    uint64_t hashParams() const { return hashParams_; }
+    const cl_guide_config& config() const { return cfg_; }
+    const uint32_t* resolutions() const { return res_; }
+
+    cl_status setParams(const float* p, uint64_t n, std::string* err);
+    cl_status getParams(float* p, uint64_t n, std::string* err);
+    cl_status forward(const float* in9, uint32_t n, float* out48, std::string* err);
+    cl_status gradient(const float* rec13, uint32_t n, double* loss, float* grad, std::string* err);
+    cl_status trainStepHost(const float* rec13, uint32_t n, double* loss, std::string* err);
+    cl_status sample(const float* in9, const float* u3, uint32_t n, float* dir, float* pdf, std::string* err);
+    cl_status pdf(const float* in9, const float* dir, uint32_t n, float* pdf, std::string* err);
+
+    // Device-side use: one training step on the records rec[0, min(*count,
+    // batch)) (count in device memory), enqueued on the network's stream.
+    // The loss lands in lossDev (device double) when the stream reaches it.
+    cl_status trainDevice(const float4* rec, const uint32_t* count, std::string* err);
+    guide::GridView grid() const;
+    const uint2*    fwdFrags() const { return wf_.as<uint2>(); }
+    const double*   lossDev() const { return scal_.as<double>() + 1; }
+    uint64_t        steps() const { return step_; }
+    void            setStream(cudaStream_t st) { st_ = st; }
+
+private:
+    cl_status upload(const float* rec13, uint32_t n, std::string* err);
+    cl_status computeGradient(const float4* rec, const uint32_t* count, std::string* err);
+    cl_status refreshCopies(std::string* err);
+
+    cl_guide_config cfg_;
+    uint32_t        res_[guide::kLevels] = {};
+    uint32_t        denseMask_ = 0;
+    uint64_t        hashParams_ = 0;
+    cudaStream_t    st_ = nullptr;
+    int             numSMs_ = 148;
+    int             trainBlocks_ = 0;
+    uint64_t        step_ = 0;
+
+    DevBuf params_, grad_, m_, v_; // FP32 [hash | mlp]
+    DevBuf table_;                 // bf16 copy of the hash table
+    DevBuf wf_, wb_;               // bf16 weight fragments (forward, backward)
+    DevBuf acts_, deltas_;         // training staging, batch rows
+    DevBuf scal_;                  // {sum w, loss, count (u32)}
+    DevBuf rec_, io_, io2_;        // host-entry staging
+};
+
+void guideDefaultConfig(cl_guide_config* c);
+cl_status guideResolutions(float nmin, float nmax, uint32_t* res);
+
+} // namespace clb

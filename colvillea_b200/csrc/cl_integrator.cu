@@ -159,11 +159,43 @@ __device__ __forceinline__ void startPath(const Params& P, const WaveParams& wp,
     P.q.rqSlot[q][idx] = slot;
 }
 
+// Guided path tracing: training records of a finished path.  Recorded vertex
+// k holds the throughput T_k that reached it and the path radiance L_k after
+// its own emitter sample; (L - L_k) / T_k estimates f |cos| L_i / p of the
+// direction sampled at k, whose luminance is the record's weight.
+__device__ __noinline__ void flushRecords(GuideDev g, const uint4* psInfo, Counters* ctr, uint32_t slot,
+                                          uint32_t stride, float lx, float ly, float lz)
+{
+    uint32_t mask = psInfo[slot].w;
+    const float4* h = g.hist + size_t(slot / stride) * g.histDepth * kHistF4;
+    while (mask)
+    {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1u;
+        const float4* e  = h + k * kHistF4;
+        float4        e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3], e4 = e[4];
+        float         w  = 0.0f;
+        if (e0.w > 0.0f) w += 0.2126f * (lx - e4.x) / e0.w;
+        if (e1.w > 0.0f) w += 0.7152f * (ly - e4.y) / e1.w;
+        if (e2.w > 0.0f) w += 0.0722f * (lz - e4.z) / e2.w;
+        if (!(w > 0.0f) || !(w < FLT_MAX)) continue;
+        uint32_t idx = atomicAdd(&ctr->recCount, 1u);
+        if (idx >= g.recCap) continue;
+        float4* r = g.rec + size_t(idx) * kRecordF4;
+        r[0]      = make_float4(e0.x, e0.y, e0.z, w);
+        r[1]      = make_float4(e1.x, e1.y, e1.z, 0.0f);
+        r[2]      = make_float4(e2.x, e2.y, e2.z, 0.0f);
+        r[3]      = make_float4(e3.x, e3.y, e3.z, 0.0f);
+    }
+}
+
 // Film write of finished paths, then regeneration of their slots.  Called by
 // every lane of the warp.
 __device__ __forceinline__ void finishPaths(const Params& P, const WaveParams& wp, int nxt, bool finish, uint32_t slot,
                                             f3 L)
 {
+    if (finish && wp.recStride && slot % wp.recStride == 0u)
+        flushRecords(P.g, P.q.psInfo, P.q.ctr, slot, wp.recStride, L.x, L.y, L.z);
     if (finish)
     {
         uint32_t pix = P.q.psInfo[slot].x;
@@ -331,7 +363,11 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
 // rays), from the class queues written by kTraceClosest; -1 = every ray of
 // the ray queue.  Specialising keeps each instantiation free of the other
 // modes' and materials' code.
-template <bool DL, int CMP, bool ALIAS, int MAT>
+// GUIDE (path tracing, corrected estimator, BSDF classes): one-sample MIS of
+// the BSDF (probability bsdfFrac) and the network's vMF mixture for this ray
+// (kGuideInfer); every pdf of the BSDF strategy - emitter-sample MIS, the
+// throughput update and the escaped-ray MIS - becomes the mixture pdf.
+template <bool DL, int CMP, bool ALIAS, int MAT, bool GUIDE = false>
 __global__ void __launch_bounds__(128) kShade(Params P, int cur)
 {
     const WaveParams wp = *P.wp;
@@ -351,7 +387,8 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
         bool     valid = i < n;
         if (MAT >= 0 && valid) i = P.q.classIdx[size_t(MAT) * P.q.slots + i];
         bool     pushShadow = false, shadow1 = false, shadow2 = false, pushRay = false, finish = false;
-        uint32_t slot = 0u, info2 = 0u;
+        uint32_t slot = 0u, info2 = 0u, recBit = 0u, vDepth = 0u;
+        f3       tIn{0, 0, 0};
         f3       L{0, 0, 0}, T{1, 1, 1}, E{0, 0, 0}, pHit{0, 0, 0}, sdir{0, 0, 0}, Li{0, 0, 0}, sdir2{0, 0, 0},
             Ld{0, 0, 0}, ndir{0, 0, 0};
         if (valid)
@@ -361,6 +398,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             float4 rd     = P.q.rqD[cur][i];
             uint4  info   = P.q.psInfo[slot];
             uint32_t depth = info.z & 0xffu;
+            vDepth         = depth;
             Rng    rng{info.x % wp.W, info.x / wp.W, info.y, info.z >> 8};
             T             = ld3(P.q.psT[slot]);
             E             = ld3(P.q.psE[slot]);
@@ -395,6 +433,17 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 if (MAT >= 0) bsdf.type = uint32_t(MAT);
                 pHit         = a.p;
                 f3    wo     = -d;
+                guide::Lobes G;
+                const float  gf = P.g.bsdfFrac;
+                if (GUIDE)
+                {
+                    const float4* lb = P.g.lobes + size_t(i) * kLobeF4;
+#pragma unroll
+                    for (int k = 0; k < guide::kLobes; ++k) G.l[k] = lb[k];
+                    float4 w0 = lb[8], w1 = lb[9];
+                    G.w[0] = w0.x, G.w[1] = w0.y, G.w[2] = w0.z, G.w[3] = w0.w;
+                    G.w[4] = w1.x, G.w[5] = w1.y, G.w[6] = w1.z, G.w[7] = w1.w;
+                }
                 f2    u      = rng.next2D();
                 Frame fr{a.dpdv, a.dpdu, (!DL && compatFrame) ? a.ng : a.ns};
                 // Emitter sampling with MIS (raygeneration.cu:332-384 / 174-227).
@@ -416,6 +465,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                         if (nonzero(f))
                         {
                             float bp = bsdfPdf(bsdf, woL, wiL, compatPdf);
+                            if (GUIDE) bp = gf * bp + (1.0f - gf) * guide::mixturePdf(G, ldir);
                             float c  = (DL && compatEsc) ? wiL.z : fabsf(wiL.z);
                             f3    baseV = DL ? value : T * value;
                             float w, pl;
@@ -439,11 +489,27 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                     }
                 }
                 // BSDF sampling with MIS (raygeneration.cu:391-455 / 234-281).
+                float us  = GUIDE ? rng.next1D() : 0.0f;
                 f2    u2  = rng.next2D();
                 f3    woL = fr.toLocal(wo);
                 f3    wiL{0, 0, 0};
                 float bp = 0.0f;
-                f3    f  = bsdfSample(bsdf, woL, u2, &wiL, &bp);
+                f3    f{0.0f, 0.0f, 0.0f};
+                f3    gdir{0.0f, 0.0f, 0.0f};
+                if (!GUIDE || us < gf)
+                    f = bsdfSample(bsdf, woL, u2, &wiL, &bp);
+                else
+                {
+                    gdir = guide::mixtureSample(G, (us - gf) / (1.0f - gf), u2.x, u2.y);
+                    wiL  = fr.toLocal(gdir);
+                    f    = bsdfEval(bsdf, woL, wiL);
+                    bp   = bsdfPdf(bsdf, woL, wiL, false);
+                }
+                if (GUIDE && nonzero(f))
+                {
+                    if (us < gf) gdir = fr.toWorld(wiL);
+                    bp = gf * bp + (1.0f - gf) * guide::mixturePdf(G, gdir);
+                }
                 // The corrected estimator stops paths whose sampled pdf is not
                 // positive (0 or NaN at the rim of the cosine warp); the
                 // reference's update divides by it (raygeneration.cu:430).
@@ -451,7 +517,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                     finish = true;
                 else
                 {
-                    f3    dir      = fr.toWorld(wiL);
+                    f3    dir      = GUIDE ? gdir : fr.toWorld(wiL);
                     float lightPdf = sc.hasDome ? domePdf(sc.dome, dir, !compatEsc) : 0.0f;
                     if (DL)
                     {
@@ -472,6 +538,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                     {
                         float c = fabsf(wiL.z);
                         f3    tk{f.x * c / bp, f.y * c / bp, f.z * c / bp};
+                        tIn        = T;
                         T          = T * tk;
                         bool alive = true;
                         if (wp.rrStart > 0u && depth >= wp.rrStart)
@@ -504,6 +571,19 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                             pushRay = true;
                             ndir    = dir;
                             info2   = (depth + 1u) | (rng.ctr << 8);
+                            if (GUIDE && wp.recStride && slot % wp.recStride == 0u && depth <= P.g.histDepth)
+                            {
+                                // Training history of this vertex (flushRecords).
+                                float4* h = P.g.hist + (size_t(slot / wp.recStride) * P.g.histDepth + depth - 1u) *
+                                                           kHistF4;
+                                f3 pn = (a.p - f3{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]}) * P.g.boxScale;
+                                h[0]  = make_float4(pn.x, pn.y, pn.z, tIn.x);
+                                h[1]  = make_float4(a.ns.x, a.ns.y, a.ns.z, tIn.y);
+                                h[2]  = make_float4(wo.x, wo.y, wo.z, tIn.z);
+                                h[3]  = make_float4(dir.x, dir.y, dir.z, 0.0f);
+                                h[4]  = make_float4(L.x, L.y, L.z, 0.0f);
+                                recBit = 1u << (depth - 1u);
+                            }
                         }
                         else
                             finish = true;
@@ -521,7 +601,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 uint32_t tag     = slot | (finish ? kLastFlag : 0u);
                 P.q.sqO[sIdx]    = make_float4(pHit.x, pHit.y, pHit.z, __uint_as_float(tag));
                 P.q.sqD[sIdx]    = make_float4(sdir.x, sdir.y, sdir.z, shadow1 ? 1.0f : 0.0f);
-                P.q.sqL[sIdx]    = make_float4(Li.x, Li.y, Li.z, 0.0f);
+                P.q.sqL[sIdx]    = make_float4(Li.x, Li.y, Li.z, __uint_as_float(vDepth));
                 if (DL)
                 {
                     P.q.sqD2[sIdx] = make_float4(sdir2.x, sdir2.y, sdir2.z, shadow2 ? 1.0f : 0.0f);
@@ -544,6 +624,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             P.q.rqD[nxt][rIdx]    = make_float4(ndir.x, ndir.y, ndir.z, FLT_MAX);
             P.q.rqSlot[nxt][rIdx] = slot;
             P.q.psInfo[slot].z    = info2;
+            if (GUIDE && recBit) P.q.psInfo[slot].w |= recBit;
             P.q.psT[slot]         = make_float4(T.x, T.y, T.z, 0.0f);
             P.q.psE[slot]         = make_float4(E.x, E.y, E.z, 0.0f);
         }
@@ -573,8 +654,18 @@ __global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
             uint32_t tag = __float_as_uint(P.q.sqO[i].w);
             slot         = tag & ~kLastFlag;
             L            = ld3(P.q.psL[slot]);
-            if (P.q.vis[DL ? 2 * i : i]) L = L + ld3(P.q.sqL[i]);
+            float4 li = P.q.sqL[i];
+            if (P.q.vis[DL ? 2 * i : i]) L = L + ld3(li);
             if (DL && P.q.vis[2 * i + 1]) L = L + ld3(P.q.sqL2[i]);
+            if (!DL && wp.recStride && slot % wp.recStride == 0u)
+            {
+                // Guiding: the recorded vertex's radiance snapshot includes
+                // its own emitter sample (flushRecords).
+                uint32_t d = __float_as_uint(li.w);
+                if (d >= 1u && d <= P.g.histDepth && ((P.q.psInfo[slot].w >> (d - 1u)) & 1u))
+                    P.g.hist[(size_t(slot / wp.recStride) * P.g.histDepth + d - 1u) * kHistF4 + 4] =
+                        make_float4(L.x, L.y, L.z, 0.0f);
+            }
             if (tag & kLastFlag)
                 finish = true;
             else
@@ -582,6 +673,88 @@ __global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
         }
         finishPaths(P, wp, nxt, finish, slot, L);
     }
+}
+
+// Guided path tracing: network inference for the rays of the guided shading
+// classes (after kTraceClosest).  Each warp takes 32 rays of the class queues
+// (concatenated), encodes hit position, shading normal and outgoing direction
+// into its shared-memory tile, runs the MLP on the tensor cores (two 16-row
+// tiles) and writes the head's lobes for each ray.  Rays whose vertex is the
+// last one (depth == maxDepth) are not shaded and are skipped.
+constexpr int kGuideInferWarps = 8;
+constexpr int kGuideInferSmem  = guide::kFwdFragBytes + kGuideInferWarps * 32 * guide::kXS * 2;
+__global__ void __launch_bounds__(kGuideInferWarps * 32) kGuideInfer(Params P, guide::GridView g,
+                                                                     const uint2* __restrict__ wfG, int cur)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint2*         wf   = reinterpret_cast<uint2*>(smem);
+    const uint32_t lane = laneId(), warp = threadIdx.x >> 5;
+    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + guide::kFwdFragBytes + warp * 32 * guide::kXS * 2);
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(wfG);
+        uint4*       dst = reinterpret_cast<uint4*>(wf);
+        for (int k = threadIdx.x; k < guide::kFwdFrags * 16; k += blockDim.x) dst[k] = __ldg(src + k);
+    }
+    __syncthreads();
+    const uint32_t maxDepth = P.wp->maxDepth;
+    const uint32_t mask     = P.g.classMask;
+    const uint32_t n0 = (mask & 1u) ? loadCount(&P.q.ctr->classCount[0]) : 0u;
+    const uint32_t n1 = (mask & 2u) ? loadCount(&P.q.ctr->classCount[1]) : 0u;
+    const uint32_t n2 = (mask & 4u) ? loadCount(&P.q.ctr->classCount[2]) : 0u;
+    const uint32_t n  = n0 + n1 + n2;
+    const f3       bmin{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]};
+    for (;;)
+    {
+        uint32_t base = warpFetch(&P.q.ctr->fetchInfer);
+        if (base >= n) break;
+        uint32_t k     = base + lane;
+        bool     valid = k < n;
+        uint32_t i     = 0u;
+        if (valid)
+        {
+            uint32_t c   = k < n0 ? 0u : (k < n0 + n1 ? 1u : 2u);
+            uint32_t pos = k - (c == 0u ? 0u : (c == 1u ? n0 : n0 + n1));
+            i            = P.q.classIdx[size_t(c) * P.q.slots + pos];
+            if ((P.q.psInfo[P.q.rqSlot[cur][i]].z & 0xffu) == maxDepth) valid = false;
+        }
+        __nv_bfloat16* row = x + lane * guide::kXS;
+        const uint32_t vm  = __ballot_sync(kFull, valid);
+        if (lane == 0u && vm) atomicAdd(&P.q.ctr->inferred, (unsigned long long)__popc(vm));
+        if (valid)
+        {
+            float4  hh = P.q.hit[i];
+            float4  rd = P.q.rqD[cur][i];
+            HitAttr a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
+            guide::encodeRow(g, (a.p - bmin) * P.g.boxScale, a.ns, f3{-rd.x, -rd.y, -rd.z}, row);
+        }
+        else
+            guide::zeroRow(row);
+        __syncwarp();
+        float out[2][6][4];
+        guide::mlpInfer<2>(wf, x, lane, out);
+        __syncwarp();
+        float* o = reinterpret_cast<float*>(x);
+        guide::storeOut<2>(out, o, lane);
+        __syncwarp();
+        if (valid)
+        {
+            guide::Lobes L;
+            guide::headLobes(o + lane * guide::kOS, &L);
+            float4* dst = P.g.lobes + size_t(i) * kLobeF4;
+#pragma unroll
+            for (int j = 0; j < guide::kLobes; ++j) dst[j] = L.l[j];
+            dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
+            dst[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
+        }
+        __syncwarp();
+    }
+}
+
+// Records beyond the capacity were dropped; the training step reads the
+// clamped count.
+__global__ void kClampRecords(Counters* c, uint32_t cap)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) c->trainCount = min(c->recCount, cap);
 }
 
 // Initial fill: slot s starts path s.
@@ -604,6 +777,7 @@ __global__ void kAdvance(Counters* c, int cur)
     c->fetchShade    = 0u;
     c->fetchShadow   = 0u;
     c->fetchResolve  = 0u;
+    c->fetchInfer    = 0u;
     for (int k = 0; k < 4; ++k)
     {
         c->classCount[k] = 0u;
@@ -660,6 +834,12 @@ template <bool DL, int MAT> ShadeFn shadeKernelM(uint32_t flags)
     return al ? kShade<DL, 2, true, MAT> : kShade<DL, 2, false, MAT>;
 }
 
+// Guided path-tracing shading of BSDF class MAT (corrected estimator only).
+template <int MAT> ShadeFn shadeKernelGuided(uint32_t flags)
+{
+    return (flags & CL_DOME_ALIAS) ? kShade<false, 0, true, MAT, true> : kShade<false, 0, false, MAT, true>;
+}
+
 // Shading kernel of class `mat` (0-2 BSDF type, 3 escaped rays).
 template <bool DL> ShadeFn shadeKernelT(int mat, uint32_t flags)
 {
@@ -672,8 +852,18 @@ template <bool DL> ShadeFn shadeKernelT(int mat, uint32_t flags)
     }
 }
 
-ShadeFn shadeKernel(bool dl, int mat, uint32_t flags)
+ShadeFn shadeKernel(bool dl, int mat, uint32_t flags, bool guided = false)
 {
+    if (guided && !dl)
+    {
+        switch (mat)
+        {
+            case 0: return shadeKernelGuided<0>(flags);
+            case 1: return shadeKernelGuided<1>(flags);
+            case 2: return shadeKernelGuided<2>(flags);
+            default: break;
+        }
+    }
     return dl ? shadeKernelT<true>(mat, flags) : shadeKernelT<false>(mat, flags);
 }
 } // namespace
@@ -729,6 +919,10 @@ cl_status Integrator::init(std::string* err)
                 &b, dl ? (const void*)kShadowResolve<true> : (const void*)kShadowResolve<false>, 128, 0),
             err);
     shadowBlocks_ = std::max(1, b) * numSMs_;
+    CL_CUDA(cudaFuncSetAttribute(kGuideInfer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideInferSmem), err);
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideInfer, kGuideInferWarps * 32, kGuideInferSmem),
+            err);
+    inferBlocks_ = std::max(1, b) * numSMs_;
     CL_TRY(ctr_.alloc(sizeof(Counters), err));
     CL_TRY(wp_.alloc(sizeof(WaveParams), err));
     CL_CUDA(cudaMemsetAsync(ctr_.p, 0, sizeof(Counters), stream_), err);
@@ -881,6 +1075,20 @@ cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, s
     CL_CUDA(cudaMemcpyAsync(vtx_.p, vtx.data(), vtx.size() * 4, cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaMemcpyAsync(triIdx_.p, tidx.data(), tidx.size() * 4, cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaMemcpyAsync(triPos_.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    // Scene box for the guiding network's position input (uniform scale).
+    {
+        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        for (size_t v = 0; v < nv; ++v)
+            for (int q = 0; q < 3; ++q)
+            {
+                lo[q] = std::min(lo[q], vtx[v * 12 + q]);
+                hi[q] = std::max(hi[q], vtx[v * 12 + q]);
+            }
+        float ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+        ext       = std::max(ext, 1e-6f) * 1.002f;
+        for (int q = 0; q < 3; ++q) boxMin_[q] = lo[q] - 0.001f * ext;
+        boxScale_ = 1.0f / ext;
+    }
     CL_CUDA(cudaEventRecord(evA_, stream_), err);
     CL_TRY(buildWideBvh(triPos_.f(), uint32_t(nt), stream_, &bvh_, err));
     CL_CUDA(cudaEventRecord(evB_, stream_), err);
@@ -1103,6 +1311,18 @@ Params Integrator::params() const
     P.q.slots     = slots_;
     P.q.shadowCap = shadowCap_;
     P.wp          = wp_.as<const WaveParams>();
+    if (guide_)
+    {
+        P.g.lobes     = lobes_.as<float4>();
+        P.g.hist      = hist_.as<float4>();
+        P.g.rec       = rec_.as<float4>();
+        P.g.recCap    = recCap_;
+        P.g.classMask = guideCfg_.class_mask;
+        P.g.bsdfFrac  = guideCfg_.bsdf_fraction;
+        P.g.boxScale  = boxScale_;
+        for (int q = 0; q < 3; ++q) P.g.boxMin[q] = boxMin_[q];
+        P.g.histDepth = histDepth_;
+    }
     return P;
 }
 
@@ -1120,7 +1340,13 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
         kTraceClosest<false, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
             P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur], &c->fetchTrace, P.q.hit, c, classifyView());
     if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
-    for (int m = 0; m < 4; ++m) shadeKernel(dl, m, cfg_.flags)<<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
+    const uint32_t gmask = guide_ ? guideCfg_.class_mask : 0u;
+    if (gmask)
+        kGuideInfer<<<inferBlocks_, kGuideInferWarps * 32, kGuideInferSmem, stream_>>>(P, guide_->grid(),
+                                                                                       guide_->fwdFrags(), cur);
+    if (profile) CL_CUDA(cudaEventRecord(evS_[4], stream_), err);
+    for (int m = 0; m < 4; ++m)
+        shadeKernel(dl, m, cfg_.flags, m < 3 && ((gmask >> m) & 1u))<<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
     if (profile) CL_CUDA(cudaEventRecord(evS_[2], stream_), err);
     if (dl && st)
         kTraceShadow<true, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
@@ -1176,6 +1402,44 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     if (spp == 0) return CL_OK;
     CL_TRY(ensureFilm(err));
     CL_TRY(ensureQueues(err));
+    msRender_ = msTrace_ = msShade_ = msShadow_ = msInfer_ = 0.0f;
+    waves_ = 0;
+    lastRaysC_ = lastRaysS_ = lastNodes_ = lastTris_ = lastNodesS_ = lastTrisS_ = 0;
+    if (guide_)
+    {
+        CL_TRY(ensureGuideBuffers(err));
+        // Online training: one step on the records of each of the first
+        // train_spp samples per pixel, then plain guided rendering.
+        while (spp > 0 && guide_->steps() < guideCfg_.train_spp)
+        {
+            CL_TRY(renderPass(1, true, err));
+            --spp;
+            Counters* dc = ctr_.as<Counters>();
+            CL_CUDA(cudaEventRecord(evA_, stream_), err);
+            kClampRecords<<<1, 32, 0, stream_>>>(dc, recCap_);
+            CL_CUDA(cudaGetLastError(), err);
+            CL_TRY(guide_->trainDevice(rec_.as<const float4>(), &dc->trainCount, err));
+            CL_CUDA(cudaEventRecord(evB_, stream_), err);
+            CL_CUDA(cudaMemcpyAsync(hostCount_, &dc->recCount, 8, cudaMemcpyDeviceToHost, stream_), err);
+            double loss = 0.0;
+            CL_CUDA(cudaMemcpyAsync(&loss, guide_->lossDev(), 8, cudaMemcpyDeviceToHost, stream_), err);
+            CL_CUDA(cudaEventSynchronize(evB_), err);
+            CL_CUDA(cudaStreamSynchronize(stream_), err);
+            float t = 0.0f;
+            CL_CUDA(cudaEventElapsedTime(&t, evA_, evB_), err);
+            msTrain_ += t;
+            msRender_ += t;
+            guideRecordsLast_ = hostCount_[0];
+            guideSamples_ += std::min(hostCount_[1], guideCfg_.batch);
+            guideLoss_ = loss;
+        }
+    }
+    if (spp > 0) CL_TRY(renderPass(spp, false, err));
+    return CL_OK;
+}
+
+cl_status Integrator::renderPass(uint32_t spp, bool record, std::string* err)
+{
     const bool dl      = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
     const bool profile = cfg_.flags & CL_PROFILE_STAGES;
 
@@ -1187,6 +1451,7 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     wp.rrStart     = cfg_.rr_start_depth;
     wp.flags       = cfg_.flags;
     wp.dl          = dl ? 1u : 0u;
+    wp.recStride   = record ? recStride_ : 0u;
     wp.totalPaths  = (unsigned long long)W_ * H_ * spp;
     memcpy(wp.cam, &camera_, sizeof(camera_));
     CL_CUDA(cudaMemcpyAsync(wp_.p, hostWp_, sizeof(WaveParams), cudaMemcpyHostToDevice, stream_), err);
@@ -1202,8 +1467,6 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     CL_CUDA(cudaGetLastError(), err);
     if (!profile && !graphValid_) CL_TRY(captureGraph(err));
 
-    msTrace_ = msShade_ = msShadow_ = 0.0f;
-    waves_   = 0;
     Counters* dc = ctr_.as<Counters>();
     // Every path needs at most maxDepth waves and at least one path per slot
     // finishes per maxDepth waves, so this bound is never reached by a
@@ -1223,11 +1486,13 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
             {
                 CL_TRY(launchWave(w & 1, true, err));
                 CL_CUDA(cudaStreamSynchronize(stream_), err);
-                float a = 0, b = 0, c = 0;
+                float a = 0, b = 0, c = 0, d = 0;
                 CL_CUDA(cudaEventElapsedTime(&a, evS_[0], evS_[1]), err);
-                CL_CUDA(cudaEventElapsedTime(&b, evS_[1], evS_[2]), err);
+                CL_CUDA(cudaEventElapsedTime(&d, evS_[1], evS_[4]), err);
+                CL_CUDA(cudaEventElapsedTime(&b, evS_[4], evS_[2]), err);
                 CL_CUDA(cudaEventElapsedTime(&c, evS_[2], evS_[3]), err);
                 msTrace_ += a;
+                msInfer_ += d;
                 msShade_ += b;
                 msShadow_ += c;
             }
@@ -1243,7 +1508,9 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     Counters ch;
     CL_CUDA(cudaMemcpyAsync(&ch, ctr_.p, sizeof(Counters), cudaMemcpyDeviceToHost, stream_), err);
     CL_CUDA(cudaEventSynchronize(evB_), err);
-    CL_CUDA(cudaEventElapsedTime(&msRender_, evA_, evB_), err);
+    float msPass = 0.0f;
+    CL_CUDA(cudaEventElapsedTime(&msPass, evA_, evB_), err);
+    msRender_ += msPass;
     if (ch.error)
     {
         *err = std::string("device error flags ") + std::to_string(ch.error) +
@@ -1254,15 +1521,98 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     pathsDone_ += wp.totalPaths;
     raysClosest_ += ch.raysClosest;
     raysShadow_ += ch.raysShadow;
-    lastRaysC_  = ch.raysClosest;
-    lastRaysS_  = ch.raysShadow;
-    lastNodes_  = ch.statNodes;
-    lastTris_   = ch.statTris;
-    lastNodesS_ = ch.statNodesS;
-    lastTrisS_  = ch.statTrisS;
-    launches_   = waves_;
+    lastRaysC_ += ch.raysClosest;
+    lastRaysS_ += ch.raysShadow;
+    lastNodes_ += ch.statNodes;
+    lastTris_ += ch.statTris;
+    lastNodesS_ += ch.statNodesS;
+    lastTrisS_ += ch.statTrisS;
+    guideInferred_ += ch.inferred;
+    launches_ = waves_;
     iteration_ += spp;
     filmSpp_ += spp;
+    return CL_OK;
+}
+
+cl_status Integrator::ensureGuideBuffers(std::string* err)
+{
+    const uint64_t wh    = uint64_t(W_) * H_;
+    const uint32_t batch = guideCfg_.batch;
+    recStride_           = uint32_t(std::max<uint64_t>(1, wh / batch));
+    histSlots_           = (slots_ + recStride_ - 1) / recStride_;
+    histDepth_           = std::min(cfg_.max_depth, 32u);
+    recCap_              = uint32_t(std::min<uint64_t>(4ull * batch, 1ull << 26));
+    const size_t lb = size_t(slots_) * kLobeF4 * 16, hb = size_t(histSlots_) * histDepth_ * kHistF4 * 16,
+                 rb = size_t(recCap_) * kRecordF4 * 16;
+    if (lobes_.bytes != lb)
+    {
+        CL_TRY(lobes_.alloc(lb, err));
+        graphValid_ = false;
+    }
+    if (hist_.bytes != hb)
+    {
+        CL_TRY(hist_.alloc(hb, err));
+        graphValid_ = false;
+    }
+    if (rec_.bytes != rb)
+    {
+        CL_TRY(rec_.alloc(rb, err));
+        graphValid_ = false;
+    }
+    return CL_OK;
+}
+
+cl_status Integrator::setGuiding(const cl_guide_config* cfg, std::string* err)
+{
+    if (!cfg)
+    {
+        guide_.reset();
+        lobes_.release();
+        hist_.release();
+        rec_.release();
+        graphValid_ = false;
+        return resetIteration(err);
+    }
+    if (type_ != CL_INTEGRATOR_PATH_TRACING)
+    {
+        *err = "guiding needs the path-tracing integrator";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (cfg_.flags & CL_COMPAT_ALL)
+    {
+        *err = "guiding needs the corrected estimator (no CL_COMPAT_* flag)";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (cfg->class_mask & ~7u)
+    {
+        *err = "guide class_mask has bits beyond the three BSDF classes";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::unique_ptr<GuideNet> g(new GuideNet(*cfg));
+    CL_TRY(g->init(stream_, err));
+    guide_    = std::move(g);
+    guideCfg_ = *cfg;
+    guideSamples_ = guideRecordsLast_ = guideInferred_ = 0;
+    guideLoss_ = 0.0;
+    msTrain_ = msInfer_ = 0.0f;
+    graphValid_ = false;
+    return resetIteration(err);
+}
+
+cl_status Integrator::guideStats(cl_guide_stats* s, std::string* err) const
+{
+    if (!guide_)
+    {
+        *err = "guiding is off";
+        return CL_ERR_STATE;
+    }
+    s->steps           = guide_->steps();
+    s->samples_trained = guideSamples_;
+    s->records_last    = guideRecordsLast_;
+    s->inferred        = guideInferred_;
+    s->last_loss       = guideLoss_;
+    s->ms_train        = msTrain_;
+    s->ms_infer        = msInfer_;
     return CL_OK;
 }
 

@@ -3,8 +3,10 @@
 
 #include "cl_bvh.cuh"
 #include "cl_dome.h"
+#include "cl_guide.h"
 #include "cl_internal.h"
 
+#include <memory>
 #include <vector>
 
 namespace clb
@@ -34,7 +36,8 @@ struct SceneDev
 // Per-render values, in device memory so that captured graphs stay valid.
 struct WaveParams
 {
-    uint32_t           W, H, frame0, maxDepth, rrStart, flags, dl, pad;
+    uint32_t           W, H, frame0, maxDepth, rrStart, flags, dl;
+    uint32_t           recStride; // guiding: slots s with s % recStride == 0 record training data (0: off)
     unsigned long long totalPaths;
     float              cam[12];
 };
@@ -51,6 +54,11 @@ struct Counters
     unsigned long long raysClosest, raysShadow;
     unsigned long long statNodes, statTris;
     unsigned long long statNodesS, statTrisS;
+    uint32_t           fetchInfer; // guiding: inference fetch over the guided class queues
+    uint32_t           recCount;   // guiding: training records appended (may exceed the capacity)
+    uint32_t           trainCount; // guiding: records the training step reads (clamped)
+    uint32_t           pad2;
+    unsigned long long inferred;   // guiding: network evaluations
 };
 
 struct QueueDev
@@ -77,10 +85,28 @@ struct QueueDev
     uint32_t  shadowCap;
 };
 
+// Guided path tracing: per-ray mixtures, per-slot vertex histories and the
+// training records (no counterpart in the reference).
+constexpr int kLobeF4 = 10; // 8 x {mu, kappa}, weights 0-3, weights 4-7
+constexpr int kHistF4 = 5;  // {p, T.x} {n, T.y} {wo, T.z} {omega, -} {L snapshot, -}
+struct GuideDev
+{
+    float4*  lobes;     // kLobeF4 per ray-queue index
+    float4*  hist;      // (slots / recStride) x maxDepth x kHistF4
+    float4*  rec;       // kRecordF4 per record
+    uint32_t recCap;
+    uint32_t classMask; // guided BSDF classes
+    float    bsdfFrac;
+    float    boxScale;  // 1 / largest scene extent
+    float    boxMin[3];
+    uint32_t histDepth;
+};
+
 struct Params
 {
     SceneDev          sc;
     QueueDev          q;
+    GuideDev          g;
     const WaveParams* wp;
 };
 
@@ -109,10 +135,16 @@ public:
     cl_status domeTables(float* pU, float* cU, float* pV, float* cV, std::string* err);
     cl_status domeAliasSample(const float* u2, float* dir, float* pdf, float* val, uint32_t n, std::string* err);
 
+    cl_status setGuiding(const cl_guide_config* cfg, std::string* err);
+    GuideNet* guideNet() const { return guide_.get(); }
+    cl_status guideStats(cl_guide_stats* s, std::string* err) const;
+
     uint32_t width() const { return W_; }
     uint32_t height() const { return H_; }
 
 private:
+    cl_status renderPass(uint32_t spp, bool record, std::string* err);
+    cl_status ensureGuideBuffers(std::string* err);
     cl_status ensureFilm(std::string* err);
     cl_status ensureQueues(std::string* err);
     cl_status clearFilm(std::string* err);
@@ -167,6 +199,17 @@ private:
     uint64_t  lastNodes_ = 0, lastTris_ = 0, lastNodesS_ = 0, lastTrisS_ = 0, lastRaysC_ = 0, lastRaysS_ = 0;
     float     msBvh_ = 0, msDome_ = 0, msRender_ = 0, msTrace_ = 0, msShade_ = 0, msShadow_ = 0;
     cudaEvent_t evA_ = nullptr, evB_ = nullptr, evS_[6] = {};
+
+    // Guiding.
+    std::unique_ptr<GuideNet> guide_;
+    cl_guide_config           guideCfg_{};
+    DevBuf                    lobes_, hist_, rec_;
+    uint32_t                  recStride_ = 0, recCap_ = 0, histSlots_ = 0, histDepth_ = 0;
+    float                     boxMin_[3] = {0, 0, 0}, boxScale_ = 1.0f;
+    int                       inferBlocks_ = 0;
+    uint64_t                  guideSamples_ = 0, guideRecordsLast_ = 0, guideInferred_ = 0;
+    double                    guideLoss_ = 0.0;
+    float                     msTrain_ = 0.0f, msInfer_ = 0.0f;
 };
 
 } // namespace clb

@@ -302,6 +302,90 @@ cl_status cl_dome_build_tables_noalloc(const float* texels, uint32_t width, uint
                                        float* cdfU, float* pV_c, float* cdfV, uint32_t* alias_row,
                                        uint32_t* alias_col, void* stream);
 
+/* ---- Neural path guiding.
+ * No counterpart in the reference (its path tracer samples the BSDF only).
+ * A guiding network maps (position, shading normal, outgoing direction) to a
+ * mixture of CL_GUIDE_LOBES von Mises-Fisher lobes over incident directions:
+ *   position: multiresolution hash grid, CL_GUIDE_LEVELS levels x 2 features,
+ *             2^log2_table bf16 entries per level, trilinear interpolation;
+ *   normal, outgoing direction: one-blob encoding of (theta/pi, phi/2pi+1/2),
+ *             16 Gaussian bins per scalar;
+ *   MLP 96 -> 64 -> 64 -> 64 -> 64 -> 48, ReLU, no biases, BF16 operands
+ *             and FP32 accumulation on the tensor cores;
+ *   head: outputs 5k..5k+4 = (mu_xyz, log kappa, weight logit) of lobe k;
+ *             mu normalised, kappa = exp(clamp(., -5, 7)), softmax weights.
+ * Training minimises the KL divergence to the product f |cos| L_i with
+ * Adam: loss = -sum_s (w_s / sum w) log p(omega_s), w_s = the luminance of
+ * f |cos| L_i / p_sample of the recorded direction.
+ * Parameters (flat FP32, the layout of cl_guide_get_params): the hash table
+ * [level][entry][feature], then W0 (64x96), W1..W3 (64x64), W4 (48x64),
+ * each row-major [out][in].
+ * Record layouts of the host entry points:
+ *   in9:   position in [0,1]^3 (scene box), shading normal, outgoing dir;
+ *   rec13: in9, then the sampled direction omega (3) and the weight w. */
+enum
+{
+    CL_GUIDE_LEVELS  = 16,
+    CL_GUIDE_OUTPUTS = 48,
+    CL_GUIDE_LOBES   = 8
+};
+typedef struct cl_guide cl_guide;
+typedef struct cl_guide_config
+{
+    uint32_t log2_table;                   /* entries per level: 2^log2_table, 8..24 (19) */
+    uint32_t resolutions[CL_GUIDE_LEVELS]; /* per-level grid resolution; all 0: from n_min, n_max */
+    float    n_min, n_max;                 /* coarsest and finest resolution (16, 1024) */
+    float    learning_rate;                /* Adam (1e-2) */
+    float    beta1, beta2, epsilon;        /* (0.9, 0.99, 1e-10) */
+    float    bsdf_fraction;                /* one-sample MIS: probability of BSDF sampling, [0, 1] (0.5) */
+    uint32_t batch;                        /* training samples per step (2^18) */
+    uint32_t train_spp;                    /* one training step after each of the first train_spp spp (32) */
+    uint32_t class_mask;                   /* guided BSDFs: bit 0 diffuse, 1 conductor, 2 dielectric (3) */
+    uint32_t seed;                         /* parameter initialisation */
+} cl_guide_config;
+
+typedef struct cl_guide_stats
+{
+    uint64_t steps;            /* training steps taken */
+    uint64_t samples_trained;  /* training samples consumed */
+    uint64_t records_last;     /* records collected during the last training spp */
+    uint64_t inferred;         /* network evaluations by the integrator */
+    double   last_loss;        /* loss of the last step */
+    float    ms_train;         /* device time of training so far */
+    float    ms_infer;         /* device time of inference (CL_PROFILE_STAGES renders) */
+} cl_guide_stats;
+
+void      cl_guide_default_config(cl_guide_config* config);
+/* Level resolutions floor(n_min * b^l), b = (n_max / n_min)^(1/15) (host only). */
+cl_status cl_guide_default_resolutions(float n_min, float n_max, uint32_t* resolutions16);
+cl_status cl_guide_create(const cl_guide_config* config, cl_guide** out);
+cl_status cl_guide_destroy(cl_guide* guide);
+cl_status cl_guide_param_count(const cl_guide* guide, uint64_t* count);
+cl_status cl_guide_get_resolutions(const cl_guide* guide, uint32_t* resolutions16);
+/* Replaces all parameters and resets Adam's moments and step count. */
+cl_status cl_guide_set_params(cl_guide* guide, const float* params, uint64_t count);
+cl_status cl_guide_get_params(const cl_guide* guide, float* params, uint64_t count);
+/* Raw head outputs (count x 48). */
+cl_status cl_guide_forward(cl_guide* guide, const float* in9, uint32_t count, float* out48);
+/* Loss and gradient (param_count floats) of one batch, parameters unchanged. */
+cl_status cl_guide_gradient(cl_guide* guide, const float* rec13, uint32_t count, double* loss, float* grad);
+/* One Adam step on one batch. */
+cl_status cl_guide_train_step(cl_guide* guide, const float* rec13, uint32_t count, double* loss);
+/* Mixture sampling (u3: lobe, then the two direction uniforms) and pdf. */
+cl_status cl_guide_sample(cl_guide* guide, const float* in9, const float* u3, uint32_t count, float* dir3,
+                          float* pdf);
+cl_status cl_guide_pdf(cl_guide* guide, const float* in9, const float* dir3, uint32_t count, float* pdf);
+
+/* Guided path tracing: the path tracer samples each vertex of a guided class
+ * from the one-sample MIS mixture bsdf_fraction * BSDF + (1 - bsdf_fraction)
+ * * network, trains the network online on the paths it traces, and keeps an
+ * unbiased estimator.  Needs CL_INTEGRATOR_PATH_TRACING and the corrected estimator
+ * (no CL_COMPAT_* flag).  NULL switches guiding off.  Resets the iteration. */
+cl_status cl_integrator_set_guiding(cl_integrator* integrator, const cl_guide_config* config);
+/* The integrator's network (owned by the integrator), or NULL when off. */
+cl_status cl_integrator_get_guide(cl_integrator* integrator, cl_guide** guide);
+cl_status cl_integrator_guide_stats(cl_integrator* integrator, cl_guide_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,7 +9,7 @@ from colvillea_b200 import _native
 
 def declared_functions():
     text = open(_native.HEADER).read()
-    return sorted(set(re.findall(r"\bcl_status\s+(cl_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(?:cl_status|void)\s+(cl_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_header_declares_the_boundary():

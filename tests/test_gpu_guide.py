@@ -1,0 +1,244 @@
+"""Neural path guiding on the GPU against the FP64 oracle (oracle/pyguide.py).
+
+* forward: the tensor-core MLP (BF16 operands, FP32 accumulation) against the
+  oracle with the same BF16 roundings of weights, inputs and activations;
+* gradients (loss, MLP weights, hash table) against the oracle's FP64
+  back-propagation with the same BF16 roundings, and the BF16 error against
+  the unrounded FP64 gradient;
+* Adam's first step; the mixture sampler against its pdf;
+* training on samples of a known distribution, and guided rendering:
+  unbiased against the plain tracer, with per-step training statistics.
+"""
+import numpy as np
+import pytest
+
+import colvillea_b200 as cb
+import pyguide as G
+from colvillea_b200 import scenes
+
+from test_gpu_render import allowed, welch_fail_fraction
+
+pytestmark = pytest.mark.gpu
+
+LOG2T = 14
+
+
+def unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def make_guide(batch=8192, **kw):
+    return cb.Guide.create(cb.GuideConfig(log2_table=LOG2T, batch=batch, n_min=4, n_max=512, **kw))
+
+
+def random_params(g, rng, hash_scale=0.5):
+    p = g.get_params()
+    nh = p.size - G.mlp_param_count()
+    p[:nh] = rng.uniform(-hash_scale, hash_scale, nh)
+    g.set_params(p)
+    return g.get_params().astype(np.float64)
+
+
+def inputs(rng, n):
+    return np.concatenate([rng.uniform(0, 1, (n, 3)), unit(rng, n), unit(rng, n)], 1).astype(np.float32)
+
+
+def split(in9):
+    x = in9.astype(np.float64)
+    return x[:, 0:3], x[:, 3:6], x[:, 6:9]
+
+
+def test_forward_matches_oracle():
+    rng = np.random.default_rng(10)
+    g = make_guide()
+    p = random_params(g, rng)
+    res = g.resolutions()
+    in9 = inputs(rng, 5000)
+    out = g.forward(in9).astype(np.float64)
+    ref = G.network(p, LOG2T, res, *split(in9))
+    err = np.abs(out - ref)
+    scale = np.abs(ref).mean()
+    print(f"[guide] forward: mean |ref| {scale:.4f}, mean err {err.mean():.2e}, p99 {np.quantile(err, 0.99):.2e}, "
+          f"max {err.max():.2e}")
+    # BF16 rounding of hidden activations can flip by one unit where the
+    # FP32 and FP64 sums straddle a rounding boundary; everything else agrees.
+    assert err.mean() < 2e-3 * scale
+    assert np.quantile(err, 0.99) < 2e-2 * scale
+    assert err.max() < 0.1 * scale
+    g.close()
+
+
+def records(rng, n, in9=None):
+    in9 = inputs(rng, n) if in9 is None else in9
+    om = unit(rng, n)
+    w = rng.uniform(0.1, 2.0, n)
+    return np.concatenate([in9, om, w[:, None]], 1).astype(np.float32)
+
+
+def oracle_grads(p, res, rec):
+    x = rec.astype(np.float64)
+    return G.loss_and_grads(p, LOG2T, res, x[:, 0:3], x[:, 3:6], x[:, 6:9], x[:, 9:12], x[:, 12])
+
+
+def test_gradient_matches_oracle():
+    rng = np.random.default_rng(11)
+    g = make_guide()
+    p = random_params(g, rng, hash_scale=0.3)
+    res = g.resolutions()
+    rec = records(rng, 4096)
+    loss, grad = g.gradient(rec)
+    loss_ref, grad_ref = oracle_grads(p, res, rec)
+    G.ROUND_BF16 = False
+    try:
+        _, grad_fp64 = oracle_grads(p, res, rec)
+    finally:
+        G.ROUND_BF16 = True
+    nh = p.size - G.mlp_param_count()
+    print(f"[guide] loss gpu {loss:.6f} oracle {loss_ref:.6f}")
+    assert abs(loss - loss_ref) < 1e-3 * abs(loss_ref) + 1e-5
+    blocks = [("hash", slice(0, nh))]
+    off = nh
+    for l, (o, i) in enumerate(G.LAYERS):
+        blocks.append((f"W{l}", slice(off, off + o * i)))
+        off += o * i
+    # Tolerances: against the oracle with the same BF16 roundings the GPU
+    # differs only by FP32-vs-FP64 summation (and the rare BF16 rounding flip
+    # it causes): 2% in norm.  Against the unrounded FP64 gradient the error
+    # is BF16's own - on random directions the batch gradient is a sum of
+    # largely cancelling per-sample terms, so 2^-9 roundings grow to several
+    # per cent - and the GPU may not exceed the BF16 oracle's own error by
+    # more than 25% + 0.5%.
+    for name, sl in blocks:
+        a, b, c = grad[sl].astype(np.float64), grad_ref[sl], grad_fp64[sl]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        rel64 = np.linalg.norm(a - c) / np.linalg.norm(c)
+        relB = np.linalg.norm(b - c) / np.linalg.norm(c)
+        cos = np.dot(a, c) / (np.linalg.norm(a) * np.linalg.norm(c))
+        print(f"[guide] grad {name}: rel err vs BF16 oracle {rel:.2e}, vs FP64 {rel64:.2e} (BF16 oracle vs FP64 "
+              f"{relB:.2e}), cosine vs FP64 {cos:.6f}")
+        assert rel < 2e-2, name
+        assert rel64 < 1.25 * relB + 5e-3 and cos > 0.99, name
+    g.close()
+
+
+def test_adam_first_step():
+    rng = np.random.default_rng(12)
+    g = make_guide()
+    p0 = random_params(g, rng, hash_scale=0.3)
+    rec = records(rng, 2048)
+    _, grad = g.gradient(rec)
+    g.train_step(rec)
+    p1 = g.get_params().astype(np.float64)
+    gr = grad.astype(np.float64)
+    lr, eps = 1e-2, 1e-10
+    # step 1: m_hat = g, v_hat = g^2, so the update is lr g / (|g| + eps)
+    big = np.abs(gr) > 1e-4 * np.abs(gr).max()
+    exp = p0 - lr * gr / (np.abs(gr) + eps)
+    np.testing.assert_allclose(p1[big], exp[big], rtol=0, atol=2e-6)
+    assert np.all(p1[gr == 0] == p0[gr == 0])
+    g.close()
+
+
+def test_sampler_and_pdf():
+    rng = np.random.default_rng(13)
+    g = make_guide()
+    p = random_params(g, rng)
+    rows = inputs(rng, 4)
+    n = 50000
+    in9 = np.repeat(rows, n, 0)
+    d, pdf = g.sample(in9, rng.uniform(size=(len(in9), 3)))
+    out = g.forward(rows).astype(np.float64)
+    np.testing.assert_allclose(np.linalg.norm(d, axis=1), 1, atol=2e-6)
+    ref = G.mixture_pdf(np.repeat(out, n, 0), d.astype(np.float64))
+    np.testing.assert_allclose(pdf, ref, rtol=2e-4)
+    for r in range(4):
+        inv = 1.0 / pdf[r * n:(r + 1) * n].astype(np.float64)
+        assert abs(inv.mean() - 4 * np.pi) < 5 * inv.std() / np.sqrt(n) + 1e-3
+    dirs = unit(rng, len(in9)).astype(np.float32)
+    pg = g.pdf(in9, dirs)
+    np.testing.assert_allclose(pg, G.mixture_pdf(np.repeat(out, n, 0), dirs.astype(np.float64)), rtol=2e-4)
+    g.close()
+
+
+def vmf_samples(rng, mu, kappa):
+    n = len(mu)
+    u1, u2 = rng.uniform(size=n), rng.uniform(size=n)
+    w = 1 + np.log(u1 + (1 - u1) * np.exp(-2 * kappa)) / kappa
+    s = np.sqrt(np.maximum(0, 1 - w * w))
+    t, b = G.basis(mu)
+    ph = 2 * np.pi * u2
+    return w[:, None] * mu + s[:, None] * (np.cos(ph)[:, None] * t + np.sin(ph)[:, None] * b)
+
+
+def target_mu(pos):
+    m = np.stack([np.cos(4 * pos[:, 0]), np.sin(4 * pos[:, 0]), 2 * pos[:, 1] - 1], 1)
+    return m / np.linalg.norm(m, axis=1, keepdims=True)
+
+
+def test_training_learns_a_distribution():
+    """Samples of a position-dependent vMF (kappa 20): the trained mixture's
+    held-out log-likelihood approaches the target's (log(20/2pi) - 1 = 0.16)
+    from the untrained network's (about log(1/4pi) = -2.5)."""
+    rng = np.random.default_rng(14)
+    g = make_guide(batch=16384)
+    kappa = 20.0
+
+    def batch(n):
+        in9 = inputs(rng, n)
+        om = vmf_samples(rng, target_mu(in9[:, :3].astype(np.float64)), kappa)
+        return np.concatenate([in9, om, np.ones((n, 1))], 1).astype(np.float32)
+
+    held = batch(8192)
+
+    def loglik():
+        out = g.forward(held[:, :9]).astype(np.float64)
+        return float(np.mean(G.log_pdf(out, held[:, 9:12].astype(np.float64))[0]))
+
+    l0 = loglik()
+    losses = [g.train_step(batch(16384)) for _ in range(300)]
+    l1 = loglik()
+    print(f"[guide] held-out log-likelihood {l0:.3f} -> {l1:.3f} (target 0.159); "
+          f"loss {losses[0]:.3f} -> {np.mean(losses[-20:]):.3f}")
+    assert l0 < -2.0
+    assert l1 > -0.6
+    assert np.mean(losses[-20:]) < losses[0] - 2.0
+    g.close()
+
+
+def test_guided_integrator_api_errors():
+    s = scenes.config1(0, 32, 32)
+    dl = cb.load_scene(s, itype=cb.IntegratorType.WavefrontDirectLighting, flags=cb.DOME_ALIAS)
+    with pytest.raises(cb.ClError):
+        dl.setGuiding(cb.GuideConfig(log2_table=12))
+    dl.close()
+    comp = cb.load_scene(s, flags=cb.COMPAT_ALL)
+    with pytest.raises(cb.ClError):
+        comp.setGuiding(cb.GuideConfig(log2_table=12))
+    assert comp.guide() is None
+    comp.close()
+
+
+def test_guided_render_is_unbiased():
+    """Guided path tracing (online training for the first 16 spp) against the
+    plain tracer with the same corrected estimator: per-pixel Welch tests."""
+    s = scenes.config1(0, 96, 96)
+    spp_g, spp_p = 128, 512
+    it = cb.load_scene(s, flags=cb.DOME_ALIAS | cb.FILM_FP64)
+    it.setGuiding(cb.GuideConfig(log2_table=16, batch=1 << 14, train_spp=16, class_mask=7))
+    it.render(spp_g)
+    g1, g2 = it.readbackFilmStats()
+    gs = it.guideStats()
+    it.close()
+    ref = cb.load_scene(s, flags=cb.DOME_ALIAS | cb.FILM_FP64)
+    ref.render(spp_p)
+    r1, r2 = ref.readbackFilmStats()
+    ref.close()
+    frac = welch_fail_fraction(g1, g2, spp_g, r1, r2, spp_p)
+    gm, rm = g1.mean() / spp_g, r1.mean() / spp_p
+    print(f"[guide] render: Welch fail {frac:.4f} (allowed {allowed(g1.size):.4f}); mean guided {gm:.5f} "
+          f"plain {rm:.5f}; stats {gs}")
+    assert gs["steps"] == 16 and gs["records_last"] > 1000 and gs["inferred"] > 0
+    assert np.isfinite(gs["last_loss"])
+    assert frac <= allowed(g1.size)
+    assert abs(gm - rm) / rm < 5e-3
