@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--profile", type=int, default=0, metavar="SPP",
                     help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
+    ap.add_argument("--no-relmse", action="store_true", help="skip the guided-vs-plain equal-time relMSE")
+    ap.add_argument("--relmse-ref-spp", type=int, default=8192, help="spp of the FP64 reference image")
+    ap.add_argument("--relmse-seeds", type=int, default=3)
+    ap.add_argument("--relmse-spp", type=int, default=128, help="guided spp (training included)")
     return ap.parse_args()
 
 
@@ -189,6 +193,35 @@ def cpu_baseline(scene, seconds, threads):
     return {"value": round(len(pix) / dt / 1e6, 6), "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{len(pix)} of {npx} pixels (evenly strided), 1 spp, {dt:.1f} s; "
                       f"{int(cnt[0])} closest + {int(cnt[1])} shadow rays ({(cnt[0] + cnt[1]) / dt / 1e6:.3f} Mrays/s)"}
+
+
+def guided_relmse(args):
+    """Second half of the metric: equal-time relMSE of neural-guided vs plain
+    path tracing against an FP64-accumulated plain reference, on cfg3 (the
+    cfg1 scene at 1920x1080, 128 guided spp including online training: one
+    Adam step on 2^18 records after each of the first 32 spp)."""
+    import colvillea_b200 as cb
+    from colvillea_b200 import evaluate, scenes
+    s = scenes.config3(0)
+    t0 = time.perf_counter()
+    ref = evaluate.reference(s, args.relmse_ref_spp)
+    t_ref = time.perf_counter() - t0
+    guide = cb.GuideConfig()
+    r = evaluate.equal_time(s, ref, args.relmse_spp, seeds=args.relmse_seeds, guide=guide)
+    mlp = evaluate.mlp_throughput(s, guide)
+    peak = None
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        peak = float(json.load(open(p)).get("bf16_tflops", 0)) or None
+    rnd = lambda v: [round(x, 6) for x in v] if isinstance(v, list) else (round(v, 6) if isinstance(v, float) else v)
+    return {"workload": f"cfg3: cfg1 scene (10,242 tris) at {s.width}x{s.height}, max depth {s.max_depth}, RR from "
+                        f"{s.rr_start}; guided {args.relmse_spp} spp incl. training ({guide.train_spp} Adam steps, "
+                        f"batch {guide.batch}, lr {guide.learning_rate:g}, BSDF fraction {guide.bsdf_fraction:g}, "
+                        f"guided classes mask {guide.class_mask}); plain at the same device time",
+            "reference": f"plain, corrected estimator, {args.relmse_ref_spp} spp, FP64 film ({t_ref:.1f} s)",
+            **{k: rnd(v) for k, v in r.items()},
+            "mlp": {**{k: rnd(v) for k, v in mlp.items()}, "bf16_peak_tflops": peak,
+                    "infer_frac_of_peak": round(mlp["infer_tflops"] / peak, 4) if peak and mlp["infer_tflops"] else None}}
 
 
 def run_reference(args):
@@ -346,6 +379,8 @@ def main():
         line["e2e"] = e2e
     if dist.world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(s, args.cpu_seconds, os.cpu_count() or 1)
+    if dist.world == 1 and not args.no_relmse:
+        line["relmse"] = guided_relmse(args)
     print(json.dumps(line))
     dist.close()
     return 0

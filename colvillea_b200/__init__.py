@@ -126,6 +126,10 @@ class Integrator:
         N.call("cl_get_film_size", self._h, ctypes.byref(w), ctypes.byref(h))
         return w.value, h.value
 
+    def setIterationIndex(self, iteration):
+        """Clear the film and continue from progressive frame `iteration`."""
+        N.call("cl_set_iteration", self._h, int(iteration))
+
     def resetIterationIndex(self):
         N.call("cl_reset_iteration", self._h)
 
@@ -253,17 +257,20 @@ class Guide:
         N.call("cl_guide_forward", self._h, _ptr(in9), len(in9), _ptr(out))
         return out
 
-    def gradient(self, rec13):
-        rec13 = _f32(rec13)
+    def gradient(self, rec14):
+        """rec14 rows: position, normal, wo, omega, weight, BSDF pdf of omega."""
+        rec14 = _f32(rec14)
+        assert rec14.ndim == 2 and rec14.shape[1] == 14
         g = np.zeros(self.param_count(), np.float32)
         loss = ctypes.c_double()
-        N.call("cl_guide_gradient", self._h, _ptr(rec13), len(rec13), ctypes.byref(loss), _ptr(g))
+        N.call("cl_guide_gradient", self._h, _ptr(rec14), len(rec14), ctypes.byref(loss), _ptr(g))
         return loss.value, g
 
-    def train_step(self, rec13):
-        rec13 = _f32(rec13)
+    def train_step(self, rec14):
+        rec14 = _f32(rec14)
+        assert rec14.ndim == 2 and rec14.shape[1] == 14
         loss = ctypes.c_double()
-        N.call("cl_guide_train_step", self._h, _ptr(rec13), len(rec13), ctypes.byref(loss))
+        N.call("cl_guide_train_step", self._h, _ptr(rec14), len(rec14), ctypes.byref(loss))
         return loss.value
 
     def sample(self, in9, u3):

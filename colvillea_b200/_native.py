@@ -74,7 +74,8 @@ class GuideConfig(ctypes.Structure):
     _fields_ = [("log2_table", u32), ("resolutions", u32 * 16), ("n_min", ctypes.c_float), ("n_max", ctypes.c_float),
                 ("learning_rate", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
                 ("epsilon", ctypes.c_float), ("bsdf_fraction", ctypes.c_float), ("batch", u32),
-                ("train_spp", u32), ("class_mask", u32), ("seed", u32)]
+                ("train_spp", u32), ("class_mask", u32), ("seed", u32), ("learn_selection", u32),
+                ("weight_clamp", ctypes.c_float)]
 
 
 class GuideStats(ctypes.Structure):
@@ -101,6 +102,7 @@ _SIGS = {
     "cl_resize": [vp, u32, u32],
     "cl_get_film_size": [vp, ctypes.POINTER(u32), ctypes.POINTER(u32)],
     "cl_reset_iteration": [vp],
+    "cl_set_iteration": [vp, u32],
     "cl_get_stats": [vp, ctypes.POINTER(Stats)],
     "cl_last_error": [ctypes.c_char_p, ctypes.c_size_t],
     "cl_trace_rays": [vp, vp, u32, vp, vp, vp, vp],

@@ -193,6 +193,12 @@ cl_status cl_reset_iteration(cl_integrator* it)
     return guarded([&](std::string* e) { return it->impl.resetIteration(e); });
 }
 
+cl_status cl_set_iteration(cl_integrator* it, uint32_t iteration)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.setIteration(iteration, e); });
+}
+
 cl_status cl_get_stats(cl_integrator* it, cl_stats* stats)
 {
     CL_NEED(it);
@@ -415,16 +421,16 @@ cl_status cl_guide_forward(cl_guide* guide, const float* in9, uint32_t count, fl
     return guarded([&](std::string* e) { return guide->net->forward(in9, count, out48, e); });
 }
 
-cl_status cl_guide_gradient(cl_guide* guide, const float* rec13, uint32_t count, double* loss, float* grad)
+cl_status cl_guide_gradient(cl_guide* guide, const float* rec14, uint32_t count, double* loss, float* grad)
 {
     CL_NEED(guide);
-    return guarded([&](std::string* e) { return guide->net->gradient(rec13, count, loss, grad, e); });
+    return guarded([&](std::string* e) { return guide->net->gradient(rec14, count, loss, grad, e); });
 }
 
-cl_status cl_guide_train_step(cl_guide* guide, const float* rec13, uint32_t count, double* loss)
+cl_status cl_guide_train_step(cl_guide* guide, const float* rec14, uint32_t count, double* loss)
 {
     CL_NEED(guide);
-    return guarded([&](std::string* e) { return guide->net->trainStepHost(rec13, count, loss, e); });
+    return guarded([&](std::string* e) { return guide->net->trainStepHost(rec14, count, loss, e); });
 }
 
 cl_status cl_guide_sample(cl_guide* guide, const float* in9, const float* u3, uint32_t count, float* dir3, float* pdf)

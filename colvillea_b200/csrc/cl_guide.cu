@@ -170,8 +170,17 @@ struct TrainArgs
     float2*        gradTable;
     __nv_bfloat16* acts;
     __nv_bfloat16* deltas;
-    double*        scal; // [0] sum of weights, [1] loss
+    double*        scal; // [0] sum of weights, [1] loss, [3] sum of clamped weights
+    int            learnSel;
+    float          clamp;    // weight clamp (x batch mean), 0 = off
 };
+
+// Training weight of a record: clamped to clamp x the batch mean when set.
+__device__ __forceinline__ float trainWeight(float w, const TrainArgs& a, uint32_t nB)
+{
+    if (a.clamp > 0.0f && nB > 0u) w = fminf(w, a.clamp * float(a.scal[0] / double(nB)));
+    return w;
+}
 
 // A step trains on B = min(count, batch) samples; when more records were
 // collected, sample j takes record floor(j * count / B) (an even subsample).
@@ -180,13 +189,18 @@ __device__ __forceinline__ uint32_t recordOf(uint32_t j, uint32_t count, uint32_
     return count > nB ? uint32_t(uint64_t(j) * count / nB) : j;
 }
 
-__global__ void kTrainPrep(TrainArgs a)
+// Sum of the batch's weights into scal[slot] (slot 0: raw; slot 3: clamped,
+// after slot 0 is complete).
+__global__ void kTrainPrep(TrainArgs a, int slot)
 {
     __shared__ double part[32];
     const uint32_t count = *a.count, nB = min(count, a.batch);
     double         s     = 0.0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < nB; j += gridDim.x * blockDim.x)
-        s += double(a.rec[kRecordF4 * size_t(recordOf(j, count, nB))].w);
+    {
+        float w = a.rec[kRecordF4 * size_t(recordOf(j, count, nB))].w;
+        s += double(slot ? trainWeight(w, a, nB) : w);
+    }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (laneIdx() == 0) part[threadIdx.x >> 5] = s;
     __syncthreads();
@@ -194,7 +208,7 @@ __global__ void kTrainPrep(TrainArgs a)
     {
         double t = 0.0;
         for (int w = 0; w < int(blockDim.x >> 5); ++w) t += part[w];
-        if (t != 0.0) atomicAdd(&a.scal[0], t);
+        if (t != 0.0) atomicAdd(&a.scal[slot], t);
     }
 }
 
@@ -347,7 +361,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
     loadFrags(wb, a.wb, kBwdFrags * 32);
     __syncthreads();
     const uint32_t count = *a.count, nB = min(count, a.batch);
-    const double   wsum  = a.scal[0];
+    const double   wsum  = a.clamp > 0.0f ? a.scal[3] : a.scal[0];
     const float    invW  = wsum > 0.0 ? float(1.0 / wsum) : 0.0f;
     const uint32_t g = lane >> 2, t = lane & 3u, r = lane & 15u, half = lane >> 4;
     for (uint32_t tile = blockIdx.x * kTrainWarps + warp; tile * 16u < nB; tile += gridDim.x * kTrainWarps)
@@ -409,7 +423,22 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
                 float4 r0 = R[0], r3 = R[3];
                 float  gr[kOut];
                 float  lp = headLossGrad(o + lane * kOS, f3{r3.x, r3.y, r3.z}, gr);
-                float  s  = -r0.w * invW;
+                if (a.learnSel)
+                {
+                    // -log((1 - a) p_bsdf + a p_guide): lobe gradients scaled
+                    // by a p_guide / p_mix, selection logit (p_g - p_b) / p_mix da.
+                    const float x   = o[lane * kOS + kSelOut];
+                    const float sg  = 1.0f / (1.0f + expf(-x));
+                    const float al  = kSelMin + (kSelMax - kSelMin) * sg;
+                    const float pg  = expf(lp), pb = r3.w;
+                    const float pm  = fmaxf((1.0f - al) * pb + al * pg, 1e-30f);
+                    const float sc  = al * pg / pm;
+#pragma unroll
+                    for (int c = 0; c < 5 * kLobes; ++c) gr[c] *= sc;
+                    gr[kSelOut] = (pg - pb) / pm * (kSelMax - kSelMin) * sg * (1.0f - sg);
+                    lp          = logf(pm);
+                }
+                float  s  = -trainWeight(r0.w, a, nB) * invW;
                 lossPart  = s * lp;
 #pragma unroll
                 for (int c = 0; c < kOut / 2; ++c) drow[c] = packBf16(gr[2 * c] * s, gr[2 * c + 1] * s);
@@ -555,24 +584,49 @@ __global__ void __launch_bounds__(128) kWeightGrad(const __nv_bfloat16* __restri
     }
 }
 
-// Adam (FP32 master parameters); clears the gradient it consumed and
-// refreshes the bf16 copy of the hash table.
-__global__ void kAdam(float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m, float* __restrict__ v,
-                      uint64_t n, uint64_t hashN, float lr, float b1, float b2, float eps, float c1, float c2,
-                      __nv_bfloat16* __restrict__ table)
+// Adam (FP32 master parameters) over float4 groups - the hash block and
+// every weight block hold multiples of 4 floats - with two groups in flight
+// per thread; clears the gradient it consumed and refreshes the bf16 copy
+// of the hash table.  a = lr / (1 - beta1^t), ic2 = 1 / (1 - beta2^t).
+struct AdamK
 {
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+    float b1, b2, eps, a, ic2;
+};
+__device__ __forceinline__ float adam1(float p, float& m, float& v, float g, const AdamK& k)
+{
+    m = k.b1 * m + (1.0f - k.b1) * g;
+    v = k.b2 * v + (1.0f - k.b2) * g * g;
+    return p - __fdividef(k.a * m, sqrtf(v * k.ic2) + k.eps);
+}
+__device__ __forceinline__ void adam4(float4* __restrict__ p, float4* __restrict__ grad, float4* __restrict__ m,
+                                      float4* __restrict__ v, uint2* __restrict__ table, uint64_t i, uint64_t hash4,
+                                      float4 g, float4 mi, float4 vi, float4 pi, const AdamK& k)
+{
+    pi.x = adam1(pi.x, mi.x, vi.x, g.x, k);
+    pi.y = adam1(pi.y, mi.y, vi.y, g.y, k);
+    pi.z = adam1(pi.z, mi.z, vi.z, g.z, k);
+    pi.w = adam1(pi.w, mi.w, vi.w, g.w, k);
+    grad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    m[i]    = mi;
+    v[i]    = vi;
+    p[i]    = pi;
+    if (i < hash4) table[i] = make_uint2(packBf16(pi.x, pi.y), packBf16(pi.z, pi.w));
+}
+__global__ void __launch_bounds__(256) kAdam(float4* __restrict__ p, float4* __restrict__ grad,
+                                             float4* __restrict__ m, float4* __restrict__ v, uint64_t n4,
+                                             uint64_t hash4, AdamK k, uint2* __restrict__ table)
+{
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    uint64_t       i      = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+    for (; i + stride < n4; i += 2 * stride)
     {
-        float gi = grad[i];
-        grad[i]  = 0.0f;
-        float mi = b1 * m[i] + (1.0f - b1) * gi;
-        float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-        m[i]     = mi;
-        v[i]     = vi;
-        float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
-        p[i]     = pi;
-        if (i < hashN) table[i] = __float2bfloat16_rn(pi);
+        const uint64_t j  = i + stride;
+        float4         g0 = grad[i], m0 = m[i], v0 = v[i], p0 = p[i];
+        float4         g1 = grad[j], m1 = m[j], v1 = v[j], p1 = p[j];
+        adam4(p, grad, m, v, table, i, hash4, g0, m0, v0, p0, k);
+        adam4(p, grad, m, v, table, j, hash4, g1, m1, v1, p1, k);
     }
+    if (i < n4) adam4(p, grad, m, v, table, i, hash4, grad[i], m[i], v[i], p[i], k);
 }
 
 int gridFor(uint64_t n, int block, int cap)
@@ -601,6 +655,8 @@ void guideDefaultConfig(cl_guide_config* c)
     c->train_spp     = 32;
     c->class_mask    = 3u;
     c->seed          = 1;
+    c->learn_selection = 0u;
+    c->weight_clamp    = 0.0f;
 }
 
 cl_status guideResolutions(float nmin, float nmax, uint32_t* res)
@@ -624,7 +680,8 @@ cl_status GuideNet::init(cudaStream_t st, std::string* err)
     }
     if (cfg_.batch == 0 || cfg_.batch > (1u << 24) || !(cfg_.learning_rate > 0.0f) || !(cfg_.bsdf_fraction >= 0.0f) ||
         !(cfg_.bsdf_fraction <= 1.0f) || !(cfg_.beta1 >= 0.0f && cfg_.beta1 < 1.0f) ||
-        !(cfg_.beta2 >= 0.0f && cfg_.beta2 < 1.0f) || !(cfg_.epsilon >= 0.0f))
+        !(cfg_.beta2 >= 0.0f && cfg_.beta2 < 1.0f) || !(cfg_.epsilon >= 0.0f) || cfg_.learn_selection > 1u ||
+        !(cfg_.weight_clamp >= 0.0f))
     {
         *err = "guide: batch, learning rate, Adam or bsdf_fraction out of range";
         return CL_ERR_INVALID_ARG;
@@ -804,10 +861,10 @@ cl_status GuideNet::pdf(const float* in9, const float* dir, uint32_t n, float* p
     return CL_OK;
 }
 
-// rec13 rows -> device records; the record count goes to scal[2] (u32).
-cl_status GuideNet::upload(const float* rec13, uint32_t n, std::string* err)
+// rec14 rows -> device records; the record count goes to scal[2] (u32).
+cl_status GuideNet::upload(const float* rec14, uint32_t n, std::string* err)
 {
-    if (!rec13 || n == 0)
+    if (!rec14 || n == 0)
     {
         *err = "guide: empty or null batch";
         return CL_ERR_INVALID_ARG;
@@ -815,12 +872,12 @@ cl_status GuideNet::upload(const float* rec13, uint32_t n, std::string* err)
     std::vector<float> h(size_t(n) * 16, 0.0f);
     for (uint32_t i = 0; i < n; ++i)
     {
-        const float* s = rec13 + 13 * size_t(i);
+        const float* s = rec14 + 14 * size_t(i);
         float*       d = h.data() + 16 * size_t(i);
         d[0] = s[0], d[1] = s[1], d[2] = s[2], d[3] = s[12];
         d[4] = s[3], d[5] = s[4], d[6] = s[5];
         d[8] = s[6], d[9] = s[7], d[10] = s[8];
-        d[12] = s[9], d[13] = s[10], d[14] = s[11];
+        d[12] = s[9], d[13] = s[10], d[14] = s[11], d[15] = s[13];
     }
     CL_TRY(rec_.alloc(h.size() * 4, err));
     CL_CUDA(cudaMemcpyAsync(rec_.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st_), err);
@@ -832,6 +889,7 @@ cl_status GuideNet::upload(const float* rec13, uint32_t n, std::string* err)
 cl_status GuideNet::computeGradient(const float4* rec, const uint32_t* count, std::string* err)
 {
     CL_CUDA(cudaMemsetAsync(scal_.p, 0, 16, st_), err);
+    CL_CUDA(cudaMemsetAsync(scal_.as<double>() + 3, 0, 8, st_), err);
     TrainArgs a;
     a.rec       = rec;
     a.count     = count;
@@ -843,8 +901,15 @@ cl_status GuideNet::computeGradient(const float4* rec, const uint32_t* count, st
     a.acts      = acts_.as<__nv_bfloat16>();
     a.deltas    = deltas_.as<__nv_bfloat16>();
     a.scal      = scal_.as<double>();
-    kTrainPrep<<<numSMs_ * 2, 256, 0, st_>>>(a);
+    a.learnSel  = cfg_.learn_selection ? 1 : 0;
+    a.clamp     = cfg_.weight_clamp;
+    kTrainPrep<<<numSMs_ * 2, 256, 0, st_>>>(a, 0);
     CL_CUDA(cudaGetLastError(), err);
+    if (a.clamp > 0.0f)
+    {
+        kTrainPrep<<<numSMs_ * 2, 256, 0, st_>>>(a, 3);
+        CL_CUDA(cudaGetLastError(), err);
+    }
     kTrainFwdBwd<<<trainBlocks_, kTrainWarps * 32, kTrainSmem, st_>>>(a);
     CL_CUDA(cudaGetLastError(), err);
     dim3 gg((cfg_.batch + kGradChunk - 1) / kGradChunk, kLayers);
@@ -860,10 +925,11 @@ cl_status GuideNet::trainDevice(const float4* rec, const uint32_t* count, std::s
     ++step_;
     const float c1 = float(1.0 - std::pow(double(cfg_.beta1), double(step_)));
     const float c2 = float(1.0 - std::pow(double(cfg_.beta2), double(step_)));
-    const uint64_t n = paramCount();
-    kAdam<<<gridFor(n, 256, numSMs_ * 16), 256, 0, st_>>>(params_.f(), grad_.f(), m_.f(), v_.f(), n, hashParams_,
-                                                         cfg_.learning_rate, cfg_.beta1, cfg_.beta2, cfg_.epsilon, c1,
-                                                         c2, table_.as<__nv_bfloat16>());
+    const uint64_t n4 = paramCount() / 4;
+    AdamK          k{cfg_.beta1, cfg_.beta2, cfg_.epsilon, cfg_.learning_rate / c1, 1.0f / c2};
+    kAdam<<<gridFor(n4 / 2, 256, numSMs_ * 8), 256, 0, st_>>>(params_.as<float4>(), grad_.as<float4>(),
+                                                              m_.as<float4>(), v_.as<float4>(), n4, hashParams_ / 4, k,
+                                                              table_.as<uint2>());
     CL_CUDA(cudaGetLastError(), err);
     kFrags<<<((kFwdFrags + kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
                                                                          wb_.as<uint2>());
@@ -871,14 +937,14 @@ cl_status GuideNet::trainDevice(const float4* rec, const uint32_t* count, std::s
     return CL_OK;
 }
 
-cl_status GuideNet::gradient(const float* rec13, uint32_t n, double* loss, float* grad, std::string* err)
+cl_status GuideNet::gradient(const float* rec14, uint32_t n, double* loss, float* grad, std::string* err)
 {
     if (!grad || !loss)
     {
         *err = "guide: null output";
         return CL_ERR_INVALID_ARG;
     }
-    CL_TRY(upload(rec13, n, err));
+    CL_TRY(upload(rec14, n, err));
     const uint32_t* cnt = reinterpret_cast<const uint32_t*>(scal_.as<unsigned char>() + 16);
     CL_TRY(computeGradient(rec_.as<const float4>(), cnt, err));
     CL_CUDA(cudaMemcpyAsync(grad, grad_.p, paramCount() * 4, cudaMemcpyDeviceToHost, st_), err);
@@ -888,9 +954,9 @@ cl_status GuideNet::gradient(const float* rec13, uint32_t n, double* loss, float
     return CL_OK;
 }
 
-cl_status GuideNet::trainStepHost(const float* rec13, uint32_t n, double* loss, std::string* err)
+cl_status GuideNet::trainStepHost(const float* rec14, uint32_t n, double* loss, std::string* err)
 {
-    CL_TRY(upload(rec13, n, err));
+    CL_TRY(upload(rec14, n, err));
     const uint32_t* cnt = reinterpret_cast<const uint32_t*>(scal_.as<unsigned char>() + 16);
     CL_TRY(trainDevice(rec_.as<const float4>(), cnt, err));
     if (loss) CL_CUDA(cudaMemcpyAsync(loss, scal_.as<double>() + 1, 8, cudaMemcpyDeviceToHost, st_), err);

@@ -26,6 +26,8 @@ constexpr int kXS = 104; // encoded-input tile row stride (bf16): 208 B, conflic
 constexpr int kOS = 49;  // output tile row stride (f32)
 constexpr int kDS = 56;  // output-gradient tile row stride (bf16): 112 B
 constexpr float kKappaMin = -5.0f, kKappaMax = 7.0f;
+constexpr float kSelMin = 0.05f, kSelMax = 0.95f; // learned guide-selection probability range
+constexpr int   kSelOut = 5 * kLobes;           // head output of its logit
 
 // Layer l: W_l is [out][in] row-major inside the flat MLP parameter block.
 __host__ __device__ constexpr int layerIn(int l) { return l == 0 ? kIn : kWidth; }
@@ -137,6 +139,23 @@ __device__ __forceinline__ void oneBlob(f3 d, __nv_bfloat16* dst)
         float a  = th - c, b = ph - c;
         dst[i]         = __float2bfloat16_rn(expf(-a * a * 128.0f));
         dst[kBlob + i] = __float2bfloat16_rn(expf(-b * b * 128.0f));
+    }
+}
+
+// The same encoding as 16 packed bf16 pairs (register-resident rows).
+__device__ __forceinline__ void oneBlobPacked(f3 d, uint32_t* dst)
+{
+    float th = acosf(fminf(fmaxf(d.z, -1.0f), 1.0f)) * kInvPi;
+    float ph = atan2f(d.y, d.x) * (0.5f * kInvPi) + 0.5f;
+#pragma unroll
+    for (int i = 0; i < kBlob; i += 2)
+    {
+        float c0 = (float(i) + 0.5f) * (1.0f / kBlob), c1 = (float(i) + 1.5f) * (1.0f / kBlob);
+        float a0 = th - c0, a1 = th - c1, b0 = ph - c0, b1 = ph - c1;
+        __nv_bfloat162 t = __floats2bfloat162_rn(expf(-a0 * a0 * 128.0f), expf(-a1 * a1 * 128.0f));
+        __nv_bfloat162 u = __floats2bfloat162_rn(expf(-b0 * b0 * 128.0f), expf(-b1 * b1 * 128.0f));
+        dst[i / 2]             = *reinterpret_cast<uint32_t*>(&t);
+        dst[(kBlob + i) / 2]   = *reinterpret_cast<uint32_t*>(&u);
     }
 }
 
@@ -361,13 +380,20 @@ __device__ __forceinline__ void storeOut(const float (&out)[MT][6][4], float* ti
 struct Lobes
 {
     float4 l[kLobes]; // {mu.xyz, kappa}
-    float  w[kLobes]; // normalised weights
+    float  w[kLobes]; // weights; they sum to the probability of sampling the guide
 };
 
-// Lobe parameters from the 40 used head outputs o[5k..5k+4] = (mu_xyz, log
-// kappa, weight logit).
-__device__ __forceinline__ void headLobes(const float* o, Lobes* L)
+__device__ __forceinline__ float selectionProb(float logit)
 {
+    return kSelMin + (kSelMax - kSelMin) / (1.0f + expf(-logit));
+}
+
+// Lobe parameters from the head outputs o[5k..5k+4] = (mu_xyz, log kappa,
+// weight logit); the weights are normalised to `alpha`, the probability of
+// sampling the guide (alpha < 0: learned, from output 40).
+__device__ __forceinline__ void headLobes(const float* o, Lobes* L, float alpha = 1.0f)
+{
+    if (alpha < 0.0f) alpha = selectionProb(o[kSelOut]);
     float mx = -FLT_MAX;
 #pragma unroll
     for (int k = 0; k < kLobes; ++k) mx = fmaxf(mx, o[5 * k + 4]);
@@ -379,7 +405,7 @@ __device__ __forceinline__ void headLobes(const float* o, Lobes* L)
         L->w[k] = e;
         s += e;
     }
-    const float inv = 1.0f / s;
+    const float inv = alpha / s;
 #pragma unroll
     for (int k = 0; k < kLobes; ++k)
     {
@@ -416,7 +442,8 @@ __device__ __forceinline__ void onb(f3 n, f3* t, f3* b)
     *b         = {bb, sign + n.y * n.y * a, -n.y};
 }
 
-// Lobe by u0 over the weights' CDF; direction by Jakob's inversion (2012):
+// Lobe by u0 in [0, sum of weights) over the weights' CDF; direction by
+// Jakob's inversion (2012):
 // w = 1 + log(u1 + (1 - u1) e^{-2 kappa}) / kappa, phi = 2 pi u2.
 __device__ __forceinline__ f3 mixtureSample(const Lobes& L, float u0, float u1, float u2)
 {

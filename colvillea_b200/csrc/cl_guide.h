@@ -8,7 +8,7 @@
 namespace clb
 {
 // One training record in device memory (4 float4):
-// {p.xyz in [0,1]^3, w} {n.xyz, -} {wo.xyz, -} {omega.xyz, -}.
+// {p.xyz in [0,1]^3, w} {n.xyz, -} {wo.xyz, -} {omega.xyz, BSDF pdf of omega}.
 constexpr int kRecordF4 = 4;
 
 class GuideNet
@@ -26,8 +26,8 @@ public:
     cl_status setParams(const float* p, uint64_t n, std::string* err);
     cl_status getParams(float* p, uint64_t n, std::string* err);
     cl_status forward(const float* in9, uint32_t n, float* out48, std::string* err);
-    cl_status gradient(const float* rec13, uint32_t n, double* loss, float* grad, std::string* err);
-    cl_status trainStepHost(const float* rec13, uint32_t n, double* loss, std::string* err);
+    cl_status gradient(const float* rec14, uint32_t n, double* loss, float* grad, std::string* err);
+    cl_status trainStepHost(const float* rec14, uint32_t n, double* loss, std::string* err);
     cl_status sample(const float* in9, const float* u3, uint32_t n, float* dir, float* pdf, std::string* err);
     cl_status pdf(const float* in9, const float* dir, uint32_t n, float* pdf, std::string* err);
 
@@ -42,7 +42,7 @@ public:
     void            setStream(cudaStream_t st) { st_ = st; }
 
 private:
-    cl_status upload(const float* rec13, uint32_t n, std::string* err);
+    cl_status upload(const float* rec14, uint32_t n, std::string* err);
     cl_status computeGradient(const float4* rec, const uint32_t* count, std::string* err);
     cl_status refreshCopies(std::string* err);
 

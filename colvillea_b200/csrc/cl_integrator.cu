@@ -185,7 +185,7 @@ __device__ __noinline__ void flushRecords(GuideDev g, const uint4* psInfo, Count
         r[0]      = make_float4(e0.x, e0.y, e0.z, w);
         r[1]      = make_float4(e1.x, e1.y, e1.z, 0.0f);
         r[2]      = make_float4(e2.x, e2.y, e2.z, 0.0f);
-        r[3]      = make_float4(e3.x, e3.y, e3.z, 0.0f);
+        r[3]      = make_float4(e3.x, e3.y, e3.z, e3.w);
     }
 }
 
@@ -364,9 +364,10 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
 // the ray queue.  Specialising keeps each instantiation free of the other
 // modes' and materials' code.
 // GUIDE (path tracing, corrected estimator, BSDF classes): one-sample MIS of
-// the BSDF (probability bsdfFrac) and the network's vMF mixture for this ray
-// (kGuideInfer); every pdf of the BSDF strategy - emitter-sample MIS, the
-// throughput update and the escaped-ray MIS - becomes the mixture pdf.
+// the BSDF and the network's vMF mixture for this ray (kGuideMlp), which is
+// sampled with probability a = the sum of its lobe weights (1 - bsdf_fraction,
+// or learned); every pdf of the BSDF strategy - emitter-sample MIS, the
+// throughput update and the escaped-ray MIS - becomes (1 - a) p_bsdf + a p_guide.
 template <bool DL, int CMP, bool ALIAS, int MAT, bool GUIDE = false>
 __global__ void __launch_bounds__(128) kShade(Params P, int cur)
 {
@@ -434,7 +435,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 pHit         = a.p;
                 f3    wo     = -d;
                 guide::Lobes G;
-                const float  gf = P.g.bsdfFrac;
+                float        gf = 1.0f; // probability of BSDF sampling: 1 - sum of the lobe weights
                 if (GUIDE)
                 {
                     const float4* lb = P.g.lobes + size_t(i) * kLobeF4;
@@ -443,6 +444,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                     float4 w0 = lb[8], w1 = lb[9];
                     G.w[0] = w0.x, G.w[1] = w0.y, G.w[2] = w0.z, G.w[3] = w0.w;
                     G.w[4] = w1.x, G.w[5] = w1.y, G.w[6] = w1.z, G.w[7] = w1.w;
+                    gf = 1.0f - (((w0.x + w0.y) + (w0.z + w0.w)) + ((w1.x + w1.y) + (w1.z + w1.w)));
                 }
                 f2    u      = rng.next2D();
                 Frame fr{a.dpdv, a.dpdu, (!DL && compatFrame) ? a.ng : a.ns};
@@ -465,7 +467,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                         if (nonzero(f))
                         {
                             float bp = bsdfPdf(bsdf, woL, wiL, compatPdf);
-                            if (GUIDE) bp = gf * bp + (1.0f - gf) * guide::mixturePdf(G, ldir);
+                            if (GUIDE) bp = gf * bp + guide::mixturePdf(G, ldir);
                             float c  = (DL && compatEsc) ? wiL.z : fabsf(wiL.z);
                             f3    baseV = DL ? value : T * value;
                             float w, pl;
@@ -500,15 +502,16 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                     f = bsdfSample(bsdf, woL, u2, &wiL, &bp);
                 else
                 {
-                    gdir = guide::mixtureSample(G, (us - gf) / (1.0f - gf), u2.x, u2.y);
+                    gdir = guide::mixtureSample(G, us - gf, u2.x, u2.y);
                     wiL  = fr.toLocal(gdir);
                     f    = bsdfEval(bsdf, woL, wiL);
                     bp   = bsdfPdf(bsdf, woL, wiL, false);
                 }
+                const float bpB = bp; // BSDF pdf of the sampled direction (training records)
                 if (GUIDE && nonzero(f))
                 {
                     if (us < gf) gdir = fr.toWorld(wiL);
-                    bp = gf * bp + (1.0f - gf) * guide::mixturePdf(G, gdir);
+                    bp = gf * bp + guide::mixturePdf(G, gdir);
                 }
                 // The corrected estimator stops paths whose sampled pdf is not
                 // positive (0 or NaN at the rim of the cosine warp); the
@@ -580,7 +583,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                                 h[0]  = make_float4(pn.x, pn.y, pn.z, tIn.x);
                                 h[1]  = make_float4(a.ns.x, a.ns.y, a.ns.z, tIn.y);
                                 h[2]  = make_float4(wo.x, wo.y, wo.z, tIn.z);
-                                h[3]  = make_float4(dir.x, dir.y, dir.z, 0.0f);
+                                h[3]  = make_float4(dir.x, dir.y, dir.z, bpB);
                                 h[4]  = make_float4(L.x, L.y, L.z, 0.0f);
                                 recBit = 1u << (depth - 1u);
                             }
@@ -675,16 +678,75 @@ __global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
     }
 }
 
-// Guided path tracing: network inference for the rays of the guided shading
-// classes (after kTraceClosest).  Each warp takes 32 rays of the class queues
-// (concatenated), encodes hit position, shading normal and outgoing direction
-// into its shared-memory tile, runs the MLP on the tensor cores (two 16-row
-// tiles) and writes the head's lobes for each ray.  Rays whose vertex is the
-// last one (depth == maxDepth) are not shaded and are skipped.
-constexpr int kGuideInferWarps = 8;
-constexpr int kGuideInferSmem  = guide::kFwdFragBytes + kGuideInferWarps * 32 * guide::kXS * 2;
-__global__ void __launch_bounds__(kGuideInferWarps * 32) kGuideInfer(Params P, guide::GridView g,
-                                                                     const uint2* __restrict__ wfG, int cur)
+// Guided path tracing: network inference after kTraceClosest for the rays of
+// the guided shading classes (class queues concatenated in class order), in
+// two passes:
+//   kGuideEncode - one thread per ray: hit position and shading normal, the
+//     16-level hash-grid gathers and the one-blob encodings -> a 96-wide
+//     bf16 input row enc[k] and the ray's queue index encIdx[k] (kNoRay for a
+//     last vertex, depth == maxDepth, which is not shaded);
+//   kGuideMlp - persistent warps stream 32 rows at a time through the MLP
+//     on the tensor cores and write each ray's lobes.
+// The encoding is a chain of dependent gathers (queue -> path state -> hit ->
+// vertices -> table) and runs at full occupancy on its own; the MLP pass
+// keeps its weights in shared memory and reads its rows sequentially.
+constexpr uint32_t kNoRay          = 0xffffffffu;
+constexpr int      kGuideMlpWarps  = 8;
+constexpr int      kGuideMlpSmem   = guide::kFwdFragBytes + kGuideMlpWarps * 32 * guide::kXS * 2;
+constexpr int      kGuideEncBlock  = 128;
+
+__device__ __forceinline__ uint32_t guidedCounts(const Params& P, uint32_t* n0, uint32_t* n1)
+{
+    const uint32_t mask = P.g.classMask;
+    *n0                 = (mask & 1u) ? loadCount(&P.q.ctr->classCount[0]) : 0u;
+    *n1                 = (mask & 2u) ? loadCount(&P.q.ctr->classCount[1]) : 0u;
+    const uint32_t n2   = (mask & 4u) ? loadCount(&P.q.ctr->classCount[2]) : 0u;
+    return *n0 + *n1 + n2;
+}
+
+__global__ void __launch_bounds__(kGuideEncBlock, 6) kGuideEncode(Params P, guide::GridView g, int cur)
+{
+    uint32_t       n0, n1;
+    const uint32_t n        = guidedCounts(P, &n0, &n1);
+    const uint32_t maxDepth = P.wp->maxDepth;
+    const f3       bmin{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]};
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    {
+        const uint32_t c   = k < n0 ? 0u : (k < n0 + n1 ? 1u : 2u);
+        const uint32_t pos = k - (c == 0u ? 0u : (c == 1u ? n0 : n0 + n1));
+        const uint32_t i   = P.q.classIdx[size_t(c) * P.q.slots + pos];
+        uint4*         dst = P.g.enc + size_t(k) * (guide::kIn / 8);
+        uint32_t       r[guide::kIn / 2];
+        uint32_t       ray = i;
+        if ((P.q.psInfo[P.q.rqSlot[cur][i]].z & 0xffu) == maxDepth)
+        {
+            ray = kNoRay;
+#pragma unroll
+            for (int q = 0; q < guide::kIn / 2; ++q) r[q] = 0u;
+        }
+        else
+        {
+            float4  hh = P.q.hit[i];
+            float4  rd = P.q.rqD[cur][i];
+            HitAttr a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
+            f3      pn = guide::clampUnit((a.p - bmin) * P.g.boxScale);
+#pragma unroll
+            for (int l = 0; l < guide::kLevels; ++l)
+            {
+                float2 f = guide::encodeLevel(g, l, pn);
+                r[l]     = guide::packBf16(f.x, f.y);
+            }
+            guide::oneBlobPacked(a.ns, r + guide::kHashF / 2);
+            guide::oneBlobPacked(f3{-rd.x, -rd.y, -rd.z}, r + (guide::kHashF + 2 * guide::kBlob) / 2);
+        }
+#pragma unroll
+        for (int q = 0; q < guide::kIn / 8; ++q) dst[q] = make_uint4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+        P.g.encIdx[k] = ray;
+    }
+}
+
+__global__ void __launch_bounds__(kGuideMlpWarps * 32, 2) kGuideMlp(Params P, const uint2* __restrict__ wfG,
+                                                                        float alpha)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2*         wf   = reinterpret_cast<uint2*>(smem);
@@ -696,39 +758,23 @@ __global__ void __launch_bounds__(kGuideInferWarps * 32) kGuideInfer(Params P, g
         for (int k = threadIdx.x; k < guide::kFwdFrags * 16; k += blockDim.x) dst[k] = __ldg(src + k);
     }
     __syncthreads();
-    const uint32_t maxDepth = P.wp->maxDepth;
-    const uint32_t mask     = P.g.classMask;
-    const uint32_t n0 = (mask & 1u) ? loadCount(&P.q.ctr->classCount[0]) : 0u;
-    const uint32_t n1 = (mask & 2u) ? loadCount(&P.q.ctr->classCount[1]) : 0u;
-    const uint32_t n2 = (mask & 4u) ? loadCount(&P.q.ctr->classCount[2]) : 0u;
-    const uint32_t n  = n0 + n1 + n2;
-    const f3       bmin{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]};
-    for (;;)
+    uint32_t       n0, n1;
+    const uint32_t n = guidedCounts(P, &n0, &n1);
+    for (uint32_t tile = blockIdx.x * kGuideMlpWarps + warp; tile * 32u < n; tile += gridDim.x * kGuideMlpWarps)
     {
-        uint32_t base = warpFetch(&P.q.ctr->fetchInfer);
-        if (base >= n) break;
-        uint32_t k     = base + lane;
-        bool     valid = k < n;
-        uint32_t i     = 0u;
-        if (valid)
+        const uint32_t k0 = tile * 32u;
+        const uint4*   src = P.g.enc + size_t(k0) * (guide::kIn / 8);
+#pragma unroll
+        for (int q = 0; q < guide::kIn / 8; ++q)
         {
-            uint32_t c   = k < n0 ? 0u : (k < n0 + n1 ? 1u : 2u);
-            uint32_t pos = k - (c == 0u ? 0u : (c == 1u ? n0 : n0 + n1));
-            i            = P.q.classIdx[size_t(c) * P.q.slots + pos];
-            if ((P.q.psInfo[P.q.rqSlot[cur][i]].z & 0xffu) == maxDepth) valid = false;
+            const uint32_t j = lane + 32u * q, rr = j / 12u, cc = j % 12u;
+            uint4          v = make_uint4(0u, 0u, 0u, 0u);
+            if (k0 + rr < n) v = src[j];
+            *reinterpret_cast<uint4*>(x + rr * guide::kXS + cc * 8) = v;
         }
-        __nv_bfloat16* row = x + lane * guide::kXS;
-        const uint32_t vm  = __ballot_sync(kFull, valid);
+        const uint32_t ray = k0 + lane < n ? P.g.encIdx[k0 + lane] : kNoRay;
+        const uint32_t vm  = __ballot_sync(kFull, ray != kNoRay);
         if (lane == 0u && vm) atomicAdd(&P.q.ctr->inferred, (unsigned long long)__popc(vm));
-        if (valid)
-        {
-            float4  hh = P.q.hit[i];
-            float4  rd = P.q.rqD[cur][i];
-            HitAttr a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
-            guide::encodeRow(g, (a.p - bmin) * P.g.boxScale, a.ns, f3{-rd.x, -rd.y, -rd.z}, row);
-        }
-        else
-            guide::zeroRow(row);
         __syncwarp();
         float out[2][6][4];
         guide::mlpInfer<2>(wf, x, lane, out);
@@ -736,11 +782,11 @@ __global__ void __launch_bounds__(kGuideInferWarps * 32) kGuideInfer(Params P, g
         float* o = reinterpret_cast<float*>(x);
         guide::storeOut<2>(out, o, lane);
         __syncwarp();
-        if (valid)
+        if (ray != kNoRay)
         {
             guide::Lobes L;
-            guide::headLobes(o + lane * guide::kOS, &L);
-            float4* dst = P.g.lobes + size_t(i) * kLobeF4;
+            guide::headLobes(o + lane * guide::kOS, &L, alpha);
+            float4* dst = P.g.lobes + size_t(ray) * kLobeF4;
 #pragma unroll
             for (int j = 0; j < guide::kLobes; ++j) dst[j] = L.l[j];
             dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
@@ -919,10 +965,11 @@ cl_status Integrator::init(std::string* err)
                 &b, dl ? (const void*)kShadowResolve<true> : (const void*)kShadowResolve<false>, 128, 0),
             err);
     shadowBlocks_ = std::max(1, b) * numSMs_;
-    CL_CUDA(cudaFuncSetAttribute(kGuideInfer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideInferSmem), err);
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideInfer, kGuideInferWarps * 32, kGuideInferSmem),
-            err);
+    CL_CUDA(cudaFuncSetAttribute(kGuideMlp, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideMlpSmem), err);
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideMlp, kGuideMlpWarps * 32, kGuideMlpSmem), err);
     inferBlocks_ = std::max(1, b) * numSMs_;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideEncode, kGuideEncBlock, 0), err);
+    encodeBlocks_ = std::max(1, b) * numSMs_;
     CL_TRY(ctr_.alloc(sizeof(Counters), err));
     CL_TRY(wp_.alloc(sizeof(WaveParams), err));
     CL_CUDA(cudaMemsetAsync(ctr_.p, 0, sizeof(Counters), stream_), err);
@@ -1314,6 +1361,8 @@ Params Integrator::params() const
     if (guide_)
     {
         P.g.lobes     = lobes_.as<float4>();
+        P.g.enc       = enc_.as<uint4>();
+        P.g.encIdx    = encIdx_.u();
         P.g.hist      = hist_.as<float4>();
         P.g.rec       = rec_.as<float4>();
         P.g.recCap    = recCap_;
@@ -1342,8 +1391,11 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
     const uint32_t gmask = guide_ ? guideCfg_.class_mask : 0u;
     if (gmask)
-        kGuideInfer<<<inferBlocks_, kGuideInferWarps * 32, kGuideInferSmem, stream_>>>(P, guide_->grid(),
-                                                                                       guide_->fwdFrags(), cur);
+    {
+        kGuideEncode<<<encodeBlocks_, kGuideEncBlock, 0, stream_>>>(P, guide_->grid(), cur);
+        kGuideMlp<<<inferBlocks_, kGuideMlpWarps * 32, kGuideMlpSmem, stream_>>>(
+            P, guide_->fwdFrags(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
+    }
     if (profile) CL_CUDA(cudaEventRecord(evS_[4], stream_), err);
     for (int m = 0; m < 4; ++m)
         shadeKernel(dl, m, cfg_.flags, m < 3 && ((gmask >> m) & 1u))<<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
@@ -1559,6 +1611,12 @@ cl_status Integrator::ensureGuideBuffers(std::string* err)
         CL_TRY(rec_.alloc(rb, err));
         graphValid_ = false;
     }
+    if (enc_.bytes != size_t(slots_) * guide::kIn * 2)
+    {
+        CL_TRY(enc_.alloc(size_t(slots_) * guide::kIn * 2, err));
+        CL_TRY(encIdx_.alloc(size_t(slots_) * 4, err));
+        graphValid_ = false;
+    }
     return CL_OK;
 }
 
@@ -1568,6 +1626,8 @@ cl_status Integrator::setGuiding(const cl_guide_config* cfg, std::string* err)
     {
         guide_.reset();
         lobes_.release();
+        enc_.release();
+        encIdx_.release();
         hist_.release();
         rec_.release();
         graphValid_ = false;
@@ -1681,9 +1741,11 @@ cl_status Integrator::resize(uint32_t w, uint32_t h, std::string* err)
     return CL_OK;
 }
 
-cl_status Integrator::resetIteration(std::string* err)
+cl_status Integrator::resetIteration(std::string* err) { return setIteration(0u, err); }
+
+cl_status Integrator::setIteration(uint32_t iteration, std::string* err)
 {
-    iteration_ = 0;
+    iteration_ = iteration;
     return clearFilm(err);
 }
 

@@ -88,10 +88,12 @@ struct QueueDev
 // Guided path tracing: per-ray mixtures, per-slot vertex histories and the
 // training records (no counterpart in the reference).
 constexpr int kLobeF4 = 10; // 8 x {mu, kappa}, weights 0-3, weights 4-7
-constexpr int kHistF4 = 5;  // {p, T.x} {n, T.y} {wo, T.z} {omega, -} {L snapshot, -}
+constexpr int kHistF4 = 5;  // {p, T.x} {n, T.y} {wo, T.z} {omega, BSDF pdf} {L snapshot, -}
 struct GuideDev
 {
     float4*  lobes;     // kLobeF4 per ray-queue index
+    uint4*   enc;       // encoded network inputs, 96 bf16 per guided ray (concatenated class order)
+    uint32_t* encIdx;   // ray-queue index of each encoded row (kNoRay: skipped)
     float4*  hist;      // (slots / recStride) x maxDepth x kHistF4
     float4*  rec;       // kRecordF4 per record
     uint32_t recCap;
@@ -127,6 +129,7 @@ public:
     cl_status readbackFilmStats(double* sum, double* sumsq, size_t count, std::string* err);
     cl_status resize(uint32_t w, uint32_t h, std::string* err);
     cl_status resetIteration(std::string* err);
+    cl_status setIteration(uint32_t iteration, std::string* err);
     void      stats(cl_stats* s) const;
     cl_status traceRays(const float* rays, uint32_t n, float* t, uint32_t* prim, float* b1, float* b2,
                         std::string* err);
@@ -203,10 +206,10 @@ private:
     // Guiding.
     std::unique_ptr<GuideNet> guide_;
     cl_guide_config           guideCfg_{};
-    DevBuf                    lobes_, hist_, rec_;
+    DevBuf                    lobes_, hist_, rec_, enc_, encIdx_;
     uint32_t                  recStride_ = 0, recCap_ = 0, histSlots_ = 0, histDepth_ = 0;
     float                     boxMin_[3] = {0, 0, 0}, boxScale_ = 1.0f;
-    int                       inferBlocks_ = 0;
+    int                       inferBlocks_ = 0, encodeBlocks_ = 0;
     uint64_t                  guideSamples_ = 0, guideRecordsLast_ = 0, guideInferred_ = 0;
     double                    guideLoss_ = 0.0;
     float                     msTrain_ = 0.0f, msInfer_ = 0.0f;

@@ -214,6 +214,10 @@ cl_status cl_readback_film_stats(cl_integrator* integrator, double* sum, double*
 cl_status cl_resize(cl_integrator* integrator, uint32_t width, uint32_t height);
 cl_status cl_get_film_size(cl_integrator* integrator, uint32_t* width, uint32_t* height);
 cl_status cl_reset_iteration(cl_integrator* integrator);
+/* Like cl_reset_iteration, but the next render continues from progressive
+ * frame `iteration` (the sampler's frame key): independent render seeds for
+ * the same scene.  No counterpart in the reference. */
+cl_status cl_set_iteration(cl_integrator* integrator, uint32_t iteration);
 cl_status cl_get_stats(cl_integrator* integrator, cl_stats* stats);
 /* Last error message of the calling thread. */
 cl_status cl_last_error(char* buffer, size_t size);
@@ -320,9 +324,13 @@ cl_status cl_dome_build_tables_noalloc(const float* texels, uint32_t width, uint
  * Parameters (flat FP32, the layout of cl_guide_get_params): the hash table
  * [level][entry][feature], then W0 (64x96), W1..W3 (64x64), W4 (48x64),
  * each row-major [out][in].
+ * With learn_selection, output 40 gives the probability of sampling the
+ * network, a = 0.05 + 0.9 sigmoid(o40), and the loss uses the density the
+ * tracer samples from, p = (1 - a) p_bsdf + a p_guide.
  * Record layouts of the host entry points:
  *   in9:   position in [0,1]^3 (scene box), shading normal, outgoing dir;
- *   rec13: in9, then the sampled direction omega (3) and the weight w. */
+ *   rec14: in9, then the sampled direction omega (3), the weight w and the
+ *          BSDF pdf of omega (used with learn_selection). */
 enum
 {
     CL_GUIDE_LEVELS  = 16,
@@ -342,6 +350,12 @@ typedef struct cl_guide_config
     uint32_t train_spp;                    /* one training step after each of the first train_spp spp (32) */
     uint32_t class_mask;                   /* guided BSDFs: bit 0 diffuse, 1 conductor, 2 dielectric (3) */
     uint32_t seed;                         /* parameter initialisation */
+    uint32_t learn_selection;              /* 1: the probability of sampling the network is learned (head
+                                              output 40) and training minimises -log of the whole one-sample
+                                              MIS density; 0: it is 1 - bsdf_fraction and training minimises
+                                              -log of the network's mixture (0) */
+    float    weight_clamp;                 /* training weights above weight_clamp x the batch mean are
+                                              clamped to it (robust fit to heavy-tailed records); 0 = off */
 } cl_guide_config;
 
 typedef struct cl_guide_stats
@@ -352,7 +366,7 @@ typedef struct cl_guide_stats
     uint64_t inferred;         /* network evaluations by the integrator */
     double   last_loss;        /* loss of the last step */
     float    ms_train;         /* device time of training so far */
-    float    ms_infer;         /* device time of inference (CL_PROFILE_STAGES renders) */
+    float    ms_infer;         /* last render with CL_PROFILE_STAGES: device time of inference */
 } cl_guide_stats;
 
 void      cl_guide_default_config(cl_guide_config* config);
@@ -368,10 +382,11 @@ cl_status cl_guide_get_params(const cl_guide* guide, float* params, uint64_t cou
 /* Raw head outputs (count x 48). */
 cl_status cl_guide_forward(cl_guide* guide, const float* in9, uint32_t count, float* out48);
 /* Loss and gradient (param_count floats) of one batch, parameters unchanged. */
-cl_status cl_guide_gradient(cl_guide* guide, const float* rec13, uint32_t count, double* loss, float* grad);
+cl_status cl_guide_gradient(cl_guide* guide, const float* rec14, uint32_t count, double* loss, float* grad);
 /* One Adam step on one batch. */
-cl_status cl_guide_train_step(cl_guide* guide, const float* rec13, uint32_t count, double* loss);
-/* Mixture sampling (u3: lobe, then the two direction uniforms) and pdf. */
+cl_status cl_guide_train_step(cl_guide* guide, const float* rec14, uint32_t count, double* loss);
+/* Sampling and pdf of the network's vMF mixture alone (u3: lobe, then the
+ * two direction uniforms). */
 cl_status cl_guide_sample(cl_guide* guide, const float* in9, const float* u3, uint32_t count, float* dir3,
                           float* pdf);
 cl_status cl_guide_pdf(cl_guide* guide, const float* in9, const float* dir3, uint32_t count, float* pdf);

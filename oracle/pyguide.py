@@ -193,17 +193,56 @@ def head_grad(out, omega):
     return out_g
 
 
-def loss_and_grads(params, log2T, res, pos, nrm, wo, omega, weight):
-    """Loss and gradient of the flat parameter vector (same layout)."""
+SEL_MIN, SEL_MAX = 0.05, 0.95
+SEL_OUT = 5 * N_LOBES                  # head output 40: logit of the guide-selection probability
+
+
+def selection(out):
+    """Learned probability of sampling the guide: SEL_MIN + (SEL_MAX - SEL_MIN) sigmoid(o40)."""
+    return SEL_MIN + (SEL_MAX - SEL_MIN) / (1.0 + np.exp(-out[:, SEL_OUT]))
+
+
+def mix_log_pdf(out, omega, pb):
+    """log of the one-sample MIS density (1 - a) p_bsdf + a p_guide."""
+    a = selection(out)
+    pg = np.exp(log_pdf(out, omega)[0])
+    return np.log((1 - a) * pb + a * pg)
+
+
+def mix_grad(out, omega, pb):
+    """d log p_mix / d out: the lobe gradient scaled by a p_g / p_mix, and
+    (p_g - p_b) / p_mix da/do40 for the selection logit."""
+    a = selection(out)
+    pg = np.exp(log_pdf(out, omega)[0])
+    pm = (1 - a) * pb + a * pg
+    g = head_grad(out, omega) * (a * pg / pm)[:, None]
+    sg = 1.0 / (1.0 + np.exp(-out[:, SEL_OUT]))
+    g[:, SEL_OUT] = (pg - pb) / pm * (SEL_MAX - SEL_MIN) * sg * (1 - sg)
+    return g
+
+
+def loss_and_grads(params, log2T, res, pos, nrm, wo, omega, weight, pb=None, clamp=0.0):
+    """Loss and gradient of the flat parameter vector (same layout).  With pb
+    (the BSDF pdf of each sample's direction) the objective is the one-sample
+    MIS mixture with the learned selection probability, -log p_mix;
+    without it, -log p_guide.  clamp > 0: weights above clamp x their mean
+    are clamped to it before normalisation."""
+    if clamp > 0:
+        weight = np.minimum(weight, clamp * np.mean(weight))
     table, ws = split_params(params, log2T)
     tb = bf16(table)
     x, corners = encode(pos, nrm, wo, tb, res)
     out, acts = forward(x, ws)
-    lp, _ = log_pdf(out, omega)
+    if pb is None:
+        lp, _ = log_pdf(out, omega)
+        hg = head_grad(out, omega)
+    else:
+        lp = mix_log_pdf(out, omega, pb)
+        hg = mix_grad(out, omega, pb)
     wn = weight / np.mean(weight)
     B = len(pos)
     loss = -np.sum(wn * lp) / B
-    d = -(wn / B)[:, None] * head_grad(out, omega)               # d loss / d out
+    d = -(wn / B)[:, None] * hg                                  # d loss / d out
     gws = [None] * len(ws)
     for k in range(len(ws) - 1, -1, -1):
         db = bf16(d)

@@ -73,29 +73,32 @@ def records(rng, n, in9=None):
     in9 = inputs(rng, n) if in9 is None else in9
     om = unit(rng, n)
     w = rng.uniform(0.1, 2.0, n)
-    return np.concatenate([in9, om, w[:, None]], 1).astype(np.float32)
+    pb = rng.uniform(0.02, 2.0, n)
+    return np.concatenate([in9, om, w[:, None], pb[:, None]], 1).astype(np.float32)
 
 
-def oracle_grads(p, res, rec):
+def oracle_grads(p, res, rec, learned=False):
     x = rec.astype(np.float64)
-    return G.loss_and_grads(p, LOG2T, res, x[:, 0:3], x[:, 3:6], x[:, 6:9], x[:, 9:12], x[:, 12])
+    return G.loss_and_grads(p, LOG2T, res, x[:, 0:3], x[:, 3:6], x[:, 6:9], x[:, 9:12], x[:, 12],
+                            x[:, 13] if learned else None)
 
 
-def test_gradient_matches_oracle():
+@pytest.mark.parametrize("learned", [False, True], ids=["fixed_selection", "learned_selection"])
+def test_gradient_matches_oracle(learned):
     rng = np.random.default_rng(11)
-    g = make_guide()
+    g = make_guide(learn_selection=int(learned))
     p = random_params(g, rng, hash_scale=0.3)
     res = g.resolutions()
     rec = records(rng, 4096)
     loss, grad = g.gradient(rec)
-    loss_ref, grad_ref = oracle_grads(p, res, rec)
+    loss_ref, grad_ref = oracle_grads(p, res, rec, learned)
     G.ROUND_BF16 = False
     try:
-        _, grad_fp64 = oracle_grads(p, res, rec)
+        _, grad_fp64 = oracle_grads(p, res, rec, learned)
     finally:
         G.ROUND_BF16 = True
     nh = p.size - G.mlp_param_count()
-    print(f"[guide] loss gpu {loss:.6f} oracle {loss_ref:.6f}")
+    print(f"[guide] {'learned' if learned else 'fixed'} selection: loss gpu {loss:.6f} oracle {loss_ref:.6f}")
     assert abs(loss - loss_ref) < 1e-3 * abs(loss_ref) + 1e-5
     blocks = [("hash", slice(0, nh))]
     off = nh
@@ -119,6 +122,25 @@ def test_gradient_matches_oracle():
               f"{relB:.2e}), cosine vs FP64 {cos:.6f}")
         assert rel < 2e-2, name
         assert rel64 < 1.25 * relB + 5e-3 and cos > 0.99, name
+    g.close()
+
+
+def test_weight_clamp_gradient():
+    """weight_clamp: records above 3 x the batch mean weight count as 3 x the mean."""
+    rng = np.random.default_rng(15)
+    g = make_guide(weight_clamp=3.0)
+    p = random_params(g, rng, hash_scale=0.3)
+    res = g.resolutions()
+    rec = records(rng, 4096)
+    rec[:64, 12] = 500.0                       # heavy tail
+    loss, grad = g.gradient(rec)
+    x = rec.astype(np.float64)
+    loss_ref, grad_ref = G.loss_and_grads(p, LOG2T, res, x[:, 0:3], x[:, 3:6], x[:, 6:9], x[:, 9:12], x[:, 12],
+                                          clamp=3.0)
+    assert abs(loss - loss_ref) < 1e-3 * abs(loss_ref) + 1e-5
+    rel = np.linalg.norm(grad - grad_ref) / np.linalg.norm(grad_ref)
+    print(f"[guide] clamped weights: loss gpu {loss:.6f} oracle {loss_ref:.6f}, grad rel err {rel:.2e}")
+    assert rel < 2e-2
     g.close()
 
 
@@ -187,7 +209,7 @@ def test_training_learns_a_distribution():
     def batch(n):
         in9 = inputs(rng, n)
         om = vmf_samples(rng, target_mu(in9[:, :3].astype(np.float64)), kappa)
-        return np.concatenate([in9, om, np.ones((n, 1))], 1).astype(np.float32)
+        return np.concatenate([in9, om, np.ones((n, 1)), np.ones((n, 1))], 1).astype(np.float32)
 
     held = batch(8192)
 
@@ -219,13 +241,15 @@ def test_guided_integrator_api_errors():
     comp.close()
 
 
-def test_guided_render_is_unbiased():
+@pytest.mark.parametrize("learned", [False, True], ids=["fixed_selection", "learned_selection"])
+def test_guided_render_is_unbiased(learned):
     """Guided path tracing (online training for the first 16 spp) against the
     plain tracer with the same corrected estimator: per-pixel Welch tests."""
     s = scenes.config1(0, 96, 96)
     spp_g, spp_p = 128, 512
     it = cb.load_scene(s, flags=cb.DOME_ALIAS | cb.FILM_FP64)
-    it.setGuiding(cb.GuideConfig(log2_table=16, batch=1 << 14, train_spp=16, class_mask=7))
+    it.setGuiding(cb.GuideConfig(log2_table=16, batch=1 << 14, train_spp=16, class_mask=7,
+                                 learn_selection=int(learned)))
     it.render(spp_g)
     g1, g2 = it.readbackFilmStats()
     gs = it.guideStats()

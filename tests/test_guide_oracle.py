@@ -62,6 +62,31 @@ def test_gradients_match_finite_differences(smooth):
         assert abs(fd - g[i]) <= 1e-6 * abs(g[i]) + 1e-8 * scale + 1e-11, (i, fd, g[i])
 
 
+def test_mixture_loss_gradients_match_finite_differences(smooth):
+    """Learned selection probability: -log((1-a) p_bsdf + a p_guide)."""
+    rng = np.random.default_rng(5)
+    log2T = 8
+    res = G.resolutions(4, 64)
+    B = 24
+    p = _params(rng, log2T)
+    pos = rng.uniform(0, 1, (B, 3))
+    nrm, wo, om = _unit(rng, B), _unit(rng, B), _unit(rng, B)
+    w = rng.uniform(0.1, 2, B)
+    pb = rng.uniform(0.01, 2.0, B)
+    loss, g = G.loss_and_grads(p, log2T, res, pos, nrm, wo, om, w, pb)
+    nh = G.L_LEVELS * (1 << log2T) * 2
+    touched = np.nonzero(g[:nh])[0]
+    idx = np.concatenate([rng.choice(touched, 16, replace=False), rng.choice(np.arange(nh, p.size), 48, replace=False)])
+    scale = np.abs(g).max()
+    for i in idx:
+        q = p.copy(); q[i] += 1e-5
+        lp, _ = G.loss_and_grads(q, log2T, res, pos, nrm, wo, om, w, pb)
+        q[i] -= 2e-5
+        lm, _ = G.loss_and_grads(q, log2T, res, pos, nrm, wo, om, w, pb)
+        fd = (lp - lm) / 2e-5
+        assert abs(fd - g[i]) <= 1e-6 * abs(g[i]) + 1e-8 * scale + 1e-11, (i, fd, g[i])
+
+
 def test_head_gradient_matches_finite_differences():
     rng = np.random.default_rng(2)
     out = rng.normal(size=(16, 48))
@@ -73,6 +98,13 @@ def test_head_gradient_matches_finite_differences():
         fd = (G.log_pdf(out + d, om)[0] - G.log_pdf(out - d, om)[0]) / 2e-6
         np.testing.assert_allclose(fd, g[:, c], rtol=1e-5, atol=1e-7)
     assert np.all(g[:, 40:] == 0)
+    pb = rng.uniform(0.05, 1.5, 16)
+    gm = G.mix_grad(out, om, pb)
+    for c in list(range(41)):
+        d = np.zeros_like(out); d[:, c] = 1e-6
+        fd = (G.mix_log_pdf(out + d, om, pb) - G.mix_log_pdf(out - d, om, pb)) / 2e-6
+        np.testing.assert_allclose(fd, gm[:, c], rtol=1e-5, atol=1e-7)
+    assert np.all(gm[:, 41:] == 0)
 
 
 def test_mixture_is_normalised():
