@@ -47,7 +47,8 @@ def parse():
                     help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
     ap.add_argument("--no-relmse", action="store_true", help="skip the guided-vs-plain equal-time relMSE")
-    ap.add_argument("--relmse-ref-spp", type=int, default=8192, help="spp of the FP64 reference image")
+    ap.add_argument("--relmse-ref-spp", type=int, default=8192, help="spp of the cfg3 FP64 reference image")
+    ap.add_argument("--relmse-ref-spp4", type=int, default=8192, help="spp of the cfg4 FP64 reference image")
     ap.add_argument("--relmse-seeds", type=int, default=3)
     ap.add_argument("--relmse-spp", type=int, default=128, help="guided spp (training included)")
     return ap.parse_args()
@@ -196,32 +197,53 @@ def cpu_baseline(scene, seconds, threads):
 
 
 def guided_relmse(args):
-    """Second half of the metric: equal-time relMSE of neural-guided vs plain
-    path tracing against an FP64-accumulated plain reference, on cfg3 (the
-    cfg1 scene at 1920x1080, 128 guided spp including online training: one
-    Adam step on 2^18 records after each of the first 32 spp)."""
+    """Second half of the metric: equal-time relMSE of the neural tracers vs
+    plain path tracing against FP64-accumulated plain references.
+      cfg3: the cfg1 scene at 1920x1080, neural-guided (128 spp including
+            online training: one Adam step on 2^18 records after each of the
+            first 32 spp);
+      cfg4: the caustic scene at 1920x1080, depth 16, neural radiance cache
+            (paths end in the cache after 2 bounces, 1/16 training paths,
+            one Adam step after each of the first 32 spp)."""
     import colvillea_b200 as cb
     from colvillea_b200 import evaluate, scenes
-    s = scenes.config3(0)
+    rnd = lambda v: [round(x, 6) for x in v] if isinstance(v, list) else (round(v, 6) if isinstance(v, float) else v)
+    out = {}
+    s3 = scenes.config3(0)
     t0 = time.perf_counter()
-    ref = evaluate.reference(s, args.relmse_ref_spp)
-    t_ref = time.perf_counter() - t0
+    ref3 = evaluate.reference(s3, args.relmse_ref_spp)
+    t3 = time.perf_counter() - t0
     guide = cb.GuideConfig()
-    r = evaluate.equal_time(s, ref, args.relmse_spp, seeds=args.relmse_seeds, guide=guide)
-    mlp = evaluate.mlp_throughput(s, guide)
+    r = evaluate.equal_time(s3, ref3, args.relmse_spp, seeds=args.relmse_seeds, guide=guide)
+    mlp = evaluate.mlp_throughput(s3, guide)
     peak = None
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         peak = float(json.load(open(p)).get("bf16_tflops", 0)) or None
-    rnd = lambda v: [round(x, 6) for x in v] if isinstance(v, list) else (round(v, 6) if isinstance(v, float) else v)
-    return {"workload": f"cfg3: cfg1 scene (10,242 tris) at {s.width}x{s.height}, max depth {s.max_depth}, RR from "
-                        f"{s.rr_start}; guided {args.relmse_spp} spp incl. training ({guide.train_spp} Adam steps, "
-                        f"batch {guide.batch}, lr {guide.learning_rate:g}, BSDF fraction {guide.bsdf_fraction:g}, "
-                        f"guided classes mask {guide.class_mask}); plain at the same device time",
-            "reference": f"plain, corrected estimator, {args.relmse_ref_spp} spp, FP64 film ({t_ref:.1f} s)",
-            **{k: rnd(v) for k, v in r.items()},
-            "mlp": {**{k: rnd(v) for k, v in mlp.items()}, "bf16_peak_tflops": peak,
-                    "infer_frac_of_peak": round(mlp["infer_tflops"] / peak, 4) if peak and mlp["infer_tflops"] else None}}
+    out["cfg3_guided"] = {
+        "workload": f"cfg3: cfg1 scene (10,242 tris) at {s3.width}x{s3.height}, max depth {s3.max_depth}, RR from "
+                    f"{s3.rr_start}; guided {args.relmse_spp} spp incl. training ({guide.train_spp} Adam steps, batch "
+                    f"{guide.batch}, lr {guide.learning_rate:g}, BSDF fraction {guide.bsdf_fraction:g}, guided classes "
+                    f"mask {guide.class_mask}); plain at the same device time",
+        "reference": f"plain, corrected estimator, {args.relmse_ref_spp} spp, FP64 film ({t3:.1f} s)",
+        **{k: rnd(v) for k, v in r.items()},
+        "mlp": {**{k: rnd(v) for k, v in mlp.items()}, "bf16_peak_tflops": peak,
+                "infer_frac_of_peak": round(mlp["infer_tflops"] / peak, 4) if peak and mlp["infer_tflops"] else None}}
+    s4 = scenes.config4(0)
+    t0 = time.perf_counter()
+    ref4 = evaluate.reference(s4, args.relmse_ref_spp4)
+    t4 = time.perf_counter() - t0
+    cache = cb.RadianceCacheConfig()
+    r4 = evaluate.equal_time(s4, ref4, args.relmse_spp, seeds=args.relmse_seeds, cache=cache)
+    out["cfg4_radiance_cache"] = {
+        "workload": f"cfg4: cfg1 geometry with 60% rough glass (alpha U[0.01,0.1]), 2048x1024 HDRI with one lobe (peak "
+                    f"5000, sigma 0.5 deg), {s4.width}x{s4.height}, max depth {s4.max_depth}; radiance cache "
+                    f"{args.relmse_spp} spp incl. training ({cache.train_spp} Adam steps, batch {cache.network.batch}, "
+                    f"prefix {cache.prefix_bounces} bounces, 1/{1 << cache.train_log2_fraction} training paths); plain "
+                    f"at the same device time",
+        "reference": f"plain, corrected estimator, {args.relmse_ref_spp4} spp, FP64 film ({t4:.1f} s)",
+        **{k: rnd(v) for k, v in r4.items()}}
+    return out
 
 
 def run_reference(args):

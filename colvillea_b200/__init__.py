@@ -16,7 +16,7 @@ from . import _native as N
 from ._native import ClError
 
 __all__ = ["IntegratorType", "Integrator", "RenderConfig", "ClError", "COMPAT_ALL", "DOME_ALIAS", "FILM_FP64",
-           "PROFILE_STAGES", "TRACE_STATS", "load_scene", "GuideConfig", "Guide"]
+           "PROFILE_STAGES", "TRACE_STATS", "load_scene", "GuideConfig", "Guide", "RadianceCacheConfig", "Cache"]
 
 COMPAT_PDF, COMPAT_FRAME, COMPAT_ESCAPE, COMPAT_ALL = N.CL_COMPAT_PDF, N.CL_COMPAT_FRAME, N.CL_COMPAT_ESCAPE, N.CL_COMPAT_ALL
 DOME_ALIAS, FILM_FP64, PROFILE_STAGES, TRACE_STATS = N.CL_DOME_ALIAS, N.CL_FILM_FP64, N.CL_PROFILE_STAGES, N.CL_TRACE_STATS
@@ -284,6 +284,111 @@ class Guide:
         p = np.zeros(len(in9), np.float32)
         N.call("cl_guide_pdf", self._h, _ptr(in9), _ptr(dirs), len(in9), _ptr(p))
         return p
+
+
+def RadianceCacheConfig(**kw):
+    """cl_radiance_cache_config with the library's defaults; `network` takes a
+    dict of cl_guide_config fields (hash grid, Adam, batch)."""
+    c = N.RadianceCacheConfig()
+    N.lib().cl_radiance_cache_default_config(ctypes.byref(c))
+    for k, v in kw.items():
+        if k == "network":
+            for nk, nv in v.items():
+                if nk == "resolutions":
+                    for i, r in enumerate(nv):
+                        c.network.resolutions[i] = int(r)
+                else:
+                    setattr(c.network, nk, nv)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+class Cache:
+    """The neural radiance cache network (hash grid + one-blob encoding,
+    96-64-64-16 MLP on the tensor cores, RGB in outputs 0-2)."""
+
+    def __init__(self, handle, owned=True):
+        self._h = handle
+        self._owned = owned
+
+    @staticmethod
+    def create(network=None):
+        h = ctypes.c_void_p()
+        cfg = network if network is not None else RadianceCacheConfig().network
+        N.call("cl_cache_create", ctypes.byref(cfg), ctypes.byref(h))
+        return Cache(h)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._owned:
+            N.lib().cl_cache_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def param_count(self):
+        n = ctypes.c_uint64()
+        N.call("cl_cache_param_count", self._h, ctypes.byref(n))
+        return n.value
+
+    def resolutions(self):
+        r = np.zeros(16, np.uint32)
+        N.call("cl_cache_get_resolutions", self._h, _ptr(r))
+        return r
+
+    def get_params(self):
+        p = np.zeros(self.param_count(), np.float32)
+        N.call("cl_cache_get_params", self._h, _ptr(p), p.size)
+        return p
+
+    def set_params(self, p):
+        p = _f32(p)
+        N.call("cl_cache_set_params", self._h, _ptr(p), p.size)
+
+    def forward(self, in9):
+        in9 = _f32(in9)
+        out = np.zeros((len(in9), 16), np.float32)
+        N.call("cl_cache_forward", self._h, _ptr(in9), len(in9), _ptr(out))
+        return out
+
+    def gradient(self, rec12):
+        """rec12 rows: position, normal, wo, target RGB."""
+        rec12 = _f32(rec12)
+        assert rec12.ndim == 2 and rec12.shape[1] == 12
+        g = np.zeros(self.param_count(), np.float32)
+        loss = ctypes.c_double()
+        N.call("cl_cache_gradient", self._h, _ptr(rec12), len(rec12), ctypes.byref(loss), _ptr(g))
+        return loss.value, g
+
+    def train_step(self, rec12):
+        rec12 = _f32(rec12)
+        assert rec12.ndim == 2 and rec12.shape[1] == 12
+        loss = ctypes.c_double()
+        N.call("cl_cache_train_step", self._h, _ptr(rec12), len(rec12), ctypes.byref(loss))
+        return loss.value
+
+
+def _set_radiance_cache(self, config):
+    """Path tracing with the neural radiance cache (None: off)."""
+    N.call("cl_integrator_set_radiance_cache", self._h, ctypes.byref(config) if config is not None else None)
+
+
+def _cache(self):
+    h = ctypes.c_void_p()
+    N.call("cl_integrator_get_cache", self._h, ctypes.byref(h))
+    return Cache(h, owned=False) if h.value else None
+
+
+def _cache_stats(self):
+    s = N.GuideStats()
+    N.call("cl_integrator_cache_stats", self._h, ctypes.byref(s))
+    return s.as_dict()
+
+
+Integrator.setRadianceCache = _set_radiance_cache
+Integrator.cache = _cache
+Integrator.cacheStats = _cache_stats
 
 
 def _set_guiding(self, config):

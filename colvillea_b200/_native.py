@@ -78,6 +78,10 @@ class GuideConfig(ctypes.Structure):
                 ("weight_clamp", ctypes.c_float)]
 
 
+class RadianceCacheConfig(ctypes.Structure):
+    _fields_ = [("network", GuideConfig), ("prefix_bounces", u32), ("train_log2_fraction", u32), ("train_spp", u32)]
+
+
 class GuideStats(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_uint64), ("samples_trained", ctypes.c_uint64), ("records_last", ctypes.c_uint64),
                 ("inferred", ctypes.c_uint64), ("last_loss", ctypes.c_double), ("ms_train", ctypes.c_float),
@@ -143,7 +147,22 @@ _SIGS = {
     "cl_integrator_get_guide": [vp, ctypes.POINTER(vp)],
     "cl_integrator_guide_stats": [vp, ctypes.POINTER(GuideStats)],
 }
-_VOID = {"cl_guide_default_config"}
+_SIGS.update({
+    "cl_radiance_cache_default_config": [ctypes.POINTER(RadianceCacheConfig)],
+    "cl_cache_create": [ctypes.POINTER(GuideConfig), ctypes.POINTER(vp)],
+    "cl_cache_destroy": [vp],
+    "cl_cache_param_count": [vp, ctypes.POINTER(ctypes.c_uint64)],
+    "cl_cache_get_resolutions": [vp, vp],
+    "cl_cache_set_params": [vp, vp, ctypes.c_uint64],
+    "cl_cache_get_params": [vp, vp, ctypes.c_uint64],
+    "cl_cache_forward": [vp, vp, u32, vp],
+    "cl_cache_gradient": [vp, vp, u32, ctypes.POINTER(ctypes.c_double), vp],
+    "cl_cache_train_step": [vp, vp, u32, ctypes.POINTER(ctypes.c_double)],
+    "cl_integrator_set_radiance_cache": [vp, ctypes.POINTER(RadianceCacheConfig)],
+    "cl_integrator_get_cache": [vp, ctypes.POINTER(vp)],
+    "cl_integrator_cache_stats": [vp, ctypes.POINTER(GuideStats)],
+})
+_VOID = {"cl_guide_default_config", "cl_radiance_cache_default_config"}
 
 _lib = None
 

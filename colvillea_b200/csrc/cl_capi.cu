@@ -4,6 +4,7 @@
 // src/core/devices/cudacommon.h:13-26).
 #include "cl_integrator.h"
 
+#include <cstring>
 #include <memory>
 #include <new>
 
@@ -21,9 +22,23 @@ struct cl_guide
     }
 };
 
+// A radiance-cache network: standalone or an integrator's (borrowed).
+struct cl_cache
+{
+    clb::CacheNet*                 net = nullptr;
+    std::unique_ptr<clb::CacheNet> own;
+    cudaStream_t                   stream = nullptr;
+    ~cl_cache()
+    {
+        own.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
 struct cl_integrator
 {
     clb::Integrator impl;
+    cl_cache        cacheView; // borrowed view of impl's radiance cache
     cl_guide        guideView; // borrowed view of impl's network
     cl_integrator(cl_integrator_type t, uint32_t w, uint32_t h, const cl_render_config& c) : impl(t, w, h, c) {}
 };
@@ -472,6 +487,127 @@ cl_status cl_integrator_guide_stats(cl_integrator* it, cl_guide_stats* stats)
     CL_NEED(it);
     CL_NEED(stats);
     return guarded([&](std::string* e) { return it->impl.guideStats(stats, e); });
+}
+
+// ---- Neural radiance cache ----
+void cl_radiance_cache_default_config(cl_radiance_cache_config* config)
+{
+    if (!config) return;
+    std::memset(config, 0, sizeof(*config));
+    clb::guideDefaultConfig(&config->network);
+    config->network.train_spp  = 0;
+    config->network.class_mask = 0;
+    config->prefix_bounces      = 2;
+    config->train_log2_fraction = 4;
+    config->train_spp           = 32;
+}
+
+cl_status cl_cache_create(const cl_guide_config* network, cl_cache** out)
+{
+    CL_NEED(network);
+    CL_NEED(out);
+    *out = nullptr;
+    return guarded([&](std::string* e) -> cl_status {
+        std::unique_ptr<cl_cache> c(new cl_cache());
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            c->stream = nullptr;
+            cudaGetLastError();
+            *e = "cudaStreamCreate failed";
+            return CL_ERR_CUDA;
+        }
+        c->own.reset(new clb::CacheNet(*network));
+        c->net = c->own.get();
+        CL_TRY(c->net->init(c->stream, e));
+        *out = c.release();
+        return CL_OK;
+    });
+}
+
+cl_status cl_cache_destroy(cl_cache* cache)
+{
+    if (cache && !cache->own)
+    {
+        clb::setLastError("an integrator's radiance cache is destroyed with the integrator");
+        return CL_ERR_INVALID_ARG;
+    }
+    delete cache;
+    return CL_OK;
+}
+
+cl_status cl_cache_param_count(const cl_cache* cache, uint64_t* count)
+{
+    CL_NEED(cache);
+    CL_NEED(count);
+    *count = cache->net->paramCount();
+    return CL_OK;
+}
+
+cl_status cl_cache_get_resolutions(const cl_cache* cache, uint32_t* resolutions16)
+{
+    CL_NEED(cache);
+    CL_NEED(resolutions16);
+    for (int l = 0; l < CL_GUIDE_LEVELS; ++l) resolutions16[l] = cache->net->resolutions()[l];
+    return CL_OK;
+}
+
+cl_status cl_cache_set_params(cl_cache* cache, const float* params, uint64_t count)
+{
+    CL_NEED(cache);
+    return guarded([&](std::string* e) { return cache->net->setParams(params, count, e); });
+}
+
+cl_status cl_cache_get_params(const cl_cache* cache, float* params, uint64_t count)
+{
+    CL_NEED(cache);
+    return guarded([&](std::string* e) { return cache->net->getParams(params, count, e); });
+}
+
+cl_status cl_cache_forward(cl_cache* cache, const float* in9, uint32_t count, float* out16)
+{
+    CL_NEED(cache);
+    return guarded([&](std::string* e) { return cache->net->forward(in9, count, out16, e); });
+}
+
+cl_status cl_cache_gradient(cl_cache* cache, const float* rec12, uint32_t count, double* loss, float* grad)
+{
+    CL_NEED(cache);
+    return guarded([&](std::string* e) { return cache->net->gradient(rec12, count, loss, grad, e); });
+}
+
+cl_status cl_cache_train_step(cl_cache* cache, const float* rec12, uint32_t count, double* loss)
+{
+    CL_NEED(cache);
+    return guarded([&](std::string* e) { return cache->net->trainStepHost(rec12, count, loss, e); });
+}
+
+cl_status cl_integrator_set_radiance_cache(cl_integrator* it, const cl_radiance_cache_config* config)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.setRadianceCache(config, e); });
+}
+
+cl_status cl_integrator_get_cache(cl_integrator* it, cl_cache** cache)
+{
+    CL_NEED(it);
+    CL_NEED(cache);
+    clb::CacheNet* net = it->impl.cacheNet();
+    if (!net)
+    {
+        *cache = nullptr;
+        return CL_OK;
+    }
+    it->cacheView.net    = net;
+    it->cacheView.stream = nullptr;
+    *cache               = &it->cacheView;
+    return CL_OK;
+}
+
+cl_status cl_integrator_cache_stats(cl_integrator* it, cl_guide_stats* stats)
+{
+    CL_NEED(it);
+    CL_NEED(stats);
+    return guarded([&](std::string* e) { return it->impl.cacheStats(stats, e); });
 }
 
 } // extern "C"

@@ -1,12 +1,14 @@
-// Guiding network kernels: parameter initialisation, fragment-ordered weight
-// copies, inference, the fused training forward/backward pass, the
-// weight-gradient reduction over the batch, and Adam.  No counterpart in the
-// reference renderer.
+// Hash-grid + tensor-core MLP networks of the path tracer (no counterpart in
+// the reference renderer): the guiding network and the radiance cache share
+// the encoding, the fused training forward/backward pass, the
+// weight-gradient reduction over the batch and Adam; they differ in shape
+// (MlpShape) and in the loss at the head (GuideLoss, CacheLoss).
 #include "cl_guide.h"
 
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 namespace clb
@@ -15,10 +17,10 @@ using namespace guide;
 
 namespace
 {
-constexpr int kInferWarps = 8;  // inference: 8 warps x 32 samples per CTA pass
-constexpr int kTrainWarps = 4;  // training forward/backward: 4 warps x 16 samples
-constexpr int kGradChunk  = 4096; // samples per weight-gradient block
-constexpr int kGradStep   = 64;   // samples staged in shared memory per step
+constexpr int kInferWarps = 8;            // inference: 8 warps x 32 samples per CTA pass
+constexpr int kTrainWarps = 4;            // training forward/backward: 4 warps x 16 samples
+constexpr int kGradChunk  = 4096;         // samples per weight-gradient block
+constexpr int kGradStep   = 64;           // samples staged in shared memory per step
 constexpr int kXTile      = 32 * kXS * 2; // bytes of a 32-row encoded tile (6656)
 
 __device__ __forceinline__ uint32_t laneIdx() { return threadIdx.x & 31u; }
@@ -37,9 +39,9 @@ __device__ __forceinline__ float uniformPM1(uint64_t seed, uint64_t i)
 }
 
 // Hash entries U[-1e-4, 1e-4]; W_l Glorot-uniform sqrt(6 / (in + out)).
-__global__ void kInitParams(float* p, uint64_t hashN, uint32_t seed)
+template <class S> __global__ void kInitParams(float* p, uint64_t hashN, uint32_t seed)
 {
-    uint64_t n = hashN + kMlpParams;
+    uint64_t n = hashN + S::kParams;
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
     {
         float u = uniformPM1(seed, i);
@@ -48,8 +50,8 @@ __global__ void kInitParams(float* p, uint64_t hashN, uint32_t seed)
         else
         {
             int o = int(i - hashN), l = 0;
-            while (l < kLayers - 1 && o >= weightOffset(l + 1)) ++l;
-            p[i] = u * sqrtf(6.0f / float(layerIn(l) + layerOut(l)));
+            while (l < S::kLayers - 1 && o >= S::woff(l + 1)) ++l;
+            p[i] = u * sqrtf(6.0f / float(S::in(l) + S::out(l)));
         }
     }
 }
@@ -64,27 +66,27 @@ __global__ void kTableCopy(const float* __restrict__ p, __nv_bfloat16* __restric
 // (g, t): b0 = W[8nt+g][16kt+2t .. +1], b1 = W[8nt+g][16kt+2t+8 .. +9].
 // Backward fragment (kt over outputs, nt over inputs): b0 = W[16kt+2t][8nt+g],
 // W[16kt+2t+1][8nt+g]; b1 the same 8 rows further down.
-__global__ void kFrags(const float* __restrict__ mlp, uint2* __restrict__ wf, uint2* __restrict__ wb)
+template <class S> __global__ void kFrags(const float* __restrict__ mlp, uint2* __restrict__ wf, uint2* __restrict__ wb)
 {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < kFwdFrags * 32)
+    if (e < S::kFwdFrags * 32)
     {
         int f = e >> 5, lane = e & 31, l = 0;
-        while (l < kLayers - 1 && f >= fwdFragOffset(l + 1)) ++l;
-        int          loc = f - fwdFragOffset(l), kt = loc / fwdNT(l), nt = loc % fwdNT(l);
-        int          g = lane >> 2, t = lane & 3, K = layerIn(l);
-        const float* W   = mlp + weightOffset(l) + (nt * 8 + g) * K + kt * 16 + 2 * t;
+        while (l < S::kLayers - 1 && f >= S::fwdOff(l + 1)) ++l;
+        int          loc = f - S::fwdOff(l), kt = loc / S::fwdNT(l), nt = loc % S::fwdNT(l);
+        int          g = lane >> 2, t = lane & 3, K = S::in(l);
+        const float* W   = mlp + S::woff(l) + (nt * 8 + g) * K + kt * 16 + 2 * t;
         wf[e]            = make_uint2(packBf16(W[0], W[1]), packBf16(W[8], W[9]));
         return;
     }
-    e -= kFwdFrags * 32;
-    if (e < kBwdFrags * 32)
+    e -= S::kFwdFrags * 32;
+    if (e < S::kBwdFrags * 32)
     {
         int f = e >> 5, lane = e & 31, l = 0;
-        while (l < kLayers - 1 && f >= bwdFragOffset(l + 1)) ++l;
-        int          loc = f - bwdFragOffset(l), kt = loc / bwdNT(l), nt = loc % bwdNT(l);
-        int          g = lane >> 2, t = lane & 3, K = layerIn(l);
-        const float* W   = mlp + weightOffset(l) + (kt * 16 + 2 * t) * K + nt * 8 + g;
+        while (l < S::kLayers - 1 && f >= S::bwdOff(l + 1)) ++l;
+        int          loc = f - S::bwdOff(l), kt = loc / S::bwdNT(l), nt = loc % S::bwdNT(l);
+        int          g = lane >> 2, t = lane & 3, K = S::in(l);
+        const float* W   = mlp + S::woff(l) + (kt * 16 + 2 * t) * K + nt * 8 + g;
         wb[e]            = make_uint2(packBf16(W[0], W[K]), packBf16(W[8 * K], W[9 * K]));
     }
 }
@@ -98,16 +100,17 @@ __device__ __forceinline__ void loadFrags(uint2* dst, const uint2* __restrict__ 
 
 __device__ __forceinline__ f3 ldf3(const float* p) { return {p[0], p[1], p[2]}; }
 
-// Forward pass of `n` host-given samples (in9 rows) -> raw head outputs.
+// Forward pass of `n` host-given samples (in9 rows) -> raw outputs.
+template <class S>
 __global__ void __launch_bounds__(kInferWarps * 32) kInferUnit(GridView g, const uint2* __restrict__ wfG,
                                                                 const float* __restrict__ in9, uint32_t n,
-                                                                float* __restrict__ out48)
+                                                                float* __restrict__ out)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2*         wf   = reinterpret_cast<uint2*>(smem);
     const uint32_t lane = laneIdx(), warp = threadIdx.x >> 5;
-    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + kFwdFragBytes + warp * kXTile);
-    loadFrags(wf, wfG, kFwdFrags * 32);
+    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + S::kFwdBytes + warp * kXTile);
+    loadFrags(wf, wfG, S::kFwdFrags * 32);
     __syncthreads();
     for (uint32_t base = (blockIdx.x * kInferWarps + warp) * 32u; base < n; base += gridDim.x * kInferWarps * 32u)
     {
@@ -120,19 +123,19 @@ __global__ void __launch_bounds__(kInferWarps * 32) kInferUnit(GridView g, const
         else
             zeroRow(x + lane * kXS);
         __syncwarp();
-        float out[2][6][4];
-        mlpInfer<2>(wf, x, lane, out);
+        float acc[2][S::kOut / 8][4];
+        mlpInfer<S, 2>(wf, x, lane, acc);
         __syncwarp();
         float* o = reinterpret_cast<float*>(x);
-        storeOut<2>(out, o, lane);
+        storeOut<S, 2>(acc, o, lane);
         __syncwarp();
         if (i < n)
-            for (int c = 0; c < kOut; ++c) out48[size_t(i) * kOut + c] = o[lane * kOS + c];
+            for (int c = 0; c < S::kOut; ++c) out[size_t(i) * S::kOut + c] = o[lane * S::kOS + c];
         __syncwarp();
     }
 }
 
-// Mixture sample / pdf of given head outputs.
+// Mixture sample / pdf of given guide outputs (the network's mixture alone).
 __global__ void kSampleUnit(const float* __restrict__ out48, const float* __restrict__ u3, uint32_t n,
                             float* __restrict__ dir, float* __restrict__ pdf)
 {
@@ -170,8 +173,8 @@ struct TrainArgs
     float2*        gradTable;
     __nv_bfloat16* acts;
     __nv_bfloat16* deltas;
-    double*        scal; // [0] sum of weights, [1] loss, [3] sum of clamped weights
-    int            learnSel;
+    double*        scal;     // [0] sum of weights, [1] loss, [3] sum of clamped weights
+    int            learnSel; // guide: learned selection probability
     float          clamp;    // weight clamp (x batch mean), 0 = off
 };
 
@@ -272,6 +275,63 @@ __device__ __forceinline__ float headLossGrad(const float* o, f3 om, float* grad
     return m + logf(R);
 }
 
+} // namespace
+
+// Per-sample loss l(o) and dl/do of the guiding network: -log p_guide(omega),
+// or with the learned selection probability -log((1 - a) p_bsdf + a p_guide)
+// (lobe gradients scaled by a p_guide / p_mix, selection logit
+// (p_guide - p_bsdf) / p_mix da/dlogit).  Record: omega in r3.xyz, the BSDF
+// pdf of omega in r3.w.
+struct GuideLoss
+{
+    static constexpr int kOut = GuideShape::kOut;
+    __device__ static float eval(const float* o, float4 r3, int learnSel, float* grad)
+    {
+        float lp = headLossGrad(o, f3{r3.x, r3.y, r3.z}, grad);
+        if (learnSel)
+        {
+            const float x  = o[kSelOut];
+            const float sg = 1.0f / (1.0f + expf(-x));
+            const float al = kSelMin + (kSelMax - kSelMin) * sg;
+            const float pg = expf(lp), pb = r3.w;
+            const float pm = fmaxf((1.0f - al) * pb + al * pg, 1e-30f);
+            const float sc = al * pg / pm;
+#pragma unroll
+            for (int c = 0; c < 5 * kLobes; ++c) grad[c] *= sc;
+            grad[kSelOut] = (pg - pb) / pm * (kSelMax - kSelMin) * sg * (1.0f - sg);
+            lp            = logf(pm);
+        }
+#pragma unroll
+        for (int c = 0; c < kOut; ++c) grad[c] = -grad[c];
+        return -lp;
+    }
+};
+
+// Radiance cache: relative L2 of the RGB prediction o[0..2] against the
+// path-traced target r3.xyz (Mueller et al. 2021): mean over the channels of
+// (o - y)^2 / (o^2 + 0.01), the denominator held constant in the gradient.
+struct CacheLoss
+{
+    static constexpr int kOut = CacheShape::kOut;
+    __device__ static float eval(const float* o, float4 r3, int, float* grad)
+    {
+        const float y[3] = {r3.x, r3.y, r3.z};
+        float       l    = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+        {
+            const float d = o[c] - y[c], den = o[c] * o[c] + 0.01f;
+            l += d * d / den;
+            grad[c] = (2.0f / 3.0f) * d / den;
+        }
+#pragma unroll
+        for (int c = 3; c < kOut; ++c) grad[c] = 0.0f;
+        return l * (1.0f / 3.0f);
+    }
+};
+
+namespace
+{
 // A fragments (k-tiles kt < KT) of a 16-row tile -> bf16 rows of a staging
 // matrix (row stride ld, starting at column 0 of `base`), rows < valid.
 template <int KT>
@@ -335,30 +395,34 @@ __device__ __forceinline__ void backHidden(const uint2* __restrict__ wbL, const 
     }
 }
 
-constexpr int kTrainXBytes    = 16 * kXS * 2;                // 3328: encoded inputs, then head outputs
-constexpr int kTrainDBytes    = 16 * kDS * 2;                // 1792: head-output gradients
-constexpr int kTrainWarpBytes = kTrainXBytes + kTrainDBytes + 16 * 3 * 4;
-constexpr int kTrainSmem      = kFwdFragBytes + kBwdFragBytes + kTrainWarps * kTrainWarpBytes;
-static_assert(16 * kOS * 4 <= kTrainXBytes, "output tile must fit in the input tile");
-static_assert(kTrainWarpBytes % 16 == 0, "warp staging must stay 16-byte aligned");
+template <class S> struct TrainSmem
+{
+    static constexpr int kX    = 16 * kXS * 2;    // encoded inputs, then the outputs (16 x kOS floats)
+    static constexpr int kD    = 16 * S::kDS * 2; // output gradients
+    static constexpr int kWarp = (kX + kD + 16 * 3 * 4 + 15) / 16 * 16;
+    static constexpr int kAll  = S::kFwdBytes + S::kBwdBytes + kTrainWarps * kWarp;
+    static_assert(16 * S::kOS * 4 <= kX, "output tile must fit in the input tile");
+};
 
 // Forward and backward pass of the training batch, 16 samples per warp tile:
 // encodes, runs the MLP keeping every layer's input in registers, writes the
 // inputs and the back-propagated output gradients of every layer (bf16) for
 // the weight-gradient reduction, accumulates the loss, and scatters the
 // input gradient of the hash features to the table gradient (float2 atomics).
-__global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
+template <class S, class LOSS> __global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
 {
+    using TS = TrainSmem<S>;
+    constexpr int NT = S::kOut / 8, NH = S::kHidden;
     extern __shared__ __align__(16) unsigned char smem[];
     uint2*         wf   = reinterpret_cast<uint2*>(smem);
-    uint2*         wb   = reinterpret_cast<uint2*>(smem + kFwdFragBytes);
+    uint2*         wb   = reinterpret_cast<uint2*>(smem + S::kFwdBytes);
     const uint32_t lane = laneIdx(), warp = threadIdx.x >> 5;
-    unsigned char* ws   = smem + kFwdFragBytes + kBwdFragBytes + warp * kTrainWarpBytes;
+    unsigned char* ws   = smem + S::kFwdBytes + S::kBwdBytes + warp * TS::kWarp;
     __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(ws);
-    __nv_bfloat16* dT   = reinterpret_cast<__nv_bfloat16*>(ws + kTrainXBytes);
-    float*         posS = reinterpret_cast<float*>(ws + kTrainXBytes + kTrainDBytes);
-    loadFrags(wf, a.wf, kFwdFrags * 32);
-    loadFrags(wb, a.wb, kBwdFrags * 32);
+    __nv_bfloat16* dT   = reinterpret_cast<__nv_bfloat16*>(ws + TS::kX);
+    float*         posS = reinterpret_cast<float*>(ws + TS::kX + TS::kD);
+    loadFrags(wf, a.wf, S::kFwdFrags * 32);
+    loadFrags(wb, a.wb, S::kBwdFrags * 32);
     __syncthreads();
     const uint32_t count = *a.count, nB = min(count, a.batch);
     const double   wsum  = a.clamp > 0.0f ? a.scal[3] : a.scal[0];
@@ -401,87 +465,87 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
         {
             uint32_t rr = e / 12u, c = e % 12u;
             if (rr < rows)
-                reinterpret_cast<uint4*>(a.acts + size_t(j0 + rr) * kActRow)[c] =
+                reinterpret_cast<uint4*>(a.acts + size_t(j0 + rr) * S::kActRow)[c] =
                     reinterpret_cast<const uint4*>(x + rr * kXS)[c];
         }
-        uint32_t h[4][1][4][4];
-        float    out[1][6][4];
-        mlpForward<1>(wf, x, lane, h, out);
+        uint32_t h[NH + 1][1][4][4];
+        float    out[1][NT][4];
+        mlpForward<S, 1>(wf, x, lane, h, out);
 #pragma unroll
-        for (int l = 0; l < 4; ++l)
-            storeA<4>(h[l][0], a.acts + size_t(j0) * kActRow + actOffset(l + 1), kActRow, rows, lane);
+        for (int l = 0; l <= NH; ++l)
+            storeA<4>(h[l][0], a.acts + size_t(j0) * S::kActRow + S::actOff(l + 1), S::kActRow, rows, lane);
         __syncwarp();
         float* o = reinterpret_cast<float*>(x);
-        storeOut<1>(out, o, lane);
+        storeOut<S, 1>(out, o, lane);
         __syncwarp();
         float lossPart = 0.0f;
         if (lane < 16u)
         {
-            uint32_t* drow = reinterpret_cast<uint32_t*>(dT + lane * kDS);
+            uint32_t* drow = reinterpret_cast<uint32_t*>(dT + lane * S::kDS);
             if (valid)
             {
                 float4 r0 = R[0], r3 = R[3];
-                float  gr[kOut];
-                float  lp = headLossGrad(o + lane * kOS, f3{r3.x, r3.y, r3.z}, gr);
-                if (a.learnSel)
-                {
-                    // -log((1 - a) p_bsdf + a p_guide): lobe gradients scaled
-                    // by a p_guide / p_mix, selection logit (p_g - p_b) / p_mix da.
-                    const float x   = o[lane * kOS + kSelOut];
-                    const float sg  = 1.0f / (1.0f + expf(-x));
-                    const float al  = kSelMin + (kSelMax - kSelMin) * sg;
-                    const float pg  = expf(lp), pb = r3.w;
-                    const float pm  = fmaxf((1.0f - al) * pb + al * pg, 1e-30f);
-                    const float sc  = al * pg / pm;
+                float  gr[S::kOut];
+                float  l  = LOSS::eval(o + lane * S::kOS, r3, a.learnSel, gr);
+                float  sw = trainWeight(r0.w, a, nB) * invW;
+                lossPart  = sw * l;
 #pragma unroll
-                    for (int c = 0; c < 5 * kLobes; ++c) gr[c] *= sc;
-                    gr[kSelOut] = (pg - pb) / pm * (kSelMax - kSelMin) * sg * (1.0f - sg);
-                    lp          = logf(pm);
-                }
-                float  s  = -trainWeight(r0.w, a, nB) * invW;
-                lossPart  = s * lp;
-#pragma unroll
-                for (int c = 0; c < kOut / 2; ++c) drow[c] = packBf16(gr[2 * c] * s, gr[2 * c + 1] * s);
+                for (int c = 0; c < S::kOut / 2; ++c) drow[c] = packBf16(gr[2 * c] * sw, gr[2 * c + 1] * sw);
             }
             else
 #pragma unroll
-                for (int c = 0; c < kOut / 2; ++c) drow[c] = 0u;
+                for (int c = 0; c < S::kOut / 2; ++c) drow[c] = 0u;
         }
         for (int off = 16; off > 0; off >>= 1) lossPart += __shfl_xor_sync(0xffffffffu, lossPart, off);
         if (lane == 0 && lossPart != 0.0f) atomicAdd(&a.scal[1], double(lossPart));
         __syncwarp();
-        for (uint32_t e = lane; e < 16u * 6u; e += 32u)
+        for (uint32_t e = lane; e < 16u * (S::kOut / 8); e += 32u)
         {
-            uint32_t rr = e / 6u, c = e % 6u;
+            uint32_t rr = e / (S::kOut / 8), c = e % (S::kOut / 8);
             if (rr < rows)
-                reinterpret_cast<uint4*>(a.deltas + size_t(j0 + rr) * kDeltaRow + deltaOffset(4))[c] =
-                    reinterpret_cast<const uint4*>(dT + rr * kDS)[c];
+                reinterpret_cast<uint4*>(a.deltas + size_t(j0 + rr) * S::kDeltaRow + S::deltaOff(NH + 1))[c] =
+                    reinterpret_cast<const uint4*>(dT + rr * S::kDS)[c];
         }
-        // Backward: layer 4 (3 k-tiles over its 48 outputs), then 3, 2, 1.
-        uint32_t d4[4][4], d3[4][4];
+        // Backward: the output layer (kOut/16 k-tiles), then the hidden layers.
+        uint32_t da[4][4], db[4][4];
 #pragma unroll
-        for (int kt = 0; kt < 3; ++kt) loadA(d4[kt], dT, kDS, kt, lane);
-        d4[3][0] = d4[3][1] = d4[3][2] = d4[3][3] = 0u;
-        backHidden<3>(wb + bwdFragOffset(4) * 32, d4, h[3][0], d3, lane);
-        storeA<4>(d3, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(3), kDeltaRow, rows, lane);
-        backHidden<4>(wb + bwdFragOffset(3) * 32, d3, h[2][0], d4, lane);
-        storeA<4>(d4, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(2), kDeltaRow, rows, lane);
-        backHidden<4>(wb + bwdFragOffset(2) * 32, d4, h[1][0], d3, lane);
-        storeA<4>(d3, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(1), kDeltaRow, rows, lane);
-        backHidden<4>(wb + bwdFragOffset(1) * 32, d3, h[0][0], d4, lane);
-        storeA<4>(d4, a.deltas + size_t(j0) * kDeltaRow + deltaOffset(0), kDeltaRow, rows, lane);
+        for (int kt = 0; kt < 4; ++kt)
+        {
+            if (kt < S::kOut / 16)
+                loadA(da[kt], dT, S::kDS, kt, lane);
+            else
+                da[kt][0] = da[kt][1] = da[kt][2] = da[kt][3] = 0u;
+        }
+        backHidden<S::kOut / 16>(wb + S::bwdOff(NH + 1) * 32, da, h[NH][0], db, lane);
+        storeA<4>(db, a.deltas + size_t(j0) * S::kDeltaRow + S::deltaOff(NH), S::kDeltaRow, rows, lane);
+#pragma unroll
+        for (int l = NH; l >= 1; --l)
+        {
+            // output gradient of layer l is in db when (NH - l) is even
+            if (((NH - l) & 1) == 0)
+            {
+                backHidden<4>(wb + S::bwdOff(l) * 32, db, h[l - 1][0], da, lane);
+                storeA<4>(da, a.deltas + size_t(j0) * S::kDeltaRow + S::deltaOff(l - 1), S::kDeltaRow, rows, lane);
+            }
+            else
+            {
+                backHidden<4>(wb + S::bwdOff(l) * 32, da, h[l - 1][0], db, lane);
+                storeA<4>(db, a.deltas + size_t(j0) * S::kDeltaRow + S::deltaOff(l - 1), S::kDeltaRow, rows, lane);
+            }
+        }
+        const uint32_t(&d0)[4][4] = (NH & 1) ? da : db;
         // Layer 0: gradient of the 32 hash features (FP32).
         float gx[4][4];
 #pragma unroll
         for (int n = 0; n < 4; ++n) gx[n][0] = gx[n][1] = gx[n][2] = gx[n][3] = 0.0f;
-        const uint2* w0 = wb + bwdFragOffset(0) * 32;
+        const uint2* w0 = wb;
 #pragma unroll
         for (int kt = 0; kt < 4; ++kt)
 #pragma unroll
             for (int nt = 0; nt < 4; ++nt)
             {
                 uint2 b = w0[(kt * 4 + nt) * 32 + lane];
-                mma16816(gx[nt], d4[kt], b.x, b.y);
+                mma16816(gx[nt], d0[kt], b.x, b.y);
             }
         // Column 8nt + 2t + f is feature f of level 4nt + t.
 #pragma unroll
@@ -492,16 +556,16 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
             for (int hr = 0; hr < 2; ++hr)
             {
                 const uint32_t rr = g + 8u * hr;
-                const float    d0 = gx[nt][2 * hr], d1 = gx[nt][2 * hr + 1];
-                if (rr >= rows || (d0 == 0.0f && d1 == 0.0f)) continue;
-                f3     p    = {posS[3 * rr], posS[3 * rr + 1], posS[3 * rr + 2]};
-                Cell   c    = gridCell(a.g.res[level], p);
-                float2* gb  = a.gradTable + (size_t(level) << a.g.log2T);
+                const float    d0v = gx[nt][2 * hr], d1v = gx[nt][2 * hr + 1];
+                if (rr >= rows || (d0v == 0.0f && d1v == 0.0f)) continue;
+                f3      p  = {posS[3 * rr], posS[3 * rr + 1], posS[3 * rr + 2]};
+                Cell    c  = gridCell(a.g.res[level], p);
+                float2* gb = a.gradTable + (size_t(level) << a.g.log2T);
 #pragma unroll
                 for (int k = 0; k < 8; ++k)
                 {
                     float w = cornerWeight(c, k);
-                    atomicAdd(gb + cornerIndex(a.g, level, c, k), make_float2(w * d0, w * d1));
+                    atomicAdd(gb + cornerIndex(a.g, level, c, k), make_float2(w * d0v, w * d1v));
                 }
             }
         }
@@ -514,13 +578,14 @@ __global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
 // 64 samples at a time and read transposed with ldmatrix.trans; warp w owns
 // output rows 16w..16w+15 of the layer; FP32 partials go to the gradient with
 // one atomicAdd per element per block.
+template <class S>
 __global__ void __launch_bounds__(128) kWeightGrad(const __nv_bfloat16* __restrict__ acts,
                                                    const __nv_bfloat16* __restrict__ deltas, const uint32_t* count,
                                                    uint32_t batch, float* __restrict__ gradMlp)
 {
     __shared__ __align__(16) __nv_bfloat16 dS[kGradStep][kWidth + 8];
     __shared__ __align__(16) __nv_bfloat16 aS[kGradStep][kIn + 8];
-    const int      l = blockIdx.y, O = layerOut(l), I = layerIn(l);
+    const int      l = blockIdx.y, O = S::out(l), I = S::in(l);
     const uint32_t nB = min(*count, batch);
     const uint32_t s0 = blockIdx.x * kGradChunk, s1 = min(s0 + uint32_t(kGradChunk), nB);
     if (s0 >= s1) return;
@@ -535,16 +600,18 @@ __global__ void __launch_bounds__(128) kWeightGrad(const __nv_bfloat16* __restri
         __syncthreads();
         for (int e = threadIdx.x; e < kGradStep * dq; e += blockDim.x)
         {
-            int  rr = e / dq, c = e % dq;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (s + rr < s1) v = __ldg(reinterpret_cast<const uint4*>(deltas + size_t(s + rr) * kDeltaRow + deltaOffset(l)) + c);
+            int   rr = e / dq, c = e % dq;
+            uint4 v  = make_uint4(0u, 0u, 0u, 0u);
+            if (s + rr < s1)
+                v = __ldg(reinterpret_cast<const uint4*>(deltas + size_t(s + rr) * S::kDeltaRow + S::deltaOff(l)) + c);
             reinterpret_cast<uint4*>(&dS[rr][0])[c] = v;
         }
         for (int e = threadIdx.x; e < kGradStep * aq; e += blockDim.x)
         {
-            int  rr = e / aq, c = e % aq;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (s + rr < s1) v = __ldg(reinterpret_cast<const uint4*>(acts + size_t(s + rr) * kActRow + actOffset(l)) + c);
+            int   rr = e / aq, c = e % aq;
+            uint4 v  = make_uint4(0u, 0u, 0u, 0u);
+            if (s + rr < s1)
+                v = __ldg(reinterpret_cast<const uint4*>(acts + size_t(s + rr) * S::kActRow + S::actOff(l)) + c);
             reinterpret_cast<uint4*>(&aS[rr][0])[c] = v;
         }
         __syncthreads();
@@ -569,7 +636,7 @@ __global__ void __launch_bounds__(128) kWeightGrad(const __nv_bfloat16* __restri
     }
     if (!active) return;
     const uint32_t g = lane >> 2, t = lane & 3u;
-    float*         G = gradMlp + weightOffset(l);
+    float*         G = gradMlp + S::woff(l);
 #pragma unroll
     for (int nt = 0; nt < 12; ++nt)
     {
@@ -643,18 +710,18 @@ int gridFor(uint64_t n, int block, int cap)
 void guideDefaultConfig(cl_guide_config* c)
 {
     std::memset(c, 0, sizeof(*c));
-    c->log2_table    = 19;
-    c->n_min         = 16.0f;
-    c->n_max         = 1024.0f;
-    c->learning_rate = 1e-2f;
-    c->beta1         = 0.9f;
-    c->beta2         = 0.99f;
-    c->epsilon       = 1e-10f;
-    c->bsdf_fraction = 0.5f;
-    c->batch         = 1u << 18;
-    c->train_spp     = 32;
-    c->class_mask    = 3u;
-    c->seed          = 1;
+    c->log2_table      = 19;
+    c->n_min           = 16.0f;
+    c->n_max           = 1024.0f;
+    c->learning_rate   = 1e-2f;
+    c->beta1           = 0.9f;
+    c->beta2           = 0.99f;
+    c->epsilon         = 1e-10f;
+    c->bsdf_fraction   = 0.5f;
+    c->batch           = 1u << 18;
+    c->train_spp       = 32;
+    c->class_mask      = 3u;
+    c->seed            = 1;
     c->learn_selection = 0u;
     c->weight_clamp    = 0.0f;
 }
@@ -667,15 +734,15 @@ cl_status guideResolutions(float nmin, float nmax, uint32_t* res)
     return CL_OK;
 }
 
-GuideNet::GuideNet(const cl_guide_config& c) : cfg_(c) {}
-GuideNet::~GuideNet() = default;
+template <class S, class L> HashNet<S, L>::HashNet(const cl_guide_config& c) : cfg_(c) {}
+template <class S, class L> HashNet<S, L>::~HashNet() = default;
 
-cl_status GuideNet::init(cudaStream_t st, std::string* err)
+template <class S, class L> cl_status HashNet<S, L>::init(cudaStream_t st, std::string* err)
 {
     st_ = st;
     if (cfg_.log2_table < 8 || cfg_.log2_table > 24)
     {
-        *err = "guide: log2_table must be in [8, 24]";
+        *err = "network: log2_table must be in [8, 24]";
         return CL_ERR_INVALID_ARG;
     }
     if (cfg_.batch == 0 || cfg_.batch > (1u << 24) || !(cfg_.learning_rate > 0.0f) || !(cfg_.bsdf_fraction >= 0.0f) ||
@@ -683,7 +750,7 @@ cl_status GuideNet::init(cudaStream_t st, std::string* err)
         !(cfg_.beta2 >= 0.0f && cfg_.beta2 < 1.0f) || !(cfg_.epsilon >= 0.0f) || cfg_.learn_selection > 1u ||
         !(cfg_.weight_clamp >= 0.0f))
     {
-        *err = "guide: batch, learning rate, Adam or bsdf_fraction out of range";
+        *err = "network: batch, learning rate, Adam, bsdf_fraction, learn_selection or weight_clamp out of range";
         return CL_ERR_INVALID_ARG;
     }
     bool given = false;
@@ -694,7 +761,7 @@ cl_status GuideNet::init(cudaStream_t st, std::string* err)
         {
             if (cfg_.resolutions[l] < 1u || cfg_.resolutions[l] > (1u << 24))
             {
-                *err = "guide: resolutions must be in [1, 2^24]";
+                *err = "network: resolutions must be in [1, 2^24]";
                 return CL_ERR_INVALID_ARG;
             }
             res_[l] = cfg_.resolutions[l];
@@ -702,7 +769,7 @@ cl_status GuideNet::init(cudaStream_t st, std::string* err)
     }
     else if (guideResolutions(cfg_.n_min, cfg_.n_max, res_) != CL_OK)
     {
-        *err = "guide: n_min/n_max out of range";
+        *err = "network: n_min/n_max out of range";
         return CL_ERR_INVALID_ARG;
     }
     const uint64_t T = 1ull << cfg_.log2_table;
@@ -717,24 +784,27 @@ cl_status GuideNet::init(cudaStream_t st, std::string* err)
     int dev = 0;
     CL_CUDA(cudaGetDevice(&dev), err);
     CL_CUDA(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, dev), err);
-    CL_CUDA(cudaFuncSetAttribute(kInferUnit, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kFwdFragBytes + kInferWarps * kXTile),
+    CL_CUDA(cudaFuncSetAttribute(kInferUnit<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 S::kFwdBytes + kInferWarps * kXTile),
             err);
-    CL_CUDA(cudaFuncSetAttribute(kTrainFwdBwd, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem), err);
+    CL_CUDA(cudaFuncSetAttribute(kTrainFwdBwd<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrainSmem<S>::kAll),
+            err);
     int occ = 0;
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kTrainFwdBwd, kTrainWarps * 32, kTrainSmem), err);
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kTrainFwdBwd<S, L>, kTrainWarps * 32,
+                                                          TrainSmem<S>::kAll),
+            err);
     trainBlocks_ = numSMs_ * (occ > 0 ? occ : 1);
     CL_TRY(params_.alloc(n * 4, err));
     CL_TRY(grad_.alloc(n * 4, err));
     CL_TRY(m_.alloc(n * 4, err));
     CL_TRY(v_.alloc(n * 4, err));
     CL_TRY(table_.alloc(hashParams_ * 2, err));
-    CL_TRY(wf_.alloc(kFwdFragBytes, err));
-    CL_TRY(wb_.alloc(kBwdFragBytes, err));
-    CL_TRY(acts_.alloc(size_t(cfg_.batch) * kActRow * 2, err));
-    CL_TRY(deltas_.alloc(size_t(cfg_.batch) * kDeltaRow * 2, err));
+    CL_TRY(wf_.alloc(S::kFwdBytes, err));
+    CL_TRY(wb_.alloc(S::kBwdBytes, err));
+    CL_TRY(acts_.alloc(size_t(cfg_.batch) * S::kActRow * 2, err));
+    CL_TRY(deltas_.alloc(size_t(cfg_.batch) * S::kDeltaRow * 2, err));
     CL_TRY(scal_.alloc(64, err));
-    kInitParams<<<gridFor(n, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), hashParams_, cfg_.seed);
+    kInitParams<S><<<gridFor(n, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), hashParams_, cfg_.seed);
     CL_CUDA(cudaGetLastError(), err);
     CL_CUDA(cudaMemsetAsync(grad_.p, 0, n * 4, st_), err);
     CL_CUDA(cudaMemsetAsync(m_.p, 0, n * 4, st_), err);
@@ -746,7 +816,7 @@ cl_status GuideNet::init(cudaStream_t st, std::string* err)
     return CL_OK;
 }
 
-GridView GuideNet::grid() const
+template <class S, class L> GridView HashNet<S, L>::grid() const
 {
     GridView g;
     g.table     = table_.as<const __nv_bfloat162>();
@@ -757,22 +827,22 @@ GridView GuideNet::grid() const
     return g;
 }
 
-cl_status GuideNet::refreshCopies(std::string* err)
+template <class S, class L> cl_status HashNet<S, L>::refreshCopies(std::string* err)
 {
     kTableCopy<<<gridFor(hashParams_, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), table_.as<__nv_bfloat16>(),
                                                                         hashParams_);
     CL_CUDA(cudaGetLastError(), err);
-    kFrags<<<((kFwdFrags + kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
-                                                                         wb_.as<uint2>());
+    kFrags<S><<<((S::kFwdFrags + S::kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_,
+                                                                                  wf_.as<uint2>(), wb_.as<uint2>());
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }
 
-cl_status GuideNet::setParams(const float* p, uint64_t n, std::string* err)
+template <class S, class L> cl_status HashNet<S, L>::setParams(const float* p, uint64_t n, std::string* err)
 {
     if (!p || n != paramCount())
     {
-        *err = "guide: parameter count mismatch";
+        *err = "network: parameter count mismatch";
         return CL_ERR_INVALID_ARG;
     }
     CL_CUDA(cudaMemcpyAsync(params_.p, p, n * 4, cudaMemcpyHostToDevice, st_), err);
@@ -785,11 +855,11 @@ cl_status GuideNet::setParams(const float* p, uint64_t n, std::string* err)
     return CL_OK;
 }
 
-cl_status GuideNet::getParams(float* p, uint64_t n, std::string* err)
+template <class S, class L> cl_status HashNet<S, L>::getParams(float* p, uint64_t n, std::string* err)
 {
     if (!p || n != paramCount())
     {
-        *err = "guide: parameter count mismatch";
+        *err = "network: parameter count mismatch";
         return CL_ERR_INVALID_ARG;
     }
     CL_CUDA(cudaMemcpyAsync(p, params_.p, n * 4, cudaMemcpyDeviceToHost, st_), err);
@@ -797,35 +867,43 @@ cl_status GuideNet::getParams(float* p, uint64_t n, std::string* err)
     return CL_OK;
 }
 
-cl_status GuideNet::forward(const float* in9, uint32_t n, float* out48, std::string* err)
+template <class S, class L>
+cl_status HashNet<S, L>::forward(const float* in9, uint32_t n, float* out, std::string* err)
 {
-    if ((!in9 || !out48) && n)
+    if ((!in9 || !out) && n)
     {
-        *err = "guide: null buffer";
+        *err = "network: null buffer";
         return CL_ERR_INVALID_ARG;
     }
     if (n == 0) return CL_OK;
     CL_TRY(io_.alloc(size_t(n) * 9 * 4, err));
-    CL_TRY(io2_.alloc(size_t(n) * kOut * 4, err));
+    CL_TRY(io2_.alloc(size_t(n) * S::kOut * 4, err));
     CL_CUDA(cudaMemcpyAsync(io_.p, in9, size_t(n) * 9 * 4, cudaMemcpyHostToDevice, st_), err);
-    const int smem = kFwdFragBytes + kInferWarps * kXTile;
-    kInferUnit<<<gridFor(n, kInferWarps * 32, numSMs_ * 2), kInferWarps * 32, smem, st_>>>(grid(), fwdFrags(), io_.f(),
-                                                                                           n, io2_.f());
+    const int smem = S::kFwdBytes + kInferWarps * kXTile;
+    kInferUnit<S><<<gridFor(n, kInferWarps * 32, numSMs_ * 2), kInferWarps * 32, smem, st_>>>(grid(), fwdFrags(),
+                                                                                              io_.f(), n, io2_.f());
     CL_CUDA(cudaGetLastError(), err);
-    CL_CUDA(cudaMemcpyAsync(out48, io2_.p, size_t(n) * kOut * 4, cudaMemcpyDeviceToHost, st_), err);
+    CL_CUDA(cudaMemcpyAsync(out, io2_.p, size_t(n) * S::kOut * 4, cudaMemcpyDeviceToHost, st_), err);
     CL_CUDA(cudaStreamSynchronize(st_), err);
     return CL_OK;
 }
 
-cl_status GuideNet::sample(const float* in9, const float* u3, uint32_t n, float* dir, float* pdf, std::string* err)
+template <class S, class L>
+cl_status HashNet<S, L>::sample(const float* in9, const float* u3, uint32_t n, float* dir, float* pdf,
+                                std::string* err)
 {
+    if (!std::is_same<S, GuideShape>::value)
+    {
+        *err = "sampling is defined for the guiding network only";
+        return CL_ERR_STATE;
+    }
     if (n == 0) return CL_OK;
     if (!in9 || !u3 || !dir || !pdf)
     {
-        *err = "guide: null buffer";
+        *err = "network: null buffer";
         return CL_ERR_INVALID_ARG;
     }
-    std::vector<float> out(size_t(n) * kOut);
+    std::vector<float> out(size_t(n) * S::kOut);
     CL_TRY(forward(in9, n, out.data(), err));
     DevBuf u, d, p;
     CL_TRY(u.alloc(size_t(n) * 12, err));
@@ -840,15 +918,21 @@ cl_status GuideNet::sample(const float* in9, const float* u3, uint32_t n, float*
     return CL_OK;
 }
 
-cl_status GuideNet::pdf(const float* in9, const float* dir, uint32_t n, float* pdf, std::string* err)
+template <class S, class L>
+cl_status HashNet<S, L>::pdf(const float* in9, const float* dir, uint32_t n, float* pdf, std::string* err)
 {
+    if (!std::is_same<S, GuideShape>::value)
+    {
+        *err = "the pdf is defined for the guiding network only";
+        return CL_ERR_STATE;
+    }
     if (n == 0) return CL_OK;
     if (!in9 || !dir || !pdf)
     {
-        *err = "guide: null buffer";
+        *err = "network: null buffer";
         return CL_ERR_INVALID_ARG;
     }
-    std::vector<float> out(size_t(n) * kOut);
+    std::vector<float> out(size_t(n) * S::kOut);
     CL_TRY(forward(in9, n, out.data(), err));
     DevBuf d, p;
     CL_TRY(d.alloc(size_t(n) * 12, err));
@@ -861,23 +945,28 @@ cl_status GuideNet::pdf(const float* in9, const float* dir, uint32_t n, float* p
     return CL_OK;
 }
 
-// rec14 rows -> device records; the record count goes to scal[2] (u32).
-cl_status GuideNet::upload(const float* rec14, uint32_t n, std::string* err)
+// Host records (kRecFloats per row) -> device records; the record count
+// goes to scal[2] (u32).  Guide rows: in9, omega, w, BSDF pdf of omega;
+// cache rows: in9, target RGB (weight 1).
+template <class S, class L> cl_status HashNet<S, L>::upload(const float* rec, uint32_t n, std::string* err)
 {
-    if (!rec14 || n == 0)
+    if (!rec || n == 0)
     {
-        *err = "guide: empty or null batch";
+        *err = "network: empty or null batch";
         return CL_ERR_INVALID_ARG;
     }
+    constexpr int      kf = kRecFloats;
     std::vector<float> h(size_t(n) * 16, 0.0f);
     for (uint32_t i = 0; i < n; ++i)
     {
-        const float* s = rec14 + 14 * size_t(i);
+        const float* s = rec + kf * size_t(i);
         float*       d = h.data() + 16 * size_t(i);
-        d[0] = s[0], d[1] = s[1], d[2] = s[2], d[3] = s[12];
+        d[0] = s[0], d[1] = s[1], d[2] = s[2];
         d[4] = s[3], d[5] = s[4], d[6] = s[5];
         d[8] = s[6], d[9] = s[7], d[10] = s[8];
-        d[12] = s[9], d[13] = s[10], d[14] = s[11], d[15] = s[13];
+        d[12] = s[9], d[13] = s[10], d[14] = s[11];
+        d[3]  = kf == 14 ? s[12] : 1.0f;
+        d[15] = kf == 14 ? s[13] : 0.0f;
     }
     CL_TRY(rec_.alloc(h.size() * 4, err));
     CL_CUDA(cudaMemcpyAsync(rec_.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, st_), err);
@@ -886,7 +975,8 @@ cl_status GuideNet::upload(const float* rec14, uint32_t n, std::string* err)
     return CL_OK;
 }
 
-cl_status GuideNet::computeGradient(const float4* rec, const uint32_t* count, std::string* err)
+template <class S, class L>
+cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* count, std::string* err)
 {
     CL_CUDA(cudaMemsetAsync(scal_.p, 0, 16, st_), err);
     CL_CUDA(cudaMemsetAsync(scal_.as<double>() + 3, 0, 8, st_), err);
@@ -910,41 +1000,43 @@ cl_status GuideNet::computeGradient(const float4* rec, const uint32_t* count, st
         kTrainPrep<<<numSMs_ * 2, 256, 0, st_>>>(a, 3);
         CL_CUDA(cudaGetLastError(), err);
     }
-    kTrainFwdBwd<<<trainBlocks_, kTrainWarps * 32, kTrainSmem, st_>>>(a);
+    kTrainFwdBwd<S, L><<<trainBlocks_, kTrainWarps * 32, TrainSmem<S>::kAll, st_>>>(a);
     CL_CUDA(cudaGetLastError(), err);
-    dim3 gg((cfg_.batch + kGradChunk - 1) / kGradChunk, kLayers);
-    kWeightGrad<<<gg, 128, 0, st_>>>(acts_.as<const __nv_bfloat16>(), deltas_.as<const __nv_bfloat16>(), count,
-                                     cfg_.batch, grad_.f() + hashParams_);
+    dim3 gg((cfg_.batch + kGradChunk - 1) / kGradChunk, S::kLayers);
+    kWeightGrad<S><<<gg, 128, 0, st_>>>(acts_.as<const __nv_bfloat16>(), deltas_.as<const __nv_bfloat16>(), count,
+                                        cfg_.batch, grad_.f() + hashParams_);
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }
 
-cl_status GuideNet::trainDevice(const float4* rec, const uint32_t* count, std::string* err)
+template <class S, class L>
+cl_status HashNet<S, L>::trainDevice(const float4* rec, const uint32_t* count, std::string* err)
 {
     CL_TRY(computeGradient(rec, count, err));
     ++step_;
-    const float c1 = float(1.0 - std::pow(double(cfg_.beta1), double(step_)));
-    const float c2 = float(1.0 - std::pow(double(cfg_.beta2), double(step_)));
+    const float    c1 = float(1.0 - std::pow(double(cfg_.beta1), double(step_)));
+    const float    c2 = float(1.0 - std::pow(double(cfg_.beta2), double(step_)));
     const uint64_t n4 = paramCount() / 4;
     AdamK          k{cfg_.beta1, cfg_.beta2, cfg_.epsilon, cfg_.learning_rate / c1, 1.0f / c2};
     kAdam<<<gridFor(n4 / 2, 256, numSMs_ * 8), 256, 0, st_>>>(params_.as<float4>(), grad_.as<float4>(),
                                                               m_.as<float4>(), v_.as<float4>(), n4, hashParams_ / 4, k,
                                                               table_.as<uint2>());
     CL_CUDA(cudaGetLastError(), err);
-    kFrags<<<((kFwdFrags + kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
-                                                                         wb_.as<uint2>());
+    kFrags<S><<<((S::kFwdFrags + S::kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_,
+                                                                                  wf_.as<uint2>(), wb_.as<uint2>());
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }
 
-cl_status GuideNet::gradient(const float* rec14, uint32_t n, double* loss, float* grad, std::string* err)
+template <class S, class L>
+cl_status HashNet<S, L>::gradient(const float* rec, uint32_t n, double* loss, float* grad, std::string* err)
 {
     if (!grad || !loss)
     {
-        *err = "guide: null output";
+        *err = "network: null output";
         return CL_ERR_INVALID_ARG;
     }
-    CL_TRY(upload(rec14, n, err));
+    CL_TRY(upload(rec, n, err));
     const uint32_t* cnt = reinterpret_cast<const uint32_t*>(scal_.as<unsigned char>() + 16);
     CL_TRY(computeGradient(rec_.as<const float4>(), cnt, err));
     CL_CUDA(cudaMemcpyAsync(grad, grad_.p, paramCount() * 4, cudaMemcpyDeviceToHost, st_), err);
@@ -954,14 +1046,18 @@ cl_status GuideNet::gradient(const float* rec14, uint32_t n, double* loss, float
     return CL_OK;
 }
 
-cl_status GuideNet::trainStepHost(const float* rec14, uint32_t n, double* loss, std::string* err)
+template <class S, class L>
+cl_status HashNet<S, L>::trainStepHost(const float* rec, uint32_t n, double* loss, std::string* err)
 {
-    CL_TRY(upload(rec14, n, err));
+    CL_TRY(upload(rec, n, err));
     const uint32_t* cnt = reinterpret_cast<const uint32_t*>(scal_.as<unsigned char>() + 16);
     CL_TRY(trainDevice(rec_.as<const float4>(), cnt, err));
     if (loss) CL_CUDA(cudaMemcpyAsync(loss, scal_.as<double>() + 1, 8, cudaMemcpyDeviceToHost, st_), err);
     CL_CUDA(cudaStreamSynchronize(st_), err);
     return CL_OK;
 }
+
+template class HashNet<GuideShape, GuideLoss>;
+template class HashNet<CacheShape, CacheLoss>;
 
 } // namespace clb

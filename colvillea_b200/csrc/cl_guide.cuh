@@ -20,41 +20,51 @@ namespace clb
 {
 namespace guide
 {
-constexpr int kLevels = 16, kFeat = 2, kHashF = 32, kBlob = 16, kIn = 96, kWidth = 64, kOut = 48, kLobes = 8;
-constexpr int kLayers = 5;
+constexpr int kLevels = 16, kFeat = 2, kHashF = 32, kBlob = 16, kIn = 96, kWidth = 64, kLobes = 8;
 constexpr int kXS = 104; // encoded-input tile row stride (bf16): 208 B, conflict-free ldmatrix rows
-constexpr int kOS = 49;  // output tile row stride (f32)
-constexpr int kDS = 56;  // output-gradient tile row stride (bf16): 112 B
 constexpr float kKappaMin = -5.0f, kKappaMax = 7.0f;
 constexpr float kSelMin = 0.05f, kSelMax = 0.95f; // learned guide-selection probability range
 constexpr int   kSelOut = 5 * kLobes;           // head output of its logit
 
-// Layer l: W_l is [out][in] row-major inside the flat MLP parameter block.
-__host__ __device__ constexpr int layerIn(int l) { return l == 0 ? kIn : kWidth; }
-__host__ __device__ constexpr int layerOut(int l) { return l == kLayers - 1 ? kOut : kWidth; }
-__host__ __device__ constexpr int weightOffset(int l) { return l == 0 ? 0 : kIn * kWidth + (l - 1) * kWidth * kWidth; }
-constexpr int kMlpParams = kIn * kWidth + 3 * kWidth * kWidth + kWidth * kOut; // 21504
-
-// Forward fragments of layer l: (in/16) k-tiles x (out/8) n-tiles; backward
-// fragments: (out/16) k-tiles x (in/8) n-tiles, only the 32 hash-grid columns
-// of layer 0 (the one-blob inputs get no gradient).
-__host__ __device__ constexpr int fwdKT(int l) { return layerIn(l) / 16; }
-__host__ __device__ constexpr int fwdNT(int l) { return layerOut(l) / 8; }
-__host__ __device__ constexpr int bwdKT(int l) { return layerOut(l) / 16; }
-__host__ __device__ constexpr int bwdNT(int l) { return l == 0 ? kHashF / 8 : layerIn(l) / 8; }
-__host__ __device__ constexpr int fwdFragOffset(int l) { return l == 0 ? 0 : fwdFragOffset(l - 1) + fwdKT(l - 1) * fwdNT(l - 1); }
-__host__ __device__ constexpr int bwdFragOffset(int l) { return l == 0 ? 0 : bwdFragOffset(l - 1) + bwdKT(l - 1) * bwdNT(l - 1); }
-constexpr int kFwdFrags = fwdFragOffset(kLayers); // 168
-constexpr int kBwdFrags = bwdFragOffset(kLayers); // 136
-constexpr int kFwdFragBytes = kFwdFrags * 32 * 8;
-constexpr int kBwdFragBytes = kBwdFrags * 32 * 8;
-
-// Training staging rows: inputs of every layer [96 | 64 | 64 | 64 | 64] and
-// output gradients of every layer [64 | 64 | 64 | 64 | 48], bf16.
-constexpr int kActRow   = kIn + 4 * kWidth;  // 352
-constexpr int kDeltaRow = 4 * kWidth + kOut; // 304
-__host__ __device__ constexpr int actOffset(int l) { return l == 0 ? 0 : kIn + (l - 1) * kWidth; }
-__host__ __device__ constexpr int deltaOffset(int l) { return l * kWidth; }
+// Network shape: 96 encoded inputs -> 64 (layer 0) -> NH hidden layers of
+// 64 -> NO outputs (a multiple of 16), ReLU between layers, no biases.  W_l
+// is [out][in] row-major in the flat parameter block.
+//   forward fragments of layer l: (in/16) k-tiles x (out/8) n-tiles;
+//   backward fragments: (out/16) k-tiles x (in/8) n-tiles, only the 32
+//   hash-grid columns at layer 0 (the one-blob inputs get no gradient).
+// Training staging rows: the input of every layer [96 | 64 ...] and the
+// output gradient of every layer [64 ... | NO], bf16.
+template <int NH, int NO> struct MlpShape
+{
+    static_assert(NO % 16 == 0 && NH >= 1, "outputs: a multiple of 16; at least one hidden layer");
+    static constexpr int kHidden = NH, kLayers = NH + 2, kOut = NO;
+    __host__ __device__ static constexpr int in(int l) { return l == 0 ? kIn : kWidth; }
+    __host__ __device__ static constexpr int out(int l) { return l == NH + 1 ? NO : kWidth; }
+    __host__ __device__ static constexpr int woff(int l) { return l == 0 ? 0 : kIn * kWidth + (l - 1) * kWidth * kWidth; }
+    static constexpr int kParams = kIn * kWidth + NH * kWidth * kWidth + kWidth * NO;
+    __host__ __device__ static constexpr int fwdNT(int l) { return out(l) / 8; }
+    __host__ __device__ static constexpr int bwdNT(int l) { return l == 0 ? kHashF / 8 : in(l) / 8; }
+    __host__ __device__ static constexpr int fwdOff(int l) { return l == 0 ? 0 : 48 + (l - 1) * 32; }
+    __host__ __device__ static constexpr int bwdOff(int l) { return l == 0 ? 0 : 16 + (l - 1) * 32; }
+    static constexpr int kFwdFrags = 48 + NH * 32 + 4 * (NO / 8);
+    static constexpr int kBwdFrags = 16 + NH * 32 + (NO / 16) * 8;
+    static constexpr int kFwdBytes = kFwdFrags * 32 * 8;
+    static constexpr int kBwdBytes = kBwdFrags * 32 * 8;
+    static constexpr int kActRow   = kIn + (NH + 1) * kWidth;
+    static constexpr int kDeltaRow = (NH + 1) * kWidth + NO;
+    __host__ __device__ static constexpr int actOff(int l) { return l == 0 ? 0 : kIn + (l - 1) * kWidth; }
+    __host__ __device__ static constexpr int deltaOff(int l) { return l * kWidth; }
+    static constexpr int kOS = NO + 1; // output tile row stride (f32)
+    static constexpr int kDS = NO + 8; // output-gradient tile row stride (bf16), conflict-free ldmatrix rows
+};
+// The guiding network (4 hidden layers, 48 outputs: 8 vMF lobes + selection)
+// and the radiance cache (2 hidden layers, RGB in the first 3 of 16 outputs).
+using GuideShape = MlpShape<3, 48>;
+using CacheShape = MlpShape<1, 16>;
+constexpr int kOut          = GuideShape::kOut;
+constexpr int kOS           = GuideShape::kOS;
+constexpr int kMlpParams    = GuideShape::kParams;   // 21504
+constexpr int kFwdFragBytes = GuideShape::kFwdBytes;
 
 // Hash grid: table[l * T + index] holds the 2 features of an entry.
 struct GridView
@@ -252,121 +262,104 @@ __device__ __forceinline__ void hiddenLayer(const uint2* __restrict__ wf, const 
         for (int j = 0; j < 4; ++j) accToA(acc[m][2 * j], acc[m][2 * j + 1], out[m][j]);
 }
 
-// Forward pass of MT 16-row tiles.  `x`: the warp's encoded-input tile
-// (MT*16 rows, stride kXS); `wf`: forward fragments (shared memory).
-// h[m][l]: A fragments of the input of layer l+1 (l = 0..3), kept for the
-// backward pass; out: head outputs (6 n-tiles of accumulators).
+// Layer 0: the encoded-input tile (MT*16 rows, stride kXS, shared memory)
+// -> ReLU activations as A fragments.
 template <int MT>
+__device__ __forceinline__ void inputLayer(const uint2* __restrict__ wf, const __nv_bfloat16* x, uint32_t lane,
+                                           uint32_t (&h)[MT][4][4])
+{
+    float acc[MT][8][4];
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int n = 0; n < 8; ++n) acc[m][n][0] = acc[m][n][1] = acc[m][n][2] = acc[m][n][3] = 0.0f;
+#pragma unroll
+    for (int kt = 0; kt < 6; ++kt)
+    {
+        uint32_t a[MT][4];
+#pragma unroll
+        for (int m = 0; m < MT; ++m) loadA(a[m], x + m * 16 * kXS, kXS, kt, lane);
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+        {
+            uint2 b = wf[(kt * 8 + nt) * 32 + lane];
+#pragma unroll
+            for (int m = 0; m < MT; ++m) mma16816(acc[m][nt], a[m], b.x, b.y);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) accToA(acc[m][2 * j], acc[m][2 * j + 1], h[m][j]);
+}
+
+// Last layer: 64 inputs (A fragments) -> NO/8 n-tiles of FP32 outputs.
+template <class S, int MT>
+__device__ __forceinline__ void outputLayer(const uint2* __restrict__ wl, const uint32_t (&in)[MT][4][4],
+                                            float (&out)[MT][S::kOut / 8][4], uint32_t lane)
+{
+    constexpr int NT = S::kOut / 8;
+#pragma unroll
+    for (int m = 0; m < MT; ++m)
+#pragma unroll
+        for (int n = 0; n < NT; ++n) out[m][n][0] = out[m][n][1] = out[m][n][2] = out[m][n][3] = 0.0f;
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt)
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+        {
+            uint2 b = wl[(kt * NT + nt) * 32 + lane];
+#pragma unroll
+            for (int m = 0; m < MT; ++m) mma16816(out[m][nt], in[m][kt], b.x, b.y);
+        }
+}
+
+// Forward pass of MT 16-row tiles.  `x`: the warp's encoded-input tile;
+// `wf`: forward fragments (shared memory).  h[l]: A fragments of the input
+// of layer l+1, kept for the backward pass; out: the outputs' accumulators.
+template <class S, int MT>
 __device__ __forceinline__ void mlpForward(const uint2* __restrict__ wf, const __nv_bfloat16* x, uint32_t lane,
-                                           uint32_t (&h)[4][MT][4][4], float (&out)[MT][6][4])
+                                           uint32_t (&h)[S::kHidden + 1][MT][4][4], float (&out)[MT][S::kOut / 8][4])
 {
-    {
-        float acc[MT][8][4];
+    inputLayer<MT>(wf, x, lane, h[0]);
 #pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int n = 0; n < 8; ++n) acc[m][n][0] = acc[m][n][1] = acc[m][n][2] = acc[m][n][3] = 0.0f;
-#pragma unroll
-        for (int kt = 0; kt < 6; ++kt)
-        {
-            uint32_t a[MT][4];
-#pragma unroll
-            for (int m = 0; m < MT; ++m) loadA(a[m], x + m * 16 * kXS, kXS, kt, lane);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt)
-            {
-                uint2 b = wf[(kt * 8 + nt) * 32 + lane];
-#pragma unroll
-                for (int m = 0; m < MT; ++m) mma16816(acc[m][nt], a[m], b.x, b.y);
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) accToA(acc[m][2 * j], acc[m][2 * j + 1], h[0][m][j]);
-    }
-    hiddenLayer<MT>(wf + fwdFragOffset(1) * 32, h[0], h[1], lane);
-    hiddenLayer<MT>(wf + fwdFragOffset(2) * 32, h[1], h[2], lane);
-    hiddenLayer<MT>(wf + fwdFragOffset(3) * 32, h[2], h[3], lane);
-    const uint2* w4 = wf + fwdFragOffset(4) * 32;
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int n = 0; n < 6; ++n) out[m][n][0] = out[m][n][1] = out[m][n][2] = out[m][n][3] = 0.0f;
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt)
-#pragma unroll
-        for (int nt = 0; nt < 6; ++nt)
-        {
-            uint2 b = w4[(kt * 6 + nt) * 32 + lane];
-#pragma unroll
-            for (int m = 0; m < MT; ++m) mma16816(out[m][nt], h[3][m][kt], b.x, b.y);
-        }
+    for (int l = 1; l <= S::kHidden; ++l) hiddenLayer<MT>(wf + S::fwdOff(l) * 32, h[l - 1], h[l], lane);
+    outputLayer<S, MT>(wf + S::fwdOff(S::kHidden + 1) * 32, h[S::kHidden], out, lane);
 }
 
-// Inference-only forward (no activations kept): the same arithmetic, fewer
-// live registers.
-template <int MT>
+// Inference-only forward (activations ping-pong between two register sets).
+template <class S, int MT>
 __device__ __forceinline__ void mlpInfer(const uint2* __restrict__ wf, const __nv_bfloat16* x, uint32_t lane,
-                                         float (&out)[MT][6][4])
+                                         float (&out)[MT][S::kOut / 8][4])
 {
-    uint32_t h0[MT][4][4], h1[MT][4][4];
+    uint32_t ha[MT][4][4], hb[MT][4][4];
+    inputLayer<MT>(wf, x, lane, ha);
+#pragma unroll
+    for (int l = 1; l <= S::kHidden; ++l)
     {
-        float acc[MT][8][4];
-#pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int n = 0; n < 8; ++n) acc[m][n][0] = acc[m][n][1] = acc[m][n][2] = acc[m][n][3] = 0.0f;
-#pragma unroll
-        for (int kt = 0; kt < 6; ++kt)
-        {
-            uint32_t a[MT][4];
-#pragma unroll
-            for (int m = 0; m < MT; ++m) loadA(a[m], x + m * 16 * kXS, kXS, kt, lane);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt)
-            {
-                uint2 b = wf[(kt * 8 + nt) * 32 + lane];
-#pragma unroll
-                for (int m = 0; m < MT; ++m) mma16816(acc[m][nt], a[m], b.x, b.y);
-            }
-        }
-#pragma unroll
-        for (int m = 0; m < MT; ++m)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) accToA(acc[m][2 * j], acc[m][2 * j + 1], h0[m][j]);
+        if (l & 1)
+            hiddenLayer<MT>(wf + S::fwdOff(l) * 32, ha, hb, lane);
+        else
+            hiddenLayer<MT>(wf + S::fwdOff(l) * 32, hb, ha, lane);
     }
-    hiddenLayer<MT>(wf + fwdFragOffset(1) * 32, h0, h1, lane);
-    hiddenLayer<MT>(wf + fwdFragOffset(2) * 32, h1, h0, lane);
-    hiddenLayer<MT>(wf + fwdFragOffset(3) * 32, h0, h1, lane);
-    const uint2* w4 = wf + fwdFragOffset(4) * 32;
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int n = 0; n < 6; ++n) out[m][n][0] = out[m][n][1] = out[m][n][2] = out[m][n][3] = 0.0f;
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt)
-#pragma unroll
-        for (int nt = 0; nt < 6; ++nt)
-        {
-            uint2 b = w4[(kt * 6 + nt) * 32 + lane];
-#pragma unroll
-            for (int m = 0; m < MT; ++m) mma16816(out[m][nt], h1[m][kt], b.x, b.y);
-        }
+    if (S::kHidden & 1)
+        outputLayer<S, MT>(wf + S::fwdOff(S::kHidden + 1) * 32, hb, out, lane);
+    else
+        outputLayer<S, MT>(wf + S::fwdOff(S::kHidden + 1) * 32, ha, out, lane);
 }
 
-// Accumulator tiles (6 n-tiles) -> rows of a float tile (stride kOS).
-template <int MT>
-__device__ __forceinline__ void storeOut(const float (&out)[MT][6][4], float* tile, uint32_t lane)
+// Output accumulators -> rows of a float tile (stride S::kOS).
+template <class S, int MT>
+__device__ __forceinline__ void storeOut(const float (&out)[MT][S::kOut / 8][4], float* tile, uint32_t lane)
 {
     const uint32_t g = lane >> 2, t = lane & 3u;
 #pragma unroll
     for (int m = 0; m < MT; ++m)
 #pragma unroll
-        for (int n = 0; n < 6; ++n)
+        for (int n = 0; n < S::kOut / 8; ++n)
         {
-            float* r0 = tile + (m * 16 + g) * kOS + n * 8 + 2 * t;
-            float* r1 = r0 + 8 * kOS;
+            float* r0 = tile + (m * 16 + g) * S::kOS + n * 8 + 2 * t;
+            float* r1 = r0 + 8 * S::kOS;
             r0[0]     = out[m][n][0];
             r0[1]     = out[m][n][1];
             r1[0]     = out[m][n][2];

@@ -1,33 +1,44 @@
-// Guiding network, host side: parameters, Adam state, training staging and
-// the kernels' launch sequence (no counterpart in the reference renderer).
+// Hash-grid + tensor-core MLP networks, host side: parameters, Adam state,
+// training staging and the kernels' launch sequence.  Two instances: the
+// guiding network and the radiance cache (no counterpart in the reference
+// renderer).
 #pragma once
 
 #include "cl_guide.cuh"
 #include "cl_internal.h"
 
+#include <type_traits>
+
 namespace clb
 {
 // One training record in device memory (4 float4):
-// {p.xyz in [0,1]^3, w} {n.xyz, -} {wo.xyz, -} {omega.xyz, BSDF pdf of omega}.
+// {p.xyz in [0,1]^3, w} {n.xyz, -} {wo.xyz, -} {y.xyz, yw}, where y, yw are
+// the guide's sampled direction and its BSDF pdf, or the cache's target RGB.
 constexpr int kRecordF4 = 4;
 
-class GuideNet
+struct GuideLoss; // -log p of the vMF mixture (or of the one-sample MIS density)
+struct CacheLoss; // relative L2 of the predicted radiance
+
+template <class S, class L> class HashNet
 {
 public:
-    explicit GuideNet(const cl_guide_config& c);
-    ~GuideNet();
+    // Host record floats: guide {in9, omega, w, BSDF pdf}, cache {in9, RGB}.
+    static constexpr int kRecFloats = std::is_same<S, guide::GuideShape>::value ? 14 : 12;
+
+    explicit HashNet(const cl_guide_config& c);
+    ~HashNet();
     cl_status init(cudaStream_t st, std::string* err);
 
-    uint64_t paramCount() const { return hashParams_ + uint64_t(guide::kMlpParams); }
+    uint64_t paramCount() const { return hashParams_ + uint64_t(S::kParams); }
     uint64_t hashParams() const { return hashParams_; }
     const cl_guide_config& config() const { return cfg_; }
     const uint32_t* resolutions() const { return res_; }
 
     cl_status setParams(const float* p, uint64_t n, std::string* err);
     cl_status getParams(float* p, uint64_t n, std::string* err);
-    cl_status forward(const float* in9, uint32_t n, float* out48, std::string* err);
-    cl_status gradient(const float* rec14, uint32_t n, double* loss, float* grad, std::string* err);
-    cl_status trainStepHost(const float* rec14, uint32_t n, double* loss, std::string* err);
+    cl_status forward(const float* in9, uint32_t n, float* out, std::string* err);
+    cl_status gradient(const float* rec, uint32_t n, double* loss, float* grad, std::string* err);
+    cl_status trainStepHost(const float* rec, uint32_t n, double* loss, std::string* err);
     cl_status sample(const float* in9, const float* u3, uint32_t n, float* dir, float* pdf, std::string* err);
     cl_status pdf(const float* in9, const float* dir, uint32_t n, float* pdf, std::string* err);
 
@@ -39,10 +50,9 @@ public:
     const uint2*    fwdFrags() const { return wf_.as<uint2>(); }
     const double*   lossDev() const { return scal_.as<double>() + 1; }
     uint64_t        steps() const { return step_; }
-    void            setStream(cudaStream_t st) { st_ = st; }
 
 private:
-    cl_status upload(const float* rec14, uint32_t n, std::string* err);
+    cl_status upload(const float* rec, uint32_t n, std::string* err);
     cl_status computeGradient(const float4* rec, const uint32_t* count, std::string* err);
     cl_status refreshCopies(std::string* err);
 
@@ -59,9 +69,12 @@ private:
     DevBuf table_;                 // bf16 copy of the hash table
     DevBuf wf_, wb_;               // bf16 weight fragments (forward, backward)
     DevBuf acts_, deltas_;         // training staging, batch rows
-    DevBuf scal_;                  // {sum w, loss, count (u32)}
+    DevBuf scal_;                  // {sum w, loss, count (u32), sum of clamped w}
     DevBuf rec_, io_, io2_;        // host-entry staging
 };
+
+using GuideNet = HashNet<guide::GuideShape, GuideLoss>;
+using CacheNet = HashNet<guide::CacheShape, CacheLoss>;
 
 void guideDefaultConfig(cl_guide_config* c);
 cl_status guideResolutions(float nmin, float nmax, uint32_t* res);

@@ -152,7 +152,10 @@ __device__ __forceinline__ void startPath(const Params& P, const WaveParams& wp,
     d          = normalize(d);
     P.q.psInfo[slot]   = make_uint4(pix, frame, 1u | (rng.ctr << 8), 0u);
     P.q.psT[slot]      = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    P.q.psE[slot]      = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // Radiance cache: one path in trainMask + 1 (Fibonacci hash of the path
+    // index) is a training path.
+    const bool train = wp.cacheTrain && ((uint32_t((p * 0x9E3779B97F4A7C15ull) >> 40) & P.c.trainMask) == 0u);
+    P.q.psE[slot]      = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(train ? kCacheTrainBit : 0u));
     P.q.psL[slot]      = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     P.q.rqO[q][idx]    = make_float4(pos.x, pos.y, pos.z, 0.0f);
     P.q.rqD[q][idx]    = make_float4(d.x, d.y, d.z, FLT_MAX);
@@ -189,6 +192,35 @@ __device__ __noinline__ void flushRecords(GuideDev g, const uint4* psInfo, Count
     }
 }
 
+// Radiance cache: training records of a finished training path.  Recorded
+// vertex k holds the throughput T_k that reached it and the path radiance
+// L_k before its emitter sample; (L - L_k) / T_k is the radiance the path
+// gathered from k on, an estimate of the outgoing radiance at k.
+__device__ __noinline__ void flushCacheRecords(CacheDev c, const float4* psE, Counters* ctr, uint32_t slot, float lx,
+                                               float ly, float lz)
+{
+    uint32_t      mask = __float_as_uint(psE[slot].w) & ~kCacheTrainBit;
+    const float4* h    = c.hist + size_t(slot) * c.histDepth * kCacheHistF4;
+    while (mask)
+    {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1u;
+        const float4* e  = h + k * kCacheHistF4;
+        float4        e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3];
+        if (!(e0.w > 0.0f) || !(e1.w > 0.0f) || !(e2.w > 0.0f)) continue;
+        float ty = fmaxf((lx - e3.x) / e0.w, 0.0f), tg = fmaxf((ly - e3.y) / e1.w, 0.0f),
+              tb = fmaxf((lz - e3.z) / e2.w, 0.0f);
+        if (!(ty < FLT_MAX) || !(tg < FLT_MAX) || !(tb < FLT_MAX)) continue;
+        uint32_t idx = atomicAdd(&ctr->cacheRec, 1u);
+        if (idx >= c.recCap) continue;
+        float4* r = c.rec + size_t(idx) * kRecordF4;
+        r[0]      = make_float4(e0.x, e0.y, e0.z, 1.0f);
+        r[1]      = make_float4(e1.x, e1.y, e1.z, 0.0f);
+        r[2]      = make_float4(e2.x, e2.y, e2.z, 0.0f);
+        r[3]      = make_float4(ty, tg, tb, 0.0f);
+    }
+}
+
 // Film write of finished paths, then regeneration of their slots.  Called by
 // every lane of the warp.
 __device__ __forceinline__ void finishPaths(const Params& P, const WaveParams& wp, int nxt, bool finish, uint32_t slot,
@@ -196,6 +228,8 @@ __device__ __forceinline__ void finishPaths(const Params& P, const WaveParams& w
 {
     if (finish && wp.recStride && slot % wp.recStride == 0u)
         flushRecords(P.g, P.q.psInfo, P.q.ctr, slot, wp.recStride, L.x, L.y, L.z);
+    if (finish && wp.cacheTrain && (__float_as_uint(P.q.psE[slot].w) & ~kCacheTrainBit))
+        flushCacheRecords(P.c, P.q.psE, P.q.ctr, slot, L.x, L.y, L.z);
     if (finish)
     {
         uint32_t pix = P.q.psInfo[slot].x;
@@ -388,7 +422,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
         bool     valid = i < n;
         if (MAT >= 0 && valid) i = P.q.classIdx[size_t(MAT) * P.q.slots + i];
         bool     pushShadow = false, shadow1 = false, shadow2 = false, pushRay = false, finish = false;
-        uint32_t slot = 0u, info2 = 0u, recBit = 0u, vDepth = 0u;
+        uint32_t slot = 0u, info2 = 0u, recBit = 0u, vDepth = 0u, cst = 0u;
         f3       tIn{0, 0, 0};
         f3       L{0, 0, 0}, T{1, 1, 1}, E{0, 0, 0}, pHit{0, 0, 0}, sdir{0, 0, 0}, Li{0, 0, 0}, sdir2{0, 0, 0},
             Ld{0, 0, 0}, ndir{0, 0, 0};
@@ -402,7 +436,9 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             vDepth         = depth;
             Rng    rng{info.x % wp.W, info.x / wp.W, info.y, info.z >> 8};
             T             = ld3(P.q.psT[slot]);
-            E             = ld3(P.q.psE[slot]);
+            float4 e4     = P.q.psE[slot];
+            E             = ld3(e4);
+            cst           = __float_as_uint(e4.w);
             L             = ld3(P.q.psL[slot]);
             f3       d    = ld3(rd);
             uint32_t prim = __float_as_uint(hh.y);
@@ -425,12 +461,31 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 }
                 finish = true;
             }
+            else if (!DL && P.c.termDepth && depth == P.c.termDepth && !(cst & kCacheTrainBit))
+            {
+                // The path ends in the radiance cache (kMlpPass's prediction).
+                float4 cl = P.c.L[i];
+                L         = L + T * f3{cl.x, cl.y, cl.z};
+                finish    = true;
+            }
             else if (!DL && depth == wp.maxDepth)
                 finish = true;
             else
             {
                 HitAttr a    = hitAttributes(sc, prim, hh.z, hh.w);
                 Bsdf    bsdf = loadMaterial(sc.mats, a.material);
+                if (!DL && (cst & kCacheTrainBit) && wp.cacheTrain && depth <= P.c.histDepth)
+                {
+                    // Radiance-cache training path: vertex history (flushCacheRecords).
+                    float4* h = P.c.hist + (size_t(slot) * P.c.histDepth + depth - 1u) * kCacheHistF4;
+                    f3 pn = (a.p - f3{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]}) * P.g.boxScale;
+                    h[0]  = make_float4(pn.x, pn.y, pn.z, T.x);
+                    h[1]  = make_float4(a.ns.x, a.ns.y, a.ns.z, T.y);
+                    h[2]  = make_float4(-d.x, -d.y, -d.z, T.z);
+                    h[3]  = make_float4(L.x, L.y, L.z, 0.0f);
+                    cst |= 1u << (depth - 1u);
+                    reinterpret_cast<uint32_t*>(P.q.psE + slot)[3] = cst;
+                }
                 if (MAT >= 0) bsdf.type = uint32_t(MAT);
                 pHit         = a.p;
                 f3    wo     = -d;
@@ -629,7 +684,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             P.q.psInfo[slot].z    = info2;
             if (GUIDE && recBit) P.q.psInfo[slot].w |= recBit;
             P.q.psT[slot]         = make_float4(T.x, T.y, T.z, 0.0f);
-            P.q.psE[slot]         = make_float4(E.x, E.y, E.z, 0.0f);
+            P.q.psE[slot]         = make_float4(E.x, E.y, E.z, __uint_as_float(cst));
         }
         if (pushRay || (pushShadow && finish)) P.q.psL[slot] = make_float4(L.x, L.y, L.z, 0.0f);
         finishPaths(P, wp, nxt, finish && !pushShadow, slot, L);
@@ -692,7 +747,7 @@ __global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
 // keeps its weights in shared memory and reads its rows sequentially.
 constexpr uint32_t kNoRay          = 0xffffffffu;
 constexpr int      kGuideMlpWarps  = 8;
-constexpr int      kGuideMlpSmem   = guide::kFwdFragBytes + kGuideMlpWarps * 32 * guide::kXS * 2;
+constexpr int      kGuideMlpSmem   = guide::GuideShape::kFwdBytes + kGuideMlpWarps * 32 * guide::kXS * 2;
 constexpr int      kGuideEncBlock  = 128;
 
 __device__ __forceinline__ uint32_t guidedCounts(const Params& P, uint32_t* n0, uint32_t* n1)
@@ -718,7 +773,10 @@ __global__ void __launch_bounds__(kGuideEncBlock, 6) kGuideEncode(Params P, guid
         uint4*         dst = P.g.enc + size_t(k) * (guide::kIn / 8);
         uint32_t       r[guide::kIn / 2];
         uint32_t       ray = i;
-        if ((P.q.psInfo[P.q.rqSlot[cur][i]].z & 0xffu) == maxDepth)
+        const uint32_t slot  = P.q.rqSlot[cur][i];
+        const uint32_t depth = P.q.psInfo[slot].z & 0xffu;
+        if (depth == maxDepth ||
+            (P.c.termDepth && depth == P.c.termDepth && !(__float_as_uint(P.q.psE[slot].w) & kCacheTrainBit)))
         {
             ray = kNoRay;
 #pragma unroll
@@ -745,25 +803,83 @@ __global__ void __launch_bounds__(kGuideEncBlock, 6) kGuideEncode(Params P, guid
     }
 }
 
-__global__ void __launch_bounds__(kGuideMlpWarps * 32, 2) kGuideMlp(Params P, const uint2* __restrict__ wfG,
-                                                                        float alpha)
+// Radiance cache, first pass: the rays of the surface classes that end
+// their path here (depth == termDepth, not a training path) are compacted
+// (warp-aggregated append) and encoded like kGuideEncode's.
+__global__ void __launch_bounds__(kGuideEncBlock, 6) kCacheEncode(Params P, guide::GridView g, int cur)
+{
+    const uint32_t n0 = loadCount(&P.q.ctr->classCount[0]), n1 = loadCount(&P.q.ctr->classCount[1]);
+    const uint32_t n  = n0 + n1 + loadCount(&P.q.ctr->classCount[2]);
+    const f3       bmin{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]};
+    const uint32_t lane = laneId();
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x)
+    {
+        const uint32_t k    = base + lane;
+        bool           term = false;
+        uint32_t       i = 0u, slot = 0u;
+        if (k < n)
+        {
+            const uint32_t c   = k < n0 ? 0u : (k < n0 + n1 ? 1u : 2u);
+            const uint32_t pos = k - (c == 0u ? 0u : (c == 1u ? n0 : n0 + n1));
+            i                  = P.q.classIdx[size_t(c) * P.q.slots + pos];
+            slot               = P.q.rqSlot[cur][i];
+            term = (P.q.psInfo[slot].z & 0xffu) == P.c.termDepth && !(__float_as_uint(P.q.psE[slot].w) & kCacheTrainBit);
+        }
+        const uint32_t idx = warpAppend(&P.q.ctr->cacheCount, term);
+        if (!term) continue;
+        float4   hh = P.q.hit[i];
+        float4   rd = P.q.rqD[cur][i];
+        HitAttr  a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
+        f3       pn = guide::clampUnit((a.p - bmin) * P.g.boxScale);
+        uint32_t r[guide::kIn / 2];
+#pragma unroll
+        for (int l = 0; l < guide::kLevels; ++l)
+        {
+            float2 f = guide::encodeLevel(g, l, pn);
+            r[l]     = guide::packBf16(f.x, f.y);
+        }
+        guide::oneBlobPacked(a.ns, r + guide::kHashF / 2);
+        guide::oneBlobPacked(f3{-rd.x, -rd.y, -rd.z}, r + (guide::kHashF + 2 * guide::kBlob) / 2);
+        uint4* dst = P.c.enc + size_t(idx) * (guide::kIn / 8);
+#pragma unroll
+        for (int q = 0; q < guide::kIn / 8; ++q) dst[q] = make_uint4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+        P.c.encIdx[idx] = i;
+    }
+}
+
+// Second pass of both networks: persistent warps stream 32 encoded rows at a
+// time through the MLP on the tensor cores.  Guide (S = GuideShape): the
+// head's lobes per ray, their weights summing to the probability of sampling
+// the guide (alpha; < 0: learned).  Cache (S = CacheShape): the predicted
+// radiance per ray, clamped to be non-negative.
+template <class S, bool CACHE>
+__global__ void __launch_bounds__(kGuideMlpWarps * 32, 2) kMlpPass(Params P, const uint2* __restrict__ wfG,
+                                                                   float alpha)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2*         wf   = reinterpret_cast<uint2*>(smem);
     const uint32_t lane = laneId(), warp = threadIdx.x >> 5;
-    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + guide::kFwdFragBytes + warp * 32 * guide::kXS * 2);
+    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + S::kFwdBytes + warp * 32 * guide::kXS * 2);
     {
         const uint4* src = reinterpret_cast<const uint4*>(wfG);
         uint4*       dst = reinterpret_cast<uint4*>(wf);
-        for (int k = threadIdx.x; k < guide::kFwdFrags * 16; k += blockDim.x) dst[k] = __ldg(src + k);
+        for (int k = threadIdx.x; k < S::kFwdFrags * 16; k += blockDim.x) dst[k] = __ldg(src + k);
     }
     __syncthreads();
-    uint32_t       n0, n1;
-    const uint32_t n = guidedCounts(P, &n0, &n1);
+    uint32_t n;
+    if (CACHE)
+        n = loadCount(&P.q.ctr->cacheCount);
+    else
+    {
+        uint32_t n0, n1;
+        n = guidedCounts(P, &n0, &n1);
+    }
+    const uint4*    enc    = CACHE ? P.c.enc : P.g.enc;
+    const uint32_t* encIdx = CACHE ? P.c.encIdx : P.g.encIdx;
     for (uint32_t tile = blockIdx.x * kGuideMlpWarps + warp; tile * 32u < n; tile += gridDim.x * kGuideMlpWarps)
     {
-        const uint32_t k0 = tile * 32u;
-        const uint4*   src = P.g.enc + size_t(k0) * (guide::kIn / 8);
+        const uint32_t k0  = tile * 32u;
+        const uint4*   src = enc + size_t(k0) * (guide::kIn / 8);
 #pragma unroll
         for (int q = 0; q < guide::kIn / 8; ++q)
         {
@@ -772,35 +888,47 @@ __global__ void __launch_bounds__(kGuideMlpWarps * 32, 2) kGuideMlp(Params P, co
             if (k0 + rr < n) v = src[j];
             *reinterpret_cast<uint4*>(x + rr * guide::kXS + cc * 8) = v;
         }
-        const uint32_t ray = k0 + lane < n ? P.g.encIdx[k0 + lane] : kNoRay;
+        const uint32_t ray = k0 + lane < n ? encIdx[k0 + lane] : kNoRay;
         const uint32_t vm  = __ballot_sync(kFull, ray != kNoRay);
-        if (lane == 0u && vm) atomicAdd(&P.q.ctr->inferred, (unsigned long long)__popc(vm));
+        if (lane == 0u && vm)
+            atomicAdd(CACHE ? &P.q.ctr->cacheQueries : &P.q.ctr->inferred, (unsigned long long)__popc(vm));
         __syncwarp();
-        float out[2][6][4];
-        guide::mlpInfer<2>(wf, x, lane, out);
+        float out[2][S::kOut / 8][4];
+        guide::mlpInfer<S, 2>(wf, x, lane, out);
         __syncwarp();
         float* o = reinterpret_cast<float*>(x);
-        guide::storeOut<2>(out, o, lane);
+        guide::storeOut<S, 2>(out, o, lane);
         __syncwarp();
         if (ray != kNoRay)
         {
-            guide::Lobes L;
-            guide::headLobes(o + lane * guide::kOS, &L, alpha);
-            float4* dst = P.g.lobes + size_t(ray) * kLobeF4;
+            const float* row = o + lane * S::kOS;
+            if (CACHE)
+                P.c.L[ray] = make_float4(fmaxf(row[0], 0.0f), fmaxf(row[1], 0.0f), fmaxf(row[2], 0.0f), 0.0f);
+            else
+            {
+                guide::Lobes L;
+                guide::headLobes(row, &L, alpha);
+                float4* dst = P.g.lobes + size_t(ray) * kLobeF4;
 #pragma unroll
-            for (int j = 0; j < guide::kLobes; ++j) dst[j] = L.l[j];
-            dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
-            dst[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
+                for (int j = 0; j < guide::kLobes; ++j) dst[j] = L.l[j];
+                dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
+                dst[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
+            }
         }
         __syncwarp();
     }
 }
+constexpr int kCacheMlpSmem = guide::CacheShape::kFwdBytes + kGuideMlpWarps * 32 * guide::kXS * 2;
 
 // Records beyond the capacity were dropped; the training step reads the
 // clamped count.
 __global__ void kClampRecords(Counters* c, uint32_t cap)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) c->trainCount = min(c->recCount, cap);
+}
+__global__ void kClampCacheRecords(Counters* c, uint32_t cap)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) c->cacheTrainCount = min(c->cacheRec, cap);
 }
 
 // Initial fill: slot s starts path s.
@@ -824,6 +952,7 @@ __global__ void kAdvance(Counters* c, int cur)
     c->fetchShadow   = 0u;
     c->fetchResolve  = 0u;
     c->fetchInfer    = 0u;
+    c->cacheCount    = 0u;
     for (int k = 0; k < 4; ++k)
     {
         c->classCount[k] = 0u;
@@ -965,8 +1094,21 @@ cl_status Integrator::init(std::string* err)
                 &b, dl ? (const void*)kShadowResolve<true> : (const void*)kShadowResolve<false>, 128, 0),
             err);
     shadowBlocks_ = std::max(1, b) * numSMs_;
-    CL_CUDA(cudaFuncSetAttribute(kGuideMlp, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideMlpSmem), err);
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideMlp, kGuideMlpWarps * 32, kGuideMlpSmem), err);
+    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::GuideShape, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kGuideMlpSmem),
+            err);
+    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::CacheShape, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kCacheMlpSmem),
+            err);
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kMlpPass<guide::CacheShape, true>, kGuideMlpWarps * 32,
+                                                          kCacheMlpSmem),
+            err);
+    cacheMlpBlocks_ = std::max(1, b) * numSMs_;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kCacheEncode, kGuideEncBlock, 0), err);
+    cacheEncodeBlocks_ = std::max(1, b) * numSMs_;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kMlpPass<guide::GuideShape, false>, kGuideMlpWarps * 32,
+                                                          kGuideMlpSmem),
+            err);
     inferBlocks_ = std::max(1, b) * numSMs_;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideEncode, kGuideEncBlock, 0), err);
     encodeBlocks_ = std::max(1, b) * numSMs_;
@@ -1368,9 +1510,21 @@ Params Integrator::params() const
         P.g.recCap    = recCap_;
         P.g.classMask = guideCfg_.class_mask;
         P.g.bsdfFrac  = guideCfg_.bsdf_fraction;
-        P.g.boxScale  = boxScale_;
-        for (int q = 0; q < 3; ++q) P.g.boxMin[q] = boxMin_[q];
         P.g.histDepth = histDepth_;
+    }
+    for (int q = 0; q < 3; ++q) P.g.boxMin[q] = boxMin_[q];
+    P.g.boxScale = boxScale_;
+    if (cache_)
+    {
+        P.c.L         = cacheL_.as<float4>();
+        P.c.enc       = cacheEnc_.as<uint4>();
+        P.c.encIdx    = cacheEncIdx_.u();
+        P.c.hist      = cacheHist_.as<float4>();
+        P.c.rec       = cacheRec_.as<float4>();
+        P.c.recCap    = cacheRecCap_;
+        P.c.termDepth = cacheCfg_.prefix_bounces + 1u;
+        P.c.trainMask = (1u << cacheCfg_.train_log2_fraction) - 1u;
+        P.c.histDepth = cacheHistDepth_;
     }
     return P;
 }
@@ -1393,8 +1547,14 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     if (gmask)
     {
         kGuideEncode<<<encodeBlocks_, kGuideEncBlock, 0, stream_>>>(P, guide_->grid(), cur);
-        kGuideMlp<<<inferBlocks_, kGuideMlpWarps * 32, kGuideMlpSmem, stream_>>>(
+        kMlpPass<guide::GuideShape, false><<<inferBlocks_, kGuideMlpWarps * 32, kGuideMlpSmem, stream_>>>(
             P, guide_->fwdFrags(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
+    }
+    if (cache_)
+    {
+        kCacheEncode<<<cacheEncodeBlocks_, kGuideEncBlock, 0, stream_>>>(P, cache_->grid(), cur);
+        kMlpPass<guide::CacheShape, true><<<cacheMlpBlocks_, kGuideMlpWarps * 32, kCacheMlpSmem, stream_>>>(
+            P, cache_->fwdFrags(), 1.0f);
     }
     if (profile) CL_CUDA(cudaEventRecord(evS_[4], stream_), err);
     for (int m = 0; m < 4; ++m)
@@ -1457,40 +1617,73 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     msRender_ = msTrace_ = msShade_ = msShadow_ = msInfer_ = 0.0f;
     waves_ = 0;
     lastRaysC_ = lastRaysS_ = lastNodes_ = lastTris_ = lastNodesS_ = lastTrisS_ = 0;
-    if (guide_)
+    if (guide_) CL_TRY(ensureGuideBuffers(err));
+    if (cache_) CL_TRY(ensureCacheBuffers(err));
+    // Online training: one step per network on the records of each sample
+    // per pixel while a network trains (the guide for its first train_spp
+    // spp; the cache for its first train_spp spp, or for every spp when 0),
+    // then the remaining samples in one pass.
+    for (;;)
     {
-        CL_TRY(ensureGuideBuffers(err));
-        // Online training: one step on the records of each of the first
-        // train_spp samples per pixel, then plain guided rendering.
-        while (spp > 0 && guide_->steps() < guideCfg_.train_spp)
-        {
-            CL_TRY(renderPass(1, true, err));
-            --spp;
-            Counters* dc = ctr_.as<Counters>();
-            CL_CUDA(cudaEventRecord(evA_, stream_), err);
-            kClampRecords<<<1, 32, 0, stream_>>>(dc, recCap_);
-            CL_CUDA(cudaGetLastError(), err);
-            CL_TRY(guide_->trainDevice(rec_.as<const float4>(), &dc->trainCount, err));
-            CL_CUDA(cudaEventRecord(evB_, stream_), err);
-            CL_CUDA(cudaMemcpyAsync(hostCount_, &dc->recCount, 8, cudaMemcpyDeviceToHost, stream_), err);
-            double loss = 0.0;
-            CL_CUDA(cudaMemcpyAsync(&loss, guide_->lossDev(), 8, cudaMemcpyDeviceToHost, stream_), err);
-            CL_CUDA(cudaEventSynchronize(evB_), err);
-            CL_CUDA(cudaStreamSynchronize(stream_), err);
-            float t = 0.0f;
-            CL_CUDA(cudaEventElapsedTime(&t, evA_, evB_), err);
-            msTrain_ += t;
-            msRender_ += t;
-            guideRecordsLast_ = hostCount_[0];
-            guideSamples_ += std::min(hostCount_[1], guideCfg_.batch);
-            guideLoss_ = loss;
-        }
+        const bool tg = guide_ && guide_->steps() < guideCfg_.train_spp;
+        const bool tc = cache_ && (cacheCfg_.train_spp == 0u || cache_->steps() < cacheCfg_.train_spp);
+        if (spp == 0 || (!tg && !tc)) break;
+        CL_TRY(renderPass(1, tg, tc, err));
+        --spp;
+        if (tg) CL_TRY(trainGuide(err));
+        if (tc) CL_TRY(trainCache(err));
     }
-    if (spp > 0) CL_TRY(renderPass(spp, false, err));
+    if (spp > 0) CL_TRY(renderPass(spp, false, false, err));
     return CL_OK;
 }
 
-cl_status Integrator::renderPass(uint32_t spp, bool record, std::string* err)
+cl_status Integrator::trainGuide(std::string* err)
+{
+    Counters* dc = ctr_.as<Counters>();
+    CL_CUDA(cudaEventRecord(evA_, stream_), err);
+    kClampRecords<<<1, 32, 0, stream_>>>(dc, recCap_);
+    CL_CUDA(cudaGetLastError(), err);
+    CL_TRY(guide_->trainDevice(rec_.as<const float4>(), &dc->trainCount, err));
+    CL_CUDA(cudaEventRecord(evB_, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(hostCount_, &dc->recCount, 8, cudaMemcpyDeviceToHost, stream_), err);
+    double loss = 0.0;
+    CL_CUDA(cudaMemcpyAsync(&loss, guide_->lossDev(), 8, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaEventSynchronize(evB_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    float t = 0.0f;
+    CL_CUDA(cudaEventElapsedTime(&t, evA_, evB_), err);
+    msTrain_ += t;
+    msRender_ += t;
+    guideRecordsLast_ = hostCount_[0];
+    guideSamples_ += std::min(hostCount_[1], guideCfg_.batch);
+    guideLoss_ = loss;
+    return CL_OK;
+}
+
+cl_status Integrator::trainCache(std::string* err)
+{
+    Counters* dc = ctr_.as<Counters>();
+    CL_CUDA(cudaEventRecord(evA_, stream_), err);
+    kClampCacheRecords<<<1, 32, 0, stream_>>>(dc, cacheRecCap_);
+    CL_CUDA(cudaGetLastError(), err);
+    CL_TRY(cache_->trainDevice(cacheRec_.as<const float4>(), &dc->cacheTrainCount, err));
+    CL_CUDA(cudaEventRecord(evB_, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(hostCount_ + 2, &dc->cacheRec, 8, cudaMemcpyDeviceToHost, stream_), err);
+    double loss = 0.0;
+    CL_CUDA(cudaMemcpyAsync(&loss, cache_->lossDev(), 8, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaEventSynchronize(evB_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    float t = 0.0f;
+    CL_CUDA(cudaEventElapsedTime(&t, evA_, evB_), err);
+    msCacheTrain_ += t;
+    msRender_ += t;
+    cacheRecordsLast_ = hostCount_[2];
+    cacheSamples_ += std::min(hostCount_[3], cacheCfg_.network.batch);
+    cacheLoss_ = loss;
+    return CL_OK;
+}
+
+cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std::string* err)
 {
     const bool dl      = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
     const bool profile = cfg_.flags & CL_PROFILE_STAGES;
@@ -1504,6 +1697,7 @@ cl_status Integrator::renderPass(uint32_t spp, bool record, std::string* err)
     wp.flags       = cfg_.flags;
     wp.dl          = dl ? 1u : 0u;
     wp.recStride   = record ? recStride_ : 0u;
+    wp.cacheTrain  = cacheTrain ? 1u : 0u;
     wp.totalPaths  = (unsigned long long)W_ * H_ * spp;
     memcpy(wp.cam, &camera_, sizeof(camera_));
     CL_CUDA(cudaMemcpyAsync(wp_.p, hostWp_, sizeof(WaveParams), cudaMemcpyHostToDevice, stream_), err);
@@ -1580,6 +1774,7 @@ cl_status Integrator::renderPass(uint32_t spp, bool record, std::string* err)
     lastNodesS_ += ch.statNodesS;
     lastTrisS_ += ch.statTrisS;
     guideInferred_ += ch.inferred;
+    cacheQueries_ += ch.cacheQueries;
     launches_ = waves_;
     iteration_ += spp;
     filmSpp_ += spp;
@@ -1673,6 +1868,92 @@ cl_status Integrator::guideStats(cl_guide_stats* s, std::string* err) const
     s->last_loss       = guideLoss_;
     s->ms_train        = msTrain_;
     s->ms_infer        = msInfer_;
+    return CL_OK;
+}
+
+cl_status Integrator::ensureCacheBuffers(std::string* err)
+{
+    cacheHistDepth_ = std::min(cfg_.max_depth, 31u);
+    cacheRecCap_    = uint32_t(std::min<uint64_t>(4ull * cacheCfg_.network.batch, 1ull << 26));
+    const size_t lb = size_t(slots_) * 16, eb = size_t(slots_) * guide::kIn * 2,
+                 hb = size_t(slots_) * cacheHistDepth_ * kCacheHistF4 * 16, rb = size_t(cacheRecCap_) * kRecordF4 * 16;
+    if (cacheL_.bytes != lb)
+    {
+        CL_TRY(cacheL_.alloc(lb, err));
+        CL_TRY(cacheEncIdx_.alloc(size_t(slots_) * 4, err));
+        graphValid_ = false;
+    }
+    if (cacheEnc_.bytes != eb)
+    {
+        CL_TRY(cacheEnc_.alloc(eb, err));
+        graphValid_ = false;
+    }
+    if (cacheHist_.bytes != hb)
+    {
+        CL_TRY(cacheHist_.alloc(hb, err));
+        graphValid_ = false;
+    }
+    if (cacheRec_.bytes != rb)
+    {
+        CL_TRY(cacheRec_.alloc(rb, err));
+        graphValid_ = false;
+    }
+    return CL_OK;
+}
+
+cl_status Integrator::setRadianceCache(const cl_radiance_cache_config* cfg, std::string* err)
+{
+    if (!cfg)
+    {
+        cache_.reset();
+        cacheL_.release();
+        cacheEnc_.release();
+        cacheEncIdx_.release();
+        cacheHist_.release();
+        cacheRec_.release();
+        graphValid_ = false;
+        return resetIteration(err);
+    }
+    if (type_ != CL_INTEGRATOR_PATH_TRACING)
+    {
+        *err = "the radiance cache needs the path-tracing integrator";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (cfg_.flags & CL_COMPAT_ALL)
+    {
+        *err = "the radiance cache needs the corrected estimator (no CL_COMPAT_* flag)";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (cfg->prefix_bounces < 1u || cfg->prefix_bounces > 254u || cfg->train_log2_fraction > 16u)
+    {
+        *err = "radiance cache: prefix_bounces must be in [1, 254], train_log2_fraction in [0, 16]";
+        return CL_ERR_INVALID_ARG;
+    }
+    std::unique_ptr<CacheNet> c(new CacheNet(cfg->network));
+    CL_TRY(c->init(stream_, err));
+    cache_    = std::move(c);
+    cacheCfg_ = *cfg;
+    cacheSamples_ = cacheRecordsLast_ = cacheQueries_ = 0;
+    cacheLoss_    = 0.0;
+    msCacheTrain_ = 0.0f;
+    graphValid_   = false;
+    return resetIteration(err);
+}
+
+cl_status Integrator::cacheStats(cl_guide_stats* s, std::string* err) const
+{
+    if (!cache_)
+    {
+        *err = "the radiance cache is off";
+        return CL_ERR_STATE;
+    }
+    s->steps           = cache_->steps();
+    s->samples_trained = cacheSamples_;
+    s->records_last    = cacheRecordsLast_;
+    s->inferred        = cacheQueries_;
+    s->last_loss       = cacheLoss_;
+    s->ms_train        = msCacheTrain_;
+    s->ms_infer        = 0.0f;
     return CL_OK;
 }
 

@@ -38,6 +38,8 @@ struct WaveParams
 {
     uint32_t           W, H, frame0, maxDepth, rrStart, flags, dl;
     uint32_t           recStride; // guiding: slots s with s % recStride == 0 record training data (0: off)
+    uint32_t           cacheTrain; // radiance cache: 1 = training paths are traced and recorded this pass
+    uint32_t           pad3;
     unsigned long long totalPaths;
     float              cam[12];
 };
@@ -59,6 +61,11 @@ struct Counters
     uint32_t           trainCount; // guiding: records the training step reads (clamped)
     uint32_t           pad2;
     unsigned long long inferred;   // guiding: network evaluations
+    uint32_t           cacheCount; // radiance cache: rays terminating into the cache this wave (compacted)
+    uint32_t           cacheRec;   // radiance cache: training records appended (may exceed the capacity)
+    uint32_t           cacheTrainCount; // radiance cache: records the training step reads (clamped)
+    uint32_t           pad4;
+    unsigned long long cacheQueries; // radiance cache: network evaluations
 };
 
 struct QueueDev
@@ -104,11 +111,31 @@ struct GuideDev
     uint32_t histDepth;
 };
 
+// Radiance cache (no counterpart in the reference): paths terminate into the
+// cache at depth termDepth = prefix + 1; training paths (path index hash &
+// trainMask == 0) continue to the maximum depth and record every vertex.
+// psE.w of a slot holds kCacheTrainBit and the mask of recorded depths.
+constexpr uint32_t kCacheTrainBit = 0x80000000u;
+constexpr int      kCacheHistF4   = 4; // {p, T.x} {n, T.y} {wo, T.z} {L before the vertex's emitter sample, -}
+struct CacheDev
+{
+    float4*   L;         // per ray-queue index: predicted outgoing radiance
+    uint4*    enc;       // encoded inputs of the terminating rays (compacted)
+    uint32_t* encIdx;    // their ray-queue indices
+    float4*   hist;      // slots x histDepth x kCacheHistF4
+    float4*   rec;       // kRecordF4 per training record
+    uint32_t  recCap;
+    uint32_t  termDepth; // 0: cache off
+    uint32_t  trainMask;
+    uint32_t  histDepth;
+};
+
 struct Params
 {
     SceneDev          sc;
     QueueDev          q;
     GuideDev          g;
+    CacheDev          c;
     const WaveParams* wp;
 };
 
@@ -141,13 +168,19 @@ public:
     cl_status setGuiding(const cl_guide_config* cfg, std::string* err);
     GuideNet* guideNet() const { return guide_.get(); }
     cl_status guideStats(cl_guide_stats* s, std::string* err) const;
+    cl_status setRadianceCache(const cl_radiance_cache_config* cfg, std::string* err);
+    CacheNet* cacheNet() const { return cache_.get(); }
+    cl_status cacheStats(cl_guide_stats* s, std::string* err) const;
 
     uint32_t width() const { return W_; }
     uint32_t height() const { return H_; }
 
 private:
-    cl_status renderPass(uint32_t spp, bool record, std::string* err);
+    cl_status renderPass(uint32_t spp, bool record, bool cacheTrain, std::string* err);
     cl_status ensureGuideBuffers(std::string* err);
+    cl_status ensureCacheBuffers(std::string* err);
+    cl_status trainGuide(std::string* err);
+    cl_status trainCache(std::string* err);
     cl_status ensureFilm(std::string* err);
     cl_status ensureQueues(std::string* err);
     cl_status clearFilm(std::string* err);
@@ -213,6 +246,16 @@ private:
     uint64_t                  guideSamples_ = 0, guideRecordsLast_ = 0, guideInferred_ = 0;
     double                    guideLoss_ = 0.0;
     float                     msTrain_ = 0.0f, msInfer_ = 0.0f;
+
+    // Radiance cache.
+    std::unique_ptr<CacheNet>  cache_;
+    cl_radiance_cache_config   cacheCfg_{};
+    DevBuf                     cacheL_, cacheEnc_, cacheEncIdx_, cacheHist_, cacheRec_;
+    uint32_t                   cacheRecCap_ = 0, cacheHistDepth_ = 0;
+    int                        cacheEncodeBlocks_ = 0, cacheMlpBlocks_ = 0;
+    uint64_t                   cacheSamples_ = 0, cacheRecordsLast_ = 0, cacheQueries_ = 0;
+    double                     cacheLoss_ = 0.0;
+    float                      msCacheTrain_ = 0.0f;
 };
 
 } // namespace clb

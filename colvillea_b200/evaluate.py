@@ -1,17 +1,19 @@
 """Image-quality measurement: relMSE against an FP64-accumulated reference and
-the equal-time comparison of guided and plain path tracing (no counterpart in
-the reference renderer, which has neither guiding nor an error metric).
+the equal-time comparison of neural (guided and/or radiance-cached) and plain
+path tracing (no counterpart in the reference renderer, which has neither
+networks nor an error metric).
 
 relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + 1e-2).
-Equal time: the guided tracer renders `spp` samples per pixel (its time
+Equal time: the neural tracer renders `spp` samples per pixel (its time
 includes online training); the plain tracer then renders as many samples as
-fit in the same device time.  Both use the corrected estimator and the alias
+fit in the same device time.  The reference's own noise adds equally to both
+relMSE values.  Both use the corrected estimator and the alias
 dome sampler; every seed is a disjoint range of progressive frame indices
 (the sampler's frame key), and every seed trains a fresh network.
 """
 import numpy as np
 
-from . import DOME_ALIAS, FILM_FP64, GuideConfig, load_scene
+from . import DOME_ALIAS, FILM_FP64, GuideConfig, RadianceCacheConfig, load_scene
 
 FLAGS = DOME_ALIAS | FILM_FP64
 # FLOPs per sample of the guiding MLP (96-64-64-64-64-48, multiply-adds x 2)
@@ -26,7 +28,7 @@ def relmse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref * ref + 1e-2)))
 
 
-def reference(scene, spp, chunk=256, max_depth=None, frame0=0):
+def reference(scene, spp, chunk=256, max_depth=None, frame0=1 << 30):
     """FP64-accumulated plain render (mean per pixel, (H*W, 3))."""
     it = load_scene(scene, flags=FLAGS, max_depth=max_depth)
     it.setIterationIndex(frame0)
@@ -48,34 +50,42 @@ def _render(it, spp, frame0):
     return s1 / spp, ms
 
 
-def equal_time(scene, ref, spp, seeds=3, guide=None, max_depth=None, seed_stride=1 << 20):
-    """Guided (spp samples, training included) vs plain at the guided render's
-    device time, over `seeds` disjoint frame ranges.  Returns a dict."""
-    guide = guide if guide is not None else GuideConfig()
+def equal_time(scene, ref, spp, seeds=3, guide=None, cache=None, max_depth=None, seed_stride=1 << 20):
+    """The neural tracer - guiding (`guide`, a GuideConfig) and/or the
+    radiance cache (`cache`, a RadianceCacheConfig); guiding alone when both
+    are None - renders `spp` samples (training included); the plain tracer
+    then renders as many as fit in the same device time.  Over `seeds`
+    disjoint frame ranges, every seed with fresh networks.  Returns a dict."""
+    if guide is None and cache is None:
+        guide = GuideConfig()
     plain = load_scene(scene, flags=FLAGS, max_depth=max_depth)
-    _, ms_probe = _render(plain, 8, 0)          # warm-up and per-spp cost
-    ms_probe = _render(plain, 32, 0)[1] / 32
-    gi = load_scene(scene, flags=FLAGS, max_depth=max_depth)
-    out = {"spp_guided": spp, "seeds": seeds, "relmse_guided": [], "relmse_plain": [], "spp_plain": [],
-           "ms_guided": [], "ms_plain": [], "train_ms": [], "final_loss": []}
+    _render(plain, 8, 0)                        # warm-up
+    ms_probe = _render(plain, 32, 0)[1] / 32    # per-spp cost
+    nt = load_scene(scene, flags=FLAGS, max_depth=max_depth)
+    out = {"spp_neural": spp, "seeds": seeds, "relmse_neural": [], "relmse_plain": [], "spp_plain": [],
+           "ms_neural": [], "ms_plain": [], "train_ms": [], "bias_neural": []}
     for k in range(seeds):
         f0 = (k + 1) * seed_stride
-        gi.setGuiding(guide)                    # fresh network, trained online in this render
-        img_g, ms_g = _render(gi, spp, f0)
-        gs = gi.guideStats()
-        n_p = max(1, int(round(ms_g / ms_probe)))
+        if guide is not None:
+            nt.setGuiding(guide)                # fresh networks, trained online in this render
+        if cache is not None:
+            nt.setRadianceCache(cache)
+        img_n, ms_n = _render(nt, spp, f0)
+        tr = (nt.guideStats()["ms_train"] if guide is not None else 0.0) + \
+             (nt.cacheStats()["ms_train"] if cache is not None else 0.0)
+        n_p = max(1, int(round(ms_n / ms_probe)))
         img_p, ms_p = _render(plain, n_p, f0)
-        out["relmse_guided"].append(relmse(img_g, ref))
+        out["relmse_neural"].append(relmse(img_n, ref))
         out["relmse_plain"].append(relmse(img_p, ref))
+        out["bias_neural"].append(float((img_n.mean() - ref.mean()) / ref.mean()))
         out["spp_plain"].append(n_p)
-        out["ms_guided"].append(ms_g)
+        out["ms_neural"].append(ms_n)
         out["ms_plain"].append(ms_p)
-        out["train_ms"].append(gs["ms_train"])
-        out["final_loss"].append(gs["last_loss"])
-    gi.close()
+        out["train_ms"].append(tr)
+    nt.close()
     plain.close()
-    rg, rp = float(np.mean(out["relmse_guided"])), float(np.mean(out["relmse_plain"]))
-    out.update({"relmse_guided_mean": rg, "relmse_plain_mean": rp, "plain_over_guided": rp / rg,
+    rn, rp = float(np.mean(out["relmse_neural"])), float(np.mean(out["relmse_plain"]))
+    out.update({"relmse_neural_mean": rn, "relmse_plain_mean": rp, "plain_over_neural": rp / rn,
                 "plain_ms_per_spp": ms_probe})
     return out
 

@@ -401,6 +401,51 @@ cl_status cl_integrator_set_guiding(cl_integrator* integrator, const cl_guide_co
 cl_status cl_integrator_get_guide(cl_integrator* integrator, cl_guide** guide);
 cl_status cl_integrator_guide_stats(cl_integrator* integrator, cl_guide_stats* stats);
 
+/* ---- Neural radiance cache.
+ * No counterpart in the reference.  A second hash-grid network, 96 -> 64 ->
+ * 64 -> 16 (ReLU; outputs 0-2: RGB), predicts the outgoing radiance at a
+ * path vertex from (position, shading normal, outgoing direction), with the
+ * same encoding as the guiding network.  Path tracing with the cache: a
+ * path is shaded normally for `prefix_bounces` vertices and terminates into
+ * the cache at the next one (its radiance is throughput x prediction; no
+ * emitter sample there).  One path in 2^train_log2_fraction (by a hash of
+ * the path index) is a training path: it is traced to max_depth, and each of
+ * its vertices k yields the record (x_k, n_k, wo_k) -> (L - L_k) / T_k, the
+ * radiance the path gathered from k on divided by the throughput that
+ * reached k.  Training minimises the relative L2 loss (o - y)^2 / (o^2 +
+ * 0.01) with Adam, one step on up to `network.batch` records after each of
+ * the first train_spp samples per pixel (0: after every sample).  The cache
+ * trades bias for shorter paths.
+ * Host record layout of the cache's own entry points:
+ *   rec12: in9 (as for the guiding network), then the target RGB. */
+typedef struct cl_cache cl_cache;
+typedef struct cl_radiance_cache_config
+{
+    cl_guide_config network;       /* hash grid, Adam and batch (the guiding-only fields are ignored) */
+    uint32_t        prefix_bounces; /* shaded vertices before the cache terminates a path (2) */
+    uint32_t        train_log2_fraction; /* 1 / 2^k of the paths are training paths (4) */
+    uint32_t        train_spp;      /* training steps after the first train_spp spp; 0 = after every spp (32) */
+} cl_radiance_cache_config;
+
+void      cl_radiance_cache_default_config(cl_radiance_cache_config* config);
+cl_status cl_cache_create(const cl_guide_config* network, cl_cache** out);
+cl_status cl_cache_destroy(cl_cache* cache);
+cl_status cl_cache_param_count(const cl_cache* cache, uint64_t* count);
+cl_status cl_cache_get_resolutions(const cl_cache* cache, uint32_t* resolutions16);
+cl_status cl_cache_set_params(cl_cache* cache, const float* params, uint64_t count);
+cl_status cl_cache_get_params(const cl_cache* cache, float* params, uint64_t count);
+/* Raw outputs (count x 16; RGB in 0-2). */
+cl_status cl_cache_forward(cl_cache* cache, const float* in9, uint32_t count, float* out16);
+cl_status cl_cache_gradient(cl_cache* cache, const float* rec12, uint32_t count, double* loss, float* grad);
+cl_status cl_cache_train_step(cl_cache* cache, const float* rec12, uint32_t count, double* loss);
+/* Path tracing with the radiance cache (CL_INTEGRATOR_PATH_TRACING, no
+ * CL_COMPAT_* flag); NULL switches it off.  Combines with guiding.  Resets
+ * the iteration. */
+cl_status cl_integrator_set_radiance_cache(cl_integrator* integrator, const cl_radiance_cache_config* config);
+cl_status cl_integrator_get_cache(cl_integrator* integrator, cl_cache** cache);
+/* steps, samples_trained, records_last, inferred (cache queries), last_loss, ms_train. */
+cl_status cl_integrator_cache_stats(cl_integrator* integrator, cl_guide_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,16 +59,20 @@ def resolutions(nmin, nmax):
     return np.floor(nmin * b ** np.arange(L_LEVELS)).astype(np.int64)
 
 
-def mlp_param_count():
-    return sum(o * i for o, i in LAYERS)
+def mlp_param_count(layers=LAYERS):
+    return sum(o * i for o, i in layers)
 
 
-def split_params(params, log2T):
-    """params: flat [hash (L*T*F) | W0 | ... | W4] (each W row-major [out][in])."""
+# Radiance cache: 96 -> 64 -> 64 -> 16 (RGB in outputs 0-2).
+CACHE_LAYERS = [(WIDTH, N_IN), (WIDTH, WIDTH), (16, WIDTH)]
+
+
+def split_params(params, log2T, layers=LAYERS):
+    """params: flat [hash (L*T*F) | W0 | ... ] (each W row-major [out][in])."""
     T = 1 << log2T
     h = params[: L_LEVELS * T * F_FEAT].reshape(L_LEVELS, T, F_FEAT)
     ws, o = [], L_LEVELS * T * F_FEAT
-    for out, inn in LAYERS:
+    for out, inn in layers:
         ws.append(params[o: o + out * inn].reshape(out, inn))
         o += out * inn
     return h, ws
@@ -243,6 +247,34 @@ def loss_and_grads(params, log2T, res, pos, nrm, wo, omega, weight, pb=None, cla
     B = len(pos)
     loss = -np.sum(wn * lp) / B
     d = -(wn / B)[:, None] * hg                                  # d loss / d out
+    return loss, _backprop(d, ws, acts, table, corners)
+
+
+def cache_loss_and_grads(params, log2T, res, pos, nrm, wo, target):
+    """Radiance cache: relative L2 (o - y)^2 / (o^2 + 0.01) averaged over the
+    RGB outputs and the batch, the denominator held constant (stop-gradient)."""
+    table, ws = split_params(params, log2T, CACHE_LAYERS)
+    tb = bf16(table)
+    x, corners = encode(pos, nrm, wo, tb, res)
+    out, acts = forward(x, ws)
+    o = out[:, :3]
+    den = o * o + 0.01
+    B = len(pos)
+    loss = np.sum((o - target) ** 2 / den) / (3 * B)
+    d = np.zeros_like(out)
+    d[:, :3] = (2.0 / 3.0) * (o - target) / den / B
+    return loss, _backprop(d, ws, acts, table, corners)
+
+
+def cache_network(params, log2T, res, pos, nrm, wo):
+    table, ws = split_params(params, log2T, CACHE_LAYERS)
+    x, _ = encode(pos, nrm, wo, bf16(table), res)
+    out, _ = forward(x, ws)
+    return out
+
+
+def _backprop(d, ws, acts, table, corners):
+    """Gradient of the flat parameter vector from d loss / d out."""
     gws = [None] * len(ws)
     for k in range(len(ws) - 1, -1, -1):
         db = bf16(d)
@@ -257,8 +289,7 @@ def loss_and_grads(params, log2T, res, pos, nrm, wo, omega, weight, pb=None, cla
         for c in range(8):
             for f in range(F_FEAT):
                 np.add.at(gt[l, :, f], idx[:, c], wt[:, c] * d[:, 2 * l + f])
-    grad = np.concatenate([gt.ravel()] + [g.ravel() for g in gws])
-    return loss, grad
+    return np.concatenate([gt.ravel()] + [g.ravel() for g in gws])
 
 
 def adam(params, grad, m, v, step, lr=1e-2, b1=0.9, b2=0.99, eps=1e-10):

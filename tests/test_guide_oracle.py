@@ -153,3 +153,39 @@ def test_hash_grid_indexing():
     f, corners = G.hash_encode(np.array([[1.0, 1.0, 1.0]]), table, np.array([3] * 16))
     idx, wt = corners[0]
     assert np.isclose(wt[0, 7], 1.0) and idx[0, 7] == 3 + 3 * 4 + 3 * 16
+
+
+def test_cache_gradients_match_finite_differences(smooth):
+    """Radiance cache (96-64-64-16): relative L2 with the stop-gradient
+    denominator; the finite difference holds the denominator at the base
+    point too, so it is taken on the loss with a frozen denominator."""
+    rng = np.random.default_rng(6)
+    log2T = 8
+    T = 1 << log2T
+    res = G.resolutions(4, 64)
+    B = 24
+    p = np.concatenate([rng.uniform(-0.3, 0.3, G.L_LEVELS * T * 2)] +
+                       [rng.uniform(-1, 1, (o, i)).ravel() * np.sqrt(6 / (o + i)) for o, i in G.CACHE_LAYERS])
+    pos = rng.uniform(0, 1, (B, 3))
+    nrm, wo = _unit(rng, B), _unit(rng, B)
+    y = rng.uniform(0, 2, (B, 3))
+    loss, g = G.cache_loss_and_grads(p, log2T, res, pos, nrm, wo, y)
+    o0 = G.cache_network(p, log2T, res, pos, nrm, wo)[:, :3]
+    den = o0 * o0 + 0.01
+
+    def frozen(q):
+        o = G.cache_network(q, log2T, res, pos, nrm, wo)[:, :3]
+        return np.sum((o - y) ** 2 / den) / (3 * B)
+
+    assert np.isclose(frozen(p), loss)
+    nh = G.L_LEVELS * T * 2
+    touched = np.nonzero(g[:nh])[0]
+    idx = np.concatenate([rng.choice(touched, 16, replace=False), rng.choice(np.arange(nh, p.size), 40, replace=False)])
+    scale = np.abs(g).max()
+    for i in idx:
+        q = p.copy(); q[i] += 1e-5
+        lp = frozen(q)
+        q[i] -= 2e-5
+        lm = frozen(q)
+        fd = (lp - lm) / 2e-5
+        assert abs(fd - g[i]) <= 1e-6 * abs(g[i]) + 1e-8 * scale + 1e-11, (i, fd, g[i])
