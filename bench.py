@@ -47,11 +47,33 @@ def parse():
                     help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
     ap.add_argument("--no-relmse", action="store_true", help="skip the guided-vs-plain equal-time relMSE")
+    ap.add_argument("--profile-nets", choices=["guide", "cache"], default=None,
+                    help="short workload for ncu: cfg3 with guiding or cfg4 with the radiance cache, "
+                         "2 training spp + 2 spp")
     ap.add_argument("--relmse-ref-spp", type=int, default=8192, help="spp of the cfg3 FP64 reference image")
     ap.add_argument("--relmse-ref-spp4", type=int, default=8192, help="spp of the cfg4 FP64 reference image")
     ap.add_argument("--relmse-seeds", type=int, default=3)
     ap.add_argument("--relmse-spp", type=int, default=128, help="guided spp (training included)")
     return ap.parse_args()
+
+
+def run_profile_nets(args):
+    """A short render for ncu captures of the network kernels."""
+    import colvillea_b200 as cb
+    from colvillea_b200 import scenes
+    if args.profile_nets == "guide":
+        s = scenes.config3(0)
+        it = cb.load_scene(s, flags=cb.DOME_ALIAS | cb.FILM_FP64)
+        it.setGuiding(cb.GuideConfig(train_spp=2))
+    else:
+        s = scenes.config4(0)
+        it = cb.load_scene(s, flags=cb.DOME_ALIAS | cb.FILM_FP64)
+        it.setRadianceCache(cb.RadianceCacheConfig(train_spp=2))
+    it.render(2)
+    it.render(2)
+    print(json.dumps({"profile_nets": args.profile_nets, "last_rays_closest": it.stats()["last_rays_closest"]}))
+    it.close()
+    return 0
 
 
 def run_profile(args):
@@ -292,6 +314,8 @@ def main():
         return run_reference(args)
     if args.profile:
         return run_profile(args)
+    if args.profile_nets:
+        return run_profile_nets(args)
     import numpy as np
     import torch
     dist = Dist(args.gpus)
