@@ -16,7 +16,8 @@ from . import _native as N
 from ._native import ClError
 
 __all__ = ["IntegratorType", "Integrator", "RenderConfig", "ClError", "COMPAT_ALL", "DOME_ALIAS", "FILM_FP64",
-           "PROFILE_STAGES", "TRACE_STATS", "load_scene", "GuideConfig", "Guide", "RadianceCacheConfig", "Cache"]
+           "PROFILE_STAGES", "TRACE_STATS", "load_scene", "GuideConfig", "Guide", "RadianceCacheConfig", "Cache",
+           "load_obj", "load_hdr", "write_pfm", "read_pfm"]
 
 COMPAT_PDF, COMPAT_FRAME, COMPAT_ESCAPE, COMPAT_ALL = N.CL_COMPAT_PDF, N.CL_COMPAT_FRAME, N.CL_COMPAT_ESCAPE, N.CL_COMPAT_ALL
 DOME_ALIAS, FILM_FP64, PROFILE_STAGES, TRACE_STATS = N.CL_DOME_ALIAS, N.CL_FILM_FP64, N.CL_PROFILE_STAGES, N.CL_TRACE_STATS
@@ -411,6 +412,67 @@ def _guide_stats(self):
 Integrator.setGuiding = _set_guiding
 Integrator.guide = _guide
 Integrator.guideStats = _guide_stats
+
+
+# --- scene ingestion and film output (MeshImporter / ImageUtils, src/delegate) ---
+def load_obj(path):
+    """Meshes of a Wavefront OBJ file (one per o/g/usemtl group) as
+    scenes.Mesh: triangulated, unified vertices, normals (smooth where the
+    file has none), uvs with v flipped, tangents from the uvs."""
+    from .scenes import Mesh
+    h = ctypes.c_void_p()
+    N.call("cl_obj_load", str(path).encode(), ctypes.byref(h))
+    try:
+        n = ctypes.c_uint32()
+        N.call("cl_obj_mesh_count", h, ctypes.byref(n))
+        out = []
+        for i in range(n.value):
+            d = N.MeshDesc()
+            N.call("cl_obj_get_mesh", h, i, ctypes.byref(d))
+            nv, nt = d.num_vertices, d.num_triangles
+
+            def arr(ptr, k, dt=np.float32, ct=ctypes.c_float):
+                if not ptr:
+                    return None
+                return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ct)), shape=(k,)).astype(dt).copy()
+            pos = arr(d.positions, 3 * nv).reshape(nv, 3)
+            nrm = arr(d.normals, 3 * nv).reshape(nv, 3)
+            tan = arr(d.tangents, 3 * nv).reshape(nv, 3)
+            uv = arr(d.uvs, 2 * nv)
+            idx = arr(d.indices, 3 * nt, np.uint32, ctypes.c_uint32).reshape(nt, 3)
+            out.append(Mesh(pos, nrm, tan, None if uv is None else uv.reshape(nv, 2), idx))
+        return out
+    finally:
+        N.lib().cl_obj_free(h)
+
+
+def _take_image(ptr, w, h):
+    try:
+        return np.ctypeslib.as_array(ptr, shape=(h.value * w.value * 4,)).reshape(h.value, w.value, 4).copy()
+    finally:
+        N.lib().cl_image_free(ptr)
+
+
+def load_hdr(path):
+    """Radiance .hdr image as (h, w, 4) float32 (alpha 1), rows top to bottom."""
+    ptr, w, h = ctypes.POINTER(ctypes.c_float)(), ctypes.c_uint32(), ctypes.c_uint32()
+    N.call("cl_image_load_hdr", str(path).encode(), ctypes.byref(ptr), ctypes.byref(w), ctypes.byref(h))
+    return _take_image(ptr, w, h)
+
+
+def write_pfm(path, rgba):
+    """Writes an (h, w, 4) (or (h, w, 3)) float image, e.g. readbackFramebuffer(), as PFM."""
+    img = np.asarray(rgba, np.float32)
+    if img.shape[-1] == 3:
+        img = np.concatenate([img, np.ones(img.shape[:2] + (1,), np.float32)], -1)
+    img = np.ascontiguousarray(img)
+    N.call("cl_image_write_pfm", str(path).encode(), _ptr(img), img.shape[1], img.shape[0])
+
+
+def read_pfm(path):
+    ptr, w, h = ctypes.POINTER(ctypes.c_float)(), ctypes.c_uint32(), ctypes.c_uint32()
+    N.call("cl_image_read_pfm", str(path).encode(), ctypes.byref(ptr), ctypes.byref(w), ctypes.byref(h))
+    return _take_image(ptr, w, h)
 
 
 def load_scene(scene, itype=IntegratorType.WavefrontPathTracing, flags=COMPAT_ALL, max_depth=None, rr_start=None,

@@ -162,6 +162,18 @@ _SIGS.update({
     "cl_integrator_get_cache": [vp, ctypes.POINTER(vp)],
     "cl_integrator_cache_stats": [vp, ctypes.POINTER(GuideStats)],
 })
+_SIGS.update({
+    "cl_obj_load": [ctypes.c_char_p, ctypes.POINTER(vp)],
+    "cl_obj_mesh_count": [vp, ctypes.POINTER(u32)],
+    "cl_obj_get_mesh": [vp, u32, ctypes.POINTER(MeshDesc)],
+    "cl_obj_free": [vp],
+    "cl_image_load_hdr": [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)), ctypes.POINTER(u32),
+                          ctypes.POINTER(u32)],
+    "cl_image_free": [vp],
+    "cl_image_write_pfm": [ctypes.c_char_p, vp, u32, u32],
+    "cl_image_read_pfm": [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)), ctypes.POINTER(u32),
+                          ctypes.POINTER(u32)],
+})
 _VOID = {"cl_guide_default_config", "cl_radiance_cache_default_config"}
 
 _lib = None

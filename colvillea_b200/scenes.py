@@ -433,3 +433,30 @@ def config5(seed=0, width=3840, height=2160, terrain_n=2048, unique=128, copies=
 
 
 CONFIGS = {1: config1, 2: config2, 3: config3, 4: config4, 5: config5}
+
+
+def save_obj(path, meshes):
+    """Writes meshes as one Wavefront OBJ file (one `o` group per mesh, v/vt/vn
+    per corner; vt stores 1 - v so that the loader's v flip restores the uvs;
+    positions with 9 significant digits, exact for float32)."""
+    lines, base = [], 0
+    for i, m in enumerate(meshes):
+        lines.append(f"o mesh{i}")
+        lines += [f"v {x:.9g} {y:.9g} {z:.9g}" for x, y, z in m.positions.astype(np.float32)]
+        if m.uvs is not None:
+            lines += [f"vt {float(u):.17g} {1.0 - float(v):.17g}" for u, v in m.uvs.astype(np.float32)]
+        if m.normals is not None:
+            lines += [f"vn {x:.9g} {y:.9g} {z:.9g}" for x, y, z in m.normals.astype(np.float32)]
+        for tri in m.indices.astype(np.int64) + base + 1:
+            if m.uvs is not None and m.normals is not None:
+                lines.append("f " + " ".join(f"{k}/{k}/{k}" for k in tri))
+            elif m.normals is not None:
+                lines.append("f " + " ".join(f"{k}//{k}" for k in tri))
+            elif m.uvs is not None:
+                lines.append("f " + " ".join(f"{k}/{k}" for k in tri))
+            else:
+                lines.append("f " + " ".join(str(k) for k in tri))
+        base += len(m.positions)
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+

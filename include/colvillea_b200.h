@@ -306,6 +306,38 @@ cl_status cl_dome_build_tables_noalloc(const float* texels, uint32_t width, uint
                                        float* cdfU, float* pV_c, float* cdfV, uint32_t* alias_row,
                                        uint32_t* alias_col, void* stream);
 
+/* ---- Scene ingestion and film output.
+ * Replace the reference's asset delegates: MeshImporter::loadMeshes (assimp,
+ * src/delegate/meshimporter.cpp:41-120, flags Triangulate | GenSmoothNormals |
+ * GenUVCoords | FlipUVs | CalcTangentSpace) and
+ * ImageUtils::loadImageFromDiskRadianceHDR (stb_image,
+ * src/delegate/imageutil.cpp:98-139).  Host-side parsing; no device work.
+ *
+ * OBJ: one mesh per `o`/`g`/`usemtl` group with faces; polygons are
+ * triangulated as fans; vertices are unified per (v, vt, vn) triple; normals
+ * come from vn when every corner has one, else smooth normals (area-weighted
+ * face normals summed per position); uvs come from vt with v flipped (1 - v)
+ * when every corner has one, else none; tangents are dP/du from the uvs,
+ * summed per vertex and orthogonalised against the normal (without uvs: any
+ * perpendicular, since cl_build_meshes requires tangents).  The returned
+ * descriptors point into the cl_obj and stay valid until cl_obj_free; pass
+ * them to cl_build_meshes directly.
+ * HDR: Radiance RGBE ("#?RADIANCE", FORMAT=32-bit_rle_rgbe, "-Y h +X w",
+ * flat or new-style run-length scanlines), decoded as byte * 2^(e - 136),
+ * into RGBA32F rows top to bottom with alpha 1 (the dome texel layout);
+ * free with cl_image_free.
+ * PFM: RGB float32, rows stored bottom up (written from RGBA rows top to
+ * bottom, e.g. cl_readback_film's); read back into RGBA32F. */
+typedef struct cl_obj cl_obj;
+cl_status cl_obj_load(const char* path, cl_obj** out);
+cl_status cl_obj_mesh_count(const cl_obj* obj, uint32_t* count);
+cl_status cl_obj_get_mesh(const cl_obj* obj, uint32_t index, cl_mesh_desc* mesh);
+cl_status cl_obj_free(cl_obj* obj);
+cl_status cl_image_load_hdr(const char* path, float** rgba, uint32_t* width, uint32_t* height);
+cl_status cl_image_free(float* rgba);
+cl_status cl_image_write_pfm(const char* path, const float* rgba, uint32_t width, uint32_t height);
+cl_status cl_image_read_pfm(const char* path, float** rgba, uint32_t* width, uint32_t* height);
+
 /* ---- Neural path guiding.
  * No counterpart in the reference (its path tracer samples the BSDF only).
  * A guiding network maps (position, shading normal, outgoing direction) to a
