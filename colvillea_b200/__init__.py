@@ -91,6 +91,27 @@ class Integrator:
             descs[i] = N.InstanceDesc(mid, mat, (ctypes.c_float * 12)(*xf))
         N.call("cl_build_instances", self._h, descs, len(instances))
 
+    BVH_UPDATE = {"auto": N.CL_BVH_UPDATE_AUTO, "refit": N.CL_BVH_UPDATE_REFIT, "rebuild": N.CL_BVH_UPDATE_REBUILD}
+
+    def updateVertices(self, mesh_id, positions, normals=None, tangents=None, bvh="auto"):
+        """Shape edit (TriangleMesh::updateVertices, trianglemesh.h:111-118, then
+        RenderEngine::compileAccelStructs): new vertex positions for mesh `mesh_id`
+        (same count and triangles); the BVH is refitted ("refit"), rebuilt
+        ("rebuild") or refitted and rebuilt if its surface-area cost grew past
+        1.5x the built tree's ("auto"); the progressive iteration restarts."""
+        p = _f32(positions)
+        n = None if normals is None else _f32(normals)
+        t = None if tangents is None else _f32(tangents)
+        N.call("cl_update_mesh_vertices", self._h, mesh_id, _ptr(p), _ptr(n), _ptr(t), len(p), self.BVH_UPDATE[bvh])
+
+    def bvh(self):
+        """(nodes (n, 20) uint32, triangles (t, 12) float32): the built 8-wide BVH."""
+        s = self.stats()
+        nodes = np.empty((s["bvh_nodes"], 20), np.uint32)
+        tris = np.empty((s["triangles"], 12), np.float32)
+        N.call("cl_get_bvh", self._h, _ptr(nodes), nodes.nbytes, _ptr(tris), tris.nbytes)
+        return nodes, tris
+
     def buildMaterials(self, materials):
         descs = (N.MaterialDesc * len(materials))()
         for i, m in enumerate(materials):

@@ -25,6 +25,8 @@ CL_FILM_FP64 = 1 << 5
 CL_PROFILE_STAGES = 1 << 6
 CL_TRACE_STATS = 1 << 7
 
+CL_BVH_UPDATE_AUTO, CL_BVH_UPDATE_REFIT, CL_BVH_UPDATE_REBUILD = range(3)
+
 vp = ctypes.c_void_p
 u32 = ctypes.c_uint32
 
@@ -64,7 +66,9 @@ class Stats(ctypes.Structure):
                 ("ms_last_render", ctypes.c_float), ("ms_trace", ctypes.c_float), ("ms_shade", ctypes.c_float),
                 ("ms_shadow", ctypes.c_float), ("launches", u32), ("pad", u32), ("trace_nodes", ctypes.c_uint64),
                 ("trace_tris", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64), ("shadow_tris", ctypes.c_uint64),
-                ("last_rays_closest", ctypes.c_uint64), ("last_rays_shadow", ctypes.c_uint64)]
+                ("last_rays_closest", ctypes.c_uint64), ("last_rays_shadow", ctypes.c_uint64),
+                ("ms_bvh_update", ctypes.c_float), ("bvh_refits", u32), ("bvh_rebuilds", u32), ("pad2", u32),
+                ("bvh_sah", ctypes.c_double), ("bvh_sah_build", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -97,6 +101,8 @@ _SIGS = {
     "cl_integrator_destroy": [vp],
     "cl_build_meshes": [vp, ctypes.POINTER(MeshDesc), u32],
     "cl_build_instances": [vp, ctypes.POINTER(InstanceDesc), u32],
+    "cl_update_mesh_vertices": [vp, u32, vp, vp, vp, u32, u32],
+    "cl_get_bvh": [vp, vp, ctypes.c_size_t, vp, ctypes.c_size_t],
     "cl_build_materials": [vp, ctypes.POINTER(MaterialDesc), u32],
     "cl_build_emitters": [vp, ctypes.POINTER(EmitterDesc), u32],
     "cl_update_camera": [vp, ctypes.POINTER(Camera)],

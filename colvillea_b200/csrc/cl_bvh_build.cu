@@ -36,6 +36,19 @@ __device__ __forceinline__ float funordered(uint32_t b)
     return __uint_as_float((b & 0x80000000u) ? (b & 0x7fffffffu) : ~b);
 }
 
+// Widening of every child box before quantisation: 2^-20 of the scene
+// scale (the product is exact, so host and device agree bit for bit).
+__host__ __device__ inline float sceneMargin(const float lo[3], const float hi[3])
+{
+    float scale = 0.0f;
+    for (int a = 0; a < 3; ++a)
+    {
+        scale = fmaxf(scale, fmaxf(fabsf(lo[a]), fabsf(hi[a])));
+        scale = fmaxf(scale, hi[a] - lo[a]);
+    }
+    return scale * 9.5367431640625e-07f + 1e-30f;
+}
+
 struct Bounds
 {
     uint32_t clo[3], chi[3]; // centroid bounds (ordered ints)
@@ -383,6 +396,20 @@ __device__ __forceinline__ uint32_t quantExp(float ext)
     return ex;
 }
 
+// 8-bit planes of a child interval [lo, hi] in the frame (p, e), rounded
+// outwards so that the dequantised box p + e * q contains the interval.
+__device__ __forceinline__ void quantPlanes(float lo, float hi, float p, float e, uint32_t* ql, uint32_t* qh)
+{
+    int lo_ = int(floorf((lo - p) / e));
+    int hi_ = int(ceilf((hi - p) / e));
+    lo_     = max(0, min(255, lo_));
+    hi_     = max(0, min(255, hi_));
+    while (lo_ > 0 && p + e * float(lo_) > lo) --lo_;
+    while (hi_ < 255 && p + e * float(hi_) < hi) ++hi_;
+    *ql = uint32_t(lo_);
+    *qh = uint32_t(hi_);
+}
+
 __global__ void kCollapse(CollapseArgs A, const uint2* __restrict__ tasks, uint32_t ntasks)
 {
     uint32_t ti = blockIdx.x * blockDim.x + threadIdx.x;
@@ -518,17 +545,7 @@ __global__ void kCollapse(CollapseArgs A, const uint2* __restrict__ tasks, uint3
         }
         else
         {
-            for (int a = 0; a < 3; ++a)
-            {
-                int lo_ = int(floorf((clo[k][a] - plo[a]) / e[a]));
-                int hi_ = int(ceilf((chi[k][a] - plo[a]) / e[a]));
-                lo_     = max(0, min(255, lo_));
-                hi_     = max(0, min(255, hi_));
-                while (lo_ > 0 && plo[a] + e[a] * float(lo_) > clo[k][a]) --lo_;
-                while (hi_ < 255 && plo[a] + e[a] * float(hi_) < chi[k][a]) ++hi_;
-                ql[a] = uint32_t(lo_);
-                qh[a] = uint32_t(hi_);
-            }
+            for (int a = 0; a < 3; ++a) quantPlanes(clo[k][a], chi[k][a], plo[a], e[a], &ql[a], &qh[a]);
             uint32_t r = ch[k];
             uint32_t c = refCount(A, r);
             if (c > 3u)
@@ -699,8 +716,7 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     Bounds bh;
     CL_CUDA(cudaMemcpyAsync(&bh, bounds.p, sizeof(bh), cudaMemcpyDeviceToHost, st), err);
     CL_CUDA(cudaStreamSynchronize(st), err);
-    float scale = 0.0f;
-    for (int a = 0; a < 3; ++a)
+    float margin;
     {
         auto unord = [](uint32_t v) {
             uint32_t bits = (v & 0x80000000u) ? (v & 0x7fffffffu) : ~v;
@@ -708,11 +724,14 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
             memcpy(&f, &bits, 4);
             return f;
         };
-        float l = unord(bh.slo[a]), h = unord(bh.shi[a]);
-        scale   = std::max(scale, std::max(std::fabs(l), std::fabs(h)));
-        scale   = std::max(scale, h - l);
+        float l[3], h[3];
+        for (int a = 0; a < 3; ++a)
+        {
+            l[a] = unord(bh.slo[a]);
+            h[a] = unord(bh.shi[a]);
+        }
+        margin = sceneMargin(l, h);
     }
-    float margin = scale * 9.5367431640625e-07f + 1e-30f; // 2^-20 of the scene scale
 
     uint32_t maxNodes = n + 1;
     CL_TRY(out->nodes.alloc(size_t(maxNodes) * 80, err));
@@ -747,6 +766,7 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     A.err         = ctr.u() + 3;
 
     uint32_t ntasks = 1, depth = 0;
+    out->levels.assign({0u, 1u});
     DevBuf*  cur = &tasksA;
     DevBuf*  nxt = &tasksB;
     while (ntasks > 0)
@@ -772,6 +792,7 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
         }
         std::swap(cur, nxt);
         out->numNodes = hc[0];
+        if (hc[0] > out->levels.back()) out->levels.push_back(hc[0]);
         if (hc[1] > n)
         {
             *err = "BVH collapse emitted too many triangles";
@@ -836,6 +857,297 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
         *err = "BVH depth " + std::to_string(depth) + " exceeds the traversal stack";
         return CL_ERR_STATE;
     }
+    return CL_OK;
+}
+
+namespace
+{
+constexpr int kRefitBlock = 128;
+
+// Leaf triangles from the vertex array; scene bounds into bounds[0..5] as
+// ordered ints (min x,y,z then max x,y,z).
+__global__ void kRefitTris(float4* __restrict__ tris, uint32_t n, const float4* __restrict__ vtx,
+                           const uint4* __restrict__ triIdx, uint32_t* __restrict__ bounds)
+{
+    uint32_t i     = blockIdx.x * blockDim.x + threadIdx.x;
+    bool     valid = i < n;
+    float    l[3] = {0.0f, 0.0f, 0.0f}, h[3] = {0.0f, 0.0f, 0.0f};
+    if (valid)
+    {
+        float4*  t   = tris + 3 * size_t(i);
+        uint32_t tid = __float_as_uint(t[0].w);
+        uint4    ix  = triIdx[tid];
+        float4   a = vtx[3 * size_t(ix.x)], b = vtx[3 * size_t(ix.y)], c = vtx[3 * size_t(ix.z)];
+        t[0]         = make_float4(a.x, a.y, a.z, __uint_as_float(tid));
+        t[1]         = make_float4(b.x, b.y, b.z, 0.0f);
+        t[2]         = make_float4(c.x, c.y, c.z, 0.0f);
+        l[0] = fminf(fminf(a.x, b.x), c.x);
+        l[1] = fminf(fminf(a.y, b.y), c.y);
+        l[2] = fminf(fminf(a.z, b.z), c.z);
+        h[0] = fmaxf(fmaxf(a.x, b.x), c.x);
+        h[1] = fmaxf(fmaxf(a.y, b.y), c.y);
+        h[2] = fmaxf(fmaxf(a.z, b.z), c.z);
+    }
+    for (int a = 0; a < 3; ++a)
+    {
+        uint32_t sl = valid ? fordered(l[a]) : 0xffffffffu, sh = valid ? fordered(h[a]) : 0u;
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            sl = min(sl, __shfl_xor_sync(0xffffffffu, sl, o));
+            sh = max(sh, __shfl_xor_sync(0xffffffffu, sh, o));
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            atomicMin(bounds + a, sl);
+            atomicMax(bounds + 3 + a, sh);
+        }
+    }
+}
+
+// One tree level: child boxes from the level below (exact[]) and from the
+// leaf triangles, widened by the scene margin and requantised in a fresh
+// frame.  Topology (imask, child and triangle bases, leaf metadata, slot
+// order) is kept.
+__global__ void __launch_bounds__(kRefitBlock) kRefitLevel(uint4* __restrict__ nodes, const float4* __restrict__ tris,
+                                                           float* __restrict__ exact, uint32_t first, uint32_t count,
+                                                           const uint32_t* __restrict__ bounds)
+{
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    uint32_t node = first + t;
+    float    sl[3], sh[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        sl[a] = funordered(bounds[a]);
+        sh[a] = funordered(bounds[3 + a]);
+    }
+    float    margin = sceneMargin(sl, sh);
+    uint4*   np     = nodes + size_t(node) * 5;
+    uint4    n0 = np[0], n1 = np[1];
+    uint32_t imask = n0.w >> 24;
+    uint32_t meta[2] = {n1.z, n1.w};
+
+    float    clo[8][3], chi[8][3], plo[3], phi[3], xlo[3], xhi[3];
+    uint32_t present = 0;
+    for (int a = 0; a < 3; ++a)
+    {
+        plo[a] = xlo[a] = FLT_MAX;
+        phi[a] = xhi[a] = -FLT_MAX;
+    }
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+    {
+        for (int a = 0; a < 3; ++a)
+        {
+            clo[s][a] = FLT_MAX;
+            chi[s][a] = -FLT_MAX;
+        }
+        if (imask & (1u << s))
+        {
+            uint32_t     c = n1.x + __popc(imask & ((1u << s) - 1u));
+            const float* x = exact + 6 * size_t(c);
+            for (int a = 0; a < 3; ++a)
+            {
+                clo[s][a] = x[a];
+                chi[s][a] = x[3 + a];
+            }
+        }
+        else
+        {
+            uint32_t m = (meta[s >> 2] >> (8 * (s & 3))) & 0xffu;
+            if (!m) continue;
+            uint32_t off = m & 31u, cnt = __popc(m >> 5);
+            for (uint32_t j = 0; j < cnt; ++j)
+            {
+                const float4* tp = tris + size_t(n1.y + off + j) * 3;
+                for (int v = 0; v < 3; ++v)
+                {
+                    float4 p = tp[v];
+                    clo[s][0] = fminf(clo[s][0], p.x);
+                    clo[s][1] = fminf(clo[s][1], p.y);
+                    clo[s][2] = fminf(clo[s][2], p.z);
+                    chi[s][0] = fmaxf(chi[s][0], p.x);
+                    chi[s][1] = fmaxf(chi[s][1], p.y);
+                    chi[s][2] = fmaxf(chi[s][2], p.z);
+                }
+            }
+        }
+        present |= 1u << s;
+        for (int a = 0; a < 3; ++a)
+        {
+            xlo[a]    = fminf(xlo[a], clo[s][a]);
+            xhi[a]    = fmaxf(xhi[a], chi[s][a]);
+            clo[s][a] -= margin;
+            chi[s][a] += margin;
+            plo[a]    = fminf(plo[a], clo[s][a]);
+            phi[a]    = fmaxf(phi[a], chi[s][a]);
+        }
+    }
+
+    uint32_t ex[3];
+    float    e[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        ex[a] = quantExp(phi[a] - plo[a]);
+        e[a]  = __uint_as_float(ex[a] << 23);
+    }
+    uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+#pragma unroll
+    for (int s = 0; s < 8; ++s)
+    {
+        int      word = s >> 2, sh8 = 8 * (s & 3);
+        uint32_t ql[3] = {255u, 255u, 255u}, qh[3] = {0u, 0u, 0u};
+        if (present & (1u << s))
+            for (int a = 0; a < 3; ++a) quantPlanes(clo[s][a], chi[s][a], plo[a], e[a], &ql[a], &qh[a]);
+        for (int a = 0; a < 3; ++a)
+        {
+            qlo[a][word] |= ql[a] << sh8;
+            qhi[a][word] |= qh[a] << sh8;
+        }
+    }
+    np[0] = make_uint4(__float_as_uint(plo[0]), __float_as_uint(plo[1]), __float_as_uint(plo[2]),
+                       ex[0] | (ex[1] << 8) | (ex[2] << 16) | (imask << 24));
+    np[2] = make_uint4(qlo[0][0], qlo[0][1], qlo[1][0], qlo[1][1]);
+    np[3] = make_uint4(qlo[2][0], qlo[2][1], qhi[0][0], qhi[0][1]);
+    np[4] = make_uint4(qhi[1][0], qhi[1][1], qhi[2][0], qhi[2][1]);
+    float* x = exact + 6 * size_t(node);
+    for (int a = 0; a < 3; ++a)
+    {
+        x[a]     = xlo[a];
+        x[3 + a] = xhi[a];
+    }
+}
+
+__device__ __forceinline__ double boxArea(float lx, float ly, float lz, float hx, float hy, float hz)
+{
+    double dx = double(hx) - lx, dy = double(hy) - ly, dz = double(hz) - lz;
+    return 2.0 * (dx * dy + dy * dz + dz * dx);
+}
+
+// Sum over all child slots of (dequantised box area) x (1 for an inner
+// child, its triangle count for a leaf), into *sum.
+__global__ void kSahSum(const uint4* __restrict__ nodes, uint32_t n, double* sum)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double   c = 0.0;
+    if (i < n)
+    {
+        const uint4* np = nodes + size_t(i) * 5;
+        uint4        n0 = np[0], n1 = np[1], n2 = np[2], n3 = np[3], n4 = np[4];
+        float        px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+        float        ex = __uint_as_float((n0.w & 0xffu) << 23), ey = __uint_as_float(((n0.w >> 8) & 0xffu) << 23),
+              ez = __uint_as_float(((n0.w >> 16) & 0xffu) << 23);
+        uint32_t imask = n0.w >> 24;
+        for (int s = 0; s < 8; ++s)
+        {
+            int      w = s >> 2, sh = 8 * (s & 3);
+            uint32_t lx = ((w ? n2.y : n2.x) >> sh) & 0xffu, ly = ((w ? n2.w : n2.z) >> sh) & 0xffu,
+                     lz = ((w ? n3.y : n3.x) >> sh) & 0xffu;
+            uint32_t hx = ((w ? n3.w : n3.z) >> sh) & 0xffu, hy = ((w ? n4.y : n4.x) >> sh) & 0xffu,
+                     hz = ((w ? n4.w : n4.z) >> sh) & 0xffu;
+            if (lx > hx) continue; // empty slot
+            double weight;
+            if (imask & (1u << s))
+                weight = 1.0;
+            else
+            {
+                uint32_t m = ((w ? n1.w : n1.z) >> sh) & 0xffu;
+                weight     = double(__popc(m >> 5));
+            }
+            c += weight * boxArea(px + ex * float(lx), py + ey * float(ly), pz + ez * float(lz), px + ex * float(hx),
+                                  py + ey * float(hy), pz + ez * float(hz));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c != 0.0) atomicAdd(sum, c);
+}
+
+__global__ void kGatherTri9(const float4* __restrict__ vtx, const uint4* __restrict__ triIdx, uint32_t n,
+                            float* __restrict__ tri9)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint4 ix = triIdx[i];
+    float4 a = vtx[3 * size_t(ix.x)], b = vtx[3 * size_t(ix.y)], c = vtx[3 * size_t(ix.z)];
+    float* o = tri9 + 9 * size_t(i);
+    o[0] = a.x; o[1] = a.y; o[2] = a.z;
+    o[3] = b.x; o[4] = b.y; o[5] = b.z;
+    o[6] = c.x; o[7] = c.y; o[8] = c.z;
+}
+} // namespace
+
+cl_status refitWideBvh(WideBvh* bvh, const void* vtx, const void* triIdx, cudaStream_t st, std::string* err)
+{
+    if (!bvh->nodes.p || bvh->levels.size() < 2 || bvh->levels.back() != bvh->numNodes)
+    {
+        *err = "refit needs a built BVH";
+        return CL_ERR_STATE;
+    }
+    if (bvh->exact.bytes < size_t(bvh->numNodes) * 24) CL_TRY(bvh->exact.alloc(size_t(bvh->numNodes) * 24, err));
+    if (!bvh->scene.p) CL_TRY(bvh->scene.alloc(64, err));
+    uint32_t b0[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    CL_CUDA(cudaMemcpyAsync(bvh->scene.p, b0, sizeof(b0), cudaMemcpyHostToDevice, st), err);
+    uint32_t n = bvh->numTris;
+    kRefitTris<<<(n + 255) / 256, 256, 0, st>>>(bvh->tris.as<float4>(), n, static_cast<const float4*>(vtx),
+                                                 static_cast<const uint4*>(triIdx), bvh->scene.u());
+    CL_CUDA(cudaGetLastError(), err);
+    for (size_t d = bvh->levels.size() - 1; d-- > 0;)
+    {
+        uint32_t first = bvh->levels[d], count = bvh->levels[d + 1] - first;
+        kRefitLevel<<<(count + kRefitBlock - 1) / kRefitBlock, kRefitBlock, 0, st>>>(
+            bvh->nodes.as<uint4>(), bvh->tris.as<const float4>(), bvh->exact.f(), first, count, bvh->scene.u());
+        CL_CUDA(cudaGetLastError(), err);
+    }
+    return CL_OK;
+}
+
+cl_status wideBvhSahCost(const WideBvh& bvh, cudaStream_t st, double* cost, std::string* err)
+{
+    if (!bvh.nodes.p || bvh.numNodes == 0)
+    {
+        *err = "no BVH";
+        return CL_ERR_STATE;
+    }
+    DevBuf sum;
+    CL_TRY(sum.alloc(8, err));
+    CL_CUDA(cudaMemsetAsync(sum.p, 0, 8, st), err);
+    kSahSum<<<(bvh.numNodes + 255) / 256, 256, 0, st>>>(bvh.nodes.as<const uint4>(), bvh.numNodes, sum.as<double>());
+    CL_CUDA(cudaGetLastError(), err);
+    double                total = 0.0;
+    std::vector<uint32_t> h(20);
+    CL_CUDA(cudaMemcpyAsync(&total, sum.p, 8, cudaMemcpyDeviceToHost, st), err);
+    CL_CUDA(cudaMemcpyAsync(h.data(), bvh.nodes.p, 80, cudaMemcpyDeviceToHost, st), err);
+    CL_CUDA(cudaStreamSynchronize(st), err);
+    // Root box extent per axis: e * (largest qhi - smallest qlo) over the
+    // root's present slots (qlo words at h[8 + 2a + w], qhi at h[14 + 2a + w]).
+    double ext[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        uint32_t eb = ((h[3] >> (8 * a)) & 0xffu) << 23;
+        float    e;
+        memcpy(&e, &eb, 4);
+        uint32_t qlo = 255, qhi = 0;
+        for (int sl = 0; sl < 8; ++sl)
+        {
+            int      w = sl >> 2, sh = 8 * (sl & 3);
+            uint32_t lo = (h[8 + 2 * a + w] >> sh) & 0xffu, hi = (h[14 + 2 * a + w] >> sh) & 0xffu;
+            if (lo > hi) continue;
+            qlo = std::min(qlo, lo);
+            qhi = std::max(qhi, hi);
+        }
+        ext[a] = qhi >= qlo ? double(e) * double(qhi - qlo) : 0.0;
+    }
+    double rootArea = 2.0 * (ext[0] * ext[1] + ext[1] * ext[2] + ext[2] * ext[0]);
+    *cost           = rootArea > 0.0 ? 1.0 + total / rootArea : 0.0;
+    return CL_OK;
+}
+
+cl_status gatherTrianglePositions(const void* vtx, const void* triIdx, uint32_t n, float* tri9, cudaStream_t st,
+                                  std::string* err)
+{
+    kGatherTri9<<<(n + 255) / 256, 256, 0, st>>>(static_cast<const float4*>(vtx), static_cast<const uint4*>(triIdx),
+                                                  n, tri9);
+    CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }
 

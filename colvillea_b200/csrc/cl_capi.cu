@@ -150,6 +150,21 @@ cl_status cl_build_instances(cl_integrator* it, const cl_instance_desc* instance
     return guarded([&](std::string* e) { return it->impl.buildInstances(instances, count, e); });
 }
 
+cl_status cl_update_mesh_vertices(cl_integrator* it, uint32_t mesh_id, const float* positions, const float* normals,
+                                  const float* tangents, uint32_t num_vertices, cl_bvh_update mode)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) {
+        return it->impl.updateMeshVertices(mesh_id, positions, normals, tangents, num_vertices, uint32_t(mode), e);
+    });
+}
+
+cl_status cl_get_bvh(cl_integrator* it, void* nodes, size_t node_bytes, void* triangles, size_t triangle_bytes)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.getBvh(nodes, node_bytes, triangles, triangle_bytes, e); });
+}
+
 cl_status cl_build_materials(cl_integrator* it, const cl_material_desc* materials, uint32_t count)
 {
     CL_NEED(it);

@@ -1155,6 +1155,66 @@ cl_status Integrator::buildMeshes(const cl_mesh_desc* meshes, uint32_t n, std::s
     return CL_OK;
 }
 
+// World-space vertices of one instance: 12 floats per vertex {p.xyz, n.xyz,
+// t.xyz, u, v, flags}; normals by the inverse transpose of the linear part.
+cl_status Integrator::flattenInstance(const HostMesh& m, const float* M, uint32_t i, float* out, std::string* err)
+{
+    bool ident = M[0] == 1 && M[1] == 0 && M[2] == 0 && M[3] == 0 && M[4] == 0 && M[5] == 1 && M[6] == 0 &&
+                 M[7] == 0 && M[8] == 0 && M[9] == 0 && M[10] == 1 && M[11] == 0;
+    double a = M[0], b = M[1], c = M[2], d = M[4], e = M[5], f = M[6], g = M[8], h = M[9], k = M[10];
+    double det = a * (e * k - f * h) - b * (d * k - f * g) + c * (d * h - e * g);
+    if (!ident && std::fabs(det) < 1e-30)
+    {
+        *err = "instance " + std::to_string(i) + ": singular transform";
+        return CL_ERR_INVALID_ARG;
+    }
+    double N9[9] = {(e * k - f * h) / det, -(d * k - f * g) / det, (d * h - e * g) / det,
+                    -(b * k - c * h) / det, (a * k - c * g) / det,  -(a * h - b * g) / det,
+                    (b * f - c * e) / det,  -(a * f - c * d) / det, (a * e - b * d) / det};
+    size_t   mv    = m.pos.size() / 3;
+    uint32_t flags = (m.hasN ? 1u : 0u) | (m.hasUV ? 2u : 0u);
+    for (size_t v = 0; v < mv; ++v)
+    {
+        float p[3], nn[3] = {0, 0, 0}, t[3], uv[2] = {0, 0};
+        for (int q = 0; q < 3; ++q)
+        {
+            p[q] = m.pos[3 * v + q];
+            t[q] = m.tan[3 * v + q];
+            if (m.hasN) nn[q] = m.nrm[3 * v + q];
+        }
+        if (m.hasUV)
+        {
+            uv[0] = m.uv[2 * v];
+            uv[1] = m.uv[2 * v + 1];
+        }
+        if (!ident)
+        {
+            float P2[3], T2[3], N2[3];
+            for (int r = 0; r < 3; ++r)
+            {
+                P2[r] = float(double(M[4 * r]) * p[0] + double(M[4 * r + 1]) * p[1] + double(M[4 * r + 2]) * p[2] +
+                              double(M[4 * r + 3]));
+                T2[r] = float(double(M[4 * r]) * t[0] + double(M[4 * r + 1]) * t[1] + double(M[4 * r + 2]) * t[2]);
+                // n' = N^T n with N = inverse of the linear part: n'_r = sum_c Ninv[c][r] n_c
+                N2[r] = float(N9[3 * 0 + r] * nn[0] + N9[3 * 1 + r] * nn[1] + N9[3 * 2 + r] * nn[2]);
+            }
+            for (int q = 0; q < 3; ++q)
+            {
+                p[q]  = P2[q];
+                t[q]  = T2[q];
+                nn[q] = N2[q];
+            }
+        }
+        float* o = out + v * 12;
+        o[0] = p[0]; o[1] = p[1]; o[2] = p[2]; o[3] = nn[0];
+        o[4] = nn[1]; o[5] = nn[2]; o[6] = t[0]; o[7] = t[1];
+        float ff;
+        memcpy(&ff, &flags, 4);
+        o[8] = t[2]; o[9] = uv[0]; o[10] = uv[1]; o[11] = ff;
+    }
+    return CL_OK;
+}
+
 cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, std::string* err)
 {
     if ((!inst && n) || n == 0)
@@ -1183,66 +1243,14 @@ cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, s
     std::vector<float>    vtx(nv * 12);
     std::vector<uint32_t> tidx(nt * 4);
     std::vector<float>    tri9(nt * 9);
+    std::vector<uint32_t> vtxOff(n);
     size_t vo = 0, to = 0;
     for (uint32_t i = 0; i < n; ++i)
     {
         const HostMesh& m = meshes_[inst[i].mesh_id];
-        const float*    M = inst[i].transform;
-        bool ident = M[0] == 1 && M[1] == 0 && M[2] == 0 && M[3] == 0 && M[4] == 0 && M[5] == 1 && M[6] == 0 &&
-                     M[7] == 0 && M[8] == 0 && M[9] == 0 && M[10] == 1 && M[11] == 0;
-        // Normal matrix: inverse transpose of the linear part.
-        double a = M[0], b = M[1], c = M[2], d = M[4], e = M[5], f = M[6], g = M[8], h = M[9], k = M[10];
-        double det = a * (e * k - f * h) - b * (d * k - f * g) + c * (d * h - e * g);
-        if (!ident && std::fabs(det) < 1e-30)
-        {
-            *err = "instance " + std::to_string(i) + ": singular transform";
-            return CL_ERR_INVALID_ARG;
-        }
-        double N9[9] = {(e * k - f * h) / det, -(d * k - f * g) / det, (d * h - e * g) / det,
-                        -(b * k - c * h) / det, (a * k - c * g) / det,  -(a * h - b * g) / det,
-                        (b * f - c * e) / det,  -(a * f - c * d) / det, (a * e - b * d) / det};
+        CL_TRY(flattenInstance(m, inst[i].transform, i, &vtx[vo * 12], err));
+        vtxOff[i] = uint32_t(vo);
         size_t mv = m.pos.size() / 3;
-        uint32_t flags = (m.hasN ? 1u : 0u) | (m.hasUV ? 2u : 0u);
-        for (size_t v = 0; v < mv; ++v)
-        {
-            float p[3], nn[3] = {0, 0, 0}, t[3], uv[2] = {0, 0};
-            for (int q = 0; q < 3; ++q)
-            {
-                p[q] = m.pos[3 * v + q];
-                t[q] = m.tan[3 * v + q];
-                if (m.hasN) nn[q] = m.nrm[3 * v + q];
-            }
-            if (m.hasUV)
-            {
-                uv[0] = m.uv[2 * v];
-                uv[1] = m.uv[2 * v + 1];
-            }
-            if (!ident)
-            {
-                float P2[3], T2[3], N2[3];
-                for (int r = 0; r < 3; ++r)
-                {
-                    P2[r] = float(double(M[4 * r]) * p[0] + double(M[4 * r + 1]) * p[1] + double(M[4 * r + 2]) * p[2] +
-                                  double(M[4 * r + 3]));
-                    T2[r] = float(double(M[4 * r]) * t[0] + double(M[4 * r + 1]) * t[1] + double(M[4 * r + 2]) * t[2]);
-                    // n' = N^T n with N = inverse of the linear part: n'_r = sum_c Ninv[c][r] n_c
-                    N2[r] = float(N9[3 * 0 + r] * nn[0] + N9[3 * 1 + r] * nn[1] + N9[3 * 2 + r] * nn[2]);
-                }
-                for (int q = 0; q < 3; ++q)
-                {
-                    p[q]  = P2[q];
-                    t[q]  = T2[q];
-                    nn[q] = N2[q];
-                }
-            }
-            float* o = &vtx[(vo + v) * 12];
-            o[0] = p[0]; o[1] = p[1]; o[2] = p[2]; o[3] = nn[0];
-            o[4] = nn[1]; o[5] = nn[2]; o[6] = t[0]; o[7] = t[1];
-            uint32_t fb = flags;
-            float    ff;
-            memcpy(&ff, &fb, 4);
-            o[8] = t[2]; o[9] = uv[0]; o[10] = uv[1]; o[11] = ff;
-        }
         size_t mt = m.idx.size() / 3;
         for (size_t t = 0; t < mt; ++t)
         {
@@ -1284,13 +1292,102 @@ cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, s
     CL_CUDA(cudaEventSynchronize(evB_), err);
     CL_CUDA(cudaEventElapsedTime(&msBvh_, evA_, evB_), err);
     triPos_.release();
+    CL_TRY(wideBvhSahCost(bvh_, stream_, &sahBuild_, err));
+    sah_        = sahBuild_;
     numTris_    = uint32_t(nt);
     sceneBuilt_ = true;
     graphValid_ = false;
+    inst_.assign(inst, inst + n);
+    instVtxOff_.swap(vtxOff);
     // Material indices are checked at render time against the material count.
     maxMaterialIndex_ = 0;
     for (uint32_t i = 0; i < n; ++i) maxMaterialIndex_ = std::max(maxMaterialIndex_, inst[i].material_index);
     return CL_OK;
+}
+
+cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, const float* nrm, const float* tan,
+                                         uint32_t count, uint32_t mode, std::string* err)
+{
+    if (!sceneBuilt_)
+    {
+        *err = "no scene: build meshes and instances first";
+        return CL_ERR_STATE;
+    }
+    if (meshId >= meshes_.size())
+    {
+        *err = "mesh_id out of range";
+        return CL_ERR_INVALID_ARG;
+    }
+    HostMesh& m = meshes_[meshId];
+    if (!pos || size_t(count) * 3 != m.pos.size())
+    {
+        *err = "positions are required, with the mesh's vertex count (" + std::to_string(m.pos.size() / 3) + ")";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (mode > CL_BVH_UPDATE_REBUILD)
+    {
+        *err = "unknown BVH update mode";
+        return CL_ERR_INVALID_ARG;
+    }
+    for (size_t i = 0; i < size_t(count) * 3; ++i)
+        if (!std::isfinite(pos[i]))
+        {
+            *err = "vertex " + std::to_string(i / 3) + ": position is not finite";
+            return CL_ERR_INVALID_ARG;
+        }
+    m.pos.assign(pos, pos + size_t(count) * 3);
+    if (nrm)
+    {
+        m.nrm.assign(nrm, nrm + size_t(count) * 3);
+        m.hasN = true;
+    }
+    if (tan) m.tan.assign(tan, tan + size_t(count) * 3);
+
+    // Re-flatten the instances of this mesh into their vertex ranges.
+    std::vector<float> buf;
+    for (size_t i = 0; i < inst_.size(); ++i)
+    {
+        if (inst_[i].mesh_id != meshId) continue;
+        buf.resize(size_t(count) * 12);
+        CL_TRY(flattenInstance(m, inst_[i].transform, uint32_t(i), buf.data(), err));
+        CL_CUDA(cudaMemcpyAsync(vtx_.f() + size_t(instVtxOff_[i]) * 12, buf.data(), buf.size() * 4,
+                                cudaMemcpyHostToDevice, stream_),
+                err);
+    }
+
+    CL_CUDA(cudaEventRecord(evA_, stream_), err);
+    bool rebuild = mode == CL_BVH_UPDATE_REBUILD;
+    if (!rebuild)
+    {
+        CL_TRY(refitWideBvh(&bvh_, vtx_.p, triIdx_.p, stream_, err));
+        CL_TRY(wideBvhSahCost(bvh_, stream_, &sah_, err));
+        ++refits_;
+        // A refit keeps the topology: once the moved geometry has made the
+        // tree much costlier than a fresh build, rebuild.
+        rebuild = mode == CL_BVH_UPDATE_AUTO && sah_ > kRefitSahLimit * sahBuild_;
+    }
+    if (rebuild)
+    {
+        CL_TRY(triPos_.alloc(size_t(numTris_) * 36, err));
+        CL_TRY(gatherTrianglePositions(vtx_.p, triIdx_.p, numTris_, triPos_.f(), stream_, err));
+        cl_status st = buildWideBvh(triPos_.f(), numTris_, stream_, &bvh_, err);
+        triPos_.release();
+        if (st != CL_OK)
+        {
+            sceneBuilt_ = false;
+            return st;
+        }
+        CL_TRY(wideBvhSahCost(bvh_, stream_, &sahBuild_, err));
+        sah_        = sahBuild_;
+        graphValid_ = false; // new node and triangle buffers
+        ++rebuilds_;
+    }
+    CL_CUDA(cudaEventRecord(evB_, stream_), err);
+    CL_CUDA(cudaEventSynchronize(evB_), err);
+    CL_CUDA(cudaEventElapsedTime(&msBvhUpdate_, evA_, evB_), err);
+    // RenderEngine::compileAccelStructs (renderengine.cpp:65-77): a shape
+    // edit restarts progressive accumulation.
+    return resetIteration(err);
 }
 
 cl_status Integrator::buildMaterials(const cl_material_desc* m, uint32_t n, std::string* err)
@@ -2055,6 +2152,30 @@ void Integrator::stats(cl_stats* s) const
     s->shadow_tris    = lastTrisS_;
     s->last_rays_closest = lastRaysC_;
     s->last_rays_shadow  = lastRaysS_;
+    s->ms_bvh_update     = msBvhUpdate_;
+    s->bvh_refits        = refits_;
+    s->bvh_rebuilds      = rebuilds_;
+    s->bvh_sah           = sah_;
+    s->bvh_sah_build     = sahBuild_;
+}
+
+cl_status Integrator::getBvh(void* nodes, size_t nodeBytes, void* tris, size_t triBytes, std::string* err)
+{
+    if (!sceneBuilt_)
+    {
+        *err = "no scene";
+        return CL_ERR_STATE;
+    }
+    size_t nb = size_t(bvh_.numNodes) * 80, tb = size_t(bvh_.numTris) * 48;
+    if ((nodes && nodeBytes < nb) || (tris && triBytes < tb))
+    {
+        *err = "buffer too small: nodes need " + std::to_string(nb) + " bytes, triangles " + std::to_string(tb);
+        return CL_ERR_INVALID_ARG;
+    }
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    if (nodes) CL_CUDA(cudaMemcpy(nodes, bvh_.nodes.p, nb, cudaMemcpyDeviceToHost), err);
+    if (tris) CL_CUDA(cudaMemcpy(tris, bvh_.tris.p, tb, cudaMemcpyDeviceToHost), err);
+    return CL_OK;
 }
 
 cl_status Integrator::traceRays(const float* rays, uint32_t n, float* t, uint32_t* prim, float* b1, float* b2,

@@ -148,6 +148,8 @@ public:
 
     cl_status buildMeshes(const cl_mesh_desc* meshes, uint32_t n, std::string* err);
     cl_status buildInstances(const cl_instance_desc* inst, uint32_t n, std::string* err);
+    cl_status updateMeshVertices(uint32_t meshId, const float* pos, const float* nrm, const float* tan, uint32_t count,
+                                 uint32_t mode, std::string* err);
     cl_status buildMaterials(const cl_material_desc* m, uint32_t n, std::string* err);
     cl_status buildEmitters(const cl_emitter_desc* e, uint32_t n, std::string* err);
     cl_status updateCamera(const cl_camera* c, std::string* err);
@@ -158,6 +160,7 @@ public:
     cl_status resetIteration(std::string* err);
     cl_status setIteration(uint32_t iteration, std::string* err);
     void      stats(cl_stats* s) const;
+    cl_status getBvh(void* nodes, size_t nodeBytes, void* tris, size_t triBytes, std::string* err);
     cl_status traceRays(const float* rays, uint32_t n, float* t, uint32_t* prim, float* b1, float* b2,
                         std::string* err);
     cl_status occludedRays(const float* rays, uint32_t n, uint8_t* occ, std::string* err);
@@ -204,6 +207,15 @@ private:
         bool                  hasN = false, hasUV = false;
     };
     std::vector<HostMesh> meshes_;
+    cl_status flattenInstance(const HostMesh& m, const float* M, uint32_t i, float* out, std::string* err);
+    std::vector<cl_instance_desc> inst_;       // as built
+    std::vector<uint32_t>         instVtxOff_; // first flattened vertex of each instance
+    // Refit policy (CL_BVH_UPDATE_AUTO): rebuild when the refitted tree's
+    // surface-area cost exceeds this multiple of the cost after its build.
+    static constexpr double kRefitSahLimit = 1.5;
+    double   sahBuild_ = 0.0, sah_ = 0.0;
+    uint32_t refits_ = 0, rebuilds_ = 0;
+    float    msBvhUpdate_ = 0.0f;
 
     // Device scene.
     DevBuf   triIdx_, vtx_, mats_, triPos_;

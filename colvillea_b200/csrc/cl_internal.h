@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 namespace clb
 {
@@ -71,17 +72,43 @@ struct WideBvh
 {
     DevBuf   nodes; // 5 uint4 per node
     DevBuf   tris;  // 3 float4 per triangle, leaf order
+    DevBuf   exact; // refit: 6 floats per node, the unquantised box of its triangles
+    DevBuf   scene; // refit: scene bounds (6 ordered ints) and the SAH sum (double)
+    // Nodes of tree level d are [levels[d], levels[d + 1]): the collapse
+    // allocates each level's nodes in one launch.
+    std::vector<uint32_t> levels;
     uint32_t numNodes = 0, depth = 0, numTris = 0, buildIterations = 0;
     void     release()
     {
         nodes.release();
         tris.release();
+        exact.release();
+        scene.release();
+        levels.clear();
         numNodes = depth = numTris = 0;
     }
 };
 
 // dTri9: 9 floats per triangle (world-space vertices), device memory.
 cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err);
+
+// Refit after the vertices moved (same triangles, same vertex indices):
+// rewrites the leaf triangles from vtx (3 float4 per vertex, position in the
+// first) and triIdx (uint4 per triangle), then recomputes every node's child
+// boxes level by level from the deepest, keeping the tree's topology and
+// slot order.  Without moved vertices the nodes come out bit-identical to the
+// build's.  Asynchronous on st.
+cl_status refitWideBvh(WideBvh* bvh, const void* vtx, const void* triIdx, cudaStream_t st, std::string* err);
+
+// Surface-area cost of the built tree: sum over child slots of the slot's
+// quantised box area, times the triangle count for leaf slots, over the root
+// box area (one unit per node visit and per triangle test).  Synchronises st.
+cl_status wideBvhSahCost(const WideBvh& bvh, cudaStream_t st, double* cost, std::string* err);
+
+// Triangle positions (9 floats each, triangle order) gathered from vtx and
+// triIdx, the input of buildWideBvh.  Asynchronous on st.
+cl_status gatherTrianglePositions(const void* vtx, const void* triIdx, uint32_t n, float* tri9, cudaStream_t st,
+                                  std::string* err);
 
 // Thread-local last error message (cl_last_error).
 void setLastError(const std::string& msg);

@@ -181,6 +181,12 @@ typedef struct
     uint64_t shadow_tris;    /* ... shadow-ray triangles tested */
     uint64_t last_rays_closest; /* last render: closest-hit segments */
     uint64_t last_rays_shadow;  /* last render: shadow rays */
+    float    ms_bvh_update;     /* last cl_update_mesh_vertices: refit and/or rebuild */
+    uint32_t bvh_refits;        /* refits since the integrator was created */
+    uint32_t bvh_rebuilds;      /* rebuilds after vertex updates */
+    uint32_t pad2;
+    double   bvh_sah;           /* surface-area cost of the current tree (root = 1) */
+    double   bvh_sah_build;     /* ... right after its last full build */
 } cl_stats;
 
 typedef struct cl_integrator cl_integrator;
@@ -195,6 +201,37 @@ cl_status cl_build_meshes(cl_integrator* integrator, const cl_mesh_desc* meshes,
 /* Integrator::buildTLAS + buildGeometryEntities (integrator.h:49-54): builds the
  * 8-wide BVH on the device over all instances. */
 cl_status cl_build_instances(cl_integrator* integrator, const cl_instance_desc* instances, uint32_t count);
+/* Shape edit: new vertex positions (and optionally normals and tangents) for
+ * mesh `mesh_id` of the last cl_build_meshes, same vertex count, same
+ * triangles.  The reference's TriangleMesh::updateVertices
+ * (include/colvillea/nodes/shapes/trianglemesh.h:111-118, marks ShapeEdited)
+ * followed by RenderEngine::compileAccelStructs
+ * (src/core/librender/renderengine.cpp:65-77), which rebuilds the BLAS and
+ * calls resetIterationIndex.  Every instance of the mesh is re-flattened
+ * with its transform; then the BVH is
+ *   CL_BVH_UPDATE_REFIT    refitted: same tree, boxes recomputed bottom-up
+ *                          on the device (exact boxes, requantised);
+ *   CL_BVH_UPDATE_REBUILD  rebuilt from scratch, as the reference does;
+ *   CL_BVH_UPDATE_AUTO     refitted, then rebuilt if the refitted tree's
+ *                          surface-area cost exceeds 1.5x the cost right
+ *                          after its last build (cl_stats.bvh_sah*).
+ * The progressive iteration restarts (film cleared).  Positions must be
+ * finite.  Normals/tangents null: kept. */
+typedef enum
+{
+    CL_BVH_UPDATE_AUTO    = 0,
+    CL_BVH_UPDATE_REFIT   = 1,
+    CL_BVH_UPDATE_REBUILD = 2
+} cl_bvh_update;
+cl_status cl_update_mesh_vertices(cl_integrator* integrator, uint32_t mesh_id, const float* positions,
+                                  const float* normals, const float* tangents, uint32_t num_vertices,
+                                  cl_bvh_update mode);
+/* The built 8-wide BVH for inspection: nodes (bvh_nodes * 80 bytes, layout
+ * of cl_bvh.cuh: 5 x uint4 per node) and leaf triangles (triangles * 48
+ * bytes: 3 float4 each, {v0.xyz, prim id bits} {v1.xyz, 0} {v2.xyz, 0}).
+ * Either pointer may be null.  No counterpart in the reference. */
+cl_status cl_get_bvh(cl_integrator* integrator, void* nodes, size_t node_bytes, void* triangles,
+                     size_t triangle_bytes);
 /* Integrator::buildMaterials (integrator.h:52). */
 cl_status cl_build_materials(cl_integrator* integrator, const cl_material_desc* materials, uint32_t count);
 /* Integrator::buildEmitters (integrator.h:56-58): the last dome in the list is
