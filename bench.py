@@ -47,6 +47,7 @@ def parse():
                     help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
     ap.add_argument("--no-relmse", action="store_true", help="skip the guided-vs-plain equal-time relMSE")
+    ap.add_argument("--no-edit", action="store_true", help="skip the shape-edit (refit vs rebuild) measurement")
     ap.add_argument("--profile-nets", choices=["guide", "cache"], default=None,
                     help="short workload for ncu: cfg3 with guiding or cfg4 with the radiance cache, "
                          "2 training spp + 2 spp")
@@ -268,6 +269,31 @@ def guided_relmse(args):
     return out
 
 
+def scene_edit(it, s, args, spp=4):
+    """Shape edit of the largest mesh (the terrain): a smooth height change
+    of up to 0.5 units, then the BVH refitted or rebuilt; device times and
+    the render time of `spp` samples on each tree."""
+    import numpy as np
+    m = max(range(len(s.meshes)), key=lambda i: len(s.meshes[i].indices))
+    p = s.meshes[m].positions.copy()
+    p[:, 1] += 0.5 * np.sin(p[:, 0] * 0.7) * np.cos(p[:, 2] * 0.5)
+    st0 = it.stats()
+    out = {"mesh_triangles": int(len(s.meshes[m].indices)), "triangles": st0["triangles"],
+           "sah_before_edit": round(st0["bvh_sah_build"], 3)}
+    for mode in ("refit", "rebuild"):
+        it.updateVertices(m, p, bvh=mode)
+        st = it.stats()
+        it.render(1)  # graph re-capture after a rebuild
+        ms = 0.0
+        for _ in range(spp):
+            it.render(1)
+            ms += it.stats()["ms_last_render"]
+        out[mode] = {"bvh_ms": round(st["ms_bvh_update"], 3), "sah": round(st["bvh_sah"], 3),
+                     "render_ms_per_spp": round(ms / spp, 3)}
+    out["speedup_refit_vs_rebuild"] = round(out["rebuild"]["bvh_ms"] / max(out["refit"]["bvh_ms"], 1e-6), 1)
+    return out
+
+
 def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
@@ -387,6 +413,7 @@ def main():
         e2e = {"value": round(W * H * args.steps * dist.world / (ems * 1e-3) / 1e6, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(cam.nbytes), "d2h_bytes_per_step": int(arr.nbytes),
                "ms_per_step": round(ems / args.steps, 3)}
+    edit = scene_edit(it, s, args) if dist.world == 1 and not args.no_edit else None
     it.close()
 
     if dist.rank != 0:
@@ -423,6 +450,8 @@ def main():
     }
     if e2e:
         line["e2e"] = e2e
+    if edit:
+        line["scene_edit"] = edit
     if dist.world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(s, args.cpu_seconds, os.cpu_count() or 1)
     if dist.world == 1 and not args.no_relmse:

@@ -113,11 +113,25 @@ class Integrator:
         return nodes, tris
 
     def buildMaterials(self, materials):
+        """scenes.Material list; texture fields are 1-based indices into the
+        last buildTextures list (0 = none)."""
         descs = (N.MaterialDesc * len(materials))()
         for i, m in enumerate(materials):
             descs[i] = N.MaterialDesc(m.type, (ctypes.c_float * 3)(*m.reflectance), m.roughness, m.interior_ior,
-                                      (ctypes.c_float * 3)(*m.eta), (ctypes.c_float * 3)(*m.k))
+                                      (ctypes.c_float * 3)(*m.eta), (ctypes.c_float * 3)(*m.k),
+                                      getattr(m, "reflectance_texture", 0), getattr(m, "roughness_texture", 0),
+                                      getattr(m, "normal_texture", 0))
         N.call("cl_build_materials", self._h, descs, len(materials))
+
+    def buildTextures(self, textures):
+        """scenes.Texture list (image textures: bilinear, wrap, sRGB decode for
+        sRGB RGBA8)."""
+        keep, descs = [], (N.TextureDesc * max(1, len(textures)))()
+        for i, t in enumerate(textures):
+            d, keep_arr = texture_desc(t)
+            keep.append(keep_arr)
+            descs[i] = d
+        N.call("cl_build_textures", self._h, descs, len(textures))
 
     def buildEmitters(self, emitters):
         keep, descs = [], (N.EmitterDesc * len(emitters))()
@@ -436,6 +450,32 @@ Integrator.guideStats = _guide_stats
 
 
 # --- scene ingestion and film output (MeshImporter / ImageUtils, src/delegate) ---
+def texture_desc(t):
+    """(TextureDesc, array to keep alive) for a scenes.Texture."""
+    a = np.ascontiguousarray(t.texels)
+    if a.ndim != 3 or a.shape[2] != 4 or a.dtype not in (np.uint8, np.float32):
+        raise ValueError("texture texels must be (h, w, 4) uint8 or float32")
+    fmt = N.CL_TEXTURE_RGBA8 if a.dtype == np.uint8 else N.CL_TEXTURE_RGBA32F
+    return N.TextureDesc(fmt, a.shape[1], a.shape[0], int(bool(t.srgb)), _ptr(a)), a
+
+
+def texture_lookup(t, uv):
+    """RGBA lookups in one texture, set up like the integrator's (texture unit)."""
+    d, a = texture_desc(t)
+    uv = _f32(uv).reshape(-1, 2)
+    out = np.zeros((len(uv), 4), np.float32)
+    N.call("cl_unit_texture_lookup", ctypes.byref(d), _ptr(uv), _ptr(out), len(uv))
+    return out
+
+
+def normal_frame(inputs16):
+    """cl_unit_normal_frame: (n, 16) {wo, dpdu, dpdv, base normal, texel rgb, pull-up} -> (n, 3, 3) {s, t, n}."""
+    x = _f32(inputs16).reshape(-1, 16)
+    out = np.zeros((len(x), 9), np.float32)
+    N.call("cl_unit_normal_frame", _ptr(x), _ptr(out), len(x))
+    return out.reshape(-1, 3, 3)
+
+
 def load_obj(path):
     """Meshes of a Wavefront OBJ file (one per o/g/usemtl group) as
     scenes.Mesh: triangulated, unified vertices, normals (smooth where the
@@ -503,6 +543,8 @@ def load_scene(scene, itype=IntegratorType.WavefrontPathTracing, flags=COMPAT_AL
     cfg = RenderConfig(scene.max_depth if max_depth is None else max_depth,
                        scene.rr_start if rr_start is None else rr_start, flags, path_slots)
     it = Integrator.createIntegrator(itype, scene.width, scene.height, cfg)
+    if getattr(scene, "textures", None):
+        it.buildTextures(scene.textures)
     it.buildMaterials(scene.materials)
     it.buildBLAS(scene.meshes)
     it.buildTLAS(scene.instances)

@@ -46,7 +46,15 @@ class InstanceDesc(ctypes.Structure):
 
 class MaterialDesc(ctypes.Structure):
     _fields_ = [("type", u32), ("reflectance", ctypes.c_float * 3), ("roughness", ctypes.c_float),
-                ("interior_ior", ctypes.c_float), ("eta", ctypes.c_float * 3), ("k", ctypes.c_float * 3)]
+                ("interior_ior", ctypes.c_float), ("eta", ctypes.c_float * 3), ("k", ctypes.c_float * 3),
+                ("reflectance_texture", u32), ("roughness_texture", u32), ("normal_texture", u32)]
+
+
+CL_TEXTURE_RGBA8, CL_TEXTURE_RGBA32F = 0, 1
+
+
+class TextureDesc(ctypes.Structure):
+    _fields_ = [("format", u32), ("width", u32), ("height", u32), ("srgb", u32), ("texels", vp)]
 
 
 class EmitterDesc(ctypes.Structure):
@@ -67,7 +75,8 @@ class Stats(ctypes.Structure):
                 ("ms_shadow", ctypes.c_float), ("launches", u32), ("pad", u32), ("trace_nodes", ctypes.c_uint64),
                 ("trace_tris", ctypes.c_uint64), ("shadow_nodes", ctypes.c_uint64), ("shadow_tris", ctypes.c_uint64),
                 ("last_rays_closest", ctypes.c_uint64), ("last_rays_shadow", ctypes.c_uint64),
-                ("ms_bvh_update", ctypes.c_float), ("bvh_refits", u32), ("bvh_rebuilds", u32), ("pad2", u32),
+                ("ms_bvh_update", ctypes.c_float), ("ms_bvh_refit", ctypes.c_float), ("bvh_refits", u32),
+                ("bvh_rebuilds", u32),
                 ("bvh_sah", ctypes.c_double), ("bvh_sah_build", ctypes.c_double)]
 
     def as_dict(self):
@@ -104,6 +113,9 @@ _SIGS = {
     "cl_update_mesh_vertices": [vp, u32, vp, vp, vp, u32, u32],
     "cl_get_bvh": [vp, vp, ctypes.c_size_t, vp, ctypes.c_size_t],
     "cl_build_materials": [vp, ctypes.POINTER(MaterialDesc), u32],
+    "cl_build_textures": [vp, ctypes.POINTER(TextureDesc), u32],
+    "cl_unit_normal_frame": [vp, vp, u32],
+    "cl_unit_texture_lookup": [ctypes.POINTER(TextureDesc), vp, vp, u32],
     "cl_build_emitters": [vp, ctypes.POINTER(EmitterDesc), u32],
     "cl_update_camera": [vp, ctypes.POINTER(Camera)],
     "cl_render": [vp, u32],

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libcolvillea_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["cl_units.cu", "cl_bvh_build.cu", "cl_dome.cu", "cl_guide.cu", "cl_integrator.cu", "cl_capi.cu", "cl_io.cpp"]
+SOURCES = ["cl_units.cu", "cl_texture.cu", "cl_bvh_build.cu", "cl_dome.cu", "cl_guide.cu", "cl_integrator.cu", "cl_capi.cu", "cl_io.cpp"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

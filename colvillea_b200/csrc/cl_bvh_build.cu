@@ -1101,21 +1101,21 @@ cl_status refitWideBvh(WideBvh* bvh, const void* vtx, const void* triIdx, cudaSt
     return CL_OK;
 }
 
-cl_status wideBvhSahCost(const WideBvh& bvh, cudaStream_t st, double* cost, std::string* err)
+cl_status wideBvhSahCost(WideBvh& bvh, cudaStream_t st, double* cost, std::string* err)
 {
     if (!bvh.nodes.p || bvh.numNodes == 0)
     {
         *err = "no BVH";
         return CL_ERR_STATE;
     }
-    DevBuf sum;
-    CL_TRY(sum.alloc(8, err));
-    CL_CUDA(cudaMemsetAsync(sum.p, 0, 8, st), err);
-    kSahSum<<<(bvh.numNodes + 255) / 256, 256, 0, st>>>(bvh.nodes.as<const uint4>(), bvh.numNodes, sum.as<double>());
+    if (!bvh.scene.p) CL_TRY(bvh.scene.alloc(64, err));
+    double* sum = reinterpret_cast<double*>(bvh.scene.as<char>() + 32);
+    CL_CUDA(cudaMemsetAsync(sum, 0, 8, st), err);
+    kSahSum<<<(bvh.numNodes + 255) / 256, 256, 0, st>>>(bvh.nodes.as<const uint4>(), bvh.numNodes, sum);
     CL_CUDA(cudaGetLastError(), err);
     double                total = 0.0;
     std::vector<uint32_t> h(20);
-    CL_CUDA(cudaMemcpyAsync(&total, sum.p, 8, cudaMemcpyDeviceToHost, st), err);
+    CL_CUDA(cudaMemcpyAsync(&total, sum, 8, cudaMemcpyDeviceToHost, st), err);
     CL_CUDA(cudaMemcpyAsync(h.data(), bvh.nodes.p, 80, cudaMemcpyDeviceToHost, st), err);
     CL_CUDA(cudaStreamSynchronize(st), err);
     // Root box extent per axis: e * (largest qhi - smallest qlo) over the

@@ -61,6 +61,8 @@ cl_status unitWarp(const float*, float*, float*, uint32_t, std::string*);
 cl_status unitMakeFrame(const float*, float*, float*, uint32_t, std::string*);
 cl_status unitFrame(const float*, const float*, const float*, const float*, float*, float*, uint32_t, std::string*);
 cl_status unitPcg(const uint32_t*, uint32_t*, uint32_t, std::string*);
+cl_status unitNormalFrame(const float*, float*, uint32_t, std::string*);
+cl_status unitTextureLookup(const cl_texture_desc*, const float*, float*, uint32_t, std::string*);
 cl_status unitSeq(const uint32_t*, uint32_t, uint32_t, float*, std::string*);
 cl_status unitDomeSample(const float*, uint32_t, uint32_t, const float*, const float*, const float*, const float*,
                          const float*, float*, float*, float*, uint32_t, std::string*);
@@ -163,6 +165,12 @@ cl_status cl_get_bvh(cl_integrator* it, void* nodes, size_t node_bytes, void* tr
 {
     CL_NEED(it);
     return guarded([&](std::string* e) { return it->impl.getBvh(nodes, node_bytes, triangles, triangle_bytes, e); });
+}
+
+cl_status cl_build_textures(cl_integrator* it, const cl_texture_desc* textures, uint32_t count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.buildTextures(textures, count, e); });
 }
 
 cl_status cl_build_materials(cl_integrator* it, const cl_material_desc* materials, uint32_t count)
@@ -336,6 +344,16 @@ cl_status cl_unit_frame(const float* s, const float* t, const float* n, const fl
                         uint32_t count)
 {
     return guarded([&](std::string* e) { return clb::unitFrame(s, t, n, v, local, world, count, e); });
+}
+
+cl_status cl_unit_normal_frame(const float* in, float* frame, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitNormalFrame(in, frame, count, e); });
+}
+
+cl_status cl_unit_texture_lookup(const cl_texture_desc* texture, const float* uv, float* rgba, uint32_t count)
+{
+    return guarded([&](std::string* e) { return clb::unitTextureLookup(texture, uv, rgba, count, e); });
 }
 
 cl_status cl_unit_pcg4d(const uint32_t* in, uint32_t* out, uint32_t count)

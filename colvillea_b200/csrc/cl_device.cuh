@@ -249,6 +249,66 @@ __device__ __forceinline__ f3 reflect(f3 wo, f3 n)
     float d = 2.0f * dot(wo, n);
     return {-wo.x + d * n.x, -wo.y + d * n.y, -wo.z + d * n.z};
 }
+// ---------------------------------------------------------------------------
+// Normal-mapped shading frame (Material::getShadingFrame,
+// libkernel/base/material.h:128-287).
+// ---------------------------------------------------------------------------
+constexpr float kUpliftEps = 1.1f; // float(kNormalmapAutoAdapationUpliftEpsilon()), config.h:9
+
+// fixNormalPerturbingShadingFrame (material.h:238-285): IRay's pull-up of a
+// perturbed normal whose mirror direction of wo falls below the surface.
+__device__ __forceinline__ void fixNormalPerturbing(f3 wo, Frame* fr, f3 ng)
+{
+    if (dot(wo, ng) < 0.0f)
+    {
+        fr->n = fr->n * -1.0f;
+        ng    = ng * -1.0f;
+    }
+    if (dot(wo, ng) > 0.0f)
+    {
+        f3 r = reflect(wo, fr->n);
+        if (dot(r, ng) <= 0.0f)
+        {
+            float a  = fabsf(dot(r, ng));
+            float b  = dot(fr->n, ng);
+            f3    up = (a / b) * fr->n;
+            up       = up * kUpliftEps;
+            fr->n    = normalize(normalize(r + up) + wo);
+            fr->t    = normalize(fr->t - dot(fr->t, fr->n) * fr->n);
+            fr->s    = normalize(cross(fr->n, fr->t));
+            if (dot(fr->n, ng) < 0.0f)
+            {
+                fr->n = fr->n * -1.0f;
+                fr->t = fr->t * -1.0f;
+            }
+        }
+    }
+}
+
+// getShadingFrameImpl with a normal-map texel (material.h:164-221): the
+// texel's rgb * 2 - 1, normalised, taken from the tangent frame
+// {dpdv, dpdu, nb} to world; dpdu re-orthogonalised; everything flipped to
+// nb's side.  pullUp: reflection-only materials (diffuse, metal) also get
+// fixNormalPerturbing against nb (material.h:136-146).
+__device__ __forceinline__ Frame normalMappedFrame(f3 wo, f3 dpdu, f3 dpdv, f3 nb, f3 texel, bool pullUp)
+{
+    f3 m = texel * 2.0f;
+    m    = {m.x - 1.0f, m.y - 1.0f, m.z - 1.0f};
+    m    = normalize(m);
+    m    = Frame{dpdv, dpdu, nb}.toWorld(m);
+    f3 du = dpdu - m * dot(dpdu, m);
+    du    = normalize(du);
+    f3 dv = normalize(cross(m, du));
+    if (dot(m, nb) < 0.0f)
+    {
+        m  = m * -1.0f;
+        du = du * -1.0f;
+    }
+    Frame fr{dv, du, m};
+    if (pullUp) fixNormalPerturbing(wo, &fr, nb);
+    return fr;
+}
+
 __device__ __forceinline__ f3 refract(f3 wi, f3 n, float eta, float cosThetaT)
 {
     if (cosThetaT < 0.0f) eta = 1.0f / eta;

@@ -59,9 +59,19 @@ __device__ __forceinline__ uint32_t warpFetch(uint32_t* counter)
 
 __device__ __forceinline__ uint32_t loadCount(const uint32_t* p) { return *(const volatile uint32_t*)p; }
 
-__device__ __forceinline__ Bsdf loadMaterial(const float4* mats, uint32_t m)
+// Texture slots of a material: 1-based texture indices, 0 = none.
+struct MatTex
 {
-    float4 a = __ldg(mats + 3 * m), b = __ldg(mats + 3 * m + 1), c = __ldg(mats + 3 * m + 2);
+    uint32_t refl, rough, normal;
+};
+
+__device__ __forceinline__ Bsdf loadMaterial(const float4* mats, uint32_t m, MatTex* tx)
+{
+    float4 a = __ldg(mats + kMatF4 * m), b = __ldg(mats + kMatF4 * m + 1), c = __ldg(mats + kMatF4 * m + 2);
+    uint4  d = __ldg(reinterpret_cast<const uint4*>(mats + kMatF4 * m + 3));
+    tx->refl   = d.x;
+    tx->rough  = d.y;
+    tx->normal = d.z;
     Bsdf   s;
     s.type   = __float_as_uint(a.x);
     s.r      = {a.y, a.z, a.w};
@@ -70,6 +80,28 @@ __device__ __forceinline__ Bsdf loadMaterial(const float4* mats, uint32_t m)
     s.eta    = {b.z, b.w, c.x};
     s.k      = {c.y, c.z, c.w};
     return s;
+}
+
+__device__ __forceinline__ float4 texLookup(const unsigned long long* tex, uint32_t oneBased, f2 uv)
+{
+    return tex2D<float4>(cudaTextureObject_t(__ldg(tex + (oneBased - 1u))), uv.x, uv.y);
+}
+
+// Material::getBSDF(uv) (material.h:93-108): a reflectance texture replaces
+// the constant reflectance (diffusemtl.h:22-27, metal.h:40-45); a roughness
+// texture's red channel replaces the roughness, squared to alpha (metal.h:47-52).
+__device__ __forceinline__ void applyTextures(const unsigned long long* tex, const MatTex& tx, f2 uv, Bsdf* b)
+{
+    if (tx.refl)
+    {
+        float4 c = texLookup(tex, tx.refl, uv);
+        b->r     = {c.x, c.y, c.z};
+    }
+    if (tx.rough)
+    {
+        float r  = texLookup(tex, tx.rough, uv).x;
+        b->alpha = r * r;
+    }
 }
 
 struct HitAttr
@@ -340,7 +372,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
             int cls = -1;
             if (i < n)
                 cls = prim == kMissPrim ? kClassEscaped
-                                        : int(__float_as_uint(__ldg(&cv.mats[3 * __ldg(&cv.triIdx[prim]).w].x)));
+                                        : int(__float_as_uint(__ldg(&cv.mats[kMatF4 * __ldg(&cv.triIdx[prim]).w].x)));
 #pragma unroll
             for (int c = 0; c < 4; ++c)
             {
@@ -473,7 +505,9 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             else
             {
                 HitAttr a    = hitAttributes(sc, prim, hh.z, hh.w);
-                Bsdf    bsdf = loadMaterial(sc.mats, a.material);
+                MatTex  tx;
+                Bsdf    bsdf = loadMaterial(sc.mats, a.material, &tx);
+                if (tx.refl | tx.rough) applyTextures(sc.tex, tx, a.uv, &bsdf);
                 if (!DL && (cst & kCacheTrainBit) && wp.cacheTrain && depth <= P.c.histDepth)
                 {
                     // Radiance-cache training path: vertex history (flushCacheRecords).
@@ -502,7 +536,21 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                     gf = 1.0f - (((w0.x + w0.y) + (w0.z + w0.w)) + ((w1.x + w1.y) + (w1.z + w1.w)));
                 }
                 f2    u      = rng.next2D();
-                Frame fr{a.dpdv, a.dpdu, (!DL && compatFrame) ? a.ng : a.ns};
+                // Shading frame (Material::getShadingFrame, material.h:128-147).
+                // Path tracing passes (ng, ns) swapped (raygeneration.cu:324-330):
+                // without a normal map the frame's normal is then the geometric
+                // one (the compat quirk); with one, the map's tangent frame and
+                // the pull-up use the shading normal, kept in both estimators.
+                // The reference's direct-lighting kernel builds {dpdv, dpdu, ns}
+                // itself and ignores normal maps (raygeneration.cu:179,237).
+                Frame fr;
+                if (tx.normal && !(DL && compatFrame))
+                {
+                    float4 nt = texLookup(sc.tex, tx.normal, a.uv);
+                    fr = normalMappedFrame(wo, a.dpdu, a.dpdv, a.ns, f3{nt.x, nt.y, nt.z}, bsdf.type != kDielectric);
+                }
+                else
+                    fr = Frame{a.dpdv, a.dpdu, (!DL && compatFrame) ? a.ng : a.ns};
                 // Emitter sampling with MIS (raygeneration.cu:332-384 / 174-227).
                 if (N > 0u)
                 {
@@ -1355,11 +1403,19 @@ cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, cons
                 err);
     }
 
-    CL_CUDA(cudaEventRecord(evA_, stream_), err);
-    bool rebuild = mode == CL_BVH_UPDATE_REBUILD;
+    // Device time of the refit and/or rebuild (the surface-area cost pass
+    // and the vertex upload are not included).
+    bool  rebuild = mode == CL_BVH_UPDATE_REBUILD;
+    float ms      = 0.0f;
+    msBvhRefit_   = 0.0f;
     if (!rebuild)
     {
+        CL_CUDA(cudaEventRecord(evA_, stream_), err);
         CL_TRY(refitWideBvh(&bvh_, vtx_.p, triIdx_.p, stream_, err));
+        CL_CUDA(cudaEventRecord(evB_, stream_), err);
+        CL_CUDA(cudaEventSynchronize(evB_), err);
+        CL_CUDA(cudaEventElapsedTime(&ms, evA_, evB_), err);
+        msBvhRefit_ = ms;
         CL_TRY(wideBvhSahCost(bvh_, stream_, &sah_, err));
         ++refits_;
         // A refit keeps the topology: once the moved geometry has made the
@@ -1368,6 +1424,8 @@ cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, cons
     }
     if (rebuild)
     {
+        float msBuild = 0.0f;
+        CL_CUDA(cudaEventRecord(evA_, stream_), err);
         CL_TRY(triPos_.alloc(size_t(numTris_) * 36, err));
         CL_TRY(gatherTrianglePositions(vtx_.p, triIdx_.p, numTris_, triPos_.f(), stream_, err));
         cl_status st = buildWideBvh(triPos_.f(), numTris_, stream_, &bvh_, err);
@@ -1377,14 +1435,17 @@ cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, cons
             sceneBuilt_ = false;
             return st;
         }
+        CL_CUDA(cudaEventRecord(evB_, stream_), err);
+        CL_CUDA(cudaEventSynchronize(evB_), err);
+        CL_CUDA(cudaEventElapsedTime(&msBuild, evA_, evB_), err);
+        ms += msBuild;
+        msBvh_ = msBuild;
         CL_TRY(wideBvhSahCost(bvh_, stream_, &sahBuild_, err));
         sah_        = sahBuild_;
         graphValid_ = false; // new node and triangle buffers
         ++rebuilds_;
     }
-    CL_CUDA(cudaEventRecord(evB_, stream_), err);
-    CL_CUDA(cudaEventSynchronize(evB_), err);
-    CL_CUDA(cudaEventElapsedTime(&msBvhUpdate_, evA_, evB_), err);
+    msBvhUpdate_ = ms;
     // RenderEngine::compileAccelStructs (renderengine.cpp:65-77): a shape
     // edit restarts progressive accumulation.
     return resetIteration(err);
@@ -1397,7 +1458,8 @@ cl_status Integrator::buildMaterials(const cl_material_desc* m, uint32_t n, std:
         *err = "at least one material is required";
         return CL_ERR_INVALID_ARG;
     }
-    std::vector<float> h(size_t(n) * 12);
+    std::vector<float> h(size_t(n) * 4 * kMatF4);
+    uint32_t           maxTex = 0;
     for (uint32_t i = 0; i < n; ++i)
     {
         const cl_material_desc& d = m[i];
@@ -1406,14 +1468,34 @@ cl_status Integrator::buildMaterials(const cl_material_desc* m, uint32_t n, std:
             *err = "material " + std::to_string(i) + ": unknown type";
             return CL_ERR_INVALID_ARG;
         }
+        // GlassMtl has no textures (glass.h:17-27); DiffuseMtl no roughness.
+        if ((d.type == CL_MATERIAL_GLASS && (d.reflectance_texture || d.roughness_texture)) ||
+            (d.type == CL_MATERIAL_DIFFUSE && d.roughness_texture))
+        {
+            *err = "material " + std::to_string(i) + ": this type takes no such texture";
+            return CL_ERR_INVALID_ARG;
+        }
+        uint32_t refs[3] = {d.reflectance_texture, d.roughness_texture, d.normal_texture};
+        for (uint32_t r : refs)
+        {
+            if (r > textures_.size())
+            {
+                *err = "material " + std::to_string(i) + ": texture " + std::to_string(r) + " (1-based) of " +
+                       std::to_string(textures_.size()) + " built";
+                return CL_ERR_INVALID_ARG;
+            }
+            maxTex = std::max(maxTex, r);
+        }
         if (d.type == CL_MATERIAL_GLASS && d.interior_ior == 1.0f)
         {
             *err = "material " + std::to_string(i) + ": glass IOR must differ from 1 (roughdielectric.h:28)";
             return CL_ERR_INVALID_ARG;
         }
-        float*   o = &h[size_t(i) * 12];
+        float*   o = &h[size_t(i) * 4 * kMatF4];
         uint32_t t = d.type;
         memcpy(&o[0], &t, 4);
+        memcpy(&o[12], refs, 12);
+        o[15] = 0.0f;
         o[1]  = d.reflectance[0];
         o[2]  = d.reflectance[1];
         o[3]  = d.reflectance[2];
@@ -1429,9 +1511,16 @@ cl_status Integrator::buildMaterials(const cl_material_desc* m, uint32_t n, std:
     CL_TRY(mats_.alloc(h.size() * 4, err));
     CL_CUDA(cudaMemcpyAsync(mats_.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaStreamSynchronize(stream_), err);
-    numMaterials_ = n;
-    graphValid_   = false;
+    numMaterials_  = n;
+    maxTextureRef_ = maxTex;
+    graphValid_    = false;
     return CL_OK;
+}
+
+cl_status Integrator::buildTextures(const cl_texture_desc* t, uint32_t n, std::string* err)
+{
+    graphValid_ = false;
+    return textures_.build(t, n, stream_, err);
 }
 
 cl_status Integrator::buildEmitters(const cl_emitter_desc* e, uint32_t n, std::string* err)
@@ -1569,6 +1658,7 @@ Params Integrator::params() const
     P.sc.triIdx    = triIdx_.as<const uint4>();
     P.sc.vtx       = vtx_.as<const float4>();
     P.sc.mats      = mats_.as<const float4>();
+    P.sc.tex       = textures_.device();
     P.sc.hasDome   = hasDome_ ? 1 : 0;
     if (hasDome_) P.sc.dome = dome_.view();
     P.sc.numEmitters = uint32_t(emitters_.size());
@@ -1707,6 +1797,12 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
         *err = "an instance references material " + std::to_string(maxMaterialIndex_) + " of " +
                std::to_string(numMaterials_);
         return CL_ERR_INVALID_ARG;
+    }
+    if (maxTextureRef_ > textures_.size())
+    {
+        *err = "a material references texture " + std::to_string(maxTextureRef_) + " (1-based) of " +
+               std::to_string(textures_.size());
+        return CL_ERR_STATE;
     }
     if (spp == 0) return CL_OK;
     CL_TRY(ensureFilm(err));
@@ -2153,6 +2249,7 @@ void Integrator::stats(cl_stats* s) const
     s->last_rays_closest = lastRaysC_;
     s->last_rays_shadow  = lastRaysS_;
     s->ms_bvh_update     = msBvhUpdate_;
+    s->ms_bvh_refit      = msBvhRefit_;
     s->bvh_refits        = refits_;
     s->bvh_rebuilds      = rebuilds_;
     s->bvh_sah           = sah_;

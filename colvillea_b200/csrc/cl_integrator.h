@@ -5,6 +5,7 @@
 #include "cl_dome.h"
 #include "cl_guide.h"
 #include "cl_internal.h"
+#include "cl_texture.h"
 
 #include <memory>
 #include <vector>
@@ -21,12 +22,16 @@ struct EmitterDev
     DirectionalLight dl;
 };
 
+constexpr uint32_t kMatF4 = 4; // material record: {type, r.xyz} {alpha, etaInt, eta.xy} {eta.z, k.xyz} {textures}
+
 struct SceneDev
 {
     BvhView bvh;
     const uint4* __restrict__ triIdx;  // per primitive: i0, i1, i2, material
     const float4* __restrict__ vtx;    // 3 per vertex: {p.xyz, n.x} {n.y, n.z, t.x, t.y} {t.z, u, v, flags}
-    const float4* __restrict__ mats;   // 3 per material: {type, r.xyz} {alpha, etaInt, eta.xy} {eta.z, k.xyz}
+    const float4* __restrict__ mats;   // kMatF4 per material; the last holds the 1-based texture indices
+                                       // {reflectance, roughness, normal map, 0} as uint bits
+    const unsigned long long* __restrict__ tex; // cudaTextureObject_t per texture
     DomeView   dome;
     int        hasDome;
     uint32_t   numEmitters;
@@ -151,6 +156,7 @@ public:
     cl_status updateMeshVertices(uint32_t meshId, const float* pos, const float* nrm, const float* tan, uint32_t count,
                                  uint32_t mode, std::string* err);
     cl_status buildMaterials(const cl_material_desc* m, uint32_t n, std::string* err);
+    cl_status buildTextures(const cl_texture_desc* t, uint32_t n, std::string* err);
     cl_status buildEmitters(const cl_emitter_desc* e, uint32_t n, std::string* err);
     cl_status updateCamera(const cl_camera* c, std::string* err);
     cl_status render(uint32_t spp, std::string* err);
@@ -215,7 +221,7 @@ private:
     static constexpr double kRefitSahLimit = 1.5;
     double   sahBuild_ = 0.0, sah_ = 0.0;
     uint32_t refits_ = 0, rebuilds_ = 0;
-    float    msBvhUpdate_ = 0.0f;
+    float    msBvhUpdate_ = 0.0f, msBvhRefit_ = 0.0f;
 
     // Device scene.
     DevBuf   triIdx_, vtx_, mats_, triPos_;
@@ -226,6 +232,8 @@ private:
     uint32_t numMaterials_ = 0;
     uint32_t numTris_      = 0;
     uint32_t maxMaterialIndex_ = 0;
+    TextureSet textures_;
+    uint32_t   maxTextureRef_ = 0; // largest 1-based texture index the materials use
     bool     sceneBuilt_   = false;
 
     // Film and wavefront state.

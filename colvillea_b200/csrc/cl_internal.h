@@ -73,7 +73,7 @@ struct WideBvh
     DevBuf   nodes; // 5 uint4 per node
     DevBuf   tris;  // 3 float4 per triangle, leaf order
     DevBuf   exact; // refit: 6 floats per node, the unquantised box of its triangles
-    DevBuf   scene; // refit: scene bounds (6 ordered ints) and the SAH sum (double)
+    DevBuf   scene; // scene bounds (6 ordered ints, refit) and the SAH sum (double at byte 32)
     // Nodes of tree level d are [levels[d], levels[d + 1]): the collapse
     // allocates each level's nodes in one launch.
     std::vector<uint32_t> levels;
@@ -103,7 +103,7 @@ cl_status refitWideBvh(WideBvh* bvh, const void* vtx, const void* triIdx, cudaSt
 // Surface-area cost of the built tree: sum over child slots of the slot's
 // quantised box area, times the triangle count for leaf slots, over the root
 // box area (one unit per node visit and per triangle test).  Synchronises st.
-cl_status wideBvhSahCost(const WideBvh& bvh, cudaStream_t st, double* cost, std::string* err);
+cl_status wideBvhSahCost(WideBvh& bvh, cudaStream_t st, double* cost, std::string* err);
 
 // Triangle positions (9 floats each, triangle order) gathered from vtx and
 // triIdx, the input of buildWideBvh.  Asynchronous on st.

@@ -3,6 +3,7 @@
 // run, one item per thread, host buffers in and out.
 #include "cl_device.cuh"
 #include "cl_internal.h"
+#include "cl_texture.h"
 
 #include <vector>
 
@@ -367,6 +368,54 @@ cl_status unitFrame(const float* s, const float* t, const float* nn, const float
     CL_TRY(b.out(loc, 3 * size_t(n), &f));
     CL_TRY(b.out(wld, 3 * size_t(n), &g));
     kFrame<<<grid(n), 128>>>(a, c, d, e, f, g, n);
+    return b.finish();
+}
+
+// in: 16 floats per item {wo, dpdu, dpdv, nb, texel rgb, pullUp}; out: 9 {s, t, n}.
+__global__ void kNormalFrame(const float* in, float* out, uint32_t n)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* p = in + 16 * size_t(i);
+    f3    wo{p[0], p[1], p[2]}, du{p[3], p[4], p[5]}, dv{p[6], p[7], p[8]}, nb{p[9], p[10], p[11]};
+    f3    tx{p[12], p[13], p[14]};
+    Frame f = normalMappedFrame(wo, du, dv, nb, tx, p[15] != 0.0f);
+    float* o = out + 9 * size_t(i);
+    o[0] = f.s.x; o[1] = f.s.y; o[2] = f.s.z;
+    o[3] = f.t.x; o[4] = f.t.y; o[5] = f.t.z;
+    o[6] = f.n.x; o[7] = f.n.y; o[8] = f.n.z;
+}
+
+__global__ void kTexLookup(const unsigned long long* tex, const float* uv, float4* out, uint32_t n)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = tex2D<float4>(cudaTextureObject_t(tex[0]), uv[2 * size_t(i)], uv[2 * size_t(i) + 1]);
+}
+
+cl_status unitNormalFrame(const float* in, float* out, uint32_t n, std::string* err)
+{
+    CL_REQ(in && out);
+    if (!n) return CL_OK;
+    Batch  b(err);
+    float *x, *y;
+    CL_TRY(b.in(in, 16 * size_t(n), &x));
+    CL_TRY(b.out(out, 9 * size_t(n), &y));
+    kNormalFrame<<<grid(n), 128>>>(x, y, n);
+    return b.finish();
+}
+
+cl_status unitTextureLookup(const cl_texture_desc* t, const float* uv, float* rgba, uint32_t n, std::string* err)
+{
+    CL_REQ(t && uv && rgba);
+    if (!n) return CL_OK;
+    TextureSet ts;
+    CL_TRY(ts.build(t, 1, nullptr, err));
+    Batch  b(err);
+    float *u, *o;
+    CL_TRY(b.in(uv, 2 * size_t(n), &u));
+    CL_TRY(b.out(rgba, 4 * size_t(n), &o));
+    kTexLookup<<<grid(n), 128>>>(ts.device(), u, reinterpret_cast<float4*>(o), n);
     return b.finish();
 }
 

@@ -92,19 +92,56 @@ class TriangleMesh(_Node):
         self._scene._edit(A.ShapeEdited)
 
 
-class Material(_Node):
-    """A scenes.Material whose setters mark MaterialEdited."""
+class Texture(_Node):
+    """An image texture (ImageTexture2D, src/core/nodes/textures/imagetex2d.cpp)."""
 
     def __init__(self, scene, desc):
         super().__init__(scene)
         self.desc = desc
 
+    def setTexels(self, texels, srgb=None):
+        self.desc.texels = texels
+        if srgb is not None:
+            self.desc.srgb = srgb
+        self._scene._edit(A.TexturesEdited)
+
+
+TEXTURE_SLOTS = ("reflectance_texture", "roughness_texture", "normal_texture")
+
+
+class Material(_Node):
+    """A scenes.Material whose setters mark MaterialEdited.  Its texture slots
+    hold Texture nodes (or None); compiling turns them into the 1-based
+    indices the integrator takes."""
+
+    def __init__(self, scene, desc, textures=None):
+        super().__init__(scene)
+        self.desc = desc
+        self.textures = {k: None for k in TEXTURE_SLOTS}
+        self.textures.update(textures or {})
+
     def set(self, **fields):
         for k, v in fields.items():
-            if not hasattr(self.desc, k):
+            if k in TEXTURE_SLOTS:
+                if v is not None and v not in self._scene.textures:
+                    raise ValueError("texture is not in the scene")
+                self.textures[k] = v
+            elif not hasattr(self.desc, k):
                 raise AttributeError(k)
-            setattr(self.desc, k, v)
+            else:
+                setattr(self.desc, k, v)
         self._scene._edit(A.MaterialEdited)
+
+    def setNormalmap(self, texture):
+        """Material::setNormalmap (libkernel/base/material.h:91)."""
+        self.set(normal_texture=texture)
+
+    def compile(self, tex_index):
+        d = scenes.Material(**vars(self.desc))
+        for k in TEXTURE_SLOTS:
+            t = self.textures[k]
+            setattr(d, k, 0 if t is None else tex_index[id(t)] + 1)
+        return d
 
 
 class Emitter(_Node):
@@ -143,7 +180,7 @@ class Scene:
     """Scene API (scene.h:106-400) with edit tracking."""
 
     def __init__(self):
-        self.meshes, self.materials, self.entities, self.emitters = [], [], [], []
+        self.meshes, self.materials, self.entities, self.emitters, self.textures = [], [], [], [], []
         self.camera = None
         self.width = self.height = None
         self.actions = A.NONE
@@ -167,8 +204,20 @@ class Scene:
         self._edit(A.ShapeAdded)
         return m
 
-    def createMaterial(self, desc):
-        m = Material(self, desc)
+    def createTexture(self, desc):
+        """Scene::createTexture (scene.cpp:78-94) from a scenes.Texture."""
+        t = Texture(self, desc)
+        self.textures.append(t)
+        self._edit(A.TexturesAdded)
+        return t
+
+    def createMaterial(self, desc, **textures):
+        """A material from a scenes.Material (its texture indices ignored) and
+        Texture nodes for the slots given (reflectance_texture=..., ...)."""
+        for k, t in textures.items():
+            if k not in TEXTURE_SLOTS or (t is not None and t not in self.textures):
+                raise ValueError(f"bad texture slot {k}")
+        m = Material(self, desc, textures)
         self.materials.append(m)
         self._edit(A.MaterialAdded)
         return m
@@ -205,14 +254,28 @@ class Scene:
         self.materials.remove(material)
         self._edit(A.MaterialRemoved)
 
+    def removeTexture(self, texture):
+        if any(t is texture for m in self.materials for t in m.textures.values()):
+            raise ValueError("texture is used by a material")
+        self.textures.remove(texture)
+        self._edit(A.TexturesRemoved)
+
     def removeEmitter(self, emitter):
         self.emitters.remove(emitter)
         self._edit(A.EmitterRemoved)
 
     # --- compilation (Scene::compile*, collect*) ------------------------------
+    def compileTextures(self):
+        if self.hasAction(A.AnyTextureModification):
+            return [t.desc for t in self.textures]
+        return None
+
     def compileMaterials(self):
-        if self.hasAction(A.AnyMaterialModification):
-            return [m.desc for m in self.materials]
+        """Materials with texture indices; also after texture edits, since
+        indices move when textures are added or removed."""
+        if self.hasAction(A.AnyMaterialModification | A.AnyTextureModification):
+            idx = {id(t): i for i, t in enumerate(self.textures)}
+            return [m.compile(idx) for m in self.materials]
         return None
 
     def needsInstanceBuild(self):
@@ -249,7 +312,10 @@ class Scene:
         instances, emitters and camera (all marked added)."""
         s = Scene()
         ms = [s.createTriangleMesh(m.positions, m.normals, m.tangents, m.uvs, m.indices) for m in desc.meshes]
-        mats = [s.createMaterial(scenes.Material(**vars(m))) for m in desc.materials]
+        ts = [s.createTexture(scenes.Texture(t.texels, t.srgb)) for t in getattr(desc, "textures", [])]
+        mats = [s.createMaterial(scenes.Material(**vars(m)),
+                                 **{k: ts[getattr(m, k) - 1] for k in TEXTURE_SLOTS if getattr(m, k, 0)})
+                for m in desc.materials]
         for mesh_id, mat, xf in desc.instances:
             s.createEntity(ms[mesh_id], mats[mat], xf)
         for e in desc.emitters:
@@ -281,7 +347,12 @@ class RenderEngine:
         self.integrator.render(spp)
 
     def compileMaterials(self):
+        """compileMaterials (renderengine.cpp:54-62); textures are uploaded
+        with them (the reference uploads at Scene::createTexture)."""
+        texs = self.scene.compileTextures()
         mats = self.scene.compileMaterials()
+        if texs is not None:
+            self.integrator.buildTextures(texs)
         if mats is not None:
             self.integrator.buildMaterials(mats)
             self.integrator.resetIterationIndex()

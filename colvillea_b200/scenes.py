@@ -50,10 +50,27 @@ class Material:
     interior_ior: float = 1.5
     eta: tuple = (0.0, 0.0, 0.0)
     k: tuple = (0.0, 0.0, 0.0)
+    reflectance_texture: int = 0   # 1-based index into Scene.textures, 0 = none
+    roughness_texture: int = 0
+    normal_texture: int = 0
 
     def as_array(self):
-        return np.array([self.type, *self.reflectance, self.roughness, self.interior_ior, *self.eta, *self.k],
-                        np.float32)
+        return np.array([self.type, *self.reflectance, self.roughness, self.interior_ior, *self.eta, *self.k,
+                         self.reflectance_texture, self.roughness_texture, self.normal_texture, 0], np.float32)
+
+
+TEX_RGBA8, TEX_RGBA32F = 0, 1
+
+
+@dataclass
+class Texture:
+    """An image texture: (h, w, 4) uint8 (RGBA8, optionally sRGB) or float32 (RGBA32F)."""
+    texels: np.ndarray
+    srgb: bool = False
+
+    @property
+    def format(self):
+        return TEX_RGBA8 if self.texels.dtype == np.uint8 else TEX_RGBA32F
 
 
 @dataclass
@@ -85,6 +102,7 @@ class Scene:
     rr_start: int = 3
     name: str = ""
     info: dict = field(default_factory=dict)
+    textures: list = field(default_factory=list)
 
     @property
     def num_triangles(self):
@@ -121,7 +139,8 @@ class Scene:
             materials=np.stack([m.as_array() for m in self.materials]),
             emitters=np.stack([e.as_array() for e in self.emitters]) if self.emitters else np.zeros((0, 12), np.float32),
             dome_texels=dome.texels if dome is not None else np.zeros((1, 1, 4), np.float32),
-            camera=np.asarray(self.camera, np.float32), width=self.width, height=self.height)
+            camera=np.asarray(self.camera, np.float32), width=self.width, height=self.height,
+            textures=list(self.textures))
 
 
 @dataclass
@@ -138,6 +157,7 @@ class FlatScene:
     camera: np.ndarray
     width: int
     height: int
+    textures: list = field(default_factory=list)
 
 
 # ---------------------------------------------------------------------------
@@ -210,12 +230,12 @@ def torus_mesh(nu, nv, center, R, r):
                 uv.astype(np.float32), idx.astype(np.uint32))
 
 
-def quad_mesh(size, y=0.0):
+def quad_mesh(size, y=0.0, uv_scale=1.0):
     h = size / 2.0
     pos = np.array([[-h, y, -h], [h, y, -h], [h, y, h], [-h, y, h]], np.float32)
     nrm = np.tile(np.array([0, 1, 0], np.float32), (4, 1))
     tan = np.tile(np.array([1, 0, 0], np.float32), (4, 1))
-    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32) * np.float32(uv_scale)
     idx = np.array([[0, 2, 1], [0, 3, 2]], np.uint32)
     return Mesh(pos, nrm, tan, uv, idx)
 
@@ -343,6 +363,65 @@ def _random_material(rng, glass_frac=None, glass_alpha=(0.05, 0.3)):
 
 
 # ---------------------------------------------------------------------------
+# Procedural textures (seeded)
+# ---------------------------------------------------------------------------
+def _smooth_noise(n, cells, rng):
+    """(n, n) periodic value noise in [0, 1] (bilinear over a cells x cells lattice)."""
+    g = rng.random((cells, cells))
+    x = np.arange(n) * cells / n
+    i0 = np.floor(x).astype(int); f = x - i0; i1 = (i0 + 1) % cells
+    f = f * f * (3 - 2 * f)
+    a = g[i0][:, i0] * (1 - f)[None, :] + g[i0][:, i1] * f[None, :]
+    b = g[i1][:, i0] * (1 - f)[None, :] + g[i1][:, i1] * f[None, :]
+    return a * (1 - f)[:, None] + b * f[:, None]
+
+
+def checker_texture(n, squares, c0, c1, rng, srgb=True):
+    """RGBA8 checkerboard with noise, sRGB-encoded colours."""
+    y, x = np.mgrid[0:n, 0:n]
+    m = ((x * squares // n + y * squares // n) % 2)[..., None]
+    c = np.where(m == 1, np.asarray(c1, np.float64), np.asarray(c0, np.float64))
+    c = np.clip(c * (0.75 + 0.5 * _smooth_noise(n, 8, rng))[..., None], 0, 1)
+    out = np.empty((n, n, 4), np.uint8)
+    out[..., :3] = np.round(c * 255)
+    out[..., 3] = 255
+    return Texture(out, srgb=srgb)
+
+
+def color_texture(n, rng):
+    """RGBA32F smooth colours in [0.05, 0.95]."""
+    out = np.ones((n, n, 4), np.float32)
+    for c in range(3):
+        out[..., c] = 0.05 + 0.9 * _smooth_noise(n, 6, rng)
+    return Texture(out)
+
+
+def roughness_texture(n, rng, lo=0.05, hi=0.8):
+    """RGBA8 linear: roughness in the red channel."""
+    r = lo + (hi - lo) * _smooth_noise(n, 5, rng)
+    out = np.zeros((n, n, 4), np.uint8)
+    out[..., 0] = np.round(r * 255)
+    out[..., 3] = 255
+    return Texture(out)
+
+
+def normal_map(n, rng, tilt=0.5, cells=12):
+    """RGBA8 linear tangent-space normal map of a periodic height field:
+    n = normalize(-k dh/du, -k dh/dv, 1) with k setting the slopes' standard
+    deviation to `tilt`, stored as (n + 1) / 2."""
+    h = _smooth_noise(n, cells, rng)
+    du = np.roll(h, -1, 1) - np.roll(h, 1, 1)
+    dv = np.roll(h, -1, 0) - np.roll(h, 1, 0)
+    k = tilt / max(np.std(np.concatenate([du.ravel(), dv.ravel()])), 1e-12)
+    v = np.stack([-k * du, -k * dv, np.ones_like(h)], -1)
+    v /= np.linalg.norm(v, axis=-1, keepdims=True)
+    out = np.zeros((n, n, 4), np.uint8)
+    out[..., :3] = np.round((v + 1) * 0.5 * 255)
+    out[..., 3] = 255
+    return Texture(out)
+
+
+# ---------------------------------------------------------------------------
 # Configurations
 # ---------------------------------------------------------------------------
 def config1(seed=0, width=256, height=256, glass_frac=None, glass_alpha=(0.05, 0.3), dome=None):
@@ -360,6 +439,49 @@ def config1(seed=0, width=256, height=256, glass_frac=None, glass_alpha=(0.05, 0
     ems = [directional(), dome]
     cam = look_at_camera((0, 3, -10), (0, 0, 0), (0, 1, 0), 45.0, width, height)
     return Scene(width, height, meshes, inst, mats, ems, cam, spp=16, max_depth=5, rr_start=3, name="cfg1")
+
+
+def textured(seed=0, width=256, height=256):
+    """Config 1's layout with image textures on every material kind: an sRGB
+    checker and a normal map on the ground, RGBA32F reflectance textures,
+    metal reflectance and roughness textures, normal maps on metal and glass
+    spheres."""
+    rng = np.random.default_rng(seed + 31)
+    tex = [checker_texture(256, 8, (0.8, 0.75, 0.7), (0.15, 0.2, 0.3), rng),   # 1 ground albedo (sRGB)
+           normal_map(256, rng),                                                # 2 ground bumps
+           color_texture(64, rng), color_texture(128, rng),                     # 3, 4 diffuse colours
+           roughness_texture(64, rng),                                          # 5 metal roughness
+           checker_texture(64, 4, (1.0, 0.85, 0.6), (0.9, 0.9, 0.95), rng, srgb=False),  # 6 metal reflectance
+           normal_map(128, rng, tilt=0.8, cells=6)]                         # 7 sphere bumps
+    meshes = [quad_mesh(20.0, uv_scale=4.0)]
+    mats = [Material(MAT_DIFFUSE, reflectance=(0.5, 0.5, 0.5), reflectance_texture=1, normal_texture=2)]
+    inst = [(0, 0, IDENTITY)]
+    for i in range(32):
+        r = rng.uniform(0.2, 0.6)
+        c = (rng.uniform(-4, 4), rng.uniform(0.2, 2.0), rng.uniform(-4, 4))
+        meshes.append(sphere_mesh(2, c, r))
+        k = i % 6
+        if k == 0:
+            m = Material(MAT_DIFFUSE, reflectance=(0.5, 0.5, 0.5), reflectance_texture=3)
+        elif k == 1:
+            m = Material(MAT_DIFFUSE, reflectance=(0.5, 0.5, 0.5), reflectance_texture=4, normal_texture=7)
+        elif k == 2:
+            m = Material(MAT_METAL, reflectance=(1.0, 1.0, 1.0), roughness=0.3, eta=GOLD_ETA, k=GOLD_K,
+                         roughness_texture=5)
+        elif k == 3:
+            m = Material(MAT_METAL, reflectance=(1.0, 1.0, 1.0), roughness=0.2, eta=GOLD_ETA, k=GOLD_K,
+                         reflectance_texture=6, normal_texture=7)
+        elif k == 4:
+            m = Material(MAT_GLASS, roughness=0.15, interior_ior=1.5, normal_texture=7)
+        else:
+            m = _random_material(rng)
+        mats.append(m)
+        inst.append((len(meshes) - 1, len(mats) - 1, IDENTITY))
+    lobes = [(d, 2.0, 50.0) for d in random_upper_dirs(rng, 3)]
+    dome = Emitter(EMIT_DOME, texels=hdri(256, 128, lobes, rng))
+    cam = look_at_camera((0, 3, -10), (0, 0, 0), (0, 1, 0), 45.0, width, height)
+    return Scene(width, height, meshes, inst, mats, [directional(), dome], cam, spp=16, max_depth=5, rr_start=3,
+                 name="textured", textures=tex)
 
 
 def config2(seed=0, width=1920, height=1080, terrain_n=1024, objects=512, hdri_size=(2048, 1024)):

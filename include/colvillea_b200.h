@@ -126,7 +126,41 @@ typedef struct
     float    interior_ior;
     float    eta[3];
     float    k[3];
+    /* Textures: 1-based indices into the last cl_build_textures, 0 = none.
+     * A texture replaces the constant (DiffuseMtl/MetalMtl::getBSDF,
+     * libkernel/materials/diffusemtl.h:20-29, metal.h:37-55):
+     *   reflectance_texture  rgb: diffuse reflectance or metal specular
+     *                        reflectance (not glass);
+     *   roughness_texture    red channel: metal roughness, squared to the GGX
+     *                        alpha like the constant (metal only);
+     *   normal_texture       tangent-space normal map, n = rgb * 2 - 1, any
+     *                        type (Material::setNormalmap, material.h:91). */
+    uint32_t reflectance_texture;
+    uint32_t roughness_texture;
+    uint32_t normal_texture;
 } cl_material_desc;
+
+/* Image textures (the reference's ImageTexture2D,
+ * src/core/nodes/textures/imagetex2d.cpp:8-68): each one a CUDA array read
+ * through a texture object with bilinear filtering, wrap addressing in u and
+ * v, normalised coordinates and no mip maps.  RGBA8 texels are read as
+ * normalised floats, decoded from sRGB to linear by the texture unit before
+ * filtering when `srgb` is set; RGBA32F texels as floats.  Lookups use the
+ * hit's uv (interpolated vertex uvs, or the barycentrics (b0, b1) for meshes
+ * without uvs, optix.cu:164); texel row 0 is v = 0. */
+enum
+{
+    CL_TEXTURE_RGBA8   = 0,
+    CL_TEXTURE_RGBA32F = 1
+};
+typedef struct
+{
+    uint32_t    format; /* CL_TEXTURE_* */
+    uint32_t    width;
+    uint32_t    height;
+    uint32_t    srgb;   /* RGBA8 only */
+    const void* texels; /* width*height texels, 4 channels, rows of width */
+} cl_texture_desc;
 
 /* Emitter (EmitterType, libkernel/base/emitter.h:16-26).  Directional:
  * intensity, direction (from the light), angular radius (directional.h:19-22).
@@ -181,10 +215,10 @@ typedef struct
     uint64_t shadow_tris;    /* ... shadow-ray triangles tested */
     uint64_t last_rays_closest; /* last render: closest-hit segments */
     uint64_t last_rays_shadow;  /* last render: shadow rays */
-    float    ms_bvh_update;     /* last cl_update_mesh_vertices: refit and/or rebuild */
+    float    ms_bvh_update;     /* last cl_update_mesh_vertices: device time of the refit and/or rebuild */
+    float    ms_bvh_refit;      /* ... of its refit alone (0: none) */
     uint32_t bvh_refits;        /* refits since the integrator was created */
     uint32_t bvh_rebuilds;      /* rebuilds after vertex updates */
-    uint32_t pad2;
     double   bvh_sah;           /* surface-area cost of the current tree (root = 1) */
     double   bvh_sah_build;     /* ... right after its last full build */
 } cl_stats;
@@ -232,6 +266,11 @@ cl_status cl_update_mesh_vertices(cl_integrator* integrator, uint32_t mesh_id, c
  * Either pointer may be null.  No counterpart in the reference. */
 cl_status cl_get_bvh(cl_integrator* integrator, void* nodes, size_t node_bytes, void* triangles,
                      size_t triangle_bytes);
+/* Textures created by the scene before materials refer to them
+ * (Scene::createTexture, scene.h:151-160; compiled with the materials,
+ * RenderEngine::compileMaterials).  Replaces all textures; materials keep
+ * their indices. */
+cl_status cl_build_textures(cl_integrator* integrator, const cl_texture_desc* textures, uint32_t count);
 /* Integrator::buildMaterials (integrator.h:52). */
 cl_status cl_build_materials(cl_integrator* integrator, const cl_material_desc* materials, uint32_t count);
 /* Integrator::buildEmitters (integrator.h:56-58): the last dome in the list is
@@ -291,6 +330,13 @@ cl_status cl_unit_warp(const float* u2, float* disk, float* hemisphere, uint32_t
 cl_status cl_unit_make_frame(const float* a, float* b, float* c, uint32_t count);
 cl_status cl_unit_frame(const float* s, const float* t, const float* n, const float* v, float* local, float* world,
                         uint32_t count);
+/* Normal-mapped shading frame (Material::getShadingFrameImpl with a normal
+ * map, material.h:164-221, and fixNormalPerturbingShadingFrame,
+ * material.h:238-285): per item 16 floats {wo, dpdu, dpdv, base normal,
+ * normal-map texel rgb, pull-up (0 or 1)}; out 9 floats {s, t, n}. */
+cl_status cl_unit_normal_frame(const float* in, float* frame, uint32_t count);
+/* Lookups in one texture set up like the integrator's: uv pairs in, RGBA out. */
+cl_status cl_unit_texture_lookup(const cl_texture_desc* texture, const float* uv, float* rgba, uint32_t count);
 cl_status cl_unit_pcg4d(const uint32_t* in, uint32_t* out, uint32_t count);
 cl_status cl_unit_sampler_sequence(const uint32_t* px_py_frame, uint32_t count, uint32_t draws, float* out);
 /* HDRI dome against caller tables (reference layout): CDF sampling, pdf, eval. */

@@ -31,6 +31,7 @@
 #include <cstdio>
 #include <memory>
 #include <thread>
+#include <array>
 #include <vector>
 
 #ifdef _OPENMP
@@ -88,8 +89,10 @@ struct Scene
     MeshView              mesh{};
     const uint32_t*       triMaterial = nullptr;
     uint32_t              ntris       = 0;
-    // materials
-    std::vector<Bsdf<float>> materials;
+    // materials: constants and 1-based texture indices {reflectance, roughness, normal map}
+    std::vector<Bsdf<float>>               materials;
+    std::vector<std::array<uint32_t, 3>>   matTex;
+    std::vector<Texture>                   textures;
     // emitters: in list order (light-selection order), plus the dome
     struct Em
     {
@@ -390,8 +393,10 @@ Hit bruteforce(const Scene& s, V3<float> o, V3<float> d, float tmin, float tmax)
 extern "C" {
 
 // Layouts shared with the product's C ABI (include/colvillea_b200.h):
-//   material: 12 floats {type, r, g, b, roughness, etaInt, eta.xyz, k.xyz};
+//   material: 16 floats {type, r, g, b, roughness, etaInt, eta.xyz, k.xyz,
+//             reflectance, roughness and normal-map texture (1-based, 0 none), 0};
 //             alpha = roughness^2 (metal.h:52, glass.h:26).
+//   texture : orc_texture {format 0 RGBA8 / 1 RGBA32F, w, h, srgb, texels}.
 //   emitter : 12 floats {type(0 dir, 1 dome), intensity.xyz, direction.xyz,
 //             angularRadius, domeW, domeH, 0, 0}; dome texels separate.
 struct orc_scene_desc
@@ -410,6 +415,8 @@ struct orc_scene_desc
     uint32_t        nemitters;
     const float*    dome_texels; // RGBA32F
     const float*    camera;      // pos, d00, ddu, ddv (12 floats)
+    const orc::Texture* textures;
+    uint32_t        ntextures;
 };
 
 // Integrator flags.
@@ -442,7 +449,7 @@ void* orc_scene_create(const orc_scene_desc* d)
     buildBVH(*s);
     for (uint32_t m = 0; m < d->nmaterials; ++m)
     {
-        const float* p = d->materials + 12 * size_t(m);
+        const float* p = d->materials + 16 * size_t(m);
         Bsdf<float>  b{};
         b.type   = uint32_t(p[0]);
         b.r      = {p[1], p[2], p[3]};
@@ -453,7 +460,9 @@ void* orc_scene_create(const orc_scene_desc* d)
         b.k      = {p[9], p[10], p[11]};
         b.etaExt = 1.0f;
         s->materials.push_back(b);
+        s->matTex.push_back({uint32_t(p[12]), uint32_t(p[13]), uint32_t(p[14])});
     }
+    s->textures.assign(d->textures, d->textures + d->ntextures);
     for (uint32_t e = 0; e < d->nemitters; ++e)
     {
         const float* p = d->emitters + 12 * size_t(e);
@@ -590,11 +599,36 @@ V3<float> tracePath(const Scene& s, const orc_config& cfg, uint32_t W, uint32_t 
         }
         if (!dl && depth == cfg.max_depth) break;
 
-        HitAttr           a    = hitAttributes(s.mesh, h.id, h.b1, h.b2);
-        const Bsdf<float>& bsdf = s.materials[s.triMaterial[h.id]];
-        V3<float>         wo   = -d;
-        V2<float>         u    = rng.next2D();
-        Frame<float>      fr{a.dpdv, a.dpdu, (!dl && compatFrame) ? a.ng : a.ns};
+        HitAttr     a    = hitAttributes(s.mesh, h.id, h.b1, h.b2);
+        uint32_t    mi   = s.triMaterial[h.id];
+        Bsdf<float> bsdf = s.materials[mi];
+        const auto& tx   = s.matTex[mi];
+        // Material::getBSDF(uv): textures replace the constants (diffusemtl.h:22-27, metal.h:40-52).
+        if (tx[0])
+        {
+            F4 c   = texUnit(s.textures[tx[0] - 1], a.uv.x, a.uv.y);
+            bsdf.r = {c.v[0], c.v[1], c.v[2]};
+        }
+        if (tx[1])
+        {
+            float r    = texUnit(s.textures[tx[1] - 1], a.uv.x, a.uv.y).v[0];
+            bsdf.alpha = r * r;
+        }
+        V3<float>    wo = -d;
+        V2<float>    u  = rng.next2D();
+        // Material::getShadingFrame (material.h:128-147) with the path-tracing
+        // call site's swapped (ng, ns) (raygeneration.cu:324-330): without a
+        // normal map the compat frame's normal is ng; a normal map's tangent
+        // frame and pull-up use ns.  The direct-lighting kernel ignores normal
+        // maps (raygeneration.cu:179,237).
+        Frame<float> fr;
+        if (tx[2] && !(dl && compatFrame))
+        {
+            F4 nt = texUnit(s.textures[tx[2] - 1], a.uv.x, a.uv.y);
+            fr    = normalMappedFrame(wo, a.dpdu, a.dpdv, a.ns, V3<float>{nt.v[0], nt.v[1], nt.v[2]}, bsdf.type != 2u);
+        }
+        else
+            fr = Frame<float>{a.dpdv, a.dpdu, (!dl && compatFrame) ? a.ng : a.ns};
 
         // Emitter sampling with MIS (raygeneration.cu:332-384 / 174-227).
         if (N > 0)
@@ -996,6 +1030,41 @@ void orc_directional_sample(const float* params /*7: intensity, direction, radiu
             val[3 * i + k] = v[k];
         }
         pdf[i] = p;
+    }
+}
+
+void orc_texture_lookup(const orc::Texture* t, const float* uv, float* out, int n)
+{
+    for (int i = 0; i < n; ++i)
+    {
+        F4 c = texUnit(*t, uv[2 * i], uv[2 * i + 1]);
+        for (int k = 0; k < 4; ++k) out[4 * i + k] = c.v[k];
+    }
+}
+
+// in: 16 floats per item {wo, dpdu, dpdv, nb, texel rgb, pullUp}; out 9 {s, t, n}.
+void orc_normal_frame(const float* in, float* out, int n, int fp64)
+{
+    for (int i = 0; i < n; ++i)
+    {
+        const float* p = in + 16 * size_t(i);
+        float*       o = out + 9 * size_t(i);
+        if (fp64)
+        {
+            auto v = [&](int k) { return V3<double>{p[k], p[k + 1], p[k + 2]}; };
+            Frame<double> f = normalMappedFrame(v(0), v(3), v(6), v(9), v(12), p[15] != 0.0f);
+            V3<double> r[3] = {f.s, f.t, f.n};
+            for (int k = 0; k < 3; ++k)
+                for (int c = 0; c < 3; ++c) o[3 * k + c] = float(r[k][c]);
+        }
+        else
+        {
+            auto v = [&](int k) { return V3<float>{p[k], p[k + 1], p[k + 2]}; };
+            Frame<float> f = normalMappedFrame(v(0), v(3), v(6), v(9), v(12), p[15] != 0.0f);
+            V3<float> r[3] = {f.s, f.t, f.n};
+            for (int k = 0; k < 3; ++k)
+                for (int c = 0; c < 3; ++c) o[3 * k + c] = r[k][c];
+        }
     }
 }
 

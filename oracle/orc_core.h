@@ -271,6 +271,61 @@ template <class T> inline V3<T> reflect(V3<T> wo, V3<T> n)
     T d = T(2) * dot(wo, n);
     return {-wo.x + d * n.x, -wo.y + d * n.y, -wo.z + d * n.z};
 }
+// ---------------------------------------------------------------------------
+// Normal-mapped shading frame (Material::getShadingFrame, material.h:128-287).
+// ---------------------------------------------------------------------------
+constexpr float kUpliftEps = 1.1f; // float(kNormalmapAutoAdapationUpliftEpsilon()), config.h:9
+
+// fixNormalPerturbingShadingFrame (material.h:238-285).
+template <class T> inline void fixNormalPerturbing(V3<T> wo, Frame<T>* fr, V3<T> ng)
+{
+    if (dot(wo, ng) < T(0))
+    {
+        fr->n = fr->n * T(-1);
+        ng    = ng * T(-1);
+    }
+    if (dot(wo, ng) > T(0))
+    {
+        V3<T> r = reflect(wo, fr->n);
+        if (dot(r, ng) <= T(0))
+        {
+            T     a  = std::abs(dot(r, ng));
+            T     b  = dot(fr->n, ng);
+            V3<T> up = (a / b) * fr->n;     // a / b * shFrame.n * eps
+            up       = up * T(kUpliftEps);
+            fr->n    = normalize(normalize(r + up) + wo);
+            fr->t    = normalize(fr->t - dot(fr->t, fr->n) * fr->n);
+            fr->s    = normalize(cross(fr->n, fr->t));
+            if (dot(fr->n, ng) < T(0))
+            {
+                fr->n = fr->n * T(-1);
+                fr->t = fr->t * T(-1);
+            }
+        }
+    }
+}
+
+// getShadingFrameImpl with a normal map (material.h:164-221): nb is the
+// normal of the unmodified tangent frame {dpdv, dpdu, nb}.
+template <class T> inline Frame<T> normalMappedFrame(V3<T> wo, V3<T> dpdu, V3<T> dpdv, V3<T> nb, V3<T> texel, bool pullUp)
+{
+    V3<T> m = texel * T(2);
+    m       = {m.x - T(1), m.y - T(1), m.z - T(1)};
+    m       = normalize(m);
+    m       = Frame<T>{dpdv, dpdu, nb}.toWorld(m);
+    V3<T> du = dpdu - m * dot(dpdu, m);
+    du       = normalize(du);
+    V3<T> dv = normalize(cross(m, du));
+    if (dot(m, nb) < T(0))
+    {
+        m  = m * T(-1);
+        du = du * T(-1);
+    }
+    Frame<T> fr{dv, du, m};
+    if (pullUp) fixNormalPerturbing(wo, &fr, nb);
+    return fr;
+}
+
 template <class T> inline V3<T> refract(V3<T> wi, V3<T> n, T eta, T cosThetaT)
 {
     if (cosThetaT < T(0)) eta = T(1) / eta;

@@ -59,8 +59,22 @@ class OrcSceneDesc(ctypes.Structure):
         ("nverts", ctypes.c_uint32), ("idx", ctypes.c_void_p), ("tri_material", ctypes.c_void_p),
         ("ntris", ctypes.c_uint32), ("materials", ctypes.c_void_p), ("nmaterials", ctypes.c_uint32),
         ("emitters", ctypes.c_void_p), ("nemitters", ctypes.c_uint32), ("dome_texels", ctypes.c_void_p),
-        ("camera", ctypes.c_void_p),
+        ("camera", ctypes.c_void_p), ("textures", ctypes.c_void_p), ("ntextures", ctypes.c_uint32),
     ]
+
+
+class OrcTexture(ctypes.Structure):
+    _fields_ = [("format", ctypes.c_int), ("w", ctypes.c_int), ("h", ctypes.c_int), ("srgb", ctypes.c_int),
+                ("texels", ctypes.c_void_p)]
+
+
+def orc_texture(t):
+    """(OrcTexture, array to keep alive) for a scenes.Texture."""
+    a = np.ascontiguousarray(t.texels)
+    fmt = 0 if a.dtype == np.uint8 else 1
+    if fmt == 1:
+        a = np.ascontiguousarray(a, np.float32)
+    return OrcTexture(fmt, a.shape[1], a.shape[0], int(bool(t.srgb)), P(a)), a
 
 
 class OrcConfig(ctypes.Structure):
@@ -75,8 +89,14 @@ class OracleScene:
         self._keep = [f32(flat.pos), f32(flat.nrm), f32(flat.tan), f32(flat.uv), u32(flat.idx), u32(flat.tri_material),
                       f32(flat.materials), f32(flat.emitters), f32(flat.dome_texels), f32(flat.camera)]
         pos, nrm, tan, uv, idx, tm, mats, ems, dome, cam = self._keep
+        texs = getattr(flat, "textures", None) or []
+        tarr = (OrcTexture * max(1, len(texs)))()
+        for i, t in enumerate(texs):
+            tarr[i], a = orc_texture(t)
+            self._keep.append(a)
+        self._keep.append(tarr)
         d = OrcSceneDesc(P(pos), P(nrm), P(tan), P(uv), len(pos), P(idx), P(tm), len(idx), P(mats), len(mats),
-                         P(ems), len(ems), P(dome), P(cam))
+                         P(ems), len(ems), P(dome), P(cam), ctypes.cast(tarr, ctypes.c_void_p), len(texs))
         self.h = lib().orc_scene_create(ctypes.byref(d))
         self.width, self.height = flat.width, flat.height
         self.ntris = len(idx)
@@ -200,6 +220,23 @@ def frame(s, t, n, v):
     loc = np.zeros_like(v); wld = np.zeros_like(v)
     lib().orc_frame(P(s), P(t), P(n), P(v), P(loc), P(wld), len(v))
     return loc, wld
+
+
+def texture_lookup(t, uv):
+    """Texture-unit model (bilinear, 8-bit weights rounded half up, wrap; RGBA8 decoded first)."""
+    d, a = orc_texture(t)
+    uv = f32(uv).reshape(-1, 2)
+    out = np.zeros((len(uv), 4), np.float32)
+    lib().orc_texture_lookup(ctypes.byref(d), P(uv), P(out), len(uv))
+    return out
+
+
+def normal_frame(inputs16, fp64=False):
+    """(n, 16) {wo, dpdu, dpdv, base normal, texel rgb, pull-up} -> (n, 3, 3) {s, t, n}."""
+    x = f32(inputs16).reshape(-1, 16)
+    out = np.zeros((len(x), 9), np.float32)
+    lib().orc_normal_frame(P(x), P(out), len(x), int(fp64))
+    return out.reshape(-1, 3, 3)
 
 
 def pcg4d(v):

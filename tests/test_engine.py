@@ -47,6 +47,12 @@ def test_initial_compile_sequence():
     # no edits: progressive accumulation continues (camera unchanged is a no-op in the integrator)
     eng.startRendering(1)
     assert it.names() == ["updateCamera", "render"]
+    # a textured scene uploads its textures with the materials
+    ts, tit = Scene.fromScene(scenes.textured(0, 32, 32)), Recorder()
+    RenderEngine(tit, ts).startRendering(1)
+    calls = list(tit.calls)
+    assert [c[0] for c in calls[:3]] == ["buildTextures", "buildMaterials", "resetIterationIndex"]
+    assert len(calls[0][1][0]) == 7 and calls[1][1][0][0].reflectance_texture == 1
 
 
 def test_vertex_edit_refits():
@@ -123,3 +129,28 @@ def test_update_vertices_checks():
     with pytest.raises(ValueError):
         m.updateVertices(bad)
     assert not s.hasAction(A.ShapeEdited) or s.hasAction(A.ShapeAdded)
+
+
+def test_texture_edits():
+    s, it = Scene.fromScene(scenes.textured(0, 32, 32)), Recorder()
+    eng = RenderEngine(it, s)
+    eng.startRendering()
+    it.names()
+    t = s.textures[2]
+    t.setTexels(t.desc.texels * 0.5)
+    assert s.actions == A.TexturesEdited
+    eng.startRendering()
+    assert it.names() == ["buildTextures", "buildMaterials", "resetIterationIndex", "updateCamera", "render"]
+    # a new texture on a material; indices follow the scene's texture order
+    nt = s.createTexture(scenes.roughness_texture(16, np.random.default_rng(0)))
+    s.materials[3].set(roughness_texture=nt)
+    eng.startRendering()
+    mats = it.calls[1][1][0]
+    assert mats[3].roughness_texture == len(s.textures)
+    it.names()
+    with pytest.raises(ValueError):
+        s.removeTexture(nt)
+    s.materials[3].set(roughness_texture=None)
+    s.removeTexture(nt)
+    eng.startRendering()
+    assert it.calls[1][1][0][3].roughness_texture == 0
