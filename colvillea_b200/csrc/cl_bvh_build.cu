@@ -801,6 +801,10 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     }
     out->depth   = depth;
     out->numTris = n;
+    // Refit state (24 bytes per node), allocated with the tree so that a
+    // refit allocates nothing.
+    CL_TRY(out->exact.alloc(size_t(out->numNodes) * 24, err));
+    CL_TRY(out->scene.alloc(64, err));
     // Host validation of every index the traversal kernels will follow.
     {
         std::vector<uint32_t> h(size_t(out->numNodes) * 20);
@@ -865,14 +869,14 @@ namespace
 constexpr int kRefitBlock = 128;
 
 // Leaf triangles from the vertex array; scene bounds into bounds[0..5] as
-// ordered ints (min x,y,z then max x,y,z).
-__global__ void kRefitTris(float4* __restrict__ tris, uint32_t n, const float4* __restrict__ vtx,
-                           const uint4* __restrict__ triIdx, uint32_t* __restrict__ bounds)
+// ordered ints (min x,y,z then max x,y,z): grid-stride, reduced per block,
+// one atomic per block and value.
+__global__ void __launch_bounds__(256) kRefitTris(float4* __restrict__ tris, uint32_t n, const float4* __restrict__ vtx,
+                                                  const uint4* __restrict__ triIdx, uint32_t* __restrict__ bounds)
 {
-    uint32_t i     = blockIdx.x * blockDim.x + threadIdx.x;
-    bool     valid = i < n;
-    float    l[3] = {0.0f, 0.0f, 0.0f}, h[3] = {0.0f, 0.0f, 0.0f};
-    if (valid)
+    __shared__ uint32_t part[6][8];
+    uint32_t            ol[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, oh[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
         float4*  t   = tris + 3 * size_t(i);
         uint32_t tid = __float_as_uint(t[0].w);
@@ -881,140 +885,167 @@ __global__ void kRefitTris(float4* __restrict__ tris, uint32_t n, const float4* 
         t[0]         = make_float4(a.x, a.y, a.z, __uint_as_float(tid));
         t[1]         = make_float4(b.x, b.y, b.z, 0.0f);
         t[2]         = make_float4(c.x, c.y, c.z, 0.0f);
-        l[0] = fminf(fminf(a.x, b.x), c.x);
-        l[1] = fminf(fminf(a.y, b.y), c.y);
-        l[2] = fminf(fminf(a.z, b.z), c.z);
-        h[0] = fmaxf(fmaxf(a.x, b.x), c.x);
-        h[1] = fmaxf(fmaxf(a.y, b.y), c.y);
-        h[2] = fmaxf(fmaxf(a.z, b.z), c.z);
+        float l[3] = {fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z)};
+        float h[3] = {fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z)};
+        for (int k = 0; k < 3; ++k)
+        {
+            ol[k] = min(ol[k], fordered(l[k]));
+            oh[k] = max(oh[k], fordered(h[k]));
+        }
     }
-    for (int a = 0; a < 3; ++a)
-    {
-        uint32_t sl = valid ? fordered(l[a]) : 0xffffffffu, sh = valid ? fordered(h[a]) : 0u;
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = 0; k < 3; ++k)
         for (int o = 16; o > 0; o >>= 1)
         {
-            sl = min(sl, __shfl_xor_sync(0xffffffffu, sl, o));
-            sh = max(sh, __shfl_xor_sync(0xffffffffu, sh, o));
+            ol[k] = min(ol[k], __shfl_xor_sync(0xffffffffu, ol[k], o));
+            oh[k] = max(oh[k], __shfl_xor_sync(0xffffffffu, oh[k], o));
         }
-        if ((threadIdx.x & 31) == 0)
+    if (lane == 0)
+        for (int k = 0; k < 3; ++k)
         {
-            atomicMin(bounds + a, sl);
-            atomicMax(bounds + 3 + a, sh);
+            part[k][warp]     = ol[k];
+            part[3 + k][warp] = oh[k];
         }
+    __syncthreads();
+    if (threadIdx.x < 6)
+    {
+        int      k = threadIdx.x;
+        uint32_t v = part[k][0];
+        for (int w = 1; w < int(blockDim.x >> 5); ++w) v = k < 3 ? min(v, part[k][w]) : max(v, part[k][w]);
+        if (k < 3)
+        {
+            if (v != 0xffffffffu) atomicMin(bounds + k, v);
+        }
+        else if (v != 0u)
+            atomicMax(bounds + k, v);
     }
 }
 
-// One tree level: child boxes from the level below (exact[]) and from the
-// leaf triangles, widened by the scene margin and requantised in a fresh
-// frame.  Topology (imask, child and triangle bases, leaf metadata, slot
-// order) is kept.
-__global__ void __launch_bounds__(kRefitBlock) kRefitLevel(uint4* __restrict__ nodes, const float4* __restrict__ tris,
-                                                           float* __restrict__ exact, uint32_t first, uint32_t count,
-                                                           const uint32_t* __restrict__ bounds)
+// One tree level, eight lanes per node (lane s = child slot s): each lane
+// boxes its slot (the child's exact box from the level below, or its leaf
+// triangles), the group reduces the node's exact and widened boxes, every
+// lane quantises its own slot in the node's frame, and lane 0 writes the
+// node.  Topology (imask, child and triangle bases, leaf metadata, slot
+// order) is kept; the result equals kCollapse's for unchanged triangles.
+__global__ void __launch_bounds__(128) kRefitLevel(uint4* __restrict__ nodes, const float4* __restrict__ tris,
+                                                   float* __restrict__ exact, uint32_t first, uint32_t count,
+                                                   const uint32_t* __restrict__ bounds)
 {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    uint32_t node = first + t;
+    uint32_t g     = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t t     = g >> 3;
+    int      s     = int(g & 7u);
+    bool     valid = t < count;
+    uint32_t node  = first + (valid ? t : 0u);
     float    sl[3], sh[3];
     for (int a = 0; a < 3; ++a)
     {
         sl[a] = funordered(bounds[a]);
         sh[a] = funordered(bounds[3 + a]);
     }
-    float    margin = sceneMargin(sl, sh);
-    uint4*   np     = nodes + size_t(node) * 5;
-    uint4    n0 = np[0], n1 = np[1];
-    uint32_t imask = n0.w >> 24;
-    uint32_t meta[2] = {n1.z, n1.w};
-
-    float    clo[8][3], chi[8][3], plo[3], phi[3], xlo[3], xhi[3];
-    uint32_t present = 0;
-    for (int a = 0; a < 3; ++a)
+    float  margin = sceneMargin(sl, sh);
+    uint4* np     = nodes + size_t(node) * 5;
+    uint4  n0 = make_uint4(0, 0, 0, 0), n1 = make_uint4(0, 0, 0, 0);
+    if (valid)
     {
-        plo[a] = xlo[a] = FLT_MAX;
-        phi[a] = xhi[a] = -FLT_MAX;
+        n0 = np[0];
+        n1 = np[1];
     }
-#pragma unroll
-    for (int s = 0; s < 8; ++s)
+    uint32_t imask = n0.w >> 24;
+    float    lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    bool     present = false;
+    if (valid)
     {
-        for (int a = 0; a < 3; ++a)
-        {
-            clo[s][a] = FLT_MAX;
-            chi[s][a] = -FLT_MAX;
-        }
         if (imask & (1u << s))
         {
             uint32_t     c = n1.x + __popc(imask & ((1u << s) - 1u));
             const float* x = exact + 6 * size_t(c);
             for (int a = 0; a < 3; ++a)
             {
-                clo[s][a] = x[a];
-                chi[s][a] = x[3 + a];
+                lo[a] = x[a];
+                hi[a] = x[3 + a];
             }
+            present = true;
         }
         else
         {
-            uint32_t m = (meta[s >> 2] >> (8 * (s & 3))) & 0xffu;
-            if (!m) continue;
-            uint32_t off = m & 31u, cnt = __popc(m >> 5);
-            for (uint32_t j = 0; j < cnt; ++j)
+            uint32_t m = ((s < 4 ? n1.z : n1.w) >> (8 * (s & 3))) & 0xffu;
+            if (m)
             {
-                const float4* tp = tris + size_t(n1.y + off + j) * 3;
-                for (int v = 0; v < 3; ++v)
+                uint32_t off = m & 31u, cnt = __popc(m >> 5);
+                for (uint32_t j = 0; j < cnt; ++j)
                 {
-                    float4 p = tp[v];
-                    clo[s][0] = fminf(clo[s][0], p.x);
-                    clo[s][1] = fminf(clo[s][1], p.y);
-                    clo[s][2] = fminf(clo[s][2], p.z);
-                    chi[s][0] = fmaxf(chi[s][0], p.x);
-                    chi[s][1] = fmaxf(chi[s][1], p.y);
-                    chi[s][2] = fmaxf(chi[s][2], p.z);
+                    const float4* tp = tris + size_t(n1.y + off + j) * 3;
+                    for (int v = 0; v < 3; ++v)
+                    {
+                        float4 p = tp[v];
+                        lo[0] = fminf(lo[0], p.x);
+                        lo[1] = fminf(lo[1], p.y);
+                        lo[2] = fminf(lo[2], p.z);
+                        hi[0] = fmaxf(hi[0], p.x);
+                        hi[1] = fmaxf(hi[1], p.y);
+                        hi[2] = fmaxf(hi[2], p.z);
+                    }
                 }
+                present = true;
             }
         }
-        present |= 1u << s;
-        for (int a = 0; a < 3; ++a)
+    }
+    // Exact box of the node and its widened frame box (group of 8 lanes).
+    float xlo[3], xhi[3], clo[3], chi[3], plo[3], phi[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        xlo[a] = lo[a];
+        xhi[a] = hi[a];
+        clo[a] = present ? lo[a] - margin : FLT_MAX;
+        chi[a] = present ? hi[a] + margin : -FLT_MAX;
+        plo[a] = clo[a];
+        phi[a] = chi[a];
+        for (int o = 1; o < 8; o <<= 1)
         {
-            xlo[a]    = fminf(xlo[a], clo[s][a]);
-            xhi[a]    = fmaxf(xhi[a], chi[s][a]);
-            clo[s][a] -= margin;
-            chi[s][a] += margin;
-            plo[a]    = fminf(plo[a], clo[s][a]);
-            phi[a]    = fmaxf(phi[a], chi[s][a]);
+            xlo[a] = fminf(xlo[a], __shfl_xor_sync(0xffffffffu, xlo[a], o, 8));
+            xhi[a] = fmaxf(xhi[a], __shfl_xor_sync(0xffffffffu, xhi[a], o, 8));
+            plo[a] = fminf(plo[a], __shfl_xor_sync(0xffffffffu, plo[a], o, 8));
+            phi[a] = fmaxf(phi[a], __shfl_xor_sync(0xffffffffu, phi[a], o, 8));
         }
     }
-
-    uint32_t ex[3];
-    float    e[3];
+    uint32_t ex[3], ql[3] = {255u, 255u, 255u}, qh[3] = {0u, 0u, 0u};
     for (int a = 0; a < 3; ++a)
     {
         ex[a] = quantExp(phi[a] - plo[a]);
-        e[a]  = __uint_as_float(ex[a] << 23);
+        if (present) quantPlanes(clo[a], chi[a], plo[a], __uint_as_float(ex[a] << 23), &ql[a], &qh[a]);
     }
-    uint32_t qlo[3][2] = {{0, 0}, {0, 0}, {0, 0}}, qhi[3][2] = {{0, 0}, {0, 0}, {0, 0}};
-#pragma unroll
-    for (int s = 0; s < 8; ++s)
-    {
-        int      word = s >> 2, sh8 = 8 * (s & 3);
-        uint32_t ql[3] = {255u, 255u, 255u}, qh[3] = {0u, 0u, 0u};
-        if (present & (1u << s))
-            for (int a = 0; a < 3; ++a) quantPlanes(clo[s][a], chi[s][a], plo[a], e[a], &ql[a], &qh[a]);
-        for (int a = 0; a < 3; ++a)
-        {
-            qlo[a][word] |= ql[a] << sh8;
-            qhi[a][word] |= qh[a] << sh8;
-        }
-    }
-    np[0] = make_uint4(__float_as_uint(plo[0]), __float_as_uint(plo[1]), __float_as_uint(plo[2]),
-                       ex[0] | (ex[1] << 8) | (ex[2] << 16) | (imask << 24));
-    np[2] = make_uint4(qlo[0][0], qlo[0][1], qlo[1][0], qlo[1][1]);
-    np[3] = make_uint4(qlo[2][0], qlo[2][1], qhi[0][0], qhi[0][1]);
-    np[4] = make_uint4(qhi[1][0], qhi[1][1], qhi[2][0], qhi[2][1]);
-    float* x = exact + 6 * size_t(node);
+    // Pack the slot bytes: OR within each quad of lanes, then bring the
+    // second quad's words to lane 0.
+    uint32_t wl[3], wh[3];
     for (int a = 0; a < 3; ++a)
     {
-        x[a]     = xlo[a];
-        x[3 + a] = xhi[a];
+        wl[a] = ql[a] << (8 * (s & 3));
+        wh[a] = qh[a] << (8 * (s & 3));
+        for (int o = 1; o < 4; o <<= 1)
+        {
+            wl[a] |= __shfl_xor_sync(0xffffffffu, wl[a], o, 8);
+            wh[a] |= __shfl_xor_sync(0xffffffffu, wh[a], o, 8);
+        }
+    }
+    uint32_t wl1[3], wh1[3];
+    for (int a = 0; a < 3; ++a)
+    {
+        wl1[a] = __shfl_down_sync(0xffffffffu, wl[a], 4, 8);
+        wh1[a] = __shfl_down_sync(0xffffffffu, wh[a], 4, 8);
+    }
+    if (valid && s == 0)
+    {
+        np[0] = make_uint4(__float_as_uint(plo[0]), __float_as_uint(plo[1]), __float_as_uint(plo[2]),
+                           ex[0] | (ex[1] << 8) | (ex[2] << 16) | (imask << 24));
+        np[2] = make_uint4(wl[0], wl1[0], wl[1], wl1[1]);
+        np[3] = make_uint4(wl[2], wl1[2], wh[0], wh1[0]);
+        np[4] = make_uint4(wh[1], wh1[1], wh[2], wh1[2]);
+        float* x = exact + 6 * size_t(node);
+        for (int a = 0; a < 3; ++a)
+        {
+            x[a]     = xlo[a];
+            x[3 + a] = xhi[a];
+        }
     }
 }
 
@@ -1083,18 +1114,32 @@ cl_status refitWideBvh(WideBvh* bvh, const void* vtx, const void* triIdx, cudaSt
         *err = "refit needs a built BVH";
         return CL_ERR_STATE;
     }
-    if (bvh->exact.bytes < size_t(bvh->numNodes) * 24) CL_TRY(bvh->exact.alloc(size_t(bvh->numNodes) * 24, err));
-    if (!bvh->scene.p) CL_TRY(bvh->scene.alloc(64, err));
-    uint32_t b0[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-    CL_CUDA(cudaMemcpyAsync(bvh->scene.p, b0, sizeof(b0), cudaMemcpyHostToDevice, st), err);
+    if (bvh->exact.bytes < size_t(bvh->numNodes) * 24 || !bvh->scene.p)
+    {
+        *err = "refit buffers missing";
+        return CL_ERR_STATE;
+    }
+    // Bounds start at (+inf ordered, -inf ordered): 0xff bytes for the
+    // minima, zero bytes for the maxima.
+    CL_CUDA(cudaMemsetAsync(bvh->scene.p, 0xff, 12, st), err);
+    CL_CUDA(cudaMemsetAsync(bvh->scene.u() + 3, 0, 12, st), err);
     uint32_t n = bvh->numTris;
-    kRefitTris<<<(n + 255) / 256, 256, 0, st>>>(bvh->tris.as<float4>(), n, static_cast<const float4*>(vtx),
-                                                 static_cast<const uint4*>(triIdx), bvh->scene.u());
+    static int sms = 0;
+    if (!sms)
+    {
+        int dev = 0;
+        CL_CUDA(cudaGetDevice(&dev), err);
+        CL_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), err);
+    }
+    uint32_t blocks = std::min<uint32_t>((n + 255) / 256, uint32_t(sms) * 8u);
+    kRefitTris<<<blocks, 256, 0, st>>>(bvh->tris.as<float4>(), n, static_cast<const float4*>(vtx),
+                                       static_cast<const uint4*>(triIdx), bvh->scene.u());
     CL_CUDA(cudaGetLastError(), err);
     for (size_t d = bvh->levels.size() - 1; d-- > 0;)
     {
         uint32_t first = bvh->levels[d], count = bvh->levels[d + 1] - first;
-        kRefitLevel<<<(count + kRefitBlock - 1) / kRefitBlock, kRefitBlock, 0, st>>>(
+        uint64_t lanes = uint64_t(count) * 8u;
+        kRefitLevel<<<uint32_t((lanes + kRefitBlock - 1) / kRefitBlock), kRefitBlock, 0, st>>>(
             bvh->nodes.as<uint4>(), bvh->tris.as<const float4>(), bvh->exact.f(), first, count, bvh->scene.u());
         CL_CUDA(cudaGetLastError(), err);
     }
