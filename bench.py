@@ -398,7 +398,8 @@ def main():
         arr = film.numpy()
         cam = np.ascontiguousarray(s.camera, np.float32)
         for _ in range(args.warmup):
-            it.updateCamera(cam); it.render(1); it.readbackFramebuffer(arr)
+            it.updateCamera(cam); it.render(1); it.readbackFramebufferAsync(arr)
+        it.readbackWait()
         dist.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -406,13 +407,17 @@ def main():
         for _ in range(args.steps):
             it.updateCamera(cam)
             it.render(1)
-            it.readbackFramebuffer(arr)
+            it.readbackFramebufferAsync(arr)   # step k's copy overlaps step k+1's render
+        it.readbackWait()
         e1.record()
         torch.cuda.synchronize()
         ems = dist.max(e0.elapsed_time(e1))
         e2e = {"value": round(W * H * args.steps * dist.world / (ems * 1e-3) / 1e6, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(cam.nbytes), "d2h_bytes_per_step": int(arr.nbytes),
-               "ms_per_step": round(ems / args.steps, 3)}
+               "ms_per_step": round(ems / args.steps, 3),
+               "pipeline": "camera H2D, render, film mean resolved on the device and copied to pinned host memory "
+                           "on a copy stream (cl_readback_film_async); each step's copy overlaps the next render, "
+                           "the last one is waited for inside the timed region"}
     edit = scene_edit(it, s, args) if dist.world == 1 and not args.no_edit else None
     it.close()
 

@@ -177,6 +177,21 @@ class Integrator:
         N.call("cl_readback_film", self._h, _ptr(out), out.nbytes)
         return out
 
+    def readbackFramebufferAsync(self, out):
+        """Queues the readback of the mean radiance into `out` ((H, W, 4) float32,
+        best in page-locked memory) and returns; the copy overlaps the next
+        render.  `out` is complete after readbackWait()."""
+        w, h = self._size
+        if out.shape != (h, w, 4) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous ({h}, {w}, 4) float32 array")
+        N.call("cl_readback_film_async", self._h, _ptr(out), out.nbytes)
+        self._pending = out
+        return out
+
+    def readbackWait(self):
+        N.call("cl_readback_wait", self._h)
+        self._pending = None
+
     def readbackFilmStats(self):
         """FP64 per-pixel (sum, sumsq) of per-sample radiance, each (H*W, 3)."""
         w, h = self._size

@@ -120,6 +120,8 @@ _SIGS = {
     "cl_update_camera": [vp, ctypes.POINTER(Camera)],
     "cl_render": [vp, u32],
     "cl_readback_film": [vp, vp, ctypes.c_size_t],
+    "cl_readback_film_async": [vp, vp, ctypes.c_size_t],
+    "cl_readback_wait": [vp],
     "cl_readback_film_stats": [vp, vp, vp, ctypes.c_size_t],
     "cl_resize": [vp, u32, u32],
     "cl_get_film_size": [vp, ctypes.POINTER(u32), ctypes.POINTER(u32)],

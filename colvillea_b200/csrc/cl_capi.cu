@@ -203,6 +203,18 @@ cl_status cl_readback_film(cl_integrator* it, float* rgba, size_t bytes)
     return guarded([&](std::string* e) { return it->impl.readbackFilm(rgba, bytes, e); });
 }
 
+cl_status cl_readback_film_async(cl_integrator* it, float* rgba, size_t bytes)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.readbackFilmAsync(rgba, bytes, e); });
+}
+
+cl_status cl_readback_wait(cl_integrator* it)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.readbackWait(e); });
+}
+
 cl_status cl_readback_film_stats(cl_integrator* it, double* sum, double* sumsq, size_t count)
 {
     CL_NEED(it);

@@ -1099,7 +1099,11 @@ Integrator::Integrator(cl_integrator_type type, uint32_t w, uint32_t h, const cl
 Integrator::~Integrator()
 {
     if (graph_) cudaGraphExecDestroy(graph_);
+    if (copyStream_) cudaStreamSynchronize(copyStream_);
     if (stream_) cudaStreamSynchronize(stream_);
+    if (evResolved_) cudaEventDestroy(evResolved_);
+    if (evCopied_) cudaEventDestroy(evCopied_);
+    if (copyStream_) cudaStreamDestroy(copyStream_);
     if (evA_) cudaEventDestroy(evA_);
     if (evB_) cudaEventDestroy(evB_);
     for (auto& e : evS_)
@@ -1126,6 +1130,9 @@ cl_status Integrator::init(std::string* err)
     CL_CUDA(cudaGetDevice(&dev), err);
     CL_CUDA(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, dev), err);
     CL_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), err);
+    CL_CUDA(cudaStreamCreateWithFlags(&copyStream_, cudaStreamNonBlocking), err);
+    CL_CUDA(cudaEventCreateWithFlags(&evResolved_, cudaEventDisableTiming), err);
+    CL_CUDA(cudaEventCreateWithFlags(&evCopied_, cudaEventDisableTiming), err);
     CL_CUDA(cudaEventCreate(&evA_), err);
     CL_CUDA(cudaEventCreate(&evB_), err);
     for (auto& e : evS_) CL_CUDA(cudaEventCreate(&e), err);
@@ -2150,6 +2157,33 @@ cl_status Integrator::cacheStats(cl_guide_stats* s, std::string* err) const
     return CL_OK;
 }
 
+// Mean radiance of the film into the staging buffer (alpha 1).
+__global__ void kResolveFilm(const float4* __restrict__ film, float4* __restrict__ out, uint32_t n, float inv)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        float4 f = film[i];
+        out[i]   = make_float4(f.x * inv, f.y * inv, f.z * inv, 1.0f);
+    }
+}
+
+cl_status Integrator::resolveFilm(std::string* err)
+{
+    size_t np = size_t(W_) * H_;
+    CL_TRY(ensureFilm(err));
+    if (resolve_.bytes != np * 16)
+    {
+        CL_CUDA(cudaStreamSynchronize(copyStream_), err); // no copy may still read the old buffer
+        CL_TRY(resolve_.alloc(np * 16, err));
+    }
+    // The staging buffer is reused: the previous copy out of it must be done.
+    CL_CUDA(cudaStreamWaitEvent(stream_, evCopied_, 0), err);
+    float inv = filmSpp_ ? 1.0f / float(filmSpp_) : 0.0f;
+    kResolveFilm<<<numSMs_ * 4, 256, 0, stream_>>>(film_.as<const float4>(), resolve_.as<float4>(), uint32_t(np), inv);
+    CL_CUDA(cudaGetLastError(), err);
+    return CL_OK;
+}
+
 cl_status Integrator::readbackFilm(float* rgba, size_t bytes, std::string* err)
 {
     size_t np = size_t(W_) * H_;
@@ -2158,17 +2192,31 @@ cl_status Integrator::readbackFilm(float* rgba, size_t bytes, std::string* err)
         *err = "film buffer too small";
         return CL_ERR_INVALID_ARG;
     }
-    CL_TRY(ensureFilm(err));
-    CL_CUDA(cudaMemcpyAsync(rgba, film_.p, np * 16, cudaMemcpyDeviceToHost, stream_), err);
+    CL_TRY(resolveFilm(err));
+    CL_CUDA(cudaMemcpyAsync(rgba, resolve_.p, np * 16, cudaMemcpyDeviceToHost, stream_), err);
     CL_CUDA(cudaStreamSynchronize(stream_), err);
-    float inv = filmSpp_ ? 1.0f / float(filmSpp_) : 0.0f;
-    for (size_t i = 0; i < np; ++i)
+    return CL_OK;
+}
+
+cl_status Integrator::readbackFilmAsync(float* rgba, size_t bytes, std::string* err)
+{
+    size_t np = size_t(W_) * H_;
+    if (!rgba || bytes < np * 16)
     {
-        rgba[4 * i]     = rgba[4 * i] * inv;
-        rgba[4 * i + 1] = rgba[4 * i + 1] * inv;
-        rgba[4 * i + 2] = rgba[4 * i + 2] * inv;
-        rgba[4 * i + 3] = 1.0f;
+        *err = "film buffer too small";
+        return CL_ERR_INVALID_ARG;
     }
+    CL_TRY(resolveFilm(err));
+    CL_CUDA(cudaEventRecord(evResolved_, stream_), err);
+    CL_CUDA(cudaStreamWaitEvent(copyStream_, evResolved_, 0), err);
+    CL_CUDA(cudaMemcpyAsync(rgba, resolve_.p, np * 16, cudaMemcpyDeviceToHost, copyStream_), err);
+    CL_CUDA(cudaEventRecord(evCopied_, copyStream_), err);
+    return CL_OK;
+}
+
+cl_status Integrator::readbackWait(std::string* err)
+{
+    CL_CUDA(cudaEventSynchronize(evCopied_), err);
     return CL_OK;
 }
 

@@ -161,6 +161,8 @@ public:
     cl_status updateCamera(const cl_camera* c, std::string* err);
     cl_status render(uint32_t spp, std::string* err);
     cl_status readbackFilm(float* rgba, size_t bytes, std::string* err);
+    cl_status readbackFilmAsync(float* rgba, size_t bytes, std::string* err);
+    cl_status readbackWait(std::string* err);
     cl_status readbackFilmStats(double* sum, double* sumsq, size_t count, std::string* err);
     cl_status resize(uint32_t w, uint32_t h, std::string* err);
     cl_status resetIteration(std::string* err);
@@ -191,6 +193,7 @@ private:
     cl_status trainGuide(std::string* err);
     cl_status trainCache(std::string* err);
     cl_status ensureFilm(std::string* err);
+    cl_status resolveFilm(std::string* err);
     cl_status ensureQueues(std::string* err);
     cl_status clearFilm(std::string* err);
     cl_status captureGraph(std::string* err);
@@ -238,6 +241,11 @@ private:
 
     // Film and wavefront state.
     DevBuf film_, film64_;
+    // Film readback: mean radiance staged on the device, copied out on its own
+    // stream so that a copy overlaps the next render.
+    DevBuf       resolve_;
+    cudaStream_t copyStream_ = nullptr;
+    cudaEvent_t  evResolved_ = nullptr, evCopied_ = nullptr;
     DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
     DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_, vis_, classIdx_;
     uint32_t slots_ = 0, shadowCap_ = 0;

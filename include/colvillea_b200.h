@@ -284,6 +284,14 @@ cl_status cl_render(cl_integrator* integrator, uint32_t spp);
 /* Integrator::readbackFramebuffer (integrator.h:72): linear HDR mean radiance,
  * RGBA32F, width*height*4 floats (alpha = 1). */
 cl_status cl_readback_film(cl_integrator* integrator, float* rgba, size_t bytes);
+/* The same readback, returning once it is queued: the mean is staged on the
+ * device and copied into `rgba` on a copy stream, so that the copy overlaps
+ * the next cl_render.  `rgba` must stay valid (and is best page-locked) until
+ * cl_readback_wait returns; a later readback of either kind waits for this
+ * one's copy before reusing the staging buffer.  No counterpart in the
+ * reference. */
+cl_status cl_readback_film_async(cl_integrator* integrator, float* rgba, size_t bytes);
+cl_status cl_readback_wait(cl_integrator* integrator);
 /* FP64 film (CL_FILM_FP64): per-pixel sum and sum of squares, 3 doubles each. */
 cl_status cl_readback_film_stats(cl_integrator* integrator, double* sum, double* sumsq, size_t count);
 /* Integrator::resize / getFilmSize / resetIterationIndex (integrator.h:64,74,76). */

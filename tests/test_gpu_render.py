@@ -144,3 +144,28 @@ def test_resize_and_errors(native):
     with pytest.raises(cb.ClError):
         bad.render(1)  # nothing built yet
     bad.close()
+
+
+def test_async_readback_pipeline():
+    """cl_readback_film_async: each frame's mean arrives intact while the next
+    render runs; equal to the synchronous readback and to sum / spp."""
+    import torch
+    s = scenes.config1(0, 64, 48)
+    it = cb.load_scene(s, flags=cb.COMPAT_ALL | cb.FILM_FP64)
+    bufs = [torch.empty((48, 64, 4), dtype=torch.float32, pin_memory=True).numpy() for _ in range(3)]
+    want = []
+    for k in range(3):
+        it.render(1)
+        want.append(it.readbackFramebuffer().copy())
+        it.readbackFramebufferAsync(bufs[k])
+        if k < 2:
+            it.readbackWait()          # the next readback reuses the staging buffer anyway
+    it.render(2)                       # overlaps the last copy
+    it.readbackWait()
+    for k in range(3):
+        np.testing.assert_array_equal(bufs[k], want[k])
+    s1, _ = it.readbackFilmStats()
+    img = it.readbackFramebuffer()
+    np.testing.assert_allclose(img[..., :3].reshape(-1, 3), s1 / 5, rtol=1e-5, atol=1e-6)
+    assert np.all(img[..., 3] == 1)
+    it.close()
