@@ -35,19 +35,43 @@ struct BvhView
 {
     const uint4* __restrict__ nodes;
     const float4* __restrict__ tris;
+    // Traversal stack entries per thread: the tree's depth + 1 (a ray holds
+    // at most one pending node group per level), at most kStackDepth.  The
+    // kernels' dynamic shared memory is stackDepth * kTraceBlock * 8 bytes,
+    // so that a shallow tree leaves more of the SM's on-chip memory to L1.
+    uint32_t stackDepth;
 };
+
+__host__ __device__ constexpr size_t traceStackBytes(uint32_t depth) { return size_t(depth) * kTraceBlock * 8u; }
 
 struct TraceCounters
 {
     uint32_t nodes, tris;
 };
 
-// Exact float of byte b of `word`: PRMT builds 0x4B0000bb (= 2^23 + byte as
-// a float) and one FADD removes 2^23; both run on full-rate pipes (an I2F
-// conversion would go through the quarter-rate XU pipe).
-__device__ __forceinline__ float byteAt(uint32_t word, int b)
+// Quantised planes are decoded exactly without a conversion instruction:
+// PRMT builds 0x4B0000bb (= 2^23 + byte as a float) and a subtraction of
+// 2^23 leaves the byte (an I2F would go through the quarter-rate XU pipe).
+// Byte b of wa and of wb as 2^23 + byte (floats), for the paired plane math.
+__device__ __forceinline__ float2 bytePair(uint32_t wa, uint32_t wb, int b)
 {
-    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7440u | uint32_t(b))) - 8388608.0f;
+    return make_float2(__uint_as_float(__byte_perm(wa, 0x4B000000u, 0x7440u | uint32_t(b))),
+                       __uint_as_float(__byte_perm(wb, 0x4B000000u, 0x7440u | uint32_t(b))));
+}
+
+// Three-input minimum and maximum (sm_100 min.f32 / max.f32 with three
+// operands; exact, like the nested two-input forms).
+__device__ __forceinline__ float max3f(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
 }
 
 // Intersects the ray with the 8 children of one node; returns the hit mask:
@@ -76,29 +100,41 @@ __device__ __forceinline__ uint32_t intersectNode(const BvhView& bvh, uint32_t i
     uint32_t loxA = nx ? n3.z : n2.x, loxB = nx ? n3.w : n2.y, hixA = nx ? n2.x : n3.z, hixB = nx ? n2.y : n3.w;
     uint32_t loyA = ny ? n4.x : n2.z, loyB = ny ? n4.y : n2.w, hiyA = ny ? n2.z : n4.x, hiyB = ny ? n2.w : n4.y;
     uint32_t lozA = nz ? n4.z : n3.x, lozB = nz ? n4.w : n3.y, hizA = nz ? n3.x : n4.z, hizB = nz ? n3.y : n4.w;
-    uint32_t hits = 0;
+    // Slots b and b + 4 as one float2 pair: 2^23 + byte from PRMT, exact
+    // byte by FADD2, plane distance by FFMA2 (each lane IEEE round to
+    // nearest, so the values equal the scalar fmaf(q, scale, offset)); the
+    // slab interval by 3-input min/max.
+    const float2 bias = make_float2(-8388608.0f, -8388608.0f);
+    const float2 sX = make_float2(idx_, idx_), sY = make_float2(idy, idy), sZ = make_float2(idz, idz);
+    const float2 oX = make_float2(ox, ox), oY = make_float2(oy, oy), oZ = make_float2(oz, oz);
+    uint32_t     hitSlots = 0;
 #pragma unroll
-    for (int s = 0; s < 8; ++s)
+    for (int b = 0; b < 4; ++b)
     {
-        const int b   = s & 3;
-        uint32_t  lx  = s < 4 ? loxA : loxB, hx = s < 4 ? hixA : hixB;
-        uint32_t  ly  = s < 4 ? loyA : loyB, hy = s < 4 ? hiyA : hiyB;
-        uint32_t  lz  = s < 4 ? lozA : lozB, hz = s < 4 ? hizA : hizB;
-        float tnx = __fmaf_rn(byteAt(lx, b), idx_, ox), tfx = __fmaf_rn(byteAt(hx, b), idx_, ox);
-        float tny = __fmaf_rn(byteAt(ly, b), idy, oy), tfy = __fmaf_rn(byteAt(hy, b), idy, oy);
-        float tnz = __fmaf_rn(byteAt(lz, b), idz, oz), tfz = __fmaf_rn(byteAt(hz, b), idz, oz);
-        float tn  = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-        float tf  = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-        if (tn <= tf)
-        {
-            if (imask & (1u << s))
-                hits |= 1u << (24 + (s ^ oct));
-            else
-            {
-                uint32_t meta = (s < 4 ? n1.z : n1.w) >> (8 * b) & 0xffu;
-                hits |= (meta >> 5) << (meta & 31u);
-            }
-        }
+        float2 tnx = __ffma2_rn(__fadd2_rn(bytePair(loxA, loxB, b), bias), sX, oX);
+        float2 tfx = __ffma2_rn(__fadd2_rn(bytePair(hixA, hixB, b), bias), sX, oX);
+        float2 tny = __ffma2_rn(__fadd2_rn(bytePair(loyA, loyB, b), bias), sY, oY);
+        float2 tfy = __ffma2_rn(__fadd2_rn(bytePair(hiyA, hiyB, b), bias), sY, oY);
+        float2 tnz = __ffma2_rn(__fadd2_rn(bytePair(lozA, lozB, b), bias), sZ, oZ);
+        float2 tfz = __ffma2_rn(__fadd2_rn(bytePair(hizA, hizB, b), bias), sZ, oZ);
+        float  tn0 = max3f(tnx.x, tny.x, fmaxf(tnz.x, tmin)), tf0 = min3f(tfx.x, tfy.x, fminf(tfz.x, tmax));
+        float  tn1 = max3f(tnx.y, tny.y, fmaxf(tnz.y, tmin)), tf1 = min3f(tfx.y, tfy.y, fminf(tfz.y, tmax));
+        hitSlots |= (tn0 <= tf0 ? 1u << b : 0u) | (tn1 <= tf1 ? 1u << (b + 4) : 0u);
+    }
+    // Inner children: slot s -> key s ^ oct (bit permutation of the mask).
+    uint32_t k = hitSlots & imask;
+    k          = (oct & 1u) ? (((k & 0x55u) << 1) | ((k >> 1) & 0x55u)) : k;
+    k          = (oct & 2u) ? (((k & 0x33u) << 2) | ((k >> 2) & 0x33u)) : k;
+    k          = (oct & 4u) ? (((k & 0x0fu) << 4) | ((k >> 4) & 0x0fu)) : k;
+    uint32_t hits = k << 24;
+    // Leaf children: their triangle ranges (unary count << 5 | offset).
+    uint32_t leaf = hitSlots & ~imask;
+    while (leaf)
+    {
+        uint32_t sl   = __ffs(leaf) - 1;
+        leaf &= leaf - 1u;
+        uint32_t meta = ((sl < 4 ? n1.z : n1.w) >> (8 * (sl & 3u))) & 0xffu;
+        hits |= (meta >> 5) << (meta & 31u);
     }
     return hits;
 }
@@ -139,7 +175,7 @@ __device__ __forceinline__ void travInit(Trav& s, f3 o, f3 d, float tmin, float 
 // rays; the reference searches for the closest hit there, optix.cu:99-109,
 // which gives the same visibility).  Closest: smallest t in (tmin, tmax),
 // ties to the lower primitive id.  `stack` points at this thread's column of
-// a shared [kStackDepth][kTraceBlock] array.  Returns true when the ray is
+// a shared [bvh.stackDepth][kTraceBlock] array.  Returns true when the ray is
 // finished (s.best: primitive id or kMissPrim; s.bt, s.b1, s.b2).
 template <bool ANY, bool STATS>
 __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* stack, TraceCounters* cnt, uint32_t* err)
@@ -153,7 +189,7 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
         uint32_t child = s.ng.x + __popc(imask & ((1u << slot) - 1u));
         if (s.ng.y > 0x00ffffffu)
         {
-            if (s.sp >= kStackDepth)
+            if (s.sp >= int(bvh.stackDepth))
             {
                 atomicOr(err, 1u);
                 s.best = kMissPrim;

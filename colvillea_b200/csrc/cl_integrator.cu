@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
                                                                 uint32_t* fetch, float4* __restrict__ hitOut,
                                                                 Counters* ctr, ClassifyView cv)
 {
-    __shared__ uint2 stack[kStackDepth * kTraceBlock];
+    extern __shared__ uint2 stack[];
     const uint32_t   n = loadCount(count);
     TraceCounters    tc{0u, 0u};
     for (;;)
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
 template <bool DL, bool STATS>
 __global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
 {
-    __shared__ uint2 stack[kStackDepth * kTraceBlock];
+    extern __shared__ uint2 stack[];
     const uint32_t   n = loadCount(&P.q.ctr->shadowCount) * (DL ? 2u : 1u);
     TraceCounters    tc{0u, 0u};
     for (;;)
@@ -1012,7 +1012,7 @@ __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const floa
                                                          const float4* __restrict__ D, uint32_t n,
                                                          uint8_t* __restrict__ occ, uint32_t* err)
 {
-    __shared__ uint2 stack[kStackDepth * kTraceBlock];
+    extern __shared__ uint2 stack[];
     uint32_t         i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4        o = O[i], d = D[i];
@@ -1139,7 +1139,10 @@ cl_status Integrator::init(std::string* err)
     CL_CUDA(cudaMallocHost((void**)&hostWp_, sizeof(WaveParams)), err);
     CL_CUDA(cudaMallocHost((void**)&hostCount_, 64), err);
     int b = 0;
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTraceClosest<false, true>, kTraceBlock, 0), err);
+    // Occupancy at the deepest supported stack (the launches use less).
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTraceClosest<false, true>, kTraceBlock,
+                                                          traceStackBytes(kStackDepth)),
+            err);
     traceBlocks_ = std::max(1, b) * numSMs_;
     bool dl = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)shadeKernel(dl, 2, cfg_.flags), 128, 0),
@@ -1652,6 +1655,12 @@ cl_status Integrator::ensureQueues(std::string* err)
     return CL_OK;
 }
 
+BvhView Integrator::bvhView() const
+{
+    return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(),
+                   std::min<uint32_t>(bvh_.depth + 1u, uint32_t(kStackDepth))};
+}
+
 ClassifyView Integrator::classifyView() const
 {
     return ClassifyView{triIdx_.as<const uint4>(), mats_.as<const float4>(), classIdx_.u(), slots_};
@@ -1660,8 +1669,7 @@ ClassifyView Integrator::classifyView() const
 Params Integrator::params() const
 {
     Params P{};
-    P.sc.bvh.nodes = bvh_.nodes.as<const uint4>();
-    P.sc.bvh.tris  = bvh_.tris.as<const float4>();
+    P.sc.bvh       = bvhView();
     P.sc.triIdx    = triIdx_.as<const uint4>();
     P.sc.vtx       = vtx_.as<const float4>();
     P.sc.mats      = mats_.as<const float4>();
@@ -1731,10 +1739,10 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     const bool st = cfg_.flags & CL_TRACE_STATS;
     if (profile) CL_CUDA(cudaEventRecord(evS_[0], stream_), err);
     if (st)
-        kTraceClosest<true, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+        kTraceClosest<true, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
             P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur], &c->fetchTrace, P.q.hit, c, classifyView());
     else
-        kTraceClosest<false, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
+        kTraceClosest<false, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
             P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur], &c->fetchTrace, P.q.hit, c, classifyView());
     if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
     const uint32_t gmask = guide_ ? guideCfg_.class_mask : 0u;
@@ -1755,13 +1763,13 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
         shadeKernel(dl, m, cfg_.flags, m < 3 && ((gmask >> m) & 1u))<<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
     if (profile) CL_CUDA(cudaEventRecord(evS_[2], stream_), err);
     if (dl && st)
-        kTraceShadow<true, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
+        kTraceShadow<true, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
     else if (dl)
-        kTraceShadow<true, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
+        kTraceShadow<true, false><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
     else if (st)
-        kTraceShadow<false, true><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
+        kTraceShadow<false, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
     else
-        kTraceShadow<false, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(P);
+        kTraceShadow<false, false><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
     if (dl)
         kShadowResolve<true><<<shadowBlocks_, 128, 0, stream_>>>(P, cur);
     else
@@ -2354,8 +2362,8 @@ cl_status Integrator::traceRays(const float* rays, uint32_t n, float* t, uint32_
         Counters c0{};
         c0.rayCount[0] = m;
         CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
-        kTraceClosest<false, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
-            BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, rqO_[0].as<float4>(),
+        kTraceClosest<false, false><<<traceBlocks_, kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
+            bvhView(), rqO_[0].as<float4>(),
             rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc, ClassifyView{});
         CL_CUDA(cudaGetLastError(), err);
         CL_CUDA(cudaMemcpyAsync(h.data(), hit_.p, m * 16, cudaMemcpyDeviceToHost, stream_), err);
@@ -2407,8 +2415,8 @@ cl_status Integrator::occludedRays(const float* rays, uint32_t n, uint8_t* occ, 
     CL_CUDA(cudaMemcpyAsync(o.p, ho.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaMemcpyAsync(d.p, hd.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaMemsetAsync(ctr_.p, 0, sizeof(Counters), stream_), err);
-    kOccluded<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, stream_>>>(
-        BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, o.as<float4>(), d.as<float4>(), n,
+    kOccluded<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
+        bvhView(), o.as<float4>(), d.as<float4>(), n,
         r.as<uint8_t>(), &ctr_.as<Counters>()->error);
     CL_CUDA(cudaGetLastError(), err);
     CL_CUDA(cudaMemcpyAsync(occ, r.p, n, cudaMemcpyDeviceToHost, stream_), err);
@@ -2446,8 +2454,8 @@ cl_status Integrator::traceStats(const float* rays, uint32_t n, uint64_t* nodes,
         Counters c0{};
         c0.rayCount[0] = m;
         CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
-        kTraceClosest<true, false><<<traceBlocks_, kTraceBlock, 0, stream_>>>(
-            BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>()}, rqO_[0].as<float4>(),
+        kTraceClosest<true, false><<<traceBlocks_, kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
+            bvhView(), rqO_[0].as<float4>(),
             rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc, ClassifyView{});
         CL_CUDA(cudaGetLastError(), err);
         Counters ch;

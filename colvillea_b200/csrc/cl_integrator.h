@@ -200,6 +200,7 @@ private:
     cl_status launchWave(int cur, bool profile, std::string* err);
     Params    params() const;
     ClassifyView classifyView() const;
+    BvhView      bvhView() const;
 
     cl_integrator_type type_;
     uint32_t           W_, H_;
