@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
     ap.add_argument("--no-relmse", action="store_true", help="skip the guided-vs-plain equal-time relMSE")
     ap.add_argument("--no-edit", action="store_true", help="skip the shape-edit (refit vs rebuild) measurement")
+    ap.add_argument("--extended", action="store_true",
+                    help="cfg4 radiance cache + guiding and cfg5 (4K, both networks) against FP64 references")
+    ap.add_argument("--ext-ref-spp4", type=int, default=65536, help="spp of the cfg4 reference for --extended")
+    ap.add_argument("--ext-ref-spp5", type=int, default=2048, help="spp of the cfg5 reference for --extended")
+    ap.add_argument("--ext-spp5", type=int, default=256, help="neural spp on cfg5 (training included)")
     ap.add_argument("--profile-nets", choices=["guide", "cache"], default=None,
                     help="short workload for ncu: cfg3 with guiding or cfg4 with the radiance cache, "
                          "2 training spp + 2 spp")
@@ -185,9 +190,9 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the closest-hit kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "trace_closest_cfg2.json")
+def ncu_traffic(config=2):
+    """Per-ray DRAM bytes of the closest-hit kernel from the committed ncu summary of this config, if any."""
+    p = os.path.join(ROOT, "profiles", f"trace_closest_cfg{config}.json")
     if os.path.exists(p):
         d = json.load(open(p))
         return d.get("dram_bytes_per_ray")
@@ -294,6 +299,51 @@ def scene_edit(it, s, args, spp=4):
     return out
 
 
+def run_extended(args):
+    """The neural configurations not in the default line (one JSON line):
+      cfg4: the caustic scene with the radiance cache plus guiding, and the
+            cache alone, at equal time against plain, relMSE and bias
+            against a 65,536-spp FP64 plain reference;
+      cfg5: 3840x2160, depth 16, the instanced terrain scene with guiding and
+            the radiance cache both on: equal-time relMSE against plain
+            (FP64 reference), and the guiding network's inference throughput."""
+    import colvillea_b200 as cb
+    from colvillea_b200 import evaluate, scenes
+    rnd = lambda v: [round(x, 6) for x in v] if isinstance(v, list) else (round(v, 6) if isinstance(v, float) else v)
+    peak = None
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        peak = float(json.load(open(p)).get("bf16_tflops", 0)) or None
+    out = {"extended": True}
+    s4 = scenes.config4(0)
+    t0 = time.perf_counter()
+    ref4 = evaluate.reference(s4, args.ext_ref_spp4)
+    t4 = time.perf_counter() - t0
+    for name, g in (("cfg4_cache_guided", cb.GuideConfig()), ("cfg4_cache", None)):
+        r = evaluate.equal_time(s4, ref4, args.relmse_spp, seeds=args.relmse_seeds, guide=g,
+                                cache=cb.RadianceCacheConfig())
+        out[name] = {"reference": f"plain, corrected estimator, {args.ext_ref_spp4} spp, FP64 film ({t4:.1f} s)",
+                     "networks": "radiance cache + guiding" if g is not None else "radiance cache",
+                     **{k: rnd(v) for k, v in r.items()}}
+    s5 = scenes.config5(0)
+    t0 = time.perf_counter()
+    ref5 = evaluate.reference(s5, args.ext_ref_spp5)
+    t5 = time.perf_counter() - t0
+    g5 = cb.GuideConfig()
+    r5 = evaluate.equal_time(s5, ref5, args.ext_spp5, seeds=args.relmse_seeds, guide=g5, cache=cb.RadianceCacheConfig())
+    mlp = evaluate.mlp_throughput(s5, g5)
+    out["cfg5_guided_cached"] = {
+        "workload": f"cfg5: {s5.width}x{s5.height}, max depth {s5.max_depth}, {s5.num_triangles} triangles "
+                    f"({len(s5.instances)} instances), 4096x2048 HDRI + directional; guiding + radiance cache "
+                    f"{args.ext_spp5} spp incl. training; plain at the same device time",
+        "reference": f"plain, corrected estimator, {args.ext_ref_spp5} spp, FP64 film ({t5:.1f} s)",
+        **{k: rnd(v) for k, v in r5.items()},
+        "mlp": {**{k: rnd(v) for k, v in mlp.items()}, "bf16_peak_tflops": peak,
+                "infer_frac_of_peak": round(mlp["infer_tflops"] / peak, 4) if peak and mlp["infer_tflops"] else None}}
+    print(json.dumps(out))
+    return 0
+
+
 def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
@@ -342,6 +392,8 @@ def main():
         return run_profile(args)
     if args.profile_nets:
         return run_profile_nets(args)
+    if args.extended:
+        return run_extended(args)
     import numpy as np
     import torch
     dist = Dist(args.gpus)
@@ -431,7 +483,7 @@ def main():
     bytes_per_ray = RAY_IN + HIT_OUT + NODE_BYTES * nodes_per_ray + TRI_BYTES * tris_per_ray
     achieved = bytes_per_ray * rays_c / (ms_trace * 1e-3) / 1e9 if ms_trace > 0 else None
     peak, peak_kind = peaks()
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(args.config)
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
