@@ -448,6 +448,31 @@ __global__ void kCollapse(CollapseArgs A, const uint2* __restrict__ tasks, uint3
             ch[best]   = A.left[r];
             ch[cnt++]  = A.right[r];
         }
+        // Slots still free: split the largest small leaves (2-3 triangles)
+        // into smaller ones, so that their triangles get tighter boxes.
+        while (cnt < 8)
+        {
+            int   best     = -1;
+            float bestArea = -1.0f;
+            for (int k = 0; k < cnt; ++k)
+            {
+                uint32_t r = ch[k];
+                if (r & kLeafFlag) continue;
+                float dx = A.nhi[3 * size_t(r)] - A.nlo[3 * size_t(r)];
+                float dy = A.nhi[3 * size_t(r) + 1] - A.nlo[3 * size_t(r) + 1];
+                float dz = A.nhi[3 * size_t(r) + 2] - A.nlo[3 * size_t(r) + 2];
+                float area = dx * dy + dy * dz + dz * dx;
+                if (area > bestArea)
+                {
+                    bestArea = area;
+                    best     = k;
+                }
+            }
+            if (best < 0) break;
+            uint32_t r = ch[best];
+            ch[best]   = A.left[r];
+            ch[cnt++]  = A.right[r];
+        }
     }
 
     // Child boxes, parent box (widened by the margin).
