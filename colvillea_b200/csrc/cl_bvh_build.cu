@@ -242,9 +242,16 @@ __global__ void kPlocInit(uint32_t n, const uint32_t* __restrict__ ids, const fl
     bhi[i]     = make_float4(hi[3 * size_t(t)], hi[3 * size_t(t) + 1], hi[3 * size_t(t) + 2], 0.0f);
 }
 
-__global__ void __launch_bounds__(kPlocBlock) kPlocNearest(uint32_t m, const float4* __restrict__ blo,
+// The cluster count m lives in device memory (mDev), so that iterations run
+// without a host round trip; launches are sized for an upper bound of m and
+// threads past m return.  With m <= 1 the clustering is done and the
+// iteration changes nothing.
+__global__ void __launch_bounds__(kPlocBlock) kPlocNearest(const uint32_t* __restrict__ mDev,
+                                                           const float4* __restrict__ blo,
                                                            const float4* __restrict__ bhi, uint32_t* __restrict__ nn)
 {
+    const uint32_t m = *mDev;
+    if (m <= 1u) return;
     __shared__ float4 slo[kPlocBlock + 2 * kPlocRadius], shi[kPlocBlock + 2 * kPlocRadius];
     const int b0 = int(blockIdx.x) * kPlocBlock - kPlocRadius;
     for (int k = threadIdx.x; k < kPlocBlock + 2 * kPlocRadius; k += kPlocBlock)
@@ -287,13 +294,19 @@ struct PlocTree
     uint32_t* nodeCounter;
 };
 
-__global__ void kPlocMerge(uint32_t m, const uint32_t* __restrict__ C, const float4* __restrict__ blo,
-                           const float4* __restrict__ bhi, const uint32_t* __restrict__ nn, uint32_t* __restrict__ valid,
-                           uint32_t* __restrict__ C2, float4* __restrict__ blo2, float4* __restrict__ bhi2, PlocTree T,
-                           uint32_t maxInner)
+__global__ void kPlocMerge(const uint32_t* __restrict__ mDev, uint32_t mBound, const uint32_t* __restrict__ C,
+                           const float4* __restrict__ blo, const float4* __restrict__ bhi,
+                           const uint32_t* __restrict__ nn, uint32_t* __restrict__ valid, uint32_t* __restrict__ C2,
+                           float4* __restrict__ blo2, float4* __restrict__ bhi2, PlocTree T, uint32_t maxInner)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
+    const uint32_t m = *mDev;
+    uint32_t       i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mBound) return;
+    if (i >= m || m <= 1u)
+    {
+        valid[i] = 0u; // outside the live range: the scan over mBound counts nothing here
+        return;
+    }
     uint32_t j      = nn[i];
     bool     mutual = nn[j] == i;
     if (mutual && j < i)
@@ -337,17 +350,27 @@ __global__ void kPlocMerge(uint32_t m, const uint32_t* __restrict__ C, const flo
     bhi2[i]     = hi;
 }
 
-__global__ void kPlocScatter(uint32_t m, const uint32_t* __restrict__ valid, const uint32_t* __restrict__ pos,
-                             const uint32_t* __restrict__ C2, const float4* __restrict__ blo2,
-                             const float4* __restrict__ bhi2, uint32_t* __restrict__ C, float4* __restrict__ blo,
-                             float4* __restrict__ bhi)
+__global__ void kPlocScatter(const uint32_t* __restrict__ mDev, const uint32_t* __restrict__ valid,
+                             const uint32_t* __restrict__ pos, const uint32_t* __restrict__ C2,
+                             const float4* __restrict__ blo2, const float4* __restrict__ bhi2,
+                             uint32_t* __restrict__ C, float4* __restrict__ blo, float4* __restrict__ bhi)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m || !valid[i]) return;
+    const uint32_t m = *mDev;
+    uint32_t       i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m <= 1u || i >= m || !valid[i]) return;
     uint32_t d = pos[i];
     C[d]       = C2[i];
     blo[d]     = blo2[i];
     bhi[d]     = bhi2[i];
+}
+
+// Next iteration's cluster count: the survivors of this one.
+__global__ void kPlocCount(const uint32_t* __restrict__ mDev, uint32_t* __restrict__ mNext,
+                           const uint32_t* __restrict__ valid, const uint32_t* __restrict__ pos)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t m = *mDev;
+    *mNext     = m <= 1u ? m : pos[m - 1] + valid[m - 1];
 }
 
 struct CollapseArgs
@@ -626,6 +649,47 @@ __global__ void kCollapse(CollapseArgs A, const uint2* __restrict__ tasks, uint3
     np[4]     = make_uint4(qhi[1][0], qhi[1][1], qhi[2][0], qhi[2][1]);
 }
 
+// Validation of a built tree (error bits: 1 exponent outside 1..254, 2 child
+// index beyond the node count, 4 leaf triangle range outside the node's 24 or
+// the triangle count, 8 triangle ids not a permutation of 0..n-1).
+__global__ void kValidateNodes(const uint4* __restrict__ nodes, uint32_t numNodes, uint32_t n, uint32_t* err)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numNodes) return;
+    uint4    n0 = nodes[size_t(i) * 5], n1 = nodes[size_t(i) * 5 + 1];
+    uint32_t imask = n0.w >> 24, bits = 0u;
+    for (int a = 0; a < 3; ++a)
+    {
+        uint32_t e = (n0.w >> (8 * a)) & 0xffu;
+        if (e < 1u || e > 254u) bits |= 1u;
+    }
+    if (imask && uint64_t(n1.x) + __popc(imask) > numNodes) bits |= 2u;
+    for (int sl = 0; sl < 8; ++sl)
+    {
+        if (imask & (1u << sl)) continue;
+        uint32_t meta = ((sl < 4 ? n1.z : n1.w) >> (8 * (sl & 3))) & 0xffu;
+        if (!meta) continue;
+        uint32_t off = meta & 31u, unary = meta >> 5;
+        uint32_t cnt = unary == 1u ? 1u : unary == 3u ? 2u : unary == 7u ? 3u : 99u;
+        if (cnt == 99u || off + cnt > 24u || uint64_t(n1.y) + off + cnt > n) bits |= 4u;
+    }
+    if (bits) atomicOr(err, bits);
+}
+
+__global__ void kValidateTris(const float4* __restrict__ tris, uint32_t n, uint32_t* __restrict__ seen, uint32_t* err)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t id = __float_as_uint(tris[size_t(i) * 3].w);
+    if (id >= n)
+    {
+        atomicOr(err, 8u);
+        return;
+    }
+    uint32_t bit = 1u << (id & 31u);
+    if (atomicOr(seen + (id >> 5), bit) & bit) atomicOr(err, 8u);
+}
+
 } // namespace
 
 cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err)
@@ -700,23 +764,34 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
         CL_CUDA(cudaMemsetAsync(ctr.p, 0, 16, st), err);
         PlocTree T{left.u(), right.u(), nlo.f(), nhi.f(), count.u(), ctr.u()};
         kPlocInit<<<blocks, 256, 0, st>>>(n, ids2.u(), lo.f(), hi.f(), C.u(), blo.as<float4>(), bhi.as<float4>());
+        // The cluster count stays on the device (two words, this iteration's
+        // and the next's); the host reads it every kPlocCheck iterations to
+        // size the launches and to stop.
+        constexpr int kPlocCheck = 6;
+        DevBuf        mbuf;
+        CL_TRY(mbuf.alloc(8, err));
+        CL_CUDA(cudaMemcpyAsync(mbuf.p, &n, 4, cudaMemcpyHostToDevice, st), err);
         uint32_t m = n, iters = 0;
+        int      cur = 0;
         while (m > 1 && iters < 4096)
         {
-            uint32_t g = (m + kPlocBlock - 1) / kPlocBlock;
-            kPlocNearest<<<g, kPlocBlock, 0, st>>>(m, blo.as<float4>(), bhi.as<float4>(), nnb.u());
-            kPlocMerge<<<g, kPlocBlock, 0, st>>>(m, C.u(), blo.as<float4>(), bhi.as<float4>(), nnb.u(), valid.u(),
-                                                 C2.u(), blo2.as<float4>(), bhi2.as<float4>(), T, n - 1);
-            CL_CUDA(cub::DeviceScan::ExclusiveSum(scanTmp.p, scanBytes, valid.u(), pos.u(), int(m), st), err);
-            kPlocScatter<<<g, kPlocBlock, 0, st>>>(m, valid.u(), pos.u(), C2.u(), blo2.as<float4>(), bhi2.as<float4>(),
-                                                   C.u(), blo.as<float4>(), bhi.as<float4>());
+            uint32_t g = (m + kPlocBlock - 1) / kPlocBlock; // m: upper bound of the device count
+            for (int k = 0; k < kPlocCheck; ++k)
+            {
+                const uint32_t* md = mbuf.u() + cur;
+                kPlocNearest<<<g, kPlocBlock, 0, st>>>(md, blo.as<float4>(), bhi.as<float4>(), nnb.u());
+                kPlocMerge<<<g, kPlocBlock, 0, st>>>(md, m, C.u(), blo.as<float4>(), bhi.as<float4>(), nnb.u(),
+                                                     valid.u(), C2.u(), blo2.as<float4>(), bhi2.as<float4>(), T, n - 1);
+                CL_CUDA(cub::DeviceScan::ExclusiveSum(scanTmp.p, scanBytes, valid.u(), pos.u(), int(m), st), err);
+                kPlocScatter<<<g, kPlocBlock, 0, st>>>(md, valid.u(), pos.u(), C2.u(), blo2.as<float4>(),
+                                                       bhi2.as<float4>(), C.u(), blo.as<float4>(), bhi.as<float4>());
+                kPlocCount<<<1, 32, 0, st>>>(md, mbuf.u() + (cur ^ 1), valid.u(), pos.u());
+                cur ^= 1;
+                ++iters;
+            }
             CL_CUDA(cudaGetLastError(), err);
-            uint32_t tail[2];
-            CL_CUDA(cudaMemcpyAsync(&tail[0], pos.u() + (m - 1), 4, cudaMemcpyDeviceToHost, st), err);
-            CL_CUDA(cudaMemcpyAsync(&tail[1], valid.u() + (m - 1), 4, cudaMemcpyDeviceToHost, st), err);
+            CL_CUDA(cudaMemcpyAsync(&m, mbuf.u() + cur, 4, cudaMemcpyDeviceToHost, st), err);
             CL_CUDA(cudaStreamSynchronize(st), err);
-            m = tail[0] + tail[1];
-            ++iters;
         }
         if (m == 1)
         {
@@ -830,55 +905,28 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     // refit allocates nothing.
     CL_TRY(out->exact.alloc(size_t(out->numNodes) * 24, err));
     CL_TRY(out->scene.alloc(64, err));
-    // Host validation of every index the traversal kernels will follow.
+    // Validation of every index the traversal kernels will follow, on the
+    // device; one error word comes back.
     {
-        std::vector<uint32_t> h(size_t(out->numNodes) * 20);
-        CL_CUDA(cudaMemcpy(h.data(), out->nodes.p, h.size() * 4, cudaMemcpyDeviceToHost), err);
-        for (uint32_t i = 0; i < out->numNodes; ++i)
+        DevBuf verr, seen;
+        CL_TRY(verr.alloc(4, err));
+        CL_TRY(seen.alloc((size_t(n) + 31) / 32 * 4, err));
+        CL_CUDA(cudaMemsetAsync(verr.p, 0, 4, st), err);
+        CL_CUDA(cudaMemsetAsync(seen.p, 0, (size_t(n) + 31) / 32 * 4, st), err);
+        kValidateNodes<<<(out->numNodes + 255) / 256, 256, 0, st>>>(out->nodes.as<const uint4>(), out->numNodes, n,
+                                                                       verr.u());
+        kValidateTris<<<(n + 255) / 256, 256, 0, st>>>(out->tris.as<const float4>(), n, seen.u(), verr.u());
+        CL_CUDA(cudaGetLastError(), err);
+        uint32_t bad = 0;
+        CL_CUDA(cudaMemcpyAsync(&bad, verr.p, 4, cudaMemcpyDeviceToHost, st), err);
+        CL_CUDA(cudaStreamSynchronize(st), err);
+        if (bad)
         {
-            const uint32_t* q = &h[size_t(i) * 20];
-            uint32_t imask = q[3] >> 24, cb = q[4], tb = q[5];
-            for (int a = 0; a < 3; ++a)
-            {
-                uint32_t e = (q[3] >> (8 * a)) & 0xffu;
-                if (e < 1 || e > 254)
-                {
-                    *err = "BVH validation: bad exponent";
-                    return CL_ERR_STATE;
-                }
-            }
-            if (imask && uint64_t(cb) + __builtin_popcount(imask) > out->numNodes)
-            {
-                *err = "BVH validation: child index out of range";
-                return CL_ERR_STATE;
-            }
-            for (int sl = 0; sl < 8; ++sl)
-            {
-                if (imask & (1u << sl)) continue;
-                uint32_t meta = (q[6 + (sl >> 2)] >> (8 * (sl & 3))) & 0xffu;
-                if (!meta) continue;
-                uint32_t off = meta & 31u, unary = meta >> 5;
-                uint32_t cnt = unary == 1u ? 1u : unary == 3u ? 2u : unary == 7u ? 3u : 99u;
-                if (cnt == 99u || off + cnt > 24u || uint64_t(tb) + off + cnt > n)
-                {
-                    *err = "BVH validation: leaf triangle range out of bounds";
-                    return CL_ERR_STATE;
-                }
-            }
-        }
-        std::vector<float> t(size_t(n) * 12);
-        CL_CUDA(cudaMemcpy(t.data(), out->tris.p, t.size() * 4, cudaMemcpyDeviceToHost), err);
-        std::vector<uint8_t> seen(n, 0);
-        for (uint32_t i = 0; i < n; ++i)
-        {
-            uint32_t id;
-            memcpy(&id, &t[size_t(i) * 12 + 3], 4);
-            if (id >= n || seen[id])
-            {
-                *err = "BVH validation: triangle ids are not a permutation";
-                return CL_ERR_STATE;
-            }
-            seen[id] = 1;
+            *err = (bad & 1u)   ? "BVH validation: bad exponent"
+                   : (bad & 2u) ? "BVH validation: child index out of range"
+                   : (bad & 4u) ? "BVH validation: leaf triangle range out of bounds"
+                                : "BVH validation: triangle ids are not a permutation";
+            return CL_ERR_STATE;
         }
     }
     if (depth + 1 > uint32_t(kStackDepth))
