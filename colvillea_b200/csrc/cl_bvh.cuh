@@ -28,6 +28,12 @@
 namespace clb
 {
 constexpr int kStackDepth    = 24; // bound checked against the built tree depth
+// Leaf triangles tested per traversal step.  A node's triangles are tested
+// one per step and the next node is visited only after them, so the visit
+// order is unchanged; but a lane with a long leaf no longer holds its warp in
+// a loop while the other lanes wait: they take their own node steps meanwhile
+// (1 was faster than 2, 4, 8 or all at once on configs 2 and 5).
+constexpr int kTrisPerStep = 1;
 constexpr int kTraceBlock    = 128;
 constexpr uint32_t kMissPrim = 0xffffffffu;
 
@@ -139,8 +145,8 @@ __device__ __forceinline__ uint32_t intersectNode(const BvhView& bvh, uint32_t i
     return hits;
 }
 
-// Per-ray traversal state, advanced one node (plus that node's triangles) per
-// step so that a warp can refill lanes whose ray finished.
+// Per-ray traversal state, advanced one step at a time: a node test (when no
+// triangle of the previous node is pending) and one triangle test.
 struct Trav
 {
     RayPre   pre;
@@ -180,7 +186,7 @@ __device__ __forceinline__ void travInit(Trav& s, f3 o, f3 d, float tmin, float 
 template <bool ANY, bool STATS>
 __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* stack, TraceCounters* cnt, uint32_t* err)
 {
-    if (s.ng.y > 0x00ffffffu)
+    if (s.tg.y == 0u && s.ng.y > 0x00ffffffu)
     {
         uint32_t key = __ffs(s.ng.y >> 24) - 1;
         s.ng.y &= ~(1u << (24 + key));
@@ -204,7 +210,7 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
         s.ng = make_uint2(cb, (hits & 0xff000000u) | im);
         s.tg = make_uint2(tb, hits & 0x00ffffffu);
     }
-    while (s.tg.y)
+    for (int tk = 0; tk < kTrisPerStep && s.tg.y; ++tk)
     {
         uint32_t k = __ffs(s.tg.y) - 1;
         s.tg.y &= ~(1u << k);
@@ -235,7 +241,7 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
             }
         }
     }
-    if (s.ng.y <= 0x00ffffffu)
+    if (s.tg.y == 0u && s.ng.y <= 0x00ffffffu)
     {
         if (s.sp == 0) return true;
         --s.sp;
