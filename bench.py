@@ -108,18 +108,30 @@ def workload_desc(s):
 
 
 class Dist:
-    def __init__(self, gpus):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE).  NCCL
+    with CUDA tensors on GPUs; gloo with CPU tensors where CUDA is absent (the
+    multi-process tests on CPU).  The job is replicas: no data-path collective,
+    only a barrier and the max-over-ranks timing."""
+
+    def __init__(self, gpus, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = None
         if self.world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local))
+            backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            timeout = datetime.timedelta(seconds=300)
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.device = torch.device("cuda", self.local)
+                dist.init_process_group("nccl", timeout=timeout, device_id=self.device)
+            else:
+                self.device = torch.device("cpu")
+                dist.init_process_group(backend, timeout=timeout)
             self.pg = dist
 
     def barrier(self):
@@ -130,9 +142,22 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([float(x)], device="cuda")
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
+
+    def sum(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def job_rate(self, units, ms):
+        """Whole-job throughput: the units all ranks processed over the
+        slowest rank's time (per second)."""
+        return self.sum(units) / (self.max(ms) * 1e-3)
 
     def close(self):
         if self.pg:
@@ -439,9 +464,10 @@ def main():
     torch.cuda.synchronize()
     clk = clocks.stop()
     dist.barrier()
-    ms = dist.max(ev0.elapsed_time(ev1))
-    paths = W * H * args.steps * dist.world
-    value = paths / (ms * 1e-3) / 1e6
+    ms_rank = ev0.elapsed_time(ev1)
+    value = dist.job_rate(W * H * args.steps, ms_rank) / 1e6
+    mrays = dist.job_rate(rays_c + rays_s, ms_rank) / 1e6
+    ms = dist.max(ms_rank)
 
     # End to end through the public API: camera in (host), render, film out to pinned host memory.
     e2e = None
@@ -463,8 +489,10 @@ def main():
         it.readbackWait()
         e1.record()
         torch.cuda.synchronize()
-        ems = dist.max(e0.elapsed_time(e1))
-        e2e = {"value": round(W * H * args.steps * dist.world / (ems * 1e-3) / 1e6, 4), "unit": UNIT,
+        ems_rank = e0.elapsed_time(e1)
+        e2e_value = dist.job_rate(W * H * args.steps, ems_rank) / 1e6
+        ems = dist.max(ems_rank)
+        e2e = {"value": round(e2e_value, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(cam.nbytes), "d2h_bytes_per_step": int(arr.nbytes),
                "ms_per_step": round(ems / args.steps, 3),
                "pipeline": "camera H2D, render, film mean resolved on the device and copied to pinned host memory "
@@ -489,7 +517,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {**workload_desc(s), "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"},
-        "mrays_per_s": round((rays_c + rays_s) * dist.world / (ms * 1e-3) / 1e6, 2),
+        "mrays_per_s": round(mrays, 2),
         "stage_ms_per_step": {"trace": round(ms_trace / args.steps, 3), "shade": round(ms_shade / args.steps, 3),
                               "shadow": round(ms_shadow / args.steps, 3),
                               "device_total": round(ms_dev / args.steps, 3)},
