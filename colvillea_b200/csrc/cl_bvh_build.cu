@@ -7,10 +7,11 @@
 //   3. binary tree by PLOC clustering over the Morton order (Meister and
 //      Bittner 2018), SAH-quality at LBVH speed; the binary radix tree of
 //      Karras (HPG 2012) with bottom-up boxes is kept as a fallback;
-//   4. top-down collapse to 8-wide nodes, one level per launch: each wide
-//      node greedily opens its largest-area child with more than 3 triangles
-//      until it has 8 children; children with at most 3 triangles become
-//      leaf slots; slots are assigned by octant; child boxes are quantised to
+//   4. surface-area-optimal collapse to 8-wide nodes (Ylitie, Karras and
+//      Laine, HPG 2017): slot costs bottom up over the binary tree, then one
+//      level of wide nodes per launch, each taking the children that the
+//      costs' minima give it; subtrees of at most 3 triangles become leaf
+//      slots; slots are assigned by octant; child boxes are quantised to
 //      8 bits per plane, rounded outwards around a widened parent box.
 #include "cl_bvh.cuh"
 #include "cl_internal.h"
@@ -373,6 +374,95 @@ __global__ void kPlocCount(const uint32_t* __restrict__ mDev, uint32_t* __restri
     *mNext     = m <= 1u ? m : pos[m - 1] + valid[m - 1];
 }
 
+// ---------------------------------------------------------------------------
+// Surface-area-optimal collapse (Ylitie, Karras and Laine, "Efficient
+// incoherent ray traversal on GPUs through compressed wide BVHs", HPG 2017):
+// cost(n, i), i = 1..8, is the smallest surface-area cost of representing the
+// binary subtree of n with at most i slots of a wide node.
+//   dist(n, j)  = min over k of cost(left, k) + cost(right, j - k)
+//   cost(n, 1)  = A(n) c_tri |T(n)|          if |T(n)| <= 3 (a leaf slot)
+//               = dist(n, 8) + A(n) c_node   otherwise (a wide node)
+//   cost(n, i)  = min(cost(n, i - 1), dist(n, i))
+// A triangle costs A(t) c_tri for any i.  Computed bottom up (the second
+// child to arrive at a node computes it); kCollapse then distributes each
+// wide node's 8 slots by the same minima.
+// ---------------------------------------------------------------------------
+constexpr float kCostNode = 1.0f; // a wide-node visit
+constexpr float kCostTri  = 1.2f; // a triangle test, relative to a node visit (measured: 0.15-1.2)
+
+__device__ __forceinline__ float halfArea(const float* l, const float* h)
+{
+    float dx = h[0] - l[0], dy = h[1] - l[1], dz = h[2] - l[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__global__ void kDpParents(uint32_t ni, const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                           uint32_t* __restrict__ parent, uint32_t* __restrict__ leafParent)
+{
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ni) return;
+    uint32_t c[2] = {left[k], right[k]};
+    for (int q = 0; q < 2; ++q)
+    {
+        if (c[q] & kLeafFlag)
+            leafParent[c[q] & ~kLeafFlag] = k;
+        else
+            parent[c[q]] = k;
+    }
+}
+
+// Slot costs of a child reference: a triangle's for every i, else cost[].
+__device__ __forceinline__ void dpRefCosts(uint32_t r, const float* lo, const float* hi, const uint32_t* ids,
+                                           const float* cost, float c[8])
+{
+    if (r & kLeafFlag)
+    {
+        uint32_t t = ids[r & ~kLeafFlag];
+        float    a = halfArea(lo + 3 * size_t(t), hi + 3 * size_t(t)) * kCostTri;
+        for (int i = 0; i < 8; ++i) c[i] = a;
+    }
+    else
+        for (int i = 0; i < 8; ++i) c[i] = __ldcg(cost + 8 * size_t(r) + i);
+}
+
+__global__ void kDpCosts(uint32_t n, const uint32_t* __restrict__ leafParent, const uint32_t* __restrict__ parent,
+                         const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                         const float* __restrict__ lo, const float* __restrict__ hi, const uint32_t* __restrict__ ids,
+                         const float* __restrict__ nlo, const float* __restrict__ nhi,
+                         const uint32_t* __restrict__ count, float* cost, uint32_t* arrive)
+{
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint32_t node = leafParent[j];
+    while (node != 0xffffffffu)
+    {
+        __threadfence();
+        if (atomicAdd(&arrive[node], 1u) == 0u) return;
+        __threadfence();
+        float cl[8], cr[8];
+        dpRefCosts(left[node], lo, hi, ids, cost, cl);
+        dpRefCosts(right[node], lo, hi, ids, cost, cr);
+        float dist[9];
+        for (int jj = 2; jj <= 8; ++jj)
+        {
+            float d = FLT_MAX;
+            for (int k = 1; k < jj; ++k) d = fminf(d, cl[k - 1] + cr[jj - k - 1]);
+            dist[jj] = d;
+        }
+        float    A   = halfArea(nlo + 3 * size_t(node), nhi + 3 * size_t(node));
+        uint32_t cnt = count[node];
+        float    c   = cnt <= 3u ? A * kCostTri * float(cnt) : dist[8] + A * kCostNode;
+        float*   out = cost + 8 * size_t(node);
+        out[0]       = c;
+        for (int i = 2; i <= 8; ++i)
+        {
+            c          = fminf(c, dist[i]);
+            out[i - 1] = c;
+        }
+        node = parent[node];
+    }
+}
+
 struct CollapseArgs
 {
     const float*    triPos; // 9 floats per triangle, original order
@@ -384,6 +474,7 @@ struct CollapseArgs
     const float*    nlo;
     const float*    nhi;
     const uint32_t* count;
+    const float*    cost; // slot costs of the optimal collapse
     uint4*          nodes;
     float4*         tris;
     uint32_t*       nodeCounter;
@@ -446,55 +537,49 @@ __global__ void kCollapse(CollapseArgs A, const uint2* __restrict__ tasks, uint3
         ch[cnt++] = ref;
     else
     {
-        ch[cnt++] = A.left[ref];
-        ch[cnt++] = A.right[ref];
-        while (cnt < 8)
+        // Distribute the 8 slots by the cost minima: (node, budget) pairs
+        // split until a budget of 1 or the cost no longer needs the budget.
+        uint32_t sn[16], sj[16];
+        int      sp = 0;
+        sn[sp]      = ref;
+        sj[sp++]    = 8u;
+        bool root   = true;
+        while (sp > 0 && cnt < 8)
         {
-            int   best = -1;
-            float bestArea = -1.0f;
-            for (int k = 0; k < cnt; ++k)
+            uint32_t x = sn[--sp], j = sj[sp];
+            if (!root && ((x & kLeafFlag) || j == 1u))
             {
-                uint32_t r = ch[k];
-                if ((r & kLeafFlag) || A.count[r] <= 3u) continue;
-                float dx = A.nhi[3 * size_t(r)] - A.nlo[3 * size_t(r)];
-                float dy = A.nhi[3 * size_t(r) + 1] - A.nlo[3 * size_t(r) + 1];
-                float dz = A.nhi[3 * size_t(r) + 2] - A.nlo[3 * size_t(r) + 2];
-                float area = dx * dy + dy * dz + dz * dx;
-                if (area > bestArea)
+                ch[cnt++] = x;
+                continue;
+            }
+            const float* cx = A.cost + 8 * size_t(x);
+            uint32_t     i  = j;
+            if (!root)
+                while (i > 1u && cx[i - 2] == cx[j - 1]) --i; // fewest slots with the same cost
+            root = false;
+            if (i == 1u)
+            {
+                ch[cnt++] = x;
+                continue;
+            }
+            float cl[8], cr[8];
+            dpRefCosts(A.left[x], A.lo, A.hi, A.ids, A.cost, cl);
+            dpRefCosts(A.right[x], A.lo, A.hi, A.ids, A.cost, cr);
+            uint32_t bk = 1u;
+            float    bc = FLT_MAX;
+            for (uint32_t k = 1; k < i; ++k)
+            {
+                float c = cl[k - 1] + cr[i - k - 1];
+                if (c < bc)
                 {
-                    bestArea = area;
-                    best     = k;
+                    bc = c;
+                    bk = k;
                 }
             }
-            if (best < 0) break;
-            uint32_t r = ch[best];
-            ch[best]   = A.left[r];
-            ch[cnt++]  = A.right[r];
-        }
-        // Slots still free: split the largest small leaves (2-3 triangles)
-        // into smaller ones, so that their triangles get tighter boxes.
-        while (cnt < 8)
-        {
-            int   best     = -1;
-            float bestArea = -1.0f;
-            for (int k = 0; k < cnt; ++k)
-            {
-                uint32_t r = ch[k];
-                if (r & kLeafFlag) continue;
-                float dx = A.nhi[3 * size_t(r)] - A.nlo[3 * size_t(r)];
-                float dy = A.nhi[3 * size_t(r) + 1] - A.nlo[3 * size_t(r) + 1];
-                float dz = A.nhi[3 * size_t(r) + 2] - A.nlo[3 * size_t(r) + 2];
-                float area = dx * dy + dy * dz + dz * dx;
-                if (area > bestArea)
-                {
-                    bestArea = area;
-                    best     = k;
-                }
-            }
-            if (best < 0) break;
-            uint32_t r = ch[best];
-            ch[best]   = A.left[r];
-            ch[cnt++]  = A.right[r];
+            sn[sp]   = A.right[x];
+            sj[sp++] = i - bk;
+            sn[sp]   = A.left[x];
+            sj[sp++] = bk;
         }
     }
 
@@ -845,6 +930,23 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     uint2 root = make_uint2(rootRef, 0u);
     CL_CUDA(cudaMemcpyAsync(tasksA.p, &root, 8, cudaMemcpyHostToDevice, st), err);
 
+    // Slot costs of the optimal collapse, bottom up over the binary tree.
+    DevBuf dpCost, dpParent, dpLeafParent;
+    if (n > 1)
+    {
+        CL_TRY(dpCost.alloc(ni * 8 * 4, err));
+        CL_TRY(dpParent.alloc(ni * 4, err));
+        CL_TRY(dpLeafParent.alloc(nn * 4, err));
+        CL_CUDA(cudaMemsetAsync(dpParent.p, 0xff, ni * 4, st), err);
+        CL_CUDA(cudaMemsetAsync(dpLeafParent.p, 0xff, nn * 4, st), err);
+        CL_CUDA(cudaMemsetAsync(arrive.p, 0, ni * 4, st), err);
+        kDpParents<<<uint32_t((ni + 255) / 256), 256, 0, st>>>(uint32_t(n - 1), left.u(), right.u(), dpParent.u(),
+                                                               dpLeafParent.u());
+        kDpCosts<<<blocks, 256, 0, st>>>(n, dpLeafParent.u(), dpParent.u(), left.u(), right.u(), lo.f(), hi.f(),
+                                         ids2.u(), nlo.f(), nhi.f(), count.u(), dpCost.f(), arrive.u());
+        CL_CUDA(cudaGetLastError(), err);
+    }
+
     CollapseArgs A;
     A.triPos      = dTri9;
     A.lo          = lo.f();
@@ -855,6 +957,7 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     A.nlo         = nlo.f();
     A.nhi         = nhi.f();
     A.count       = count.u();
+    A.cost        = n > 1 ? dpCost.f() : nullptr; // n == 1: the root is a leaf
     A.nodes       = (uint4*)out->nodes.p;
     A.tris        = (float4*)out->tris.p;
     A.nodeCounter = ctr.u() + 0;
