@@ -80,10 +80,29 @@ __device__ __forceinline__ float min3f(float a, float b, float c)
     return r;
 }
 
+// Child-key table (shared memory, kKeyLutBytes per block): entry oct * 256 + m
+// is the 8-bit slot mask m with each slot s moved to bit s ^ oct, the order in
+// which a ray of octant oct visits the children.  One table lookup per node
+// replaces three conditional bit swaps on the busiest (integer) pipe.
+constexpr int kKeyLutBytes = 8 * 256;
+__device__ __forceinline__ void fillKeyLut(uint8_t* lut)
+{
+    for (int i = threadIdx.x; i < kKeyLutBytes; i += blockDim.x)
+    {
+        uint32_t oct = uint32_t(i) >> 8, k = uint32_t(i) & 0xffu;
+        k = (oct & 1u) ? (((k & 0x55u) << 1) | ((k >> 1) & 0x55u)) : k;
+        k = (oct & 2u) ? (((k & 0x33u) << 2) | ((k >> 2) & 0x33u)) : k;
+        k = (oct & 4u) ? (((k & 0x0fu) << 4) | ((k >> 4) & 0x0fu)) : k;
+        lut[i] = uint8_t(k);
+    }
+    __syncthreads();
+}
+
 // Intersects the ray with the 8 children of one node; returns the hit mask:
 // bits 24..31 inner-child keys (slot ^ octant), bits 0..23 triangle offsets.
 __device__ __forceinline__ uint32_t intersectNode(const BvhView& bvh, uint32_t idx, f3 o, f3 inv, uint32_t oct, float tmin,
-                                                  float tmax, uint32_t* childBase, uint32_t* triBase, uint32_t* imaskOut)
+                                                  float tmax, uint32_t* childBase, uint32_t* triBase, uint32_t* imaskOut,
+                                                  const uint8_t* keyLut)
 {
     const uint4* np = bvh.nodes + size_t(idx) * 5;
     uint4        n0 = __ldg(np + 0);
@@ -127,12 +146,8 @@ __device__ __forceinline__ uint32_t intersectNode(const BvhView& bvh, uint32_t i
         float  tn1 = max3f(tnx.y, tny.y, fmaxf(tnz.y, tmin)), tf1 = min3f(tfx.y, tfy.y, fminf(tfz.y, tmax));
         hitSlots |= (tn0 <= tf0 ? 1u << b : 0u) | (tn1 <= tf1 ? 1u << (b + 4) : 0u);
     }
-    // Inner children: slot s -> key s ^ oct (bit permutation of the mask).
-    uint32_t k = hitSlots & imask;
-    k          = (oct & 1u) ? (((k & 0x55u) << 1) | ((k >> 1) & 0x55u)) : k;
-    k          = (oct & 2u) ? (((k & 0x33u) << 2) | ((k >> 2) & 0x33u)) : k;
-    k          = (oct & 4u) ? (((k & 0x0fu) << 4) | ((k >> 4) & 0x0fu)) : k;
-    uint32_t hits = k << 24;
+    // Inner children: slot s -> key s ^ oct (bit permutation of the mask, from the table).
+    uint32_t hits = uint32_t(keyLut[(oct << 8) | (hitSlots & imask)]) << 24;
     // Leaf children: their triangle ranges (unary count << 5 | offset).
     uint32_t leaf = hitSlots & ~imask;
     while (leaf)
@@ -184,7 +199,8 @@ __device__ __forceinline__ void travInit(Trav& s, f3 o, f3 d, float tmin, float 
 // a shared [bvh.stackDepth][kTraceBlock] array.  Returns true when the ray is
 // finished (s.best: primitive id or kMissPrim; s.bt, s.b1, s.b2).
 template <bool ANY, bool STATS>
-__device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* stack, TraceCounters* cnt, uint32_t* err)
+__device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* stack, TraceCounters* cnt, uint32_t* err,
+                                         const uint8_t* keyLut)
 {
     if (s.tg.y == 0u && s.ng.y > 0x00ffffffu)
     {
@@ -205,7 +221,7 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
             ++s.sp;
         }
         uint32_t cb, tb, im;
-        uint32_t hits = intersectNode(bvh, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im);
+        uint32_t hits = intersectNode(bvh, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im, keyLut);
         if (STATS) cnt->nodes++;
         s.ng = make_uint2(cb, (hits & 0xff000000u) | im);
         s.tg = make_uint2(tb, hits & 0x00ffffffu);
@@ -254,11 +270,11 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
 template <bool ANY, bool STATS>
 __device__ __forceinline__ uint32_t traverse(const BvhView& bvh, f3 o, f3 d, float tmin, float tmax, float* tHit,
                                              float* b1Hit, float* b2Hit, uint2* stack, TraceCounters* cnt,
-                                             uint32_t* err)
+                                             uint32_t* err, const uint8_t* keyLut)
 {
     Trav s;
     travInit(s, o, d, tmin, tmax);
-    while (!travStep<ANY, STATS>(bvh, s, stack, cnt, err))
+    while (!travStep<ANY, STATS>(bvh, s, stack, cnt, err, keyLut))
     {
     }
     *tHit  = s.bt;

@@ -351,6 +351,8 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
                                                                 Counters* ctr, ClassifyView cv)
 {
     extern __shared__ uint2 stack[];
+    __shared__ uint8_t      keyLut[kKeyLutBytes];
+    fillKeyLut(keyLut);
     const uint32_t   n = loadCount(count);
     TraceCounters    tc{0u, 0u};
     for (;;)
@@ -364,7 +366,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
             float4 o = O[i], d = D[i];
             float  t, b1, b2;
             prim      = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                               stack + threadIdx.x, &tc, &ctr->error);
+                                               stack + threadIdx.x, &tc, &ctr->error, keyLut);
             hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
         }
         if (CLASSIFY)
@@ -397,6 +399,8 @@ template <bool DL, bool STATS>
 __global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
 {
     extern __shared__ uint2 stack[];
+    __shared__ uint8_t      keyLut[kKeyLutBytes];
+    fillKeyLut(keyLut);
     const uint32_t   n = loadCount(&P.q.ctr->shadowCount) * (DL ? 2u : 1u);
     TraceCounters    tc{0u, 0u};
     for (;;)
@@ -414,7 +418,7 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
             {
                 float    t, b1, b2;
                 uint32_t h = traverse<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
-                                                   &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error);
+                                                   &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
                 v = h == kMissPrim ? 1 : 0;
             }
             P.q.vis[item] = v;
@@ -1013,13 +1017,15 @@ __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const floa
                                                          uint8_t* __restrict__ occ, uint32_t* err)
 {
     extern __shared__ uint2 stack[];
+    __shared__ uint8_t      keyLut[kKeyLutBytes];
+    fillKeyLut(keyLut);
     uint32_t         i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4        o = O[i], d = D[i];
     float         t, b1, b2;
     TraceCounters tc{0u, 0u};
     uint32_t      h = traverse<true, false>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                       stack + threadIdx.x, &tc, err);
+                                       stack + threadIdx.x, &tc, err, keyLut);
     occ[i]          = h == kMissPrim ? 0 : 1;
 }
 
