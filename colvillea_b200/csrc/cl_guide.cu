@@ -4,6 +4,7 @@
 // weight-gradient reduction over the batch and Adam; they differ in shape
 // (MlpShape) and in the loss at the head (GuideLoss, CacheLoss).
 #include "cl_guide.h"
+#include "cl_mlp_tc.cuh"
 
 #include <cuda_bf16.h>
 
@@ -17,11 +18,9 @@ using namespace guide;
 
 namespace
 {
-constexpr int kInferWarps = 8;            // inference: 8 warps x 32 samples per CTA pass
 constexpr int kTrainWarps = 4;            // training forward/backward: 4 warps x 16 samples
 constexpr int kGradChunk  = 4096;         // samples per weight-gradient block
 constexpr int kGradStep   = 64;           // samples staged in shared memory per step
-constexpr int kXTile      = 32 * kXS * 2; // bytes of a 32-row encoded tile (6656)
 
 __device__ __forceinline__ uint32_t laneIdx() { return threadIdx.x & 31u; }
 
@@ -65,8 +64,12 @@ __global__ void kTableCopy(const float* __restrict__ p, __nv_bfloat16* __restric
 // Fragment-ordered bf16 weights.  Forward fragment (kt, nt) of layer l, lane
 // (g, t): b0 = W[8nt+g][16kt+2t .. +1], b1 = W[8nt+g][16kt+2t+8 .. +9].
 // Backward fragment (kt over outputs, nt over inputs): b0 = W[16kt+2t][8nt+g],
-// W[16kt+2t+1][8nt+g]; b1 the same 8 rows further down.
-template <class S> __global__ void kFrags(const float* __restrict__ mlp, uint2* __restrict__ wf, uint2* __restrict__ wb)
+// W[16kt+2t+1][8nt+g]; b1 the same 8 rows further down.  Then the weights in
+// the tensor-core canonical layout (cl_mlp_tc.cuh): 16-byte chunk e of layer
+// l, at byte 2 woff(l) + 16 e, holds W[e % N][8 (e / N) .. + 7].
+template <class S>
+__global__ void kFrags(const float* __restrict__ mlp, uint2* __restrict__ wf, uint2* __restrict__ wb,
+                       uint4* __restrict__ wt)
 {
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e < S::kFwdFrags * 32)
@@ -88,8 +91,19 @@ template <class S> __global__ void kFrags(const float* __restrict__ mlp, uint2* 
         int          g = lane >> 2, t = lane & 3, K = S::in(l);
         const float* W   = mlp + S::woff(l) + (kt * 16 + 2 * t) * K + nt * 8 + g;
         wb[e]            = make_uint2(packBf16(W[0], W[K]), packBf16(W[8 * K], W[9 * K]));
+        return;
+    }
+    e -= S::kBwdFrags * 32;
+    if (e < S::kParams / 8)
+    {
+        int l = 0;
+        while (l < S::kLayers - 1 && e >= S::woff(l + 1) / 8) ++l;
+        const int    loc = e - S::woff(l) / 8, N = S::out(l), K = S::in(l);
+        const float* W   = mlp + S::woff(l) + (loc % N) * K + 8 * (loc / N);
+        wt[e] = make_uint4(packBf16(W[0], W[1]), packBf16(W[2], W[3]), packBf16(W[4], W[5]), packBf16(W[6], W[7]));
     }
 }
+template <class S> constexpr int fragThreads() { return (S::kFwdFrags + S::kBwdFrags) * 32 + S::kParams / 8; }
 
 __device__ __forceinline__ void loadFrags(uint2* dst, const uint2* __restrict__ src, int count)
 {
@@ -100,39 +114,41 @@ __device__ __forceinline__ void loadFrags(uint2* dst, const uint2* __restrict__ 
 
 __device__ __forceinline__ f3 ldf3(const float* p) { return {p[0], p[1], p[2]}; }
 
-// Forward pass of `n` host-given samples (in9 rows) -> raw outputs.
+// Forward pass of `n` host-given samples (in9 rows) -> raw outputs, on the
+// tensor-core path of the integrator's inference (cl_mlp_tc.cuh): 128-row
+// tiles, thread t encodes row t and receives its outputs.
 template <class S>
-__global__ void __launch_bounds__(kInferWarps * 32) kInferUnit(GridView g, const uint2* __restrict__ wfG,
-                                                                const float* __restrict__ in9, uint32_t n,
-                                                                float* __restrict__ out)
+__global__ void __launch_bounds__(kTcThreads) kInferUnit(GridView g, const uint4* __restrict__ wt,
+                                                         const float* __restrict__ in9, uint32_t n,
+                                                         float* __restrict__ out, uint32_t* __restrict__ err)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint2*         wf   = reinterpret_cast<uint2*>(smem);
-    const uint32_t lane = laneIdx(), warp = threadIdx.x >> 5;
-    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + S::kFwdBytes + warp * kXTile);
-    loadFrags(wf, wfG, S::kFwdFrags * 32);
-    __syncthreads();
-    for (uint32_t base = (blockIdx.x * kInferWarps + warp) * 32u; base < n; base += gridDim.x * kInferWarps * 32u)
+    const uint32_t tmem  = tcSetup<S>(smem, wt);
+    unsigned char* tile  = smem + TcLayout<S>::kTile;
+    uint32_t       phase = 0u;
+    for (uint32_t base = blockIdx.x * kTcRows; base < n; base += gridDim.x * kTcRows)
     {
-        uint32_t i = base + lane;
+        const uint32_t i = base + threadIdx.x;
+        __align__(16) __nv_bfloat16 row[kIn];
         if (i < n)
         {
             const float* r = in9 + 9 * size_t(i);
-            encodeRow(g, ldf3(r), ldf3(r + 3), ldf3(r + 6), x + lane * kXS);
+            encodeRow(g, ldf3(r), ldf3(r + 3), ldf3(r + 6), row);
         }
         else
-            zeroRow(x + lane * kXS);
-        __syncwarp();
-        float acc[2][S::kOut / 8][4];
-        mlpInfer<S, 2>(wf, x, lane, acc);
-        __syncwarp();
-        float* o = reinterpret_cast<float*>(x);
-        storeOut<S, 2>(acc, o, lane);
-        __syncwarp();
+            zeroRow(row);
+#pragma unroll
+        for (int c = 0; c < kIn / 8; ++c) *tileChunk(tile, threadIdx.x, c) = reinterpret_cast<const uint4*>(row)[c];
+        float o[S::kOut];
+        if (!tcForward<S>(smem, tmem, phase, o))
+        {
+            if (threadIdx.x == 0) atomicOr(err, kTcTimeout);
+            break;
+        }
         if (i < n)
-            for (int c = 0; c < S::kOut; ++c) out[size_t(i) * S::kOut + c] = o[lane * S::kOS + c];
-        __syncwarp();
+            for (int c = 0; c < S::kOut; ++c) out[size_t(i) * S::kOut + c] = o[c];
     }
+    tcTeardown(tmem);
 }
 
 // Mixture sample / pdf of given guide outputs (the network's mixture alone).
@@ -784,9 +800,9 @@ template <class S, class L> cl_status HashNet<S, L>::init(cudaStream_t st, std::
     int dev = 0;
     CL_CUDA(cudaGetDevice(&dev), err);
     CL_CUDA(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, dev), err);
-    CL_CUDA(cudaFuncSetAttribute(kInferUnit<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 S::kFwdBytes + kInferWarps * kXTile),
+    CL_CUDA(cudaFuncSetAttribute(kInferUnit<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<S>::kSmem),
             err);
+    CL_CUDA(cudaFuncSetAttribute(kInferUnit<S>, cudaFuncAttributePreferredSharedMemoryCarveout, 100), err);
     CL_CUDA(cudaFuncSetAttribute(kTrainFwdBwd<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrainSmem<S>::kAll),
             err);
     int occ = 0;
@@ -801,6 +817,7 @@ template <class S, class L> cl_status HashNet<S, L>::init(cudaStream_t st, std::
     CL_TRY(table_.alloc(hashParams_ * 2, err));
     CL_TRY(wf_.alloc(S::kFwdBytes, err));
     CL_TRY(wb_.alloc(S::kBwdBytes, err));
+    CL_TRY(wt_.alloc(TcLayout<S>::kWBytes, err));
     CL_TRY(acts_.alloc(size_t(cfg_.batch) * S::kActRow * 2, err));
     CL_TRY(deltas_.alloc(size_t(cfg_.batch) * S::kDeltaRow * 2, err));
     CL_TRY(scal_.alloc(64, err));
@@ -832,8 +849,8 @@ template <class S, class L> cl_status HashNet<S, L>::refreshCopies(std::string* 
     kTableCopy<<<gridFor(hashParams_, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), table_.as<__nv_bfloat16>(),
                                                                         hashParams_);
     CL_CUDA(cudaGetLastError(), err);
-    kFrags<S><<<((S::kFwdFrags + S::kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_,
-                                                                                  wf_.as<uint2>(), wb_.as<uint2>());
+    kFrags<S><<<(fragThreads<S>() + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
+                                                               wb_.as<uint2>(), wt_.as<uint4>());
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }
@@ -879,12 +896,20 @@ cl_status HashNet<S, L>::forward(const float* in9, uint32_t n, float* out, std::
     CL_TRY(io_.alloc(size_t(n) * 9 * 4, err));
     CL_TRY(io2_.alloc(size_t(n) * S::kOut * 4, err));
     CL_CUDA(cudaMemcpyAsync(io_.p, in9, size_t(n) * 9 * 4, cudaMemcpyHostToDevice, st_), err);
-    const int smem = S::kFwdBytes + kInferWarps * kXTile;
-    kInferUnit<S><<<gridFor(n, kInferWarps * 32, numSMs_ * 2), kInferWarps * 32, smem, st_>>>(grid(), fwdFrags(),
-                                                                                              io_.f(), n, io2_.f());
+    uint32_t* flag = reinterpret_cast<uint32_t*>(scal_.as<unsigned char>() + 48);
+    CL_CUDA(cudaMemsetAsync(flag, 0, 4, st_), err);
+    kInferUnit<S><<<gridFor(n, kTcRows, numSMs_ * 2), kTcThreads, TcLayout<S>::kSmem, st_>>>(grid(), tcWeights(),
+                                                                                            io_.f(), n, io2_.f(), flag);
     CL_CUDA(cudaGetLastError(), err);
     CL_CUDA(cudaMemcpyAsync(out, io2_.p, size_t(n) * S::kOut * 4, cudaMemcpyDeviceToHost, st_), err);
+    uint32_t hf = 0u;
+    CL_CUDA(cudaMemcpyAsync(&hf, flag, 4, cudaMemcpyDeviceToHost, st_), err);
     CL_CUDA(cudaStreamSynchronize(st_), err);
+    if (hf & kTcTimeout)
+    {
+        *err = "network: a tensor-core wait ran out";
+        return CL_ERR_TIMEOUT;
+    }
     return CL_OK;
 }
 
@@ -1022,8 +1047,8 @@ cl_status HashNet<S, L>::trainDevice(const float4* rec, const uint32_t* count, s
                                                               m_.as<float4>(), v_.as<float4>(), n4, hashParams_ / 4, k,
                                                               table_.as<uint2>());
     CL_CUDA(cudaGetLastError(), err);
-    kFrags<S><<<((S::kFwdFrags + S::kBwdFrags) * 32 + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_,
-                                                                                  wf_.as<uint2>(), wb_.as<uint2>());
+    kFrags<S><<<(fragThreads<S>() + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
+                                                               wb_.as<uint2>(), wt_.as<uint4>());
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }

@@ -48,6 +48,7 @@ public:
     cl_status trainDevice(const float4* rec, const uint32_t* count, std::string* err);
     guide::GridView grid() const;
     const uint2*    fwdFrags() const { return wf_.as<uint2>(); }
+    const uint4*    tcWeights() const { return wt_.as<uint4>(); }
     const double*   lossDev() const { return scal_.as<double>() + 1; }
     uint64_t        steps() const { return step_; }
 
@@ -68,8 +69,9 @@ private:
     DevBuf params_, grad_, m_, v_; // FP32 [hash | mlp]
     DevBuf table_;                 // bf16 copy of the hash table
     DevBuf wf_, wb_;               // bf16 weight fragments (forward, backward)
+    DevBuf wt_;                    // bf16 weights in the tensor-core canonical layout
     DevBuf acts_, deltas_;         // training staging, batch rows
-    DevBuf scal_;                  // {sum w, loss, count (u32), sum of clamped w}
+    DevBuf scal_;                  // {sum w, loss, count (u32), sum of clamped w}; byte 48: inference error flags
     DevBuf rec_, io_, io2_;        // host-entry staging
 };
 

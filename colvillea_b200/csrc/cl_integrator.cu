@@ -26,6 +26,7 @@
 // (src/kernel/integrators/raygeneration.cu:59-456, src/core/devices/optix.cu:112-284);
 // Russian roulette is added (absent from the reference, path.cpp:135).
 #include "cl_integrator.h"
+#include "cl_mlp_tc.cuh"
 
 #include <cstdio>
 
@@ -798,8 +799,6 @@ __global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
 // vertices -> table) and runs at full occupancy on its own; the MLP pass
 // keeps its weights in shared memory and reads its rows sequentially.
 constexpr uint32_t kNoRay          = 0xffffffffu;
-constexpr int      kGuideMlpWarps  = 8;
-constexpr int      kGuideMlpSmem   = guide::GuideShape::kFwdBytes + kGuideMlpWarps * 32 * guide::kXS * 2;
 constexpr int      kGuideEncBlock  = 128;
 
 __device__ __forceinline__ uint32_t guidedCounts(const Params& P, uint32_t* n0, uint32_t* n1)
@@ -899,26 +898,20 @@ __global__ void __launch_bounds__(kGuideEncBlock, 6) kCacheEncode(Params P, guid
     }
 }
 
-// Second pass of both networks: persistent warps stream 32 encoded rows at a
-// time through the MLP on the tensor cores.  Guide (S = GuideShape): the
-// head's lobes per ray, their weights summing to the probability of sampling
-// the guide (alpha; < 0: learned).  Cache (S = CacheShape): the predicted
-// radiance per ray, clamped to be non-negative.
+// Second pass of both networks, on the tensor cores (tcgen05, cl_mlp_tc.cuh):
+// persistent CTAs of 128 threads stream 128 encoded rows at a time through
+// the MLP, thread t handling row t.  Guide (S = GuideShape): the head's lobes
+// per ray, their weights summing to the probability of sampling the guide
+// (alpha; < 0: learned).  Cache (S = CacheShape): the predicted radiance per
+// ray, clamped to be non-negative.
 template <class S, bool CACHE>
-__global__ void __launch_bounds__(kGuideMlpWarps * 32, 2) kMlpPass(Params P, const uint2* __restrict__ wfG,
-                                                                   float alpha)
+__global__ void __launch_bounds__(guide::kTcThreads) kMlpPass(Params P, const uint4* __restrict__ wt, float alpha)
 {
+    using namespace guide;
     extern __shared__ __align__(16) unsigned char smem[];
-    uint2*         wf   = reinterpret_cast<uint2*>(smem);
-    const uint32_t lane = laneId(), warp = threadIdx.x >> 5;
-    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(smem + S::kFwdBytes + warp * 32 * guide::kXS * 2);
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(wfG);
-        uint4*       dst = reinterpret_cast<uint4*>(wf);
-        for (int k = threadIdx.x; k < S::kFwdFrags * 16; k += blockDim.x) dst[k] = __ldg(src + k);
-    }
-    __syncthreads();
-    uint32_t n;
+    const uint32_t tmem = tcSetup<S>(smem, wt);
+    unsigned char* tile = smem + TcLayout<S>::kTile;
+    uint32_t       n;
     if (CACHE)
         n = loadCount(&P.q.ctr->cacheCount);
     else
@@ -928,49 +921,68 @@ __global__ void __launch_bounds__(kGuideMlpWarps * 32, 2) kMlpPass(Params P, con
     }
     const uint4*    enc    = CACHE ? P.c.enc : P.g.enc;
     const uint32_t* encIdx = CACHE ? P.c.encIdx : P.g.encIdx;
-    for (uint32_t tile = blockIdx.x * kGuideMlpWarps + warp; tile * 32u < n; tile += gridDim.x * kGuideMlpWarps)
+    uint32_t        phase  = 0u;
+    for (uint32_t k0 = blockIdx.x * kTcRows; k0 < n; k0 += gridDim.x * kTcRows)
     {
-        const uint32_t k0  = tile * 32u;
-        const uint4*   src = enc + size_t(k0) * (guide::kIn / 8);
-#pragma unroll
-        for (int q = 0; q < guide::kIn / 8; ++q)
-        {
-            const uint32_t j = lane + 32u * q, rr = j / 12u, cc = j % 12u;
-            uint4          v = make_uint4(0u, 0u, 0u, 0u);
-            if (k0 + rr < n) v = src[j];
-            *reinterpret_cast<uint4*>(x + rr * guide::kXS + cc * 8) = v;
-        }
-        const uint32_t ray = k0 + lane < n ? encIdx[k0 + lane] : kNoRay;
+        const uint32_t k = k0 + threadIdx.x;
+        loadTile(tile, enc, k0, n);
+        const uint32_t ray = k < n ? encIdx[k] : kNoRay;
         const uint32_t vm  = __ballot_sync(kFull, ray != kNoRay);
-        if (lane == 0u && vm)
+        if (laneId() == 0u && vm)
             atomicAdd(CACHE ? &P.q.ctr->cacheQueries : &P.q.ctr->inferred, (unsigned long long)__popc(vm));
-        __syncwarp();
-        float out[2][S::kOut / 8][4];
-        guide::mlpInfer<S, 2>(wf, x, lane, out);
-        __syncwarp();
-        float* o = reinterpret_cast<float*>(x);
-        guide::storeOut<S, 2>(out, o, lane);
-        __syncwarp();
+        float o[S::kOut];
+        if (!tcForward<S>(smem, tmem, phase, o))
+        {
+            if (threadIdx.x == 0) atomicOr(&P.q.ctr->error, kTcTimeout);
+            break;
+        }
         if (ray != kNoRay)
         {
-            const float* row = o + lane * S::kOS;
             if (CACHE)
-                P.c.L[ray] = make_float4(fmaxf(row[0], 0.0f), fmaxf(row[1], 0.0f), fmaxf(row[2], 0.0f), 0.0f);
+                P.c.L[ray] = make_float4(fmaxf(o[0], 0.0f), fmaxf(o[1], 0.0f), fmaxf(o[2], 0.0f), 0.0f);
             else
             {
-                guide::Lobes L;
-                guide::headLobes(row, &L, alpha);
+                Lobes L;
+                headLobes(o, &L, alpha);
                 float4* dst = P.g.lobes + size_t(ray) * kLobeF4;
 #pragma unroll
-                for (int j = 0; j < guide::kLobes; ++j) dst[j] = L.l[j];
+                for (int j = 0; j < kLobes; ++j) dst[j] = L.l[j];
                 dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
                 dst[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
             }
         }
-        __syncwarp();
     }
+    tcTeardown(tmem);
 }
-constexpr int kCacheMlpSmem = guide::CacheShape::kFwdBytes + kGuideMlpWarps * 32 * guide::kXS * 2;
+constexpr int kGuideMlpSmem = guide::TcLayout<guide::GuideShape>::kSmem;
+constexpr int kCacheMlpSmem = guide::TcLayout<guide::CacheShape>::kSmem;
+
+// CTAs of a tensor-core MLP kernel (guide::kTcThreads threads, `smem` bytes
+// of dynamic shared memory) that one SM holds at once: by registers, by
+// shared memory (plus the per-CTA reserve) and by TMEM columns (512 per SM,
+// guide::kTcCols per CTA).  Counted from the kernel's attributes.
+cl_status tcResidentCtas(const void* f, int smem, int* ctas, std::string* err)
+{
+    cudaFuncAttributes a;
+    int                dev = 0, regsSm = 0, smemSm = 0, reserve = 0;
+    CL_CUDA(cudaFuncGetAttributes(&a, f), err);
+    CL_CUDA(cudaGetDevice(&dev), err);
+    CL_CUDA(cudaDeviceGetAttribute(&regsSm, cudaDevAttrMaxRegistersPerMultiprocessor, dev), err);
+    CL_CUDA(cudaDeviceGetAttribute(&smemSm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev), err);
+    CL_CUDA(cudaDeviceGetAttribute(&reserve, cudaDevAttrReservedSharedMemoryPerBlock, dev), err);
+    const int warps   = guide::kTcThreads / 32;
+    const int regWarp = ((std::max(a.numRegs, 1) + 7) / 8) * 8 * 32; // per-thread count rounded to 8
+    const int byRegs  = regsSm / (regWarp * warps);
+    const int bySmem  = smemSm / (((smem + int(a.sharedSizeBytes) + reserve + 127) / 128) * 128);
+    const int byTmem  = int(512u / guide::kTcCols);
+    *ctas             = std::min(std::min(byRegs, bySmem), byTmem);
+    if (*ctas < 1)
+    {
+        *err = "tensor-core MLP pass: no CTA fits on an SM";
+        return CL_ERR_STATE;
+    }
+    return CL_OK;
+}
 
 // Records beyond the capacity were dropped; the training step reads the
 // clamped count.
@@ -1164,16 +1176,21 @@ cl_status Integrator::init(std::string* err)
     CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::CacheShape, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kCacheMlpSmem),
             err);
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kMlpPass<guide::CacheShape, true>, kGuideMlpWarps * 32,
-                                                          kCacheMlpSmem),
+    // The whole on-chip memory as shared memory: the occupancy query then
+    // counts the CTAs that the launch can hold (3 of the guide's, 4 of the
+    // cache's), not those of a default carveout.
+    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::GuideShape, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 100),
             err);
-    cacheMlpBlocks_ = std::max(1, b) * numSMs_;
+    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::CacheShape, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 100),
+            err);
+    CL_TRY(tcResidentCtas((const void*)kMlpPass<guide::CacheShape, true>, kCacheMlpSmem, &b, err));
+    cacheMlpBlocks_ = b * numSMs_;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kCacheEncode, kGuideEncBlock, 0), err);
     cacheEncodeBlocks_ = std::max(1, b) * numSMs_;
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kMlpPass<guide::GuideShape, false>, kGuideMlpWarps * 32,
-                                                          kGuideMlpSmem),
-            err);
-    inferBlocks_ = std::max(1, b) * numSMs_;
+    CL_TRY(tcResidentCtas((const void*)kMlpPass<guide::GuideShape, false>, kGuideMlpSmem, &b, err));
+    inferBlocks_ = b * numSMs_;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideEncode, kGuideEncBlock, 0), err);
     encodeBlocks_ = std::max(1, b) * numSMs_;
     CL_TRY(ctr_.alloc(sizeof(Counters), err));
@@ -1755,14 +1772,14 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     if (gmask)
     {
         kGuideEncode<<<encodeBlocks_, kGuideEncBlock, 0, stream_>>>(P, guide_->grid(), cur);
-        kMlpPass<guide::GuideShape, false><<<inferBlocks_, kGuideMlpWarps * 32, kGuideMlpSmem, stream_>>>(
-            P, guide_->fwdFrags(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
+        kMlpPass<guide::GuideShape, false><<<inferBlocks_, guide::kTcThreads, kGuideMlpSmem, stream_>>>(
+            P, guide_->tcWeights(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
     }
     if (cache_)
     {
         kCacheEncode<<<cacheEncodeBlocks_, kGuideEncBlock, 0, stream_>>>(P, cache_->grid(), cur);
-        kMlpPass<guide::CacheShape, true><<<cacheMlpBlocks_, kGuideMlpWarps * 32, kCacheMlpSmem, stream_>>>(
-            P, cache_->fwdFrags(), 1.0f);
+        kMlpPass<guide::CacheShape, true><<<cacheMlpBlocks_, guide::kTcThreads, kCacheMlpSmem, stream_>>>(
+            P, cache_->tcWeights(), 1.0f);
     }
     if (profile) CL_CUDA(cudaEventRecord(evS_[4], stream_), err);
     for (int m = 0; m < 4; ++m)
@@ -1975,7 +1992,9 @@ cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std
     {
         *err = std::string("device error flags ") + std::to_string(ch.error) +
                (ch.error & 1u ? " (traversal stack overflow)" : "") + (ch.error & 4u ? " (shadow queue overflow)" : "") +
-               (ch.error & 8u ? " (ray queue overflow)" : "");
+               (ch.error & 8u ? " (ray queue overflow)" : "") +
+               (ch.error & guide::kTcTimeout ? " (tensor-core wait ran out)" : "");
+        if (ch.error & guide::kTcTimeout) return CL_ERR_TIMEOUT;
         return (ch.error & 12u) ? CL_ERR_QUEUE_OVERFLOW : CL_ERR_STATE;
     }
     pathsDone_ += wp.totalPaths;
