@@ -909,9 +909,7 @@ __global__ void __launch_bounds__(guide::kTcThreads) kMlpPass(Params P, const ui
 {
     using namespace guide;
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t tmem = tcSetup<S>(smem, wt);
-    unsigned char* tile = smem + TcLayout<S>::kTile;
-    uint32_t       n;
+    uint32_t n;
     if (CACHE)
         n = loadCount(&P.q.ctr->cacheCount);
     else
@@ -919,6 +917,11 @@ __global__ void __launch_bounds__(guide::kTcThreads) kMlpPass(Params P, const ui
         uint32_t n0, n1;
         n = guidedCounts(P, &n0, &n1);
     }
+    // The grid is fixed (graph replay) while the row count varies by wave:
+    // CTAs without a tile skip the weight copy and the TMEM allocation.
+    if (blockIdx.x * kTcRows >= n) return;
+    const uint32_t tmem = tcSetup<S>(smem, wt);
+    unsigned char* tile = smem + TcLayout<S>::kTile;
     const uint4*    enc    = CACHE ? P.c.enc : P.g.enc;
     const uint32_t* encIdx = CACHE ? P.c.encIdx : P.g.encIdx;
     uint32_t        phase  = 0u;
