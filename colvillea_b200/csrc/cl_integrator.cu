@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             }
             else if (!DL && P.c.termDepth && depth == P.c.termDepth && !(cst & kCacheTrainBit))
             {
-                // The path ends in the radiance cache (kMlpPass's prediction).
+                // The path ends in the radiance cache (kCacheMlp's prediction).
                 float4 cl = P.c.L[i];
                 L         = L + T * f3{cl.x, cl.y, cl.z};
                 finish    = true;
@@ -788,16 +788,12 @@ __global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
 
 // Guided path tracing: network inference after kTraceClosest for the rays of
 // the guided shading classes (class queues concatenated in class order), in
-// two passes:
-//   kGuideEncode - one thread per ray: hit position and shading normal, the
-//     16-level hash-grid gathers and the one-blob encodings -> a 96-wide
-//     bf16 input row enc[k] and the ray's queue index encIdx[k] (kNoRay for a
-//     last vertex, depth == maxDepth, which is not shaded);
-//   kGuideMlp - persistent warps stream 32 rows at a time through the MLP
-//     on the tensor cores and write each ray's lobes.
+// one kernel (kGuideInfer): per 128-row tile, thread t encodes ray k0 + t
+// (hit position and shading normal, the 16-level hash-grid gathers, the
+// one-blob encodings) straight into the tensor-core A tile, then the tile goes
+// through the MLP (cl_mlp_tc.cuh) and each thread writes its ray's lobes.
 // The encoding is a chain of dependent gathers (queue -> path state -> hit ->
-// vertices -> table) and runs at full occupancy on its own; the MLP pass
-// keeps its weights in shared memory and reads its rows sequentially.
+// vertices -> table); the other CTAs' MMA chains run in its shadow.
 constexpr uint32_t kNoRay          = 0xffffffffu;
 constexpr int      kGuideEncBlock  = 128;
 
@@ -810,53 +806,44 @@ __device__ __forceinline__ uint32_t guidedCounts(const Params& P, uint32_t* n0, 
     return *n0 + *n1 + n2;
 }
 
-__global__ void __launch_bounds__(kGuideEncBlock, 6) kGuideEncode(Params P, guide::GridView g, int cur)
+// Encoded input row (r: 96 bf16 as 48 pairs) of guided ray k of the
+// concatenated class queues; returns its ray-queue index, or kNoRay (and a
+// zero row) for a last vertex (depth == maxDepth, not shaded) or a path that
+// ends in the radiance cache here.
+__device__ __forceinline__ uint32_t encodeGuideRow(const Params& P, const guide::GridView& g, int cur, uint32_t k,
+                                                   uint32_t n0, uint32_t n1, uint32_t maxDepth, f3 bmin,
+                                                   uint32_t (&r)[guide::kIn / 2])
 {
-    uint32_t       n0, n1;
-    const uint32_t n        = guidedCounts(P, &n0, &n1);
-    const uint32_t maxDepth = P.wp->maxDepth;
-    const f3       bmin{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]};
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    const uint32_t c     = k < n0 ? 0u : (k < n0 + n1 ? 1u : 2u);
+    const uint32_t pos   = k - (c == 0u ? 0u : (c == 1u ? n0 : n0 + n1));
+    const uint32_t i     = P.q.classIdx[size_t(c) * P.q.slots + pos];
+    const uint32_t slot  = P.q.rqSlot[cur][i];
+    const uint32_t depth = P.q.psInfo[slot].z & 0xffu;
+    if (depth == maxDepth ||
+        (P.c.termDepth && depth == P.c.termDepth && !(__float_as_uint(P.q.psE[slot].w) & kCacheTrainBit)))
     {
-        const uint32_t c   = k < n0 ? 0u : (k < n0 + n1 ? 1u : 2u);
-        const uint32_t pos = k - (c == 0u ? 0u : (c == 1u ? n0 : n0 + n1));
-        const uint32_t i   = P.q.classIdx[size_t(c) * P.q.slots + pos];
-        uint4*         dst = P.g.enc + size_t(k) * (guide::kIn / 8);
-        uint32_t       r[guide::kIn / 2];
-        uint32_t       ray = i;
-        const uint32_t slot  = P.q.rqSlot[cur][i];
-        const uint32_t depth = P.q.psInfo[slot].z & 0xffu;
-        if (depth == maxDepth ||
-            (P.c.termDepth && depth == P.c.termDepth && !(__float_as_uint(P.q.psE[slot].w) & kCacheTrainBit)))
-        {
-            ray = kNoRay;
 #pragma unroll
-            for (int q = 0; q < guide::kIn / 2; ++q) r[q] = 0u;
-        }
-        else
-        {
-            float4  hh = P.q.hit[i];
-            float4  rd = P.q.rqD[cur][i];
-            HitAttr a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
-            f3      pn = guide::clampUnit((a.p - bmin) * P.g.boxScale);
-#pragma unroll
-            for (int l = 0; l < guide::kLevels; ++l)
-            {
-                float2 f = guide::encodeLevel(g, l, pn);
-                r[l]     = guide::packBf16(f.x, f.y);
-            }
-            guide::oneBlobPacked(a.ns, r + guide::kHashF / 2);
-            guide::oneBlobPacked(f3{-rd.x, -rd.y, -rd.z}, r + (guide::kHashF + 2 * guide::kBlob) / 2);
-        }
-#pragma unroll
-        for (int q = 0; q < guide::kIn / 8; ++q) dst[q] = make_uint4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
-        P.g.encIdx[k] = ray;
+        for (int q = 0; q < guide::kIn / 2; ++q) r[q] = 0u;
+        return kNoRay;
     }
+    float4  hh = P.q.hit[i];
+    float4  rd = P.q.rqD[cur][i];
+    HitAttr a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
+    f3      pn = guide::clampUnit((a.p - bmin) * P.g.boxScale);
+#pragma unroll
+    for (int l = 0; l < guide::kLevels; ++l)
+    {
+        float2 f = guide::encodeLevel(g, l, pn);
+        r[l]     = guide::packBf16(f.x, f.y);
+    }
+    guide::oneBlobPacked(a.ns, r + guide::kHashF / 2);
+    guide::oneBlobPacked(f3{-rd.x, -rd.y, -rd.z}, r + (guide::kHashF + 2 * guide::kBlob) / 2);
+    return i;
 }
 
 // Radiance cache, first pass: the rays of the surface classes that end
 // their path here (depth == termDepth, not a training path) are compacted
-// (warp-aggregated append) and encoded like kGuideEncode's.
+// (warp-aggregated append) and encoded like the guide's rows (encodeGuideRow).
 __global__ void __launch_bounds__(kGuideEncBlock, 6) kCacheEncode(Params P, guide::GridView g, int cur)
 {
     const uint32_t n0 = loadCount(&P.q.ctr->classCount[0]), n1 = loadCount(&P.q.ctr->classCount[1]);
@@ -898,62 +885,88 @@ __global__ void __launch_bounds__(kGuideEncBlock, 6) kCacheEncode(Params P, guid
     }
 }
 
-// Second pass of both networks, on the tensor cores (tcgen05, cl_mlp_tc.cuh):
-// persistent CTAs of 128 threads stream 128 encoded rows at a time through
-// the MLP, thread t handling row t.  Guide (S = GuideShape): the head's lobes
-// per ray, their weights summing to the probability of sampling the guide
-// (alpha; < 0: learned).  Cache (S = CacheShape): the predicted radiance per
-// ray, clamped to be non-negative.
-template <class S, bool CACHE>
-__global__ void __launch_bounds__(guide::kTcThreads) kMlpPass(Params P, const uint4* __restrict__ wt, float alpha)
+// Guide inference, fused: persistent CTAs of 128 threads; per 128-row tile of
+// the guided rays, thread t encodes row t into the tensor-core A tile, the
+// tile goes through the MLP (tcgen05, cl_mlp_tc.cuh) and thread t writes the
+// head's lobes of its ray, their weights summing to the probability of
+// sampling the guide (alpha; < 0: learned).
+__global__ void __launch_bounds__(guide::kTcThreads) kGuideInfer(Params P, guide::GridView g, int cur,
+                                                                 const uint4* __restrict__ wt, float alpha)
 {
     using namespace guide;
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t n;
-    if (CACHE)
-        n = loadCount(&P.q.ctr->cacheCount);
-    else
-    {
-        uint32_t n0, n1;
-        n = guidedCounts(P, &n0, &n1);
-    }
+    uint32_t       n0, n1;
+    const uint32_t n = guidedCounts(P, &n0, &n1);
     // The grid is fixed (graph replay) while the row count varies by wave:
     // CTAs without a tile skip the weight copy and the TMEM allocation.
     if (blockIdx.x * kTcRows >= n) return;
-    const uint32_t tmem = tcSetup<S>(smem, wt);
-    unsigned char* tile = smem + TcLayout<S>::kTile;
-    const uint4*    enc    = CACHE ? P.c.enc : P.g.enc;
-    const uint32_t* encIdx = CACHE ? P.c.encIdx : P.g.encIdx;
-    uint32_t        phase  = 0u;
+    const uint32_t tmem     = tcSetup<GuideShape>(smem, wt);
+    unsigned char* tile     = smem + TcLayout<GuideShape>::kTile;
+    const uint32_t maxDepth = P.wp->maxDepth;
+    const f3       bmin{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]};
+    uint32_t       phase = 0u;
     for (uint32_t k0 = blockIdx.x * kTcRows; k0 < n; k0 += gridDim.x * kTcRows)
     {
         const uint32_t k = k0 + threadIdx.x;
-        loadTile(tile, enc, k0, n);
-        const uint32_t ray = k < n ? encIdx[k] : kNoRay;
-        const uint32_t vm  = __ballot_sync(kFull, ray != kNoRay);
-        if (laneId() == 0u && vm)
-            atomicAdd(CACHE ? &P.q.ctr->cacheQueries : &P.q.ctr->inferred, (unsigned long long)__popc(vm));
-        float o[S::kOut];
-        if (!tcForward<S>(smem, tmem, phase, o))
+        uint32_t       r[kIn / 2];
+        uint32_t       ray = kNoRay;
+        if (k < n)
+            ray = encodeGuideRow(P, g, cur, k, n0, n1, maxDepth, bmin, r);
+        else
+#pragma unroll
+            for (int q = 0; q < kIn / 2; ++q) r[q] = 0u;
+#pragma unroll
+        for (int c = 0; c < kIn / 8; ++c)
+            *tileChunk(tile, threadIdx.x, c) = make_uint4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+        const uint32_t vm = __ballot_sync(kFull, ray != kNoRay);
+        if (laneId() == 0u && vm) atomicAdd(&P.q.ctr->inferred, (unsigned long long)__popc(vm));
+        float o[GuideShape::kOut];
+        if (!tcForward<GuideShape>(smem, tmem, phase, o))
         {
             if (threadIdx.x == 0) atomicOr(&P.q.ctr->error, kTcTimeout);
             break;
         }
         if (ray != kNoRay)
         {
-            if (CACHE)
-                P.c.L[ray] = make_float4(fmaxf(o[0], 0.0f), fmaxf(o[1], 0.0f), fmaxf(o[2], 0.0f), 0.0f);
-            else
-            {
-                Lobes L;
-                headLobes(o, &L, alpha);
-                float4* dst = P.g.lobes + size_t(ray) * kLobeF4;
+            Lobes L;
+            headLobes(o, &L, alpha);
+            float4* dst = P.g.lobes + size_t(ray) * kLobeF4;
 #pragma unroll
-                for (int j = 0; j < kLobes; ++j) dst[j] = L.l[j];
-                dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
-                dst[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
-            }
+            for (int j = 0; j < kLobes; ++j) dst[j] = L.l[j];
+            dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
+            dst[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
         }
+    }
+    tcTeardown(tmem);
+}
+
+// Radiance-cache inference, second pass: persistent CTAs of 128 threads
+// stream 128 encoded rows at a time (compacted by kCacheEncode) through the
+// MLP on the tensor cores (tcgen05, cl_mlp_tc.cuh), thread t handling row t:
+// the predicted radiance per ray, clamped to be non-negative.
+__global__ void __launch_bounds__(guide::kTcThreads) kCacheMlp(Params P, const uint4* __restrict__ wt)
+{
+    using namespace guide;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t n = loadCount(&P.q.ctr->cacheCount);
+    if (blockIdx.x * kTcRows >= n) return; // see kGuideInfer
+    const uint32_t tmem  = tcSetup<CacheShape>(smem, wt);
+    unsigned char* tile  = smem + TcLayout<CacheShape>::kTile;
+    uint32_t       phase = 0u;
+    for (uint32_t k0 = blockIdx.x * kTcRows; k0 < n; k0 += gridDim.x * kTcRows)
+    {
+        const uint32_t k = k0 + threadIdx.x;
+        loadTile(tile, P.c.enc, k0, n);
+        const uint32_t ray = k < n ? P.c.encIdx[k] : kNoRay;
+        const uint32_t vm  = __ballot_sync(kFull, ray != kNoRay);
+        if (laneId() == 0u && vm) atomicAdd(&P.q.ctr->cacheQueries, (unsigned long long)__popc(vm));
+        float o[CacheShape::kOut];
+        if (!tcForward<CacheShape>(smem, tmem, phase, o))
+        {
+            if (threadIdx.x == 0) atomicOr(&P.q.ctr->error, kTcTimeout);
+            break;
+        }
+        if (ray != kNoRay) P.c.L[ray] = make_float4(fmaxf(o[0], 0.0f), fmaxf(o[1], 0.0f), fmaxf(o[2], 0.0f), 0.0f);
     }
     tcTeardown(tmem);
 }
@@ -1173,29 +1186,18 @@ cl_status Integrator::init(std::string* err)
                 &b, dl ? (const void*)kShadowResolve<true> : (const void*)kShadowResolve<false>, 128, 0),
             err);
     shadowBlocks_ = std::max(1, b) * numSMs_;
-    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::GuideShape, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kGuideMlpSmem),
-            err);
-    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::CacheShape, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kCacheMlpSmem),
-            err);
-    // The whole on-chip memory as shared memory: the occupancy query then
-    // counts the CTAs that the launch can hold (3 of the guide's, 4 of the
-    // cache's), not those of a default carveout.
-    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::GuideShape, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 100),
-            err);
-    CL_CUDA(cudaFuncSetAttribute(kMlpPass<guide::CacheShape, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 100),
-            err);
-    CL_TRY(tcResidentCtas((const void*)kMlpPass<guide::CacheShape, true>, kCacheMlpSmem, &b, err));
+    CL_CUDA(cudaFuncSetAttribute(kGuideInfer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideMlpSmem), err);
+    CL_CUDA(cudaFuncSetAttribute(kCacheMlp, cudaFuncAttributeMaxDynamicSharedMemorySize, kCacheMlpSmem), err);
+    // The whole on-chip memory as shared memory, so that the launch holds the
+    // CTAs counted by tcResidentCtas (3 of the guide's, 4 of the cache's).
+    CL_CUDA(cudaFuncSetAttribute(kGuideInfer, cudaFuncAttributePreferredSharedMemoryCarveout, 100), err);
+    CL_CUDA(cudaFuncSetAttribute(kCacheMlp, cudaFuncAttributePreferredSharedMemoryCarveout, 100), err);
+    CL_TRY(tcResidentCtas((const void*)kCacheMlp, kCacheMlpSmem, &b, err));
     cacheMlpBlocks_ = b * numSMs_;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kCacheEncode, kGuideEncBlock, 0), err);
     cacheEncodeBlocks_ = std::max(1, b) * numSMs_;
-    CL_TRY(tcResidentCtas((const void*)kMlpPass<guide::GuideShape, false>, kGuideMlpSmem, &b, err));
+    CL_TRY(tcResidentCtas((const void*)kGuideInfer, kGuideMlpSmem, &b, err));
     inferBlocks_ = b * numSMs_;
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kGuideEncode, kGuideEncBlock, 0), err);
-    encodeBlocks_ = std::max(1, b) * numSMs_;
     CL_TRY(ctr_.alloc(sizeof(Counters), err));
     CL_TRY(wp_.alloc(sizeof(WaveParams), err));
     CL_CUDA(cudaMemsetAsync(ctr_.p, 0, sizeof(Counters), stream_), err);
@@ -1731,8 +1733,6 @@ Params Integrator::params() const
     if (guide_)
     {
         P.g.lobes     = lobes_.as<float4>();
-        P.g.enc       = enc_.as<uint4>();
-        P.g.encIdx    = encIdx_.u();
         P.g.hist      = hist_.as<float4>();
         P.g.rec       = rec_.as<float4>();
         P.g.recCap    = recCap_;
@@ -1774,15 +1774,14 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     const uint32_t gmask = guide_ ? guideCfg_.class_mask : 0u;
     if (gmask)
     {
-        kGuideEncode<<<encodeBlocks_, kGuideEncBlock, 0, stream_>>>(P, guide_->grid(), cur);
-        kMlpPass<guide::GuideShape, false><<<inferBlocks_, guide::kTcThreads, kGuideMlpSmem, stream_>>>(
-            P, guide_->tcWeights(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
+        kGuideInfer<<<inferBlocks_, guide::kTcThreads, kGuideMlpSmem, stream_>>>(
+            P, guide_->grid(), cur, guide_->tcWeights(),
+            guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
     }
     if (cache_)
     {
         kCacheEncode<<<cacheEncodeBlocks_, kGuideEncBlock, 0, stream_>>>(P, cache_->grid(), cur);
-        kMlpPass<guide::CacheShape, true><<<cacheMlpBlocks_, guide::kTcThreads, kCacheMlpSmem, stream_>>>(
-            P, cache_->tcWeights(), 1.0f);
+        kCacheMlp<<<cacheMlpBlocks_, guide::kTcThreads, kCacheMlpSmem, stream_>>>(P, cache_->tcWeights());
     }
     if (profile) CL_CUDA(cudaEventRecord(evS_[4], stream_), err);
     for (int m = 0; m < 4; ++m)
@@ -2042,12 +2041,6 @@ cl_status Integrator::ensureGuideBuffers(std::string* err)
         CL_TRY(rec_.alloc(rb, err));
         graphValid_ = false;
     }
-    if (enc_.bytes != size_t(slots_) * guide::kIn * 2)
-    {
-        CL_TRY(enc_.alloc(size_t(slots_) * guide::kIn * 2, err));
-        CL_TRY(encIdx_.alloc(size_t(slots_) * 4, err));
-        graphValid_ = false;
-    }
     return CL_OK;
 }
 
@@ -2057,8 +2050,6 @@ cl_status Integrator::setGuiding(const cl_guide_config* cfg, std::string* err)
     {
         guide_.reset();
         lobes_.release();
-        enc_.release();
-        encIdx_.release();
         hist_.release();
         rec_.release();
         graphValid_ = false;

@@ -104,8 +104,6 @@ constexpr int kHistF4 = 5;  // {p, T.x} {n, T.y} {wo, T.z} {omega, BSDF pdf} {L 
 struct GuideDev
 {
     float4*  lobes;     // kLobeF4 per ray-queue index
-    uint4*   enc;       // encoded network inputs, 96 bf16 per guided ray (concatenated class order)
-    uint32_t* encIdx;   // ray-queue index of each encoded row (kNoRay: skipped)
     float4*  hist;      // (slots / recStride) x maxDepth x kHistF4
     float4*  rec;       // kRecordF4 per record
     uint32_t recCap;
@@ -268,10 +266,10 @@ private:
     // Guiding.
     std::unique_ptr<GuideNet> guide_;
     cl_guide_config           guideCfg_{};
-    DevBuf                    lobes_, hist_, rec_, enc_, encIdx_;
+    DevBuf                    lobes_, hist_, rec_;
     uint32_t                  recStride_ = 0, recCap_ = 0, histSlots_ = 0, histDepth_ = 0;
     float                     boxMin_[3] = {0, 0, 0}, boxScale_ = 1.0f;
-    int                       inferBlocks_ = 0, encodeBlocks_ = 0;
+    int                       inferBlocks_ = 0;
     uint64_t                  guideSamples_ = 0, guideRecordsLast_ = 0, guideInferred_ = 0;
     double                    guideLoss_ = 0.0;
     float                     msTrain_ = 0.0f, msInfer_ = 0.0f;
