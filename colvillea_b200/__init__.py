@@ -491,6 +491,15 @@ def normal_frame(inputs16):
     return out.reshape(-1, 3, 3)
 
 
+def tc_wait_timeout():
+    """cl_unit_tc_wait_timeout: the network kernels' bounded tensor-core wait on a
+    barrier that nothing arrives at.  Returns (status, seconds waited); the
+    expected status is CL_ERR_TIMEOUT after about one second."""
+    ns = ctypes.c_uint64(0)
+    st = N.lib().cl_unit_tc_wait_timeout(ctypes.byref(ns))
+    return int(st), ns.value * 1e-9
+
+
 def load_obj(path):
     """Meshes of a Wavefront OBJ file (one per o/g/usemtl group) as
     scenes.Mesh: triangulated, unified vertices, normals (smooth where the

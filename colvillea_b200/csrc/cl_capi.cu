@@ -62,6 +62,7 @@ cl_status unitMakeFrame(const float*, float*, float*, uint32_t, std::string*);
 cl_status unitFrame(const float*, const float*, const float*, const float*, float*, float*, uint32_t, std::string*);
 cl_status unitPcg(const uint32_t*, uint32_t*, uint32_t, std::string*);
 cl_status unitNormalFrame(const float*, float*, uint32_t, std::string*);
+cl_status unitTcWaitTimeout(uint64_t*, std::string*);
 cl_status unitTextureLookup(const cl_texture_desc*, const float*, float*, uint32_t, std::string*);
 cl_status unitSeq(const uint32_t*, uint32_t, uint32_t, float*, std::string*);
 cl_status unitDomeSample(const float*, uint32_t, uint32_t, const float*, const float*, const float*, const float*,
@@ -361,6 +362,11 @@ cl_status cl_unit_frame(const float* s, const float* t, const float* n, const fl
 cl_status cl_unit_normal_frame(const float* in, float* frame, uint32_t count)
 {
     return guarded([&](std::string* e) { return clb::unitNormalFrame(in, frame, count, e); });
+}
+
+cl_status cl_unit_tc_wait_timeout(uint64_t* waited_ns)
+{
+    return guarded([&](std::string* e) { return clb::unitTcWaitTimeout(waited_ns, e); });
 }
 
 cl_status cl_unit_texture_lookup(const cl_texture_desc* texture, const float* uv, float* rgba, uint32_t count)

@@ -3,6 +3,7 @@
 // run, one item per thread, host buffers in and out.
 #include "cl_device.cuh"
 #include "cl_internal.h"
+#include "cl_mlp_tc.cuh"
 #include "cl_texture.h"
 
 #include <vector>
@@ -208,6 +209,22 @@ struct Batch
 
 inline uint32_t grid(uint32_t n) { return (n + 127) / 128; }
 
+// The tensor-core kernels' bounded mbarrier wait on a barrier that nothing
+// arrives at: out[0] = 1 when the wait returned false (ran out), out[1..2] =
+// the nanoseconds waited.
+__global__ void kMbarTimeout(uint32_t* out)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    const uint32_t                             a = guide::smemAddr(&bar);
+    guide::mbarInit(a, 1u);
+    const uint64_t t0 = guide::globalTimerNs();
+    const bool     ok = guide::mbarWait(a, 0u);
+    const uint64_t dt = guide::globalTimerNs() - t0;
+    out[0]            = ok ? 0u : 1u;
+    out[1]            = uint32_t(dt);
+    out[2]            = uint32_t(dt >> 32);
+}
+
 } // namespace
 
 #define CL_REQ(cond)                                                                                                   \
@@ -403,6 +420,24 @@ cl_status unitNormalFrame(const float* in, float* out, uint32_t n, std::string* 
     CL_TRY(b.out(out, 9 * size_t(n), &y));
     kNormalFrame<<<grid(n), 128>>>(x, y, n);
     return b.finish();
+}
+
+cl_status unitTcWaitTimeout(uint64_t* waitedNs, std::string* err)
+{
+    CL_REQ(waitedNs);
+    Batch     b(err);
+    uint32_t  h[3] = {0u, 0u, 0u};
+    uint32_t* d;
+    CL_TRY(b.out(h, 3, &d));
+    kMbarTimeout<<<1, 1>>>(d);
+    CL_TRY(b.finish());
+    *waitedNs = uint64_t(h[1]) | (uint64_t(h[2]) << 32);
+    if (h[0])
+    {
+        *err = "tensor-core wait ran out (expected: nothing arrives at the barrier)";
+        return CL_ERR_TIMEOUT;
+    }
+    return CL_OK;
 }
 
 cl_status unitTextureLookup(const cl_texture_desc* t, const float* uv, float* rgba, uint32_t n, std::string* err)

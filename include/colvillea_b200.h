@@ -343,6 +343,11 @@ cl_status cl_unit_frame(const float* s, const float* t, const float* n, const fl
  * material.h:238-285): per item 16 floats {wo, dpdu, dpdv, base normal,
  * normal-map texel rgb, pull-up (0 or 1)}; out 9 floats {s, t, n}. */
 cl_status cl_unit_normal_frame(const float* in, float* frame, uint32_t count);
+/* The bounded wait of the tensor-core network kernels (an mbarrier wait of at
+ * most about one second) on a barrier that nothing arrives at: returns
+ * CL_ERR_TIMEOUT with the time waited, and the context stays usable.  No
+ * counterpart in the reference; it tests the failure path without a fault. */
+cl_status cl_unit_tc_wait_timeout(uint64_t* waited_ns);
 /* Lookups in one texture set up like the integrator's: uv pairs in, RGBA out. */
 cl_status cl_unit_texture_lookup(const cl_texture_desc* texture, const float* uv, float* rgba, uint32_t count);
 cl_status cl_unit_pcg4d(const uint32_t* in, uint32_t* out, uint32_t count);
