@@ -116,6 +116,7 @@ _SIGS = {
     "cl_build_textures": [vp, ctypes.POINTER(TextureDesc), u32],
     "cl_unit_normal_frame": [vp, vp, u32],
     "cl_unit_tc_wait_timeout": [ctypes.POINTER(ctypes.c_uint64)],
+    "cl_unit_binary_version": [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
     "cl_unit_texture_lookup": [ctypes.POINTER(TextureDesc), vp, vp, u32],
     "cl_build_emitters": [vp, ctypes.POINTER(EmitterDesc), u32],
     "cl_update_camera": [vp, ctypes.POINTER(Camera)],

@@ -4,6 +4,8 @@
 // src/core/devices/cudacommon.h:13-26).
 #include "cl_integrator.h"
 
+#include <atomic>
+
 #include <cstring>
 #include <memory>
 #include <new>
@@ -48,6 +50,17 @@ namespace clb
 static thread_local std::string gLastError;
 void setLastError(const std::string& msg) { gLastError = msg; }
 
+static std::atomic<bool> gTcSuspect{false};
+bool tcSuspect() { return gTcSuspect.load(); }
+void markTcSuspect() { gTcSuspect.store(true); }
+cl_status refuseIfTcSuspect(std::string* err)
+{
+    if (!gTcSuspect.load()) return CL_OK;
+    *err = "a tensor-core wait ran out earlier in this process; the CUDA context is suspect and network kernels "
+           "are refused (restart the process)";
+    return CL_ERR_STATE;
+}
+
 cl_status unitBsdfEval(uint32_t, const float*, const float*, const float*, float*, uint32_t, std::string*);
 cl_status unitBsdfPdf(uint32_t, const float*, const float*, const float*, float*, uint32_t, uint32_t, std::string*);
 cl_status unitBsdfSample(uint32_t, const float*, const float*, const float*, float*, float*, float*, uint32_t,
@@ -63,6 +76,7 @@ cl_status unitFrame(const float*, const float*, const float*, const float*, floa
 cl_status unitPcg(const uint32_t*, uint32_t*, uint32_t, std::string*);
 cl_status unitNormalFrame(const float*, float*, uint32_t, std::string*);
 cl_status unitTcWaitTimeout(uint64_t*, std::string*);
+cl_status unitBinaryVersion(int32_t*, int32_t*, std::string*);
 cl_status unitTextureLookup(const cl_texture_desc*, const float*, float*, uint32_t, std::string*);
 cl_status unitSeq(const uint32_t*, uint32_t, uint32_t, float*, std::string*);
 cl_status unitDomeSample(const float*, uint32_t, uint32_t, const float*, const float*, const float*, const float*,
@@ -369,6 +383,11 @@ cl_status cl_unit_tc_wait_timeout(uint64_t* waited_ns)
     return guarded([&](std::string* e) { return clb::unitTcWaitTimeout(waited_ns, e); });
 }
 
+cl_status cl_unit_binary_version(int32_t* binary_version, int32_t* ptx_version)
+{
+    return guarded([&](std::string* e) { return clb::unitBinaryVersion(binary_version, ptx_version, e); });
+}
+
 cl_status cl_unit_texture_lookup(const cl_texture_desc* texture, const float* uv, float* rgba, uint32_t count)
 {
     return guarded([&](std::string* e) { return clb::unitTextureLookup(texture, uv, rgba, count, e); });
@@ -484,31 +503,31 @@ cl_status cl_guide_get_params(const cl_guide* guide, float* params, uint64_t cou
 cl_status cl_guide_forward(cl_guide* guide, const float* in9, uint32_t count, float* out48)
 {
     CL_NEED(guide);
-    return guarded([&](std::string* e) { return guide->net->forward(in9, count, out48, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return guide->net->forward(in9, count, out48, e); });
 }
 
 cl_status cl_guide_gradient(cl_guide* guide, const float* rec14, uint32_t count, double* loss, float* grad)
 {
     CL_NEED(guide);
-    return guarded([&](std::string* e) { return guide->net->gradient(rec14, count, loss, grad, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return guide->net->gradient(rec14, count, loss, grad, e); });
 }
 
 cl_status cl_guide_train_step(cl_guide* guide, const float* rec14, uint32_t count, double* loss)
 {
     CL_NEED(guide);
-    return guarded([&](std::string* e) { return guide->net->trainStepHost(rec14, count, loss, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return guide->net->trainStepHost(rec14, count, loss, e); });
 }
 
 cl_status cl_guide_sample(cl_guide* guide, const float* in9, const float* u3, uint32_t count, float* dir3, float* pdf)
 {
     CL_NEED(guide);
-    return guarded([&](std::string* e) { return guide->net->sample(in9, u3, count, dir3, pdf, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return guide->net->sample(in9, u3, count, dir3, pdf, e); });
 }
 
 cl_status cl_guide_pdf(cl_guide* guide, const float* in9, const float* dir3, uint32_t count, float* pdf)
 {
     CL_NEED(guide);
-    return guarded([&](std::string* e) { return guide->net->pdf(in9, dir3, count, pdf, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return guide->net->pdf(in9, dir3, count, pdf, e); });
 }
 
 cl_status cl_integrator_set_guiding(cl_integrator* it, const cl_guide_config* config)
@@ -617,19 +636,19 @@ cl_status cl_cache_get_params(const cl_cache* cache, float* params, uint64_t cou
 cl_status cl_cache_forward(cl_cache* cache, const float* in9, uint32_t count, float* out16)
 {
     CL_NEED(cache);
-    return guarded([&](std::string* e) { return cache->net->forward(in9, count, out16, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return cache->net->forward(in9, count, out16, e); });
 }
 
 cl_status cl_cache_gradient(cl_cache* cache, const float* rec12, uint32_t count, double* loss, float* grad)
 {
     CL_NEED(cache);
-    return guarded([&](std::string* e) { return cache->net->gradient(rec12, count, loss, grad, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return cache->net->gradient(rec12, count, loss, grad, e); });
 }
 
 cl_status cl_cache_train_step(cl_cache* cache, const float* rec12, uint32_t count, double* loss)
 {
     CL_NEED(cache);
-    return guarded([&](std::string* e) { return cache->net->trainStepHost(rec12, count, loss, e); });
+    return guarded([&](std::string* e) { CL_TRY(clb::refuseIfTcSuspect(e)); return cache->net->trainStepHost(rec12, count, loss, e); });
 }
 
 cl_status cl_integrator_set_radiance_cache(cl_integrator* it, const cl_radiance_cache_config* config)

@@ -218,10 +218,35 @@ static __device__ __align__(256) unsigned char gDomeScratch[kScratchB];
 
 constexpr int kMaxDevices = 64;
 std::mutex    gScratchMutex;
+// Per device: the context the address was resolved in, and the address.  A
+// device address of a module variable belongs to one CUDA context, so a
+// caller that makes another context current on the same device (a context
+// created with the driver API, or the primary context re-created after
+// cudaDeviceReset) gets the address resolved again in that context.
+void*          gScratchCtx[kMaxDevices]  = {};
 unsigned char* gScratchAddr[kMaxDevices] = {};
 
-// Device address of gDomeScratch on the current device (resolved on the
-// first call per device).
+// cuCtxGetCurrent through the runtime's driver entry point (no link to the
+// driver library); null when the driver does not provide it.
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctxGetCurrentFn()
+{
+    static CtxGetCurrentFn fn = [] {
+        void*                           p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+        {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<CtxGetCurrentFn>(p);
+    }();
+    return fn;
+}
+
+// Device address of gDomeScratch in the current device's current context
+// (resolved on the first call per device and context).
 cl_status scratchAddress(unsigned char** out, std::string* err)
 {
     int dev = 0;
@@ -231,8 +256,11 @@ cl_status scratchAddress(unsigned char** out, std::string* err)
         *err = "device index out of range";
         return CL_ERR_INVALID_ARG;
     }
+    void*           ctx = nullptr;
+    CtxGetCurrentFn get = ctxGetCurrentFn();
+    if (get && get(&ctx) != 0) ctx = nullptr;
     std::lock_guard<std::mutex> lock(gScratchMutex);
-    if (!gScratchAddr[dev])
+    if (!gScratchAddr[dev] || gScratchCtx[dev] != ctx)
     {
         void*       p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, gDomeScratch);
@@ -242,7 +270,11 @@ cl_status scratchAddress(unsigned char** out, std::string* err)
             cudaGetLastError();
             return CL_ERR_CUDA;
         }
+        // The lookup makes the device's primary context current when no
+        // context was: record the context it resolved the address in.
+        if (get && get(&ctx) != 0) ctx = nullptr;
         gScratchAddr[dev] = static_cast<unsigned char*>(p);
+        gScratchCtx[dev]  = ctx;
     }
     *out = gScratchAddr[dev];
     return CL_OK;

@@ -907,6 +907,7 @@ cl_status HashNet<S, L>::forward(const float* in9, uint32_t n, float* out, std::
     CL_CUDA(cudaStreamSynchronize(st_), err);
     if (hf & kTcTimeout)
     {
+        markTcSuspect();
         *err = "network: a tensor-core wait ran out";
         return CL_ERR_TIMEOUT;
     }

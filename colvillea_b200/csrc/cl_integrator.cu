@@ -446,7 +446,10 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
     const SceneDev&  sc = P.sc;
     const uint32_t   n  = MAT < 0 ? loadCount(&P.q.ctr->rayCount[cur]) : loadCount(&P.q.ctr->classCount[MAT < 0 ? 0 : MAT]);
     const int        nxt = cur ^ 1;
-    const bool compatPdf   = CMP == 2 ? (wp.flags & CL_COMPAT_PDF) != 0 : CMP == 1;
+    // The guided mixture pdf needs the sampling densities of the BSDF: a
+    // guided kernel never takes the reference's pdf functions (setGuiding also
+    // refuses every CL_COMPAT_* flag).
+    const bool compatPdf   = !GUIDE && (CMP == 2 ? (wp.flags & CL_COMPAT_PDF) != 0 : CMP == 1);
     const bool compatFrame = CMP == 2 ? (wp.flags & CL_COMPAT_FRAME) != 0 : CMP == 1;
     const bool compatEsc   = CMP == 2 ? (wp.flags & CL_COMPAT_ESCAPE) != 0 : CMP == 1;
     const bool alias       = ALIAS;
@@ -1737,7 +1740,6 @@ Params Integrator::params() const
         P.g.rec       = rec_.as<float4>();
         P.g.recCap    = recCap_;
         P.g.classMask = guideCfg_.class_mask;
-        P.g.bsdfFrac  = guideCfg_.bsdf_fraction;
         P.g.histDepth = histDepth_;
     }
     for (int q = 0; q < 3; ++q) P.g.boxMin[q] = boxMin_[q];
@@ -1845,6 +1847,7 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
         return CL_ERR_STATE;
     }
     if (spp == 0) return CL_OK;
+    if (guide_ || cache_) CL_TRY(refuseIfTcSuspect(err));
     CL_TRY(ensureFilm(err));
     CL_TRY(ensureQueues(err));
     msRender_ = msTrace_ = msShade_ = msShadow_ = msInfer_ = 0.0f;
@@ -1996,7 +1999,11 @@ cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std
                (ch.error & 1u ? " (traversal stack overflow)" : "") + (ch.error & 4u ? " (shadow queue overflow)" : "") +
                (ch.error & 8u ? " (ray queue overflow)" : "") +
                (ch.error & guide::kTcTimeout ? " (tensor-core wait ran out)" : "");
-        if (ch.error & guide::kTcTimeout) return CL_ERR_TIMEOUT;
+        if (ch.error & guide::kTcTimeout)
+        {
+            markTcSuspect();
+            return CL_ERR_TIMEOUT;
+        }
         return (ch.error & 12u) ? CL_ERR_QUEUE_OVERFLOW : CL_ERR_STATE;
     }
     pathsDone_ += wp.totalPaths;

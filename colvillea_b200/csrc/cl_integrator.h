@@ -108,7 +108,6 @@ struct GuideDev
     float4*  rec;       // kRecordF4 per record
     uint32_t recCap;
     uint32_t classMask; // guided BSDF classes
-    float    bsdfFrac;
     float    boxScale;  // 1 / largest scene extent
     float    boxMin[3];
     uint32_t histDepth;

@@ -113,4 +113,12 @@ cl_status gatherTrianglePositions(const void* vtx, const void* triIdx, uint32_t 
 // Thread-local last error message (cl_last_error).
 void setLastError(const std::string& msg);
 
+// Process-wide: set once a tensor-core kernel reported that its bounded
+// mbarrier wait ran out.  Its tensor memory may then have been released under
+// a matrix operation still in flight, so the context is suspect and every
+// later call that would launch a network kernel is refused (CL_ERR_STATE).
+bool tcSuspect();
+void markTcSuspect();
+cl_status refuseIfTcSuspect(std::string* err);
+
 } // namespace clb

@@ -440,6 +440,16 @@ cl_status unitTcWaitTimeout(uint64_t* waitedNs, std::string* err)
     return CL_OK;
 }
 
+cl_status unitBinaryVersion(int32_t* binaryVersion, int32_t* ptxVersion, std::string* err)
+{
+    CL_REQ(binaryVersion && ptxVersion);
+    cudaFuncAttributes a{};
+    CL_CUDA(cudaFuncGetAttributes(&a, kMbarTimeout), err);
+    *binaryVersion = a.binaryVersion;
+    *ptxVersion    = a.ptxVersion;
+    return CL_OK;
+}
+
 cl_status unitTextureLookup(const cl_texture_desc* t, const float* uv, float* rgba, uint32_t n, std::string* err)
 {
     CL_REQ(t && uv && rgba);

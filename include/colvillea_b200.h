@@ -37,10 +37,17 @@ enum
     CL_ERR_CUDA           = 1, /* a CUDA runtime call failed */
     CL_ERR_OOM            = 2, /* device allocation failed */
     CL_ERR_QUEUE_OVERFLOW = 3, /* a work queue would have overflowed; items were dropped */
-    CL_ERR_TIMEOUT        = 4, /* a bounded device-side wait ran out */
+    CL_ERR_TIMEOUT        = 4, /* a bounded device-side wait ran out (see below) */
     CL_ERR_INVALID_ARG    = 5, /* bad argument (null, size, index out of range) */
     CL_ERR_STATE          = 6  /* call out of order (e.g. render before the scene is built) */
 };
+/* CL_ERR_TIMEOUT from a render or a network call means a tensor-core kernel
+ * stopped waiting for its own matrix operations after about one second and
+ * released its tensor memory while an operation may still have been in
+ * flight.  Treat the CUDA context as suspect and restart the process; the
+ * integrator refuses further renders with a network (CL_ERR_STATE).  The test
+ * entry point cl_unit_tc_wait_timeout issues no tensor-core operation and
+ * leaves the context usable. */
 
 /* IntegratorType (include/colvillea/librender/integrator.h:22-32). */
 typedef enum
@@ -348,6 +355,10 @@ cl_status cl_unit_normal_frame(const float* in, float* frame, uint32_t count);
  * CL_ERR_TIMEOUT with the time waited, and the context stays usable.  No
  * counterpart in the reference; it tests the failure path without a fault. */
 cl_status cl_unit_tc_wait_timeout(uint64_t* waited_ns);
+/* Target of the library's device code as the CUDA runtime reports it for one
+ * of its kernels (cudaFuncGetAttributes: binaryVersion 100 = sm_100a SASS).
+ * No counterpart in the reference. */
+cl_status cl_unit_binary_version(int32_t* binary_version, int32_t* ptx_version);
 /* Lookups in one texture set up like the integrator's: uv pairs in, RGBA out. */
 cl_status cl_unit_texture_lookup(const cl_texture_desc* texture, const float* uv, float* rgba, uint32_t count);
 cl_status cl_unit_pcg4d(const uint32_t* in, uint32_t* out, uint32_t count);
@@ -386,7 +397,11 @@ cl_status cl_dome_alias_sample(cl_integrator* integrator, const float* u2, float
  * Results equal the tables cl_build_emitters builds for the same texels.
  * The call is asynchronous on `stream`.  Its first call on a device resolves
  * the scratch array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture begins.  All calls
+ * current; make that first call before any stream capture begins.  The
+ * address is kept per device and per CUDA context: a caller that switches to
+ * another context on the same device (one made with the driver API, or the
+ * primary context re-created after cudaDeviceReset) gets it resolved again on
+ * its first call in that context, which then also belongs before a capture.  All calls
  * on a device share the one scratch array (each call overwrites every scratch
  * value it reads, so nothing needs clearing), so calls whose work overlaps on
  * the GPU (different streams, or threads) race: serialise them. */

@@ -7,8 +7,8 @@ stores inputs and outputs.  The oracle (oracle/liboracle.so) is pinned against
 these vectors by tests/test_oracle_golden.py; the GPU kernels are then checked
 against the oracle.
 
-Needs the reference tree (REF env var, default /root/reference); run it where
-that tree exists:  python tests/golden/gen_golden.py
+Needs the reference tree, named by the REF environment variable (no default):
+    REF=<reference checkout> python tests/golden/gen_golden.py
 """
 import ctypes
 import os
@@ -47,7 +47,10 @@ def bsdf_params(rng, n, btype):
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref")], check=True)
+    ref = os.environ.get("REF")
+    if not ref:
+        sys.exit("REF is not set: REF=<reference checkout> python tests/golden/gen_golden.py")
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), f"REF={ref}"], check=True)
     L = ctypes.CDLL(REF_LIB)
     rng = np.random.default_rng(20260101)
     g = {}

@@ -165,3 +165,11 @@ def test_unit_entry_points_reject_bad_input(native):
     # zero-size batches are valid no-ops
     z = np.zeros(1, np.float32)
     assert L.cl_unit_warp(P(z), P(z), P(z), 0) == N.CL_OK
+
+
+def test_loaded_kernels_are_sm100a(native):
+    """The CUDA runtime runs the library's sm_100a SASS (cudaFuncGetAttributes)."""
+    import ctypes
+    bv, pv = ctypes.c_int32(0), ctypes.c_int32(0)
+    N.call("cl_unit_binary_version", ctypes.byref(bv), ctypes.byref(pv))
+    assert bv.value == 100, bv.value
