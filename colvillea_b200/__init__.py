@@ -231,6 +231,11 @@ class Integrator:
         N.call("cl_get_dome_tables", self._h, _ptr(pU), _ptr(cU), _ptr(pV), _ptr(cV))
         return pU, cU, pV, cV
 
+    def domeAliasTables(self, w, h):
+        row = np.zeros(2 * h, np.uint32); col = np.zeros(2 * w * h, np.uint32)
+        N.call("cl_get_dome_alias_tables", self._h, _ptr(row), _ptr(col))
+        return row, col
+
     def domeAliasSample(self, u2):
         u2 = _f32(u2)
         n = len(u2)
@@ -459,9 +464,19 @@ def _guide_stats(self):
     return s.as_dict()
 
 
+def _guide_probe(self, capacity):
+    """First-wave rows of the fused guide inference: (n, 52) float32 per
+    guided ray {in9, ray index bits, 8 x (mu, kappa), 8 weights, pad}."""
+    rows = np.zeros((max(int(capacity), 1), 52), np.float32)
+    n = ctypes.c_uint32()
+    N.call("cl_integrator_guide_probe", self._h, int(capacity), _ptr(rows), ctypes.byref(n))
+    return rows[:n.value]
+
+
 Integrator.setGuiding = _set_guiding
 Integrator.guide = _guide
 Integrator.guideStats = _guide_stats
+Integrator.guideProbe = _guide_probe
 
 
 # --- scene ingestion and film output (MeshImporter / ImageUtils, src/delegate) ---

@@ -308,6 +308,18 @@ cl_status cl_get_dome_tables(cl_integrator* it, float* pU, float* cU, float* pV,
     return guarded([&](std::string* e) { return it->impl.domeTables(pU, cU, pV, cV, e); });
 }
 
+cl_status cl_integrator_guide_probe(cl_integrator* it, uint32_t capacity, float* rows, uint32_t* count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.guideProbe(capacity, rows, count, e); });
+}
+
+cl_status cl_get_dome_alias_tables(cl_integrator* it, uint32_t* alias_row, uint32_t* alias_col)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.domeAliasTables(alias_row, alias_col, e); });
+}
+
 cl_status cl_dome_alias_sample(cl_integrator* it, const float* u2, float* dir, float* pdf, float* value, uint32_t count)
 {
     CL_NEED(it);

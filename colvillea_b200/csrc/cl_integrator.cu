@@ -815,7 +815,7 @@ __device__ __forceinline__ uint32_t guidedCounts(const Params& P, uint32_t* n0, 
 // ends in the radiance cache here.
 __device__ __forceinline__ uint32_t encodeGuideRow(const Params& P, const guide::GridView& g, int cur, uint32_t k,
                                                    uint32_t n0, uint32_t n1, uint32_t maxDepth, f3 bmin,
-                                                   uint32_t (&r)[guide::kIn / 2])
+                                                   uint32_t (&r)[guide::kIn / 2], float* in9 = nullptr)
 {
     const uint32_t c     = k < n0 ? 0u : (k < n0 + n1 ? 1u : 2u);
     const uint32_t pos   = k - (c == 0u ? 0u : (c == 1u ? n0 : n0 + n1));
@@ -841,6 +841,12 @@ __device__ __forceinline__ uint32_t encodeGuideRow(const Params& P, const guide:
     }
     guide::oneBlobPacked(a.ns, r + guide::kHashF / 2);
     guide::oneBlobPacked(f3{-rd.x, -rd.y, -rd.z}, r + (guide::kHashF + 2 * guide::kBlob) / 2);
+    if (in9)
+    {
+        const float v[9] = {pn.x, pn.y, pn.z, a.ns.x, a.ns.y, a.ns.z, -rd.x, -rd.y, -rd.z};
+#pragma unroll
+        for (int q = 0; q < 9; ++q) in9[q] = v[q];
+    }
     return i;
 }
 
@@ -913,8 +919,10 @@ __global__ void __launch_bounds__(guide::kTcThreads) kGuideInfer(Params P, guide
         const uint32_t k = k0 + threadIdx.x;
         uint32_t       r[kIn / 2];
         uint32_t       ray = kNoRay;
+        float          in9[9];
+        const bool     probe = P.g.probe && k < P.g.probeCap;
         if (k < n)
-            ray = encodeGuideRow(P, g, cur, k, n0, n1, maxDepth, bmin, r);
+            ray = encodeGuideRow(P, g, cur, k, n0, n1, maxDepth, bmin, r, probe ? in9 : nullptr);
         else
 #pragma unroll
             for (int q = 0; q < kIn / 2; ++q) r[q] = 0u;
@@ -938,7 +946,25 @@ __global__ void __launch_bounds__(guide::kTcThreads) kGuideInfer(Params P, guide
             for (int j = 0; j < kLobes; ++j) dst[j] = L.l[j];
             dst[8] = make_float4(L.w[0], L.w[1], L.w[2], L.w[3]);
             dst[9] = make_float4(L.w[4], L.w[5], L.w[6], L.w[7]);
+            if (probe)
+            {
+                float* q = P.g.probe + size_t(k) * kProbeF;
+#pragma unroll
+                for (int j = 0; j < 9; ++j) q[j] = in9[j];
+                q[9] = __uint_as_float(ray);
+#pragma unroll
+                for (int j = 0; j < kLobeF4; ++j)
+                {
+                    const float4 v = dst[j];
+                    q[10 + 4 * j]  = v.x;
+                    q[11 + 4 * j]  = v.y;
+                    q[12 + 4 * j]  = v.z;
+                    q[13 + 4 * j]  = v.w;
+                }
+            }
         }
+        else if (probe)
+            P.g.probe[size_t(k) * kProbeF + 9] = __uint_as_float(kNoRay);
     }
     tcTeardown(tmem);
 }
@@ -1919,11 +1945,9 @@ cl_status Integrator::trainCache(std::string* err)
     return CL_OK;
 }
 
-cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std::string* err)
+cl_status Integrator::beginPass(uint32_t spp, bool record, bool cacheTrain, uint32_t* initSlots, std::string* err)
 {
-    const bool dl      = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
-    const bool profile = cfg_.flags & CL_PROFILE_STAGES;
-
+    const bool  dl = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
     WaveParams& wp = *hostWp_;
     wp.W           = W_;
     wp.H           = H_;
@@ -1943,6 +1967,16 @@ cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std
     c0.pathNext    = init;
     CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(Counters), cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaStreamSynchronize(stream_), err); // hostWp_/c0 reused next call
+    *initSlots = init;
+    return CL_OK;
+}
+
+cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std::string* err)
+{
+    const bool profile = cfg_.flags & CL_PROFILE_STAGES;
+    uint32_t   init    = 0u;
+    CL_TRY(beginPass(spp, record, cacheTrain, &init, err));
+    const WaveParams& wp = *hostWp_;
 
     CL_CUDA(cudaEventRecord(evA_, stream_), err);
     kRaygen<<<(init + 255) / 256, 256, 0, stream_>>>(params(), init);
@@ -2507,6 +2541,81 @@ cl_status Integrator::domeTables(float* pU, float* cU, float* pV, float* cV, std
     if (cU) CL_CUDA(cudaMemcpyAsync(cU, dome_.cU.p, a, cudaMemcpyDeviceToHost, stream_), err);
     if (pV) CL_CUDA(cudaMemcpyAsync(pV, dome_.pV.p, b, cudaMemcpyDeviceToHost, stream_), err);
     if (cV) CL_CUDA(cudaMemcpyAsync(cV, dome_.cV.p, b, cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    return CL_OK;
+}
+
+// Test probe of the fused guide inference: the first wave of the next
+// frame (camera rays), traced and run through kGuideInfer exactly as in a
+// render, with each guided row's network input (position in the scene box,
+// shading normal, outgoing direction), ray index and lobes copied out.  No
+// shading runs, so the film is untouched; the iteration index is kept.
+cl_status Integrator::guideProbe(uint32_t cap, float* rows, uint32_t* count, std::string* err)
+{
+    if (!rows || !count)
+    {
+        *err = "guide probe: null output";
+        return CL_ERR_INVALID_ARG;
+    }
+    if (!guide_ || !guideCfg_.class_mask)
+    {
+        *err = "guide probe: guiding is off";
+        return CL_ERR_STATE;
+    }
+    if (!sceneBuilt_ || !mats_.p || !hasCamera_)
+    {
+        *err = "guide probe needs a built scene and a camera";
+        return CL_ERR_STATE;
+    }
+    CL_TRY(refuseIfTcSuspect(err));
+    CL_TRY(ensureFilm(err));
+    CL_TRY(ensureQueues(err));
+    CL_TRY(ensureGuideBuffers(err));
+    DevBuf probe;
+    CL_TRY(probe.alloc(size_t(std::max(cap, 1u)) * kProbeF * 4, err));
+    uint32_t init = 0u;
+    CL_TRY(beginPass(1, false, false, &init, err));
+    Params P       = params();
+    P.g.probe      = probe.f();
+    P.g.probeCap   = cap;
+    Counters* c    = ctr_.as<Counters>();
+    kRaygen<<<(init + 255) / 256, 256, 0, stream_>>>(P, init);
+    kTraceClosest<false, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
+        P.sc.bvh, P.q.rqO[0], P.q.rqD[0], &c->rayCount[0], &c->fetchTrace, P.q.hit, c, classifyView());
+    kGuideInfer<<<inferBlocks_, guide::kTcThreads, kGuideMlpSmem, stream_>>>(
+        P, guide_->grid(), 0, guide_->tcWeights(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
+    CL_CUDA(cudaGetLastError(), err);
+    Counters ch;
+    CL_CUDA(cudaMemcpyAsync(&ch, ctr_.p, sizeof(Counters), cudaMemcpyDeviceToHost, stream_), err);
+    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    if (ch.error)
+    {
+        if (ch.error & guide::kTcTimeout) markTcSuspect();
+        *err = "guide probe: device error flags " + std::to_string(ch.error);
+        return (ch.error & guide::kTcTimeout) ? CL_ERR_TIMEOUT : CL_ERR_STATE;
+    }
+    uint32_t n = 0u;
+    for (int m = 0; m < 3; ++m)
+        if ((guideCfg_.class_mask >> m) & 1u) n += ch.classCount[m];
+    n      = std::min(n, cap);
+    *count = n;
+    if (n) CL_CUDA(cudaMemcpy(rows, probe.p, size_t(n) * kProbeF * 4, cudaMemcpyDeviceToHost), err);
+    return CL_OK;
+}
+
+cl_status Integrator::domeAliasTables(uint32_t* aliasRow, uint32_t* aliasCol, std::string* err)
+{
+    if (!hasDome_)
+    {
+        *err = "no dome emitter";
+        return CL_ERR_STATE;
+    }
+    if (aliasRow)
+        CL_CUDA(cudaMemcpyAsync(aliasRow, dome_.aliasRow.p, size_t(dome_.h) * 8, cudaMemcpyDeviceToHost, stream_), err);
+    if (aliasCol)
+        CL_CUDA(cudaMemcpyAsync(aliasCol, dome_.aliasCol.p, size_t(dome_.w) * dome_.h * 8, cudaMemcpyDeviceToHost,
+                                stream_),
+                err);
     CL_CUDA(cudaStreamSynchronize(stream_), err);
     return CL_OK;
 }

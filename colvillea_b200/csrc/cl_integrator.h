@@ -100,6 +100,7 @@ struct QueueDev
 // Guided path tracing: per-ray mixtures, per-slot vertex histories and the
 // training records (no counterpart in the reference).
 constexpr int kLobeF4 = 10; // 8 x {mu, kappa}, weights 0-3, weights 4-7
+constexpr int kProbeF = 52; // floats per probed guide row
 constexpr int kHistF4 = 5;  // {p, T.x} {n, T.y} {wo, T.z} {omega, BSDF pdf} {L snapshot, -}
 struct GuideDev
 {
@@ -108,6 +109,8 @@ struct GuideDev
     float4*  rec;       // kRecordF4 per record
     uint32_t recCap;
     uint32_t classMask; // guided BSDF classes
+    float*   probe;     // test probe (cl_integrator_guide_probe): per guided row k < probeCap,
+    uint32_t probeCap;  // kProbeF floats {in9, ray index bits, 40 lobe floats, 2 pad}; null in renders
     float    boxScale;  // 1 / largest scene extent
     float    boxMin[3];
     uint32_t histDepth;
@@ -171,6 +174,9 @@ public:
     cl_status occludedRays(const float* rays, uint32_t n, uint8_t* occ, std::string* err);
     cl_status traceStats(const float* rays, uint32_t n, uint64_t* nodes, uint64_t* tris, std::string* err);
     cl_status domeTables(float* pU, float* cU, float* pV, float* cV, std::string* err);
+    cl_status domeAliasTables(uint32_t* aliasRow, uint32_t* aliasCol, std::string* err);
+    cl_status guideProbe(uint32_t cap, float* rows, uint32_t* count, std::string* err);
+    cl_status beginPass(uint32_t spp, bool record, bool cacheTrain, uint32_t* initSlots, std::string* err);
     cl_status domeAliasSample(const float* u2, float* dir, float* pdf, float* val, uint32_t n, std::string* err);
 
     cl_status setGuiding(const cl_guide_config* cfg, std::string* err);

@@ -326,6 +326,10 @@ cl_status cl_trace_stats(cl_integrator* integrator, const float* rays, uint32_t 
 /* The dome's sampling tables as used by the device (reference layout,
  * hdridome.h:494-510): pUcondV_c and CDFpUcondV (w+1)*h, pV_c and CDFpV h+1. */
 cl_status cl_get_dome_tables(cl_integrator* integrator, float* pUcondV_c, float* cdfU, float* pV_c, float* cdfV);
+/* The dome's alias tables (CL_DOME_ALIAS sampling; no counterpart in the
+ * reference): alias_row 2*h uint32 {prob bits, row}, alias_col 2*w*h uint32
+ * {prob bits, column}.  Either pointer may be NULL. */
+cl_status cl_get_dome_alias_tables(cl_integrator* integrator, uint32_t* alias_row, uint32_t* alias_col);
 
 /* ---- Device functions on batches (the exact device code the integrator runs).
  * BSDF params: 11 floats per item {r.xyz, alpha, interior IOR, eta.xyz, k.xyz};
@@ -543,6 +547,15 @@ cl_status cl_integrator_set_guiding(cl_integrator* integrator, const cl_guide_co
 /* The integrator's network (owned by the integrator), or NULL when off. */
 cl_status cl_integrator_get_guide(cl_integrator* integrator, cl_guide** guide);
 cl_status cl_integrator_guide_stats(cl_integrator* integrator, cl_guide_stats* stats);
+/* Test probe of the integrator's fused guide inference (no counterpart in the
+ * reference): traces the camera rays of the next frame and runs the guide's
+ * inference on their hits exactly as a render does, without shading them (the
+ * film and the iteration index are unchanged).  For the first `capacity`
+ * guided rows it returns 52 floats each: in9 (the network input, as for
+ * cl_guide_forward), the ray index as uint32 bits (0xffffffff: not inferred),
+ * then 8 x {mu.xyz, kappa} and the 8 lobe weights (which sum to the
+ * probability of sampling the network), 2 unused.  *count = rows written. */
+cl_status cl_integrator_guide_probe(cl_integrator* integrator, uint32_t capacity, float* rows, uint32_t* count);
 
 /* ---- Neural radiance cache.
  * No counterpart in the reference.  A second hash-grid network, 96 -> 64 ->

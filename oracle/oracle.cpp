@@ -103,6 +103,7 @@ struct Scene
     bool               hasDome = false;
     Dome               dome;
     std::vector<float> domeTex, pU, cU, pV, cV;
+    std::vector<uint32_t> aliasRow, aliasCol; // set by orc_scene_set_dome_tables
     // camera
     V3<float> camPos{}, d00{}, ddu{}, ddv{};
 };
@@ -425,6 +426,7 @@ enum
     ORC_COMPAT_PDF       = 1u << 0, // Q1-Q3
     ORC_COMPAT_FRAME     = 1u << 1, // Q4 (PT only)
     ORC_COMPAT_ESCAPE    = 1u << 2, // Q5 + Q6 + Q9 + Q12 (reference MIS/escape bookkeeping)
+    ORC_DOME_ALIAS       = 1u << 4, // the GPU's alias-table dome sampler (tables set by orc_scene_set_dome_tables)
     ORC_DIRECT_LIGHTING  = 1u << 8,
 };
 
@@ -502,6 +504,34 @@ void orc_scene_dome_tables(void* sp, float* pU, float* cU, float* pV, float* cV)
     std::copy(s->cV.begin(), s->cV.end(), cV);
 }
 
+// Replaces the scene's dome tables with given ones (e.g. the GPU build's
+// FP64-built tables, rounded to FP32) and adds the alias tables used under
+// ORC_DOME_ALIAS; sizes as orc_scene_dome_tables, alias tables 2 uint32 per
+// entry (h per row, w*h per column).  Returns 0, or -1 without a dome.
+int orc_scene_set_dome_tables(void* sp, const float* pU, const float* cU, const float* pV, const float* cV,
+                              const uint32_t* aliasRow, const uint32_t* aliasCol)
+{
+    Scene* s = static_cast<Scene*>(sp);
+    if (!s->hasDome) return -1;
+    const size_t w = size_t(s->dome.w), h = size_t(s->dome.h);
+    s->pU.assign(pU, pU + (w + 1) * h);
+    s->cU.assign(cU, cU + (w + 1) * h);
+    s->pV.assign(pV, pV + h + 1);
+    s->cV.assign(cV, cV + h + 1);
+    if (aliasRow && aliasCol)
+    {
+        s->aliasRow.assign(aliasRow, aliasRow + 2 * h);
+        s->aliasCol.assign(aliasCol, aliasCol + 2 * w * h);
+    }
+    s->dome.pUcondV_c = s->pU.data();
+    s->dome.cdfU      = s->cU.data();
+    s->dome.pV_c      = s->pV.data();
+    s->dome.cdfV      = s->cV.data();
+    s->dome.aliasRow  = s->aliasRow.empty() ? nullptr : s->aliasRow.data();
+    s->dome.aliasCol  = s->aliasCol.empty() ? nullptr : s->aliasCol.data();
+    return 0;
+}
+
 // rays: 8 floats each {o.xyz, tmin, d.xyz, tmax}.
 void orc_trace(void* sp, const float* rays, uint32_t n, int bruteforce, float* t, uint32_t* id, float* b1, float* b2,
                int threads)
@@ -540,10 +570,10 @@ struct Counters
     uint64_t closest = 0, shadow = 0;
 };
 
-inline V3<float> emitterSample(const Scene& s, const Scene::Em& e, V2<float> u, V3<float>* dir, float* pdf)
+inline V3<float> emitterSample(const Scene& s, const Scene::Em& e, V2<float> u, V3<float>* dir, float* pdf, bool alias)
 {
     if (e.type == 0) return directionalSample(e.dir, u, dir, pdf);
-    return domeSample(s.dome, u, dir, pdf);
+    return domeSample(s.dome, u, dir, pdf, alias);
 }
 
 inline float maxComp(V3<float> v)
@@ -562,6 +592,7 @@ V3<float> tracePath(const Scene& s, const orc_config& cfg, uint32_t W, uint32_t 
     const bool compatFrame  = cfg.flags & ORC_COMPAT_FRAME;
     const bool compatEscape = cfg.flags & ORC_COMPAT_ESCAPE;
     const bool dl           = cfg.flags & ORC_DIRECT_LIGHTING;
+    const bool alias        = (cfg.flags & ORC_DOME_ALIAS) && !s.aliasRow.empty();
     const uint32_t N        = uint32_t(s.emitters.size());
 
     Rng       rng{px, py, frame, 0};
@@ -638,7 +669,7 @@ V3<float> tracePath(const Scene& s, const orc_config& cfg, uint32_t W, uint32_t 
             V3<float> ldir{0, 0, 0};
             float     lpdf  = 0.0f;
             const auto& em  = s.emitters[pick];
-            V3<float> value = emitterSample(s, em, us, &ldir, &lpdf);
+            V3<float> value = emitterSample(s, em, us, &ldir, &lpdf, alias);
             if (compatEscape) value = value * float(N);
             if (lpdf == 0.0f) value = {0, 0, 0};
             if (nonzero(value) && lpdf > 0.0f)

@@ -6,6 +6,8 @@
 // test.  See orc_core.h for the rules this restatement follows.
 #pragma once
 
+#include <cstring>
+
 #include "orc_core.h"
 
 #include <vector>
@@ -145,6 +147,10 @@ struct Dome
     const float* cdfU      = nullptr;
     const float* pV_c      = nullptr;
     const float* cdfV      = nullptr;
+    // Alias tables of the B200 build (not in the reference): {prob bits,
+    // alias} per row (h entries) and per column of each row (w*h entries).
+    const uint32_t* aliasRow = nullptr;
+    const uint32_t* aliasCol = nullptr;
 };
 
 // Preprocessing, FP32, in the reference's order: prefiltering
@@ -266,6 +272,60 @@ inline float pdf2D(const Dome& d, V2<float> s)
     return d.pUcondV_c[size_t(tv) * (d.w + 1) + tu] / d.pV_c[d.h];
 }
 
+// Two-level alias sampling over the same density (the GPU's dome sampler,
+// not in the reference; restated here from colvillea_b200's device code, so
+// that same-seed renders with alias sampling can be compared).  Rows by the
+// marginal table, then columns by the row's table; each level takes one
+// uniform: integer part = bucket, fraction = coin and, rescaled, the offset
+// inside the chosen cell.  pdf is the CDF sampler's (same table values).
+inline float bitsToFloat(uint32_t b)
+{
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+}
+inline V2<float> sample2DAlias(const Dome& d, V2<float> r, float* pdf)
+{
+    float    yv = r.y * float(d.h);
+    uint32_t i  = std::min(uint32_t(yv), uint32_t(d.h) - 1);
+    float    fr = yv - float(i);
+    float    p  = bitsToFloat(d.aliasRow[2 * size_t(i)]);
+    uint32_t row;
+    float    dv;
+    if (fr < p)
+    {
+        row = i;
+        dv  = fr / p;
+    }
+    else
+    {
+        row = d.aliasRow[2 * size_t(i) + 1];
+        dv  = (fr - p) / (1.0f - p);
+    }
+    float    xv = r.x * float(d.w);
+    uint32_t j  = std::min(uint32_t(xv), uint32_t(d.w) - 1);
+    float    fc = xv - float(j);
+    size_t   e  = size_t(row) * d.w + j;
+    float    q  = bitsToFloat(d.aliasCol[2 * e]);
+    uint32_t col;
+    float    du;
+    if (fc < q)
+    {
+        col = j;
+        du  = fc / q;
+    }
+    else
+    {
+        col = d.aliasCol[2 * e + 1];
+        du  = (fc - q) / (1.0f - q);
+    }
+    du = std::fmin(du, 0.99999994f);
+    dv = std::fmin(dv, 0.99999994f);
+    V2<float> uv{(float(col) + du) / float(d.w), (float(row) + dv) / float(d.h)};
+    *pdf = d.pUcondV_c[size_t(row) * (d.w + 1) + col] / d.pV_c[d.h];
+    return uv;
+}
+
 // acos argument of a direction's y: `clampY` (corrected estimator) keeps
 // directions whose y rounded past +-1 on the sphere; the reference passes y
 // unclamped (NaN there), reproduced by the compat estimator.
@@ -296,9 +356,9 @@ inline float domePdf(const Dome& d, V3<float> dir, bool clampY = false)
 }
 
 // HDRIDome::sampleDirect (hdridome.h:186-228).
-inline V3<float> domeSample(const Dome& d, V2<float> u, V3<float>* dir, float* pdf)
+inline V3<float> domeSample(const Dome& d, V2<float> u, V3<float>* dir, float* pdf, bool alias = false)
 {
-    V2<float> uv       = sample2D(d, u, pdf);
+    V2<float> uv       = alias ? sample2DAlias(d, u, pdf) : sample2D(d, u, pdf);
     float     theta    = kPiF * uv.y;
     float     phi      = -2 * kPiF * (uv.x - 0.5f);
     float     sinTheta = std::sin(theta), cosTheta = std::cos(theta);

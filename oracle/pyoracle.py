@@ -18,6 +18,7 @@ COMPAT_PDF = 1 << 0
 COMPAT_FRAME = 1 << 1
 COMPAT_ESCAPE = 1 << 2
 COMPAT_ALL = COMPAT_PDF | COMPAT_FRAME | COMPAT_ESCAPE
+DOME_ALIAS = 1 << 4
 DIRECT_LIGHTING = 1 << 8
 
 _lib = None
@@ -129,6 +130,16 @@ class OracleScene:
         pV = np.zeros(h + 1, np.float32); cV = np.zeros_like(pV)
         lib().orc_scene_dome_tables(ctypes.c_void_p(self.h), P(pU), P(cU), P(pV), P(cV))
         return pU, cU, pV, cV
+
+    def set_dome_tables(self, tables, alias=None):
+        """Use given dome tables (pU, cU, pV, cV) and, for DOME_ALIAS
+        renders, alias tables (row, col as uint32 pairs) instead of the
+        oracle's own FP32-built ones."""
+        pU, cU, pV, cV = (f32(t) for t in tables)
+        row, col = (u32(alias[0]), u32(alias[1])) if alias is not None else (None, None)
+        self._keep += [pU, cU, pV, cV, row, col]
+        r = lib().orc_scene_set_dome_tables(ctypes.c_void_p(self.h), P(pU), P(cU), P(pV), P(cV), P(row), P(col))
+        assert r == 0, "scene has no dome"
 
     def render(self, spp, max_depth=5, rr_start=0, flags=COMPAT_ALL, frame0=0, pixels=None, threads=8):
         """Returns (sum, sumsq) FP64 arrays of shape (npix, 3) and ray counters."""
