@@ -186,7 +186,10 @@ struct TrainArgs
     GridView        g;
     const uint2* __restrict__ wf;
     const uint2* __restrict__ wb;
+    const uint4* __restrict__ wt; // canonical bf16 weights (tensor-core layout)
     float2*        gradTable;
+    float*         gradMlp;       // FP32 weight gradients (the parameters after the hash table)
+    uint32_t*      err;           // device error flags (kTcTimeout)
     __nv_bfloat16* acts;
     __nv_bfloat16* deltas;
     double*        scal;     // [0] sum of weights, [1] loss, [3] sum of clamped weights
@@ -667,6 +670,308 @@ __global__ void __launch_bounds__(128) kWeightGrad(const __nv_bfloat16* __restri
     }
 }
 
+// ---------------------------------------------------------------------------
+// Training on the fifth-generation tensor cores (tcgen05): one kernel per
+// step does, for each 128-sample tile of the batch, the encoding, the
+// forward pass, the loss at the head, the backward pass and the weight
+// gradients.  A CTA of 128 threads owns one tile at a time, thread t sample
+// t (its hash-grid position stays in registers):
+//   forward, layer l:  acc[128 x out] = a_l[128 x in] . W_l^T   (M = 128,
+//                      A and B K-major) -> ReLU -> bf16 -> a_{l+1} (smem);
+//   head:              dl/do x (w / sum w) -> bf16 -> delta (smem);
+//   backward, layer l: dW_l[out x in] += delta^T . a_l  (M = 64, both
+//                      operands MN-major views of the same smem tiles, K =
+//                      the 128 samples; accumulated in TMEM over all of the
+//                      CTA's tiles), and acc[128 x in] = delta . W_l
+//                      (B = the MN-major view of the forward weights),
+//                      masked by ReLU'(a_l) -> bf16 -> delta of layer l-1;
+//                      at layer 0 the product over the 32 hash-feature
+//                      inputs is scattered to the hash table's gradient.
+// Every layer input of the tile stays in shared memory for the backward
+// pass; nothing is staged through global memory.  At the end each CTA adds
+// its weight gradients (TMEM, M = 64 layout: row r in lane 32 (r / 16) +
+// r % 16) to the global gradient.
+// ---------------------------------------------------------------------------
+template <class S> struct TrainTc
+{
+    static constexpr int L  = S::kLayers - 1; // the output layer
+    static constexpr int kW = S::kParams * 2; // canonical bf16 weights (cl_mlp_tc.cuh)
+    // Input tile of layer l (128 rows, canonical K-major, 2048 B per 8-column chunk).
+    __host__ __device__ static constexpr int act(int l)
+    {
+        return kW + (l == 0 ? 0 : kTcRows * kIn * 2 + (l - 1) * kTcRows * kWidth * 2);
+    }
+    static constexpr int kDelta = act(S::kLayers); // output-gradient tile, 64 columns (zero-padded)
+    static constexpr int kBar   = kDelta + kTcRows * kWidth * 2;
+    static constexpr int kSmem  = kBar + 16;
+    // TMEM: columns [0, 64) the layer accumulator; then dW_l (M = 64) at dw(l).
+    __host__ __device__ static constexpr uint32_t dw(int l) { return 64u + (l == 0 ? 0u : uint32_t(kIn + (l - 1) * kWidth)); }
+    static constexpr uint32_t kCols = 512;
+    static_assert(kW % 128 == 0 || kW % 16 == 0, "weights: 16-byte chunks");
+    static_assert(dw(S::kLayers) <= kCols, "weight gradients exceed tensor memory");
+    static_assert(S::kOut <= kWidth, "output gradient tile is 64 columns wide");
+};
+
+__device__ __forceinline__ void tcSyncForMma()
+{
+    asyncProxyFence();
+    tcFenceBefore();
+    __syncthreads();
+}
+
+// Waits for the committed MMAs; false in every thread when the wait ran out.
+__device__ __forceinline__ bool tcWaitAll(uint32_t bar, uint32_t& phase)
+{
+    const bool ok = mbarWait(bar, phase);
+    phase ^= 1u;
+    tcFenceAfter();
+    return __syncthreads_and(ok) != 0;
+}
+
+template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) kTrainTc(TrainArgs a)
+{
+    using T              = TrainTc<S>;
+    constexpr int L      = T::L;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const uint32_t count = *a.count, nB = min(count, a.batch);
+    const uint32_t tiles = (nB + kTcRows - 1) / kTcRows;
+    if (blockIdx.x >= tiles) return; // before any TMEM allocation
+    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+    {
+        uint4* w = reinterpret_cast<uint4*>(smem);
+        for (int i = int(t); i < T::kW / 16; i += kTcThreads) w[i] = __ldg(a.wt + i);
+    }
+    const uint32_t bar = smemAddr(smem + T::kBar);
+    if (t == 0) mbarInit(bar, 1u);
+    if (warp == 0) tmemAlloc(bar + 8u, T::kCols);
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    const uint32_t tmem  = *reinterpret_cast<volatile uint32_t*>(smem + T::kBar + 8);
+    const uint32_t tRow  = tmem + ((warp * 32u) << 16); // this warp's TMEM lanes
+    const uint32_t wS    = smemAddr(smem), dS = smemAddr(smem + T::kDelta);
+    const double   wsum  = a.clamp > 0.0f ? a.scal[3] : a.scal[0];
+    const float    invW  = wsum > 0.0 ? float(1.0 / wsum) : 0.0f;
+    uint32_t       phase = 0u;
+    bool           first = true, ok = true;
+    float          lossPart = 0.0f;
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x)
+    {
+        const uint32_t j     = tile * kTcRows + t;
+        const bool     valid = j < nB;
+        // Encoding -> a_0 row t.
+        f3       p{0.0f, 0.0f, 0.0f};
+        float4   r3{0.0f, 0.0f, 0.0f, 0.0f};
+        float    sw = 0.0f;
+        uint32_t r[kIn / 2];
+        if (valid)
+        {
+            const float4* R  = a.rec + kRecordF4 * size_t(recordOf(j, count, nB));
+            const float4  r0 = R[0], r1 = R[1], r2 = R[2];
+            r3               = R[3];
+            p                = clampUnit(f3{r0.x, r0.y, r0.z});
+            sw               = trainWeight(r0.w, a, nB) * invW;
+#pragma unroll
+            for (int l = 0; l < kLevels; ++l)
+            {
+                const float2 f = encodeLevel(a.g, l, p);
+                r[l]           = packBf16(f.x, f.y);
+            }
+            oneBlobPacked(f3{r1.x, r1.y, r1.z}, r + kHashF / 2);
+            oneBlobPacked(f3{r2.x, r2.y, r2.z}, r + (kHashF + 2 * kBlob) / 2);
+        }
+        else
+#pragma unroll
+            for (int q = 0; q < kIn / 2; ++q) r[q] = 0u;
+#pragma unroll
+        for (int c = 0; c < kIn / 8; ++c)
+            *tileChunk(smem + T::act(0), t, c) = make_uint4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+        // Forward.
+        float o[S::kOut];
+#pragma unroll 1
+        for (int l = 0; l <= L && ok; ++l)
+        {
+            tcSyncForMma();
+            if (t == 0)
+            {
+                tcFenceAfter();
+                const int      K = S::in(l), N = S::out(l);
+                const uint32_t aS = smemAddr(smem + T::act(l)), wl = wS + 2u * uint32_t(S::woff(l));
+                for (int ks = 0; ks < K / 16; ++ks)
+                    tcMma(tmem, tcDesc(aS + uint32_t(ks) * 2u * kTcChunk, kTcChunk, 128u),
+                          tcDesc(wl + uint32_t(ks * 2 * N * 16), uint32_t(N * 16), 128u), tcIdescMaj(128, N, false, false),
+                          ks > 0 ? 1u : 0u);
+                tcCommit(bar);
+            }
+            ok = tcWaitAll(bar, phase);
+            if (!ok) break;
+            if (l < L)
+            {
+                uint32_t v[kWidth / 16][16];
+#pragma unroll
+                for (int c = 0; c < kWidth / 16; ++c) tmemLd16(tRow + uint32_t(16 * c), v[c]);
+                tmemWait();
+                unsigned char* nxt = smem + T::act(l + 1);
+#pragma unroll
+                for (int c = 0; c < kWidth / 16; ++c)
+                {
+                    *tileChunk(nxt, t, 2 * c)     = packRelu8(v[c]);
+                    *tileChunk(nxt, t, 2 * c + 1) = packRelu8(v[c] + 8);
+                }
+            }
+            else
+            {
+                uint32_t v[S::kOut / 16][16];
+#pragma unroll
+                for (int c = 0; c < S::kOut / 16; ++c) tmemLd16(tRow + uint32_t(16 * c), v[c]);
+                tmemWait();
+#pragma unroll
+                for (int c = 0; c < S::kOut / 16; ++c)
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) o[16 * c + q] = __uint_as_float(v[c][q]);
+            }
+        }
+        if (!ok) break;
+        // Loss and output gradient -> delta row t (columns >= kOut zero).
+        {
+            float gr[S::kOut];
+            if (valid)
+            {
+                lossPart += sw * LOSS::eval(o, r3, a.learnSel, gr);
+#pragma unroll
+                for (int c = 0; c < S::kOut; ++c) gr[c] *= sw;
+            }
+            else
+#pragma unroll
+                for (int c = 0; c < S::kOut; ++c) gr[c] = 0.0f;
+            unsigned char* d = smem + T::kDelta;
+#pragma unroll
+            for (int c = 0; c < kWidth / 8; ++c)
+            {
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (8 * c < S::kOut)
+                    v = make_uint4(packBf16(gr[8 * c], gr[8 * c + 1]), packBf16(gr[8 * c + 2], gr[8 * c + 3]),
+                                   packBf16(gr[8 * c + 4], gr[8 * c + 5]), packBf16(gr[8 * c + 6], gr[8 * c + 7]));
+                *tileChunk(d, t, c) = v;
+            }
+        }
+        // Backward.
+#pragma unroll 1
+        for (int l = L; l >= 0 && ok; --l)
+        {
+            tcSyncForMma();
+            if (t == 0)
+            {
+                tcFenceAfter();
+                const int      K = S::out(l), I = S::in(l), N = l > 0 ? I : kHashF;
+                const uint32_t aS = smemAddr(smem + T::act(l)), wl = wS + 2u * uint32_t(S::woff(l));
+                // dW_l += delta^T a_l: A = delta (M = 64 output units, MN-major), B = a_l (N = I inputs,
+                // MN-major), K = 16 samples per instruction.
+                for (int ks = 0; ks < kTcRows / 16; ++ks)
+                    tcMma(tmem + T::dw(l), tcDesc(dS + uint32_t(ks) * 256u, 128u, kTcChunk),
+                          tcDesc(aS + uint32_t(ks) * 256u, 128u, kTcChunk), tcIdescMaj(64, I, true, true),
+                          (first && ks == 0) ? 0u : 1u);
+                // acc = delta . W_l: A = delta (K-major, K = the layer's outputs), B = W_l viewed with
+                // N = its inputs (MN-major: 8-input groups 16 K bytes apart, 8-output groups 128 B).
+                for (int ks = 0; ks < K / 16; ++ks)
+                    tcMma(tmem, tcDesc(dS + uint32_t(ks) * 2u * kTcChunk, kTcChunk, 128u),
+                          tcDesc(wl + uint32_t(ks) * 256u, 128u, uint32_t(16 * K)), tcIdescMaj(128, N, false, true),
+                          ks > 0 ? 1u : 0u);
+                tcCommit(bar);
+            }
+            ok = tcWaitAll(bar, phase);
+            if (!ok) break;
+            if (l > 0)
+            {
+                // delta of layer l-1 = acc masked by ReLU'(a_l): a zero bf16 input was a unit that was off.
+                uint32_t v[kWidth / 16][16];
+#pragma unroll
+                for (int c = 0; c < kWidth / 16; ++c) tmemLd16(tRow + uint32_t(16 * c), v[c]);
+                tmemWait();
+                const unsigned char* al = smem + T::act(l);
+                unsigned char*       d  = smem + T::kDelta;
+#pragma unroll
+                for (int c = 0; c < kWidth / 8; ++c)
+                {
+                    const uint4     m  = *tileChunk(const_cast<unsigned char*>(al), t, c);
+                    const uint32_t  mw[4] = {m.x, m.y, m.z, m.w};
+                    const uint32_t* src   = v[c >> 1] + 8 * (c & 1);
+                    uint32_t        pk[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                    {
+                        const float lo = (mw[q] & 0xffffu) ? __uint_as_float(src[2 * q]) : 0.0f;
+                        const float hi = (mw[q] >> 16) ? __uint_as_float(src[2 * q + 1]) : 0.0f;
+                        pk[q]          = packBf16(lo, hi);
+                    }
+                    *tileChunk(d, t, c) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                }
+            }
+            else
+            {
+                // Gradient of the 32 hash features (FP32): feature f of level l is column 2 l + f.
+                // (The TMEM load is warp-collective: every lane takes part, valid or not.)
+                uint32_t v[kHashF / 16][16];
+#pragma unroll
+                for (int c = 0; c < kHashF / 16; ++c) tmemLd16(tRow + uint32_t(16 * c), v[c]);
+                tmemWait();
+#pragma unroll
+                for (int lv = 0; lv < kLevels; ++lv)
+                {
+                    const float d0 = __uint_as_float(v[lv >> 3][2 * (lv & 7)]);
+                    const float d1 = __uint_as_float(v[lv >> 3][2 * (lv & 7) + 1]);
+                    if (!valid || (d0 == 0.0f && d1 == 0.0f)) continue;
+                    const Cell c  = gridCell(a.g.res[lv], p);
+                    float2*    gb = a.gradTable + (size_t(lv) << a.g.log2T);
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                    {
+                        const float w = cornerWeight(c, k);
+                        atomicAdd(gb + cornerIndex(a.g, lv, c, k), make_float2(w * d0, w * d1));
+                    }
+                }
+            }
+        }
+        first = false;
+    }
+    for (int off = 16; off > 0; off >>= 1) lossPart += __shfl_xor_sync(0xffffffffu, lossPart, off);
+    if (lane == 0 && lossPart != 0.0f) atomicAdd(&a.scal[1], double(lossPart));
+    if (!ok)
+    {
+        if (t == 0) atomicOr(a.err, kTcTimeout);
+    }
+    else if (!first)
+    {
+        // Weight gradients: row r of dW_l (M = 64) is in TMEM lane 32 (r / 16) + r % 16, so warp w
+        // holds rows 16 w .. 16 w + 15 in its lanes 0-15.
+        const int o = int(warp) * 16 + int(lane);
+#pragma unroll 1
+        for (int l = 0; l <= L; ++l)
+        {
+            const int I = S::in(l);
+            float*    G = a.gradMlp + S::woff(l);
+#pragma unroll 1
+            for (int c = 0; c < I / 16; ++c)
+            {
+                uint32_t v[16];
+                tmemLd16(tRow + T::dw(l) + uint32_t(16 * c), v);
+                tmemWait();
+                if (lane < 16u && o < S::out(l))
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                    {
+                        const float x = __uint_as_float(v[q]);
+                        if (x != 0.0f) atomicAdd(G + o * I + 16 * c + q, x);
+                    }
+            }
+        }
+    }
+    tcFenceBefore();
+    __syncthreads();
+    tcFenceAfter();
+    if (warp == 0) tmemFree(tmem, T::kCols);
+}
+
 // Adam (FP32 master parameters) over float4 groups - the hash block and
 // every weight block hold multiples of 4 floats - with two groups in flight
 // per thread; clears the gradient it consumed and refreshes the bf16 copy
@@ -805,6 +1110,7 @@ template <class S, class L> cl_status HashNet<S, L>::init(cudaStream_t st, std::
     CL_CUDA(cudaFuncSetAttribute(kInferUnit<S>, cudaFuncAttributePreferredSharedMemoryCarveout, 100), err);
     CL_CUDA(cudaFuncSetAttribute(kTrainFwdBwd<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrainSmem<S>::kAll),
             err);
+    CL_CUDA(cudaFuncSetAttribute(kTrainTc<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrainTc<S>::kSmem), err);
     int occ = 0;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kTrainFwdBwd<S, L>, kTrainWarps * 32,
                                                           TrainSmem<S>::kAll),
@@ -1006,6 +1312,7 @@ cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* coun
 {
     CL_CUDA(cudaMemsetAsync(scal_.p, 0, 16, st_), err);
     CL_CUDA(cudaMemsetAsync(scal_.as<double>() + 3, 0, 8, st_), err);
+    CL_CUDA(cudaMemsetAsync(trainErr(), 0, 4, st_), err);
     TrainArgs a;
     a.rec       = rec;
     a.count     = count;
@@ -1013,7 +1320,10 @@ cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* coun
     a.g         = grid();
     a.wf        = wf_.as<const uint2>();
     a.wb        = wb_.as<const uint2>();
+    a.wt        = wt_.as<const uint4>();
     a.gradTable = reinterpret_cast<float2*>(grad_.f());
+    a.gradMlp   = grad_.f() + hashParams_;
+    a.err       = trainErr();
     a.acts      = acts_.as<__nv_bfloat16>();
     a.deltas    = deltas_.as<__nv_bfloat16>();
     a.scal      = scal_.as<double>();
@@ -1026,11 +1336,8 @@ cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* coun
         kTrainPrep<<<numSMs_ * 2, 256, 0, st_>>>(a, 3);
         CL_CUDA(cudaGetLastError(), err);
     }
-    kTrainFwdBwd<S, L><<<trainBlocks_, kTrainWarps * 32, TrainSmem<S>::kAll, st_>>>(a);
-    CL_CUDA(cudaGetLastError(), err);
-    dim3 gg((cfg_.batch + kGradChunk - 1) / kGradChunk, S::kLayers);
-    kWeightGrad<S><<<gg, 128, 0, st_>>>(acts_.as<const __nv_bfloat16>(), deltas_.as<const __nv_bfloat16>(), count,
-                                        cfg_.batch, grad_.f() + hashParams_);
+    const uint32_t tiles = (cfg_.batch + kTcRows - 1) / kTcRows;
+    kTrainTc<S, L><<<std::min<uint32_t>(tiles, uint32_t(numSMs_)), kTcThreads, TrainTc<S>::kSmem, st_>>>(a);
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }
@@ -1068,8 +1375,7 @@ cl_status HashNet<S, L>::gradient(const float* rec, uint32_t n, double* loss, fl
     CL_CUDA(cudaMemcpyAsync(grad, grad_.p, paramCount() * 4, cudaMemcpyDeviceToHost, st_), err);
     CL_CUDA(cudaMemcpyAsync(loss, scal_.as<double>() + 1, 8, cudaMemcpyDeviceToHost, st_), err);
     CL_CUDA(cudaMemsetAsync(grad_.p, 0, paramCount() * 4, st_), err);
-    CL_CUDA(cudaStreamSynchronize(st_), err);
-    return CL_OK;
+    return checkTrainErr(err);
 }
 
 template <class S, class L>
@@ -1079,7 +1385,21 @@ cl_status HashNet<S, L>::trainStepHost(const float* rec, uint32_t n, double* los
     const uint32_t* cnt = reinterpret_cast<const uint32_t*>(scal_.as<unsigned char>() + 16);
     CL_TRY(trainDevice(rec_.as<const float4>(), cnt, err));
     if (loss) CL_CUDA(cudaMemcpyAsync(loss, scal_.as<double>() + 1, 8, cudaMemcpyDeviceToHost, st_), err);
+    return checkTrainErr(err);
+}
+
+// Synchronises the stream and reports a training kernel's timeout.
+template <class S, class L> cl_status HashNet<S, L>::checkTrainErr(std::string* err)
+{
+    uint32_t hf = 0u;
+    CL_CUDA(cudaMemcpyAsync(&hf, trainErr(), 4, cudaMemcpyDeviceToHost, st_), err);
     CL_CUDA(cudaStreamSynchronize(st_), err);
+    if (hf & kTcTimeout)
+    {
+        markTcSuspect();
+        *err = "network training: a tensor-core wait ran out";
+        return CL_ERR_TIMEOUT;
+    }
     return CL_OK;
 }
 

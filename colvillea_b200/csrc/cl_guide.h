@@ -50,6 +50,9 @@ public:
     const uint2*    fwdFrags() const { return wf_.as<uint2>(); }
     const uint4*    tcWeights() const { return wt_.as<uint4>(); }
     const double*   lossDev() const { return scal_.as<double>() + 1; }
+    // Device error flags of the last training step (kTcTimeout), read with its loss.
+    uint32_t*       trainErr() const { return reinterpret_cast<uint32_t*>(scal_.as<unsigned char>() + 52); }
+    cl_status       checkTrainErr(std::string* err);
     uint64_t        steps() const { return step_; }
 
 private:
@@ -71,7 +74,8 @@ private:
     DevBuf wf_, wb_;               // bf16 weight fragments (forward, backward)
     DevBuf wt_;                    // bf16 weights in the tensor-core canonical layout
     DevBuf acts_, deltas_;         // training staging, batch rows
-    DevBuf scal_;                  // {sum w, loss, count (u32), sum of clamped w}; byte 48: inference error flags
+    DevBuf scal_;                  // {sum w, loss, count (u32), sum of clamped w}; byte 48: inference error
+                                   // flags; byte 52: training error flags
     DevBuf rec_, io_, io2_;        // host-entry staging
 };
 

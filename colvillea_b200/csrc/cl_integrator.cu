@@ -112,10 +112,10 @@ struct HitAttr
     uint32_t material;
 };
 
-// Closest-hit attributes (optix.cu:137-227).
-__device__ __forceinline__ HitAttr hitAttributes(const SceneDev& sc, uint32_t prim, float b1, float b2)
+// Closest-hit attributes (optix.cu:137-227) of a triangle given by its
+// vertex ids and material (ti, the triangle's triIdx entry).
+__device__ __forceinline__ HitAttr hitAttributesTri(const SceneDev& sc, uint4 ti, float b1, float b2)
 {
-    uint4   ti = __ldg(sc.triIdx + prim);
     float4  a0 = __ldg(sc.vtx + 3 * size_t(ti.x)), a1 = __ldg(sc.vtx + 3 * size_t(ti.x) + 1), a2 = __ldg(sc.vtx + 3 * size_t(ti.x) + 2);
     float4  c0 = __ldg(sc.vtx + 3 * size_t(ti.y)), c1 = __ldg(sc.vtx + 3 * size_t(ti.y) + 1), c2 = __ldg(sc.vtx + 3 * size_t(ti.y) + 2);
     float4  e0 = __ldg(sc.vtx + 3 * size_t(ti.z)), e1 = __ldg(sc.vtx + 3 * size_t(ti.z) + 1), e2 = __ldg(sc.vtx + 3 * size_t(ti.z) + 2);
@@ -164,6 +164,10 @@ __device__ __forceinline__ HitAttr hitAttributes(const SceneDev& sc, uint32_t pr
     h.dpdu = dpdu;
     h.dpdv = dpdv;
     return h;
+}
+__device__ __forceinline__ HitAttr hitAttributes(const SceneDev& sc, uint32_t prim, float b1, float b2)
+{
+    return hitAttributesTri(sc, __ldg(sc.triIdx + prim), b1, b2);
 }
 
 // Camera path start (generateCameraRays, raygeneration.cu:83-102): path index
@@ -341,6 +345,7 @@ struct ClassifyView
     const float4* __restrict__ mats;
     uint32_t* classIdx;
     uint32_t  cap;
+    uint4*    hitIdx; // per ray: the hit triangle's triIdx entry (vertex ids, material), for the shading kernels
 };
 
 constexpr int kClassEscaped = 3;
@@ -374,8 +379,16 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
         {
             int cls = -1;
             if (i < n)
-                cls = prim == kMissPrim ? kClassEscaped
-                                        : int(__float_as_uint(__ldg(&cv.mats[kMatF4 * __ldg(&cv.triIdx[prim]).w].x)));
+            {
+                if (prim == kMissPrim)
+                    cls = kClassEscaped;
+                else
+                {
+                    const uint4 ti = __ldg(&cv.triIdx[prim]);
+                    cv.hitIdx[i]   = ti;
+                    cls            = int(__float_as_uint(__ldg(&cv.mats[kMatF4 * ti.w].x)));
+                }
+            }
 #pragma unroll
             for (int c = 0; c < 4; ++c)
             {
@@ -470,6 +483,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
         {
             slot          = P.q.rqSlot[cur][i];
             float4 hh     = P.q.hit[i];
+            uint4  ti     = MAT == kClassEscaped ? make_uint4(0u, 0u, 0u, 0u) : P.q.hitIdx[i];
             float4 rd     = P.q.rqD[cur][i];
             uint4  info   = P.q.psInfo[slot];
             uint32_t depth = info.z & 0xffu;
@@ -512,7 +526,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 finish = true;
             else
             {
-                HitAttr a    = hitAttributes(sc, prim, hh.z, hh.w);
+                HitAttr a    = hitAttributesTri(sc, ti, hh.z, hh.w);
                 MatTex  tx;
                 Bsdf    bsdf = loadMaterial(sc.mats, a.material, &tx);
                 if (tx.refl | tx.rough) applyTextures(sc.tex, tx, a.uv, &bsdf);
@@ -831,7 +845,7 @@ __device__ __forceinline__ uint32_t encodeGuideRow(const Params& P, const guide:
     }
     float4  hh = P.q.hit[i];
     float4  rd = P.q.rqD[cur][i];
-    HitAttr a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
+    HitAttr a  = hitAttributesTri(P.sc, P.q.hitIdx[i], hh.z, hh.w);
     f3      pn = guide::clampUnit((a.p - bmin) * P.g.boxScale);
 #pragma unroll
     for (int l = 0; l < guide::kLevels; ++l)
@@ -876,7 +890,7 @@ __global__ void __launch_bounds__(kGuideEncBlock, 6) kCacheEncode(Params P, guid
         if (!term) continue;
         float4   hh = P.q.hit[i];
         float4   rd = P.q.rqD[cur][i];
-        HitAttr  a  = hitAttributes(P.sc, __float_as_uint(hh.y), hh.z, hh.w);
+        HitAttr  a  = hitAttributesTri(P.sc, P.q.hitIdx[i], hh.z, hh.w);
         f3       pn = guide::clampUnit((a.p - bmin) * P.g.boxScale);
         uint32_t r[guide::kIn / 2];
 #pragma unroll
@@ -1283,7 +1297,8 @@ cl_status Integrator::flattenInstance(const HostMesh& m, const float* M, uint32_
         *err = "instance " + std::to_string(i) + ": singular transform";
         return CL_ERR_INVALID_ARG;
     }
-    double N9[9] = {(e * k - f * h) / det, -(d * k - f * g) / det, (d * h - e * g) / det,
+    // Inverse transpose of the linear part, row-major: IT[3 r + c] = inverse[c][r].
+    double IT[9] = {(e * k - f * h) / det, -(d * k - f * g) / det, (d * h - e * g) / det,
                     -(b * k - c * h) / det, (a * k - c * g) / det,  -(a * h - b * g) / det,
                     (b * f - c * e) / det,  -(a * f - c * d) / det, (a * e - b * d) / det};
     size_t   mv    = m.pos.size() / 3;
@@ -1310,8 +1325,8 @@ cl_status Integrator::flattenInstance(const HostMesh& m, const float* M, uint32_
                 P2[r] = float(double(M[4 * r]) * p[0] + double(M[4 * r + 1]) * p[1] + double(M[4 * r + 2]) * p[2] +
                               double(M[4 * r + 3]));
                 T2[r] = float(double(M[4 * r]) * t[0] + double(M[4 * r + 1]) * t[1] + double(M[4 * r + 2]) * t[2]);
-                // n' = N^T n with N = inverse of the linear part: n'_r = sum_c Ninv[c][r] n_c
-                N2[r] = float(N9[3 * 0 + r] * nn[0] + N9[3 * 1 + r] * nn[1] + N9[3 * 2 + r] * nn[2]);
+                // n' = (inverse of the linear part)^T n
+                N2[r] = float(IT[3 * r] * nn[0] + IT[3 * r + 1] * nn[1] + IT[3 * r + 2] * nn[2]);
             }
             for (int q = 0; q < 3; ++q)
             {
@@ -1692,6 +1707,7 @@ cl_status Integrator::ensureQueues(std::string* err)
         CL_TRY(rqSlot_[q].alloc(s * 4, err));
     }
     CL_TRY(hit_.alloc(s * 16, err));
+    CL_TRY(hitIdx_.alloc(s * 16, err));
     CL_TRY(sqO_.alloc(s * 16, err));
     CL_TRY(sqD_.alloc(s * 16, err));
     CL_TRY(sqL_.alloc(s * 16, err));
@@ -1720,7 +1736,7 @@ BvhView Integrator::bvhView() const
 
 ClassifyView Integrator::classifyView() const
 {
-    return ClassifyView{triIdx_.as<const uint4>(), mats_.as<const float4>(), classIdx_.u(), slots_};
+    return ClassifyView{triIdx_.as<const uint4>(), mats_.as<const float4>(), classIdx_.u(), slots_, hitIdx_.as<uint4>()};
 }
 
 Params Integrator::params() const
@@ -1742,6 +1758,7 @@ Params Integrator::params() const
         P.q.rqSlot[q] = rqSlot_[q].u();
     }
     P.q.hit       = hit_.as<float4>();
+    P.q.hitIdx    = hitIdx_.as<const uint4>();
     P.q.sqO       = sqO_.as<float4>();
     P.q.sqD       = sqD_.as<float4>();
     P.q.sqL       = sqL_.as<float4>();
@@ -1911,7 +1928,7 @@ cl_status Integrator::trainGuide(std::string* err)
     double loss = 0.0;
     CL_CUDA(cudaMemcpyAsync(&loss, guide_->lossDev(), 8, cudaMemcpyDeviceToHost, stream_), err);
     CL_CUDA(cudaEventSynchronize(evB_), err);
-    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    CL_TRY(guide_->checkTrainErr(err));
     float t = 0.0f;
     CL_CUDA(cudaEventElapsedTime(&t, evA_, evB_), err);
     msTrain_ += t;
@@ -1934,7 +1951,7 @@ cl_status Integrator::trainCache(std::string* err)
     double loss = 0.0;
     CL_CUDA(cudaMemcpyAsync(&loss, cache_->lossDev(), 8, cudaMemcpyDeviceToHost, stream_), err);
     CL_CUDA(cudaEventSynchronize(evB_), err);
-    CL_CUDA(cudaStreamSynchronize(stream_), err);
+    CL_TRY(cache_->checkTrainErr(err));
     float t = 0.0f;
     CL_CUDA(cudaEventElapsedTime(&t, evA_, evB_), err);
     msCacheTrain_ += t;

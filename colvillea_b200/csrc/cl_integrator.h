@@ -79,6 +79,7 @@ struct QueueDev
     float4*   rqD[2];
     uint32_t* rqSlot[2];
     float4*   hit;
+    const uint4* hitIdx; // per ray: the hit triangle's {vertex ids, material} (written with the class queues)
     float4*   sqO;  // {o.xyz, slot | kLastFlag bits}
     float4*   sqD;  // {d.xyz, -}
     float4*   sqL;  // {Li.xyz, -}
@@ -250,7 +251,7 @@ private:
     DevBuf       resolve_;
     cudaStream_t copyStream_ = nullptr;
     cudaEvent_t  evResolved_ = nullptr, evCopied_ = nullptr;
-    DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
+    DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, hitIdx_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
     DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_, vis_, classIdx_;
     uint32_t slots_ = 0, shadowCap_ = 0;
     WaveParams* hostWp_ = nullptr;   // pinned

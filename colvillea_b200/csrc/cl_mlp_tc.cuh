@@ -48,6 +48,18 @@ __host__ __device__ constexpr uint32_t tcIdesc(int n)
     return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(kTcRows >> 4) << 24);
 }
 
+// General form: M = 64 or 128, either operand K-major (0) or MN-major (bit
+// 15 for A, bit 16 for B).  An MN-major operand in the no-swizzle canonical
+// layout stores 8 consecutive M (or N) elements in 16 bytes, 8 such rows of
+// consecutive k 16 bytes apart; SBO = the stride of 8-element MN groups and
+// LBO = the stride of 8-row k groups.  The K-major tiles of this file,
+// viewed this way, are the transposed operands of the training kernel.
+__host__ __device__ constexpr uint32_t tcIdescMaj(int m, int n, bool aMN, bool bMN)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(aMN) << 15) | (uint32_t(bMN) << 16) |
+           (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
 // Shared-memory matrix descriptor: start address, LBO and SBO in 16-byte
 // units (bits 0-13, 16-29, 32-45), descriptor version 1 (bits 46-47), base
 // offset 0, no swizzle (bits 61-63 = 0).

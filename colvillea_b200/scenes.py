@@ -120,7 +120,8 @@ class Scene:
         base = 0
         for mesh_id, mat, xf in self.instances:
             m = self.meshes[mesh_id]
-            M = np.asarray(xf, np.float64).reshape(3, 4)
+            # the integrator receives the transform as float32 (cl_instance_desc)
+            M = np.asarray(xf, np.float32).astype(np.float64).reshape(3, 4)
             if np.array_equal(M, np.asarray(IDENTITY).reshape(3, 4)):
                 p, n, t = m.positions, m.normals, m.tangents
             else:
