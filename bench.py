@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--profile-nets", choices=["guide", "cache"], default=None,
                     help="short workload for ncu: cfg3 with guiding or cfg4 with the radiance cache, "
                          "2 training spp + 2 spp")
+    ap.add_argument("--guide-study", action="store_true",
+                    help="cfg3 guiding variants at equal spp (plain; guided everywhere; indirect vertices only; "
+                         "all BSDF classes; 32/64/128 training steps) against the FP64 reference (one JSON line)")
     ap.add_argument("--relmse-ref-spp", type=int, default=8192, help="spp of the cfg3 FP64 reference image")
     ap.add_argument("--relmse-ref-spp4", type=int, default=8192, help="spp of the cfg4 FP64 reference image")
     ap.add_argument("--relmse-seeds", type=int, default=3)
@@ -224,16 +227,13 @@ def ncu_traffic(config=2):
     return None
 
 
-def cpu_baseline(scene, seconds, threads):
-    """The oracle (the reference's algorithm restated in C++) on the host cores,
-    1 spp over a strided pixel sample of the same workload."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+def _oracle_rate(o, scene, seconds, threads):
+    """Paths per second of the oracle at `threads` host threads, 1 spp over an
+    evenly strided pixel sample sized to about `seconds` of work."""
     import numpy as np
     import pyoracle
-    pyoracle.build()
-    o = pyoracle.OracleScene(scene.flatten())
     npx = scene.width * scene.height
-    probe = np.arange(0, npx, max(1, npx // 2000), dtype=np.uint32)
+    probe = np.arange(0, npx, max(1, npx // (2000 if threads > 1 else 400)), dtype=np.uint32)
     t0 = time.perf_counter()
     o.render(1, max_depth=scene.max_depth, rr_start=scene.rr_start, flags=pyoracle.COMPAT_ALL, pixels=probe,
              threads=threads)
@@ -244,9 +244,23 @@ def cpu_baseline(scene, seconds, threads):
     _, _, cnt = o.render(1, max_depth=scene.max_depth, rr_start=scene.rr_start, flags=pyoracle.COMPAT_ALL,
                          pixels=pix, threads=threads)
     dt = time.perf_counter() - t0
-    return {"value": round(len(pix) / dt / 1e6, 6), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{len(pix)} of {npx} pixels (evenly strided), 1 spp, {dt:.1f} s; "
-                      f"{int(cnt[0])} closest + {int(cnt[1])} shadow rays ({(cnt[0] + cnt[1]) / dt / 1e6:.3f} Mrays/s)"}
+    sample = (f"{len(pix)} of {npx} pixels (evenly strided), 1 spp, {dt:.1f} s; {int(cnt[0])} closest + "
+              f"{int(cnt[1])} shadow rays ({(cnt[0] + cnt[1]) / dt / 1e6:.3f} Mrays/s)")
+    return round(len(pix) / dt / 1e6, 6), sample
+
+
+def cpu_baseline(scene, seconds, threads):
+    """The oracle (the reference's algorithm restated in C++) on the host cores,
+    1 spp over a strided pixel sample of the same workload: all threads, and
+    one thread (the two rates of the baseline plan)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    pyoracle.build()
+    o = pyoracle.OracleScene(scene.flatten())
+    value, sample = _oracle_rate(o, scene, seconds, threads)
+    v1, s1 = _oracle_rate(o, scene, min(seconds, 8.0), 1)
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
+            "single_thread": {"value": v1, "unit": UNIT, "cores": 1, "sample": s1}}
 
 
 def guided_relmse(args):
@@ -322,6 +336,34 @@ def scene_edit(it, s, args, spp=4):
                      "render_ms_per_spp": round(ms / spp, 3)}
     out["speedup_refit_vs_rebuild"] = round(out["rebuild"]["bvh_ms"] / max(out["refit"]["bvh_ms"], 1e-6), 1)
     return out
+
+
+def run_guide_study(args):
+    """Equal-spp table of guiding variants on cfg3 (128 spp each, training
+    included; 2 seeds): does the network lower the variance, and where."""
+    import colvillea_b200 as cb
+    from colvillea_b200 import evaluate, scenes
+    s3 = scenes.config3(0)
+    t0 = time.perf_counter()
+    ref = evaluate.reference(s3, args.relmse_ref_spp)
+    t_ref = time.perf_counter() - t0
+    G = cb.GuideConfig
+    variants = {
+        "guided": G(),
+        "guided_indirect": G(min_depth=2),
+        "guided_all_classes": G(class_mask=7),
+        "guided_train64": G(train_spp=64),
+        "guided_train128": G(train_spp=128),
+        "guided_indirect_train64": G(min_depth=2, train_spp=64),
+    }
+    rows = evaluate.equal_spp(s3, ref, args.relmse_spp, variants, seeds=2)
+    rnd = lambda d: {k: (round(v, 6) if isinstance(v, float) else ([round(x, 6) for x in v] if isinstance(v, list)
+                                                                    else v)) for k, v in d.items()}
+    print(json.dumps({"guide_study": "cfg3 (cfg1 scene, 1920x1080, depth 5, RR 3), corrected estimator, alias dome "
+                                     f"sampler; {args.relmse_spp} spp per variant incl. training; 2 seeds; reference "
+                                     f"{args.relmse_ref_spp} spp FP64 ({t_ref:.1f} s)",
+                      "rows": {k: rnd(v) for k, v in rows.items()}}))
+    return 0
 
 
 def run_extended(args):
@@ -419,6 +461,8 @@ def main():
         return run_profile_nets(args)
     if args.extended:
         return run_extended(args)
+    if args.guide_study:
+        return run_guide_study(args)
     import numpy as np
     import torch
     dist = Dist(args.gpus)
@@ -550,7 +594,12 @@ def main():
                      "timing": "kTraceClosest's CUDA-event time on its stream, in a stage-profiled pass of the "
                                "same steps"},
         "clocks": clk, "gpu_launches": launches,
-        "build": {"bvh_ms": round(st0["ms_bvh_build"], 2), "bvh_nodes": st0["bvh_nodes"],
+        # The first build of the process (cold: module loading, first allocations) and the second
+        # (the traversal-counter integrator's build of the same scene).
+        "build": {"bvh_ms": round(st0["ms_bvh_build"], 2), "bvh_ms_cold_wall": round(st0["ms_bvh_build_wall"], 2),
+                  "bvh_ms_cold_alloc": round(st0["ms_bvh_build_alloc"], 2),
+                  "bvh_ms_warm": round(sst["ms_bvh_build"], 2), "bvh_ms_warm_wall": round(sst["ms_bvh_build_wall"], 2),
+                  "bvh_ms_warm_alloc": round(sst["ms_bvh_build_alloc"], 2), "bvh_nodes": st0["bvh_nodes"],
                   "bvh_depth": st0["bvh_depth"], "dome_ms": round(st0["ms_dome_build"], 2)},
     }
     if e2e:

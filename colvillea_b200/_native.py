@@ -77,7 +77,8 @@ class Stats(ctypes.Structure):
                 ("last_rays_closest", ctypes.c_uint64), ("last_rays_shadow", ctypes.c_uint64),
                 ("ms_bvh_update", ctypes.c_float), ("ms_bvh_refit", ctypes.c_float), ("bvh_refits", u32),
                 ("bvh_rebuilds", u32),
-                ("bvh_sah", ctypes.c_double), ("bvh_sah_build", ctypes.c_double)]
+                ("bvh_sah", ctypes.c_double), ("bvh_sah_build", ctypes.c_double),
+                ("ms_bvh_build_wall", ctypes.c_float), ("ms_bvh_build_alloc", ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -88,7 +89,7 @@ class GuideConfig(ctypes.Structure):
                 ("learning_rate", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
                 ("epsilon", ctypes.c_float), ("bsdf_fraction", ctypes.c_float), ("batch", u32),
                 ("train_spp", u32), ("class_mask", u32), ("seed", u32), ("learn_selection", u32),
-                ("weight_clamp", ctypes.c_float)]
+                ("weight_clamp", ctypes.c_float), ("min_depth", u32)]
 
 
 class RadianceCacheConfig(ctypes.Structure):

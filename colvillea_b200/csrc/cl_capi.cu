@@ -50,6 +50,12 @@ namespace clb
 static thread_local std::string gLastError;
 void setLastError(const std::string& msg) { gLastError = msg; }
 
+double& allocMs()
+{
+    static thread_local double ms = 0.0;
+    return ms;
+}
+
 static std::atomic<bool> gTcSuspect{false};
 bool tcSuspect() { return gTcSuspect.load(); }
 void markTcSuspect() { gTcSuspect.store(true); }

@@ -1045,6 +1045,7 @@ void guideDefaultConfig(cl_guide_config* c)
     c->seed            = 1;
     c->learn_selection = 0u;
     c->weight_clamp    = 0.0f;
+    c->min_depth       = 1u;
 }
 
 cl_status guideResolutions(float nmin, float nmax, uint32_t* res)

@@ -28,6 +28,7 @@
 #include "cl_integrator.h"
 #include "cl_mlp_tc.cuh"
 
+#include <chrono>
 #include <cstdio>
 
 namespace clb
@@ -547,7 +548,17 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 f3    wo     = -d;
                 guide::Lobes G;
                 float        gf = 1.0f; // probability of BSDF sampling: 1 - sum of the lobe weights
-                if (GUIDE)
+                // Vertices shallower than the guide's minimum depth were not inferred: BSDF sampling
+                // alone (zero lobe weights), no training record.
+                const bool guided = GUIDE && depth >= P.g.minDepth;
+                if (GUIDE && !guided)
+#pragma unroll
+                    for (int k = 0; k < guide::kLobes; ++k)
+                    {
+                        G.l[k] = make_float4(0.0f, 0.0f, 1.0f, 1.0f);
+                        G.w[k] = 0.0f;
+                    }
+                if (guided)
                 {
                     const float4* lb = P.g.lobes + size_t(i) * kLobeF4;
 #pragma unroll
@@ -699,7 +710,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                             pushRay = true;
                             ndir    = dir;
                             info2   = (depth + 1u) | (rng.ctr << 8);
-                            if (GUIDE && wp.recStride && slot % wp.recStride == 0u && depth <= P.g.histDepth)
+                            if (guided && wp.recStride && slot % wp.recStride == 0u && depth <= P.g.histDepth)
                             {
                                 // Training history of this vertex (flushRecords).
                                 float4* h = P.g.hist + (size_t(slot / wp.recStride) * P.g.histDepth + depth - 1u) *
@@ -836,7 +847,7 @@ __device__ __forceinline__ uint32_t encodeGuideRow(const Params& P, const guide:
     const uint32_t i     = P.q.classIdx[size_t(c) * P.q.slots + pos];
     const uint32_t slot  = P.q.rqSlot[cur][i];
     const uint32_t depth = P.q.psInfo[slot].z & 0xffu;
-    if (depth == maxDepth ||
+    if (depth == maxDepth || depth < P.g.minDepth ||
         (P.c.termDepth && depth == P.c.termDepth && !(__float_as_uint(P.q.psE[slot].w) & kCacheTrainBit)))
     {
 #pragma unroll
@@ -1416,11 +1427,15 @@ cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, s
         for (int q = 0; q < 3; ++q) boxMin_[q] = lo[q] - 0.001f * ext;
         boxScale_ = 1.0f / ext;
     }
+    const auto   w0 = std::chrono::steady_clock::now();
+    const double a0 = allocMs();
     CL_CUDA(cudaEventRecord(evA_, stream_), err);
     CL_TRY(buildWideBvh(triPos_.f(), uint32_t(nt), stream_, &bvh_, err));
     CL_CUDA(cudaEventRecord(evB_, stream_), err);
     CL_CUDA(cudaEventSynchronize(evB_), err);
     CL_CUDA(cudaEventElapsedTime(&msBvh_, evA_, evB_), err);
+    msBvhWall_  = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count());
+    msBvhAlloc_ = float(allocMs() - a0);
     triPos_.release();
     CL_TRY(wideBvhSahCost(bvh_, stream_, &sahBuild_, err));
     sah_        = sahBuild_;
@@ -1506,7 +1521,9 @@ cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, cons
     }
     if (rebuild)
     {
-        float msBuild = 0.0f;
+        float        msBuild = 0.0f;
+        const auto   w0      = std::chrono::steady_clock::now();
+        const double a0      = allocMs();
         CL_CUDA(cudaEventRecord(evA_, stream_), err);
         CL_TRY(triPos_.alloc(size_t(numTris_) * 36, err));
         CL_TRY(gatherTrianglePositions(vtx_.p, triIdx_.p, numTris_, triPos_.f(), stream_, err));
@@ -1521,7 +1538,9 @@ cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, cons
         CL_CUDA(cudaEventSynchronize(evB_), err);
         CL_CUDA(cudaEventElapsedTime(&msBuild, evA_, evB_), err);
         ms += msBuild;
-        msBvh_ = msBuild;
+        msBvh_      = msBuild;
+        msBvhWall_  = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count());
+        msBvhAlloc_ = float(allocMs() - a0);
         CL_TRY(wideBvhSahCost(bvh_, stream_, &sahBuild_, err));
         sah_        = sahBuild_;
         graphValid_ = false; // new node and triangle buffers
@@ -1783,6 +1802,7 @@ Params Integrator::params() const
         P.g.rec       = rec_.as<float4>();
         P.g.recCap    = recCap_;
         P.g.classMask = guideCfg_.class_mask;
+        P.g.minDepth  = std::max(guideCfg_.min_depth, 1u);
         P.g.histDepth = histDepth_;
     }
     for (int q = 0; q < 3; ++q) P.g.boxMin[q] = boxMin_[q];
@@ -2382,6 +2402,8 @@ void Integrator::stats(cl_stats* s) const
     s->last_rays_closest = lastRaysC_;
     s->last_rays_shadow  = lastRaysS_;
     s->ms_bvh_update     = msBvhUpdate_;
+    s->ms_bvh_build_wall  = msBvhWall_;
+    s->ms_bvh_build_alloc = msBvhAlloc_;
     s->ms_bvh_refit      = msBvhRefit_;
     s->bvh_refits        = refits_;
     s->bvh_rebuilds      = rebuilds_;

@@ -110,6 +110,7 @@ struct GuideDev
     float4*  rec;       // kRecordF4 per record
     uint32_t recCap;
     uint32_t classMask; // guided BSDF classes
+    uint32_t minDepth;  // guided vertices have depth >= minDepth
     float*   probe;     // test probe (cl_integrator_guide_probe): per guided row k < probeCap,
     uint32_t probeCap;  // kProbeF floats {in9, ray index bits, 40 lobe floats, 2 pad}; null in renders
     float    boxScale;  // 1 / largest scene extent
@@ -267,6 +268,7 @@ private:
     uint32_t  waves_ = 0, launches_ = 0;
     uint64_t  lastNodes_ = 0, lastTris_ = 0, lastNodesS_ = 0, lastTrisS_ = 0, lastRaysC_ = 0, lastRaysS_ = 0;
     float     msBvh_ = 0, msDome_ = 0, msRender_ = 0, msTrace_ = 0, msShade_ = 0, msShadow_ = 0;
+    float     msBvhWall_ = 0, msBvhAlloc_ = 0; // last full build: host wall time, and its cudaMalloc share
     cudaEvent_t evA_ = nullptr, evB_ = nullptr, evS_[6] = {};
 
     // Guiding.

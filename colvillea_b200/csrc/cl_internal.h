@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -14,6 +15,10 @@
 
 namespace clb
 {
+// Host milliseconds this thread has spent in cudaMalloc (the allocation share
+// of a build's wall time).
+double& allocMs();
+
 // Device allocation owned by one object (the reference's DeviceBuffer,
 // src/core/devices/cudabuffer.h:39-96, with errors returned, not exit()).
 struct DevBuf
@@ -34,7 +39,9 @@ struct DevBuf
     {
         release();
         if (n == 0) n = 16;
-        cudaError_t e = cudaMalloc(&p, n);
+        const auto  t0 = std::chrono::steady_clock::now();
+        cudaError_t e  = cudaMalloc(&p, n);
+        allocMs() += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         if (e != cudaSuccess)
         {
             p    = nullptr;

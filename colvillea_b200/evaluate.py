@@ -112,3 +112,40 @@ def mlp_throughput(scene, guide=None, spp=8, max_depth=None):
             "train_tflops": g0["samples_trained"] * TRAIN_FLOPS / (g0["ms_train"] * 1e-3) / 1e12
             if g0["ms_train"] > 0 else None,
             "flops_per_sample": {"inference": INFER_FLOPS, "training": TRAIN_FLOPS}}
+
+
+def equal_spp(scene, ref, spp, variants, seeds=2, max_depth=None, seed_stride=1 << 20):
+    """relMSE after `spp` samples per pixel for the plain tracer and for each
+    guided variant (`variants`: name -> GuideConfig; a variant's training
+    steps are part of its `spp`), over `seeds` disjoint frame ranges with a
+    fresh network per seed.  relMSE at equal spp measures the estimators'
+    variance (their bias is zero); each entry also gives the device time, and
+    `time_ratio` = (plain relMSE x plain time) / (variant relMSE x variant
+    time), the equal-time gain of the variant when variance falls as 1 / time."""
+    plain = load_scene(scene, flags=FLAGS, max_depth=max_depth)
+    _render(plain, 8, 0)                         # warm-up
+    rows = {}
+    r, t = [], []
+    for k in range(seeds):
+        img, ms = _render(plain, spp, (k + 1) * seed_stride)
+        r.append(relmse(img, ref))
+        t.append(ms)
+    plain.close()
+    rows["plain"] = {"relmse": float(np.mean(r)), "ms": float(np.mean(t)), "per_seed": [float(x) for x in r]}
+    for name, cfg in variants.items():
+        it = load_scene(scene, flags=FLAGS, max_depth=max_depth)
+        r, t, tr = [], [], []
+        for k in range(seeds):
+            it.setGuiding(cfg)
+            img, ms = _render(it, spp, (k + 1) * seed_stride)
+            r.append(relmse(img, ref))
+            t.append(ms)
+            tr.append(it.guideStats()["ms_train"])
+        it.close()
+        rows[name] = {"relmse": float(np.mean(r)), "ms": float(np.mean(t)), "train_ms": float(np.mean(tr)),
+                      "per_seed": [float(x) for x in r]}
+    p = rows["plain"]
+    for name, v in rows.items():
+        v["spp_ratio"] = p["relmse"] / v["relmse"]
+        v["time_ratio"] = (p["relmse"] * p["ms"]) / (v["relmse"] * v["ms"])
+    return rows

@@ -228,6 +228,8 @@ typedef struct
     uint32_t bvh_rebuilds;      /* rebuilds after vertex updates */
     double   bvh_sah;           /* surface-area cost of the current tree (root = 1) */
     double   bvh_sah_build;     /* ... right after its last full build */
+    float    ms_bvh_build_wall; /* last full build: host wall time (allocations, launches and waits) */
+    float    ms_bvh_build_alloc; /* ... of which in device allocation */
 } cl_stats;
 
 typedef struct cl_integrator cl_integrator;
@@ -503,6 +505,10 @@ typedef struct cl_guide_config
                                               -log of the network's mixture (0) */
     float    weight_clamp;                 /* training weights above weight_clamp x the batch mean are
                                               clamped to it (robust fit to heavy-tailed records); 0 = off */
+    uint32_t min_depth;                    /* guided vertices: path depth >= min_depth (1 = every vertex,
+                                              the camera ray's hit included; 2 = indirect vertices only);
+                                              shallower vertices sample the BSDF alone and are neither
+                                              inferred nor recorded (0 or 1: every vertex) */
 } cl_guide_config;
 
 typedef struct cl_guide_stats
