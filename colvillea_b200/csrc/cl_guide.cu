@@ -18,10 +18,6 @@ using namespace guide;
 
 namespace
 {
-constexpr int kTrainWarps = 4;            // training forward/backward: 4 warps x 16 samples
-constexpr int kGradChunk  = 4096;         // samples per weight-gradient block
-constexpr int kGradStep   = 64;           // samples staged in shared memory per step
-
 __device__ __forceinline__ uint32_t laneIdx() { return threadIdx.x & 31u; }
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z)
@@ -61,56 +57,20 @@ __global__ void kTableCopy(const float* __restrict__ p, __nv_bfloat16* __restric
         t[i] = __float2bfloat16_rn(p[i]);
 }
 
-// Fragment-ordered bf16 weights.  Forward fragment (kt, nt) of layer l, lane
-// (g, t): b0 = W[8nt+g][16kt+2t .. +1], b1 = W[8nt+g][16kt+2t+8 .. +9].
-// Backward fragment (kt over outputs, nt over inputs): b0 = W[16kt+2t][8nt+g],
-// W[16kt+2t+1][8nt+g]; b1 the same 8 rows further down.  Then the weights in
-// the tensor-core canonical layout (cl_mlp_tc.cuh): 16-byte chunk e of layer
-// l, at byte 2 woff(l) + 16 e, holds W[e % N][8 (e / N) .. + 7].
-template <class S>
-__global__ void kFrags(const float* __restrict__ mlp, uint2* __restrict__ wf, uint2* __restrict__ wb,
-                       uint4* __restrict__ wt)
+// The weights as bf16 in the tensor-core canonical layout (cl_mlp_tc.cuh):
+// 16-byte chunk e of layer l, at byte 2 woff(l) + 16 e, holds
+// W[e % N][8 (e / N) .. + 7] (N = the layer's outputs).
+template <class S> __global__ void kFrags(const float* __restrict__ mlp, uint4* __restrict__ wt)
 {
-    int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < S::kFwdFrags * 32)
-    {
-        int f = e >> 5, lane = e & 31, l = 0;
-        while (l < S::kLayers - 1 && f >= S::fwdOff(l + 1)) ++l;
-        int          loc = f - S::fwdOff(l), kt = loc / S::fwdNT(l), nt = loc % S::fwdNT(l);
-        int          g = lane >> 2, t = lane & 3, K = S::in(l);
-        const float* W   = mlp + S::woff(l) + (nt * 8 + g) * K + kt * 16 + 2 * t;
-        wf[e]            = make_uint2(packBf16(W[0], W[1]), packBf16(W[8], W[9]));
-        return;
-    }
-    e -= S::kFwdFrags * 32;
-    if (e < S::kBwdFrags * 32)
-    {
-        int f = e >> 5, lane = e & 31, l = 0;
-        while (l < S::kLayers - 1 && f >= S::bwdOff(l + 1)) ++l;
-        int          loc = f - S::bwdOff(l), kt = loc / S::bwdNT(l), nt = loc % S::bwdNT(l);
-        int          g = lane >> 2, t = lane & 3, K = S::in(l);
-        const float* W   = mlp + S::woff(l) + (kt * 16 + 2 * t) * K + nt * 8 + g;
-        wb[e]            = make_uint2(packBf16(W[0], W[K]), packBf16(W[8 * K], W[9 * K]));
-        return;
-    }
-    e -= S::kBwdFrags * 32;
-    if (e < S::kParams / 8)
-    {
-        int l = 0;
-        while (l < S::kLayers - 1 && e >= S::woff(l + 1) / 8) ++l;
-        const int    loc = e - S::woff(l) / 8, N = S::out(l), K = S::in(l);
-        const float* W   = mlp + S::woff(l) + (loc % N) * K + 8 * (loc / N);
-        wt[e] = make_uint4(packBf16(W[0], W[1]), packBf16(W[2], W[3]), packBf16(W[4], W[5]), packBf16(W[6], W[7]));
-    }
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= S::kParams / 8) return;
+    int l = 0;
+    while (l < S::kLayers - 1 && e >= S::woff(l + 1) / 8) ++l;
+    const int    loc = e - S::woff(l) / 8, N = S::out(l), K = S::in(l);
+    const float* W   = mlp + S::woff(l) + (loc % N) * K + 8 * (loc / N);
+    wt[e] = make_uint4(packBf16(W[0], W[1]), packBf16(W[2], W[3]), packBf16(W[4], W[5]), packBf16(W[6], W[7]));
 }
-template <class S> constexpr int fragThreads() { return (S::kFwdFrags + S::kBwdFrags) * 32 + S::kParams / 8; }
-
-__device__ __forceinline__ void loadFrags(uint2* dst, const uint2* __restrict__ src, int count)
-{
-    const uint4* s = reinterpret_cast<const uint4*>(src);
-    uint4*       d = reinterpret_cast<uint4*>(dst);
-    for (int i = threadIdx.x; i < count / 2; i += blockDim.x) d[i] = __ldg(s + i);
-}
+template <class S> constexpr int fragThreads() { return S::kParams / 8; }
 
 __device__ __forceinline__ f3 ldf3(const float* p) { return {p[0], p[1], p[2]}; }
 
@@ -184,14 +144,10 @@ struct TrainArgs
     const uint32_t* count;
     uint32_t        batch;
     GridView        g;
-    const uint2* __restrict__ wf;
-    const uint2* __restrict__ wb;
     const uint4* __restrict__ wt; // canonical bf16 weights (tensor-core layout)
     float2*        gradTable;
     float*         gradMlp;       // FP32 weight gradients (the parameters after the hash table)
     uint32_t*      err;           // device error flags (kTcTimeout)
-    __nv_bfloat16* acts;
-    __nv_bfloat16* deltas;
     double*        scal;     // [0] sum of weights, [1] loss, [3] sum of clamped weights
     int            learnSel; // guide: learned selection probability
     float          clamp;    // weight clamp (x batch mean), 0 = off
@@ -351,325 +307,6 @@ struct CacheLoss
 
 namespace
 {
-// A fragments (k-tiles kt < KT) of a 16-row tile -> bf16 rows of a staging
-// matrix (row stride ld, starting at column 0 of `base`), rows < valid.
-template <int KT>
-__device__ __forceinline__ void storeA(const uint32_t (&a)[4][4], __nv_bfloat16* base, int ld, uint32_t rows,
-                                       uint32_t lane)
-{
-    const uint32_t g = lane >> 2, t = lane & 3u;
-#pragma unroll
-    for (int kt = 0; kt < KT; ++kt)
-    {
-        if (g < rows)
-        {
-            __nv_bfloat16* p = base + size_t(g) * ld + kt * 16 + 2 * t;
-            *reinterpret_cast<uint32_t*>(p)     = a[kt][0];
-            *reinterpret_cast<uint32_t*>(p + 8) = a[kt][2];
-        }
-        if (g + 8 < rows)
-        {
-            __nv_bfloat16* p = base + size_t(g + 8) * ld + kt * 16 + 2 * t;
-            *reinterpret_cast<uint32_t*>(p)     = a[kt][1];
-            *reinterpret_cast<uint32_t*>(p + 8) = a[kt][3];
-        }
-    }
-}
-
-// Backward through a layer with 64 inputs: d (KT k-tiles over the layer's
-// outputs) times W, masked by the ReLU of the layer's input (its A fragments
-// hPrev: a zero bf16 means the unit was off), rounded to bf16 -> the output
-// gradient of the layer below, as A fragments.
-template <int KT>
-__device__ __forceinline__ void backHidden(const uint2* __restrict__ wbL, const uint32_t (&d)[4][4],
-                                           const uint32_t (&hPrev)[4][4], uint32_t (&dOut)[4][4], uint32_t lane)
-{
-    float acc[8][4];
-#pragma unroll
-    for (int n = 0; n < 8; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
-#pragma unroll
-    for (int kt = 0; kt < KT; ++kt)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-        {
-            uint2 b = wbL[(kt * 8 + nt) * 32 + lane];
-            mma16816(acc[nt], d[kt], b.x, b.y);
-        }
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
-    {
-        const uint32_t lo = hPrev[nt >> 1][(nt & 1) ? 2 : 0], hi = hPrev[nt >> 1][(nt & 1) ? 3 : 1];
-        if (!(lo & 0xffffu)) acc[nt][0] = 0.0f;
-        if (!(lo >> 16)) acc[nt][1] = 0.0f;
-        if (!(hi & 0xffffu)) acc[nt][2] = 0.0f;
-        if (!(hi >> 16)) acc[nt][3] = 0.0f;
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-    {
-        dOut[j][0] = packBf16(acc[2 * j][0], acc[2 * j][1]);
-        dOut[j][1] = packBf16(acc[2 * j][2], acc[2 * j][3]);
-        dOut[j][2] = packBf16(acc[2 * j + 1][0], acc[2 * j + 1][1]);
-        dOut[j][3] = packBf16(acc[2 * j + 1][2], acc[2 * j + 1][3]);
-    }
-}
-
-template <class S> struct TrainSmem
-{
-    static constexpr int kX    = 16 * kXS * 2;    // encoded inputs, then the outputs (16 x kOS floats)
-    static constexpr int kD    = 16 * S::kDS * 2; // output gradients
-    static constexpr int kWarp = (kX + kD + 16 * 3 * 4 + 15) / 16 * 16;
-    static constexpr int kAll  = S::kFwdBytes + S::kBwdBytes + kTrainWarps * kWarp;
-    static_assert(16 * S::kOS * 4 <= kX, "output tile must fit in the input tile");
-};
-
-// Forward and backward pass of the training batch, 16 samples per warp tile:
-// encodes, runs the MLP keeping every layer's input in registers, writes the
-// inputs and the back-propagated output gradients of every layer (bf16) for
-// the weight-gradient reduction, accumulates the loss, and scatters the
-// input gradient of the hash features to the table gradient (float2 atomics).
-template <class S, class LOSS> __global__ void __launch_bounds__(kTrainWarps * 32) kTrainFwdBwd(TrainArgs a)
-{
-    using TS = TrainSmem<S>;
-    constexpr int NT = S::kOut / 8, NH = S::kHidden;
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint2*         wf   = reinterpret_cast<uint2*>(smem);
-    uint2*         wb   = reinterpret_cast<uint2*>(smem + S::kFwdBytes);
-    const uint32_t lane = laneIdx(), warp = threadIdx.x >> 5;
-    unsigned char* ws   = smem + S::kFwdBytes + S::kBwdBytes + warp * TS::kWarp;
-    __nv_bfloat16* x    = reinterpret_cast<__nv_bfloat16*>(ws);
-    __nv_bfloat16* dT   = reinterpret_cast<__nv_bfloat16*>(ws + TS::kX);
-    float*         posS = reinterpret_cast<float*>(ws + TS::kX + TS::kD);
-    loadFrags(wf, a.wf, S::kFwdFrags * 32);
-    loadFrags(wb, a.wb, S::kBwdFrags * 32);
-    __syncthreads();
-    const uint32_t count = *a.count, nB = min(count, a.batch);
-    const double   wsum  = a.clamp > 0.0f ? a.scal[3] : a.scal[0];
-    const float    invW  = wsum > 0.0 ? float(1.0 / wsum) : 0.0f;
-    const uint32_t g = lane >> 2, t = lane & 3u, r = lane & 15u, half = lane >> 4;
-    for (uint32_t tile = blockIdx.x * kTrainWarps + warp; tile * 16u < nB; tile += gridDim.x * kTrainWarps)
-    {
-        const uint32_t j0 = tile * 16u, rows = min(16u, nB - j0), j = j0 + r;
-        const bool     valid = r < rows;
-        __nv_bfloat16* row   = x + r * kXS;
-        const float4*  R     = a.rec + kRecordF4 * size_t(recordOf(valid ? j : j0, count, nB));
-        if (valid)
-        {
-            float4 r0 = R[0], rd = R[1 + half];
-            f3     p  = clampUnit(f3{r0.x, r0.y, r0.z});
-            if (half == 0)
-            {
-                posS[3 * r]     = p.x;
-                posS[3 * r + 1] = p.y;
-                posS[3 * r + 2] = p.z;
-            }
-#pragma unroll 2
-            for (int l = int(half) * 8; l < int(half) * 8 + 8; ++l)
-            {
-                float2 f = encodeLevel(a.g, l, p);
-                *reinterpret_cast<__nv_bfloat162*>(row + 2 * l) = __floats2bfloat162_rn(f.x, f.y);
-            }
-            oneBlob(f3{rd.x, rd.y, rd.z}, row + kHashF + half * 2 * kBlob);
-        }
-        else
-        {
-            uint32_t* z = reinterpret_cast<uint32_t*>(row);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) z[half * 8 + i] = 0u;
-#pragma unroll
-            for (int i = 0; i < 16; ++i) z[(kHashF + half * 2 * kBlob) / 2 + i] = 0u;
-        }
-        __syncwarp();
-        for (uint32_t e = lane; e < 16u * 12u; e += 32u)
-        {
-            uint32_t rr = e / 12u, c = e % 12u;
-            if (rr < rows)
-                reinterpret_cast<uint4*>(a.acts + size_t(j0 + rr) * S::kActRow)[c] =
-                    reinterpret_cast<const uint4*>(x + rr * kXS)[c];
-        }
-        uint32_t h[NH + 1][1][4][4];
-        float    out[1][NT][4];
-        mlpForward<S, 1>(wf, x, lane, h, out);
-#pragma unroll
-        for (int l = 0; l <= NH; ++l)
-            storeA<4>(h[l][0], a.acts + size_t(j0) * S::kActRow + S::actOff(l + 1), S::kActRow, rows, lane);
-        __syncwarp();
-        float* o = reinterpret_cast<float*>(x);
-        storeOut<S, 1>(out, o, lane);
-        __syncwarp();
-        float lossPart = 0.0f;
-        if (lane < 16u)
-        {
-            uint32_t* drow = reinterpret_cast<uint32_t*>(dT + lane * S::kDS);
-            if (valid)
-            {
-                float4 r0 = R[0], r3 = R[3];
-                float  gr[S::kOut];
-                float  l  = LOSS::eval(o + lane * S::kOS, r3, a.learnSel, gr);
-                float  sw = trainWeight(r0.w, a, nB) * invW;
-                lossPart  = sw * l;
-#pragma unroll
-                for (int c = 0; c < S::kOut / 2; ++c) drow[c] = packBf16(gr[2 * c] * sw, gr[2 * c + 1] * sw);
-            }
-            else
-#pragma unroll
-                for (int c = 0; c < S::kOut / 2; ++c) drow[c] = 0u;
-        }
-        for (int off = 16; off > 0; off >>= 1) lossPart += __shfl_xor_sync(0xffffffffu, lossPart, off);
-        if (lane == 0 && lossPart != 0.0f) atomicAdd(&a.scal[1], double(lossPart));
-        __syncwarp();
-        for (uint32_t e = lane; e < 16u * (S::kOut / 8); e += 32u)
-        {
-            uint32_t rr = e / (S::kOut / 8), c = e % (S::kOut / 8);
-            if (rr < rows)
-                reinterpret_cast<uint4*>(a.deltas + size_t(j0 + rr) * S::kDeltaRow + S::deltaOff(NH + 1))[c] =
-                    reinterpret_cast<const uint4*>(dT + rr * S::kDS)[c];
-        }
-        // Backward: the output layer (kOut/16 k-tiles), then the hidden layers.
-        uint32_t da[4][4], db[4][4];
-#pragma unroll
-        for (int kt = 0; kt < 4; ++kt)
-        {
-            if (kt < S::kOut / 16)
-                loadA(da[kt], dT, S::kDS, kt, lane);
-            else
-                da[kt][0] = da[kt][1] = da[kt][2] = da[kt][3] = 0u;
-        }
-        backHidden<S::kOut / 16>(wb + S::bwdOff(NH + 1) * 32, da, h[NH][0], db, lane);
-        storeA<4>(db, a.deltas + size_t(j0) * S::kDeltaRow + S::deltaOff(NH), S::kDeltaRow, rows, lane);
-#pragma unroll
-        for (int l = NH; l >= 1; --l)
-        {
-            // output gradient of layer l is in db when (NH - l) is even
-            if (((NH - l) & 1) == 0)
-            {
-                backHidden<4>(wb + S::bwdOff(l) * 32, db, h[l - 1][0], da, lane);
-                storeA<4>(da, a.deltas + size_t(j0) * S::kDeltaRow + S::deltaOff(l - 1), S::kDeltaRow, rows, lane);
-            }
-            else
-            {
-                backHidden<4>(wb + S::bwdOff(l) * 32, da, h[l - 1][0], db, lane);
-                storeA<4>(db, a.deltas + size_t(j0) * S::kDeltaRow + S::deltaOff(l - 1), S::kDeltaRow, rows, lane);
-            }
-        }
-        const uint32_t(&d0)[4][4] = (NH & 1) ? da : db;
-        // Layer 0: gradient of the 32 hash features (FP32).
-        float gx[4][4];
-#pragma unroll
-        for (int n = 0; n < 4; ++n) gx[n][0] = gx[n][1] = gx[n][2] = gx[n][3] = 0.0f;
-        const uint2* w0 = wb;
-#pragma unroll
-        for (int kt = 0; kt < 4; ++kt)
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt)
-            {
-                uint2 b = w0[(kt * 4 + nt) * 32 + lane];
-                mma16816(gx[nt], d0[kt], b.x, b.y);
-            }
-        // Column 8nt + 2t + f is feature f of level 4nt + t.
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-        {
-            const int level = 4 * nt + int(t);
-#pragma unroll
-            for (int hr = 0; hr < 2; ++hr)
-            {
-                const uint32_t rr = g + 8u * hr;
-                const float    d0v = gx[nt][2 * hr], d1v = gx[nt][2 * hr + 1];
-                if (rr >= rows || (d0v == 0.0f && d1v == 0.0f)) continue;
-                f3      p  = {posS[3 * rr], posS[3 * rr + 1], posS[3 * rr + 2]};
-                Cell    c  = gridCell(a.g.res[level], p);
-                float2* gb = a.gradTable + (size_t(level) << a.g.log2T);
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                {
-                    float w = cornerWeight(c, k);
-                    atomicAdd(gb + cornerIndex(a.g, level, c, k), make_float2(w * d0v, w * d1v));
-                }
-            }
-        }
-        __syncwarp();
-    }
-}
-
-// dW_l = sum_s delta_l[s]^T a_l[s] over a chunk of kGradChunk samples of the
-// batch (block (chunk, layer)): both operands are staged in shared memory
-// 64 samples at a time and read transposed with ldmatrix.trans; warp w owns
-// output rows 16w..16w+15 of the layer; FP32 partials go to the gradient with
-// one atomicAdd per element per block.
-template <class S>
-__global__ void __launch_bounds__(128) kWeightGrad(const __nv_bfloat16* __restrict__ acts,
-                                                   const __nv_bfloat16* __restrict__ deltas, const uint32_t* count,
-                                                   uint32_t batch, float* __restrict__ gradMlp)
-{
-    __shared__ __align__(16) __nv_bfloat16 dS[kGradStep][kWidth + 8];
-    __shared__ __align__(16) __nv_bfloat16 aS[kGradStep][kIn + 8];
-    const int      l = blockIdx.y, O = S::out(l), I = S::in(l);
-    const uint32_t nB = min(*count, batch);
-    const uint32_t s0 = blockIdx.x * kGradChunk, s1 = min(s0 + uint32_t(kGradChunk), nB);
-    if (s0 >= s1) return;
-    const uint32_t lane = laneIdx(), w = threadIdx.x >> 5, jm = lane >> 3;
-    const bool     active = int(w) < O / 16;
-    float          acc[12][4];
-#pragma unroll
-    for (int n = 0; n < 12; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
-    const int dq = O / 8, aq = I / 8; // uint4 per staged row
-    for (uint32_t s = s0; s < s1; s += kGradStep)
-    {
-        __syncthreads();
-        for (int e = threadIdx.x; e < kGradStep * dq; e += blockDim.x)
-        {
-            int   rr = e / dq, c = e % dq;
-            uint4 v  = make_uint4(0u, 0u, 0u, 0u);
-            if (s + rr < s1)
-                v = __ldg(reinterpret_cast<const uint4*>(deltas + size_t(s + rr) * S::kDeltaRow + S::deltaOff(l)) + c);
-            reinterpret_cast<uint4*>(&dS[rr][0])[c] = v;
-        }
-        for (int e = threadIdx.x; e < kGradStep * aq; e += blockDim.x)
-        {
-            int   rr = e / aq, c = e % aq;
-            uint4 v  = make_uint4(0u, 0u, 0u, 0u);
-            if (s + rr < s1)
-                v = __ldg(reinterpret_cast<const uint4*>(acts + size_t(s + rr) * S::kActRow + S::actOff(l)) + c);
-            reinterpret_cast<uint4*>(&aS[rr][0])[c] = v;
-        }
-        __syncthreads();
-        if (!active) continue;
-#pragma unroll
-        for (int ks = 0; ks < kGradStep / 16; ++ks)
-        {
-            uint32_t A[4];
-            ldsm4t(A, &dS[ks * 16 + (lane & 7) + 8 * (jm >> 1)][w * 16 + 8 * (jm & 1)]);
-#pragma unroll
-            for (int np = 0; np < 6; ++np)
-            {
-                if (np < I / 16)
-                {
-                    uint32_t B[4];
-                    ldsm4t(B, &aS[ks * 16 + (lane & 7) + 8 * (jm & 1)][np * 16 + 8 * (jm >> 1)]);
-                    mma16816(acc[2 * np], A, B[0], B[1]);
-                    mma16816(acc[2 * np + 1], A, B[2], B[3]);
-                }
-            }
-        }
-    }
-    if (!active) return;
-    const uint32_t g = lane >> 2, t = lane & 3u;
-    float*         G = gradMlp + S::woff(l);
-#pragma unroll
-    for (int nt = 0; nt < 12; ++nt)
-    {
-        if (nt < I / 8)
-        {
-            int o = int(w) * 16 + int(g), i = nt * 8 + 2 * int(t);
-            atomicAdd(G + o * I + i, acc[nt][0]);
-            atomicAdd(G + o * I + i + 1, acc[nt][1]);
-            atomicAdd(G + (o + 8) * I + i, acc[nt][2]);
-            atomicAdd(G + (o + 8) * I + i + 1, acc[nt][3]);
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Training on the fifth-generation tensor cores (tcgen05): one kernel per
 // step does, for each 128-sample tile of the batch, the encoding, the
@@ -707,7 +344,7 @@ template <class S> struct TrainTc
     // TMEM: columns [0, 64) the layer accumulator; then dW_l (M = 64) at dw(l).
     __host__ __device__ static constexpr uint32_t dw(int l) { return 64u + (l == 0 ? 0u : uint32_t(kIn + (l - 1) * kWidth)); }
     static constexpr uint32_t kCols = 512;
-    static_assert(kW % 128 == 0 || kW % 16 == 0, "weights: 16-byte chunks");
+    static_assert(kW % 16 == 0, "weights: 16-byte chunks");
     static_assert(dw(S::kLayers) <= kCols, "weight gradients exceed tensor memory");
     static_assert(S::kOut <= kWidth, "output gradient tile is 64 columns wide");
 };
@@ -732,7 +369,7 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
 {
     using T              = TrainTc<S>;
     constexpr int L      = T::L;
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t count = *a.count, nB = min(count, a.batch);
     const uint32_t tiles = (nB + kTcRows - 1) / kTcRows;
     if (blockIdx.x >= tiles) return; // before any TMEM allocation
@@ -1109,24 +746,13 @@ template <class S, class L> cl_status HashNet<S, L>::init(cudaStream_t st, std::
     CL_CUDA(cudaFuncSetAttribute(kInferUnit<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcLayout<S>::kSmem),
             err);
     CL_CUDA(cudaFuncSetAttribute(kInferUnit<S>, cudaFuncAttributePreferredSharedMemoryCarveout, 100), err);
-    CL_CUDA(cudaFuncSetAttribute(kTrainFwdBwd<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrainSmem<S>::kAll),
-            err);
     CL_CUDA(cudaFuncSetAttribute(kTrainTc<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, TrainTc<S>::kSmem), err);
-    int occ = 0;
-    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kTrainFwdBwd<S, L>, kTrainWarps * 32,
-                                                          TrainSmem<S>::kAll),
-            err);
-    trainBlocks_ = numSMs_ * (occ > 0 ? occ : 1);
     CL_TRY(params_.alloc(n * 4, err));
     CL_TRY(grad_.alloc(n * 4, err));
     CL_TRY(m_.alloc(n * 4, err));
     CL_TRY(v_.alloc(n * 4, err));
     CL_TRY(table_.alloc(hashParams_ * 2, err));
-    CL_TRY(wf_.alloc(S::kFwdBytes, err));
-    CL_TRY(wb_.alloc(S::kBwdBytes, err));
     CL_TRY(wt_.alloc(TcLayout<S>::kWBytes, err));
-    CL_TRY(acts_.alloc(size_t(cfg_.batch) * S::kActRow * 2, err));
-    CL_TRY(deltas_.alloc(size_t(cfg_.batch) * S::kDeltaRow * 2, err));
     CL_TRY(scal_.alloc(64, err));
     kInitParams<S><<<gridFor(n, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), hashParams_, cfg_.seed);
     CL_CUDA(cudaGetLastError(), err);
@@ -1156,8 +782,7 @@ template <class S, class L> cl_status HashNet<S, L>::refreshCopies(std::string* 
     kTableCopy<<<gridFor(hashParams_, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), table_.as<__nv_bfloat16>(),
                                                                         hashParams_);
     CL_CUDA(cudaGetLastError(), err);
-    kFrags<S><<<(fragThreads<S>() + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
-                                                               wb_.as<uint2>(), wt_.as<uint4>());
+    kFrags<S><<<(fragThreads<S>() + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wt_.as<uint4>());
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }
@@ -1319,14 +944,10 @@ cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* coun
     a.count     = count;
     a.batch     = cfg_.batch;
     a.g         = grid();
-    a.wf        = wf_.as<const uint2>();
-    a.wb        = wb_.as<const uint2>();
     a.wt        = wt_.as<const uint4>();
     a.gradTable = reinterpret_cast<float2*>(grad_.f());
     a.gradMlp   = grad_.f() + hashParams_;
     a.err       = trainErr();
-    a.acts      = acts_.as<__nv_bfloat16>();
-    a.deltas    = deltas_.as<__nv_bfloat16>();
     a.scal      = scal_.as<double>();
     a.learnSel  = cfg_.learn_selection ? 1 : 0;
     a.clamp     = cfg_.weight_clamp;
@@ -1356,8 +977,7 @@ cl_status HashNet<S, L>::trainDevice(const float4* rec, const uint32_t* count, s
                                                               m_.as<float4>(), v_.as<float4>(), n4, hashParams_ / 4, k,
                                                               table_.as<uint2>());
     CL_CUDA(cudaGetLastError(), err);
-    kFrags<S><<<(fragThreads<S>() + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wf_.as<uint2>(),
-                                                               wb_.as<uint2>(), wt_.as<uint4>());
+    kFrags<S><<<(fragThreads<S>() + 255) / 256, 256, 0, st_>>>(params_.f() + hashParams_, wt_.as<uint4>());
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }

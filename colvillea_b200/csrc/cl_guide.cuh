@@ -1,15 +1,9 @@
 // Neural path guiding network, device side (no counterpart in the reference
 // renderer): multiresolution hash grid + one-blob encoding, a 96-64-64-64-64-48
 // ReLU MLP with BF16 operands and FP32 accumulation on the tensor cores, and a
-// head of 8 von Mises-Fisher lobes.
-//
-// Tensor-core mapping (mma.sync m16n8k16, BF16 in, FP32 accumulate): a warp
-// owns 16-row tiles of samples.  The accumulator fragment of two adjacent
-// 8-column tiles is exactly the A fragment of one 16-column k-tile of the next
-// layer, so activations stay in registers from layer to layer; only the input
-// encoding (one shared-memory tile per warp) and the weights (fragment-ordered
-// in shared memory, one 8-byte load per lane per fragment) are read from
-// shared memory.
+// head of 8 von Mises-Fisher lobes.  The radiance cache uses the same encoding
+// and a 96-64-64-16 MLP.  The tensor-core passes (tcgen05, inference and
+// training) are in cl_mlp_tc.cuh and cl_guide.cu.
 #pragma once
 
 #include "cl_device.cuh"
@@ -21,7 +15,6 @@ namespace clb
 namespace guide
 {
 constexpr int kLevels = 16, kFeat = 2, kHashF = 32, kBlob = 16, kIn = 96, kWidth = 64, kLobes = 8;
-constexpr int kXS = 104; // encoded-input tile row stride (bf16): 208 B, conflict-free ldmatrix rows
 constexpr float kKappaMin = -5.0f, kKappaMax = 7.0f;
 constexpr float kSelMin = 0.05f, kSelMax = 0.95f; // learned guide-selection probability range
 constexpr int   kSelOut = 5 * kLobes;           // head output of its logit
@@ -29,11 +22,6 @@ constexpr int   kSelOut = 5 * kLobes;           // head output of its logit
 // Network shape: 96 encoded inputs -> 64 (layer 0) -> NH hidden layers of
 // 64 -> NO outputs (a multiple of 16), ReLU between layers, no biases.  W_l
 // is [out][in] row-major in the flat parameter block.
-//   forward fragments of layer l: (in/16) k-tiles x (out/8) n-tiles;
-//   backward fragments: (out/16) k-tiles x (in/8) n-tiles, only the 32
-//   hash-grid columns at layer 0 (the one-blob inputs get no gradient).
-// Training staging rows: the input of every layer [96 | 64 ...] and the
-// output gradient of every layer [64 ... | NO], bf16.
 template <int NH, int NO> struct MlpShape
 {
     static_assert(NO % 16 == 0 && NH >= 1, "outputs: a multiple of 16; at least one hidden layer");
@@ -42,29 +30,13 @@ template <int NH, int NO> struct MlpShape
     __host__ __device__ static constexpr int out(int l) { return l == NH + 1 ? NO : kWidth; }
     __host__ __device__ static constexpr int woff(int l) { return l == 0 ? 0 : kIn * kWidth + (l - 1) * kWidth * kWidth; }
     static constexpr int kParams = kIn * kWidth + NH * kWidth * kWidth + kWidth * NO;
-    __host__ __device__ static constexpr int fwdNT(int l) { return out(l) / 8; }
-    __host__ __device__ static constexpr int bwdNT(int l) { return l == 0 ? kHashF / 8 : in(l) / 8; }
-    __host__ __device__ static constexpr int fwdOff(int l) { return l == 0 ? 0 : 48 + (l - 1) * 32; }
-    __host__ __device__ static constexpr int bwdOff(int l) { return l == 0 ? 0 : 16 + (l - 1) * 32; }
-    static constexpr int kFwdFrags = 48 + NH * 32 + 4 * (NO / 8);
-    static constexpr int kBwdFrags = 16 + NH * 32 + (NO / 16) * 8;
-    static constexpr int kFwdBytes = kFwdFrags * 32 * 8;
-    static constexpr int kBwdBytes = kBwdFrags * 32 * 8;
-    static constexpr int kActRow   = kIn + (NH + 1) * kWidth;
-    static constexpr int kDeltaRow = (NH + 1) * kWidth + NO;
-    __host__ __device__ static constexpr int actOff(int l) { return l == 0 ? 0 : kIn + (l - 1) * kWidth; }
-    __host__ __device__ static constexpr int deltaOff(int l) { return l * kWidth; }
-    static constexpr int kOS = NO + 1; // output tile row stride (f32)
-    static constexpr int kDS = NO + 8; // output-gradient tile row stride (bf16), conflict-free ldmatrix rows
 };
 // The guiding network (4 hidden layers, 48 outputs: 8 vMF lobes + selection)
 // and the radiance cache (2 hidden layers, RGB in the first 3 of 16 outputs).
 using GuideShape = MlpShape<3, 48>;
 using CacheShape = MlpShape<1, 16>;
-constexpr int kOut          = GuideShape::kOut;
-constexpr int kOS           = GuideShape::kOS;
-constexpr int kMlpParams    = GuideShape::kParams;   // 21504
-constexpr int kFwdFragBytes = GuideShape::kFwdBytes;
+constexpr int kOut       = GuideShape::kOut;
+constexpr int kMlpParams = GuideShape::kParams; // 21504
 
 // Hash grid: table[l * T + index] holds the 2 features of an entry.
 struct GridView
@@ -190,7 +162,7 @@ __device__ __forceinline__ void zeroRow(__nv_bfloat16* row)
 }
 
 // ---------------------------------------------------------------------------
-// Tensor-core primitives
+// BF16 packing
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t packBf16(float lo, float hi)
 {
@@ -198,174 +170,6 @@ __device__ __forceinline__ uint32_t packBf16(float lo, float hi)
     return *reinterpret_cast<uint32_t*>(&v);
 }
 __device__ __forceinline__ float reluF(float x) { return x > 0.0f ? x : 0.0f; }
-
-__device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
-{
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-                 "{%0,%1,%2,%3};\n"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-__device__ __forceinline__ void ldsm4(uint32_t (&r)[4], const void* p)
-{
-    uint32_t a = uint32_t(__cvta_generic_to_shared(p));
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-__device__ __forceinline__ void ldsm4t(uint32_t (&r)[4], const void* p)
-{
-    uint32_t a = uint32_t(__cvta_generic_to_shared(p));
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(a));
-}
-
-// A fragments of one 16-row tile whose rows start at `tile` (stride `ld`
-// bf16), k-tile kt: lane l addresses row l & 15, column 16 kt + 8 (l >> 4).
-__device__ __forceinline__ void loadA(uint32_t (&a)[4], const __nv_bfloat16* tile, int ld, int kt, uint32_t lane)
-{
-    ldsm4(a, tile + (lane & 15u) * ld + kt * 16 + (lane >> 4) * 8);
-}
-
-// Accumulators of n-tiles 2j, 2j+1 -> A fragment of k-tile j (after ReLU).
-__device__ __forceinline__ void accToA(const float (&c0)[4], const float (&c1)[4], uint32_t (&a)[4])
-{
-    a[0] = packBf16(reluF(c0[0]), reluF(c0[1]));
-    a[1] = packBf16(reluF(c0[2]), reluF(c0[3]));
-    a[2] = packBf16(reluF(c1[0]), reluF(c1[1]));
-    a[3] = packBf16(reluF(c1[2]), reluF(c1[3]));
-}
-
-// Hidden layer from registers: in (4 k-tiles) -> out (8 n-tiles) -> ReLU.
-template <int MT>
-__device__ __forceinline__ void hiddenLayer(const uint2* __restrict__ wf, const uint32_t (&in)[MT][4][4],
-                                            uint32_t (&out)[MT][4][4], uint32_t lane)
-{
-    float acc[MT][8][4];
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int n = 0; n < 8; ++n) acc[m][n][0] = acc[m][n][1] = acc[m][n][2] = acc[m][n][3] = 0.0f;
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt)
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-        {
-            uint2 b = wf[(kt * 8 + nt) * 32 + lane];
-#pragma unroll
-            for (int m = 0; m < MT; ++m) mma16816(acc[m][nt], in[m][kt], b.x, b.y);
-        }
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) accToA(acc[m][2 * j], acc[m][2 * j + 1], out[m][j]);
-}
-
-// Layer 0: the encoded-input tile (MT*16 rows, stride kXS, shared memory)
-// -> ReLU activations as A fragments.
-template <int MT>
-__device__ __forceinline__ void inputLayer(const uint2* __restrict__ wf, const __nv_bfloat16* x, uint32_t lane,
-                                           uint32_t (&h)[MT][4][4])
-{
-    float acc[MT][8][4];
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int n = 0; n < 8; ++n) acc[m][n][0] = acc[m][n][1] = acc[m][n][2] = acc[m][n][3] = 0.0f;
-#pragma unroll
-    for (int kt = 0; kt < 6; ++kt)
-    {
-        uint32_t a[MT][4];
-#pragma unroll
-        for (int m = 0; m < MT; ++m) loadA(a[m], x + m * 16 * kXS, kXS, kt, lane);
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-        {
-            uint2 b = wf[(kt * 8 + nt) * 32 + lane];
-#pragma unroll
-            for (int m = 0; m < MT; ++m) mma16816(acc[m][nt], a[m], b.x, b.y);
-        }
-    }
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) accToA(acc[m][2 * j], acc[m][2 * j + 1], h[m][j]);
-}
-
-// Last layer: 64 inputs (A fragments) -> NO/8 n-tiles of FP32 outputs.
-template <class S, int MT>
-__device__ __forceinline__ void outputLayer(const uint2* __restrict__ wl, const uint32_t (&in)[MT][4][4],
-                                            float (&out)[MT][S::kOut / 8][4], uint32_t lane)
-{
-    constexpr int NT = S::kOut / 8;
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int n = 0; n < NT; ++n) out[m][n][0] = out[m][n][1] = out[m][n][2] = out[m][n][3] = 0.0f;
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt)
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-        {
-            uint2 b = wl[(kt * NT + nt) * 32 + lane];
-#pragma unroll
-            for (int m = 0; m < MT; ++m) mma16816(out[m][nt], in[m][kt], b.x, b.y);
-        }
-}
-
-// Forward pass of MT 16-row tiles.  `x`: the warp's encoded-input tile;
-// `wf`: forward fragments (shared memory).  h[l]: A fragments of the input
-// of layer l+1, kept for the backward pass; out: the outputs' accumulators.
-template <class S, int MT>
-__device__ __forceinline__ void mlpForward(const uint2* __restrict__ wf, const __nv_bfloat16* x, uint32_t lane,
-                                           uint32_t (&h)[S::kHidden + 1][MT][4][4], float (&out)[MT][S::kOut / 8][4])
-{
-    inputLayer<MT>(wf, x, lane, h[0]);
-#pragma unroll
-    for (int l = 1; l <= S::kHidden; ++l) hiddenLayer<MT>(wf + S::fwdOff(l) * 32, h[l - 1], h[l], lane);
-    outputLayer<S, MT>(wf + S::fwdOff(S::kHidden + 1) * 32, h[S::kHidden], out, lane);
-}
-
-// Inference-only forward (activations ping-pong between two register sets).
-template <class S, int MT>
-__device__ __forceinline__ void mlpInfer(const uint2* __restrict__ wf, const __nv_bfloat16* x, uint32_t lane,
-                                         float (&out)[MT][S::kOut / 8][4])
-{
-    uint32_t ha[MT][4][4], hb[MT][4][4];
-    inputLayer<MT>(wf, x, lane, ha);
-#pragma unroll
-    for (int l = 1; l <= S::kHidden; ++l)
-    {
-        if (l & 1)
-            hiddenLayer<MT>(wf + S::fwdOff(l) * 32, ha, hb, lane);
-        else
-            hiddenLayer<MT>(wf + S::fwdOff(l) * 32, hb, ha, lane);
-    }
-    if (S::kHidden & 1)
-        outputLayer<S, MT>(wf + S::fwdOff(S::kHidden + 1) * 32, hb, out, lane);
-    else
-        outputLayer<S, MT>(wf + S::fwdOff(S::kHidden + 1) * 32, ha, out, lane);
-}
-
-// Output accumulators -> rows of a float tile (stride S::kOS).
-template <class S, int MT>
-__device__ __forceinline__ void storeOut(const float (&out)[MT][S::kOut / 8][4], float* tile, uint32_t lane)
-{
-    const uint32_t g = lane >> 2, t = lane & 3u;
-#pragma unroll
-    for (int m = 0; m < MT; ++m)
-#pragma unroll
-        for (int n = 0; n < S::kOut / 8; ++n)
-        {
-            float* r0 = tile + (m * 16 + g) * S::kOS + n * 8 + 2 * t;
-            float* r1 = r0 + 8 * S::kOS;
-            r0[0]     = out[m][n][0];
-            r0[1]     = out[m][n][1];
-            r1[0]     = out[m][n][2];
-            r1[1]     = out[m][n][3];
-        }
-}
 
 // ---------------------------------------------------------------------------
 // vMF mixture head

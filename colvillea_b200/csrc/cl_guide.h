@@ -1,5 +1,5 @@
-// Hash-grid + tensor-core MLP networks, host side: parameters, Adam state,
-// training staging and the kernels' launch sequence.  Two instances: the
+// Hash-grid + tensor-core MLP networks, host side: parameters, Adam state and
+// the kernels' launch sequence.  Two instances: the
 // guiding network and the radiance cache (no counterpart in the reference
 // renderer).
 #pragma once
@@ -47,7 +47,6 @@ public:
     // The loss lands in lossDev (device double) when the stream reaches it.
     cl_status trainDevice(const float4* rec, const uint32_t* count, std::string* err);
     guide::GridView grid() const;
-    const uint2*    fwdFrags() const { return wf_.as<uint2>(); }
     const uint4*    tcWeights() const { return wt_.as<uint4>(); }
     const double*   lossDev() const { return scal_.as<double>() + 1; }
     // Device error flags of the last training step (kTcTimeout), read with its loss.
@@ -66,14 +65,11 @@ private:
     uint64_t        hashParams_ = 0;
     cudaStream_t    st_ = nullptr;
     int             numSMs_ = 148;
-    int             trainBlocks_ = 0;
     uint64_t        step_ = 0;
 
     DevBuf params_, grad_, m_, v_; // FP32 [hash | mlp]
     DevBuf table_;                 // bf16 copy of the hash table
-    DevBuf wf_, wb_;               // bf16 weight fragments (forward, backward)
     DevBuf wt_;                    // bf16 weights in the tensor-core canonical layout
-    DevBuf acts_, deltas_;         // training staging, batch rows
     DevBuf scal_;                  // {sum w, loss, count (u32), sum of clamped w}; byte 48: inference error
                                    // flags; byte 52: training error flags
     DevBuf rec_, io_, io2_;        // host-entry staging

@@ -166,10 +166,6 @@ __device__ __forceinline__ HitAttr hitAttributesTri(const SceneDev& sc, uint4 ti
     h.dpdv = dpdv;
     return h;
 }
-__device__ __forceinline__ HitAttr hitAttributes(const SceneDev& sc, uint32_t prim, float b1, float b2)
-{
-    return hitAttributesTri(sc, __ldg(sc.triIdx + prim), b1, b2);
-}
 
 // Camera path start (generateCameraRays, raygeneration.cu:83-102): path index
 // p -> pixel p mod W*H, frame frame0 + p / (W*H).
