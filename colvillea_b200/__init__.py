@@ -16,11 +16,12 @@ from . import _native as N
 from ._native import ClError
 
 __all__ = ["IntegratorType", "Integrator", "RenderConfig", "ClError", "COMPAT_ALL", "DOME_ALIAS", "FILM_FP64",
-           "PROFILE_STAGES", "TRACE_STATS", "load_scene", "GuideConfig", "Guide", "RadianceCacheConfig", "Cache",
+           "PROFILE_STAGES", "TRACE_STATS", "TWO_LEVEL", "load_scene", "GuideConfig", "Guide", "RadianceCacheConfig", "Cache",
            "load_obj", "load_hdr", "write_pfm", "read_pfm"]
 
 COMPAT_PDF, COMPAT_FRAME, COMPAT_ESCAPE, COMPAT_ALL = N.CL_COMPAT_PDF, N.CL_COMPAT_FRAME, N.CL_COMPAT_ESCAPE, N.CL_COMPAT_ALL
 DOME_ALIAS, FILM_FP64, PROFILE_STAGES, TRACE_STATS = N.CL_DOME_ALIAS, N.CL_FILM_FP64, N.CL_PROFILE_STAGES, N.CL_TRACE_STATS
+TWO_LEVEL = N.CL_TWO_LEVEL
 
 
 class IntegratorType(enum.IntEnum):

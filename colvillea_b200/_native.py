@@ -24,6 +24,7 @@ CL_DOME_ALIAS = 1 << 4
 CL_FILM_FP64 = 1 << 5
 CL_PROFILE_STAGES = 1 << 6
 CL_TRACE_STATS = 1 << 7
+CL_TWO_LEVEL = 1 << 8
 
 CL_BVH_UPDATE_AUTO, CL_BVH_UPDATE_REFIT, CL_BVH_UPDATE_REBUILD = range(3)
 

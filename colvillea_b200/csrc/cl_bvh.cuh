@@ -37,10 +37,28 @@ constexpr int kTrisPerStep = 1;
 constexpr int kTraceBlock    = 128;
 constexpr uint32_t kMissPrim = 0xffffffffu;
 
+// Two-level scenes (CL_TWO_LEVEL): one tree per mesh in object space, and a
+// top tree over the instances' world boxes whose leaf entries are instances
+// (the w of a top-tree triangle record holds the instance index).  A ray that
+// reaches an instance entry continues in that mesh's tree with the ray mapped
+// to object space (same parameter t: the map is affine).
+struct InstDev
+{
+    float4        w2o[3];   // object-from-world rows {m0, m1, m2, translation}
+    float4        o2w[3];   // world-from-object rows
+    const uint4*  nodes;    // the mesh's tree
+    const float4* tris;
+    uint32_t      primBase; // global id of the instance's first triangle (instance order)
+    uint32_t      triBase;  // the mesh's first entry in the triangle index pool
+    uint32_t      material;
+    uint32_t      flags;    // bit 0: the transform mirrors (negative determinant)
+};
+
 struct BvhView
 {
     const uint4* __restrict__ nodes;
     const float4* __restrict__ tris;
+    const InstDev* __restrict__ inst; // two-level: the instances (nodes/tris are the top tree); null otherwise
     // Traversal stack entries per thread: the tree's depth + 1 (a ray holds
     // at most one pending node group per level), at most kStackDepth.  The
     // kernels' dynamic shared memory is stackDepth * kTraceBlock * 8 bytes,
@@ -100,11 +118,11 @@ __device__ __forceinline__ void fillKeyLut(uint8_t* lut)
 
 // Intersects the ray with the 8 children of one node; returns the hit mask:
 // bits 24..31 inner-child keys (slot ^ octant), bits 0..23 triangle offsets.
-__device__ __forceinline__ uint32_t intersectNode(const BvhView& bvh, uint32_t idx, f3 o, f3 inv, uint32_t oct, float tmin,
-                                                  float tmax, uint32_t* childBase, uint32_t* triBase, uint32_t* imaskOut,
-                                                  const uint8_t* keyLut)
+__device__ __forceinline__ uint32_t intersectNode(const uint4* __restrict__ nodes, uint32_t idx, f3 o, f3 inv, uint32_t oct,
+                                                  float tmin, float tmax, uint32_t* childBase, uint32_t* triBase,
+                                                  uint32_t* imaskOut, const uint8_t* keyLut)
 {
-    const uint4* np = bvh.nodes + size_t(idx) * 5;
+    const uint4* np = nodes + size_t(idx) * 5;
     uint4        n0 = __ldg(np + 0);
     uint4        n1 = __ldg(np + 1);
     uint4        n2 = __ldg(np + 2);
@@ -221,7 +239,7 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
             ++s.sp;
         }
         uint32_t cb, tb, im;
-        uint32_t hits = intersectNode(bvh, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im, keyLut);
+        uint32_t hits = intersectNode(bvh.nodes, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im, keyLut);
         if (STATS) cnt->nodes++;
         s.ng = make_uint2(cb, (hits & 0xff000000u) | im);
         s.tg = make_uint2(tb, hits & 0x00ffffffu);
@@ -280,6 +298,204 @@ __device__ __forceinline__ uint32_t traverse(const BvhView& bvh, f3 o, f3 d, flo
     *tHit  = s.bt;
     *b1Hit = s.b1;
     *b2Hit = s.b2;
+    return s.best;
+}
+
+// ---------------------------------------------------------------------------
+// Two-level traversal (CL_TWO_LEVEL).  The same node and triangle steps as
+// travStep, over the top tree and, inside an instance, over its mesh's tree.
+// Entering an instance pushes what is left of the top tree's current node
+// (its remaining instance entries as a leaf group, y <= 0xffffff; its pending
+// children as a node group, y > 0xffffff) and remembers the stack depth;
+// when the mesh tree's work is done at that depth the world ray is restored
+// and the top tree continues.  Hits report (instance, local triangle id).
+// ---------------------------------------------------------------------------
+struct Trav2
+{
+    RayPre        pre;
+    f3            inv;
+    uint32_t      oct;
+    float         tmin, tmax;
+    uint2         ng, tg;
+    int           sp, blasSp;
+    uint32_t      inst;     // current instance, kMissPrim in the top tree
+    uint32_t      best, bestInst;
+    float         bt, b1, b2;
+    f3            wo, wd;   // the world-space ray
+    const uint4*  nodes;    // the tree being traversed
+    const float4* tris;
+};
+
+__device__ __forceinline__ void trav2SetRay(Trav2& s, f3 o, f3 d)
+{
+    s.pre   = rayPrepare(o, d);
+    s.inv.x = 1.0f / (fabsf(d.x) < 1e-30f ? copysignf(1e-30f, d.x) : d.x);
+    s.inv.y = 1.0f / (fabsf(d.y) < 1e-30f ? copysignf(1e-30f, d.y) : d.y);
+    s.inv.z = 1.0f / (fabsf(d.z) < 1e-30f ? copysignf(1e-30f, d.z) : d.z);
+    s.oct   = (s.inv.x < 0.0f ? 1u : 0u) | (s.inv.y < 0.0f ? 2u : 0u) | (s.inv.z < 0.0f ? 4u : 0u);
+}
+
+__device__ __forceinline__ void trav2Init(const BvhView& bvh, Trav2& s, f3 o, f3 d, float tmin, float tmax)
+{
+    trav2SetRay(s, o, d);
+    s.wo = o;
+    s.wd = d;
+    s.tmin = tmin;
+    s.tmax = tmax;
+    s.ng   = make_uint2(0u, (1u << (24 + s.oct)) | 1u);
+    s.tg   = make_uint2(0u, 0u);
+    s.sp = s.blasSp = 0;
+    s.inst  = kMissPrim;
+    s.best  = s.bestInst = kMissPrim;
+    s.bt    = tmax;
+    s.b1 = s.b2 = 0.0f;
+    s.nodes = bvh.nodes;
+    s.tris  = bvh.tris;
+}
+
+// Affine map of a point (w = 1) or a direction (w = 0) by three rows.
+__device__ __forceinline__ f3 xformPoint(const float4* __restrict__ m, f3 p)
+{
+    float4 a = __ldg(m), b = __ldg(m + 1), c = __ldg(m + 2);
+    return {a.x * p.x + a.y * p.y + a.z * p.z + a.w, b.x * p.x + b.y * p.y + b.z * p.z + b.w,
+            c.x * p.x + c.y * p.y + c.z * p.z + c.w};
+}
+__device__ __forceinline__ f3 xformDir(const float4* __restrict__ m, f3 d)
+{
+    float4 a = __ldg(m), b = __ldg(m + 1), c = __ldg(m + 2);
+    return {a.x * d.x + a.y * d.y + a.z * d.z, b.x * d.x + b.y * d.y + b.z * d.z, c.x * d.x + c.y * d.y + c.z * d.z};
+}
+
+template <bool ANY, bool STATS>
+__device__ __forceinline__ bool trav2Step(const BvhView& bvh, Trav2& s, uint2* stack, TraceCounters* cnt, uint32_t* err,
+                                          const uint8_t* keyLut)
+{
+    if (s.tg.y == 0u && s.ng.y > 0x00ffffffu)
+    {
+        uint32_t key = __ffs(s.ng.y >> 24) - 1;
+        s.ng.y &= ~(1u << (24 + key));
+        uint32_t slot  = key ^ s.oct;
+        uint32_t imask = s.ng.y & 0xffu;
+        uint32_t child = s.ng.x + __popc(imask & ((1u << slot) - 1u));
+        if (s.ng.y > 0x00ffffffu)
+        {
+            if (s.sp >= int(bvh.stackDepth))
+            {
+                atomicOr(err, 1u);
+                s.best = kMissPrim;
+                return true;
+            }
+            stack[s.sp * kTraceBlock] = s.ng;
+            ++s.sp;
+        }
+        uint32_t cb, tb, im;
+        uint32_t hits = intersectNode(s.nodes, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im, keyLut);
+        if (STATS) cnt->nodes++;
+        s.ng = make_uint2(cb, (hits & 0xff000000u) | im);
+        s.tg = make_uint2(tb, hits & 0x00ffffffu);
+    }
+    if (s.tg.y)
+    {
+        uint32_t k = __ffs(s.tg.y) - 1;
+        s.tg.y &= ~(1u << k);
+        const float4* tp = s.tris + size_t(s.tg.x + k) * 3;
+        if (s.inst != kMissPrim)
+        {
+            float4 a = __ldg(tp + 0);
+            float4 b = __ldg(tp + 1);
+            float4 c = __ldg(tp + 2);
+            if (STATS) cnt->tris++;
+            float t, u, v;
+            if (intersectTri(s.pre, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, f3{c.x, c.y, c.z}, &t, &u, &v) && t > s.tmin)
+            {
+                uint32_t id = __float_as_uint(a.w);
+                if (ANY)
+                {
+                    if (t < s.tmax)
+                    {
+                        s.bt       = t;
+                        s.best     = id;
+                        s.bestInst = s.inst;
+                        return true;
+                    }
+                }
+                else if (t < s.bt || (t == s.bt && (s.inst < s.bestInst || (s.inst == s.bestInst && id < s.best))))
+                {
+                    s.bt       = t;
+                    s.best     = id;
+                    s.bestInst = s.inst;
+                    s.b1       = u;
+                    s.b2       = v;
+                }
+            }
+        }
+        else
+        {
+            // An instance entry of the top tree: keep the rest of this node on the stack, enter the mesh tree.
+            const uint32_t id = __float_as_uint(__ldg(&tp->w));
+            const int      need = (s.ng.y > 0x00ffffffu ? 1 : 0) + (s.tg.y ? 1 : 0);
+            if (s.sp + need > int(bvh.stackDepth))
+            {
+                atomicOr(err, 1u);
+                s.best = kMissPrim;
+                return true;
+            }
+            if (s.ng.y > 0x00ffffffu) stack[(s.sp++) * kTraceBlock] = s.ng;
+            if (s.tg.y) stack[(s.sp++) * kTraceBlock] = s.tg;
+            const InstDev* in = bvh.inst + id;
+            s.blasSp          = s.sp;
+            s.inst            = id;
+            s.nodes           = in->nodes;
+            s.tris            = in->tris;
+            trav2SetRay(s, xformPoint(in->w2o, s.wo), xformDir(in->w2o, s.wd));
+            s.ng = make_uint2(0u, (1u << (24 + s.oct)) | 1u);
+            s.tg = make_uint2(0u, 0u);
+            return false;
+        }
+    }
+    if (s.tg.y == 0u && s.ng.y <= 0x00ffffffu)
+    {
+        if (s.inst != kMissPrim && s.sp == s.blasSp)
+        {
+            // The mesh tree is done: back to the top tree in world space.
+            s.inst  = kMissPrim;
+            s.nodes = bvh.nodes;
+            s.tris  = bvh.tris;
+            trav2SetRay(s, s.wo, s.wd);
+        }
+        if (s.sp == 0) return true;
+        --s.sp;
+        const uint2 e = stack[s.sp * kTraceBlock];
+        if (e.y > 0x00ffffffu)
+        {
+            s.ng = e;
+            s.tg = make_uint2(0u, 0u);
+        }
+        else
+        {
+            s.tg = e;
+            s.ng = make_uint2(0u, 0u);
+        }
+    }
+    return false;
+}
+
+// Whole two-level traversal of one ray: *inst = the hit's instance, the
+// return value its triangle id within the instance's mesh (kMissPrim: none).
+template <bool ANY, bool STATS>
+__device__ __forceinline__ uint32_t traverse2(const BvhView& bvh, f3 o, f3 d, float tmin, float tmax, float* tHit,
+                                              float* b1Hit, float* b2Hit, uint32_t* inst, uint2* stack,
+                                              TraceCounters* cnt, uint32_t* err, const uint8_t* keyLut)
+{
+    Trav2 s;
+    trav2Init(bvh, s, o, d, tmin, tmax);
+    while (!trav2Step<ANY, STATS>(bvh, s, stack, cnt, err, keyLut))
+    {
+    }
+    *tHit  = s.bt;
+    *b1Hit = s.b1;
+    *b2Hit = s.b2;
+    *inst  = s.bestInst;
     return s.best;
 }
 

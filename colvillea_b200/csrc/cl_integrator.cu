@@ -115,8 +115,21 @@ struct HitAttr
 
 // Closest-hit attributes (optix.cu:137-227) of a triangle given by its
 // vertex ids and material (ti, the triangle's triIdx entry).
+// Two-level scenes: ti.w is the instance; the vertices are the mesh's, in
+// object space, and the attributes are mapped to world space before the
+// shading frame is built (position by the instance transform, normals by the
+// inverse transpose - the rows of object-from-world read as columns -, the
+// geometric normal flipped for a mirroring transform, tangents by the linear
+// part).  The flattened path (sc.inst null) keeps world-space vertices.
+__device__ __forceinline__ f3 xformNormal(const float4* __restrict__ w2o, f3 n)
+{
+    float4 a = __ldg(w2o), b = __ldg(w2o + 1), c = __ldg(w2o + 2);
+    return {a.x * n.x + b.x * n.y + c.x * n.z, a.y * n.x + b.y * n.y + c.y * n.z, a.z * n.x + b.z * n.y + c.z * n.z};
+}
+
 __device__ __forceinline__ HitAttr hitAttributesTri(const SceneDev& sc, uint4 ti, float b1, float b2)
 {
+    const InstDev* ip = sc.bvh.inst ? sc.bvh.inst + ti.w : nullptr;
     float4  a0 = __ldg(sc.vtx + 3 * size_t(ti.x)), a1 = __ldg(sc.vtx + 3 * size_t(ti.x) + 1), a2 = __ldg(sc.vtx + 3 * size_t(ti.x) + 2);
     float4  c0 = __ldg(sc.vtx + 3 * size_t(ti.y)), c1 = __ldg(sc.vtx + 3 * size_t(ti.y) + 1), c2 = __ldg(sc.vtx + 3 * size_t(ti.y) + 2);
     float4  e0 = __ldg(sc.vtx + 3 * size_t(ti.z)), e1 = __ldg(sc.vtx + 3 * size_t(ti.z) + 1), e2 = __ldg(sc.vtx + 3 * size_t(ti.z) + 2);
@@ -124,20 +137,28 @@ __device__ __forceinline__ HitAttr hitAttributesTri(const SceneDev& sc, uint4 ti
     uint32_t flags = __float_as_uint(a2.w);
     float   b0    = 1.0f - b1 - b2;
     HitAttr h;
-    h.material = ti.w;
+    h.material = ip ? __ldg(&ip->material) : ti.w;
     h.p        = b0 * p0 + b1 * p1;
     h.p        = h.p + b2 * p2;
     if (flags & 2u)
         h.uv = {b0 * a2.y + b1 * c2.y + b2 * e2.y, b0 * a2.z + b1 * c2.z + b2 * e2.z};
     else
         h.uv = {b0, b1};
-    f3 Ng = normalize(cross(p1 - p0, p2 - p0));
+    f3 Ng = cross(p1 - p0, p2 - p0);
+    if (ip)
+    {
+        h.p = xformPoint(ip->o2w, h.p);
+        Ng  = xformNormal(ip->w2o, Ng);
+        if (__ldg(&ip->flags) & 1u) Ng = -Ng;
+    }
+    Ng = normalize(Ng);
     f3 Ns;
     if (flags & 1u)
     {
         f3 n = b0 * f3{a0.w, a1.x, a1.y} + b1 * f3{c0.w, c1.x, c1.y};
         n    = n + b2 * f3{e0.w, e1.x, e1.y};
-        Ns   = normalize(n);
+        if (ip) n = xformNormal(ip->w2o, n);
+        Ns = normalize(n);
     }
     else
         Ns = normalize(Ng);
@@ -145,6 +166,7 @@ __device__ __forceinline__ HitAttr hitAttributesTri(const SceneDev& sc, uint4 ti
     if (dot(Ng, Ns) < 0.0f) Ng = -Ng;
     f3 t    = b0 * f3{a1.z, a1.w, a2.x} + b1 * f3{c1.z, c1.w, c2.x};
     t       = t + b2 * f3{e1.z, e1.w, e2.x};
+    if (ip) t = xformDir(ip->o2w, t);
     f3 dpdu = normalize(t);
     f3 dpdv{0.0f, 0.0f, 0.0f};
     if (dot(dpdu, dpdu) > 0.0f)
@@ -336,6 +358,10 @@ __device__ __forceinline__ void warpStats(const TraceCounters& tc, unsigned long
 // instruction count by half.)  CLASSIFY: the finished batch is appended to
 // the four shading-class queues (the hit material's BSDF type, or escaped),
 // so that each shading kernel runs one BSDF per warp.
+// Resident blocks per SM of the two-level traversal kernels (their state is
+// larger than the flattened traversal's; 8 blocks would spill).
+constexpr int kTraceBlocksTwo = 5;
+
 struct ClassifyView
 {
     const uint4* __restrict__ triIdx;
@@ -347,8 +373,10 @@ struct ClassifyView
 
 constexpr int kClassEscaped = 3;
 
-template <bool STATS, bool CLASSIFY>
-__global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
+// TWO: two-level scene (CL_TWO_LEVEL); the hit's triangle index entry then
+// holds the object-space vertex ids and the instance index (its .w).
+template <bool STATS, bool CLASSIFY, bool TWO = false>
+__global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
                                                                 const float4* __restrict__ D, const uint32_t* count,
                                                                 uint32_t* fetch, float4* __restrict__ hitOut,
                                                                 Counters* ctr, ClassifyView cv)
@@ -363,13 +391,20 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
         uint32_t base = warpFetch(fetch);
         if (base >= n) break;
         uint32_t i    = base + laneId();
-        uint32_t prim = kMissPrim;
+        uint32_t prim = kMissPrim, inst = 0u, loc = 0u;
         if (i < n)
         {
             float4 o = O[i], d = D[i];
             float  t, b1, b2;
-            prim      = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                               stack + threadIdx.x, &tc, &ctr->error, keyLut);
+            if (TWO)
+            {
+                loc = traverse2<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2, &inst,
+                                              stack + threadIdx.x, &tc, &ctr->error, keyLut);
+                if (loc != kMissPrim) prim = __ldg(&bvh.inst[inst].primBase) + loc;
+            }
+            else
+                prim = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
+                                              stack + threadIdx.x, &tc, &ctr->error, keyLut);
             hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
         }
         if (CLASSIFY)
@@ -379,6 +414,14 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
             {
                 if (prim == kMissPrim)
                     cls = kClassEscaped;
+                else if (TWO)
+                {
+                    const InstDev* ip = bvh.inst + inst;
+                    uint4          ti = __ldg(&cv.triIdx[__ldg(&ip->triBase) + loc]);
+                    ti.w              = inst;
+                    cv.hitIdx[i]      = ti;
+                    cls               = int(__float_as_uint(__ldg(&cv.mats[kMatF4 * __ldg(&ip->material)].x)));
+                }
                 else
                 {
                     const uint4 ti = __ldg(&cv.triIdx[prim]);
@@ -406,8 +449,8 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceClosest(BvhView bvh, con
 // Shadow rays (any hit) of the shadow queue.  Item k is entry k (path
 // tracing) or ray k&1 of entry k>>1 (direct lighting, two rays per entry).
 // vis[k] = 1 when the ray reaches its light, 0 otherwise.
-template <bool DL, bool STATS>
-__global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
+template <bool DL, bool STATS, bool TWO = false>
+__global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTraceShadow(Params P)
 {
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
@@ -428,8 +471,13 @@ __global__ void __launch_bounds__(kTraceBlock, 8) kTraceShadow(Params P)
             if (d4.w != 0.0f)
             {
                 float    t, b1, b2;
-                uint32_t h = traverse<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
-                                                   &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
+                uint32_t h, hi;
+                if (TWO)
+                    h = traverse2<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
+                                               &t, &b1, &b2, &hi, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
+                else
+                    h = traverse<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
+                                              &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
                 v = h == kMissPrim ? 1 : 0;
             }
             P.q.vis[item] = v;
@@ -1090,6 +1138,7 @@ __global__ void kAdvance(Counters* c, int cur)
     }
 }
 
+template <bool TWO>
 __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const float4* __restrict__ O,
                                                          const float4* __restrict__ D, uint32_t n,
                                                          uint8_t* __restrict__ occ, uint32_t* err)
@@ -1102,9 +1151,14 @@ __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const floa
     float4        o = O[i], d = D[i];
     float         t, b1, b2;
     TraceCounters tc{0u, 0u};
-    uint32_t      h = traverse<true, false>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                       stack + threadIdx.x, &tc, err, keyLut);
-    occ[i]          = h == kMissPrim ? 0 : 1;
+    uint32_t      h, hi;
+    if (TWO)
+        h = traverse2<true, false>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2, &hi,
+                                   stack + threadIdx.x, &tc, err, keyLut);
+    else
+        h = traverse<true, false>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
+                                  stack + threadIdx.x, &tc, err, keyLut);
+    occ[i] = h == kMissPrim ? 0 : 1;
 }
 
 __global__ void kAliasSample(DomeView dome, const float2* __restrict__ u, float* dir, float* pdf, float* val, uint32_t n)
@@ -1228,6 +1282,10 @@ cl_status Integrator::init(std::string* err)
                                                           traceStackBytes(kStackDepth)),
             err);
     traceBlocks_ = std::max(1, b) * numSMs_;
+    CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kTraceClosest<false, true, true>, kTraceBlock,
+                                                          traceStackBytes(kStackDepth)),
+            err);
+    traceBlocksTwo_ = std::max(1, b) * numSMs_;
     bool dl = type_ == CL_INTEGRATOR_DIRECT_LIGHTING;
     CL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void*)shadeKernel(dl, 2, cfg_.flags), 128, 0),
             err);
@@ -1375,6 +1433,10 @@ cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, s
         *err = "scene too large";
         return CL_ERR_INVALID_ARG;
     }
+    if (cfg_.flags & CL_TWO_LEVEL) return buildTwoLevel(inst, n, err);
+    twoLevel_ = false;
+    blas_.clear();
+    instDev_.release();
     // Flatten instances into world space (the reference's TLAS has no
     // transforms, optix.cu:115; identity transforms are copied exactly).
     std::vector<float>    vtx(nv * 12);
@@ -1446,6 +1508,240 @@ cl_status Integrator::buildInstances(const cl_instance_desc* inst, uint32_t n, s
     return CL_OK;
 }
 
+// Two-level build (CL_TWO_LEVEL): the meshes' object-space vertices and
+// triangles in one pool each, one 8-wide BVH per instanced mesh, the instance
+// records (transforms, tree pointers, global triangle base in instance
+// order, material) and the top tree over the instances' world boxes.  A top
+// tree leaf entry is a degenerate "triangle" spanning the instance's box
+// (v0 = v2 = min, v1 = max), so the same device builder makes both levels.
+static const float kIdentity12[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+
+cl_status Integrator::uploadMeshPool(uint32_t meshId, std::string* err)
+{
+    const HostMesh&    m  = meshes_[meshId];
+    const size_t       mv = m.pos.size() / 3;
+    std::vector<float> buf(mv * 12);
+    CL_TRY(flattenInstance(m, kIdentity12, meshId, buf.data(), err));
+    CL_CUDA(cudaMemcpyAsync(vtx_.f() + size_t(meshVtxBase_[meshId]) * 12, buf.data(), buf.size() * 4,
+                            cudaMemcpyHostToDevice, stream_),
+            err);
+    return CL_OK;
+}
+
+cl_status Integrator::buildBlas(uint32_t meshId, std::string* err)
+{
+    const HostMesh&    m  = meshes_[meshId];
+    const size_t       mt = m.idx.size() / 3;
+    std::vector<float> tri9(mt * 9);
+    for (size_t t = 0; t < mt; ++t)
+        for (int q = 0; q < 3; ++q)
+            for (int c = 0; c < 3; ++c) tri9[t * 9 + 3 * q + c] = m.pos[3 * size_t(m.idx[3 * t + q]) + c];
+    DevBuf d;
+    CL_TRY(d.alloc(tri9.size() * 4, err));
+    CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    if (!blas_[meshId]) blas_[meshId].reset(new WideBvh());
+    return buildWideBvh(d.f(), uint32_t(mt), stream_, blas_[meshId].get(), err);
+}
+
+// World box of instance i (every vertex mapped, in double), widened by a
+// relative 1e-6 so that FP32 rounding of the object-space traversal cannot
+// fall outside it.
+void Integrator::instanceBox(uint32_t i, float* lo, float* hi) const
+{
+    const HostMesh& m  = meshes_[inst_[i].mesh_id];
+    const float*    M  = inst_[i].transform;
+    double          l[3] = {1e300, 1e300, 1e300}, h[3] = {-1e300, -1e300, -1e300};
+    for (size_t v = 0; v < m.pos.size() / 3; ++v)
+        for (int r = 0; r < 3; ++r)
+        {
+            double x = double(M[4 * r]) * m.pos[3 * v] + double(M[4 * r + 1]) * m.pos[3 * v + 1] +
+                       double(M[4 * r + 2]) * m.pos[3 * v + 2] + double(M[4 * r + 3]);
+            l[r] = std::min(l[r], x);
+            h[r] = std::max(h[r], x);
+        }
+    double ext = std::max(h[0] - l[0], std::max(h[1] - l[1], h[2] - l[2]));
+    for (int r = 0; r < 3; ++r)
+    {
+        double pad = 1e-6 * ext + 1e-6 * std::max(std::fabs(l[r]), std::fabs(h[r])) + 1e-30;
+        lo[r] = float(l[r] - pad);
+        hi[r] = float(h[r] + pad);
+        if (double(lo[r]) > l[r] - pad) lo[r] = std::nextafter(lo[r], -FLT_MAX);
+        if (double(hi[r]) < h[r] + pad) hi[r] = std::nextafter(hi[r], FLT_MAX);
+    }
+}
+
+cl_status Integrator::buildTopLevel(std::string* err)
+{
+    const uint32_t     n = uint32_t(inst_.size());
+    std::vector<float> tri9(size_t(n) * 9);
+    float              slo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, shi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        float lo[3], hi[3];
+        instanceBox(i, lo, hi);
+        for (int c = 0; c < 3; ++c)
+        {
+            tri9[size_t(i) * 9 + c]     = lo[c];
+            tri9[size_t(i) * 9 + 3 + c] = hi[c];
+            tri9[size_t(i) * 9 + 6 + c] = lo[c];
+            slo[c]                      = std::min(slo[c], lo[c]);
+            shi[c]                      = std::max(shi[c], hi[c]);
+        }
+    }
+    // Scene box for the networks' position input (uniform scale).
+    float ext = std::max(shi[0] - slo[0], std::max(shi[1] - slo[1], shi[2] - slo[2]));
+    ext       = std::max(ext, 1e-6f) * 1.002f;
+    for (int q = 0; q < 3; ++q) boxMin_[q] = slo[q] - 0.001f * ext;
+    boxScale_ = 1.0f / ext;
+    DevBuf d;
+    CL_TRY(d.alloc(tri9.size() * 4, err));
+    CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    CL_TRY(buildWideBvh(d.f(), n, stream_, &bvh_, err));
+    uint32_t blasDepth = 0;
+    for (const auto& b : blas_)
+        if (b) blasDepth = std::max(blasDepth, b->depth);
+    // Stack: the top tree's pending groups (depth + 1, plus the two entries
+    // pushed when a ray enters an instance) and the mesh tree's (depth + 1).
+    const uint32_t need = bvh_.depth + 3u + blasDepth + 1u;
+    if (need > uint32_t(kStackDepth))
+    {
+        *err = "two-level scene too deep for the traversal stack (top depth " + std::to_string(bvh_.depth) +
+               ", mesh depth " + std::to_string(blasDepth) + ")";
+        return CL_ERR_INVALID_ARG;
+    }
+    twoLevelStack_ = need;
+    return CL_OK;
+}
+
+cl_status Integrator::uploadInstances(std::string* err)
+{
+    const uint32_t       n = uint32_t(inst_.size());
+    std::vector<InstDev> h(n);
+    uint32_t             primBase = 0;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const float* M = inst_[i].transform;
+        const double a = M[0], b = M[1], c = M[2], d = M[4], e = M[5], f = M[6], g = M[8], hh = M[9], k = M[10];
+        const double det = a * (e * k - f * hh) - b * (d * k - f * g) + c * (d * hh - e * g);
+        if (!(std::fabs(det) > 1e-30))
+        {
+            *err = "instance " + std::to_string(i) + ": singular transform";
+            return CL_ERR_INVALID_ARG;
+        }
+        // inverse of the linear part, row-major
+        const double inv[9] = {(e * k - f * hh) / det, -(b * k - c * hh) / det, (b * f - c * e) / det,
+                               -(d * k - f * g) / det, (a * k - c * g) / det,   -(a * f - c * d) / det,
+                               (d * hh - e * g) / det, -(a * hh - b * g) / det, (a * e - b * d) / det};
+        InstDev& r = h[i];
+        for (int row = 0; row < 3; ++row)
+        {
+            r.o2w[row] = make_float4(M[4 * row], M[4 * row + 1], M[4 * row + 2], M[4 * row + 3]);
+            const double tx = -(inv[3 * row] * M[3] + inv[3 * row + 1] * M[7] + inv[3 * row + 2] * M[11]);
+            r.w2o[row] = make_float4(float(inv[3 * row]), float(inv[3 * row + 1]), float(inv[3 * row + 2]), float(tx));
+        }
+        const uint32_t mid = inst_[i].mesh_id;
+        r.nodes    = blas_[mid]->nodes.as<const uint4>();
+        r.tris     = blas_[mid]->tris.as<const float4>();
+        r.primBase = primBase;
+        r.triBase  = meshTriBase_[mid];
+        r.material = inst_[i].material_index;
+        r.flags    = det < 0.0 ? 1u : 0u;
+        primBase += uint32_t(meshes_[mid].idx.size() / 3);
+    }
+    CL_TRY(instDev_.alloc(size_t(n) * sizeof(InstDev), err));
+    CL_CUDA(cudaMemcpyAsync(instDev_.p, h.data(), size_t(n) * sizeof(InstDev), cudaMemcpyHostToDevice, stream_), err);
+    numTris_ = primBase;
+    return CL_OK;
+}
+
+cl_status Integrator::buildTwoLevel(const cl_instance_desc* inst, uint32_t n, std::string* err)
+{
+    // Pools: every mesh's object-space vertices and triangles.
+    const uint32_t nm = uint32_t(meshes_.size());
+    meshVtxBase_.assign(nm, 0u);
+    meshTriBase_.assign(nm, 0u);
+    size_t nv = 0, nt = 0;
+    for (uint32_t m = 0; m < nm; ++m)
+    {
+        meshVtxBase_[m] = uint32_t(nv);
+        meshTriBase_[m] = uint32_t(nt);
+        nv += meshes_[m].pos.size() / 3;
+        nt += meshes_[m].idx.size() / 3;
+    }
+    std::vector<uint32_t> tidx(nt * 4);
+    for (uint32_t m = 0; m < nm; ++m)
+    {
+        const HostMesh& hm = meshes_[m];
+        for (size_t t = 0; t < hm.idx.size() / 3; ++t)
+        {
+            uint32_t* o = &tidx[(meshTriBase_[m] + t) * 4];
+            for (int q = 0; q < 3; ++q) o[q] = meshVtxBase_[m] + hm.idx[3 * t + q];
+            o[3] = 0u;
+        }
+    }
+    const auto   w0 = std::chrono::steady_clock::now();
+    const double a0 = allocMs();
+    CL_CUDA(cudaEventRecord(evA_, stream_), err);
+    CL_TRY(vtx_.alloc(nv * 48, err));
+    CL_TRY(triIdx_.alloc(nt * 16, err));
+    CL_CUDA(cudaMemcpyAsync(triIdx_.p, tidx.data(), tidx.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    for (uint32_t m = 0; m < nm; ++m) CL_TRY(uploadMeshPool(m, err));
+    std::vector<bool> used(nm, false);
+    for (uint32_t i = 0; i < n; ++i) used[inst[i].mesh_id] = true;
+    blas_.clear();
+    blas_.resize(nm);  // null entries
+    for (uint32_t m = 0; m < nm; ++m)
+        if (used[m]) CL_TRY(buildBlas(m, err));
+    inst_.assign(inst, inst + n);
+    CL_TRY(buildTopLevel(err));
+    CL_TRY(uploadInstances(err));
+    CL_CUDA(cudaEventRecord(evB_, stream_), err);
+    CL_CUDA(cudaEventSynchronize(evB_), err);
+    CL_CUDA(cudaEventElapsedTime(&msBvh_, evA_, evB_), err);
+    msBvhWall_  = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count());
+    msBvhAlloc_ = float(allocMs() - a0);
+    sahBuild_ = sah_ = 0.0;
+    twoLevel_   = true;
+    sceneBuilt_ = true;
+    graphValid_ = false;
+    instVtxOff_.clear();
+    maxMaterialIndex_ = 0;
+    for (uint32_t i = 0; i < n; ++i) maxMaterialIndex_ = std::max(maxMaterialIndex_, inst[i].material_index);
+    return CL_OK;
+}
+
+// Vertex edit of a two-level scene: the mesh's pool range is rewritten, its
+// tree refitted (CL_BVH_UPDATE_REFIT, _AUTO) or rebuilt (_REBUILD), and the
+// top tree rebuilt over the instances' new boxes.
+cl_status Integrator::updateTwoLevel(uint32_t meshId, uint32_t mode, std::string* err)
+{
+    CL_TRY(uploadMeshPool(meshId, err));
+    float ms = 0.0f;
+    msBvhRefit_ = 0.0f;
+    CL_CUDA(cudaEventRecord(evA_, stream_), err);
+    if (blas_[meshId])
+    {
+        if (mode == CL_BVH_UPDATE_REBUILD)
+        {
+            CL_TRY(buildBlas(meshId, err));
+            ++rebuilds_;
+        }
+        else
+        {
+            CL_TRY(refitWideBvh(blas_[meshId].get(), vtx_.p, triIdx_.as<uint4>() + meshTriBase_[meshId], stream_, err));
+            ++refits_;
+        }
+    }
+    CL_TRY(buildTopLevel(err));
+    CL_TRY(uploadInstances(err));
+    CL_CUDA(cudaEventRecord(evB_, stream_), err);
+    CL_CUDA(cudaEventSynchronize(evB_), err);
+    CL_CUDA(cudaEventElapsedTime(&ms, evA_, evB_), err);
+    msBvhUpdate_ = ms;
+    graphValid_  = false;
+    return resetIteration(err);
+}
+
 cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, const float* nrm, const float* tan,
                                          uint32_t count, uint32_t mode, std::string* err)
 {
@@ -1483,6 +1779,7 @@ cl_status Integrator::updateMeshVertices(uint32_t meshId, const float* pos, cons
         m.hasN = true;
     }
     if (tan) m.tan.assign(tan, tan + size_t(count) * 3);
+    if (twoLevel_) return updateTwoLevel(meshId, mode, err);
 
     // Re-flatten the instances of this mesh into their vertex ranges.
     std::vector<float> buf;
@@ -1745,7 +2042,10 @@ cl_status Integrator::ensureQueues(std::string* err)
 
 BvhView Integrator::bvhView() const
 {
-    return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(),
+    if (twoLevel_)
+        return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(), instDev_.as<const InstDev>(),
+                       twoLevelStack_};
+    return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(), nullptr,
                    std::min<uint32_t>(bvh_.depth + 1u, uint32_t(kStackDepth))};
 }
 
@@ -1825,12 +2125,13 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     Counters* c = ctr_.as<Counters>();
     const bool st = cfg_.flags & CL_TRACE_STATS;
     if (profile) CL_CUDA(cudaEventRecord(evS_[0], stream_), err);
-    if (st)
-        kTraceClosest<true, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
-            P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur], &c->fetchTrace, P.q.hit, c, classifyView());
-    else
-        kTraceClosest<false, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
-            P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur], &c->fetchTrace, P.q.hit, c, classifyView());
+    {
+        const size_t sb = traceStackBytes(P.sc.bvh.stackDepth);
+        auto         k  = st ? (twoLevel_ ? kTraceClosest<true, true, true> : kTraceClosest<true, true, false>)
+                             : (twoLevel_ ? kTraceClosest<false, true, true> : kTraceClosest<false, true, false>);
+        k<<<tBlocks(), kTraceBlock, sb, stream_>>>(P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur],
+                                                      &c->fetchTrace, P.q.hit, c, classifyView());
+    }
     if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
     const uint32_t gmask = guide_ ? guideCfg_.class_mask : 0u;
     if (gmask)
@@ -1848,14 +2149,15 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
     for (int m = 0; m < 4; ++m)
         shadeKernel(dl, m, cfg_.flags, m < 3 && ((gmask >> m) & 1u))<<<shadeBlocks_, 128, 0, stream_>>>(P, cur);
     if (profile) CL_CUDA(cudaEventRecord(evS_[2], stream_), err);
-    if (dl && st)
-        kTraceShadow<true, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
-    else if (dl)
-        kTraceShadow<true, false><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
-    else if (st)
-        kTraceShadow<false, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
-    else
-        kTraceShadow<false, false><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
+    {
+        using ShadowFn = void (*)(Params);
+        const ShadowFn table[2][2][2] = {
+            {{kTraceShadow<false, false, false>, kTraceShadow<false, false, true>},
+             {kTraceShadow<false, true, false>, kTraceShadow<false, true, true>}},
+            {{kTraceShadow<true, false, false>, kTraceShadow<true, false, true>},
+             {kTraceShadow<true, true, false>, kTraceShadow<true, true, true>}}};
+        table[dl][st][twoLevel_]<<<tBlocks(), kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(P);
+    }
     if (dl)
         kShadowResolve<true><<<shadowBlocks_, 128, 0, stream_>>>(P, cur);
     else
@@ -2457,9 +2759,10 @@ cl_status Integrator::traceRays(const float* rays, uint32_t n, float* t, uint32_
         Counters c0{};
         c0.rayCount[0] = m;
         CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
-        kTraceClosest<false, false><<<traceBlocks_, kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
-            bvhView(), rqO_[0].as<float4>(),
-            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc, ClassifyView{});
+        (twoLevel_ ? kTraceClosest<false, false, true> : kTraceClosest<false, false, false>)
+            <<<tBlocks(), kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
+                bvhView(), rqO_[0].as<float4>(), rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace,
+                hit_.as<float4>(), dc, ClassifyView{});
         CL_CUDA(cudaGetLastError(), err);
         CL_CUDA(cudaMemcpyAsync(h.data(), hit_.p, m * 16, cudaMemcpyDeviceToHost, stream_), err);
         Counters ch;
@@ -2510,7 +2813,8 @@ cl_status Integrator::occludedRays(const float* rays, uint32_t n, uint8_t* occ, 
     CL_CUDA(cudaMemcpyAsync(o.p, ho.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaMemcpyAsync(d.p, hd.data(), size_t(n) * 16, cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaMemsetAsync(ctr_.p, 0, sizeof(Counters), stream_), err);
-    kOccluded<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
+    (twoLevel_ ? kOccluded<true> : kOccluded<false>)
+        <<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
         bvhView(), o.as<float4>(), d.as<float4>(), n,
         r.as<uint8_t>(), &ctr_.as<Counters>()->error);
     CL_CUDA(cudaGetLastError(), err);
@@ -2549,9 +2853,10 @@ cl_status Integrator::traceStats(const float* rays, uint32_t n, uint64_t* nodes,
         Counters c0{};
         c0.rayCount[0] = m;
         CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, stream_), err);
-        kTraceClosest<true, false><<<traceBlocks_, kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
-            bvhView(), rqO_[0].as<float4>(),
-            rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace, hit_.as<float4>(), dc, ClassifyView{});
+        (twoLevel_ ? kTraceClosest<true, false, true> : kTraceClosest<true, false, false>)
+            <<<tBlocks(), kTraceBlock, traceStackBytes(bvhView().stackDepth), stream_>>>(
+                bvhView(), rqO_[0].as<float4>(), rqD_[0].as<float4>(), &dc->rayCount[0], &dc->fetchTrace,
+                hit_.as<float4>(), dc, ClassifyView{});
         CL_CUDA(cudaGetLastError(), err);
         Counters ch;
         CL_CUDA(cudaMemcpyAsync(&ch, ctr_.p, sizeof(ch), cudaMemcpyDeviceToHost, stream_), err);
@@ -2615,8 +2920,9 @@ cl_status Integrator::guideProbe(uint32_t cap, float* rows, uint32_t* count, std
     P.g.probeCap   = cap;
     Counters* c    = ctr_.as<Counters>();
     kRaygen<<<(init + 255) / 256, 256, 0, stream_>>>(P, init);
-    kTraceClosest<false, true><<<traceBlocks_, kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
-        P.sc.bvh, P.q.rqO[0], P.q.rqD[0], &c->rayCount[0], &c->fetchTrace, P.q.hit, c, classifyView());
+    (twoLevel_ ? kTraceClosest<false, true, true> : kTraceClosest<false, true, false>)
+        <<<tBlocks(), kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
+            P.sc.bvh, P.q.rqO[0], P.q.rqD[0], &c->rayCount[0], &c->fetchTrace, P.q.hit, c, classifyView());
     kGuideInfer<<<inferBlocks_, guide::kTcThreads, kGuideMlpSmem, stream_>>>(
         P, guide_->grid(), 0, guide_->tcWeights(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
     CL_CUDA(cudaGetLastError(), err);

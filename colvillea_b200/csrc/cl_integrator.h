@@ -212,7 +212,8 @@ private:
     cl_render_config   cfg_;
     cudaStream_t       stream_ = nullptr;
     int                numSMs_ = 148;
-    int                traceBlocks_ = 0, shadeBlocks_ = 0, shadowBlocks_ = 0;
+    int                traceBlocks_ = 0, shadeBlocks_ = 0, shadowBlocks_ = 0, traceBlocksTwo_ = 0;
+    int                tBlocks() const { return twoLevel_ ? traceBlocksTwo_ : traceBlocks_; }
 
     // Meshes as given (host copies), flattened on instance build.
     struct HostMesh
@@ -225,6 +226,20 @@ private:
     cl_status flattenInstance(const HostMesh& m, const float* M, uint32_t i, float* out, std::string* err);
     std::vector<cl_instance_desc> inst_;       // as built
     std::vector<uint32_t>         instVtxOff_; // first flattened vertex of each instance
+    // Two-level scenes (CL_TWO_LEVEL): object-space pools, one tree per mesh,
+    // the instance records; bvh_ is then the top tree over the instances.
+    bool                   twoLevel_ = false;
+    std::vector<std::unique_ptr<WideBvh>> blas_; // per mesh (null: not instanced)
+    std::vector<uint32_t>  meshVtxBase_, meshTriBase_;
+    DevBuf                 instDev_;
+    uint32_t               twoLevelStack_ = 0;
+    cl_status buildTwoLevel(const cl_instance_desc* inst, uint32_t n, std::string* err);
+    cl_status uploadMeshPool(uint32_t meshId, std::string* err);
+    cl_status buildBlas(uint32_t meshId, std::string* err);
+    cl_status buildTopLevel(std::string* err);
+    cl_status uploadInstances(std::string* err);
+    cl_status updateTwoLevel(uint32_t meshId, uint32_t mode, std::string* err);
+    void      instanceBox(uint32_t i, float* lo, float* hi) const;
     // Refit policy (CL_BVH_UPDATE_AUTO): rebuild when the refitted tree's
     // surface-area cost exceeds this multiple of the cost after its build.
     static constexpr double kRefitSahLimit = 1.5;

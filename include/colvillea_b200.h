@@ -81,14 +81,21 @@ enum
     CL_PROFILE_STAGES = 1u << 6,
     /* Count BVH nodes visited and triangles tested by the traversal kernels
      * of each render (cl_get_stats); slower, for roofline accounting. */
-    CL_TRACE_STATS = 1u << 7
+    CL_TRACE_STATS = 1u << 7,
+    /* Two-level scene: one 8-wide BVH per mesh in object space and one over
+     * the instances' world boxes; rays enter an instance's tree mapped to
+     * object space (instancing without flattening; no counterpart in the
+     * reference, whose TLAS has no transforms, optix.cu:115).  Without it the
+     * instances are flattened into one world-space tree. */
+    CL_TWO_LEVEL = 1u << 8
 };
 
 typedef struct
 {
     uint32_t max_depth;      /* ray segments per path (reference: 5, path.cpp:135) */
     uint32_t rr_start_depth; /* Russian roulette from this path depth on; 0 = off */
-    uint32_t flags;          /* CL_COMPAT_*, CL_DOME_ALIAS, CL_FILM_FP64, CL_PROFILE_STAGES */
+    uint32_t flags;          /* CL_COMPAT_*, CL_DOME_ALIAS, CL_FILM_FP64, CL_PROFILE_STAGES, CL_TRACE_STATS,
+                                CL_TWO_LEVEL */
     uint32_t path_slots;     /* paths in flight; 0 = automatic */
 } cl_render_config;
 
