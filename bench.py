@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--profile", type=int, default=0, metavar="SPP",
                     help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
+    ap.add_argument("--flatten", action="store_true",
+                    help="config 5: flatten the instances into one world-space tree instead of the two-level scene")
     ap.add_argument("--no-relmse", action="store_true", help="skip the guided-vs-plain equal-time relMSE")
     ap.add_argument("--no-edit", action="store_true", help="skip the shape-edit (refit vs rebuild) measurement")
     ap.add_argument("--extended", action="store_true",
@@ -349,12 +351,16 @@ def run_guide_study(args):
     t_ref = time.perf_counter() - t0
     G = cb.GuideConfig
     variants = {
-        "guided": G(),
-        "guided_indirect": G(min_depth=2),
+        "guided_diffuse_conductor": G(class_mask=3),
+        "guided_diffuse_conductor_indirect": G(class_mask=3, min_depth=2),
+        "guided_diffuse_conductor_train128": G(class_mask=3, train_spp=128),
         "guided_all_classes": G(class_mask=7),
-        "guided_train64": G(train_spp=64),
-        "guided_train128": G(train_spp=128),
-        "guided_indirect_train64": G(min_depth=2, train_spp=64),
+        "guided_all_classes_indirect": G(class_mask=7, min_depth=2),
+        "guided_all_classes_train64": G(class_mask=7, train_spp=64),
+        "guided_all_classes_learned_selection": G(class_mask=7, learn_selection=1),
+        "guided_all_classes_bsdf_fraction_0.3": G(class_mask=7, bsdf_fraction=0.3),
+        "guided_all_classes_bsdf_fraction_0.7": G(class_mask=7, bsdf_fraction=0.7),
+        "guided_dielectric_only": G(class_mask=4),
     }
     rows = evaluate.equal_spp(s3, ref, args.relmse_spp, variants, seeds=2)
     rnd = lambda d: {k: (round(v, 6) if isinstance(v, float) else ([round(x, 6) for x in v] if isinstance(v, list)
@@ -473,12 +479,20 @@ def main():
         cbuild.build()
     s = scenes.CONFIGS[args.config](0)
     W, H = s.width, s.height
-    flags = cb.COMPAT_ALL | cb.DOME_ALIAS
+    # Config 5's repeated, transformed meshes use the two-level scene (one tree
+    # per mesh, one over the instances) unless --flatten asks for one
+    # world-space tree over the flattened instances.
+    two = args.config == 5 and not args.flatten
+    flags = cb.COMPAT_ALL | cb.DOME_ALIAS | (cb.TWO_LEVEL if two else 0)
     # The timed integrator runs the product path (waves replayed from a CUDA
     # graph); a second one with per-stage CUDA events (each wave launched and
     # synchronised on its own, about 5% slower) gives the stage times and the
     # traversal kernel's time for the roofline, over the same number of steps.
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     it = cb.load_scene(s, flags=flags, path_slots=args.slots)
+    torch.cuda.synchronize()
+    scene_mb = (free0 - torch.cuda.mem_get_info()[0]) / 2**20
     st0 = it.stats()
 
     # Traversal counters on the identical ray set of the first timed step.
@@ -600,7 +614,9 @@ def main():
                   "bvh_ms_cold_alloc": round(st0["ms_bvh_build_alloc"], 2),
                   "bvh_ms_warm": round(sst["ms_bvh_build"], 2), "bvh_ms_warm_wall": round(sst["ms_bvh_build_wall"], 2),
                   "bvh_ms_warm_alloc": round(sst["ms_bvh_build_alloc"], 2), "bvh_nodes": st0["bvh_nodes"],
-                  "bvh_depth": st0["bvh_depth"], "dome_ms": round(st0["ms_dome_build"], 2)},
+                  "bvh_depth": st0["bvh_depth"], "dome_ms": round(st0["ms_dome_build"], 2),
+                  "instancing": "two-level (one tree per mesh + instance tree)" if two else "flattened (one tree)",
+                  "scene_device_mb": round(scene_mb, 1)},
     }
     if e2e:
         line["e2e"] = e2e

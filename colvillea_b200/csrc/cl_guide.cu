@@ -678,7 +678,7 @@ void guideDefaultConfig(cl_guide_config* c)
     c->bsdf_fraction   = 0.5f;
     c->batch           = 1u << 18;
     c->train_spp       = 32;
-    c->class_mask      = 3u;
+    c->class_mask      = 7u;
     c->seed            = 1;
     c->learn_selection = 0u;
     c->weight_clamp    = 0.0f;

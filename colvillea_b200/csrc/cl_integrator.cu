@@ -383,6 +383,8 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
 {
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
+    __shared__ uint4        top[kTopNodes * 5];
+    stageTopNodes(bvh, top);
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(count);
     TraceCounters    tc{0u, 0u};
@@ -404,7 +406,7 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
             }
             else
                 prim = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                              stack + threadIdx.x, &tc, &ctr->error, keyLut);
+                                              stack + threadIdx.x, &tc, &ctr->error, keyLut, top);
             hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
         }
         if (CLASSIFY)
@@ -454,6 +456,8 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
 {
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
+    __shared__ uint4        top[kTopNodes * 5];
+    stageTopNodes(P.sc.bvh, top);
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(&P.q.ctr->shadowCount) * (DL ? 2u : 1u);
     TraceCounters    tc{0u, 0u};
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
                                                &t, &b1, &b2, &hi, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
                 else
                     h = traverse<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
-                                              &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
+                                              &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut, top);
                 v = h == kMissPrim ? 1 : 0;
             }
             P.q.vis[item] = v;
@@ -1145,6 +1149,8 @@ __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const floa
 {
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
+    __shared__ uint4        top[kTopNodes * 5];
+    stageTopNodes(bvh, top);
     fillKeyLut(keyLut);
     uint32_t         i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1157,7 +1163,7 @@ __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const floa
                                    stack + threadIdx.x, &tc, err, keyLut);
     else
         h = traverse<true, false>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                  stack + threadIdx.x, &tc, err, keyLut);
+                                  stack + threadIdx.x, &tc, err, keyLut, top);
     occ[i] = h == kMissPrim ? 0 : 1;
 }
 
@@ -2044,9 +2050,13 @@ BvhView Integrator::bvhView() const
 {
     if (twoLevel_)
         return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(), instDev_.as<const InstDev>(),
-                       twoLevelStack_};
+                       twoLevelStack_, 0u};
+    // Top nodes: the root and level 1 (the collapse allocates level d as the
+    // node range [levels[d], levels[d + 1])).
+    uint32_t top = bvh_.levels.size() > 2 ? bvh_.levels[2] : bvh_.numNodes;
+    top          = std::min(top, kTopNodes);
     return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(), nullptr,
-                   std::min<uint32_t>(bvh_.depth + 1u, uint32_t(kStackDepth))};
+                   std::min<uint32_t>(bvh_.depth + 1u, uint32_t(kStackDepth)), top};
 }
 
 ClassifyView Integrator::classifyView() const

@@ -504,7 +504,7 @@ typedef struct cl_guide_config
     float    bsdf_fraction;                /* one-sample MIS: probability of BSDF sampling, [0, 1] (0.5) */
     uint32_t batch;                        /* training samples per step (2^18) */
     uint32_t train_spp;                    /* one training step after each of the first train_spp spp (32) */
-    uint32_t class_mask;                   /* guided BSDFs: bit 0 diffuse, 1 conductor, 2 dielectric (3) */
+    uint32_t class_mask;                   /* guided BSDFs: bit 0 diffuse, 1 conductor, 2 dielectric (7) */
     uint32_t seed;                         /* parameter initialisation */
     uint32_t learn_selection;              /* 1: the probability of sampling the network is learned (head
                                               output 40) and training minimises -log of the whole one-sample
