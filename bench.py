@@ -351,16 +351,14 @@ def run_guide_study(args):
     t_ref = time.perf_counter() - t0
     G = cb.GuideConfig
     variants = {
-        "guided_diffuse_conductor": G(class_mask=3),
-        "guided_diffuse_conductor_indirect": G(class_mask=3, min_depth=2),
-        "guided_diffuse_conductor_train128": G(class_mask=3, train_spp=128),
         "guided_all_classes": G(class_mask=7),
-        "guided_all_classes_indirect": G(class_mask=7, min_depth=2),
-        "guided_all_classes_train64": G(class_mask=7, train_spp=64),
-        "guided_all_classes_learned_selection": G(class_mask=7, learn_selection=1),
-        "guided_all_classes_bsdf_fraction_0.3": G(class_mask=7, bsdf_fraction=0.3),
-        "guided_all_classes_bsdf_fraction_0.7": G(class_mask=7, bsdf_fraction=0.7),
+        "guided_all_classes_bsdf_fraction_0.7_train64": G(class_mask=7, bsdf_fraction=0.7, train_spp=64),
+        "guided_all_classes_bsdf_fraction_0.8": G(class_mask=7, bsdf_fraction=0.8),
         "guided_dielectric_only": G(class_mask=4),
+        "guided_dielectric_only_bsdf_fraction_0.7": G(class_mask=4, bsdf_fraction=0.7),
+        "guided_dielectric_only_bsdf_fraction_0.8": G(class_mask=4, bsdf_fraction=0.8),
+        "guided_dielectric_only_bsdf_fraction_0.7_train64": G(class_mask=4, bsdf_fraction=0.7, train_spp=64),
+        "guided_dielectric_only_bsdf_fraction_0.7_indirect": G(class_mask=4, bsdf_fraction=0.7, min_depth=2),
     }
     rows = evaluate.equal_spp(s3, ref, args.relmse_spp, variants, seeds=2)
     rnd = lambda d: {k: (round(v, 6) if isinstance(v, float) else ([round(x, 6) for x in v] if isinstance(v, list)

@@ -59,14 +59,15 @@ struct BvhView
     const uint4* __restrict__ nodes;
     const float4* __restrict__ tris;
     const InstDev* __restrict__ inst; // two-level: the instances (nodes/tris are the top tree); null otherwise
-    // Nodes [0, topNodes) - the root and its children - are staged in each
-    // traversal block's shared memory (flattened scenes; 0 in two-level ones).
-    uint32_t topNodes;
     // Traversal stack entries per thread: the tree's depth + 1 (a ray holds
     // at most one pending node group per level), at most kStackDepth.  The
     // kernels' dynamic shared memory is stackDepth * kTraceBlock * 8 bytes,
     // so that a shallow tree leaves more of the SM's on-chip memory to L1.
     uint32_t stackDepth;
+    // Nodes [0, topNodes) - the root and its children, at most kTopNodes - are
+    // staged in each traversal block's shared memory (flattened scenes; 0 in
+    // two-level ones).
+    uint32_t topNodes;
 };
 
 __host__ __device__ constexpr size_t traceStackBytes(uint32_t depth) { return size_t(depth) * kTraceBlock * 8u; }
@@ -77,7 +78,8 @@ constexpr uint32_t kTopNodes = 9; // the root and its (at most 8) children
 // takes part; the caller's __syncthreads makes them visible).
 __device__ __forceinline__ void stageTopNodes(const BvhView& bvh, uint4* top)
 {
-    for (uint32_t i = threadIdx.x; i < bvh.topNodes * 5u; i += blockDim.x) top[i] = __ldg(bvh.nodes + i);
+    const uint32_t n = min(bvh.topNodes, kTopNodes) * 5u;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) top[i] = __ldg(bvh.nodes + i);
 }
 
 struct TraceCounters
@@ -258,7 +260,7 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
         }
         uint32_t cb, tb, im;
         uint32_t hits = intersectNode(bvh.nodes, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im, keyLut, top,
-                                      bvh.topNodes);
+                                      min(bvh.topNodes, kTopNodes));
         if (STATS) cnt->nodes++;
         s.ng = make_uint2(cb, (hits & 0xff000000u) | im);
         s.tg = make_uint2(tb, hits & 0x00ffffffu);

@@ -365,7 +365,14 @@ __device__ __forceinline__ bool tcWaitAll(uint32_t bar, uint32_t& phase)
     return __syncthreads_and(ok) != 0;
 }
 
-template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) kTrainTc(TrainArgs a)
+// Two threads per sample row (256 per CTA): thread t serves row t % 128;
+// half h = t / 128 encodes hash levels 8h .. 8h+7 and one of the two one-blob
+// directions, converts columns 32h .. 32h+31 of each layer's accumulator
+// (warps w and w + 4 read the same TMEM lanes), and scatters the hash-feature
+// gradient of its 8 levels; the head's loss runs in half 0.
+constexpr int kTrainThreads = 2 * kTcThreads;
+
+template <class S, class LOSS> __global__ void __launch_bounds__(kTrainThreads, 1) kTrainTc(TrainArgs a)
 {
     using T              = TrainTc<S>;
     constexpr int L      = T::L;
@@ -373,10 +380,10 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
     const uint32_t count = *a.count, nB = min(count, a.batch);
     const uint32_t tiles = (nB + kTcRows - 1) / kTcRows;
     if (blockIdx.x >= tiles) return; // before any TMEM allocation
-    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u;
+    const uint32_t t = threadIdx.x, warp = t >> 5, lane = t & 31u, row = t & (kTcRows - 1u), half = t >> 7;
     {
         uint4* w = reinterpret_cast<uint4*>(smem);
-        for (int i = int(t); i < T::kW / 16; i += kTcThreads) w[i] = __ldg(a.wt + i);
+        for (int i = int(t); i < T::kW / 16; i += kTrainThreads) w[i] = __ldg(a.wt + i);
     }
     const uint32_t bar = smemAddr(smem + T::kBar);
     if (t == 0) mbarInit(bar, 1u);
@@ -385,7 +392,7 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
     __syncthreads();
     tcFenceAfter();
     const uint32_t tmem  = *reinterpret_cast<volatile uint32_t*>(smem + T::kBar + 8);
-    const uint32_t tRow  = tmem + ((warp * 32u) << 16); // this warp's TMEM lanes
+    const uint32_t tRow  = tmem + (((warp & 3u) * 32u) << 16); // this warp's TMEM lanes
     const uint32_t wS    = smemAddr(smem), dS = smemAddr(smem + T::kDelta);
     const double   wsum  = a.clamp > 0.0f ? a.scal[3] : a.scal[0];
     const float    invW  = wsum > 0.0 ? float(1.0 / wsum) : 0.0f;
@@ -394,35 +401,44 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
     float          lossPart = 0.0f;
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x)
     {
-        const uint32_t j     = tile * kTcRows + t;
+        const uint32_t j     = tile * kTcRows + row;
         const bool     valid = j < nB;
-        // Encoding -> a_0 row t.
+        // Encoding -> a_0 row `row`: this half's 8 hash levels and one direction.
         f3       p{0.0f, 0.0f, 0.0f};
         float4   r3{0.0f, 0.0f, 0.0f, 0.0f};
         float    sw = 0.0f;
-        uint32_t r[kIn / 2];
+        uint32_t hs[4 * 2], bl[kBlob];
         if (valid)
         {
             const float4* R  = a.rec + kRecordF4 * size_t(recordOf(j, count, nB));
-            const float4  r0 = R[0], r1 = R[1], r2 = R[2];
+            const float4  r0 = R[0], rd = R[1 + half];
             r3               = R[3];
             p                = clampUnit(f3{r0.x, r0.y, r0.z});
             sw               = trainWeight(r0.w, a, nB) * invW;
 #pragma unroll
-            for (int l = 0; l < kLevels; ++l)
+            for (int q = 0; q < 8; ++q)
             {
-                const float2 f = encodeLevel(a.g, l, p);
-                r[l]           = packBf16(f.x, f.y);
+                const float2 f = encodeLevel(a.g, int(8 * half) + q, p);
+                hs[q]          = packBf16(f.x, f.y);
             }
-            oneBlobPacked(f3{r1.x, r1.y, r1.z}, r + kHashF / 2);
-            oneBlobPacked(f3{r2.x, r2.y, r2.z}, r + (kHashF + 2 * kBlob) / 2);
+            oneBlobPacked(f3{rd.x, rd.y, rd.z}, bl);
         }
         else
+        {
 #pragma unroll
-            for (int q = 0; q < kIn / 2; ++q) r[q] = 0u;
+            for (int q = 0; q < 8; ++q) hs[q] = 0u;
 #pragma unroll
-        for (int c = 0; c < kIn / 8; ++c)
-            *tileChunk(smem + T::act(0), t, c) = make_uint4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+            for (int q = 0; q < kBlob; ++q) bl[q] = 0u;
+        }
+        {
+            unsigned char* a0 = smem + T::act(0);
+            *tileChunk(a0, row, int(2 * half))     = make_uint4(hs[0], hs[1], hs[2], hs[3]);
+            *tileChunk(a0, row, int(2 * half) + 1) = make_uint4(hs[4], hs[5], hs[6], hs[7]);
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                *tileChunk(a0, row, kHashF / 8 + int(4 * half) + c) =
+                    make_uint4(bl[4 * c], bl[4 * c + 1], bl[4 * c + 2], bl[4 * c + 3]);
+        }
         // Forward.
         float o[S::kOut];
 #pragma unroll 1
@@ -444,16 +460,16 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
             if (!ok) break;
             if (l < L)
             {
-                uint32_t v[kWidth / 16][16];
+                uint32_t v[2][16];
 #pragma unroll
-                for (int c = 0; c < kWidth / 16; ++c) tmemLd16(tRow + uint32_t(16 * c), v[c]);
+                for (int c = 0; c < 2; ++c) tmemLd16(tRow + 32u * half + uint32_t(16 * c), v[c]);
                 tmemWait();
                 unsigned char* nxt = smem + T::act(l + 1);
 #pragma unroll
-                for (int c = 0; c < kWidth / 16; ++c)
+                for (int c = 0; c < 2; ++c)
                 {
-                    *tileChunk(nxt, t, 2 * c)     = packRelu8(v[c]);
-                    *tileChunk(nxt, t, 2 * c + 1) = packRelu8(v[c] + 8);
+                    *tileChunk(nxt, row, int(4 * half) + 2 * c)     = packRelu8(v[c]);
+                    *tileChunk(nxt, row, int(4 * half) + 2 * c + 1) = packRelu8(v[c] + 8);
                 }
             }
             else
@@ -469,7 +485,8 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
             }
         }
         if (!ok) break;
-        // Loss and output gradient -> delta row t (columns >= kOut zero).
+        // Loss and output gradient (half 0) -> delta row (columns >= kOut zero).
+        if (half == 0u)
         {
             float gr[S::kOut];
             if (valid)
@@ -489,7 +506,7 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
                 if (8 * c < S::kOut)
                     v = make_uint4(packBf16(gr[8 * c], gr[8 * c + 1]), packBf16(gr[8 * c + 2], gr[8 * c + 3]),
                                    packBf16(gr[8 * c + 4], gr[8 * c + 5]), packBf16(gr[8 * c + 6], gr[8 * c + 7]));
-                *tileChunk(d, t, c) = v;
+                *tileChunk(d, row, c) = v;
             }
         }
         // Backward.
@@ -520,17 +537,19 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
             if (!ok) break;
             if (l > 0)
             {
-                // delta of layer l-1 = acc masked by ReLU'(a_l): a zero bf16 input was a unit that was off.
-                uint32_t v[kWidth / 16][16];
+                // delta of layer l-1 = acc masked by ReLU'(a_l) (a zero bf16 input was a unit that was off);
+                // this half's 32 columns.
+                uint32_t v[2][16];
 #pragma unroll
-                for (int c = 0; c < kWidth / 16; ++c) tmemLd16(tRow + uint32_t(16 * c), v[c]);
+                for (int c = 0; c < 2; ++c) tmemLd16(tRow + 32u * half + uint32_t(16 * c), v[c]);
                 tmemWait();
                 const unsigned char* al = smem + T::act(l);
                 unsigned char*       d  = smem + T::kDelta;
 #pragma unroll
-                for (int c = 0; c < kWidth / 8; ++c)
+                for (int c = 0; c < 4; ++c)
                 {
-                    const uint4     m  = *tileChunk(const_cast<unsigned char*>(al), t, c);
+                    const int       cc    = int(4 * half) + c;
+                    const uint4     m     = *tileChunk(const_cast<unsigned char*>(al), row, cc);
                     const uint32_t  mw[4] = {m.x, m.y, m.z, m.w};
                     const uint32_t* src   = v[c >> 1] + 8 * (c & 1);
                     uint32_t        pk[4];
@@ -541,23 +560,22 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
                         const float hi = (mw[q] >> 16) ? __uint_as_float(src[2 * q + 1]) : 0.0f;
                         pk[q]          = packBf16(lo, hi);
                     }
-                    *tileChunk(d, t, c) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                    *tileChunk(d, row, cc) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
                 }
             }
             else
             {
-                // Gradient of the 32 hash features (FP32): feature f of level l is column 2 l + f.
-                // (The TMEM load is warp-collective: every lane takes part, valid or not.)
-                uint32_t v[kHashF / 16][16];
-#pragma unroll
-                for (int c = 0; c < kHashF / 16; ++c) tmemLd16(tRow + uint32_t(16 * c), v[c]);
+                // Gradient of this half's 8 hash levels (FP32 columns 16h .. 16h+15: feature f of level l
+                // is column 2 l + f).  The TMEM load is warp-collective: every lane takes part.
+                uint32_t v[16];
+                tmemLd16(tRow + 16u * half, v);
                 tmemWait();
 #pragma unroll
-                for (int lv = 0; lv < kLevels; ++lv)
+                for (int q = 0; q < 8; ++q)
                 {
-                    const float d0 = __uint_as_float(v[lv >> 3][2 * (lv & 7)]);
-                    const float d1 = __uint_as_float(v[lv >> 3][2 * (lv & 7) + 1]);
+                    const float d0 = __uint_as_float(v[2 * q]), d1 = __uint_as_float(v[2 * q + 1]);
                     if (!valid || (d0 == 0.0f && d1 == 0.0f)) continue;
+                    const int  lv = int(8 * half) + q;
                     const Cell c  = gridCell(a.g.res[lv], p);
                     float2*    gb = a.gradTable + (size_t(lv) << a.g.log2T);
 #pragma unroll
@@ -579,16 +597,16 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTcThreads, 1) 
     }
     else if (!first)
     {
-        // Weight gradients: row r of dW_l (M = 64) is in TMEM lane 32 (r / 16) + r % 16, so warp w
-        // holds rows 16 w .. 16 w + 15 in its lanes 0-15.
-        const int o = int(warp) * 16 + int(lane);
+        // Weight gradients: row r of dW_l (M = 64) is in TMEM lane 32 (r / 16) + r % 16, so warps w and
+        // w + 4 hold rows 16 (w % 4) .. + 15 in their lanes 0-15; the halves take alternate 16-column groups.
+        const int o = int(warp & 3u) * 16 + int(lane);
 #pragma unroll 1
         for (int l = 0; l <= L; ++l)
         {
             const int I = S::in(l);
             float*    G = a.gradMlp + S::woff(l);
 #pragma unroll 1
-            for (int c = 0; c < I / 16; ++c)
+            for (int c = int(half); c < I / 16; c += 2)
             {
                 uint32_t v[16];
                 tmemLd16(tRow + T::dw(l) + uint32_t(16 * c), v);
@@ -959,7 +977,7 @@ cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* coun
         CL_CUDA(cudaGetLastError(), err);
     }
     const uint32_t tiles = (cfg_.batch + kTcRows - 1) / kTcRows;
-    kTrainTc<S, L><<<std::min<uint32_t>(tiles, uint32_t(numSMs_)), kTcThreads, TrainTc<S>::kSmem, st_>>>(a);
+    kTrainTc<S, L><<<std::min<uint32_t>(tiles, uint32_t(numSMs_)), kTrainThreads, TrainTc<S>::kSmem, st_>>>(a);
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }

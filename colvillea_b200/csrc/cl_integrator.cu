@@ -2048,15 +2048,24 @@ cl_status Integrator::ensureQueues(std::string* err)
 
 BvhView Integrator::bvhView() const
 {
+    // Named members (not an aggregate list): the struct's field order is no
+    // part of this function's contract.
+    BvhView v{};
+    v.nodes = bvh_.nodes.as<const uint4>();
+    v.tris  = bvh_.tris.as<const float4>();
     if (twoLevel_)
-        return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(), instDev_.as<const InstDev>(),
-                       twoLevelStack_, 0u};
+    {
+        v.inst       = instDev_.as<const InstDev>();
+        v.stackDepth = twoLevelStack_;
+        v.topNodes   = 0u;
+        return v;
+    }
+    v.inst       = nullptr;
+    v.stackDepth = std::min<uint32_t>(bvh_.depth + 1u, uint32_t(kStackDepth));
     // Top nodes: the root and level 1 (the collapse allocates level d as the
     // node range [levels[d], levels[d + 1])).
-    uint32_t top = bvh_.levels.size() > 2 ? bvh_.levels[2] : bvh_.numNodes;
-    top          = std::min(top, kTopNodes);
-    return BvhView{bvh_.nodes.as<const uint4>(), bvh_.tris.as<const float4>(), nullptr,
-                   std::min<uint32_t>(bvh_.depth + 1u, uint32_t(kStackDepth)), top};
+    v.topNodes = std::min(bvh_.levels.size() > 2 ? bvh_.levels[2] : bvh_.numNodes, kTopNodes);
+    return v;
 }
 
 ClassifyView Integrator::classifyView() const
