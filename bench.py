@@ -96,8 +96,9 @@ def run_profile(args):
     for _ in range(args.profile):
         it.render(1)
         st = it.stats()
-        print(json.dumps({k: st[k] for k in ("ms_last_render", "ms_trace", "ms_shade", "ms_shadow", "waves",
-                                             "last_rays_closest", "last_rays_shadow")}))
+        print(json.dumps({**{k: st[k] for k in ("ms_last_render", "ms_trace", "ms_shade", "ms_shadow", "waves",
+                                                "last_rays_closest", "last_rays_shadow")},
+                          "wave_rays_closest": it.waveRays()}))
     it.close()
     return 0
 

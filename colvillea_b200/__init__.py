@@ -232,6 +232,13 @@ class Integrator:
         N.call("cl_get_dome_tables", self._h, _ptr(pU), _ptr(cU), _ptr(pV), _ptr(cV))
         return pU, cU, pV, cV
 
+    def waveRays(self):
+        """CL_PROFILE_STAGES: closest-hit rays of each wave of the last render."""
+        buf = np.zeros(256, np.uint64)
+        n = ctypes.c_uint32()
+        N.call("cl_get_wave_rays", self._h, _ptr(buf), len(buf), ctypes.byref(n))
+        return [int(x) for x in buf[:min(n.value, len(buf))]]
+
     def domeAliasTables(self, w, h):
         row = np.zeros(2 * h, np.uint32); col = np.zeros(2 * w * h, np.uint32)
         N.call("cl_get_dome_alias_tables", self._h, _ptr(row), _ptr(col))

@@ -138,6 +138,7 @@ _SIGS = {
     "cl_trace_stats": [vp, vp, u32, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)],
     "cl_get_dome_tables": [vp, vp, vp, vp, vp],
     "cl_get_dome_alias_tables": [vp, vp, vp],
+    "cl_get_wave_rays": [vp, vp, u32, ctypes.POINTER(ctypes.c_uint32)],
     "cl_integrator_guide_probe": [vp, u32, vp, ctypes.POINTER(ctypes.c_uint32)],
     "cl_dome_alias_sample": [vp, vp, vp, vp, vp, u32],
     "cl_unit_bsdf_eval": [u32, vp, vp, vp, vp, u32],

@@ -314,6 +314,12 @@ cl_status cl_get_dome_tables(cl_integrator* it, float* pU, float* cU, float* pV,
     return guarded([&](std::string* e) { return it->impl.domeTables(pU, cU, pV, cV, e); });
 }
 
+cl_status cl_get_wave_rays(cl_integrator* it, uint64_t* rays, uint32_t capacity, uint32_t* count)
+{
+    CL_NEED(it);
+    return guarded([&](std::string* e) { return it->impl.waveRays(rays, capacity, count, e); });
+}
+
 cl_status cl_integrator_guide_probe(cl_integrator* it, uint32_t capacity, float* rows, uint32_t* count)
 {
     CL_NEED(it);

@@ -2232,6 +2232,7 @@ cl_status Integrator::render(uint32_t spp, std::string* err)
     CL_TRY(ensureQueues(err));
     msRender_ = msTrace_ = msShade_ = msShadow_ = msInfer_ = 0.0f;
     waves_ = 0;
+    waveRays_.clear();
     lastRaysC_ = lastRaysS_ = lastNodes_ = lastTris_ = lastNodesS_ = lastTrisS_ = 0;
     if (guide_) CL_TRY(ensureGuideBuffers(err));
     if (cache_) CL_TRY(ensureCacheBuffers(err));
@@ -2321,7 +2322,8 @@ cl_status Integrator::beginPass(uint32_t spp, bool record, bool cacheTrain, uint
     c0.pathNext    = init;
     CL_CUDA(cudaMemcpyAsync(ctr_.p, &c0, sizeof(Counters), cudaMemcpyHostToDevice, stream_), err);
     CL_CUDA(cudaStreamSynchronize(stream_), err); // hostWp_/c0 reused next call
-    *initSlots = init;
+    waveRaysSeen_ = 0ull;
+    *initSlots    = init;
     return CL_OK;
 }
 
@@ -2355,7 +2357,11 @@ cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std
             for (int w = 0; w < 4; ++w)
             {
                 CL_TRY(launchWave(w & 1, true, err));
+                unsigned long long rc = 0ull;
+                CL_CUDA(cudaMemcpyAsync(&rc, &dc->raysClosest, 8, cudaMemcpyDeviceToHost, stream_), err);
                 CL_CUDA(cudaStreamSynchronize(stream_), err);
+                waveRays_.push_back(rc - waveRaysSeen_);
+                waveRaysSeen_ = rc;
                 float a = 0, b = 0, c = 0, d = 0;
                 CL_CUDA(cudaEventElapsedTime(&a, evS_[0], evS_[1]), err);
                 CL_CUDA(cudaEventElapsedTime(&d, evS_[1], evS_[4]), err);
@@ -2960,6 +2966,19 @@ cl_status Integrator::guideProbe(uint32_t cap, float* rows, uint32_t* count, std
     n      = std::min(n, cap);
     *count = n;
     if (n) CL_CUDA(cudaMemcpy(rows, probe.p, size_t(n) * kProbeF * 4, cudaMemcpyDeviceToHost), err);
+    return CL_OK;
+}
+
+cl_status Integrator::waveRays(uint64_t* out, uint32_t cap, uint32_t* count, std::string* err) const
+{
+    if (!count || (!out && cap))
+    {
+        *err = "null argument";
+        return CL_ERR_INVALID_ARG;
+    }
+    const uint32_t n = uint32_t(std::min<size_t>(cap, waveRays_.size()));
+    for (uint32_t i = 0; i < n; ++i) out[i] = waveRays_[i];
+    *count = uint32_t(waveRays_.size());
     return CL_OK;
 }
 

@@ -177,6 +177,7 @@ public:
     cl_status traceStats(const float* rays, uint32_t n, uint64_t* nodes, uint64_t* tris, std::string* err);
     cl_status domeTables(float* pU, float* cU, float* pV, float* cV, std::string* err);
     cl_status domeAliasTables(uint32_t* aliasRow, uint32_t* aliasCol, std::string* err);
+    cl_status waveRays(uint64_t* out, uint32_t cap, uint32_t* count, std::string* err) const;
     cl_status guideProbe(uint32_t cap, float* rows, uint32_t* count, std::string* err);
     cl_status beginPass(uint32_t spp, bool record, bool cacheTrain, uint32_t* initSlots, std::string* err);
     cl_status domeAliasSample(const float* u2, float* dir, float* pdf, float* val, uint32_t n, std::string* err);
@@ -284,6 +285,8 @@ private:
     uint64_t  lastNodes_ = 0, lastTris_ = 0, lastNodesS_ = 0, lastTrisS_ = 0, lastRaysC_ = 0, lastRaysS_ = 0;
     float     msBvh_ = 0, msDome_ = 0, msRender_ = 0, msTrace_ = 0, msShade_ = 0, msShadow_ = 0;
     float     msBvhWall_ = 0, msBvhAlloc_ = 0; // last full build: host wall time, and its cudaMalloc share
+    std::vector<uint64_t> waveRays_;       // CL_PROFILE_STAGES: closest-hit rays of each wave of the last render
+    unsigned long long    waveRaysSeen_ = 0;
     cudaEvent_t evA_ = nullptr, evB_ = nullptr, evS_[6] = {};
 
     // Guiding.

@@ -319,6 +319,11 @@ cl_status cl_reset_iteration(cl_integrator* integrator);
  * the same scene.  No counterpart in the reference. */
 cl_status cl_set_iteration(cl_integrator* integrator, uint32_t iteration);
 cl_status cl_get_stats(cl_integrator* integrator, cl_stats* stats);
+/* Profiling (CL_PROFILE_STAGES; no counterpart in the reference): the
+ * closest-hit rays traced by each wave of the last render, in launch order
+ * (the units of each closest-hit kernel launch).  Writes up to `capacity`
+ * counts; *count = the number of waves. */
+cl_status cl_get_wave_rays(cl_integrator* integrator, uint64_t* rays, uint32_t capacity, uint32_t* count);
 /* Last error message of the calling thread. */
 cl_status cl_last_error(char* buffer, size_t size);
 

@@ -194,29 +194,42 @@ def test_cfg5_reduced_same_seed_image(cfg5r):
 
 
 # --- two-level instancing (CL_TWO_LEVEL) ---------------------------------------
-# The oracle traces the flattened world-space triangles; the GPU maps rays
-# into each instance's object space.  The transform changes the rounding of
-# the watertight test, so t agrees to a few FP32 ulps rather than exactly,
-# and near-ties (a ray through a shared edge or two surfaces within that
-# tolerance) may resolve to the other triangle.
-T_REL = 2e-5
+# The oracle traces the flattened world-space triangles (vertices mapped in
+# FP64, rounded to FP32); the GPU maps rays into each instance's object space.
+# The two see the same triangle through different roundings: a vertex moves
+# by up to about DP (absolute, scene units) between them, which moves the hit
+# along the ray by DP / |cos| (cos: ray direction against the triangle's
+# normal), so grazing hits differ the most.  Near-ties (a ray through a shared
+# edge, or two surfaces within that bound) may resolve to the other triangle.
+DP, T_REL = 1e-4, 2e-5
 
 
-def check_hits_two_level(it, os_, rays, label):
+def hit_cosines(flat, prim, d):
+    idx = flat.idx[prim]
+    p0, p1, p2 = flat.pos[idx[:, 0]].astype(np.float64), flat.pos[idx[:, 1]], flat.pos[idx[:, 2]]
+    n = np.cross(p1 - p0, p2 - p0)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+    return np.abs(np.sum(n * d, axis=1))
+
+
+def check_hits_two_level(it, os_, rays, label, flat):
     t, i, b1, b2 = it.traceRays(rays)
     to, io, _, _ = os_.trace(rays, threads=THREADS)
     hit_g, hit_o = i != NO_HIT, io != NO_HIT
     same = i == io
-    scale = np.maximum(np.abs(to), 1.0)
-    near = np.abs(t - to) <= T_REL * scale
-    bad = ~same & ~(hit_g & hit_o & near)
-    dt = np.abs(t[same & hit_g] - to[same & hit_g]) / scale[same & hit_g]
+    eq = same & hit_g
+    cos = np.ones(len(rays))
+    cos[eq] = hit_cosines(flat, io[eq], rays[eq, 4:7].astype(np.float64))
+    tol = DP / np.maximum(cos, 1e-6) + T_REL * np.maximum(np.abs(to), 1.0)
+    near = np.abs(t - to) <= tol
+    bad = ~same & ~(hit_g & hit_o & (np.abs(t - to) <= DP / 1e-3 + T_REL * np.abs(to)))
+    dtc = (np.abs(t - to) * cos)[eq]
     print(f"[scale] {label}: {len(rays)} rays, hit fraction {hit_g.mean():.3f}, id differences {int((~same).sum())} "
-          f"(near-ties {int((~same & hit_g & hit_o & near).sum())}, other {int(bad.sum())}); max rel |dt| on equal ids "
-          f"{dt.max() if len(dt) else 0:.2e}")
+          f"(near-ties {int((~same & hit_g & hit_o).sum()) - int(bad.sum())}, other {int(bad.sum())}); on equal ids "
+          f"max |dt| {np.abs(t - to)[eq].max() if eq.any() else 0:.2e}, max |dt| cos {dtc.max() if eq.any() else 0:.2e}")
     assert int(bad.sum()) == 0
     assert (~same).mean() < 1e-3
-    assert (dt <= T_REL).all()
+    assert near[eq].all()
 
 
 def test_cfg5_reduced_two_level_hits(native, oracle, cfg5r):
@@ -232,7 +245,7 @@ def test_cfg5_reduced_two_level_hits(native, oracle, cfg5r):
     rng = np.random.default_rng(13)
     cam = camera_rays(s, rng, 1 << 15)
     rays = np.concatenate([cam, surface_rays(o, cam[:1 << 14], rng), world_rays(s, rng, 1 << 14)])[:1 << 16]
-    check_hits_two_level(it, o, rays, "cfg5-reduced two-level")
+    check_hits_two_level(it, o, rays, "cfg5-reduced two-level", s.flatten())
     occ_g = it.occludedRays(rays)
     occ_o = o.occluded(rays, threads=THREADS)
     assert np.mean(occ_g != occ_o) < 1e-3
@@ -259,9 +272,10 @@ def test_two_level_vertex_edit(native, oracle):
         it.updateVertices(m, p, bvh=mode)
         s.meshes[m] = scenes.Mesh(p.astype(np.float32), s.meshes[m].normals, s.meshes[m].tangents, s.meshes[m].uvs,
                                   s.meshes[m].indices)
-        o = oracle.OracleScene(s.flatten())
+        flat = s.flatten()
+        o = oracle.OracleScene(flat)
         rays = np.concatenate([world_rays(s, rng, 1 << 14), camera_rays(s, rng, 1 << 14)])
-        check_hits_two_level(it, o, rays, f"two-level edit ({mode})")
+        check_hits_two_level(it, o, rays, f"two-level edit ({mode})", flat)
     it.close()
 
 
