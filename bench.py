@@ -46,8 +46,8 @@ def parse():
     ap.add_argument("--profile", type=int, default=0, metavar="SPP",
                     help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
-    ap.add_argument("--flatten", action="store_true",
-                    help="config 5: flatten the instances into one world-space tree instead of the two-level scene")
+    ap.add_argument("--two-level", action="store_true",
+                    help="two-level scene (one tree per mesh, one over the instances) instead of flattened instances")
     ap.add_argument("--no-relmse", action="store_true", help="skip the guided-vs-plain equal-time relMSE")
     ap.add_argument("--no-edit", action="store_true", help="skip the shape-edit (refit vs rebuild) measurement")
     ap.add_argument("--extended", action="store_true",
@@ -299,6 +299,15 @@ def guided_relmse(args):
         **{k: rnd(v) for k, v in r.items()},
         "mlp": {**{k: rnd(v) for k, v in mlp.items()}, "bf16_peak_tflops": peak,
                 "infer_frac_of_peak": round(mlp["infer_tflops"] / peak, 4) if peak and mlp["infer_tflops"] else None}}
+    # The best equal-time guiding configuration of the equal-spp study on this scene (bench.py --guide-study):
+    # the network guides the rough-dielectric vertices only, sampled with probability 0.2.
+    tuned = cb.GuideConfig(class_mask=4, bsdf_fraction=0.8)
+    rt = evaluate.equal_time(s3, ref3, args.relmse_spp, seeds=args.relmse_seeds, guide=tuned)
+    out["cfg3_guided_tuned"] = {
+        "workload": f"cfg3 as above; guided classes mask {tuned.class_mask} (rough dielectric), BSDF fraction "
+                    f"{tuned.bsdf_fraction:g}, {tuned.train_spp} Adam steps; plain at the same device time",
+        "reference": out["cfg3_guided"]["reference"],
+        **{k: rnd(v) for k, v in rt.items()}}
     s4 = scenes.config4(0)
     t0 = time.perf_counter()
     ref4 = evaluate.reference(s4, args.relmse_ref_spp4)
@@ -478,10 +487,11 @@ def main():
         cbuild.build()
     s = scenes.CONFIGS[args.config](0)
     W, H = s.width, s.height
-    # Config 5's repeated, transformed meshes use the two-level scene (one tree
-    # per mesh, one over the instances) unless --flatten asks for one
-    # world-space tree over the flattened instances.
-    two = args.config == 5 and not args.flatten
+    # --two-level: config 5's repeated, transformed meshes as a two-level scene
+    # (one tree per mesh, one over the instances) instead of one world-space
+    # tree over the flattened instances (the default: faster to trace and to
+    # build, 60% more scene memory on config 5).
+    two = args.two_level
     flags = cb.COMPAT_ALL | cb.DOME_ALIAS | (cb.TWO_LEVEL if two else 0)
     # The timed integrator runs the product path (waves replayed from a CUDA
     # graph); a second one with per-stage CUDA events (each wave launched and
