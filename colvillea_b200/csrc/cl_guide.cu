@@ -151,6 +151,9 @@ struct TrainArgs
     double*        scal;     // [0] sum of weights, [1] loss, [3] sum of clamped weights
     int            learnSel; // guide: learned selection probability
     float          clamp;    // weight clamp (x batch mean), 0 = off
+    uint4*         enc;      // encoded inputs: per 128-sample tile, 24,576 B in the tensor-core tile layout
+    float4*        aux;      // per sample: {p.xyz (clamped to the unit cube), training weight / sum}, then the
+                             // record's 4th float4 (guide: omega, BSDF pdf; cache: target RGB)
 };
 
 // Training weight of a record: clamped to clamp x the batch mean when set.
@@ -333,14 +336,14 @@ template <class S> struct TrainTc
 {
     static constexpr int L  = S::kLayers - 1; // the output layer
     static constexpr int kW = S::kParams * 2; // canonical bf16 weights (cl_mlp_tc.cuh)
-    // Input tile of layer l (128 rows, canonical K-major, 2048 B per 8-column chunk).
-    __host__ __device__ static constexpr int act(int l)
-    {
-        return kW + (l == 0 ? 0 : kTcRows * kIn * 2 + (l - 1) * kTcRows * kWidth * 2);
-    }
+    static constexpr int kA0 = kTcRows * kIn * 2;  // an encoded-input tile (24,576 B)
+    // Input tile of layer l (128 rows, canonical K-major, 2048 B per 8-column chunk); layer 0's input is one of
+    // two encoded-tile buffers (a0(b)): the next tile's bulk copy fills the other one.
+    __host__ __device__ static constexpr int a0(int b) { return kW + b * kA0; }
+    __host__ __device__ static constexpr int act(int l) { return kW + 2 * kA0 + (l - 1) * kTcRows * kWidth * 2; }
     static constexpr int kDelta = act(S::kLayers); // output-gradient tile, 64 columns (zero-padded)
-    static constexpr int kBar   = kDelta + kTcRows * kWidth * 2;
-    static constexpr int kSmem  = kBar + 16;
+    static constexpr int kBar   = kDelta + kTcRows * kWidth * 2; // MMA mbarrier, TMEM address, 2 load mbarriers
+    static constexpr int kSmem  = kBar + 32;
     // TMEM: columns [0, 64) the layer accumulator; then dW_l (M = 64) at dw(l).
     __host__ __device__ static constexpr uint32_t dw(int l) { return 64u + (l == 0 ? 0u : uint32_t(kIn + (l - 1) * kWidth)); }
     static constexpr uint32_t kCols = 512;
@@ -365,6 +368,50 @@ __device__ __forceinline__ bool tcWaitAll(uint32_t bar, uint32_t& phase)
     return __syncthreads_and(ok) != 0;
 }
 
+// Encoding of the training batch, one thread per sample (many warps hide the
+// hash-grid gathers): the 96 encoded inputs go to tile j / 128 in the
+// tensor-core tile layout (chunk c of row r at c * 2048 + r * 16, so that a
+// tile is one contiguous 24,576-byte block for the training kernel's bulk
+// copy), with the sample's clamped position, normalised training weight and
+// loss inputs beside it.  Rows past the batch in the last tile are zero.
+__global__ void __launch_bounds__(256, 4) kTrainEncode(TrainArgs a)
+{
+    const uint32_t count = *a.count, nB = min(count, a.batch);
+    const uint32_t rows  = (nB + kTcRows - 1) / kTcRows * kTcRows;
+    const double   wsum  = a.clamp > 0.0f ? a.scal[3] : a.scal[0];
+    const float    invW  = wsum > 0.0 ? float(1.0 / wsum) : 0.0f;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < rows; j += gridDim.x * blockDim.x)
+    {
+        uint32_t r[kIn / 2];
+        float4   pw{0.0f, 0.0f, 0.0f, 0.0f}, r3{0.0f, 0.0f, 0.0f, 0.0f};
+        if (j < nB)
+        {
+            const float4* R  = a.rec + kRecordF4 * size_t(recordOf(j, count, nB));
+            const float4  r0 = R[0], r1 = R[1], r2 = R[2];
+            r3               = R[3];
+            const f3 p       = clampUnit(f3{r0.x, r0.y, r0.z});
+            pw               = make_float4(p.x, p.y, p.z, trainWeight(r0.w, a, nB) * invW);
+#pragma unroll
+            for (int l = 0; l < kLevels; ++l)
+            {
+                const float2 f = encodeLevel(a.g, l, p);
+                r[l]           = packBf16(f.x, f.y);
+            }
+            oneBlobPacked(f3{r1.x, r1.y, r1.z}, r + kHashF / 2);
+            oneBlobPacked(f3{r2.x, r2.y, r2.z}, r + (kHashF + 2 * kBlob) / 2);
+        }
+        else
+#pragma unroll
+            for (int q = 0; q < kIn / 2; ++q) r[q] = 0u;
+        uint4* tile = a.enc + size_t(j / kTcRows) * (kTcRows * kIn / 8);
+#pragma unroll
+        for (int c = 0; c < kIn / 8; ++c)
+            tile[c * kTcRows + (j % kTcRows)] = make_uint4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+        a.aux[2 * size_t(j)]     = pw;
+        a.aux[2 * size_t(j) + 1] = r3;
+    }
+}
+
 // Two threads per sample row (256 per CTA): thread t serves row t % 128;
 // half h = t / 128 encodes hash levels 8h .. 8h+7 and one of the two one-blob
 // directions, converts columns 32h .. 32h+31 of each layer's accumulator
@@ -386,7 +433,13 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTrainThreads, 
         for (int i = int(t); i < T::kW / 16; i += kTrainThreads) w[i] = __ldg(a.wt + i);
     }
     const uint32_t bar = smemAddr(smem + T::kBar);
-    if (t == 0) mbarInit(bar, 1u);
+    const uint32_t lbar[2] = {bar + 16u, bar + 24u}; // encoded-tile bulk copies into a0(0), a0(1)
+    if (t == 0)
+    {
+        mbarInit(bar, 1u);
+        mbarInit(lbar[0], 1u);
+        mbarInit(lbar[1], 1u);
+    }
     if (warp == 0) tmemAlloc(bar + 8u, T::kCols);
     tcFenceBefore();
     __syncthreads();
@@ -394,50 +447,37 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTrainThreads, 
     const uint32_t tmem  = *reinterpret_cast<volatile uint32_t*>(smem + T::kBar + 8);
     const uint32_t tRow  = tmem + (((warp & 3u) * 32u) << 16); // this warp's TMEM lanes
     const uint32_t wS    = smemAddr(smem), dS = smemAddr(smem + T::kDelta);
-    const double   wsum  = a.clamp > 0.0f ? a.scal[3] : a.scal[0];
-    const float    invW  = wsum > 0.0 ? float(1.0 / wsum) : 0.0f;
-    uint32_t       phase = 0u;
+    constexpr uint32_t kTileU4 = kTcRows * kIn / 8;
+    if (t == 0) bulkLoad(smemAddr(smem + T::a0(0)), a.enc + size_t(blockIdx.x) * kTileU4, T::kA0, lbar[0]);
+    uint32_t       phase = 0u, lphase[2] = {0u, 0u};
+    int            pending = 1; // 1 + the buffer whose bulk copy was issued and not yet waited for (0: none)
     bool           first = true, ok = true;
     float          lossPart = 0.0f;
-    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x)
+    uint32_t       it = 0u;
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++it)
     {
+        const uint32_t b     = it & 1u;
         const uint32_t j     = tile * kTcRows + row;
         const bool     valid = j < nB;
-        // Encoding -> a_0 row `row`: this half's 8 hash levels and one direction.
-        f3       p{0.0f, 0.0f, 0.0f};
-        float4   r3{0.0f, 0.0f, 0.0f, 0.0f};
-        float    sw = 0.0f;
-        uint32_t hs[4 * 2], bl[kBlob];
-        if (valid)
+        const float4   pw    = a.aux[2 * size_t(j)];
+        const float4   r3    = half == 0u ? a.aux[2 * size_t(j) + 1] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const f3       p{pw.x, pw.y, pw.z};
+        const float    sw = pw.w;
+        // This tile's encoded inputs (bulk copy issued one tile ahead), then the next tile's copy into
+        // the other buffer, whose last readers (this CTA's previous MMAs) have completed.
+        if (!__syncthreads_and(mbarWait(lbar[b], lphase[b])))
         {
-            const float4* R  = a.rec + kRecordF4 * size_t(recordOf(j, count, nB));
-            const float4  r0 = R[0], rd = R[1 + half];
-            r3               = R[3];
-            p                = clampUnit(f3{r0.x, r0.y, r0.z});
-            sw               = trainWeight(r0.w, a, nB) * invW;
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-            {
-                const float2 f = encodeLevel(a.g, int(8 * half) + q, p);
-                hs[q]          = packBf16(f.x, f.y);
-            }
-            oneBlobPacked(f3{rd.x, rd.y, rd.z}, bl);
+            ok = false; // the copy may still land: `pending` keeps its buffer for the final wait
+            break;
         }
-        else
+        lphase[b] ^= 1u;
+        pending = 0;
+        if (tile + gridDim.x < tiles)
         {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) hs[q] = 0u;
-#pragma unroll
-            for (int q = 0; q < kBlob; ++q) bl[q] = 0u;
-        }
-        {
-            unsigned char* a0 = smem + T::act(0);
-            *tileChunk(a0, row, int(2 * half))     = make_uint4(hs[0], hs[1], hs[2], hs[3]);
-            *tileChunk(a0, row, int(2 * half) + 1) = make_uint4(hs[4], hs[5], hs[6], hs[7]);
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                *tileChunk(a0, row, kHashF / 8 + int(4 * half) + c) =
-                    make_uint4(bl[4 * c], bl[4 * c + 1], bl[4 * c + 2], bl[4 * c + 3]);
+            if (t == 0)
+                bulkLoad(smemAddr(smem + T::a0(b ^ 1u)), a.enc + size_t(tile + gridDim.x) * kTileU4, T::kA0,
+                         lbar[b ^ 1u]);
+            pending = int(b ^ 1u) + 1;
         }
         // Forward.
         float o[S::kOut];
@@ -449,7 +489,8 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTrainThreads, 
             {
                 tcFenceAfter();
                 const int      K = S::in(l), N = S::out(l);
-                const uint32_t aS = smemAddr(smem + T::act(l)), wl = wS + 2u * uint32_t(S::woff(l));
+                const uint32_t aS = smemAddr(smem + (l == 0 ? T::a0(int(b)) : T::act(l)));
+                const uint32_t wl = wS + 2u * uint32_t(S::woff(l));
                 for (int ks = 0; ks < K / 16; ++ks)
                     tcMma(tmem, tcDesc(aS + uint32_t(ks) * 2u * kTcChunk, kTcChunk, 128u),
                           tcDesc(wl + uint32_t(ks * 2 * N * 16), uint32_t(N * 16), 128u), tcIdescMaj(128, N, false, false),
@@ -518,7 +559,8 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTrainThreads, 
             {
                 tcFenceAfter();
                 const int      K = S::out(l), I = S::in(l), N = l > 0 ? I : kHashF;
-                const uint32_t aS = smemAddr(smem + T::act(l)), wl = wS + 2u * uint32_t(S::woff(l));
+                const uint32_t aS = smemAddr(smem + (l == 0 ? T::a0(int(b)) : T::act(l)));
+                const uint32_t wl = wS + 2u * uint32_t(S::woff(l));
                 // dW_l += delta^T a_l: A = delta (M = 64 output units, MN-major), B = a_l (N = I inputs,
                 // MN-major), K = 16 samples per instruction.
                 for (int ks = 0; ks < kTcRows / 16; ++ks)
@@ -589,6 +631,9 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTrainThreads, 
         }
         first = false;
     }
+    // A bulk copy issued for a tile this CTA no longer processes (a wait ran out) must land before the
+    // CTA's shared memory is released: wait for it, again with a bound.
+    if (pending) mbarWait(lbar[pending - 1], lphase[pending - 1]);
     for (int off = 16; off > 0; off >>= 1) lossPart += __shfl_xor_sync(0xffffffffu, lossPart, off);
     if (lane == 0 && lossPart != 0.0f) atomicAdd(&a.scal[1], double(lossPart));
     if (!ok)
@@ -772,6 +817,11 @@ template <class S, class L> cl_status HashNet<S, L>::init(cudaStream_t st, std::
     CL_TRY(table_.alloc(hashParams_ * 2, err));
     CL_TRY(wt_.alloc(TcLayout<S>::kWBytes, err));
     CL_TRY(scal_.alloc(64, err));
+    {
+        const size_t tiles = (size_t(cfg_.batch) + kTcRows - 1) / kTcRows;
+        CL_TRY(enc_.alloc(tiles * TrainTc<S>::kA0, err));
+        CL_TRY(aux_.alloc(tiles * kTcRows * 32, err));
+    }
     kInitParams<S><<<gridFor(n, 256, numSMs_ * 8), 256, 0, st_>>>(params_.f(), hashParams_, cfg_.seed);
     CL_CUDA(cudaGetLastError(), err);
     CL_CUDA(cudaMemsetAsync(grad_.p, 0, n * 4, st_), err);
@@ -966,6 +1016,8 @@ cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* coun
     a.gradTable = reinterpret_cast<float2*>(grad_.f());
     a.gradMlp   = grad_.f() + hashParams_;
     a.err       = trainErr();
+    a.enc       = enc_.as<uint4>();
+    a.aux       = aux_.as<float4>();
     a.scal      = scal_.as<double>();
     a.learnSel  = cfg_.learn_selection ? 1 : 0;
     a.clamp     = cfg_.weight_clamp;
@@ -977,6 +1029,8 @@ cl_status HashNet<S, L>::computeGradient(const float4* rec, const uint32_t* coun
         CL_CUDA(cudaGetLastError(), err);
     }
     const uint32_t tiles = (cfg_.batch + kTcRows - 1) / kTcRows;
+    kTrainEncode<<<gridFor(size_t(tiles) * kTcRows, 256, numSMs_ * 8), 256, 0, st_>>>(a);
+    CL_CUDA(cudaGetLastError(), err);
     kTrainTc<S, L><<<std::min<uint32_t>(tiles, uint32_t(numSMs_)), kTrainThreads, TrainTc<S>::kSmem, st_>>>(a);
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;

@@ -73,6 +73,7 @@ private:
     DevBuf scal_;                  // {sum w, loss, count (u32), sum of clamped w}; byte 48: inference error
                                    // flags; byte 52: training error flags
     DevBuf rec_, io_, io2_;        // host-entry staging
+    DevBuf enc_, aux_;             // training: encoded batch in tensor-core tiles, per-sample loss inputs
 };
 
 using GuideNet = HashNet<guide::GuideShape, GuideLoss>;

@@ -141,6 +141,18 @@ __device__ __forceinline__ bool mbarWait(uint32_t bar, uint32_t parity)
     return true;
 }
 
+// One-dimensional bulk copy (TMA, no multicast) of `bytes` (a multiple of
+// 16; both addresses 16-byte aligned) from this GPU's global memory into this
+// CTA's shared memory, completing on the mbarrier `bar` (which the issuing
+// thread arms with the byte count).
+__device__ __forceinline__ void bulkLoad(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
 // Per-CTA setup: weights (canonical layout, global) -> shared memory, the
 // mbarrier, and kTcCols TMEM columns (warp 0).  Returns the TMEM address.
 template <class S>
