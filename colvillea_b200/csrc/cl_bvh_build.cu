@@ -777,33 +777,37 @@ __global__ void kValidateTris(const float4* __restrict__ tris, uint32_t n, uint3
 
 } // namespace
 
-cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err)
+cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err,
+                       BuildArena* arena)
 {
     out->release();
+    BuildArena  localArena;
+    BuildArena& mem = arena ? *arena : localArena;
+    mem.reset();
     if (n == 0)
     {
         *err = "cannot build a BVH over zero triangles";
         return CL_ERR_INVALID_ARG;
     }
-    DevBuf lo, hi, keys, keys2, ids, ids2, left, right, parent, nlo, nhi, count, arrive, bounds, tmp, tasksA, tasksB,
+    ScratchBuf lo, hi, keys, keys2, ids, ids2, left, right, parent, nlo, nhi, count, arrive, bounds, tmp, tasksA, tasksB,
         ctr;
     size_t nn = n;
-    CL_TRY(lo.alloc(nn * 3 * 4, err));
-    CL_TRY(hi.alloc(nn * 3 * 4, err));
-    CL_TRY(keys.alloc(nn * 8, err));
-    CL_TRY(keys2.alloc(nn * 8, err));
-    CL_TRY(ids.alloc(nn * 4, err));
-    CL_TRY(ids2.alloc(nn * 4, err));
+    CL_TRY(mem.take(lo, nn * 3 * 4, err));
+    CL_TRY(mem.take(hi, nn * 3 * 4, err));
+    CL_TRY(mem.take(keys, nn * 8, err));
+    CL_TRY(mem.take(keys2, nn * 8, err));
+    CL_TRY(mem.take(ids, nn * 4, err));
+    CL_TRY(mem.take(ids2, nn * 4, err));
     size_t ni = nn > 1 ? nn - 1 : 1;
-    CL_TRY(left.alloc(ni * 4, err));
-    CL_TRY(right.alloc(ni * 4, err));
-    CL_TRY(parent.alloc((2 * nn) * 4, err));
-    CL_TRY(nlo.alloc(ni * 3 * 4, err));
-    CL_TRY(nhi.alloc(ni * 3 * 4, err));
-    CL_TRY(count.alloc(ni * 4, err));
-    CL_TRY(arrive.alloc(ni * 4, err));
-    CL_TRY(bounds.alloc(sizeof(Bounds), err));
-    CL_TRY(ctr.alloc(16, err));
+    CL_TRY(mem.take(left, ni * 4, err));
+    CL_TRY(mem.take(right, ni * 4, err));
+    CL_TRY(mem.take(parent, (2 * nn) * 4, err));
+    CL_TRY(mem.take(nlo, ni * 3 * 4, err));
+    CL_TRY(mem.take(nhi, ni * 3 * 4, err));
+    CL_TRY(mem.take(count, ni * 4, err));
+    CL_TRY(mem.take(arrive, ni * 4, err));
+    CL_TRY(mem.take(bounds, sizeof(Bounds), err));
+    CL_TRY(mem.take(ctr, 16, err));
 
     Bounds b0;
     for (int a = 0; a < 3; ++a)
@@ -821,7 +825,7 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     CL_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpBytes, (uint64_t*)keys.p, (uint64_t*)keys2.p, ids.u(), ids2.u(),
                                             int(n), 0, 63, st),
             err);
-    CL_TRY(tmp.alloc(tmpBytes, err));
+    CL_TRY(mem.take(tmp, tmpBytes, err));
     CL_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmpBytes, (uint64_t*)keys.p, (uint64_t*)keys2.p, ids.u(), ids2.u(),
                                             int(n), 0, 63, st),
             err);
@@ -833,19 +837,19 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     uint32_t rootRef = kLeafFlag; // a single triangle: the root is a leaf
     if (n > 1)
     {
-        DevBuf C, C2, blo, bhi, blo2, bhi2, nnb, valid, pos, scanTmp;
-        CL_TRY(C.alloc(nn * 4, err));
-        CL_TRY(C2.alloc(nn * 4, err));
-        CL_TRY(blo.alloc(nn * 16, err));
-        CL_TRY(bhi.alloc(nn * 16, err));
-        CL_TRY(blo2.alloc(nn * 16, err));
-        CL_TRY(bhi2.alloc(nn * 16, err));
-        CL_TRY(nnb.alloc(nn * 4, err));
-        CL_TRY(valid.alloc(nn * 4, err));
-        CL_TRY(pos.alloc(nn * 4, err));
+        ScratchBuf C, C2, blo, bhi, blo2, bhi2, nnb, valid, pos, scanTmp;
+        CL_TRY(mem.take(C, nn * 4, err));
+        CL_TRY(mem.take(C2, nn * 4, err));
+        CL_TRY(mem.take(blo, nn * 16, err));
+        CL_TRY(mem.take(bhi, nn * 16, err));
+        CL_TRY(mem.take(blo2, nn * 16, err));
+        CL_TRY(mem.take(bhi2, nn * 16, err));
+        CL_TRY(mem.take(nnb, nn * 4, err));
+        CL_TRY(mem.take(valid, nn * 4, err));
+        CL_TRY(mem.take(pos, nn * 4, err));
         size_t scanBytes = 0;
         CL_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scanBytes, valid.u(), pos.u(), int(n), st), err);
-        CL_TRY(scanTmp.alloc(scanBytes, err));
+        CL_TRY(mem.take(scanTmp, scanBytes, err));
         CL_CUDA(cudaMemsetAsync(ctr.p, 0, 16, st), err);
         PlocTree T{left.u(), right.u(), nlo.f(), nhi.f(), count.u(), ctr.u()};
         kPlocInit<<<blocks, 256, 0, st>>>(n, ids2.u(), lo.f(), hi.f(), C.u(), blo.as<float4>(), bhi.as<float4>());
@@ -853,8 +857,8 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
         // and the next's); the host reads it every kPlocCheck iterations to
         // size the launches and to stop.
         constexpr int kPlocCheck = 6;
-        DevBuf        mbuf;
-        CL_TRY(mbuf.alloc(8, err));
+        ScratchBuf    mbuf;
+        CL_TRY(mem.take(mbuf, 8, err));
         CL_CUDA(cudaMemcpyAsync(mbuf.p, &n, 4, cudaMemcpyHostToDevice, st), err);
         uint32_t m = n, iters = 0;
         int      cur = 0;
@@ -922,8 +926,8 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     CL_TRY(out->nodes.alloc(size_t(maxNodes) * 80, err));
     CL_TRY(out->tris.alloc(nn * 48, err));
     size_t taskCap = nn / 2 + 8;
-    CL_TRY(tasksA.alloc(taskCap * 8, err));
-    CL_TRY(tasksB.alloc(taskCap * 8, err));
+    CL_TRY(mem.take(tasksA, taskCap * 8, err));
+    CL_TRY(mem.take(tasksB, taskCap * 8, err));
     // ctr: [0] node counter, [1] tri counter, [2] next task count, [3] error
     uint32_t c0[4] = {1u, 0u, 0u, 0u};
     CL_CUDA(cudaMemcpyAsync(ctr.p, c0, 16, cudaMemcpyHostToDevice, st), err);
@@ -931,12 +935,12 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     CL_CUDA(cudaMemcpyAsync(tasksA.p, &root, 8, cudaMemcpyHostToDevice, st), err);
 
     // Slot costs of the optimal collapse, bottom up over the binary tree.
-    DevBuf dpCost, dpParent, dpLeafParent;
+    ScratchBuf dpCost, dpParent, dpLeafParent;
     if (n > 1)
     {
-        CL_TRY(dpCost.alloc(ni * 8 * 4, err));
-        CL_TRY(dpParent.alloc(ni * 4, err));
-        CL_TRY(dpLeafParent.alloc(nn * 4, err));
+        CL_TRY(mem.take(dpCost, ni * 8 * 4, err));
+        CL_TRY(mem.take(dpParent, ni * 4, err));
+        CL_TRY(mem.take(dpLeafParent, nn * 4, err));
         CL_CUDA(cudaMemsetAsync(dpParent.p, 0xff, ni * 4, st), err);
         CL_CUDA(cudaMemsetAsync(dpLeafParent.p, 0xff, nn * 4, st), err);
         CL_CUDA(cudaMemsetAsync(arrive.p, 0, ni * 4, st), err);
@@ -970,8 +974,8 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
 
     uint32_t ntasks = 1, depth = 0;
     out->levels.assign({0u, 1u});
-    DevBuf*  cur = &tasksA;
-    DevBuf*  nxt = &tasksB;
+    ScratchBuf* cur = &tasksA;
+    ScratchBuf* nxt = &tasksB;
     while (ntasks > 0)
     {
         ++depth;
@@ -1011,9 +1015,9 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
     // Validation of every index the traversal kernels will follow, on the
     // device; one error word comes back.
     {
-        DevBuf verr, seen;
-        CL_TRY(verr.alloc(4, err));
-        CL_TRY(seen.alloc((size_t(n) + 31) / 32 * 4, err));
+        ScratchBuf verr, seen;
+        CL_TRY(mem.take(verr, 4, err));
+        CL_TRY(mem.take(seen, (size_t(n) + 31) / 32 * 4, err));
         CL_CUDA(cudaMemsetAsync(verr.p, 0, 4, st), err);
         CL_CUDA(cudaMemsetAsync(seen.p, 0, (size_t(n) + 31) / 32 * 4, st), err);
         kValidateNodes<<<(out->numNodes + 255) / 256, 256, 0, st>>>(out->nodes.as<const uint4>(), out->numNodes, n,

@@ -1534,7 +1534,7 @@ cl_status Integrator::uploadMeshPool(uint32_t meshId, std::string* err)
     return CL_OK;
 }
 
-cl_status Integrator::buildBlas(uint32_t meshId, std::string* err)
+cl_status Integrator::buildBlas(uint32_t meshId, BuildArena* arena, std::string* err)
 {
     const HostMesh&    m  = meshes_[meshId];
     const size_t       mt = m.idx.size() / 3;
@@ -1546,7 +1546,7 @@ cl_status Integrator::buildBlas(uint32_t meshId, std::string* err)
     CL_TRY(d.alloc(tri9.size() * 4, err));
     CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
     if (!blas_[meshId]) blas_[meshId].reset(new WideBvh());
-    return buildWideBvh(d.f(), uint32_t(mt), stream_, blas_[meshId].get(), err);
+    return buildWideBvh(d.f(), uint32_t(mt), stream_, blas_[meshId].get(), err, arena);
 }
 
 // World box of instance i (every vertex mapped, in double), widened by a
@@ -1576,7 +1576,7 @@ void Integrator::instanceBox(uint32_t i, float* lo, float* hi) const
     }
 }
 
-cl_status Integrator::buildTopLevel(std::string* err)
+cl_status Integrator::buildTopLevel(BuildArena* arena, std::string* err)
 {
     const uint32_t     n = uint32_t(inst_.size());
     std::vector<float> tri9(size_t(n) * 9);
@@ -1602,7 +1602,7 @@ cl_status Integrator::buildTopLevel(std::string* err)
     DevBuf d;
     CL_TRY(d.alloc(tri9.size() * 4, err));
     CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
-    CL_TRY(buildWideBvh(d.f(), n, stream_, &bvh_, err));
+    CL_TRY(buildWideBvh(d.f(), n, stream_, &bvh_, err, arena));
     uint32_t blasDepth = 0;
     for (const auto& b : blas_)
         if (b) blasDepth = std::max(blasDepth, b->depth);
@@ -1696,10 +1696,11 @@ cl_status Integrator::buildTwoLevel(const cl_instance_desc* inst, uint32_t n, st
     for (uint32_t i = 0; i < n; ++i) used[inst[i].mesh_id] = true;
     blas_.clear();
     blas_.resize(nm);  // null entries
+    BuildArena arena;  // the builds' temporaries, allocated once for all the meshes
     for (uint32_t m = 0; m < nm; ++m)
-        if (used[m]) CL_TRY(buildBlas(m, err));
+        if (used[m]) CL_TRY(buildBlas(m, &arena, err));
     inst_.assign(inst, inst + n);
-    CL_TRY(buildTopLevel(err));
+    CL_TRY(buildTopLevel(&arena, err));
     CL_TRY(uploadInstances(err));
     CL_CUDA(cudaEventRecord(evB_, stream_), err);
     CL_CUDA(cudaEventSynchronize(evB_), err);
@@ -1729,7 +1730,7 @@ cl_status Integrator::updateTwoLevel(uint32_t meshId, uint32_t mode, std::string
     {
         if (mode == CL_BVH_UPDATE_REBUILD)
         {
-            CL_TRY(buildBlas(meshId, err));
+            CL_TRY(buildBlas(meshId, nullptr, err));
             ++rebuilds_;
         }
         else
@@ -1738,7 +1739,7 @@ cl_status Integrator::updateTwoLevel(uint32_t meshId, uint32_t mode, std::string
             ++refits_;
         }
     }
-    CL_TRY(buildTopLevel(err));
+    CL_TRY(buildTopLevel(nullptr, err));
     CL_TRY(uploadInstances(err));
     CL_CUDA(cudaEventRecord(evB_, stream_), err);
     CL_CUDA(cudaEventSynchronize(evB_), err);

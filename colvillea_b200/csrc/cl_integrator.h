@@ -236,8 +236,8 @@ private:
     uint32_t               twoLevelStack_ = 0;
     cl_status buildTwoLevel(const cl_instance_desc* inst, uint32_t n, std::string* err);
     cl_status uploadMeshPool(uint32_t meshId, std::string* err);
-    cl_status buildBlas(uint32_t meshId, std::string* err);
-    cl_status buildTopLevel(std::string* err);
+    cl_status buildBlas(uint32_t meshId, BuildArena* arena, std::string* err);
+    cl_status buildTopLevel(BuildArena* arena, std::string* err);
     cl_status uploadInstances(std::string* err);
     cl_status updateTwoLevel(uint32_t meshId, uint32_t mode, std::string* err);
     void      instanceBox(uint32_t i, float* lo, float* hi) const;

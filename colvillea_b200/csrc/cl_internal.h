@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -96,8 +97,45 @@ struct WideBvh
     }
 };
 
-// dTri9: 9 floats per triangle (world-space vertices), device memory.
-cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err);
+// A builder temporary: device memory taken from a build arena, with DevBuf's
+// accessors; it owns nothing (release() is a no-op).
+struct ScratchBuf
+{
+    void*  p     = nullptr;
+    size_t bytes = 0;
+    void      release() {}
+    float*    f() const { return static_cast<float*>(p); }
+    uint32_t* u() const { return static_cast<uint32_t*>(p); }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Grow-only device memory for the builder's temporaries: the k-th temporary of
+// a build reuses the k-th block of the previous build that shared the arena
+// (growing it when too small), so a sequence of builds (one per mesh of a
+// two-level scene) allocates, and frees - a synchronising cudaFree - once.
+class BuildArena
+{
+public:
+    void      reset() { used_ = 0; }
+    cl_status take(ScratchBuf& s, size_t bytes, std::string* err)
+    {
+        if (used_ == blocks_.size()) blocks_.emplace_back(new DevBuf());
+        DevBuf& b = *blocks_[used_++];
+        if (b.bytes < bytes) CL_TRY(b.alloc(bytes, err));
+        s.p     = b.p;
+        s.bytes = bytes;
+        return CL_OK;
+    }
+
+private:
+    std::vector<std::unique_ptr<DevBuf>> blocks_;
+    size_t                               used_ = 0;
+};
+
+// dTri9: 9 floats per triangle (world-space vertices), device memory.  The
+// builder's temporaries come from `arena` (a local one when null).
+cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh* out, std::string* err,
+                       BuildArena* arena = nullptr);
 
 // Refit after the vertices moved (same triangles, same vertex indices):
 // rewrites the leaf triangles from vtx (3 float4 per vertex, position in the
