@@ -361,20 +361,18 @@ def run_guide_study(args):
     t_ref = time.perf_counter() - t0
     G = cb.GuideConfig
     variants = {
-        "guided_all_classes": G(class_mask=7),
-        "guided_all_classes_bsdf_fraction_0.7_train64": G(class_mask=7, bsdf_fraction=0.7, train_spp=64),
-        "guided_all_classes_bsdf_fraction_0.8": G(class_mask=7, bsdf_fraction=0.8),
-        "guided_dielectric_only": G(class_mask=4),
-        "guided_dielectric_only_bsdf_fraction_0.7": G(class_mask=4, bsdf_fraction=0.7),
         "guided_dielectric_only_bsdf_fraction_0.8": G(class_mask=4, bsdf_fraction=0.8),
-        "guided_dielectric_only_bsdf_fraction_0.7_train64": G(class_mask=4, bsdf_fraction=0.7, train_spp=64),
-        "guided_dielectric_only_bsdf_fraction_0.7_indirect": G(class_mask=4, bsdf_fraction=0.7, min_depth=2),
+        "guided_dielectric_only_bsdf_fraction_0.9": G(class_mask=4, bsdf_fraction=0.9),
+        "guided_dielectric_only_bsdf_fraction_0.8_batch2^19": G(class_mask=4, bsdf_fraction=0.8, batch=1 << 19),
+        "guided_dielectric_only_bsdf_fraction_0.8_lr3e-3": G(class_mask=4, bsdf_fraction=0.8, learning_rate=3e-3),
+        "guided_all_classes_bsdf_fraction_0.9": G(class_mask=7, bsdf_fraction=0.9),
+        "guided_dielectric_conductor_bsdf_fraction_0.8": G(class_mask=6, bsdf_fraction=0.8),
     }
-    rows = evaluate.equal_spp(s3, ref, args.relmse_spp, variants, seeds=2)
+    rows = evaluate.equal_spp(s3, ref, args.relmse_spp, variants, seeds=args.relmse_seeds)
     rnd = lambda d: {k: (round(v, 6) if isinstance(v, float) else ([round(x, 6) for x in v] if isinstance(v, list)
                                                                     else v)) for k, v in d.items()}
     print(json.dumps({"guide_study": "cfg3 (cfg1 scene, 1920x1080, depth 5, RR 3), corrected estimator, alias dome "
-                                     f"sampler; {args.relmse_spp} spp per variant incl. training; 2 seeds; reference "
+                                     f"sampler; {args.relmse_spp} spp per variant incl. training; {args.relmse_seeds} seeds; reference "
                                      f"{args.relmse_ref_spp} spp FP64 ({t_ref:.1f} s)",
                       "rows": {k: rnd(v) for k, v in rows.items()}}))
     return 0
