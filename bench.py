@@ -59,8 +59,11 @@ def parse():
                     help="short workload for ncu: cfg3 with guiding or cfg4 with the radiance cache, "
                          "2 training spp + 2 spp")
     ap.add_argument("--guide-study", action="store_true",
-                    help="cfg3 guiding variants at equal spp (plain; guided everywhere; indirect vertices only; "
-                         "all BSDF classes; 32/64/128 training steps) against the FP64 reference (one JSON line)")
+                    help="guiding variants at equal spp against an FP64 reference (one JSON line): on cfg3 "
+                         "guided BSDF classes and selection probabilities; on cfg4/cfg5 the same with the "
+                         "radiance cache (see --study-config)")
+    ap.add_argument("--study-config", type=int, default=3, choices=[3, 4, 5],
+                    help="scene of --guide-study (3: guiding alone; 4, 5: radiance cache with and without guiding)")
     ap.add_argument("--relmse-ref-spp", type=int, default=8192, help="spp of the cfg3 FP64 reference image")
     ap.add_argument("--relmse-ref-spp4", type=int, default=8192, help="spp of the cfg4 FP64 reference image")
     ap.add_argument("--relmse-seeds", type=int, default=3)
@@ -351,29 +354,52 @@ def scene_edit(it, s, args, spp=4):
 
 
 def run_guide_study(args):
-    """Equal-spp table of guiding variants on cfg3 (128 spp each, training
-    included; 2 seeds): does the network lower the variance, and where."""
+    """Equal-spp table of guiding variants (training included): does the
+    network lower the error, and where.  cfg3: guiding alone, by guided BSDF
+    classes and selection probability.  cfg4, cfg5: the radiance cache alone
+    and with guiding variants (the relMSE then includes the cache's bias)."""
     import colvillea_b200 as cb
     from colvillea_b200 import evaluate, scenes
-    s3 = scenes.config3(0)
+    G, C = cb.GuideConfig, cb.RadianceCacheConfig
+    if args.study_config == 3:
+        sc, spp, ref_spp = scenes.config3(0), args.relmse_spp, args.relmse_ref_spp
+        variants = {
+            "guided_dielectric_only_bsdf_fraction_0.8": G(class_mask=4, bsdf_fraction=0.8),
+            "guided_dielectric_only_bsdf_fraction_0.9": G(class_mask=4, bsdf_fraction=0.9),
+            "guided_dielectric_only_bsdf_fraction_0.8_batch2^19": G(class_mask=4, bsdf_fraction=0.8, batch=1 << 19),
+            "guided_dielectric_only_bsdf_fraction_0.8_lr3e-3": G(class_mask=4, bsdf_fraction=0.8, learning_rate=3e-3),
+            "guided_all_classes_bsdf_fraction_0.9": G(class_mask=7, bsdf_fraction=0.9),
+            "guided_dielectric_conductor_bsdf_fraction_0.8": G(class_mask=6, bsdf_fraction=0.8),
+            "guided_all_classes_bsdf_fraction_0.5_min_alpha_0.1": G(min_alpha=0.1),
+            "guided_all_classes_bsdf_fraction_0.8_min_alpha_0.1": G(bsdf_fraction=0.8, min_alpha=0.1),
+        }
+        label = "cfg3 (cfg1 scene, 1920x1080, depth 5, RR 3)"
+    else:
+        sc = scenes.config4(0) if args.study_config == 4 else scenes.config5(0)
+        spp = args.relmse_spp if args.study_config == 4 else args.ext_spp5
+        ref_spp = args.relmse_ref_spp4 if args.study_config == 4 else args.ext_ref_spp5
+        variants = {
+            "cache": {"cache": C()},
+            "cache_guided_all_classes_bsdf_fraction_0.5": {"cache": C(), "guide": G()},
+            "cache_guided_diffuse_conductor_bsdf_fraction_0.5": {"cache": C(), "guide": G(class_mask=3)},
+            "cache_guided_all_classes_bsdf_fraction_0.5_min_alpha_0.1": {"cache": C(), "guide": G(min_alpha=0.1)},
+            "cache_guided_all_classes_bsdf_fraction_0.8": {"cache": C(), "guide": G(bsdf_fraction=0.8)},
+            "cache_guided_dielectric_only_bsdf_fraction_0.8": {"cache": C(), "guide": G(class_mask=4,
+                                                                                     bsdf_fraction=0.8)},
+            "guided_all_classes_bsdf_fraction_0.5": G(),
+            "guided_all_classes_bsdf_fraction_0.5_min_alpha_0.1": G(min_alpha=0.1),
+        }
+        label = (f"cfg{args.study_config} ({sc.width}x{sc.height}, depth {sc.max_depth}, RR {sc.rr_start}, "
+                 f"{sc.num_triangles} triangles)")
     t0 = time.perf_counter()
-    ref = evaluate.reference(s3, args.relmse_ref_spp)
+    ref = evaluate.reference(sc, ref_spp)
     t_ref = time.perf_counter() - t0
-    G = cb.GuideConfig
-    variants = {
-        "guided_dielectric_only_bsdf_fraction_0.8": G(class_mask=4, bsdf_fraction=0.8),
-        "guided_dielectric_only_bsdf_fraction_0.9": G(class_mask=4, bsdf_fraction=0.9),
-        "guided_dielectric_only_bsdf_fraction_0.8_batch2^19": G(class_mask=4, bsdf_fraction=0.8, batch=1 << 19),
-        "guided_dielectric_only_bsdf_fraction_0.8_lr3e-3": G(class_mask=4, bsdf_fraction=0.8, learning_rate=3e-3),
-        "guided_all_classes_bsdf_fraction_0.9": G(class_mask=7, bsdf_fraction=0.9),
-        "guided_dielectric_conductor_bsdf_fraction_0.8": G(class_mask=6, bsdf_fraction=0.8),
-    }
-    rows = evaluate.equal_spp(s3, ref, args.relmse_spp, variants, seeds=args.relmse_seeds)
+    rows = evaluate.equal_spp(sc, ref, spp, variants, seeds=args.relmse_seeds)
     rnd = lambda d: {k: (round(v, 6) if isinstance(v, float) else ([round(x, 6) for x in v] if isinstance(v, list)
                                                                     else v)) for k, v in d.items()}
-    print(json.dumps({"guide_study": "cfg3 (cfg1 scene, 1920x1080, depth 5, RR 3), corrected estimator, alias dome "
-                                     f"sampler; {args.relmse_spp} spp per variant incl. training; {args.relmse_seeds} seeds; reference "
-                                     f"{args.relmse_ref_spp} spp FP64 ({t_ref:.1f} s)",
+    print(json.dumps({"guide_study": f"{label}, corrected estimator, alias dome sampler; {spp} spp per variant incl. "
+                                     f"training; {args.relmse_seeds} seeds; reference {ref_spp} spp FP64 "
+                                     f"({t_ref:.1f} s)",
                       "rows": {k: rnd(v) for k, v in rows.items()}}))
     return 0
 

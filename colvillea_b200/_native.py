@@ -90,7 +90,8 @@ class GuideConfig(ctypes.Structure):
                 ("learning_rate", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float),
                 ("epsilon", ctypes.c_float), ("bsdf_fraction", ctypes.c_float), ("batch", u32),
                 ("train_spp", u32), ("class_mask", u32), ("seed", u32), ("learn_selection", u32),
-                ("weight_clamp", ctypes.c_float), ("min_depth", u32)]
+                ("weight_clamp", ctypes.c_float), ("min_depth", u32),
+                ("min_alpha", ctypes.c_float)]
 
 
 class RadianceCacheConfig(ctypes.Structure):

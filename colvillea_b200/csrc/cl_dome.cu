@@ -9,6 +9,10 @@
 //     pV_c and CDFpV (h+1).  They serve the CDF sampler and every pdf lookup;
 //   * alias tables for O(1) sampling of the same density: per row over
 //     columns (w*h entries) and over rows (h entries), Vose's method in FP64.
+// One block per row (kDomeRowTables) and one for the marginal
+// (kDomeMarginalTable) with the row in shared memory: rows of up to 16,384
+// texels.  Wider rows take the one-thread-per-row kernels over global
+// scratch (kDomeWeights, kDomeRows, kDomeMarginal).
 // Texel weights are sin(theta_v) * luminance(texel) at texel centres
 // (hdridome.h:319-323, luminance weights math.h:155-158).
 #include "cl_dome.h"
@@ -70,7 +74,8 @@ __device__ void voseBuild(const double* wgt, int n, double total, uint2* out, ui
     }
 }
 
-// One thread per row: FP64 row sums, CDF row, alias row.
+// Rows wider than the shared-memory path takes: one thread per row, FP64 row
+// sums, CDF row, alias row.
 __global__ void kDomeRows(const double* __restrict__ wgt, int w, int h, float* __restrict__ pU, float* __restrict__ cU,
                           double* __restrict__ rowC, uint2* __restrict__ aliasCol, uint32_t* scratchIdx,
                           double* scratchQ)
@@ -111,7 +116,7 @@ __global__ void kDomeRows(const double* __restrict__ wgt, int w, int h, float* _
               scratchQ + size_t(v) * w);
 }
 
-// Single thread: marginal over rows.
+// Marginal over more rows than the shared-memory path takes: one thread.
 __global__ void kDomeMarginal(const double* __restrict__ rowC, int h, float* __restrict__ pV, float* __restrict__ cV,
                               uint2* __restrict__ aliasRow, uint32_t* scratchIdx, double* scratchQ)
 {
@@ -143,15 +148,257 @@ __global__ void kDomeMarginal(const double* __restrict__ rowC, int h, float* __r
     voseBuild(rowC, h, sum, aliasRow, scratchIdx, scratchIdx + h, scratchQ);
 }
 
+// ---------------------------------------------------------------------------
+// One table per block, in shared memory: the path for rows whose table fits
+// in 227 KB (16,384 texels; the kernels above serve wider ones).
+// ---------------------------------------------------------------------------
+constexpr int kDomeThreads = 256;
+
+// Shared memory of one n-entry table: q (double, n) | chunk totals (double,
+// T+1) | small counts (uint32, T+1) | Vose work list (uint32, n).
+size_t domeTableSmem(int n)
+{
+    return size_t(n) * 12 + size_t(kDomeThreads + 1) * 12;
+}
+
+// The table of the n FP64 weights in q[0, n):
+//   * total: thread t sums its chunk [t*k, t*k+k) in order, thread 0 adds the
+//     chunk totals in order; CDF entry i+1 is (offset of the chunk + prefix
+//     within the chunk) / total, so the CDF is non-decreasing and its last
+//     prefix equals the total exactly;
+//   * p[0, n) = float(weights), p[n] = float(total / n), c[0] = 0, c[n] = 1
+//     (all-zero weights: p = 0, c[i] = i / n), as kDomeRows/kDomeMarginal;
+//   * the alias table by Vose's method on q = w * n / total, with the small
+//     and large work lists in index order (one shared list: small from the
+//     front, large from the back).  Thread 0 pairs them.  Both lists are
+//     stacks, so an entry that changes list is the next one popped from the
+//     other; the loop keeps it in registers, reads the initial lists from
+//     their tops down, and writes the same table as voseBuild.
+// Returns the total to every thread.
+__device__ double domeTable(double* q, int n, float* __restrict__ p, float* __restrict__ c, uint2* __restrict__ alias)
+{
+    double*   part = q + n;
+    uint32_t* cnt  = reinterpret_cast<uint32_t*>(part + kDomeThreads + 1);
+    uint32_t* list = cnt + kDomeThreads + 1;
+    const int t    = threadIdx.x;
+    const int k    = (n + kDomeThreads - 1) / kDomeThreads;
+    const int b    = min(n, t * k);
+    const int e    = min(n, b + k);
+
+    double loc = 0.0;
+    for (int i = b; i < e; ++i) loc += q[i];
+    part[t] = loc;
+    __syncthreads();
+    if (t == 0)
+    {
+        double off = 0.0;
+        for (int j = 0; j < kDomeThreads; ++j)
+        {
+            double x = part[j];
+            part[j]  = off;
+            off += x;
+        }
+        part[kDomeThreads] = off;
+    }
+    __syncthreads();
+    const double sum = part[kDomeThreads];
+    const double off = part[t];
+    const double cv  = sum / double(n);
+    if (cv > 0.0)
+    {
+        double acc = 0.0;
+        for (int i = b; i < e; ++i)
+        {
+            p[i] = float(q[i]);
+            acc += q[i];
+            if (i + 1 < n) c[i + 1] = float((off + acc) / sum);
+        }
+        if (t == 0)
+        {
+            c[0] = 0.0f;
+            c[n] = 1.0f;
+            p[n] = float(cv);
+        }
+    }
+    else
+    {
+        for (int i = b; i < e; ++i)
+        {
+            p[i] = 0.0f;
+            c[i] = float(i) / float(n);
+        }
+        if (t == 0)
+        {
+            c[n] = 1.0f;
+            p[n] = 0.0f;
+        }
+    }
+    if (!(sum > 0.0))
+    {
+        for (int i = b; i < e; ++i) alias[i] = make_uint2(__float_as_uint(1.0f), uint32_t(i));
+        return sum;
+    }
+
+    uint32_t nsLoc = 0;
+    for (int i = b; i < e; ++i)
+    {
+        q[i] = q[i] * double(n) / sum;
+        nsLoc += q[i] < 1.0 ? 1u : 0u;
+    }
+    cnt[t] = nsLoc;
+    __syncthreads();
+    if (t == 0)
+    {
+        uint32_t o = 0;
+        for (int j = 0; j < kDomeThreads; ++j)
+        {
+            uint32_t x = cnt[j];
+            cnt[j]     = o;
+            o += x;
+        }
+        cnt[kDomeThreads] = o;
+    }
+    __syncthreads();
+    {
+        uint32_t si = cnt[t], li = uint32_t(b) - cnt[t];
+        for (int i = b; i < e; ++i)
+        {
+            if (q[i] < 1.0)
+                list[si++] = uint32_t(i);
+            else
+                list[n - 1 - int(li++)] = uint32_t(i);
+        }
+    }
+    __syncthreads();
+    if (t != 0) return sum;
+
+    int ns = int(cnt[kDomeThreads]), nl = n - ns;
+    if (ns > 0 && nl > 0)
+    {
+        uint32_t l  = list[--ns];
+        double   ql = q[l];
+        uint32_t g  = list[n - nl];
+        --nl;
+        double   qg  = q[g];
+        // Next entries of the two initial lists, read one step ahead.
+        uint32_t sN  = ns > 0 ? list[ns - 1] : 0u;
+        double   sNq = ns > 0 ? q[sN] : 0.0;
+        uint32_t lN  = nl > 0 ? list[n - nl] : 0u;
+        double   lNq = nl > 0 ? q[lN] : 0.0;
+        for (;;)
+        {
+            alias[l] = make_uint2(__float_as_uint(float(ql)), g);
+            qg       = (qg + ql) - 1.0;
+            if (qg < 1.0)
+            {
+                // g turns small and is paired next.
+                if (nl == 0)
+                {
+                    alias[g] = make_uint2(__float_as_uint(1.0f), g);
+                    break;
+                }
+                l  = g;
+                ql = qg;
+                g  = lN;
+                qg = lNq;
+                --nl;
+                if (nl > 0)
+                {
+                    lN  = list[n - nl];
+                    lNq = q[lN];
+                }
+            }
+            else
+            {
+                // g stays large and stays the top of the large list.
+                if (ns == 0)
+                {
+                    alias[g] = make_uint2(__float_as_uint(1.0f), g);
+                    break;
+                }
+                l  = sN;
+                ql = sNq;
+                --ns;
+                if (ns > 0)
+                {
+                    sN  = list[ns - 1];
+                    sNq = q[sN];
+                }
+            }
+        }
+    }
+    for (int i = 0; i < ns; ++i) alias[list[i]] = make_uint2(__float_as_uint(1.0f), list[i]);
+    for (int j = 0; j < nl; ++j) alias[list[n - 1 - j]] = make_uint2(__float_as_uint(1.0f), list[n - 1 - j]);
+    return sum;
+}
+
+// Block v: the texel weights of row v (as kDomeWeights) into shared memory,
+// then the row's tables.
+__global__ void __launch_bounds__(kDomeThreads) kDomeRowTables(const float4* __restrict__ tex, int w, int h,
+                                                               float* __restrict__ pU, float* __restrict__ cU,
+                                                               double* __restrict__ rowC, uint2* __restrict__ aliasCol)
+{
+    extern __shared__ __align__(16) unsigned char domeSmem[];
+    double*      q     = reinterpret_cast<double*>(domeSmem);
+    const int    v     = blockIdx.x;
+    const double sinth = sin(3.14159265358979323846 * (double(v) + 0.5) / double(h));
+    for (int u = threadIdx.x; u < w; u += kDomeThreads)
+    {
+        float4 t   = tex[size_t(v) * w + u];
+        double lum = double(t.x) * 0.212671 + double(t.y) * 0.71516 + double(t.z) * 0.072169;
+        q[u]       = sinth * lum;
+    }
+    __syncthreads();
+    double sum = domeTable(q, w, pU + size_t(v) * (w + 1), cU + size_t(v) * (w + 1), aliasCol + size_t(v) * w);
+    if (threadIdx.x == 0) rowC[v] = sum / double(w);
+}
+
+// One block: the marginal over the row integrals.
+__global__ void __launch_bounds__(kDomeThreads) kDomeMarginalTable(const double* __restrict__ rowC, int h,
+                                                                   float* __restrict__ pV, float* __restrict__ cV,
+                                                                   uint2* __restrict__ aliasRow)
+{
+    extern __shared__ __align__(16) unsigned char domeSmem[];
+    double* q = reinterpret_cast<double*>(domeSmem);
+    for (int v = threadIdx.x; v < h; v += kDomeThreads) q[v] = rowC[v];
+    __syncthreads();
+    domeTable(q, h, pV, cV, aliasRow);
+}
+
+// Largest table the shared-memory kernels take (227 KB per block).
+constexpr size_t kDomeSmemMax = 227u * 1024u;
+
 } // namespace
 
 cl_status launchDomeBuild(const float4* dTex, int w, int h, cudaStream_t st, const DomeScratch& s, float* pU, float* cU,
                           float* pV, float* cV, uint2* aliasRow, uint2* aliasCol, std::string* err)
 {
-    dim3 g((w + 127) / 128, h);
-    kDomeWeights<<<g, 128, 0, st>>>(dTex, w, h, s.weights);
-    kDomeRows<<<(h + 63) / 64, 64, 0, st>>>(s.weights, w, h, pU, cU, s.rowC, aliasCol, s.idx, s.q);
-    kDomeMarginal<<<1, 32, 0, st>>>(s.rowC, h, pV, cV, aliasRow, s.idx, s.q);
+    // Rows: one block per row in shared memory when the row fits, else one
+    // thread per row over the global scratch.
+    const size_t smemW = domeTableSmem(w), smemH = domeTableSmem(h);
+    if (smemW <= kDomeSmemMax)
+    {
+        if (smemW > 48u * 1024u)
+            CL_CUDA(cudaFuncSetAttribute(kDomeRowTables, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemW)), err);
+        kDomeRowTables<<<h, kDomeThreads, smemW, st>>>(dTex, w, h, pU, cU, s.rowC, aliasCol);
+    }
+    else
+    {
+        dim3 g((w + 127) / 128, h);
+        kDomeWeights<<<g, 128, 0, st>>>(dTex, w, h, s.weights);
+        kDomeRows<<<(h + 63) / 64, 64, 0, st>>>(s.weights, w, h, pU, cU, s.rowC, aliasCol, s.idx, s.q);
+    }
+    if (smemH <= kDomeSmemMax)
+    {
+        if (smemH > 48u * 1024u)
+            CL_CUDA(cudaFuncSetAttribute(kDomeMarginalTable, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemH)),
+                    err);
+        kDomeMarginalTable<<<1, kDomeThreads, smemH, st>>>(s.rowC, h, pV, cV, aliasRow);
+    }
+    else
+    {
+        kDomeMarginal<<<1, 32, 0, st>>>(s.rowC, h, pV, cV, aliasRow, s.idx, s.q);
+    }
     CL_CUDA(cudaGetLastError(), err);
     return CL_OK;
 }

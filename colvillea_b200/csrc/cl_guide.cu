@@ -620,12 +620,12 @@ template <class S, class LOSS> __global__ void __launch_bounds__(kTrainThreads, 
                     const int  lv = int(8 * half) + q;
                     const Cell c  = gridCell(a.g.res[lv], p);
                     float2*    gb = a.gradTable + (size_t(lv) << a.g.log2T);
+                    uint32_t   idx[8];
+                    float      w[8];
+                    cornerIndices(a.g, lv, c, idx);
+                    cornerWeights(c, w);
 #pragma unroll
-                    for (int k = 0; k < 8; ++k)
-                    {
-                        const float w = cornerWeight(c, k);
-                        atomicAdd(gb + cornerIndex(a.g, lv, c, k), make_float2(w * d0, w * d1));
-                    }
+                    for (int k = 0; k < 8; ++k) atomicAdd(gb + idx[k], make_float2(w[k] * d0, w[k] * d1));
                 }
             }
         }
@@ -746,6 +746,7 @@ void guideDefaultConfig(cl_guide_config* c)
     c->learn_selection = 0u;
     c->weight_clamp    = 0.0f;
     c->min_depth       = 1u;
+    c->min_alpha       = 0.0f;
 }
 
 cl_status guideResolutions(float nmin, float nmax, uint32_t* res)
@@ -770,9 +771,10 @@ template <class S, class L> cl_status HashNet<S, L>::init(cudaStream_t st, std::
     if (cfg_.batch == 0 || cfg_.batch > (1u << 24) || !(cfg_.learning_rate > 0.0f) || !(cfg_.bsdf_fraction >= 0.0f) ||
         !(cfg_.bsdf_fraction <= 1.0f) || !(cfg_.beta1 >= 0.0f && cfg_.beta1 < 1.0f) ||
         !(cfg_.beta2 >= 0.0f && cfg_.beta2 < 1.0f) || !(cfg_.epsilon >= 0.0f) || cfg_.learn_selection > 1u ||
-        !(cfg_.weight_clamp >= 0.0f))
+        !(cfg_.weight_clamp >= 0.0f) || !(cfg_.min_alpha >= 0.0f && cfg_.min_alpha <= 1.0f))
     {
-        *err = "network: batch, learning rate, Adam, bsdf_fraction, learn_selection or weight_clamp out of range";
+        *err = "network: batch, learning rate, Adam, bsdf_fraction, learn_selection, weight_clamp or min_alpha out of "
+               "range";
         return CL_ERR_INVALID_ARG;
     }
     bool given = false;

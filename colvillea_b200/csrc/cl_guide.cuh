@@ -48,13 +48,6 @@ struct GridView
     uint32_t res[kLevels];
 };
 
-__device__ __forceinline__ uint32_t gridIndex(uint32_t x, uint32_t y, uint32_t z, uint32_t r1, bool dense,
-                                              uint32_t mask)
-{
-    if (dense) return x + r1 * (y + r1 * z);
-    return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & mask;
-}
-
 // Cell and interpolation weights of level l for p in [0,1]^3 (clamped): the
 // cell index is clamped to res-1 so that p = 1 interpolates with weight 1.
 struct Cell
@@ -69,17 +62,46 @@ __device__ __forceinline__ Cell gridCell(uint32_t res, f3 p)
     float       ix = fminf(floorf(x), top), iy = fminf(floorf(y), top), iz = fminf(floorf(z), top);
     return {uint32_t(ix), uint32_t(iy), uint32_t(iz), x - ix, y - iy, z - iz};
 }
-__device__ __forceinline__ float cornerWeight(const Cell& c, int k)
+// The 8 corner weights, corner k's the product (a b) d of a = wx or 1 - wx,
+// b = wy or 1 - wy, d = wz or 1 - wz by bits 0, 1, 2 of k; the 4 products
+// a b are shared by the two z layers.
+__device__ __forceinline__ void cornerWeights(const Cell& c, float (&w)[8])
 {
-    float a = (k & 1) ? c.wx : 1.0f - c.wx;
-    float b = (k & 2) ? c.wy : 1.0f - c.wy;
-    float d = (k & 4) ? c.wz : 1.0f - c.wz;
-    return a * b * d;
+    const float ax[2] = {1.0f - c.wx, c.wx}, by[2] = {1.0f - c.wy, c.wy}, dz[2] = {1.0f - c.wz, c.wz};
+    float       ab[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ab[k] = ax[k & 1] * by[k >> 1];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) w[k] = ab[k & 3] * dz[k >> 2];
 }
-__device__ __forceinline__ uint32_t cornerIndex(const GridView& g, int l, const Cell& c, int k)
+// The 8 corner indices of level l (corner k: +1 along x, y, z for bits 0, 1,
+// 2 of k).  A dense level indexes x + r1 (y + r1 z) (r1 = res + 1), so the
+// corners add 1, r1 and r1^2 to the cell's index; a hashed level indexes
+// (x ^ y P1 ^ z P2) & (T - 1) with P1 = 2654435761, P2 = 805459861 (Mueller
+// et al. 2022), built from the per-axis terms, (y + 1) P1 = y P1 + P1 (mod
+// 2^32).  The dense/hashed choice depends on the level only, so it is uniform
+// across a warp.
+__device__ __forceinline__ void cornerIndices(const GridView& g, int l, const Cell& c, uint32_t (&idx)[8])
 {
-    const uint32_t r1 = g.res[l] + 1u;
-    return gridIndex(c.x + (k & 1), c.y + ((k >> 1) & 1), c.z + ((k >> 2) & 1), r1, (g.denseMask >> l) & 1u, g.mask);
+    if ((g.denseMask >> l) & 1u)
+    {
+        const uint32_t r1 = g.res[l] + 1u, b = c.x + r1 * (c.y + r1 * c.z), b4 = b + r1 * r1;
+        idx[0] = b;
+        idx[1] = b + 1u;
+        idx[2] = b + r1;
+        idx[3] = b + r1 + 1u;
+        idx[4] = b4;
+        idx[5] = b4 + 1u;
+        idx[6] = b4 + r1;
+        idx[7] = b4 + r1 + 1u;
+    }
+    else
+    {
+        const uint32_t y[2] = {c.y * 2654435761u, c.y * 2654435761u + 2654435761u};
+        const uint32_t z[2] = {c.z * 805459861u, c.z * 805459861u + 805459861u};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) idx[k] = ((c.x + uint32_t(k & 1)) ^ y[(k >> 1) & 1] ^ z[k >> 2]) & g.mask;
+    }
 }
 __device__ __forceinline__ f3 clampUnit(f3 p)
 {
@@ -88,22 +110,22 @@ __device__ __forceinline__ f3 clampUnit(f3 p)
 // Trilinear features of level l (8 independent 4-byte gathers).
 __device__ __forceinline__ float2 encodeLevel(const GridView& g, int l, f3 p)
 {
-    Cell           c    = gridCell(g.res[l], p);
-    const size_t   base = size_t(l) << g.log2T;
-    uint32_t       idx[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) idx[k] = cornerIndex(g, l, c, k);
+    const Cell                          c  = gridCell(g.res[l], p);
+    const __nv_bfloat162* __restrict__ tl = g.table + (size_t(l) << g.log2T);
+    uint32_t                            idx[8];
+    cornerIndices(g, l, c, idx);
     __nv_bfloat162 t[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) t[k] = __ldg(g.table + base + idx[k]);
+    for (int k = 0; k < 8; ++k) t[k] = __ldg(tl + idx[k]);
+    float w[8];
+    cornerWeights(c, w);
     float f0 = 0.0f, f1 = 0.0f;
 #pragma unroll
     for (int k = 0; k < 8; ++k)
     {
-        float  w = cornerWeight(c, k);
         float2 v = __bfloat1622float2(t[k]);
-        f0       = fmaf(w, v.x, f0);
-        f1       = fmaf(w, v.y, f1);
+        f0       = fmaf(w[k], v.x, f0);
+        f1       = fmaf(w[k], v.y, f1);
     }
     return {f0, f1};
 }
@@ -207,9 +229,9 @@ __device__ __forceinline__ void headLobes(const float* o, Lobes* L, float alpha 
     for (int k = 0; k < kLobes; ++k)
     {
         float x = o[5 * k], y = o[5 * k + 1], z = o[5 * k + 2];
-        float n = fmaxf(sqrtf(x * x + y * y + z * z), 1e-6f);
+        float rn  = 1.0f / fmaxf(sqrtf(x * x + y * y + z * z), 1e-6f);
         float kap = expf(fminf(fmaxf(o[5 * k + 3], kKappaMin), kKappaMax));
-        L->l[k]   = make_float4(x / n, y / n, z / n, kap);
+        L->l[k]   = make_float4(x * rn, y * rn, z * rn, kap);
         L->w[k] *= inv;
     }
 }

@@ -596,9 +596,11 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 f3    wo     = -d;
                 guide::Lobes G;
                 float        gf = 1.0f; // probability of BSDF sampling: 1 - sum of the lobe weights
-                // Vertices shallower than the guide's minimum depth were not inferred: BSDF sampling
-                // alone (zero lobe weights), no training record.
-                const bool guided = GUIDE && depth >= P.g.minDepth;
+                // Vertices shallower than the guide's minimum depth were not inferred, and near-specular
+                // ones (GGX alpha below the guide's minimum) are not guided: BSDF sampling alone (zero
+                // lobe weights), no training record.
+                const bool guided =
+                    GUIDE && depth >= P.g.minDepth && (bsdf.type == kDiffuse || bsdf.alpha >= P.g.minAlpha);
                 if (GUIDE && !guided)
 #pragma unroll
                     for (int k = 0; k < guide::kLobes; ++k)
@@ -1542,11 +1544,13 @@ cl_status Integrator::buildBlas(uint32_t meshId, BuildArena* arena, std::string*
     for (size_t t = 0; t < mt; ++t)
         for (int q = 0; q < 3; ++q)
             for (int c = 0; c < 3; ++c) tri9[t * 9 + 3 * q + c] = m.pos[3 * size_t(m.idx[3 * t + q]) + c];
-    DevBuf d;
-    CL_TRY(d.alloc(tri9.size() * 4, err));
+    BuildArena  local;
+    BuildArena& mem = arena ? *arena : local;
+    ScratchBuf  d;
+    CL_TRY(mem.input(d, tri9.size() * 4, err));
     CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
     if (!blas_[meshId]) blas_[meshId].reset(new WideBvh());
-    return buildWideBvh(d.f(), uint32_t(mt), stream_, blas_[meshId].get(), err, arena);
+    return buildWideBvh(d.f(), uint32_t(mt), stream_, blas_[meshId].get(), err, &mem);
 }
 
 // World box of instance i (every vertex mapped, in double), widened by a
@@ -1599,10 +1603,12 @@ cl_status Integrator::buildTopLevel(BuildArena* arena, std::string* err)
     ext       = std::max(ext, 1e-6f) * 1.002f;
     for (int q = 0; q < 3; ++q) boxMin_[q] = slo[q] - 0.001f * ext;
     boxScale_ = 1.0f / ext;
-    DevBuf d;
-    CL_TRY(d.alloc(tri9.size() * 4, err));
+    BuildArena  local;
+    BuildArena& mem = arena ? *arena : local;
+    ScratchBuf  d;
+    CL_TRY(mem.input(d, tri9.size() * 4, err));
     CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
-    CL_TRY(buildWideBvh(d.f(), n, stream_, &bvh_, err, arena));
+    CL_TRY(buildWideBvh(d.f(), n, stream_, &bvh_, err, &mem));
     uint32_t blasDepth = 0;
     for (const auto& b : blas_)
         if (b) blasDepth = std::max(blasDepth, b->depth);
@@ -2119,6 +2125,7 @@ Params Integrator::params() const
         P.g.recCap    = recCap_;
         P.g.classMask = guideCfg_.class_mask;
         P.g.minDepth  = std::max(guideCfg_.min_depth, 1u);
+        P.g.minAlpha  = guideCfg_.min_alpha;
         P.g.histDepth = histDepth_;
     }
     for (int q = 0; q < 3; ++q) P.g.boxMin[q] = boxMin_[q];

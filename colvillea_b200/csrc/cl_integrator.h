@@ -111,6 +111,7 @@ struct GuideDev
     uint32_t recCap;
     uint32_t classMask; // guided BSDF classes
     uint32_t minDepth;  // guided vertices have depth >= minDepth
+    float    minAlpha;  // and, at conductors and dielectrics, GGX alpha >= minAlpha
     float*   probe;     // test probe (cl_integrator_guide_probe): per guided row k < probeCap,
     uint32_t probeCap;  // kProbeF floats {in9, ray index bits, 40 lobe floats, 2 pad}; null in renders
     float    boxScale;  // 1 / largest scene extent

@@ -126,10 +126,20 @@ public:
         s.bytes = bytes;
         return CL_OK;
     }
+    // Device copy of a build's input, kept apart from the temporaries (which
+    // reset() recycles): one block that grows and is reused by the next build.
+    cl_status input(ScratchBuf& s, size_t bytes, std::string* err)
+    {
+        if (input_.bytes < bytes) CL_TRY(input_.alloc(bytes, err));
+        s.p     = input_.p;
+        s.bytes = bytes;
+        return CL_OK;
+    }
 
 private:
     std::vector<std::unique_ptr<DevBuf>> blocks_;
     size_t                               used_ = 0;
+    DevBuf                               input_;
 };
 
 // dTri9: 9 floats per triangle (world-space vertices), device memory.  The

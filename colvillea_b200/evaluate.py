@@ -116,12 +116,15 @@ def mlp_throughput(scene, guide=None, spp=8, max_depth=None):
 
 def equal_spp(scene, ref, spp, variants, seeds=2, max_depth=None, seed_stride=1 << 20):
     """relMSE after `spp` samples per pixel for the plain tracer and for each
-    guided variant (`variants`: name -> GuideConfig; a variant's training
-    steps are part of its `spp`), over `seeds` disjoint frame ranges with a
-    fresh network per seed.  relMSE at equal spp measures the estimators'
-    variance (their bias is zero); each entry also gives the device time, and
-    `time_ratio` = (plain relMSE x plain time) / (variant relMSE x variant
-    time), the equal-time gain of the variant when variance falls as 1 / time."""
+    variant (`variants`: name -> GuideConfig, or name -> {"guide": GuideConfig
+    or None, "cache": RadianceCacheConfig or None}; a variant's training steps
+    are part of its `spp`), over `seeds` disjoint frame ranges with fresh
+    networks per seed.  For guiding alone, relMSE at equal spp measures the
+    estimators' variance (their bias is zero); with the radiance cache it
+    includes the cache's bias (`bias` per variant).  Each entry also gives the
+    device time, and `time_ratio` = (plain relMSE x plain time) / (variant
+    relMSE x variant time), the equal-time gain of the variant when its error
+    falls as 1 / time."""
     plain = load_scene(scene, flags=FLAGS, max_depth=max_depth)
     _render(plain, 8, 0)                         # warm-up
     rows = {}
@@ -133,17 +136,23 @@ def equal_spp(scene, ref, spp, variants, seeds=2, max_depth=None, seed_stride=1 
     plain.close()
     rows["plain"] = {"relmse": float(np.mean(r)), "ms": float(np.mean(t)), "per_seed": [float(x) for x in r]}
     for name, cfg in variants.items():
+        guide, cache = (cfg.get("guide"), cfg.get("cache")) if isinstance(cfg, dict) else (cfg, None)
         it = load_scene(scene, flags=FLAGS, max_depth=max_depth)
-        r, t, tr = [], [], []
+        r, t, tr, b = [], [], [], []
         for k in range(seeds):
-            it.setGuiding(cfg)
+            if guide is not None:
+                it.setGuiding(guide)
+            if cache is not None:
+                it.setRadianceCache(cache)
             img, ms = _render(it, spp, (k + 1) * seed_stride)
             r.append(relmse(img, ref))
             t.append(ms)
-            tr.append(it.guideStats()["ms_train"])
+            b.append(float((img.mean() - ref.mean()) / ref.mean()))
+            tr.append((it.guideStats()["ms_train"] if guide is not None else 0.0) +
+                      (it.cacheStats()["ms_train"] if cache is not None else 0.0))
         it.close()
         rows[name] = {"relmse": float(np.mean(r)), "ms": float(np.mean(t)), "train_ms": float(np.mean(tr)),
-                      "per_seed": [float(x) for x in r]}
+                      "per_seed": [float(x) for x in r], "bias": [round(x, 5) for x in b]}
     p = rows["plain"]
     for name, v in rows.items():
         v["spp_ratio"] = p["relmse"] / v["relmse"]

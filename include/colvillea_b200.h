@@ -521,6 +521,10 @@ typedef struct cl_guide_config
                                               the camera ray's hit included; 2 = indirect vertices only);
                                               shallower vertices sample the BSDF alone and are neither
                                               inferred nor recorded (0 or 1: every vertex) */
+    float    min_alpha;                    /* guided conductor and dielectric vertices: GGX alpha (after
+                                              textures) >= min_alpha; smoother ones sample the BSDF alone
+                                              and are not recorded; diffuse vertices are not affected
+                                              (0 = every vertex of the guided classes) */
 } cl_guide_config;
 
 typedef struct cl_guide_stats

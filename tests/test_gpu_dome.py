@@ -71,3 +71,58 @@ def test_alias_sampler_pdf_and_distribution(dome_scene):
     p = sst.chi2.sf(chi2, keep.sum() - 1)
     print(f"[alias] chi2 {chi2:.1f} over {keep.sum()} cells, p = {p:.3g}")
     assert p > 1e-4
+
+
+def dome_tables_fp64(tex):
+    """The tables of one dome in FP64 (numpy), for the two device paths."""
+    h, w = tex.shape[:2]
+    t = tex.astype(np.float64)
+    lum = t[..., 0] * 0.212671 + t[..., 1] * 0.71516 + t[..., 2] * 0.072169
+    wgt = np.sin(np.pi * (np.arange(h) + 0.5) / h)[:, None] * lum
+    rows = wgt.sum(axis=1)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        cdf = np.where(rows[:, None] > 0, np.cumsum(wgt, axis=1) / rows[:, None], np.arange(1, w + 1) / w)
+        pdf = np.where(rows[:, None] > 0, wgt / rows[:, None], 1.0 / w)
+    rc = rows / w
+    return wgt, cdf, pdf, rc, np.cumsum(rc) / rc.sum(), rc / rc.sum()
+
+
+def alias_row_mass(col, w, h):
+    prob = col[0::2].view(np.float32).astype(np.float64).reshape(h, w)
+    alias = col[1::2].astype(np.int64).reshape(h, w)
+    assert np.all((prob >= 0) & (prob <= 1)) and np.all((alias >= 0) & (alias < w))
+    mass = prob.copy()
+    np.add.at(mass, (np.broadcast_to(np.arange(h)[:, None], (h, w)), alias), 1.0 - prob)
+    return mass / w
+
+
+@pytest.mark.parametrize("w,h", [(16384, 12), (20480, 6)], ids=["block-per-row", "thread-per-row"])
+def test_wide_rows_both_paths(w, h):
+    """Rows of 16,384 texels take the shared-memory kernels (one block per
+    row), wider ones the thread-per-row kernels; both against FP64 numpy,
+    with a black row and a black band of columns."""
+    rng = np.random.default_rng(w)
+    tex = scenes.hdri(w, h, [(d, 2.0, 300.0) for d in scenes.random_upper_dirs(rng, 4)], rng)
+    tex[h // 2] = 0.0
+    tex[:, w // 5: w // 5 + 700] = 0.0
+    it = cb.Integrator.createIntegrator(cb.IntegratorType.WavefrontPathTracing, 8, 8)
+    try:
+        it.buildEmitters([scenes.Emitter(scenes.EMIT_DOME, texels=tex)])
+        pU, cU, pV, cV = it.domeTables(w, h)
+        ar, ac = it.domeAliasTables(w, h)
+    finally:
+        it.close()
+    wgt, cdf, pdf, rc, cdfV, pdfV = dome_tables_fp64(tex)
+    pU = pU.reshape(h, w + 1); cU = cU.reshape(h, w + 1)
+    np.testing.assert_allclose(pU[:, :w], wgt, rtol=3e-7, atol=0)
+    np.testing.assert_allclose(pU[:, w], rc, rtol=3e-7, atol=0)
+    np.testing.assert_allclose(cU[:, 1:], cdf, rtol=3e-7, atol=1e-12)
+    assert np.all(cU[:, 0] == 0) and np.all(cU[:, w] == 1) and np.all(np.diff(cU, axis=1) >= 0)
+    assert np.all(pU[h // 2] == 0)
+    np.testing.assert_allclose(pV[:h], rc, rtol=3e-7, atol=0)
+    np.testing.assert_allclose(cV[1:], cdfV, rtol=3e-7, atol=1e-12)
+    assert cV[0] == 0 and cV[h] == 1 and np.all(np.diff(cV) >= 0)
+    np.testing.assert_allclose(alias_row_mass(ac, w, h), pdf, rtol=1e-4, atol=1e-12)
+    np.testing.assert_allclose(alias_row_mass(ar, h, 1)[0], pdfV, rtol=1e-4, atol=1e-12)
+    black = ac.reshape(h, w, 2)[h // 2]
+    assert np.all(black[:, 1] == np.arange(w)) and np.all(black[:, 0].view(np.float32) == 1.0)
