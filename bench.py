@@ -62,6 +62,9 @@ def parse():
                     help="guiding variants at equal spp against an FP64 reference (one JSON line): on cfg3 "
                          "guided BSDF classes and selection probabilities; on cfg4/cfg5 the same with the "
                          "radiance cache (see --study-config)")
+    ap.add_argument("--cache-study", action="store_true",
+                    help="with --guide-study on cfg4/cfg5: radiance-cache training variants (steps, batch, "
+                         "learning rate) instead of the guiding variants")
     ap.add_argument("--study-config", type=int, default=3, choices=[3, 4, 5],
                     help="scene of --guide-study (3: guiding alone; 4, 5: radiance cache with and without guiding)")
     ap.add_argument("--relmse-ref-spp", type=int, default=8192, help="spp of the cfg3 FP64 reference image")
@@ -364,14 +367,17 @@ def run_guide_study(args):
     if args.study_config == 3:
         sc, spp, ref_spp = scenes.config3(0), args.relmse_spp, args.relmse_ref_spp
         variants = {
+            "guided_all_classes_bsdf_fraction_0.5": G(),
+            "guided_all_classes_bsdf_fraction_0.5_indirect_only": G(min_depth=2),
+            "guided_all_classes_bsdf_fraction_0.5_64_training_steps": G(train_spp=64),
+            "guided_all_classes_learned_selection": G(learn_selection=1),
+            "guided_diffuse_conductor_bsdf_fraction_0.5": G(class_mask=3),
+            "guided_all_classes_bsdf_fraction_0.8": G(bsdf_fraction=0.8),
+            "guided_all_classes_bsdf_fraction_0.8_min_alpha_0.1": G(bsdf_fraction=0.8, min_alpha=0.1),
+            "guided_dielectric_only_bsdf_fraction_0.5": G(class_mask=4),
             "guided_dielectric_only_bsdf_fraction_0.8": G(class_mask=4, bsdf_fraction=0.8),
             "guided_dielectric_only_bsdf_fraction_0.9": G(class_mask=4, bsdf_fraction=0.9),
-            "guided_dielectric_only_bsdf_fraction_0.8_batch2^19": G(class_mask=4, bsdf_fraction=0.8, batch=1 << 19),
-            "guided_dielectric_only_bsdf_fraction_0.8_lr3e-3": G(class_mask=4, bsdf_fraction=0.8, learning_rate=3e-3),
-            "guided_all_classes_bsdf_fraction_0.9": G(class_mask=7, bsdf_fraction=0.9),
             "guided_dielectric_conductor_bsdf_fraction_0.8": G(class_mask=6, bsdf_fraction=0.8),
-            "guided_all_classes_bsdf_fraction_0.5_min_alpha_0.1": G(min_alpha=0.1),
-            "guided_all_classes_bsdf_fraction_0.8_min_alpha_0.1": G(bsdf_fraction=0.8, min_alpha=0.1),
         }
         label = "cfg3 (cfg1 scene, 1920x1080, depth 5, RR 3)"
     else:
@@ -379,6 +385,13 @@ def run_guide_study(args):
         spp = args.relmse_spp if args.study_config == 4 else args.ext_spp5
         ref_spp = args.relmse_ref_spp4 if args.study_config == 4 else args.ext_ref_spp5
         variants = {
+            "cache": {"cache": C()},
+            "cache_128_training_steps": {"cache": C(train_spp=128)},
+            "cache_every_spp_training": {"cache": C(train_spp=spp)},
+            "cache_batch_2^20": {"cache": C(network={"batch": 1 << 20})},
+            "cache_every_spp_training_lr_3e-3": {"cache": C(train_spp=spp, network={"learning_rate": 3e-3})},
+            "cache_every_spp_training_beta2_0.999": {"cache": C(train_spp=spp, network={"beta2": 0.999})},
+        } if args.cache_study else {
             "cache": {"cache": C()},
             "cache_guided_all_classes_bsdf_fraction_0.5": {"cache": C(), "guide": G()},
             "cache_guided_diffuse_conductor_bsdf_fraction_0.5": {"cache": C(), "guide": G(class_mask=3)},
@@ -406,12 +419,14 @@ def run_guide_study(args):
 
 def run_extended(args):
     """The neural configurations not in the default line (one JSON line):
-      cfg4: the caustic scene with the radiance cache plus guiding, and the
-            cache alone, at equal time against plain, relMSE and bias
-            against a 65,536-spp FP64 plain reference;
+      cfg4: the caustic scene with the radiance cache plus guiding (library
+            defaults and the studies' guiding configuration), and the cache
+            alone, at equal time against plain, relMSE and bias against a
+            65,536-spp FP64 plain reference;
       cfg5: 3840x2160, depth 16, the instanced terrain scene with guiding and
-            the radiance cache both on: equal-time relMSE against plain
-            (FP64 reference), and the guiding network's inference throughput."""
+            the radiance cache both on (library defaults, and the studies'
+            configuration): equal-time relMSE against plain (FP64
+            reference), and the guiding network's inference throughput."""
     import colvillea_b200 as cb
     from colvillea_b200 import evaluate, scenes
     rnd = lambda v: [round(x, 6) for x in v] if isinstance(v, list) else (round(v, 6) if isinstance(v, float) else v)
@@ -424,12 +439,17 @@ def run_extended(args):
     t0 = time.perf_counter()
     ref4 = evaluate.reference(s4, args.ext_ref_spp4)
     t4 = time.perf_counter() - t0
-    for name, g in (("cfg4_cache_guided", cb.GuideConfig()), ("cfg4_cache", None)):
+    # As specified (guiding with the library's defaults on top of the cache), the cache alone, and the cache with
+    # the guiding configuration of the equal-spp studies (rough-dielectric vertices, selection probability 0.2).
+    tuned_guide = dict(class_mask=4, bsdf_fraction=0.8)
+    for name, g, label in (("cfg4_cache_guided", cb.GuideConfig(), "radiance cache + guiding (defaults)"),
+                           ("cfg4_cache", None, "radiance cache"),
+                           ("cfg4_cache_guided_tuned", cb.GuideConfig(**tuned_guide),
+                            "radiance cache + guiding (rough dielectric only, BSDF fraction 0.8)")):
         r = evaluate.equal_time(s4, ref4, args.relmse_spp, seeds=args.relmse_seeds, guide=g,
                                 cache=cb.RadianceCacheConfig())
         out[name] = {"reference": f"plain, corrected estimator, {args.ext_ref_spp4} spp, FP64 film ({t4:.1f} s)",
-                     "networks": "radiance cache + guiding" if g is not None else "radiance cache",
-                     **{k: rnd(v) for k, v in r.items()}}
+                     "networks": label, **{k: rnd(v) for k, v in r.items()}}
     s5 = scenes.config5(0)
     t0 = time.perf_counter()
     ref5 = evaluate.reference(s5, args.ext_ref_spp5)
@@ -445,6 +465,15 @@ def run_extended(args):
         **{k: rnd(v) for k, v in r5.items()},
         "mlp": {**{k: rnd(v) for k, v in mlp.items()}, "bf16_peak_tflops": peak,
                 "infer_frac_of_peak": round(mlp["infer_tflops"] / peak, 4) if peak and mlp["infer_tflops"] else None}}
+    # Both networks on, configured by the cfg5 studies (bench.py --guide-study [--cache-study] --study-config 5):
+    # the cache trained for the first 128 spp, guiding on the rough-dielectric vertices only.
+    c5 = cb.RadianceCacheConfig(train_spp=128)
+    r5t = evaluate.equal_time(s5, ref5, args.ext_spp5, seeds=args.relmse_seeds, guide=cb.GuideConfig(**tuned_guide),
+                              cache=c5)
+    out["cfg5_guided_cached_tuned"] = {
+        "workload": f"cfg5 as above; radiance cache trained for the first {c5.train_spp} spp, guiding on the rough-"
+                    f"dielectric vertices only (BSDF fraction 0.8); plain at the same device time",
+        "reference": out["cfg5_guided_cached"]["reference"], **{k: rnd(v) for k, v in r5t.items()}}
     print(json.dumps(out))
     return 0
 

@@ -884,7 +884,8 @@ cl_status buildWideBvh(const float* dTri9, uint32_t n, cudaStream_t st, WideBvh*
         }
         if (m == 1)
         {
-            CL_CUDA(cudaMemcpy(&rootRef, C.p, 4, cudaMemcpyDeviceToHost), err);
+            CL_CUDA(cudaMemcpyAsync(&rootRef, C.p, 4, cudaMemcpyDeviceToHost, st), err);
+            CL_CUDA(cudaStreamSynchronize(st), err);
             out->buildIterations = iters;
         }
         else

@@ -26,6 +26,9 @@
 // (src/kernel/integrators/raygeneration.cu:59-456, src/core/devices/optix.cu:112-284);
 // Russian roulette is added (absent from the reference, path.cpp:135).
 #include "cl_integrator.h"
+
+#include <atomic>
+#include <thread>
 #include "cl_mlp_tc.cuh"
 
 #include <chrono>
@@ -1536,7 +1539,7 @@ cl_status Integrator::uploadMeshPool(uint32_t meshId, std::string* err)
     return CL_OK;
 }
 
-cl_status Integrator::buildBlas(uint32_t meshId, BuildArena* arena, std::string* err)
+cl_status Integrator::buildBlas(uint32_t meshId, BuildArena* arena, cudaStream_t st, std::string* err)
 {
     const HostMesh&    m  = meshes_[meshId];
     const size_t       mt = m.idx.size() / 3;
@@ -1548,9 +1551,73 @@ cl_status Integrator::buildBlas(uint32_t meshId, BuildArena* arena, std::string*
     BuildArena& mem = arena ? *arena : local;
     ScratchBuf  d;
     CL_TRY(mem.input(d, tri9.size() * 4, err));
-    CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, stream_), err);
+    CL_CUDA(cudaMemcpyAsync(d.p, tri9.data(), tri9.size() * 4, cudaMemcpyHostToDevice, st), err);
     if (!blas_[meshId]) blas_[meshId].reset(new WideBvh());
-    return buildWideBvh(d.f(), uint32_t(mt), stream_, blas_[meshId].get(), err, &mem);
+    return buildWideBvh(d.f(), uint32_t(mt), st, blas_[meshId].get(), err, &mem);
+}
+
+// The trees of the instanced meshes.  They are independent, and each build
+// waits on the host for its own small launches (cluster counts, collapse
+// levels), so up to kBuildThreads host threads build them at once, each on
+// its own stream with its own build arena.  Returns after every build ended.
+cl_status Integrator::buildBlasAll(const std::vector<uint32_t>& meshes, std::string* err)
+{
+    constexpr unsigned kBuildThreads = 4;
+    const unsigned     nw            = unsigned(std::min<size_t>(kBuildThreads, meshes.size()));
+    for (uint32_t m : meshes)
+        if (!blas_[m]) blas_[m].reset(new WideBvh());
+    if (nw <= 1)
+    {
+        BuildArena arena;
+        for (uint32_t m : meshes) CL_TRY(buildBlas(m, &arena, stream_, err));
+        return CL_OK;
+    }
+    int dev = 0;
+    CL_CUDA(cudaGetDevice(&dev), err);
+    std::atomic<size_t>      next{0};
+    std::atomic<bool>        failed{false};
+    std::vector<cl_status>   res(nw, CL_OK);
+    std::vector<std::string> msg(nw);
+    std::vector<double>      allocs(nw, 0.0);
+    std::vector<std::thread> workers;
+    for (unsigned w = 0; w < nw; ++w)
+        workers.emplace_back([&, w] {
+            cudaStream_t s = nullptr;
+            if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+            {
+                cudaGetLastError();
+                res[w] = CL_ERR_CUDA;
+                msg[w] = "two-level build: no stream for a build thread";
+                failed = true;
+                return;
+            }
+            const double a0 = allocMs();
+            {
+                BuildArena arena;
+                for (size_t k; !failed && (k = next++) < meshes.size();)
+                {
+                    const cl_status r = buildBlas(meshes[k], &arena, s, &msg[w]);
+                    if (r != CL_OK)
+                    {
+                        res[w] = r;
+                        failed = true;
+                        break;
+                    }
+                }
+                cudaStreamSynchronize(s); // before the arena's temporaries are freed
+            }
+            allocs[w] = allocMs() - a0;
+            cudaStreamDestroy(s);
+        });
+    for (auto& t : workers) t.join();
+    for (unsigned w = 0; w < nw; ++w) allocMs() += allocs[w];
+    for (unsigned w = 0; w < nw; ++w)
+        if (res[w] != CL_OK)
+        {
+            *err = msg[w];
+            return res[w];
+        }
+    return CL_OK;
 }
 
 // World box of instance i (every vertex mapped, in double), widened by a
@@ -1701,12 +1768,13 @@ cl_status Integrator::buildTwoLevel(const cl_instance_desc* inst, uint32_t n, st
     std::vector<bool> used(nm, false);
     for (uint32_t i = 0; i < n; ++i) used[inst[i].mesh_id] = true;
     blas_.clear();
-    blas_.resize(nm);  // null entries
-    BuildArena arena;  // the builds' temporaries, allocated once for all the meshes
+    blas_.resize(nm); // null entries
+    std::vector<uint32_t> todo;
     for (uint32_t m = 0; m < nm; ++m)
-        if (used[m]) CL_TRY(buildBlas(m, &arena, err));
+        if (used[m]) todo.push_back(m);
+    CL_TRY(buildBlasAll(todo, err));
     inst_.assign(inst, inst + n);
-    CL_TRY(buildTopLevel(&arena, err));
+    CL_TRY(buildTopLevel(nullptr, err));
     CL_TRY(uploadInstances(err));
     CL_CUDA(cudaEventRecord(evB_, stream_), err);
     CL_CUDA(cudaEventSynchronize(evB_), err);
@@ -1736,7 +1804,7 @@ cl_status Integrator::updateTwoLevel(uint32_t meshId, uint32_t mode, std::string
     {
         if (mode == CL_BVH_UPDATE_REBUILD)
         {
-            CL_TRY(buildBlas(meshId, nullptr, err));
+            CL_TRY(buildBlas(meshId, nullptr, stream_, err));
             ++rebuilds_;
         }
         else

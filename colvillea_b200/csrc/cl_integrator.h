@@ -237,7 +237,8 @@ private:
     uint32_t               twoLevelStack_ = 0;
     cl_status buildTwoLevel(const cl_instance_desc* inst, uint32_t n, std::string* err);
     cl_status uploadMeshPool(uint32_t meshId, std::string* err);
-    cl_status buildBlas(uint32_t meshId, BuildArena* arena, std::string* err);
+    cl_status buildBlas(uint32_t meshId, BuildArena* arena, cudaStream_t st, std::string* err);
+    cl_status buildBlasAll(const std::vector<uint32_t>& meshes, std::string* err);
     cl_status buildTopLevel(BuildArena* arena, std::string* err);
     cl_status uploadInstances(std::string* err);
     cl_status updateTwoLevel(uint32_t meshId, uint32_t mode, std::string* err);
