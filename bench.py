@@ -581,8 +581,9 @@ def main():
         st = it.stats()
         ms_dev += st["ms_last_render"]
         rays_c += st["last_rays_closest"]; rays_s += st["last_rays_shadow"]
-        # kRaygen, then per wave: kTraceClosest, 4 x kShade, kTraceShadow, kShadowResolve, kAdvance
-        launches += 1 + 8 * st["waves"]
+        # kRaygen, then per wave: kTraceClosest, kClassifyHits (flattened scenes), 4 x kShade, kTraceShadow,
+        # kShadowResolve, kAdvance
+        launches += 1 + (8 if two else 9) * st["waves"]
     ev1.record()
     torch.cuda.synchronize()
     clk = clocks.stop()

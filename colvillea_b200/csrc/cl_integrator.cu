@@ -354,13 +354,6 @@ __device__ __forceinline__ void warpStats(const TraceCounters& tc, unsigned long
     }
 }
 
-// Closest-hit traversal of a ray queue.  Persistent warps fetch 32
-// consecutive rays at a time (one atomicAdd per warp) and each lane runs its
-// ray to completion.  (Refilling finished lanes mid-warp was measured slower
-// on B200: the per-step warp vote forces reconvergence and raised the
-// instruction count by half.)  CLASSIFY: the finished batch is appended to
-// the four shading-class queues (the hit material's BSDF type, or escaped),
-// so that each shading kernel runs one BSDF per warp.
 // Resident blocks per SM of the two-level traversal kernels (their state is
 // larger than the flattened traversal's; 8 blocks would spill).
 constexpr int kTraceBlocksTwo = 5;
@@ -376,8 +369,99 @@ struct ClassifyView
 
 constexpr int kClassEscaped = 3;
 
-// TWO: two-level scene (CL_TWO_LEVEL); the hit's triangle index entry then
-// holds the object-space vertex ids and the instance index (its .w).
+// Shading class of a finished closest-hit ray (-1: none), with the hit's
+// triangle index entry written for the shading kernels.
+template <bool TWO>
+__device__ __forceinline__ int classifyHit(const BvhView& bvh, const ClassifyView& cv, uint32_t i, uint32_t prim,
+                                           uint32_t inst, uint32_t loc)
+{
+    if (prim == kMissPrim) return kClassEscaped;
+    if (TWO)
+    {
+        const InstDev* ip = bvh.inst + inst;
+        uint4          ti = __ldg(&cv.triIdx[__ldg(&ip->triBase) + loc]);
+        ti.w              = inst;
+        cv.hitIdx[i]      = ti;
+        return int(__float_as_uint(__ldg(&cv.mats[kMatF4 * __ldg(&ip->material)].x)));
+    }
+    const uint4 ti = __ldg(&cv.triIdx[prim]);
+    cv.hitIdx[i]   = ti;
+    return int(__float_as_uint(__ldg(&cv.mats[kMatF4 * ti.w].x)));
+}
+
+// Appends ray i of each lane with cls >= 0 to its class queue (every lane of
+// the warp calls it; one atomicAdd per class and warp).
+__device__ __forceinline__ void appendClasses(Counters* ctr, const ClassifyView& cv, int cls, uint32_t i)
+{
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+    {
+        uint32_t k = warpAppend(&ctr->classCount[c], cls == c);
+        if (cls == c)
+        {
+            if (k < cv.cap)
+                cv.classIdx[size_t(c) * cv.cap + k] = i;
+            else
+                atomicOr(&ctr->error, 8u);
+        }
+    }
+}
+
+// Warp-local supply of queue entries for the persistent traversal kernels.
+// A warp takes 32 consecutive entries per atomicAdd and hands them to its
+// idle lanes in lane order, so that a lane whose ray has finished takes the
+// next ray while the others continue (the warp no longer waits for its
+// longest ray), and the rays of a warp stay within a few chunks of the queue.
+// The warp's unstarted entries [x, y) live in shared memory (they are only
+// touched when lanes are refilled); x = kMissPrim: the queue is exhausted.
+__device__ __forceinline__ void supplyInit(uint2* ws)
+{
+    if (laneId() == 0u) *ws = make_uint2(0u, 0u);
+    __syncwarp();
+}
+
+// Every lane calls it with the same `want` (the lanes to supply); returns
+// the supplied lane's entry, kMissPrim for the others.
+__device__ __forceinline__ uint32_t supplyLanes(uint2* ws, uint32_t* fetch, uint32_t n, uint32_t want)
+{
+    const uint32_t lane = laneId(), lt = (1u << lane) - 1u;
+    uint2          w    = *ws;
+    uint32_t       item = kMissPrim;
+    while (want && w.x != kMissPrim)
+    {
+        if (w.x >= w.y)
+        {
+            const uint32_t nb = warpFetch(fetch);
+            w                 = nb >= n ? make_uint2(kMissPrim, kMissPrim) : make_uint2(nb, min(nb + 32u, n));
+            if (nb >= n) break;
+        }
+        const uint32_t avail = w.y - w.x, r = __popc(want & lt);
+        const bool     mine  = (want >> lane) & 1u;
+        if (mine && r < avail) item = w.x + r;
+        w.x += min(uint32_t(__popc(want)), avail);
+        want = __ballot_sync(kFull, mine && r >= avail);
+    }
+    __syncwarp();
+    if (lane == 0u) *ws = w;
+    __syncwarp();
+    return item;
+}
+
+// Ray indices of the wave queues stay below this (kTraceClosest and the
+// shadow kernel keep kMissPrim as their idle-lane mark).
+constexpr uint32_t kMaxPathSlots = 0x0fffffffu;
+
+// Closest-hit traversal of a ray queue by persistent warps.  Flattened
+// scenes: each lane traverses one ray at a time and takes the next from the
+// warp's supply when it finishes; the hits' shading classes are appended by
+// kClassifyHits afterwards, in ray order (a class lookup inside the step loop
+// would stall the whole warp on one lane's dependent gathers).  Two-level
+// scenes: the warp fetches 32 consecutive rays, each lane runs its ray to
+// completion, and CLASSIFY appends each finished ray to one of the four
+// shading-class queues (the hit material's BSDF type, or escaped), so that
+// each shading kernel runs one BSDF per warp.  TWO: two-level scene
+// (CL_TWO_LEVEL); the hit's triangle index entry then holds the object-space
+// vertex ids and the instance index (its .w).
 template <bool STATS, bool CLASSIFY, bool TWO = false>
 __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
                                                                 const float4* __restrict__ D, const uint32_t* count,
@@ -387,68 +471,134 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
     __shared__ uint4        top[kTopNodes * 5];
+    __shared__ uint2        supply[kTraceBlock / 32];
     stageTopNodes(bvh, top);
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(count);
     TraceCounters    tc{0u, 0u};
-    for (;;)
+    if constexpr (!TWO)
     {
-        uint32_t base = warpFetch(fetch);
-        if (base >= n) break;
-        uint32_t i    = base + laneId();
-        uint32_t prim = kMissPrim, inst = 0u, loc = 0u;
-        if (i < n)
+        // Idle lanes are refilled once at least kRefillIdle of them are idle.
+        uint2* ws = supply + (threadIdx.x >> 5);
+        supplyInit(ws);
+        Trav     s;
+        uint32_t ray = kMissPrim;
+        for (;;)
         {
-            float4 o = O[i], d = D[i];
-            float  t, b1, b2;
-            if (TWO)
+            const uint32_t idle = __ballot_sync(kFull, ray == kMissPrim);
+            if (uint32_t(__popc(idle)) >= kRefillIdle)
             {
+                if (ws->x != kMissPrim)
+                {
+                    const uint32_t item = supplyLanes(ws, fetch, n, idle);
+                    if (item != kMissPrim)
+                    {
+                        ray            = item;
+                        const float4 o = O[item], d = D[item];
+                        travInit(s, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w);
+                    }
+                }
+                if (__all_sync(kFull, ray == kMissPrim)) break;
+            }
+            if (ray != kMissPrim)
+                for (uint32_t k = 0; k < kRefillSteps; ++k)
+                    if (travStep<false, STATS>(bvh, s, stack + threadIdx.x, &tc, &ctr->error, keyLut, top))
+                    {
+                        hitOut[ray] = make_float4(s.bt, __uint_as_float(s.best), s.b1, s.b2);
+                        ray         = kMissPrim;
+                        break;
+                    }
+        }
+    }
+    else
+    {
+        for (;;)
+        {
+            uint32_t base = warpFetch(fetch);
+            if (base >= n) break;
+            uint32_t i    = base + laneId();
+            uint32_t prim = kMissPrim, inst = 0u, loc = 0u;
+            if (i < n)
+            {
+                float4 o = O[i], d = D[i];
+                float  t, b1, b2;
                 loc = traverse2<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2, &inst,
                                               stack + threadIdx.x, &tc, &ctr->error, keyLut);
                 if (loc != kMissPrim) prim = __ldg(&bvh.inst[inst].primBase) + loc;
+                hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
             }
-            else
-                prim = traverse<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                              stack + threadIdx.x, &tc, &ctr->error, keyLut, top);
-            hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
-        }
-        if (CLASSIFY)
-        {
-            int cls = -1;
-            if (i < n)
-            {
-                if (prim == kMissPrim)
-                    cls = kClassEscaped;
-                else if (TWO)
-                {
-                    const InstDev* ip = bvh.inst + inst;
-                    uint4          ti = __ldg(&cv.triIdx[__ldg(&ip->triBase) + loc]);
-                    ti.w              = inst;
-                    cv.hitIdx[i]      = ti;
-                    cls               = int(__float_as_uint(__ldg(&cv.mats[kMatF4 * __ldg(&ip->material)].x)));
-                }
-                else
-                {
-                    const uint4 ti = __ldg(&cv.triIdx[prim]);
-                    cv.hitIdx[i]   = ti;
-                    cls            = int(__float_as_uint(__ldg(&cv.mats[kMatF4 * ti.w].x)));
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-            {
-                uint32_t k = warpAppend(&ctr->classCount[c], cls == c);
-                if (cls == c)
-                {
-                    if (k < cv.cap)
-                        cv.classIdx[size_t(c) * cv.cap + k] = i;
-                    else
-                        atomicOr(&ctr->error, 8u);
-                }
-            }
+            if (CLASSIFY) appendClasses(ctr, cv, i < n ? classifyHit<true>(bvh, cv, i, prim, inst, loc) : -1, i);
         }
     }
     if (STATS) warpStats(tc, &ctr->statNodes, &ctr->statTris);
+}
+
+// Shading classes of a wave's closest hits (flattened scenes).  A block
+// takes tiles of kClassifyTile consecutive rays (kClassifyPer per thread,
+// in ray order), counts each class over the tile with warp ballots and a
+// block scan, reserves the tile's range of each class queue with one
+// atomicAdd per class, and writes the rays there in ray order; the hit's
+// triangle index entry is written for the shading kernels.  Grid-stride
+// over the wave's ray count (read on the device).
+constexpr int kClassifyThreads = 256;
+constexpr int kClassifyPer     = 4;
+constexpr int kClassifyTile    = kClassifyThreads * kClassifyPer;
+__global__ void __launch_bounds__(kClassifyThreads) kClassifyHits(BvhView bvh, const float4* __restrict__ hit,
+                                                                  const uint32_t* count, Counters* ctr, ClassifyView cv)
+{
+    constexpr int  kWarps = kClassifyThreads / 32;
+    __shared__ uint32_t wcount[kClassifyPer][kWarps][4]; // rays of class c in (round r, warp w)
+    __shared__ uint32_t cbase[4];
+    const uint32_t n = loadCount(count);
+    const uint32_t w = threadIdx.x >> 5, lane = laneId(), lt = (1u << lane) - 1u;
+    for (uint32_t tile = blockIdx.x * uint32_t(kClassifyTile); tile < n; tile += gridDim.x * uint32_t(kClassifyTile))
+    {
+        int cls[kClassifyPer];
+#pragma unroll
+        for (int r = 0; r < kClassifyPer; ++r)
+        {
+            const uint32_t i = tile + uint32_t(r * kClassifyThreads) + threadIdx.x;
+            cls[r]           = i < n ? classifyHit<false>(bvh, cv, i, __float_as_uint(__ldg(&hit[i].y)), 0u, 0u) : -1;
+        }
+        uint32_t rank[kClassifyPer];
+#pragma unroll
+        for (int r = 0; r < kClassifyPer; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                const uint32_t m = __ballot_sync(kFull, cls[r] == c);
+                if (cls[r] == c) rank[r] = __popc(m & lt);
+                if (lane == 0u) wcount[r][w][c] = __popc(m);
+            }
+        __syncthreads();
+        // Exclusive scan over (round, warp) per class, in ray order, by the first 4 threads; then the reservation.
+        if (threadIdx.x < 4u)
+        {
+            const int c   = int(threadIdx.x);
+            uint32_t  sum = 0u;
+            for (int r = 0; r < kClassifyPer; ++r)
+                for (int k = 0; k < kWarps; ++k)
+                {
+                    const uint32_t v = wcount[r][k][c];
+                    wcount[r][k][c]  = sum;
+                    sum += v;
+                }
+            cbase[c] = sum ? atomicAdd(&ctr->classCount[c], sum) : 0u;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kClassifyPer; ++r)
+            if (cls[r] >= 0)
+            {
+                const uint32_t i = tile + uint32_t(r * kClassifyThreads) + threadIdx.x;
+                const uint32_t k = cbase[cls[r]] + wcount[r][w][cls[r]] + rank[r];
+                if (k < cv.cap)
+                    cv.classIdx[size_t(cls[r]) * cv.cap + k] = i;
+                else
+                    atomicOr(&ctr->error, 8u);
+            }
+        __syncthreads();
+    }
 }
 
 // Shadow rays (any hit) of the shadow queue.  Item k is entry k (path
@@ -460,34 +610,76 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
     __shared__ uint4        top[kTopNodes * 5];
+    __shared__ uint2        supply[kTraceBlock / 32];
     stageTopNodes(P.sc.bvh, top);
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(&P.q.ctr->shadowCount) * (DL ? 2u : 1u);
     TraceCounters    tc{0u, 0u};
-    for (;;)
+    if constexpr (!TWO)
     {
-        uint32_t base = warpFetch(&P.q.ctr->fetchShadow);
-        if (base >= n) break;
-        uint32_t item = base + laneId();
-        if (item < n)
+        // Idle lanes refilled as in kTraceClosest.
+        uint2* ws = supply + (threadIdx.x >> 5);
+        supplyInit(ws);
+        Trav     s;
+        uint32_t ray = kMissPrim;
+        for (;;)
         {
-            uint32_t e  = DL ? item >> 1 : item;
-            float4   o4 = P.q.sqO[e];
-            float4   d4 = (DL && (item & 1u)) ? P.q.sqD2[e] : P.q.sqD[e];
-            uint8_t  v  = 0;
-            if (d4.w != 0.0f)
+            const uint32_t idle = __ballot_sync(kFull, ray == kMissPrim);
+            if (uint32_t(__popc(idle)) >= kRefillIdle)
             {
-                float    t, b1, b2;
-                uint32_t h, hi;
-                if (TWO)
-                    h = traverse2<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
-                                               &t, &b1, &b2, &hi, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
-                else
-                    h = traverse<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX,
-                                              &t, &b1, &b2, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut, top);
-                v = h == kMissPrim ? 1 : 0;
+                if (ws->x != kMissPrim)
+                {
+                    const uint32_t item = supplyLanes(ws, &P.q.ctr->fetchShadow, n, idle);
+                    if (item != kMissPrim)
+                    {
+                        const uint32_t e  = DL ? item >> 1 : item;
+                        const float4   o4 = P.q.sqO[e];
+                        const float4   d4 = (DL && (item & 1u)) ? P.q.sqD2[e] : P.q.sqD[e];
+                        if (d4.w != 0.0f)
+                        {
+                            ray = item;
+                            travInit(s, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX);
+                        }
+                        else
+                            P.q.vis[item] = 0; // no emitter sample on this entry
+                    }
+                }
+                if (__all_sync(kFull, ray == kMissPrim) && ws->x == kMissPrim) break;
             }
-            P.q.vis[item] = v;
+            if (ray != kMissPrim)
+                for (uint32_t k = 0; k < kRefillSteps; ++k)
+                    if (travStep<true, STATS>(P.sc.bvh, s, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut, top))
+                    {
+                        P.q.vis[ray] = s.best == kMissPrim ? 1 : 0;
+                        ray          = kMissPrim;
+                        break;
+                    }
+        }
+    }
+    else
+    {
+        for (;;)
+        {
+            uint32_t base = warpFetch(&P.q.ctr->fetchShadow);
+            if (base >= n) break;
+            uint32_t item = base + laneId();
+            if (item < n)
+            {
+                uint32_t e  = DL ? item >> 1 : item;
+                float4   o4 = P.q.sqO[e];
+                float4   d4 = (DL && (item & 1u)) ? P.q.sqD2[e] : P.q.sqD[e];
+                uint8_t  v  = 0;
+                if (d4.w != 0.0f)
+                {
+                    float    t, b1, b2;
+                    uint32_t hi;
+                    uint32_t h = traverse2<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps,
+                                                        FLT_MAX, &t, &b1, &b2, &hi, stack + threadIdx.x, &tc,
+                                                        &P.q.ctr->error, keyLut);
+                    v = h == kMissPrim ? 1 : 0;
+                }
+                P.q.vis[item] = v;
+            }
         }
     }
     if (STATS) warpStats(tc, &P.q.ctr->statNodesS, &P.q.ctr->statTrisS);
@@ -2091,6 +2283,11 @@ cl_status Integrator::clearFilm(std::string* err)
 cl_status Integrator::ensureQueues(std::string* err)
 {
     uint32_t slots = cfg_.path_slots ? cfg_.path_slots : (1u << 21);
+    if (slots > kMaxPathSlots)
+    {
+        *err = "path_slots " + std::to_string(slots) + " above the maximum " + std::to_string(kMaxPathSlots);
+        return CL_ERR_INVALID_ARG;
+    }
     if (slots == slots_ && rqO_[0].p) return CL_OK;
     size_t s = slots;
     for (int q = 0; q < 2; ++q)
@@ -2226,6 +2423,10 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
                              : (twoLevel_ ? kTraceClosest<false, true, true> : kTraceClosest<false, true, false>);
         k<<<tBlocks(), kTraceBlock, sb, stream_>>>(P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur],
                                                       &c->fetchTrace, P.q.hit, c, classifyView());
+        if (profile) CL_CUDA(cudaEventRecord(evS_[5], stream_), err);
+        if (!twoLevel_)
+            kClassifyHits<<<numSMs_ * 8, kClassifyThreads, 0, stream_>>>(P.sc.bvh, P.q.hit, &c->rayCount[cur], c,
+                                                                         classifyView());
     }
     if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
     const uint32_t gmask = guide_ ? guideCfg_.class_mask : 0u;
@@ -2438,14 +2639,15 @@ cl_status Integrator::renderPass(uint32_t spp, bool record, bool cacheTrain, std
                 CL_CUDA(cudaStreamSynchronize(stream_), err);
                 waveRays_.push_back(rc - waveRaysSeen_);
                 waveRaysSeen_ = rc;
-                float a = 0, b = 0, c = 0, d = 0;
-                CL_CUDA(cudaEventElapsedTime(&a, evS_[0], evS_[1]), err);
+                float a = 0, b = 0, c = 0, d = 0, e = 0;
+                CL_CUDA(cudaEventElapsedTime(&a, evS_[0], evS_[5]), err);
+                CL_CUDA(cudaEventElapsedTime(&e, evS_[5], evS_[1]), err);
                 CL_CUDA(cudaEventElapsedTime(&d, evS_[1], evS_[4]), err);
                 CL_CUDA(cudaEventElapsedTime(&b, evS_[4], evS_[2]), err);
                 CL_CUDA(cudaEventElapsedTime(&c, evS_[2], evS_[3]), err);
                 msTrace_ += a;
                 msInfer_ += d;
-                msShade_ += b;
+                msShade_ += b + e;
                 msShadow_ += c;
             }
         }
@@ -3024,6 +3226,9 @@ cl_status Integrator::guideProbe(uint32_t cap, float* rows, uint32_t* count, std
     (twoLevel_ ? kTraceClosest<false, true, true> : kTraceClosest<false, true, false>)
         <<<tBlocks(), kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
             P.sc.bvh, P.q.rqO[0], P.q.rqD[0], &c->rayCount[0], &c->fetchTrace, P.q.hit, c, classifyView());
+    if (!twoLevel_)
+        kClassifyHits<<<numSMs_ * 8, kClassifyThreads, 0, stream_>>>(P.sc.bvh, P.q.hit, &c->rayCount[0], c,
+                                                                     classifyView());
     kGuideInfer<<<inferBlocks_, guide::kTcThreads, kGuideMlpSmem, stream_>>>(
         P, guide_->grid(), 0, guide_->tcWeights(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
     CL_CUDA(cudaGetLastError(), err);

@@ -96,7 +96,7 @@ typedef struct
     uint32_t rr_start_depth; /* Russian roulette from this path depth on; 0 = off */
     uint32_t flags;          /* CL_COMPAT_*, CL_DOME_ALIAS, CL_FILM_FP64, CL_PROFILE_STAGES, CL_TRACE_STATS,
                                 CL_TWO_LEVEL */
-    uint32_t path_slots;     /* paths in flight; 0 = automatic */
+    uint32_t path_slots;     /* paths in flight; 0 = automatic (2^21); at most 2^28 - 1 */
 } cl_render_config;
 
 /* A triangle mesh (TriMesh, include/colvillea/libkernel/shapes/trimesh.h:16-32).
@@ -218,8 +218,8 @@ typedef struct
     float    ms_bvh_build;
     float    ms_dome_build;
     float    ms_last_render; /* device time of the last cl_render */
-    float    ms_trace;       /* last render, CL_PROFILE_STAGES: closest-hit kernels */
-    float    ms_shade;       /* ... shading kernels */
+    float    ms_trace;       /* last render, CL_PROFILE_STAGES: the closest-hit traversal kernel */
+    float    ms_shade;       /* ... shading-class queues and shading kernels */
     float    ms_shadow;      /* ... shadow kernels */
     uint32_t launches;       /* last render: closest-hit kernel launches */
     uint32_t pad;
