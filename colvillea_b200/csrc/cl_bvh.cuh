@@ -64,10 +64,6 @@ struct BvhView
     // kernels' dynamic shared memory is stackDepth * kTraceBlock * 8 bytes,
     // so that a shallow tree leaves more of the SM's on-chip memory to L1.
     uint32_t stackDepth;
-    // Nodes [0, topNodes) - the root and its children, at most kTopNodes - are
-    // staged in each traversal block's shared memory (flattened scenes; 0 in
-    // two-level ones).
-    uint32_t topNodes;
 };
 
 // Lane refill in the persistent traversal kernels of flattened scenes: a lane
@@ -82,16 +78,6 @@ constexpr uint32_t kRefillIdle  = 4;
 constexpr uint32_t kRefillSteps = 4;
 
 __host__ __device__ constexpr size_t traceStackBytes(uint32_t depth) { return size_t(depth) * kTraceBlock * 8u; }
-
-constexpr uint32_t kTopNodes = 9; // the root and its (at most 8) children
-
-// Copies the staged top nodes into shared memory (every thread of the block
-// takes part; the caller's __syncthreads makes them visible).
-__device__ __forceinline__ void stageTopNodes(const BvhView& bvh, uint4* top)
-{
-    const uint32_t n = min(bvh.topNodes, kTopNodes) * 5u;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) top[i] = __ldg(bvh.nodes + i);
-}
 
 struct TraceCounters
 {
@@ -145,20 +131,10 @@ __device__ __forceinline__ void fillKeyLut(uint8_t* lut)
 // bits 24..31 inner-child keys (slot ^ octant), bits 0..23 triangle offsets.
 __device__ __forceinline__ uint32_t intersectNode(const uint4* __restrict__ nodes, uint32_t idx, f3 o, f3 inv, uint32_t oct,
                                                   float tmin, float tmax, uint32_t* childBase, uint32_t* triBase,
-                                                  uint32_t* imaskOut, const uint8_t* keyLut, const uint4* top = nullptr,
-                                                  uint32_t topCount = 0u)
+                                                  uint32_t* imaskOut, const uint8_t* keyLut)
 {
-    uint4 n0, n1, n2, n3, n4;
-    if (idx < topCount)
-    {
-        const uint4* np = top + idx * 5u;
-        n0 = np[0], n1 = np[1], n2 = np[2], n3 = np[3], n4 = np[4];
-    }
-    else
-    {
-        const uint4* np = nodes + size_t(idx) * 5;
-        n0 = __ldg(np + 0), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
-    }
+    const uint4* np = nodes + size_t(idx) * 5;
+    const uint4  n0 = __ldg(np + 0), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
     float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
     float sx = __uint_as_float((n0.w & 0xffu) << 23);
     float sy = __uint_as_float(((n0.w >> 8) & 0xffu) << 23);
@@ -249,7 +225,7 @@ __device__ __forceinline__ void travInit(Trav& s, f3 o, f3 d, float tmin, float 
 // finished (s.best: primitive id or kMissPrim; s.bt, s.b1, s.b2).
 template <bool ANY, bool STATS>
 __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* stack, TraceCounters* cnt, uint32_t* err,
-                                         const uint8_t* keyLut, const uint4* top)
+                                         const uint8_t* keyLut)
 {
     if (s.tg.y == 0u && s.ng.y > 0x00ffffffu)
     {
@@ -270,8 +246,7 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
             ++s.sp;
         }
         uint32_t cb, tb, im;
-        uint32_t hits = intersectNode(bvh.nodes, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im, keyLut, top,
-                                      min(bvh.topNodes, kTopNodes));
+        uint32_t hits = intersectNode(bvh.nodes, child, s.pre.o, s.inv, s.oct, s.tmin, s.bt, &cb, &tb, &im, keyLut);
         if (STATS) cnt->nodes++;
         s.ng = make_uint2(cb, (hits & 0xff000000u) | im);
         s.tg = make_uint2(tb, hits & 0x00ffffffu);
@@ -320,11 +295,11 @@ __device__ __forceinline__ bool travStep(const BvhView& bvh, Trav& s, uint2* sta
 template <bool ANY, bool STATS>
 __device__ __forceinline__ uint32_t traverse(const BvhView& bvh, f3 o, f3 d, float tmin, float tmax, float* tHit,
                                              float* b1Hit, float* b2Hit, uint2* stack, TraceCounters* cnt,
-                                             uint32_t* err, const uint8_t* keyLut, const uint4* top)
+                                             uint32_t* err, const uint8_t* keyLut)
 {
     Trav s;
     travInit(s, o, d, tmin, tmax);
-    while (!travStep<ANY, STATS>(bvh, s, stack, cnt, err, keyLut, top))
+    while (!travStep<ANY, STATS>(bvh, s, stack, cnt, err, keyLut))
     {
     }
     *tHit  = s.bt;

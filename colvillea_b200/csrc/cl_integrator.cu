@@ -354,9 +354,12 @@ __device__ __forceinline__ void warpStats(const TraceCounters& tc, unsigned long
     }
 }
 
-// Resident blocks per SM of the two-level traversal kernels (their state is
-// larger than the flattened traversal's; 8 blocks would spill).
-constexpr int kTraceBlocksTwo = 5;
+// Resident blocks per SM of the traversal kernels.  Flattened scenes: 7
+// (72 registers; 8 blocks at 64 registers was 3% slower on config 2 with the
+// lane refill, 6 blocks the same as 7).  Two-level scenes: 5 (their state is
+// larger; 8 blocks would spill).
+constexpr int kTraceBlocksFlat = 7;
+constexpr int kTraceBlocksTwo  = 5;
 
 struct ClassifyView
 {
@@ -463,16 +466,14 @@ constexpr uint32_t kMaxPathSlots = 0x0fffffffu;
 // (CL_TWO_LEVEL); the hit's triangle index entry then holds the object-space
 // vertex ids and the instance index (its .w).
 template <bool STATS, bool CLASSIFY, bool TWO = false>
-__global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
+__global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : kTraceBlocksFlat) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
                                                                 const float4* __restrict__ D, const uint32_t* count,
                                                                 uint32_t* fetch, float4* __restrict__ hitOut,
                                                                 Counters* ctr, ClassifyView cv)
 {
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
-    __shared__ uint4        top[kTopNodes * 5];
     __shared__ uint2        supply[kTraceBlock / 32];
-    stageTopNodes(bvh, top);
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(count);
     TraceCounters    tc{0u, 0u};
@@ -502,7 +503,7 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
             }
             if (ray != kMissPrim)
                 for (uint32_t k = 0; k < kRefillSteps; ++k)
-                    if (travStep<false, STATS>(bvh, s, stack + threadIdx.x, &tc, &ctr->error, keyLut, top))
+                    if (travStep<false, STATS>(bvh, s, stack + threadIdx.x, &tc, &ctr->error, keyLut))
                     {
                         hitOut[ray] = make_float4(s.bt, __uint_as_float(s.best), s.b1, s.b2);
                         ray         = kMissPrim;
@@ -605,13 +606,11 @@ __global__ void __launch_bounds__(kClassifyThreads) kClassifyHits(BvhView bvh, c
 // tracing) or ray k&1 of entry k>>1 (direct lighting, two rays per entry).
 // vis[k] = 1 when the ray reaches its light, 0 otherwise.
 template <bool DL, bool STATS, bool TWO = false>
-__global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTraceShadow(Params P)
+__global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : kTraceBlocksFlat) kTraceShadow(Params P)
 {
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
-    __shared__ uint4        top[kTopNodes * 5];
     __shared__ uint2        supply[kTraceBlock / 32];
-    stageTopNodes(P.sc.bvh, top);
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(&P.q.ctr->shadowCount) * (DL ? 2u : 1u);
     TraceCounters    tc{0u, 0u};
@@ -648,7 +647,7 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : 8) kTrace
             }
             if (ray != kMissPrim)
                 for (uint32_t k = 0; k < kRefillSteps; ++k)
-                    if (travStep<true, STATS>(P.sc.bvh, s, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut, top))
+                    if (travStep<true, STATS>(P.sc.bvh, s, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut))
                     {
                         P.q.vis[ray] = s.best == kMissPrim ? 1 : 0;
                         ray          = kMissPrim;
@@ -1346,8 +1345,6 @@ __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const floa
 {
     extern __shared__ uint2 stack[];
     __shared__ uint8_t      keyLut[kKeyLutBytes];
-    __shared__ uint4        top[kTopNodes * 5];
-    stageTopNodes(bvh, top);
     fillKeyLut(keyLut);
     uint32_t         i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -1360,7 +1357,7 @@ __global__ void __launch_bounds__(kTraceBlock) kOccluded(BvhView bvh, const floa
                                    stack + threadIdx.x, &tc, err, keyLut);
     else
         h = traverse<true, false>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2,
-                                  stack + threadIdx.x, &tc, err, keyLut, top);
+                                  stack + threadIdx.x, &tc, err, keyLut);
     occ[i] = h == kMissPrim ? 0 : 1;
 }
 
@@ -2329,14 +2326,10 @@ BvhView Integrator::bvhView() const
     {
         v.inst       = instDev_.as<const InstDev>();
         v.stackDepth = twoLevelStack_;
-        v.topNodes   = 0u;
         return v;
     }
     v.inst       = nullptr;
     v.stackDepth = std::min<uint32_t>(bvh_.depth + 1u, uint32_t(kStackDepth));
-    // Top nodes: the root and level 1 (the collapse allocates level d as the
-    // node range [levels[d], levels[d + 1])).
-    v.topNodes = std::min(bvh_.levels.size() > 2 ? bvh_.levels[2] : bvh_.numNodes, kTopNodes);
     return v;
 }
 
