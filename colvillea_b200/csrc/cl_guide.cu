@@ -84,7 +84,6 @@ __global__ void __launch_bounds__(kTcThreads) kInferUnit(GridView g, const uint4
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t tmem  = tcSetup<S>(smem, wt);
-    unsigned char* tile  = smem + TcLayout<S>::kTile;
     uint32_t       phase = 0u;
     for (uint32_t base = blockIdx.x * kTcRows; base < n; base += gridDim.x * kTcRows)
     {
@@ -97,10 +96,11 @@ __global__ void __launch_bounds__(kTcThreads) kInferUnit(GridView g, const uint4
         }
         else
             zeroRow(row);
+        uint32_t packed[kIn / 2];
 #pragma unroll
-        for (int c = 0; c < kIn / 8; ++c) *tileChunk(tile, threadIdx.x, c) = reinterpret_cast<const uint4*>(row)[c];
+        for (int q = 0; q < kIn / 2; ++q) packed[q] = reinterpret_cast<const uint32_t*>(row)[q];
         float o[S::kOut];
-        if (!tcForward<S>(smem, tmem, phase, o))
+        if (!tcForward<S>(smem, tmem, packed, phase, o))
         {
             if (threadIdx.x == 0) atomicOr(err, kTcTimeout);
             break;

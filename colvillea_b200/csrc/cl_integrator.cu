@@ -1179,7 +1179,6 @@ __global__ void __launch_bounds__(guide::kTcThreads) kGuideInfer(Params P, guide
     // CTAs without a tile skip the weight copy and the TMEM allocation.
     if (blockIdx.x * kTcRows >= n) return;
     const uint32_t tmem     = tcSetup<GuideShape>(smem, wt);
-    unsigned char* tile     = smem + TcLayout<GuideShape>::kTile;
     const uint32_t maxDepth = P.wp->maxDepth;
     const f3       bmin{P.g.boxMin[0], P.g.boxMin[1], P.g.boxMin[2]};
     uint32_t       phase = 0u;
@@ -1195,13 +1194,10 @@ __global__ void __launch_bounds__(guide::kTcThreads) kGuideInfer(Params P, guide
         else
 #pragma unroll
             for (int q = 0; q < kIn / 2; ++q) r[q] = 0u;
-#pragma unroll
-        for (int c = 0; c < kIn / 8; ++c)
-            *tileChunk(tile, threadIdx.x, c) = make_uint4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
         const uint32_t vm = __ballot_sync(kFull, ray != kNoRay);
         if (laneId() == 0u && vm) atomicAdd(&P.q.ctr->inferred, (unsigned long long)__popc(vm));
         float o[GuideShape::kOut];
-        if (!tcForward<GuideShape>(smem, tmem, phase, o))
+        if (!tcForward<GuideShape>(smem, tmem, r, phase, o))
         {
             if (threadIdx.x == 0) atomicOr(&P.q.ctr->error, kTcTimeout);
             break;
@@ -1249,17 +1245,22 @@ __global__ void __launch_bounds__(guide::kTcThreads) kCacheMlp(Params P, const u
     const uint32_t n = loadCount(&P.q.ctr->cacheCount);
     if (blockIdx.x * kTcRows >= n) return; // see kGuideInfer
     const uint32_t tmem  = tcSetup<CacheShape>(smem, wt);
-    unsigned char* tile  = smem + TcLayout<CacheShape>::kTile;
     uint32_t       phase = 0u;
     for (uint32_t k0 = blockIdx.x * kTcRows; k0 < n; k0 += gridDim.x * kTcRows)
     {
         const uint32_t k = k0 + threadIdx.x;
-        loadTile(tile, P.c.enc, k0, n);
+        uint32_t       r[kIn / 2];
+#pragma unroll
+        for (int c = 0; c < kIn / 8; ++c)
+        {
+            const uint4 v = k < n ? __ldg(P.c.enc + size_t(k) * (kIn / 8) + c) : make_uint4(0u, 0u, 0u, 0u);
+            r[4 * c] = v.x, r[4 * c + 1] = v.y, r[4 * c + 2] = v.z, r[4 * c + 3] = v.w;
+        }
         const uint32_t ray = k < n ? P.c.encIdx[k] : kNoRay;
         const uint32_t vm  = __ballot_sync(kFull, ray != kNoRay);
         if (laneId() == 0u && vm) atomicAdd(&P.q.ctr->cacheQueries, (unsigned long long)__popc(vm));
         float o[CacheShape::kOut];
-        if (!tcForward<CacheShape>(smem, tmem, phase, o))
+        if (!tcForward<CacheShape>(smem, tmem, r, phase, o))
         {
             if (threadIdx.x == 0) atomicOr(&P.q.ctr->error, kTcTimeout);
             break;
@@ -1497,7 +1498,7 @@ cl_status Integrator::init(std::string* err)
     CL_CUDA(cudaFuncSetAttribute(kGuideInfer, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideMlpSmem), err);
     CL_CUDA(cudaFuncSetAttribute(kCacheMlp, cudaFuncAttributeMaxDynamicSharedMemorySize, kCacheMlpSmem), err);
     // The whole on-chip memory as shared memory, so that the launch holds the
-    // CTAs counted by tcResidentCtas (3 of the guide's, 4 of the cache's).
+    // CTAs counted by tcResidentCtas (4 of the guide's and of the cache's).
     CL_CUDA(cudaFuncSetAttribute(kGuideInfer, cudaFuncAttributePreferredSharedMemoryCarveout, 100), err);
     CL_CUDA(cudaFuncSetAttribute(kCacheMlp, cudaFuncAttributePreferredSharedMemoryCarveout, 100), err);
     CL_TRY(tcResidentCtas((const void*)kCacheMlp, kCacheMlpSmem, &b, err));

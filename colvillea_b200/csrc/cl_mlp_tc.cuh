@@ -2,20 +2,27 @@
 // cores (tcgen05): inference for the path tracer (guide lobes, radiance-cache
 // prediction) and for the network entry points.
 //
-// A CTA of 128 threads owns a 128-row tile of encoded samples.  Per layer one
-// thread issues K/16 `tcgen05.mma.cta_group::1.kind::f16` (M = 128, N = the
-// layer's outputs, K = 16; BF16 operands from shared memory, FP32 accumulator
-// in tensor memory) and commits them to an mbarrier.  Thread t then reads row
-// t of the accumulator from TMEM lane t (`tcgen05.ld.32x32b`, warp w owns
-// lanes 32w..32w+31), applies ReLU, rounds to BF16 and writes the row back as
-// the next layer's A operand; after the last layer each thread holds its own
-// row of outputs, so the head (vMF lobes, radiance) runs per thread.
+// A CTA of 128 threads owns a 128-row tile of encoded samples; thread t owns
+// row t, which lives in TMEM lane t (warp w accesses lanes 32w..32w+31).  The
+// CTA's 128 TMEM columns hold the layer's FP32 accumulator in [0, 64) and its
+// BF16 input rows (the MMA's A operand, two values per 32-bit column, lower
+// index in the low half) in [64, 64 + K/2).  Per layer each thread stores its
+// input row into TMEM (`tcgen05.st.32x32b`), one thread issues K/16
+// `tcgen05.mma.cta_group::1.kind::f16` (M = 128, N = the layer's outputs,
+// K = 16; A from tensor memory, B = the weights from shared memory) and
+// commits them to an mbarrier, and thread t reads row t of the accumulator
+// (`tcgen05.ld.32x32b`), applies ReLU and rounds to BF16: the next layer's
+// input row, which goes straight back to TMEM.  Activations never pass
+// through shared memory, so a CTA needs only the weights there.  After the
+// last layer each thread holds its own row of outputs, so the head (vMF
+// lobes, radiance) runs per thread.
 //
-// Shared-memory operands use the no-swizzle K-major canonical layout: 8-row x
-// 16-byte core matrices, rows 16 B apart.  A tile (128 rows x K): the 8-column
-// chunk c of row r at c * 2048 + r * 16 (LBO, the K-chunk stride, 2048 B; SBO,
-// the 8-row-group stride, 128 B).  Weights of layer l (N x K, W[n][k]): chunk
-// c of row n at 2 woff(l) + (c N + n) * 16 (LBO = 16 N, SBO = 128).
+// The weights use the no-swizzle K-major canonical shared-memory layout:
+// 8-row x 16-byte core matrices, rows 16 B apart; the 8-column chunk c of row
+// n of layer l (N x K, W[n][k]) at 2 woff(l) + (c N + n) * 16 (LBO = 16 N,
+// SBO = 128).  The training kernel (cl_guide.cu) keeps its activation tiles in
+// shared memory in the same layout (chunk c of row r at c * 2048 + r * 16),
+// because its backward products read them as MN-major operands.
 #pragma once
 
 #include "cl_guide.cuh"
@@ -24,18 +31,18 @@ namespace clb
 {
 namespace guide
 {
-constexpr int      kTcRows      = 128;               // rows per tile (the MMA's M)
-constexpr int      kTcThreads   = 128;               // one thread per row
-constexpr uint32_t kTcChunk     = kTcRows * 16;      // bytes of one 8-column chunk of a tile
-constexpr int      kTcTileBytes = kTcRows * kIn * 2; // an encoded-input tile (24,576 B)
-constexpr uint32_t kTcCols      = 64;                // TMEM columns per CTA (FP32 accumulator, N <= 64)
-constexpr uint32_t kTcTimeout   = 0x10u;             // device error flag: a tensor-core wait ran out
+constexpr int      kTcRows    = 128;          // rows per tile (the MMA's M)
+constexpr int      kTcThreads = 128;          // one thread per row
+constexpr uint32_t kTcChunk   = kTcRows * 16; // bytes of one 8-column chunk of a shared-memory tile (training)
+constexpr uint32_t kTcCols    = 128;          // TMEM columns per inference CTA
+constexpr uint32_t kTcAcol    = 64;           // first TMEM column of the A operand (accumulator: [0, 64))
+constexpr uint32_t kTcTimeout = 0x10u;        // device error flag: a tensor-core wait ran out
+static_assert(kTcAcol + kIn / 2 <= kTcCols && kWidth <= int(kTcAcol), "TMEM columns of an inference CTA");
 
 template <class S> struct TcLayout
 {
     static constexpr int kWBytes = S::kParams * 2; // canonical-layout BF16 weights
-    static constexpr int kTile   = kWBytes;        // A tile offset (16-byte aligned)
-    static constexpr int kBar    = kTile + kTcTileBytes;
+    static constexpr int kBar    = kWBytes;
     static constexpr int kSmem   = kBar + 16;      // + mbarrier and the TMEM address
     static_assert(kWBytes % 16 == 0, "weights: 16-byte chunks");
 };
@@ -77,6 +84,13 @@ __device__ __forceinline__ void tcMma(uint32_t d, uint64_t a, uint64_t b, uint32
                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
                  "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
 }
+// The same with A (K-major, 128 rows x 16) in tensor memory at column address a.
+__device__ __forceinline__ void tcMmaTs(uint32_t d, uint32_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d),
+                 "r"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
 __device__ __forceinline__ void tcCommit(uint32_t bar)
 {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -108,6 +122,16 @@ __device__ __forceinline__ void tmemLd16(uint32_t taddr, uint32_t (&v)[16])
                  : "r"(taddr));
 }
 __device__ __forceinline__ void tmemWait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// 16 consecutive 32-bit columns of this thread's TMEM lane <- v.
+__device__ __forceinline__ void tmemSt16(uint32_t taddr, const uint32_t* v)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15, %16};" ::"r"(taddr),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+                 "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+                 : "memory");
+}
+__device__ __forceinline__ void tmemWaitSt() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void mbarInit(uint32_t bar, uint32_t count)
 {
@@ -176,26 +200,10 @@ __device__ __forceinline__ void tcTeardown(uint32_t tmem)
     if (threadIdx.x < 32) tmemFree(tmem, kTcCols);
 }
 
-// Row r of the A tile, 8-column chunk c (16 bytes).
+// Row r of a shared-memory tile (training), 8-column chunk c (16 bytes).
 __device__ __forceinline__ uint4* tileChunk(unsigned char* tile, uint32_t row, int c)
 {
     return reinterpret_cast<uint4*>(tile + c * kTcChunk + row * 16u);
-}
-
-// Encoded rows k0 .. k0 + 127 of `enc` (kIn / 8 chunks each; rows >= n are
-// zero) -> the A tile.  Warp w loads its own rows 32w .. 32w + 31 with
-// contiguous 512-byte reads.
-__device__ __forceinline__ void loadTile(unsigned char* tile, const uint4* __restrict__ enc, uint32_t k0, uint32_t n)
-{
-    constexpr uint32_t kC   = kIn / 8;
-    const uint32_t     lane = threadIdx.x & 31u, r0 = threadIdx.x & ~31u;
-    const uint4*       src  = enc + size_t(k0 + r0) * kC;
-#pragma unroll
-    for (uint32_t q = 0; q < kC; ++q)
-    {
-        const uint32_t j = lane + 32u * q, r = j / kC, c = j % kC;
-        *tileChunk(tile, r0 + r, int(c)) = k0 + r0 + r < n ? __ldg(src + j) : make_uint4(0u, 0u, 0u, 0u);
-    }
 }
 
 __device__ __forceinline__ uint4 packRelu8(const uint32_t* v)
@@ -206,22 +214,24 @@ __device__ __forceinline__ uint4 packRelu8(const uint32_t* v)
                       packBf16(reluF(__uint_as_float(v[6])), reluF(__uint_as_float(v[7]))));
 }
 
-// Forward pass of the tile in shared memory (the encoded inputs, written by
-// every thread before the call).  Thread t receives row t's outputs.  `phase`
-// is the mbarrier's parity, carried across tiles.  Returns false (in every
-// thread) when a tensor-core wait ran out; the tile's outputs are then
-// undefined.
+// Forward pass of the tile whose row t is thread t's `in` (the 96 encoded
+// inputs as 48 packed BF16 pairs; zero for rows without a sample).  Thread t
+// receives row t's outputs.  `phase` is the mbarrier's parity, carried across
+// tiles.  Returns false (in every thread) when a tensor-core wait ran out; the
+// tile's outputs are then undefined.
 template <class S>
-__device__ __forceinline__ bool tcForward(unsigned char* smem, uint32_t tmem, uint32_t& phase, float (&out)[S::kOut])
+__device__ __forceinline__ bool tcForward(unsigned char* smem, uint32_t tmem, const uint32_t (&in)[kIn / 2],
+                                          uint32_t& phase, float (&out)[S::kOut])
 {
-    unsigned char* tile = smem + TcLayout<S>::kTile;
-    const uint32_t wS = smemAddr(smem), aS = smemAddr(tile), bar = smemAddr(smem + TcLayout<S>::kBar);
-    const uint32_t row   = threadIdx.x;
+    const uint32_t wS = smemAddr(smem), bar = smemAddr(smem + TcLayout<S>::kBar);
     const uint32_t taddr = tmem + ((threadIdx.x & ~31u) << 16); // this warp's TMEM lanes
+    tmemSt16(taddr + kTcAcol, in);
+    tmemSt16(taddr + kTcAcol + 16u, in + 16);
+    tmemSt16(taddr + kTcAcol + 32u, in + 32);
 #pragma unroll 1
     for (int l = 0; l < S::kLayers; ++l)
     {
-        asyncProxyFence();
+        tmemWaitSt();
         tcFenceBefore();
         __syncthreads();
         if (threadIdx.x == 0)
@@ -230,8 +240,8 @@ __device__ __forceinline__ bool tcForward(unsigned char* smem, uint32_t tmem, ui
             const int      K = S::in(l), N = S::out(l);
             const uint32_t idesc = tcIdesc(N), wl = wS + 2u * uint32_t(S::woff(l));
             for (int ks = 0; ks < K / 16; ++ks)
-                tcMma(tmem, tcDesc(aS + uint32_t(ks) * 2u * kTcChunk, kTcChunk, 128u),
-                      tcDesc(wl + uint32_t(ks * 2 * N * 16), uint32_t(N * 16), 128u), idesc, ks > 0 ? 1u : 0u);
+                tcMmaTs(tmem, tmem + kTcAcol + uint32_t(8 * ks),
+                        tcDesc(wl + uint32_t(ks * 2 * N * 16), uint32_t(N * 16), 128u), idesc, ks > 0 ? 1u : 0u);
             tcCommit(bar);
         }
         const bool ok = mbarWait(bar, phase);
@@ -244,12 +254,14 @@ __device__ __forceinline__ bool tcForward(unsigned char* smem, uint32_t tmem, ui
 #pragma unroll
             for (int c = 0; c < kWidth / 16; ++c) tmemLd16(taddr + uint32_t(16 * c), v[c]);
             tmemWait();
+            uint32_t a[kWidth / 2];
 #pragma unroll
             for (int c = 0; c < kWidth / 16; ++c)
-            {
-                *tileChunk(tile, row, 2 * c)     = packRelu8(v[c]);
-                *tileChunk(tile, row, 2 * c + 1) = packRelu8(v[c] + 8);
-            }
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    a[8 * c + j] = packBf16(reluF(__uint_as_float(v[c][2 * j])), reluF(__uint_as_float(v[c][2 * j + 1])));
+            tmemSt16(taddr + kTcAcol, a);
+            tmemSt16(taddr + kTcAcol + 16u, a + 16);
         }
         else
         {
