@@ -36,10 +36,12 @@ RAY_IN, HIT_OUT, NODE_BYTES, TRI_BYTES = 32, 16, 80, 48
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=6)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--spp-per-step", type=int, default=0,
+                    help="spp of each step's render call (0 = the configuration's frame: 64 for config 2)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -109,13 +111,14 @@ def run_profile(args):
     return 0
 
 
-def workload_desc(s):
+def workload_desc(s, spp_per_step=None):
+    n = spp_per_step or s.spp
     return {"workload": f"{s.name}: wavefront path tracing {s.width}x{s.height}, max depth {s.max_depth}, RR from "
                         f"{s.rr_start}, {s.num_triangles} triangles, {s.dome().texels.shape[1]}x"
-                        f"{s.dome().texels.shape[0]} HDRI dome + directional light; 1 step = 1 spp over the image "
-                        f"({s.spp} steps = the {s.spp}-spp frame)",
+                        f"{s.dome().texels.shape[0]} HDRI dome + directional light; 1 step = one render call of "
+                        f"{n} spp over the image (the configured frame is {s.spp} spp)",
             "image": [s.width, s.height], "triangles": s.num_triangles, "max_depth": s.max_depth,
-            "rr_start": s.rr_start, "spp_per_step": 1, "estimator": "reference (compat Q1-Q9) + alias dome sampler",
+            "rr_start": s.rr_start, "spp_per_step": n, "estimator": "reference (compat Q1-Q9) + alias dome sampler",
             "l2": "inputs larger than L2 (BVH + scene + film > 126 MB), no flush", "seed": 0}
 
 
@@ -510,7 +513,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": round(v, 6), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * elapsed / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_desc(s),
+            "config": {**workload_desc(s, args.spp_per_step), "parallelism": "host threads"},
             "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"each step: 1 spp over {nstep} of {npx} pixels (strided), all host threads"},
             "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -557,16 +560,21 @@ def main():
     scene_mb = (free0 - torch.cuda.mem_get_info()[0]) / 2**20
     st0 = it.stats()
 
+    # A step is one render call of `spp` iterations: the configured frame
+    # (64 spp for config 2) by default.  Within a call the persistent
+    # scheduler starts the next iteration's paths in the slots that finished
+    # paths free, so the waves stay full until the last iteration drains.
+    spp = args.spp_per_step or s.spp
     # Traversal counters on the identical ray set of the first timed step.
     sit = cb.load_scene(s, flags=flags | cb.TRACE_STATS)
-    if args.warmup:
-        sit.render(args.warmup)
-    sit.render(1)
+    for _ in range(args.warmup):
+        sit.render(spp)
+    sit.render(spp)
     sst = sit.stats()
     sit.close()
 
     for _ in range(args.warmup):
-        it.render(1)
+        it.render(spp)
     dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(dist.local)
@@ -577,7 +585,7 @@ def main():
     rays_c = rays_s = 0
     launches = 0
     for _ in range(args.steps):
-        it.render(1)
+        it.render(spp)
         st = it.stats()
         ms_dev += st["ms_last_render"]
         rays_c += st["last_rays_closest"]; rays_s += st["last_rays_shadow"]
@@ -589,22 +597,33 @@ def main():
     clk = clocks.stop()
     dist.barrier()
     ms_rank = ev0.elapsed_time(ev1)
+    # For comparison: one iteration per render call (the reference's render()
+    # granularity), where every call ends with its waves draining.
+    n1 = 32
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    it.render(1)
+    e0.record()
+    for _ in range(n1):
+        it.render(1)
+    e1.record()
+    torch.cuda.synchronize()
+    value_1spp = dist.job_rate(W * H * n1, e0.elapsed_time(e1)) / 1e6
 
     # Stage times (CUDA events on the integrator's stream) over the same steps.
     pit = cb.load_scene(s, flags=flags | cb.PROFILE_STAGES, path_slots=args.slots)
     for _ in range(args.warmup):
-        pit.render(1)
+        pit.render(spp)
     ms_trace = ms_shade = ms_shadow = 0.0
     prays_c = 0
     trace_launches = 0
     for _ in range(args.steps):
-        pit.render(1)
+        pit.render(spp)
         st = pit.stats()
         ms_trace += st["ms_trace"]; ms_shade += st["ms_shade"]; ms_shadow += st["ms_shadow"]
         prays_c += st["last_rays_closest"]
         trace_launches += st["waves"]
     pit.close()
-    value = dist.job_rate(W * H * args.steps, ms_rank) / 1e6
+    value = dist.job_rate(W * H * spp * args.steps, ms_rank) / 1e6
     mrays = dist.job_rate(rays_c + rays_s, ms_rank) / 1e6
     ms = dist.max(ms_rank)
 
@@ -615,7 +634,7 @@ def main():
         arr = film.numpy()
         cam = np.ascontiguousarray(s.camera, np.float32)
         for _ in range(args.warmup):
-            it.updateCamera(cam); it.render(1); it.readbackFramebufferAsync(arr)
+            it.updateCamera(cam); it.render(spp); it.readbackFramebufferAsync(arr)
         it.readbackWait()
         dist.barrier()
         torch.cuda.synchronize()
@@ -623,13 +642,13 @@ def main():
         e0.record()
         for _ in range(args.steps):
             it.updateCamera(cam)
-            it.render(1)
+            it.render(spp)
             it.readbackFramebufferAsync(arr)   # step k's copy overlaps step k+1's render
         it.readbackWait()
         e1.record()
         torch.cuda.synchronize()
         ems_rank = e0.elapsed_time(e1)
-        e2e_value = dist.job_rate(W * H * args.steps, ems_rank) / 1e6
+        e2e_value = dist.job_rate(W * H * spp * args.steps, ems_rank) / 1e6
         ems = dist.max(ems_rank)
         e2e = {"value": round(e2e_value, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(cam.nbytes), "d2h_bytes_per_step": int(arr.nbytes),
@@ -655,11 +674,13 @@ def main():
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {**workload_desc(s), "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"},
+        "config": {**workload_desc(s, spp), "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"},
         "mrays_per_s": round(mrays, 2),
-        "stage_ms_per_step": {"trace": round(ms_trace / args.steps, 3), "shade": round(ms_shade / args.steps, 3),
-                              "shadow": round(ms_shadow / args.steps, 3),
-                              "device_total": round(ms_dev / args.steps, 3)},
+        "value_1spp_per_call": round(value_1spp, 2),
+        "stage_ms_per_spp": {"trace": round(ms_trace / (args.steps * spp), 3),
+                             "shade": round(ms_shade / (args.steps * spp), 3),
+                             "shadow": round(ms_shadow / (args.steps * spp), 3),
+                             "device_total": round(ms_dev / (args.steps * spp), 3)},
         "roofline": {"kernel": "kTraceClosest (8-wide BVH closest hit)", "bound": "hbm",
                      "achieved": round(achieved, 1) if achieved else None, "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4) if achieved else None,
