@@ -41,7 +41,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=2)
     ap.add_argument("--spp-per-step", type=int, default=0,
-                    help="spp of each step's render call (0 = the configuration's frame: 64 for config 2)")
+                    help="spp of each step's render call (0 = the configuration's frame, at most 64: 64 for config 2)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -111,8 +111,14 @@ def run_profile(args):
     return 0
 
 
-def workload_desc(s, spp_per_step=None):
-    n = spp_per_step or s.spp
+def step_spp(s, spp_per_step=0):
+    """spp of one bench step's render call: the configured frame (64 for
+    config 2), at most 64 (config 5's 256-spp 4K frame would take ~10 s)."""
+    return spp_per_step or min(s.spp, 64)
+
+
+def workload_desc(s, spp_per_step=0):
+    n = step_spp(s, spp_per_step)
     return {"workload": f"{s.name}: wavefront path tracing {s.width}x{s.height}, max depth {s.max_depth}, RR from "
                         f"{s.rr_start}, {s.num_triangles} triangles, {s.dome().texels.shape[1]}x"
                         f"{s.dome().texels.shape[0]} HDRI dome + directional light; 1 step = one render call of "
@@ -564,7 +570,7 @@ def main():
     # (64 spp for config 2) by default.  Within a call the persistent
     # scheduler starts the next iteration's paths in the slots that finished
     # paths free, so the waves stay full until the last iteration drains.
-    spp = args.spp_per_step or s.spp
+    spp = step_spp(s, args.spp_per_step)
     # Traversal counters on the identical ray set of the first timed step.
     sit = cb.load_scene(s, flags=flags | cb.TRACE_STATS)
     for _ in range(args.warmup):
