@@ -368,6 +368,7 @@ struct ClassifyView
     uint32_t* classIdx;
     uint32_t  cap;
     uint4*    hitIdx; // per ray: the hit triangle's triIdx entry (vertex ids, material), for the shading kernels
+    uint32_t* hitInst; // two-level scenes: per ray, the hit's instance (kTraceClosest -> kClassifyHits)
 };
 
 constexpr int kClassEscaped = 3;
@@ -454,17 +455,26 @@ __device__ __forceinline__ uint32_t supplyLanes(uint2* ws, uint32_t* fetch, uint
 // shadow kernel keep kMissPrim as their idle-lane mark).
 constexpr uint32_t kMaxPathSlots = 0x0fffffffu;
 
-// Closest-hit traversal of a ray queue by persistent warps.  Flattened
-// scenes: each lane traverses one ray at a time and takes the next from the
-// warp's supply when it finishes; the hits' shading classes are appended by
-// kClassifyHits afterwards, in ray order (a class lookup inside the step loop
-// would stall the whole warp on one lane's dependent gathers).  Two-level
-// scenes: the warp fetches 32 consecutive rays, each lane runs its ray to
-// completion, and CLASSIFY appends each finished ray to one of the four
-// shading-class queues (the hit material's BSDF type, or escaped), so that
-// each shading kernel runs one BSDF per warp.  TWO: two-level scene
-// (CL_TWO_LEVEL); the hit's triangle index entry then holds the object-space
-// vertex ids and the instance index (its .w).
+// Traversal state of a flattened (Trav) or two-level (Trav2) scene.
+template <bool TWO> struct TravOf
+{
+    using T = Trav;
+};
+template <> struct TravOf<true>
+{
+    using T = Trav2;
+};
+
+// Closest-hit traversal of a ray queue by persistent warps: each lane
+// traverses one ray at a time and takes the next from the warp's supply when
+// it finishes.  The hits' shading classes are appended by kClassifyHits
+// afterwards, in ray order (a class lookup inside the step loop would stall
+// the whole warp on one lane's dependent gathers).  CLASSIFY: the launch is
+// a wave's (kClassifyHits follows); without it the hits are final (the ray
+// query entry points).  TWO: two-level scene (CL_TWO_LEVEL); with CLASSIFY a
+// hit holds the instance-local triangle id and cv.hitInst its instance, which
+// kClassifyHits turns into the global id and the triangle index entry
+// (object-space vertex ids, the instance in .w).
 template <bool STATS, bool CLASSIFY, bool TWO = false>
 __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : kTraceBlocksFlat) kTraceClosest(BvhView bvh, const float4* __restrict__ O,
                                                                 const float4* __restrict__ D, const uint32_t* count,
@@ -477,75 +487,81 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : kTraceBlo
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(count);
     TraceCounters    tc{0u, 0u};
-    if constexpr (!TWO)
+    // Idle lanes are refilled once at least kRefillIdle of them are idle.
+    uint2* ws = supply + (threadIdx.x >> 5);
+    supplyInit(ws);
+    typename TravOf<TWO>::T s;
+    uint32_t                ray = kMissPrim;
+    for (;;)
     {
-        // Idle lanes are refilled once at least kRefillIdle of them are idle.
-        uint2* ws = supply + (threadIdx.x >> 5);
-        supplyInit(ws);
-        Trav     s;
-        uint32_t ray = kMissPrim;
-        for (;;)
+        const uint32_t idle = __ballot_sync(kFull, ray == kMissPrim);
+        if (uint32_t(__popc(idle)) >= kRefillIdle)
         {
-            const uint32_t idle = __ballot_sync(kFull, ray == kMissPrim);
-            if (uint32_t(__popc(idle)) >= kRefillIdle)
+            if (ws->x != kMissPrim)
             {
-                if (ws->x != kMissPrim)
+                const uint32_t item = supplyLanes(ws, fetch, n, idle);
+                if (item != kMissPrim)
                 {
-                    const uint32_t item = supplyLanes(ws, fetch, n, idle);
-                    if (item != kMissPrim)
-                    {
-                        ray            = item;
-                        const float4 o = O[item], d = D[item];
+                    ray            = item;
+                    const float4 o = O[item], d = D[item];
+                    if constexpr (TWO)
+                        trav2Init(bvh, s, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w);
+                    else
                         travInit(s, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w);
-                    }
                 }
-                if (__all_sync(kFull, ray == kMissPrim)) break;
             }
-            if (ray != kMissPrim)
-                for (uint32_t k = 0; k < kRefillSteps; ++k)
-                    if (travStep<false, STATS>(bvh, s, stack + threadIdx.x, &tc, &ctr->error, keyLut))
-                    {
-                        hitOut[ray] = make_float4(s.bt, __uint_as_float(s.best), s.b1, s.b2);
-                        ray         = kMissPrim;
-                        break;
-                    }
+            if (__all_sync(kFull, ray == kMissPrim)) break;
         }
-    }
-    else
-    {
-        for (;;)
-        {
-            uint32_t base = warpFetch(fetch);
-            if (base >= n) break;
-            uint32_t i    = base + laneId();
-            uint32_t prim = kMissPrim, inst = 0u, loc = 0u;
-            if (i < n)
+        if (ray != kMissPrim)
+            for (uint32_t k = 0; k < kRefillSteps; ++k)
             {
-                float4 o = O[i], d = D[i];
-                float  t, b1, b2;
-                loc = traverse2<false, STATS>(bvh, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, o.w, d.w, &t, &b1, &b2, &inst,
-                                              stack + threadIdx.x, &tc, &ctr->error, keyLut);
-                if (loc != kMissPrim) prim = __ldg(&bvh.inst[inst].primBase) + loc;
-                hitOut[i] = make_float4(t, __uint_as_float(prim), b1, b2);
+                bool done;
+                if constexpr (TWO)
+                    done = trav2Step<false, STATS>(bvh, s, stack + threadIdx.x, &tc, &ctr->error, keyLut);
+                else
+                    done = travStep<false, STATS>(bvh, s, stack + threadIdx.x, &tc, &ctr->error, keyLut);
+                if (done)
+                {
+                    if constexpr (TWO)
+                    {
+                        if (CLASSIFY)
+                        {
+                            // The instance-local id; kClassifyHits makes it global.
+                            hitOut[ray]     = make_float4(s.bt, __uint_as_float(s.best), s.b1, s.b2);
+                            cv.hitInst[ray] = s.bestInst;
+                        }
+                        else
+                        {
+                            const uint32_t prim =
+                                s.best == kMissPrim ? kMissPrim : __ldg(&bvh.inst[s.bestInst].primBase) + s.best;
+                            hitOut[ray] = make_float4(s.bt, __uint_as_float(prim), s.b1, s.b2);
+                        }
+                    }
+                    else
+                        hitOut[ray] = make_float4(s.bt, __uint_as_float(s.best), s.b1, s.b2);
+                    ray = kMissPrim;
+                    break;
+                }
             }
-            if (CLASSIFY) appendClasses(ctr, cv, i < n ? classifyHit<true>(bvh, cv, i, prim, inst, loc) : -1, i);
-        }
     }
     if (STATS) warpStats(tc, &ctr->statNodes, &ctr->statTris);
 }
 
-// Shading classes of a wave's closest hits (flattened scenes).  A block
+// Shading classes of a wave's closest hits.  A block
 // takes tiles of kClassifyTile consecutive rays (kClassifyPer per thread,
 // in ray order), counts each class over the tile with warp ballots and a
 // block scan, reserves the tile's range of each class queue with one
 // atomicAdd per class, and writes the rays there in ray order; the hit's
-// triangle index entry is written for the shading kernels.  Grid-stride
-// over the wave's ray count (read on the device).
+// triangle index entry is written for the shading kernels.  Two-level
+// scenes (TWO): the hit's instance-local triangle id and instance (from
+// kTraceClosest) become the global id, written back into the hit.
+// Grid-stride over the wave's ray count (read on the device).
 constexpr int kClassifyThreads = 256;
 constexpr int kClassifyPer     = 4;
 constexpr int kClassifyTile    = kClassifyThreads * kClassifyPer;
-__global__ void __launch_bounds__(kClassifyThreads) kClassifyHits(BvhView bvh, const float4* __restrict__ hit,
-                                                                  const uint32_t* count, Counters* ctr, ClassifyView cv)
+template <bool TWO>
+__global__ void __launch_bounds__(kClassifyThreads) kClassifyHits(BvhView bvh, float4* hit, const uint32_t* count,
+                                                                  Counters* ctr, ClassifyView cv)
 {
     constexpr int  kWarps = kClassifyThreads / 32;
     __shared__ uint32_t wcount[kClassifyPer][kWarps][4]; // rays of class c in (round r, warp w)
@@ -559,7 +575,20 @@ __global__ void __launch_bounds__(kClassifyThreads) kClassifyHits(BvhView bvh, c
         for (int r = 0; r < kClassifyPer; ++r)
         {
             const uint32_t i = tile + uint32_t(r * kClassifyThreads) + threadIdx.x;
-            cls[r]           = i < n ? classifyHit<false>(bvh, cv, i, __float_as_uint(__ldg(&hit[i].y)), 0u, 0u) : -1;
+            cls[r]           = -1;
+            if (i < n)
+            {
+                const uint32_t h = __float_as_uint(hit[i].y);
+                if constexpr (TWO)
+                {
+                    const uint32_t inst = cv.hitInst[i];
+                    const uint32_t prim = h == kMissPrim ? kMissPrim : __ldg(&bvh.inst[inst].primBase) + h;
+                    hit[i].y            = __uint_as_float(prim);
+                    cls[r]              = classifyHit<true>(bvh, cv, i, prim, inst, h);
+                }
+                else
+                    cls[r] = classifyHit<false>(bvh, cv, i, h, 0u, 0u);
+            }
         }
         uint32_t rank[kClassifyPer];
 #pragma unroll
@@ -614,72 +643,53 @@ __global__ void __launch_bounds__(kTraceBlock, TWO ? kTraceBlocksTwo : kTraceBlo
     fillKeyLut(keyLut);
     const uint32_t   n = loadCount(&P.q.ctr->shadowCount) * (DL ? 2u : 1u);
     TraceCounters    tc{0u, 0u};
-    if constexpr (!TWO)
+    // Idle lanes refilled as in kTraceClosest.
+    uint2* ws = supply + (threadIdx.x >> 5);
+    supplyInit(ws);
+    typename TravOf<TWO>::T s;
+    uint32_t                ray = kMissPrim;
+    for (;;)
     {
-        // Idle lanes refilled as in kTraceClosest.
-        uint2* ws = supply + (threadIdx.x >> 5);
-        supplyInit(ws);
-        Trav     s;
-        uint32_t ray = kMissPrim;
-        for (;;)
+        const uint32_t idle = __ballot_sync(kFull, ray == kMissPrim);
+        if (uint32_t(__popc(idle)) >= kRefillIdle)
         {
-            const uint32_t idle = __ballot_sync(kFull, ray == kMissPrim);
-            if (uint32_t(__popc(idle)) >= kRefillIdle)
+            if (ws->x != kMissPrim)
             {
-                if (ws->x != kMissPrim)
+                const uint32_t item = supplyLanes(ws, &P.q.ctr->fetchShadow, n, idle);
+                if (item != kMissPrim)
                 {
-                    const uint32_t item = supplyLanes(ws, &P.q.ctr->fetchShadow, n, idle);
-                    if (item != kMissPrim)
+                    const uint32_t e  = DL ? item >> 1 : item;
+                    const float4   o4 = P.q.sqO[e];
+                    const float4   d4 = (DL && (item & 1u)) ? P.q.sqD2[e] : P.q.sqD[e];
+                    if (d4.w != 0.0f)
                     {
-                        const uint32_t e  = DL ? item >> 1 : item;
-                        const float4   o4 = P.q.sqO[e];
-                        const float4   d4 = (DL && (item & 1u)) ? P.q.sqD2[e] : P.q.sqD[e];
-                        if (d4.w != 0.0f)
-                        {
-                            ray = item;
-                            travInit(s, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX);
-                        }
+                        ray = item;
+                        if constexpr (TWO)
+                            trav2Init(P.sc.bvh, s, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX);
                         else
-                            P.q.vis[item] = 0; // no emitter sample on this entry
+                            travInit(s, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps, FLT_MAX);
                     }
+                    else
+                        P.q.vis[item] = 0; // no emitter sample on this entry
                 }
-                if (__all_sync(kFull, ray == kMissPrim) && ws->x == kMissPrim) break;
             }
-            if (ray != kMissPrim)
-                for (uint32_t k = 0; k < kRefillSteps; ++k)
-                    if (travStep<true, STATS>(P.sc.bvh, s, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut))
-                    {
-                        P.q.vis[ray] = s.best == kMissPrim ? 1 : 0;
-                        ray          = kMissPrim;
-                        break;
-                    }
+            if (__all_sync(kFull, ray == kMissPrim) && ws->x == kMissPrim) break;
         }
-    }
-    else
-    {
-        for (;;)
-        {
-            uint32_t base = warpFetch(&P.q.ctr->fetchShadow);
-            if (base >= n) break;
-            uint32_t item = base + laneId();
-            if (item < n)
+        if (ray != kMissPrim)
+            for (uint32_t k = 0; k < kRefillSteps; ++k)
             {
-                uint32_t e  = DL ? item >> 1 : item;
-                float4   o4 = P.q.sqO[e];
-                float4   d4 = (DL && (item & 1u)) ? P.q.sqD2[e] : P.q.sqD[e];
-                uint8_t  v  = 0;
-                if (d4.w != 0.0f)
+                bool done;
+                if constexpr (TWO)
+                    done = trav2Step<true, STATS>(P.sc.bvh, s, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
+                else
+                    done = travStep<true, STATS>(P.sc.bvh, s, stack + threadIdx.x, &tc, &P.q.ctr->error, keyLut);
+                if (done)
                 {
-                    float    t, b1, b2;
-                    uint32_t hi;
-                    uint32_t h = traverse2<true, STATS>(P.sc.bvh, f3{o4.x, o4.y, o4.z}, f3{d4.x, d4.y, d4.z}, kRayEps,
-                                                        FLT_MAX, &t, &b1, &b2, &hi, stack + threadIdx.x, &tc,
-                                                        &P.q.ctr->error, keyLut);
-                    v = h == kMissPrim ? 1 : 0;
+                    P.q.vis[ray] = s.best == kMissPrim ? 1 : 0;
+                    ray          = kMissPrim;
+                    break;
                 }
-                P.q.vis[item] = v;
             }
-        }
     }
     if (STATS) warpStats(tc, &P.q.ctr->statNodesS, &P.q.ctr->statTrisS);
 }
@@ -2296,6 +2306,7 @@ cl_status Integrator::ensureQueues(std::string* err)
     }
     CL_TRY(hit_.alloc(s * 16, err));
     CL_TRY(hitIdx_.alloc(s * 16, err));
+    CL_TRY(hitInst_.alloc(s * 4, err));
     CL_TRY(sqO_.alloc(s * 16, err));
     CL_TRY(sqD_.alloc(s * 16, err));
     CL_TRY(sqL_.alloc(s * 16, err));
@@ -2336,7 +2347,8 @@ BvhView Integrator::bvhView() const
 
 ClassifyView Integrator::classifyView() const
 {
-    return ClassifyView{triIdx_.as<const uint4>(), mats_.as<const float4>(), classIdx_.u(), slots_, hitIdx_.as<uint4>()};
+    return ClassifyView{triIdx_.as<const uint4>(), mats_.as<const float4>(), classIdx_.u(), slots_, hitIdx_.as<uint4>(),
+                        hitInst_.u()};
 }
 
 Params Integrator::params() const
@@ -2418,9 +2430,8 @@ cl_status Integrator::launchWave(int cur, bool profile, std::string* err)
         k<<<tBlocks(), kTraceBlock, sb, stream_>>>(P.sc.bvh, P.q.rqO[cur], P.q.rqD[cur], &c->rayCount[cur],
                                                       &c->fetchTrace, P.q.hit, c, classifyView());
         if (profile) CL_CUDA(cudaEventRecord(evS_[5], stream_), err);
-        if (!twoLevel_)
-            kClassifyHits<<<numSMs_ * 8, kClassifyThreads, 0, stream_>>>(P.sc.bvh, P.q.hit, &c->rayCount[cur], c,
-                                                                         classifyView());
+        (twoLevel_ ? kClassifyHits<true> : kClassifyHits<false>)<<<numSMs_ * 8, kClassifyThreads, 0, stream_>>>(
+            P.sc.bvh, P.q.hit, &c->rayCount[cur], c, classifyView());
     }
     if (profile) CL_CUDA(cudaEventRecord(evS_[1], stream_), err);
     const uint32_t gmask = guide_ ? guideCfg_.class_mask : 0u;
@@ -3220,9 +3231,8 @@ cl_status Integrator::guideProbe(uint32_t cap, float* rows, uint32_t* count, std
     (twoLevel_ ? kTraceClosest<false, true, true> : kTraceClosest<false, true, false>)
         <<<tBlocks(), kTraceBlock, traceStackBytes(P.sc.bvh.stackDepth), stream_>>>(
             P.sc.bvh, P.q.rqO[0], P.q.rqD[0], &c->rayCount[0], &c->fetchTrace, P.q.hit, c, classifyView());
-    if (!twoLevel_)
-        kClassifyHits<<<numSMs_ * 8, kClassifyThreads, 0, stream_>>>(P.sc.bvh, P.q.hit, &c->rayCount[0], c,
-                                                                     classifyView());
+    (twoLevel_ ? kClassifyHits<true> : kClassifyHits<false>)<<<numSMs_ * 8, kClassifyThreads, 0, stream_>>>(
+        P.sc.bvh, P.q.hit, &c->rayCount[0], c, classifyView());
     kGuideInfer<<<inferBlocks_, guide::kTcThreads, kGuideMlpSmem, stream_>>>(
         P, guide_->grid(), 0, guide_->tcWeights(), guideCfg_.learn_selection ? -1.0f : 1.0f - guideCfg_.bsdf_fraction);
     CL_CUDA(cudaGetLastError(), err);

@@ -270,7 +270,7 @@ private:
     DevBuf       resolve_;
     cudaStream_t copyStream_ = nullptr;
     cudaEvent_t  evResolved_ = nullptr, evCopied_ = nullptr;
-    DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, hitIdx_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
+    DevBuf rqO_[2], rqD_[2], rqSlot_[2], hit_, hitIdx_, hitInst_, sqO_, sqD_, sqL_, sqD2_, sqL2_;
     DevBuf psInfo_, psT_, psE_, psL_, ctr_, wp_, vis_, classIdx_;
     uint32_t slots_ = 0, shadowCap_ = 0;
     WaveParams* hostWp_ = nullptr;   // pinned
