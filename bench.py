@@ -45,8 +45,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU baseline sample size")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--profile", type=int, default=0, metavar="SPP",
-                    help="profiling run for ncu: build the workload, render SPP iterations, print stage times")
+    ap.add_argument("--profile", type=int, default=0, metavar="CALLS",
+                    help="profiling run for ncu: build the workload, make CALLS render calls, print stage times")
+    ap.add_argument("--profile-spp", type=int, default=1,
+                    help="iterations per render call of --profile (more than one keeps the waves full)")
     ap.add_argument("--slots", type=int, default=0, help="paths in flight (0 = automatic)")
     ap.add_argument("--two-level", action="store_true",
                     help="two-level scene (one tree per mesh, one over the instances) instead of flattened instances")
@@ -102,7 +104,7 @@ def run_profile(args):
     s = scenes.CONFIGS[args.config](0)
     it = cb.load_scene(s, flags=cb.COMPAT_ALL | cb.DOME_ALIAS | cb.PROFILE_STAGES, path_slots=args.slots)
     for _ in range(args.profile):
-        it.render(1)
+        it.render(args.profile_spp)
         st = it.stats()
         print(json.dumps({**{k: st[k] for k in ("ms_last_render", "ms_trace", "ms_shade", "ms_shadow", "waves",
                                                 "last_rays_closest", "last_rays_shadow")},
