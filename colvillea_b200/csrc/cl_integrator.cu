@@ -720,10 +720,12 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
     const bool compatEsc   = CMP == 2 ? (wp.flags & CL_COMPAT_ESCAPE) != 0 : CMP == 1;
     const bool alias       = ALIAS;
     const uint32_t N       = sc.numEmitters;
-    for (;;)
+    // Static assignment of 32-ray batches to warps (grid-stride): a dynamic
+    // fetch would put a same-address atomicAdd at the head of every batch's
+    // chain of dependent gathers.
+    const uint32_t gw = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32u; base < n; base += gw * 32u)
     {
-        uint32_t base = warpFetch(MAT < 0 ? &P.q.ctr->fetchShade : &P.q.ctr->fetchClass[MAT < 0 ? 0 : MAT]);
-        if (base >= n) break;
         uint32_t i     = base + laneId();
         bool     valid = i < n;
         if (MAT >= 0 && valid) i = P.q.classIdx[size_t(MAT) * P.q.slots + i];
@@ -1034,10 +1036,9 @@ __global__ void __launch_bounds__(128) kShadowResolve(Params P, int cur)
     const WaveParams wp  = *P.wp;
     const uint32_t   n   = loadCount(&P.q.ctr->shadowCount);
     const int        nxt = cur ^ 1;
-    for (;;)
+    const uint32_t gw = gridDim.x * (blockDim.x >> 5); // static 32-entry batches, as in kShade
+    for (uint32_t base = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32u; base < n; base += gw * 32u)
     {
-        uint32_t base = warpFetch(&P.q.ctr->fetchResolve);
-        if (base >= n) break;
         uint32_t i      = base + laneId();
         bool     finish = false;
         uint32_t slot   = 0u;
@@ -1337,15 +1338,12 @@ __global__ void kAdvance(Counters* c, int cur)
     c->rayCount[cur] = 0u;
     c->shadowCount   = 0u;
     c->fetchTrace    = 0u;
-    c->fetchShade    = 0u;
     c->fetchShadow   = 0u;
-    c->fetchResolve  = 0u;
     c->fetchInfer    = 0u;
     c->cacheCount    = 0u;
     for (int k = 0; k < 4; ++k)
     {
         c->classCount[k] = 0u;
-        c->fetchClass[k] = 0u;
     }
 }
 

@@ -53,10 +53,9 @@ struct Counters
 {
     uint32_t           rayCount[2];
     uint32_t           shadowCount;
-    uint32_t           fetchTrace, fetchShade, fetchShadow, fetchResolve;
+    uint32_t           fetchTrace, fetchShadow; // traversal kernels' ray supplies
     uint32_t           error;
     uint32_t           classCount[4]; // per shading class: diffuse, conductor, dielectric, escaped
-    uint32_t           fetchClass[4];
     unsigned long long pathNext;
     unsigned long long raysClosest, raysShadow;
     unsigned long long statNodes, statTris;
