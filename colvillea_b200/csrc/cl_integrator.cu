@@ -740,6 +740,10 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
             float4 hh     = P.q.hit[i];
             uint4  ti     = MAT == kClassEscaped ? make_uint4(0u, 0u, 0u, 0u) : P.q.hitIdx[i];
             float4 rd     = P.q.rqD[cur][i];
+            // Surface classes: the hit exists, so its vertex gathers start with the
+            // path-state loads instead of after the depth tests that need them.
+            HitAttr a0{};
+            if constexpr (MAT >= 0 && MAT != kClassEscaped) a0 = hitAttributesTri(sc, ti, hh.z, hh.w);
             uint4  info   = P.q.psInfo[slot];
             uint32_t depth = info.z & 0xffu;
             vDepth         = depth;
@@ -781,7 +785,7 @@ __global__ void __launch_bounds__(128) kShade(Params P, int cur)
                 finish = true;
             else
             {
-                HitAttr a    = hitAttributesTri(sc, ti, hh.z, hh.w);
+                HitAttr a    = (MAT >= 0 && MAT != kClassEscaped) ? a0 : hitAttributesTri(sc, ti, hh.z, hh.w);
                 MatTex  tx;
                 Bsdf    bsdf = loadMaterial(sc.mats, a.material, &tx);
                 if (tx.refl | tx.rough) applyTextures(sc.tex, tx, a.uv, &bsdf);
