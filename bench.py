@@ -2,10 +2,11 @@
 
 Workload (cfg2): 1920x1080 image, ~4.7M-triangle scene (1024x1024-vertex fBm
 terrain + 512 icosphere/torus meshes), 2048x1024 HDRI dome + directional
-light, max depth 8, Russian roulette from depth 3.  One step = one progressive
-iteration (1 sample per pixel over the whole image, 2,073,600 camera paths);
-64 steps make the configuration's 64-spp frame.  The reference's estimator
-(compat flags) with the B200 alias-table dome sampler.
+light, max depth 8, Russian roulette from depth 3.  One step = one render call
+of the configuration's 64-spp frame (64 x 2,073,600 camera paths; within the
+call the next iteration's paths start in the slots that finished paths free).
+The rate at one iteration per call is reported beside it.  The reference's
+estimator (compat flags) with the B200 alias-table dome sampler.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -521,7 +522,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": round(v, 6), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * elapsed / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {**workload_desc(s, args.spp_per_step), "parallelism": "host threads"},
+            "config": workload_desc(s, args.spp_per_step), "parallelism": "host threads",
             "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"each step: 1 spp over {nstep} of {npx} pixels (strided), all host threads"},
             "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -682,7 +683,8 @@ def main():
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {**workload_desc(s, spp), "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU"},
+        "config": workload_desc(s, spp),
+        "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
         "mrays_per_s": round(mrays, 2),
         "value_1spp_per_call": round(value_1spp, 2),
         "stage_ms_per_spp": {"trace": round(ms_trace / (args.steps * spp), 3),
