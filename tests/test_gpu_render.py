@@ -144,6 +144,12 @@ def test_resize_and_errors(native):
     with pytest.raises(cb.ClError):
         bad.render(1)  # nothing built yet
     bad.close()
+    # Path slots beyond 2^28 - 1: the traversal kernels' idle-lane mark needs ray indices below that.
+    big = cb.load_scene(s, path_slots=1 << 28)
+    with pytest.raises(cb.ClError) as e:
+        big.render(1)
+    assert "path_slots" in str(e.value)
+    big.close()
 
 
 def test_async_readback_pipeline():
