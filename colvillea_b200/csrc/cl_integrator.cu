@@ -393,24 +393,6 @@ __device__ __forceinline__ int classifyHit(const BvhView& bvh, const ClassifyVie
     return int(__float_as_uint(__ldg(&cv.mats[kMatF4 * ti.w].x)));
 }
 
-// Appends ray i of each lane with cls >= 0 to its class queue (every lane of
-// the warp calls it; one atomicAdd per class and warp).
-__device__ __forceinline__ void appendClasses(Counters* ctr, const ClassifyView& cv, int cls, uint32_t i)
-{
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-    {
-        uint32_t k = warpAppend(&ctr->classCount[c], cls == c);
-        if (cls == c)
-        {
-            if (k < cv.cap)
-                cv.classIdx[size_t(c) * cv.cap + k] = i;
-            else
-                atomicOr(&ctr->error, 8u);
-        }
-    }
-}
-
 // Warp-local supply of queue entries for the persistent traversal kernels.
 // A warp takes 32 consecutive entries per atomicAdd and hands them to its
 // idle lanes in lane order, so that a lane whose ray has finished takes the
