@@ -298,8 +298,8 @@ cl_status cl_update_camera(cl_integrator* integrator, const cl_camera* camera);
 /* Integrator::render (integrator.h:61): `spp` progressive iterations.  Within
  * one call the paths of the next iteration start in the slots that finished
  * paths free, so several iterations per call keep the device busy where one
- * per call ends with small draining waves (config 2: 338 Mpaths/s at 1 spp
- * per call, 382 at 4, 392 at 64). */
+ * per call ends with small draining waves (config 2: 350 Mpaths/s at 1 spp
+ * per call, 400 at 64). */
 cl_status cl_render(cl_integrator* integrator, uint32_t spp);
 /* Integrator::readbackFramebuffer (integrator.h:72): linear HDR mean radiance,
  * RGBA32F, width*height*4 floats (alpha = 1). */
