@@ -127,7 +127,8 @@ def workload_desc(s, spp_per_step=0):
                         f"{s.dome().texels.shape[0]} HDRI dome + directional light; 1 step = one render call of "
                         f"{n} spp over the image (the configured frame is {s.spp} spp)",
             "image": [s.width, s.height], "triangles": s.num_triangles, "max_depth": s.max_depth,
-            "rr_start": s.rr_start, "spp_per_step": n, "estimator": "reference (compat Q1-Q9) + alias dome sampler",
+            "rr_start": s.rr_start, "spp_per_step": n,
+            "estimator": "reference (compat pdf, frame and escape flags) + alias dome sampler",
             "l2": "inputs larger than L2 (BVH + scene + film > 126 MB), no flush", "seed": 0}
 
 

@@ -59,8 +59,11 @@ typedef enum
 /* Render configuration flags. */
 enum
 {
-    /* Reproduce the reference's pdf functions (SmoothDiffuse/RoughConductor/
-     * RoughDielectric::pdf, quirks Q1-Q3 of the survey). */
+    /* Reproduce the reference's pdf functions as written, which differ from
+     * the densities their sample functions draw from: RoughConductor::pdf
+     * returns pdfAll(wo) (roughconductor.h), SmoothDiffuse::pdf cos(wo) / pi
+     * (smoothdiffuse.h) and RoughDielectric::pdf carries an extra cos(H)
+     * factor (roughdielectric.h). */
     CL_COMPAT_PDF = 1u << 0,
     /* Path tracing: shading frame normal = geometric normal, as the reference's
      * swapped getShadingFrame arguments (raygeneration.cu:324-330). */

@@ -423,8 +423,8 @@ struct orc_scene_desc
 // Integrator flags.
 enum
 {
-    ORC_COMPAT_PDF       = 1u << 0, // Q1-Q3
-    ORC_COMPAT_FRAME     = 1u << 1, // Q4 (PT only)
+    ORC_COMPAT_PDF       = 1u << 0, // the reference's pdf functions (conductor pdfAll(wo), diffuse cos(wo), dielectric extra cos(H))
+    ORC_COMPAT_FRAME     = 1u << 1, // PT only: shading-frame normal = geometric normal (the reference's swapped arguments)
     ORC_COMPAT_ESCAPE    = 1u << 2, // Q5 + Q6 + Q9 + Q12 (reference MIS/escape bookkeeping)
     ORC_DOME_ALIAS       = 1u << 4, // the GPU's alias-table dome sampler (tables set by orc_scene_set_dome_tables)
     ORC_DIRECT_LIGHTING  = 1u << 8,
@@ -746,7 +746,7 @@ V3<float> tracePath(const Scene& s, const orc_config& cfg, uint32_t W, uint32_t 
         }
         if (compatEscape)
         {
-            if (!(lightPdf > 0.0f)) break; // Q6
+            if (!(lightPdf > 0.0f)) break; // the reference continues a path only where the dome pdf is non-zero
             float w = misBalanced(bp, lightPdf);
             E       = {f.x * c * w / bp, f.y * c * w / bp, f.z * c * w / bp};
         }

@@ -52,7 +52,8 @@ def test_ggx_fresnel_warps_frames(oracle, golden):
 
 
 def test_fixed_pdfs_differ_from_reference_only_where_quirks_apply(oracle, golden):
-    """compat=False corrects Q1-Q3; the sampled pdf then equals pdf(wo, wi)."""
+    """compat=False uses the sampling densities instead of the reference's pdf functions (conductor pdfAll(wo),
+    diffuse cos(wo), dielectric extra cos(H)); the sampled pdf then equals pdf(wo, wi)."""
     for btype, name in ((0, "diffuse"), (1, "conductor"), (2, "dielectric")):
         g = lambda k: golden[f"{name}_{k}"]
         wi, spdf, sval = oracle.bsdf_sample(btype, g("params"), g("wo"), g("u2"))
