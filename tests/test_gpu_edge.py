@@ -95,3 +95,30 @@ def test_zero_spp_render_is_a_no_op():
     d1, _ = it.readbackFilmStats()
     it.close()
     assert np.allclose(c1, d1, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("depth,rr", [(1, 3), (2, 1), (12, 1)])
+def test_depth_and_roulette_bounds(oracle, depth, rr):
+    """Camera rays only (depth 1), roulette from the first vertex, and deep paths."""
+    s = dataclasses.replace(scenes.config1(0, 64, 48), max_depth=depth, rr_start=rr)
+    gm, cm, st, cnt = _render_both(s, 8, cb.COMPAT_ALL, oracle.COMPAT_ALL, oracle)
+    _check_same_seed(gm, cm, st, cnt, f"max depth {depth}, roulette from {rr}")
+    if depth == 1:
+        assert int(st["rays_closest"]) == 64 * 48 * 8
+
+
+@pytest.mark.parametrize("keep", [scenes.EMIT_DIRECTIONAL, scenes.EMIT_DOME])
+def test_direct_lighting_single_emitter(oracle, keep):
+    base = scenes.config1(0, 64, 48)
+    s = dataclasses.replace(base, emitters=[e for e in base.emitters if e.type == keep])
+    it = cb.load_scene(s, itype=cb.IntegratorType.WavefrontDirectLighting, flags=cb.COMPAT_ALL | cb.FILM_FP64)
+    it.render(8)
+    g1, _ = it.readbackFilmStats()
+    it.close()
+    o = oracle.OracleScene(s.flatten())
+    c1, _, _ = o.render(8, max_depth=1, flags=oracle.COMPAT_ALL | oracle.DIRECT_LIGHTING)
+    rel = np.abs(g1 - c1) / (np.abs(c1) + 8e-2)
+    print(f"[edge] DL, {'directional' if keep == scenes.EMIT_DIRECTIONAL else 'dome'} only: median rel "
+          f"{np.median(rel):.2e}, p99 {np.quantile(rel, 0.99):.2e}")
+    assert np.isfinite(g1).all() and g1.max() > 0.0
+    assert np.quantile(rel, 0.5) < 1e-4 and np.quantile(rel, 0.99) < 5e-2
