@@ -590,11 +590,15 @@ def load_scene(scene, itype=IntegratorType.WavefrontPathTracing, flags=COMPAT_AL
     cfg = RenderConfig(scene.max_depth if max_depth is None else max_depth,
                        scene.rr_start if rr_start is None else rr_start, flags, path_slots)
     it = Integrator.createIntegrator(itype, scene.width, scene.height, cfg)
-    if getattr(scene, "textures", None):
-        it.buildTextures(scene.textures)
-    it.buildMaterials(scene.materials)
-    it.buildBLAS(scene.meshes)
-    it.buildTLAS(scene.instances)
-    it.buildEmitters(scene.emitters)
-    it.updateCamera(scene.camera)
+    try:
+        if getattr(scene, "textures", None):
+            it.buildTextures(scene.textures)
+        it.buildMaterials(scene.materials)
+        it.buildBLAS(scene.meshes)
+        it.buildTLAS(scene.instances)
+        it.buildEmitters(scene.emitters)
+        it.updateCamera(scene.camera)
+    except BaseException:
+        it.close()  # a refused build step must not leave the integrator's device memory behind
+        raise
     return it

@@ -122,3 +122,39 @@ def test_direct_lighting_single_emitter(oracle, keep):
           f"{np.median(rel):.2e}, p99 {np.quantile(rel, 0.99):.2e}")
     assert np.isfinite(g1).all() and g1.max() > 0.0
     assert np.quantile(rel, 0.5) < 1e-4 and np.quantile(rel, 0.99) < 5e-2
+
+
+EXTREME = {
+    "conductor alpha 1e-4": scenes.Material(scenes.MAT_METAL, reflectance=(1.0, 1.0, 1.0), roughness=0.01,
+                                            eta=scenes.GOLD_ETA, k=scenes.GOLD_K),
+    "conductor alpha 1": scenes.Material(scenes.MAT_METAL, reflectance=(1.0, 1.0, 1.0), roughness=1.0,
+                                         eta=scenes.GOLD_ETA, k=scenes.GOLD_K),
+    "glass alpha 1e-4": scenes.Material(scenes.MAT_GLASS, roughness=0.01, interior_ior=1.5),
+    "glass ior 2.4": scenes.Material(scenes.MAT_GLASS, roughness=0.3, interior_ior=2.4),
+    "glass ior 1.00001": scenes.Material(scenes.MAT_GLASS, roughness=0.3, interior_ior=1.00001),
+    "black diffuse": scenes.Material(scenes.MAT_DIFFUSE, reflectance=(0.0, 0.0, 0.0)),
+}
+
+
+@pytest.mark.parametrize("name", list(EXTREME))
+@pytest.mark.parametrize("compat", [True, False])
+def test_extreme_materials(oracle, name, compat):
+    """Every sphere takes one material at the end of its parameter range (roughness 0.01 and 1, IOR near 1 and
+    2.4, zero albedo); the ground stays diffuse.  Near-specular lobes (alpha 1e-4) make per-pixel values huge in
+    the reference estimator (its pdf functions), and the same seeds still give the same paths."""
+    base = scenes.config1(0, 64, 48)
+    s = dataclasses.replace(base, materials=[base.materials[0]] + [EXTREME[name]] * (len(base.materials) - 1))
+    gflags, oflags = (cb.COMPAT_ALL, oracle.COMPAT_ALL) if compat else (0, 0)
+    gm, cm, st, cnt = _render_both(s, 8, gflags, oflags, oracle)
+    _check_same_seed(gm, cm, st, cnt, f"{name}, {'reference' if compat else 'corrected'} estimator")
+
+
+def test_index_matched_glass_is_rejected():
+    """A rough dielectric whose interior IOR equals the exterior's 1.0 has no refraction half-vector
+    (roughdielectric.h divides by |wo + eta wi| = 0); the material build refuses it instead of rendering NaN."""
+    base = scenes.config1(0, 16, 16)
+    s = dataclasses.replace(base, materials=[base.materials[0]] + [
+        scenes.Material(scenes.MAT_GLASS, roughness=0.3, interior_ior=1.0)] * (len(base.materials) - 1))
+    with pytest.raises(cb.ClError) as e:
+        cb.load_scene(s, flags=cb.COMPAT_ALL)
+    assert "IOR" in str(e.value)
