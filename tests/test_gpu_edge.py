@@ -158,3 +158,44 @@ def test_index_matched_glass_is_rejected():
     with pytest.raises(cb.ClError) as e:
         cb.load_scene(s, flags=cb.COMPAT_ALL)
     assert "IOR" in str(e.value)
+
+
+@pytest.mark.parametrize("view", ["sky", "away"])
+def test_every_camera_ray_escapes(oracle, view):
+    """A view of the sky only: every camera ray escapes (the escaped-ray class alone, no shading vertex), so the
+    film is the dome's radiance and no shadow ray is traced."""
+    base = scenes.config1(0, 48, 32)
+    pos, at = ((0.0, 3.0, 0.0), (0.0, 100.0, 0.5)) if view == "sky" else ((0.0, 3.0, -40.0), (0.0, 30.0, -100.0))
+    s = dataclasses.replace(base, camera=scenes.look_at_camera(pos, at, (0.0, 0.0, 1.0) if view == "sky" else
+                                                               (0.0, 1.0, 0.0), 45.0, 48, 32))
+    gm, cm, st, cnt = _render_both(s, 4, cb.COMPAT_ALL, oracle.COMPAT_ALL, oracle)
+    _check_same_seed(gm, cm, st, cnt, "camera looking up" if view == "sky" else "camera looking away from the scene")
+    assert int(st["rays_closest"]) == 48 * 32 * 4 and int(st["rays_shadow"]) == 0
+    assert gm.min() > 0.0
+
+
+def test_degenerate_triangles(oracle, native):
+    """Zero-area triangles (a repeated vertex, collinear vertices) mixed into the scene: the builder keeps them,
+    no ray hits them, and the image equals the scene's without them."""
+    base = scenes.config1(0, 64, 48)
+    rng = np.random.default_rng(7)
+    n = 300
+    p0 = rng.uniform(-4.0, 4.0, (n, 3)).astype(np.float32)
+    p0[:, 1] = rng.uniform(0.1, 2.0, n)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    pos = np.concatenate([p0, p0 + d, p0 + 2.0 * d]).astype(np.float32)     # collinear: v, v + d, v + 2d
+    idx = np.stack([np.arange(n), np.arange(n) + n, np.arange(n) + 2 * n], 1).astype(np.uint32)
+    idx[: n // 2, 2] = idx[: n // 2, 0]                                     # half of them: a repeated vertex
+    nv = len(pos)
+    nrm = np.tile(np.array([0, 1, 0], np.float32), (nv, 1))
+    tan = np.tile(np.array([1, 0, 0], np.float32), (nv, 1))
+    mesh = scenes.Mesh(pos, nrm, tan, np.zeros((nv, 2), np.float32), idx)
+    s = dataclasses.replace(base, meshes=base.meshes + [mesh],
+                            instances=base.instances + [(len(base.meshes), 0, scenes.IDENTITY)])
+    gm, cm, st, cnt = _render_both(s, 8, cb.COMPAT_ALL, oracle.COMPAT_ALL, oracle)
+    _check_same_seed(gm, cm, st, cnt, "300 zero-area triangles added")
+    it = cb.load_scene(base, flags=cb.COMPAT_ALL | cb.FILM_FP64)
+    it.render(8)
+    b1, _ = it.readbackFilmStats()
+    it.close()
+    assert np.allclose(gm, b1 / 8, rtol=1e-12, atol=0.0)  # FP64 film sums: atomic order only
