@@ -199,3 +199,35 @@ def test_degenerate_triangles(oracle, native):
     b1, _ = it.readbackFilmStats()
     it.close()
     assert np.allclose(gm, b1 / 8, rtol=1e-12, atol=0.0)  # FP64 film sums: atomic order only
+
+
+def _mirrored_instances_scene():
+    """Config 1 with every sphere instance under its own affine map about its centre: a rotation, scales
+    U[0.6, 1.4] per axis (ellipsoids) and, for every other sphere, a reflection (negative determinant)."""
+    base = scenes.config1(0, 64, 48)
+    rng = np.random.default_rng(11)
+    inst = [base.instances[0]]
+    for k, (mesh_id, mat, _) in enumerate(base.instances[1:]):
+        c = base.meshes[mesh_id].positions.astype(np.float64).mean(0)
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                      [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+        A = R @ np.diag(rng.uniform(0.6, 1.4, 3))
+        if k % 2 == 0:
+            A = A @ np.diag([-1.0, 1.0, 1.0])
+        M = np.concatenate([A, (c - A @ c)[:, None]], 1)
+        inst.append((mesh_id, mat, tuple(float(v) for v in M.ravel())))
+    return dataclasses.replace(base, instances=inst)
+
+
+@pytest.mark.parametrize("two_level", [False, True])
+def test_mirrored_and_anisotropic_instances(oracle, two_level):
+    """Instance transforms with reflections and unequal axis scales, flattened and as a two-level scene
+    (normals by the inverse transpose, the geometric normal flipped for a reflecting map)."""
+    s = _mirrored_instances_scene()
+    flags = cb.COMPAT_ALL | (cb.TWO_LEVEL if two_level else 0)
+    gm, cm, st, cnt = _render_both(s, 8, flags, oracle.COMPAT_ALL, oracle)
+    _check_same_seed(gm, cm, st, cnt, f"reflected, anisotropic instances, {'two-level' if two_level else 'flattened'}")
