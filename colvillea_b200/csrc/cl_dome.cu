@@ -438,8 +438,9 @@ cl_status buildDome(const float* hostTexels, int w, int h, cudaStream_t st, Dome
 // ---------------------------------------------------------------------------
 // Allocation-free variant of the dome build (cl_dome_build_tables_noalloc).
 //
-// For callers that cannot allocate device memory: code recording a CUDA
-// graph by stream capture, or hosts whose allocator owns all device memory.
+// For callers that cannot allocate device memory: hosts whose allocator owns
+// all device memory (a pool reserved at start-up), and render callbacks that
+// must not allocate.
 // The scratch of launchDomeBuild comes from one static device array instead
 // of cudaMalloc.  In host code `gDomeScratch` names a host-side stand-in, not
 // the device array, so its device address is resolved once per device with

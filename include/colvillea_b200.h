@@ -403,10 +403,11 @@ cl_status cl_dome_alias_sample(cl_integrator* integrator, const float* u2, float
 
 /* ---- Allocation-free dome preprocessing.
  * No counterpart in the reference.  For callers that cannot allocate device
- * memory: code running while a CUDA stream is being captured into a graph,
- * or hosts whose allocator owns all device memory (a memory pool handed out
- * to the renderer), where cudaMalloc is either illegal or would bypass the
- * pool.  The caller passes device buffers for the input and every output;
+ * memory: hosts whose allocator owns all device memory (a pool reserved at
+ * start-up and handed out to the renderer, where a cudaMalloc would bypass
+ * the pool's accounting or fail once the pool holds the memory), and host
+ * applications whose render callbacks must not allocate.  The caller passes
+ * device buffers for the input and every output;
  * the function allocates nothing.  Its FP64 scratch (texel weights, row
  * integrals, alias work lists) lives in one static device array of
  * CL_DOME_NOALLOC_SCRATCH_BYTES (about 12 MiB) that every GPU loading the

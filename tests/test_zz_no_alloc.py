@@ -1,8 +1,8 @@
 """cl_dome_build_tables_noalloc: the dome preprocessing for callers that cannot
 allocate device memory.
 
-Such callers (code recording a CUDA graph by stream capture, hosts whose
-allocator owns all device memory) hand in device buffers for the texels and
+Such callers (hosts whose allocator owns all device memory in a pool, render
+callbacks that must not allocate) hand in device buffers for the texels and
 every table; the function's FP64 scratch is a static device array, so it
 calls no allocator.  Here the test plays that caller: it allocates the
 buffers itself (with torch) and compares the tables of two calls in a row,
