@@ -85,3 +85,38 @@ def test_direct_lighting_runs(cfg1, oracle):
     assert np.isfinite(s1).all() and cnt[1] > 0
     p1, _, _ = os_.render(4, max_depth=1, flags=oracle.COMPAT_ALL)
     assert s1.sum() > p1.sum()  # direct light adds to the camera-ray environment term
+
+
+def test_edge_scene_properties(oracle):
+    """The checker on the edge-case scenes the GPU tests use: without emitters the film is black and no shadow
+    ray is traced; at depth 1 only camera rays are traced; zero-area triangles change no pixel; a view of the sky
+    only traces camera rays and sees the dome."""
+    import dataclasses
+    base = scenes.config1(0, 24, 16)
+    n_cam = 24 * 16 * 2
+
+    def run(s, spp=2):
+        o = oracle.OracleScene(s.flatten())
+        c1, _, cnt = o.render(spp, max_depth=s.max_depth, rr_start=s.rr_start, flags=oracle.COMPAT_ALL)
+        return c1, cnt
+
+    c1, cnt = run(dataclasses.replace(base, emitters=[]))
+    assert np.all(c1 == 0.0) and int(cnt[1]) == 0 and int(cnt[0]) == n_cam
+    c1, cnt = run(dataclasses.replace(base, max_depth=1))
+    assert int(cnt[0]) == n_cam and int(cnt[1]) == 0 and c1.max() > 0.0
+    ref, rcnt = run(base)
+    rng = np.random.default_rng(3)
+    p = rng.uniform(-3.0, 3.0, (50, 3)).astype(np.float32)
+    pos = np.concatenate([p, p + 1.0, p + 2.0]).astype(np.float32)         # collinear corners
+    idx = np.stack([np.arange(50), np.arange(50) + 50, np.arange(50) + 100], 1).astype(np.uint32)
+    nv = len(pos)
+    mesh = scenes.Mesh(pos, np.tile(np.float32([0, 1, 0]), (nv, 1)), np.tile(np.float32([1, 0, 0]), (nv, 1)),
+                       np.zeros((nv, 2), np.float32), idx)
+    deg = dataclasses.replace(base, meshes=base.meshes + [mesh],
+                              instances=base.instances + [(len(base.meshes), 0, scenes.IDENTITY)])
+    c1, cnt = run(deg)
+    assert np.array_equal(c1, ref) and np.array_equal(cnt, rcnt)
+    sky = dataclasses.replace(base, camera=scenes.look_at_camera((0.0, 3.0, 0.0), (0.0, 100.0, 0.5),
+                                                                 (0.0, 0.0, 1.0), 45.0, 24, 16))
+    c1, cnt = run(sky)
+    assert int(cnt[0]) == n_cam and int(cnt[1]) == 0 and c1.min() > 0.0
