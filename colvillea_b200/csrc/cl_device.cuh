@@ -37,7 +37,6 @@ struct f2
     float x, y;
 };
 
-__device__ __forceinline__ f3 mk3(float a, float b, float c) { return f3{a, b, c}; }
 __device__ __forceinline__ f3 operator+(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ f3 operator-(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 __device__ __forceinline__ f3 operator*(f3 a, f3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
