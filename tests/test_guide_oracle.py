@@ -189,3 +189,14 @@ def test_cache_gradients_match_finite_differences(smooth):
         lm = frozen(q)
         fd = (lp - lm) / 2e-5
         assert abs(fd - g[i]) <= 1e-6 * abs(g[i]) + 1e-8 * scale + 1e-11, (i, fd, g[i])
+
+
+@pytest.mark.parametrize("n_min,n_max", [(16, 1024), (4, 512), (16, 2048), (2, 4096), (16, 1000), (8, 8)])
+def test_library_level_resolutions_match_the_oracle(native, n_min, n_max):
+    """The library's host-side table of hash-grid resolutions (cl_guide_default_resolutions, no GPU needed)
+    equals the oracle's floor(n_min b^l), b = (n_max / n_min)^(1/15); with (16, 1024) the finest level is
+    1023 (b^15 rounds just below 64)."""
+    import colvillea_b200 as cb
+    r = cb.default_resolutions(n_min, n_max).astype(np.int64)
+    np.testing.assert_array_equal(r, G.resolutions(n_min, n_max))
+    assert np.all(np.diff(r) >= 0) and r[0] == n_min
