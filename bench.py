@@ -250,25 +250,29 @@ def ncu_traffic(config=2):
 
 
 def _oracle_rate(o, scene, seconds, threads):
-    """Paths per second of the oracle at `threads` host threads, 1 spp over an
-    evenly strided pixel sample sized to about `seconds` of work."""
+    """Paths per second of the oracle at `threads` host threads over an evenly
+    strided pixel sample sized to about `seconds` of work: 1 spp over part of
+    the image, or several spp over all of it.  A pass shorter than half the
+    target is rescaled from its own time and run again; the last pass is the
+    one reported."""
     import numpy as np
     import pyoracle
     npx = scene.width * scene.height
-    probe = np.arange(0, npx, max(1, npx // (2000 if threads > 1 else 400)), dtype=np.uint32)
-    t0 = time.perf_counter()
-    o.render(1, max_depth=scene.max_depth, rr_start=scene.rr_start, flags=pyoracle.COMPAT_ALL, pixels=probe,
-             threads=threads)
-    dt = max(time.perf_counter() - t0, 1e-3)
-    want = int(min(npx, max(1000, len(probe) * seconds / dt)))
-    pix = np.linspace(0, npx - 1, want).astype(np.uint32)
-    t0 = time.perf_counter()
-    _, _, cnt = o.render(1, max_depth=scene.max_depth, rr_start=scene.rr_start, flags=pyoracle.COMPAT_ALL,
-                         pixels=pix, threads=threads)
-    dt = time.perf_counter() - t0
-    sample = (f"{len(pix)} of {npx} pixels (evenly strided), 1 spp, {dt:.1f} s; {int(cnt[0])} closest + "
+    want, spp = min(npx, 2000 if threads > 1 else 400), 1
+    while True:
+        pix = np.linspace(0, npx - 1, want).astype(np.uint32)
+        t0 = time.perf_counter()
+        _, _, cnt = o.render(spp, max_depth=scene.max_depth, rr_start=scene.rr_start, flags=pyoracle.COMPAT_ALL,
+                             pixels=pix, threads=threads)
+        dt = max(time.perf_counter() - t0, 1e-4)
+        if dt >= 0.5 * seconds or (want == npx and spp >= 64):
+            break
+        paths = int(len(pix) * spp * min(seconds / dt, 1000.0))   # paths for about `seconds` at this pass's rate
+        want = min(npx, max(want, paths))
+        spp = min(64, max(1, -(-paths // npx)))
+    sample = (f"{len(pix)} of {npx} pixels (evenly strided), {spp} spp, {dt:.1f} s; {int(cnt[0])} closest + "
               f"{int(cnt[1])} shadow rays ({(cnt[0] + cnt[1]) / dt / 1e6:.3f} Mrays/s)")
-    return round(len(pix) / dt / 1e6, 6), sample
+    return round(len(pix) * spp / dt / 1e6, 6), sample
 
 
 def cpu_baseline(scene, seconds, threads):
